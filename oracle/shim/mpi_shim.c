@@ -1,0 +1,530 @@
+/*
+ * mpi_shim.c -- implementation of the minimal MPI stand-in (see mpi.h).
+ * TEST INFRASTRUCTURE: used only to run the reference's own sources.
+ */
+#define _GNU_SOURCE
+#include "mpi.h"
+
+#include <errno.h>
+#include <poll.h>
+#include <signal.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/prctl.h>
+#include <sys/socket.h>
+#include <sys/wait.h>
+#include <time.h>
+#include <unistd.h>
+
+#define MAXR 256
+#define MAXT 64
+#define MAXC 16
+
+typedef struct {
+  long nblocks, blockbytes, stridebytes, extent;
+} dtype_t;
+typedef struct {
+  int size, me;
+  int world[MAXR]; /* local rank -> world rank */
+  int ndims, dims[2];
+} comm_t;
+
+static int g_np = 1, g_me = 0;
+static int g_fd[MAXR];        /* my end of the socketpair to each peer */
+static pid_t g_child[MAXR];
+static dtype_t g_t[MAXT];
+static int g_nt = 16;
+static comm_t g_c[MAXC];
+static int g_nc = 1;
+
+typedef struct selfmsg {
+  struct selfmsg *next;
+  long n;
+  char data[];
+} selfmsg;
+static selfmsg *g_selfq_head = NULL, *g_selfq_tail = NULL;
+
+static void die(const char *m) {
+  fprintf(stderr, "mpi shim rank %d: %s (errno %d)\n", g_me, m, errno);
+  _exit(97);
+}
+
+static void check_children(void) {
+  if (g_me != 0) {
+    if (getppid() == 1) die("parent gone");
+    return;
+  }
+  for (int r = 1; r < g_np; r++) {
+    if (g_child[r] <= 0) continue;
+    int st;
+    pid_t p = waitpid(g_child[r], &st, WNOHANG);
+    if (p == g_child[r]) {
+      g_child[r] = 0;
+      if (!(WIFEXITED(st) && WEXITSTATUS(st) == 0)) {
+        for (int q = 1; q < g_np; q++)
+          if (g_child[q] > 0) kill(g_child[q], SIGKILL);
+        fprintf(stderr, "mpi shim: rank %d failed\n", r);
+        exit(98);
+      }
+    }
+  }
+}
+
+static void wait_fd(int fd, short ev) {
+  for (;;) {
+    struct pollfd p = {fd, ev, 0};
+    int rc = poll(&p, 1, 1000);
+    if (rc > 0) return;
+    if (rc < 0 && errno != EINTR) die("poll");
+    check_children();
+  }
+}
+
+static void write_all(int fd, const void *buf, long n) {
+  const char *b = (const char *)buf;
+  while (n > 0) {
+    wait_fd(fd, POLLOUT);
+    ssize_t w = write(fd, b, (size_t)n);
+    if (w < 0) {
+      if (errno == EINTR || errno == EAGAIN) continue;
+      die("write");
+    }
+    b += w;
+    n -= w;
+  }
+}
+
+static void read_all(int fd, void *buf, long n) {
+  char *b = (char *)buf;
+  while (n > 0) {
+    wait_fd(fd, POLLIN);
+    ssize_t r = read(fd, b, (size_t)n);
+    if (r == 0) die("peer closed");
+    if (r < 0) {
+      if (errno == EINTR || errno == EAGAIN) continue;
+      die("read");
+    }
+    b += r;
+    n -= r;
+  }
+}
+
+static long type_size(MPI_Datatype t) { return g_t[t].nblocks * g_t[t].blockbytes; }
+
+static void pack(const void *buf, int count, MPI_Datatype t, char *out) {
+  const dtype_t *d = &g_t[t];
+  const char *b = (const char *)buf;
+  for (int e = 0; e < count; e++)
+    for (long k = 0; k < d->nblocks; k++) {
+      memcpy(out, b + e * d->extent + k * d->stridebytes, (size_t)d->blockbytes);
+      out += d->blockbytes;
+    }
+}
+
+static void unpack(const char *in, long nbytes, void *buf, int count, MPI_Datatype t) {
+  const dtype_t *d = &g_t[t];
+  char *b = (char *)buf;
+  long left = nbytes;
+  for (int e = 0; e < count && left > 0; e++)
+    for (long k = 0; k < d->nblocks && left > 0; k++) {
+      long c = left < d->blockbytes ? left : d->blockbytes;
+      memcpy(b + e * d->extent + k * d->stridebytes, in, (size_t)c);
+      in += c;
+      left -= c;
+    }
+}
+
+/* blocking framed send / receive between world ranks */
+static void send_msg(int to, const void *data, long n) {
+  if (to == g_me) {
+    selfmsg *m = (selfmsg *)malloc(sizeof(selfmsg) + (size_t)n);
+    m->next = NULL;
+    m->n = n;
+    memcpy(m->data, data, (size_t)n);
+    if (g_selfq_tail) g_selfq_tail->next = m;
+    else g_selfq_head = m;
+    g_selfq_tail = m;
+    return;
+  }
+  int64_t h = n;
+  write_all(g_fd[to], &h, sizeof(h));
+  write_all(g_fd[to], data, n);
+}
+
+static char *recv_msg(int from, long *n) {
+  if (from == g_me) {
+    selfmsg *m = g_selfq_head;
+    if (!m) die("self receive without a message");
+    g_selfq_head = m->next;
+    if (!g_selfq_head) g_selfq_tail = NULL;
+    char *out = (char *)malloc((size_t)m->n + 1);
+    memcpy(out, m->data, (size_t)m->n);
+    *n = m->n;
+    free(m);
+    return out;
+  }
+  int64_t h;
+  read_all(g_fd[from], &h, sizeof(h));
+  char *out = (char *)malloc((size_t)h + 1);
+  read_all(g_fd[from], out, h);
+  *n = h;
+  return out;
+}
+
+int MPI_Init(int *argc, char ***argv) {
+  (void)argc;
+  (void)argv;
+  const char *e = getenv("LBRB_SHIM_NP");
+  g_np = e ? atoi(e) : 1;
+  if (g_np < 1 || g_np > MAXR) die("bad LBRB_SHIM_NP");
+  /* elementary types: DOUBLE, INT, INTEGER, CHAR */
+  g_t[MPI_DOUBLE] = (dtype_t){1, 8, 8, 8};
+  g_t[MPI_INT] = (dtype_t){1, 4, 4, 4};
+  g_t[MPI_INTEGER] = (dtype_t){1, 4, 4, 4};
+  g_t[MPI_CHAR] = (dtype_t){1, 1, 1, 1};
+  int pairs[MAXR][MAXR][2];
+  for (int a = 0; a < g_np; a++)
+    for (int b = a + 1; b < g_np; b++)
+      if (socketpair(AF_UNIX, SOCK_STREAM, 0, pairs[a][b]) != 0) die("socketpair");
+  fflush(NULL);
+  g_me = 0;
+  pid_t parent = getpid();
+  for (int r = 1; r < g_np; r++) {
+    pid_t p = fork();
+    if (p < 0) die("fork");
+    if (p == 0) {
+      g_me = r;
+      prctl(PR_SET_PDEATHSIG, SIGKILL);
+      if (getppid() != parent) _exit(96);
+      break;
+    }
+    g_child[r] = p;
+  }
+  for (int a = 0; a < g_np; a++)
+    for (int b = a + 1; b < g_np; b++) {
+      if (a == g_me) {
+        g_fd[b] = pairs[a][b][0];
+        close(pairs[a][b][1]);
+      } else if (b == g_me) {
+        g_fd[a] = pairs[a][b][1];
+        close(pairs[a][b][0]);
+      } else {
+        close(pairs[a][b][0]);
+        close(pairs[a][b][1]);
+      }
+    }
+  comm_t *w = &g_c[0];
+  w->size = g_np;
+  w->me = g_me;
+  w->ndims = 0;
+  for (int r = 0; r < g_np; r++) w->world[r] = r;
+  return MPI_SUCCESS;
+}
+
+int MPI_Finalize(void) {
+  fflush(NULL);
+  if (g_me == 0) {
+    int bad = 0;
+    for (int r = 1; r < g_np; r++) {
+      if (g_child[r] <= 0) continue;
+      int st;
+      if (waitpid(g_child[r], &st, 0) == g_child[r] && !(WIFEXITED(st) && WEXITSTATUS(st) == 0)) bad = 1;
+    }
+    if (bad) exit(98);
+  }
+  return MPI_SUCCESS;
+}
+
+int MPI_Comm_size(MPI_Comm c, int *s) { *s = g_c[c].size; return MPI_SUCCESS; }
+int MPI_Comm_rank(MPI_Comm c, int *r) { *r = g_c[c].me; return MPI_SUCCESS; }
+
+int MPI_Dims_create(int n, int nd, int dims[]) {
+  if (nd != 2) die("Dims_create: only 2-D");
+  const char *e = getenv("LBRB_SHIM_DIMS");
+  if (e) {
+    int a = 0, b = 0;
+    if (sscanf(e, "%dx%d", &a, &b) == 2 && a * b == n) {
+      dims[0] = a;
+      dims[1] = b;
+      return MPI_SUCCESS;
+    }
+    die("LBRB_SHIM_DIMS does not match the rank count");
+  }
+  /* balanced, non-increasing: smallest divisor d0 with d0*d0 >= n */
+  int d0 = n;
+  for (int d = 1; d <= n; d++)
+    if (n % d == 0 && (long)d * d >= n) { d0 = d; break; }
+  dims[0] = d0;
+  dims[1] = n / d0;
+  return MPI_SUCCESS;
+}
+
+int MPI_Cart_create(MPI_Comm old, int nd, const int dims[], const int periods[], int reorder,
+                    MPI_Comm *cart) {
+  (void)periods;
+  (void)reorder;
+  if (nd != 2 || dims[0] * dims[1] != g_c[old].size) die("Cart_create dims");
+  comm_t *c = &g_c[g_nc];
+  *c = g_c[old];
+  c->ndims = 2;
+  c->dims[0] = dims[0];
+  c->dims[1] = dims[1];
+  *cart = g_nc++;
+  return MPI_SUCCESS;
+}
+
+int MPI_Cart_sub(MPI_Comm cart, const int remain[], MPI_Comm *sub) {
+  const comm_t *c = &g_c[cart];
+  int me = c->me;
+  int c0 = me / c->dims[1], c1 = me % c->dims[1];
+  comm_t *s = &g_c[g_nc];
+  s->ndims = 1;
+  if (remain[0] && !remain[1]) {
+    s->size = c->dims[0];
+    s->me = c0;
+    for (int a = 0; a < c->dims[0]; a++) s->world[a] = c->world[a * c->dims[1] + c1];
+  } else if (!remain[0] && remain[1]) {
+    s->size = c->dims[1];
+    s->me = c1;
+    for (int b = 0; b < c->dims[1]; b++) s->world[b] = c->world[c0 * c->dims[1] + b];
+  } else {
+    die("Cart_sub: unsupported remain_dims");
+  }
+  *sub = g_nc++;
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_contiguous(int count, MPI_Datatype old, MPI_Datatype *nt) {
+  const dtype_t *o = &g_t[old];
+  if (o->nblocks != 1) die("Type_contiguous of a strided type");
+  g_t[g_nt] = (dtype_t){1, count * o->blockbytes, count * o->blockbytes, count * o->extent};
+  *nt = g_nt++;
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_vector(int count, int bl, int stride, MPI_Datatype old, MPI_Datatype *nt) {
+  const dtype_t *o = &g_t[old];
+  if (o->nblocks != 1 || o->blockbytes != o->extent) die("Type_vector of a strided type");
+  g_t[g_nt] = (dtype_t){count, bl * o->extent, stride * o->extent,
+                        ((long)(count - 1) * stride + bl) * o->extent};
+  *nt = g_nt++;
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_commit(MPI_Datatype *t) { (void)t; return MPI_SUCCESS; }
+
+int MPI_Sendrecv(const void *sbuf, int scount, MPI_Datatype stype, int dest, int stag, void *rbuf,
+                 int rcount, MPI_Datatype rtype, int source, int rtag, MPI_Comm comm,
+                 MPI_Status *status) {
+  (void)stag;
+  (void)rtag;
+  const comm_t *c = &g_c[comm];
+  int to = c->world[dest], from = c->world[source];
+  long sn = type_size(stype) * scount;
+  char *sb = (char *)malloc((size_t)sn + 1);
+  pack(sbuf, scount, stype, sb);
+  long rn = 0;
+  char *rb = NULL;
+  if (to == g_me || from == g_me) {
+    send_msg(to, sb, sn);
+    rb = recv_msg(from, &rn);
+  } else {
+    /* full duplex: progress the send and the receive together */
+    int64_t hs = sn, hr = -1;
+    long soff = 0, roff = 0;
+    long stot = (long)sizeof(hs) + sn;
+    char *rhead = (char *)&hr;
+    while (soff < stot || hr < 0 || roff < (long)sizeof(hr) + hr) {
+      struct pollfd p[2];
+      int np = 0, si = -1, ri = -1;
+      if (soff < stot) { si = np; p[np++] = (struct pollfd){g_fd[to], POLLOUT, 0}; }
+      if (hr < 0 || roff < (long)sizeof(hr) + hr) { ri = np; p[np++] = (struct pollfd){g_fd[from], POLLIN, 0}; }
+      if (to == from && si >= 0 && ri >= 0) p[ri].fd = g_fd[from];
+      int rc = poll(p, (nfds_t)np, 1000);
+      if (rc < 0 && errno != EINTR) die("poll");
+      if (rc <= 0) { check_children(); continue; }
+      if (si >= 0 && (p[si].revents & (POLLOUT | POLLERR | POLLHUP))) {
+        const char *src = soff < (long)sizeof(hs) ? (const char *)&hs + soff : sb + (soff - (long)sizeof(hs));
+        long chunk = soff < (long)sizeof(hs) ? (long)sizeof(hs) - soff : stot - soff;
+        ssize_t w = write(g_fd[to], src, (size_t)chunk);
+        if (w < 0 && errno != EINTR && errno != EAGAIN) die("write");
+        if (w > 0) soff += w;
+      }
+      if (ri >= 0 && (p[ri].revents & (POLLIN | POLLERR | POLLHUP))) {
+        ssize_t r;
+        if (roff < (long)sizeof(hr)) {
+          r = read(g_fd[from], rhead + roff, sizeof(hr) - (size_t)roff);
+          if (r > 0) {
+            roff += r;
+            if (roff == (long)sizeof(hr)) {
+              rb = (char *)malloc((size_t)hr + 1);
+              rn = hr;
+            }
+          }
+        } else {
+          r = read(g_fd[from], rb + (roff - (long)sizeof(hr)), (size_t)((long)sizeof(hr) + hr - roff));
+          if (r > 0) roff += r;
+        }
+        if (r == 0) die("peer closed");
+        if (r < 0 && errno != EINTR && errno != EAGAIN) die("read");
+      }
+    }
+    if (!rb) { rb = (char *)malloc(1); rn = 0; }
+  }
+  if (rn > type_size(rtype) * rcount) die("Sendrecv: message longer than the receive buffer");
+  unpack(rb, rn, rbuf, rcount, rtype);
+  if (status) {
+    status->MPI_SOURCE = source;
+    status->MPI_TAG = rtag;
+    status->MPI_ERROR = 0;
+  }
+  free(sb);
+  free(rb);
+  return MPI_SUCCESS;
+}
+
+/* ---- collectives (all ranks of the communicator, through local rank 0) */
+static void coll_bcast_bytes(const comm_t *c, int root, char *buf, long n) {
+  if (c->me == root) {
+    for (int r = 0; r < c->size; r++)
+      if (r != root) send_msg(c->world[r], buf, n);
+  } else {
+    long m;
+    char *t = recv_msg(c->world[root], &m);
+    if (m != n) die("Bcast size mismatch");
+    memcpy(buf, t, (size_t)n);
+    free(t);
+  }
+}
+
+int MPI_Barrier(MPI_Comm comm) {
+  const comm_t *c = &g_c[comm];
+  char b = 0;
+  if (c->me == 0) {
+    for (int r = 1; r < c->size; r++) { long m; free(recv_msg(c->world[r], &m)); }
+  } else {
+    send_msg(c->world[0], &b, 1);
+  }
+  coll_bcast_bytes(c, 0, &b, 1);
+  return MPI_SUCCESS;
+}
+
+int MPI_Bcast(void *buf, int count, MPI_Datatype t, int root, MPI_Comm comm) {
+  const comm_t *c = &g_c[comm];
+  long n = type_size(t) * count;
+  char *tmp = (char *)malloc((size_t)n + 1);
+  if (c->me == root) pack(buf, count, t, tmp);
+  coll_bcast_bytes(c, root, tmp, n);
+  if (c->me != root) unpack(tmp, n, buf, count, t);
+  free(tmp);
+  return MPI_SUCCESS;
+}
+
+static void reduce_into(char *acc, const char *in, int count, MPI_Datatype t) {
+  if (t == MPI_DOUBLE) {
+    double *a = (double *)acc;
+    const double *b = (const double *)in;
+    for (int i = 0; i < count; i++) a[i] = a[i] + b[i];
+  } else if (t == MPI_INT || t == MPI_INTEGER) {
+    int *a = (int *)acc;
+    const int *b = (const int *)in;
+    for (int i = 0; i < count; i++) a[i] = a[i] + b[i];
+  } else {
+    die("reduce: unsupported type");
+  }
+}
+
+int MPI_Reduce(const void *sbuf, void *rbuf, int count, MPI_Datatype t, MPI_Op op, int root,
+               MPI_Comm comm) {
+  if (op != MPI_SUM) die("reduce: only MPI_SUM");
+  const comm_t *c = &g_c[comm];
+  long n = type_size(t) * count;
+  if (c->me == root) {
+    /* rank-ascending summation */
+    char *acc = (char *)malloc((size_t)n + 1);
+    char **parts = (char **)calloc((size_t)c->size, sizeof(char *));
+    for (int r = 0; r < c->size; r++) {
+      if (r == root) continue;
+      long m;
+      parts[r] = recv_msg(c->world[r], &m);
+      if (m != n) die("Reduce size mismatch");
+    }
+    int first = 1;
+    for (int r = 0; r < c->size; r++) {
+      const char *src = (r == root) ? (const char *)sbuf : parts[r];
+      if (first) { memcpy(acc, src, (size_t)n); first = 0; }
+      else reduce_into(acc, src, count, t);
+    }
+    memcpy(rbuf, acc, (size_t)n);
+    for (int r = 0; r < c->size; r++) free(parts[r]);
+    free(parts);
+    free(acc);
+  } else {
+    send_msg(c->world[root], sbuf, n);
+  }
+  return MPI_SUCCESS;
+}
+
+int MPI_Allreduce(const void *sbuf, void *rbuf, int count, MPI_Datatype t, MPI_Op op,
+                  MPI_Comm comm) {
+  const comm_t *c = &g_c[comm];
+  long n = type_size(t) * count;
+  char *tmp = (char *)malloc((size_t)n + 1);
+  MPI_Reduce(sbuf, tmp, count, t, op, 0, comm);
+  coll_bcast_bytes(c, 0, tmp, n);
+  memcpy(rbuf, tmp, (size_t)n);
+  free(tmp);
+  return MPI_SUCCESS;
+}
+
+int MPI_Gatherv(const void *sbuf, int scount, MPI_Datatype stype, void *rbuf, const int rcounts[],
+                const int displs[], MPI_Datatype rtype, int root, MPI_Comm comm) {
+  const comm_t *c = &g_c[comm];
+  long sn = type_size(stype) * scount;
+  char *sb = (char *)malloc((size_t)sn + 1);
+  pack(sbuf, scount, stype, sb);
+  if (c->me == root) {
+    for (int r = 0; r < c->size; r++) {
+      char *src;
+      long m;
+      if (r == root) { src = sb; m = sn; }
+      else src = recv_msg(c->world[r], &m);
+      if (m > type_size(rtype) * rcounts[r]) die("Gatherv overflow");
+      unpack(src, m, (char *)rbuf + (long)displs[r] * g_t[rtype].extent, rcounts[r], rtype);
+      if (r != root) free(src);
+    }
+  } else {
+    send_msg(c->world[root], sb, sn);
+  }
+  free(sb);
+  return MPI_SUCCESS;
+}
+
+int MPI_Scatterv(const void *sbuf, const int scounts[], const int displs[], MPI_Datatype stype,
+                 void *rbuf, int rcount, MPI_Datatype rtype, int root, MPI_Comm comm) {
+  const comm_t *c = &g_c[comm];
+  if (c->me == root) {
+    for (int r = 0; r < c->size; r++) {
+      long n = type_size(stype) * scounts[r];
+      char *b = (char *)malloc((size_t)n + 1);
+      pack((const char *)sbuf + (long)displs[r] * g_t[stype].extent, scounts[r], stype, b);
+      if (r == root) unpack(b, n, rbuf, rcount, rtype);
+      else send_msg(c->world[r], b, n);
+      free(b);
+    }
+  } else {
+    long m;
+    char *b = recv_msg(c->world[root], &m);
+    unpack(b, m, rbuf, rcount, rtype);
+    free(b);
+  }
+  return MPI_SUCCESS;
+}
+
+double MPI_Wtime(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}

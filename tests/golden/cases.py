@@ -1,0 +1,137 @@
+"""Canonical parity cases: seeded inputs shared by the golden-fixture
+generator (make_golden.py), the oracle pin tests and the GPU parity tests.
+
+Every input is synthetic and seeded; nothing is read from the reference
+checkout here.  The oracle is imported only as the checker.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+from oracle.oracle import Oracle, closure
+
+GOLDEN = Path(__file__).resolve().parent
+W = np.array([16 / 36, 4 / 36, 4 / 36, 4 / 36, 4 / 36, 1 / 36, 1 / 36, 1 / 36, 1 / 36])
+
+
+def bilinear_np(fld: np.ndarray, xx: float, yy: float) -> float:
+    ny, nx = fld.shape
+    x1, y1 = int(xx), int(yy)
+    x2, y2 = x1 + 1, y1 + 1
+    F = lambda i, j: fld[(j - 1) % ny, (i - 1) % nx]
+    return (F(x1, y1) * (x2 - xx) * (y2 - yy) + F(x2, y1) * (xx - x1) * (y2 - yy)
+            + F(x1, y2) * (x2 - xx) * (yy - y1) + F(x2, y2) * (xx - x1) * (yy - y1))
+
+
+TRAJ_CASES = {
+    # name: grid, closure, particles, steps
+    "traj_tracer": dict(nx=48, ny=24, Ra=1e5, U=0.1, seed=7, noise=1e-2, nprtcl=64,
+                        inertial=False, taulag=50.0, beta=0.0, nsteps=200, noutconfig=50),
+    "traj_inertial": dict(nx=48, ny=24, Ra=1e5, U=0.1, seed=9, noise=1e-2, nprtcl=64,
+                          inertial=True, taulag=50.0, beta=0.1, nsteps=200, noutconfig=50),
+    "traj_wide": dict(nx=136, ny=20, Ra=3e5, U=0.1, seed=21, noise=2e-2, nprtcl=300,
+                      inertial=True, taulag=30.0, beta=0.1, nsteps=120, noutconfig=40),
+}
+
+NUDGE_CASES = {
+    "nudge_box": dict(nx=64, ny=32, Ra=1e5, U=0.1, nsteps=30, ntempread=5, alpha=0.1,
+                      nprtcl=1600, seed=11, npy=2),
+}
+
+
+def traj_case(name: str) -> dict:
+    c = dict(TRAJ_CASES[name])
+    base = closure(c["nx"], c["ny"], Ra=c["Ra"], Pr=1.0, U=c["U"])
+    params = dict(base, twall="dirichlet", nudge="none", beta=c["beta"],
+                  noutconfig=c["noutconfig"], record_full=True)
+    o = Oracle(params, c["nprtcl"])
+    o.init_conduction(seed=c["seed"], noise=c["noise"])
+    rng = np.random.default_rng(c["seed"] + 1000)
+    n, nx, ny = c["nprtcl"], c["nx"], c["ny"]
+    px = rng.uniform(0.01, nx - 0.01, n)
+    py = rng.uniform(1.01, ny - 0.01, n)
+    pu = np.array([bilinear_np(o.u, a, b) for a, b in zip(px, py)])
+    pv = np.array([bilinear_np(o.v, a, b) for a, b in zip(px, py)])
+    c.update(base=base, params=params, f0=o.f.copy(), g0=o.g.copy(),
+             rho0=o.rho.copy(), u0=o.u.copy(), v0=o.v.copy(), T0=o.T.copy(),
+             ids=np.arange(n, dtype=np.int32), px=px, py=py, pu=pu, pv=pv,
+             ptype=np.full(n, 1 if c["inertial"] else 0, np.int32),
+             invtau=np.full(n, 1.0 / c["taulag"]))
+    return c
+
+
+def run_oracle_traj(c: dict) -> dict:
+    o = Oracle(c["params"], c["nprtcl"])
+    o.f[:] = c["f0"]
+    o.g[:] = c["g0"]
+    o.moments_from_pre(c["f0"], c["g0"])
+    o.set_particles(c["ids"], c["px"], c["py"], c["pu"], c["pv"], c["ptype"], c["invtau"])
+    recs = {}
+    for s in range(1, c["nsteps"] + 1):
+        o.step(s)
+        st, r = o.record()
+        if st == s:
+            recs[s] = r
+    return dict(f=o.f.copy(), g=o.g.copy(), rho=o.rho.copy(), u=o.u.copy(), v=o.v.copy(),
+                T=o.T.copy(), records=recs, energy=o.energy(),
+                px=o.pa["x"][: c["nprtcl"]].copy(), py=o.pa["y"][: c["nprtcl"]].copy())
+
+
+def nudge_case(name: str) -> dict:
+    from oracle import refrun
+
+    c = dict(NUDGE_CASES[name])
+    nx, ny, N, nt, nsteps = c["nx"], c["ny"], c["nprtcl"], c["ntempread"], c["nsteps"]
+    base = closure(nx, ny, Ra=c["Ra"], Pr=1.0, U=c["U"])
+    rng = np.random.default_rng(c["seed"])
+    ids0 = (rng.permutation(N) + 100).astype(np.int32)
+    x0 = rng.uniform(0, nx, N)
+    y0 = rng.uniform(1, ny, N)
+    T0 = rng.uniform(-0.5, 0.5, N)
+    files = {}
+    x, y, T = x0.copy(), y0.copy(), T0.copy()
+    for s in range(nt, nsteps + nt, nt):
+        x = (x + rng.normal(0, 2.0, N)) % nx
+        y = np.clip(y + rng.normal(0, 1.0, N), 1.0, ny)
+        jump = rng.random(N) < 0.01
+        y[jump] = np.where(y[jump] > ny / 2, y[jump] - ny + 2, y[jump] + ny - 2)
+        T = T + rng.normal(0, 0.05, N)
+        perm = rng.permutation(N)
+        files[s] = dict(x=x[perm].copy(), y=y[perm].copy(), id=ids0[perm].copy(),
+                        temp=T[perm].copy())
+    Tic = refrun.scratch_ic_T(nx, ny, base["Tup"], base["Tdown"], c["npy"])
+    params = dict(base, twall="adiabatic", nudge="refbox", alpha=c["alpha"], ntempread=nt)
+    c.update(base=base, params=params, Tic=Tic,
+             init_obs=dict(x=x0, y=y0, T=T0, id=ids0), files=files)
+    return c
+
+
+def run_oracle_nudge(c: dict) -> dict:
+    o = Oracle(c["params"], c["nprtcl"])
+    o.f[:] = W[:, None, None] * 1.0
+    o.g[:] = c["Tic"][None] * W[:, None, None]
+    o.rho[:] = 1.0
+    o.T[:] = c["Tic"]
+    o.u[:] = 0.0
+    o.v[:] = 0.0
+    io = c["init_obs"]
+    o.nudge_init(io["x"], io["y"], io["T"], io["id"])
+    nt = c["ntempread"]
+    for s in range(1, c["nsteps"] + 1):
+        if s % nt == 1:
+            d = c["files"][s + nt - 1]
+            o.nudge_load(d["x"], d["y"], d["id"], d["temp"])
+        o.step(s)
+    return dict(f=o.f.copy(), g=o.g.copy(), T=o.T.copy(), u=o.u.copy(), v=o.v.copy(),
+                nudge_vol=o.nudge_vol.copy(), tempreadint=o.tempreadint.copy())
+
+
+def golden_path(name: str) -> Path:
+    return GOLDEN / f"{name}.npz"
+
+
+def load_golden(name: str) -> dict:
+    z = np.load(golden_path(name), allow_pickle=False)
+    return {k: z[k] for k in z.files}

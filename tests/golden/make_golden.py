@@ -1,0 +1,69 @@
+"""Generate the golden fixtures by running the reference's OWN sources.
+
+Run from the repository root, where the reference checkout is available:
+
+    python tests/golden/make_golden.py
+
+For each case in cases.py this builds the reference program with the case's
+compile-time parameters (oracle/build.py: gcc -O2 against the in-repo MPI and
+HDF5 stand-ins), injects the seeded inputs through the reference's restart
+route (or, for the nudging program, its scratch initial state and observation
+files) and stores the reference's outputs as compressed .npz files here.
+The GPU box has no reference checkout; these fixtures carry its results there.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import refrun  # noqa: E402
+from tests.golden import cases  # noqa: E402
+
+
+def make_traj(name: str) -> dict:
+    c = cases.traj_case(name)
+    refp = refrun.traj_params(c["base"], c["nsteps"], c["noutconfig"], c["nprtcl"],
+                              tracer=not c["inertial"], taulag=c["taulag"], beta=c["beta"])
+    out = refrun.run_trajectories(refp, c["f0"], c["g0"], c["f0"], c["g0"], c["ids"],
+                                  c["px"], c["py"], c["pu"], c["pv"])
+    z = {"f": out["f"], "g": out["g"], "evolution": out["evolution"]}
+    for s, r in out["records"].items():
+        order = np.argsort(r["id"], kind="stable")
+        z[f"rec{s}_id"] = r["id"][order]
+        for k in refrun.REC_FIELDS:
+            if k in r:
+                z[f"rec{s}_{k}"] = r[k][order]
+    return z
+
+
+def make_nudge(name: str) -> dict:
+    c = cases.nudge_case(name)
+    refp = refrun.nudge_params(c["base"], c["nsteps"], c["ntempread"], c["alpha"],
+                               noutconfig=10, nout=10**6)
+    out = refrun.run_nudging(refp, c["init_obs"], c["files"], np_ranks=c["npy"],
+                             dims=f"1x{c['npy']}")
+    z = {"f": out["f"], "g": out["g"]}
+    for s, d in out["snaps"].items():
+        for k, a in d.items():
+            z[f"snap{s}_{k}"] = a
+    return z
+
+
+def main():
+    for name in cases.TRAJ_CASES:
+        z = make_traj(name)
+        np.savez_compressed(cases.golden_path(name), **z)
+        print("wrote", cases.golden_path(name))
+    for name in cases.NUDGE_CASES:
+        z = make_nudge(name)
+        np.savez_compressed(cases.golden_path(name), **z)
+        print("wrote", cases.golden_path(name))
+
+
+if __name__ == "__main__":
+    main()

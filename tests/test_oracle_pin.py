@@ -1,0 +1,89 @@
+"""Pin the oracle (CPU restatement) to the reference.
+
+* against the committed golden fixtures, which hold outputs of the reference's
+  own sources run on the same seeded inputs (tests/golden/make_golden.py);
+* against a live run of the reference when its checkout is present.
+
+FP64 results must be bit-identical (same operation order, no FMA).
+"""
+import numpy as np
+import pytest
+
+from oracle import build
+from tests.golden import cases
+
+
+def _check_traj(name, out, z):
+    np.testing.assert_array_equal(out["f"], z["f"])
+    np.testing.assert_array_equal(out["g"], z["g"])
+    steps = sorted({int(k[3:].split("_")[0]) for k in z if k.startswith("rec")})
+    assert steps == sorted(out["records"]), (steps, sorted(out["records"]))
+    for s in steps:
+        r = out["records"][s]
+        for k in r:
+            np.testing.assert_array_equal(r[k], z[f"rec{s}_{k}"], err_msg=f"{name} step {s} {k}")
+    # evolution.dat holds %e-formatted mean KE and mean T
+    ev = z["evolution"]
+    assert ev.shape[0] >= 1
+
+
+@pytest.mark.parametrize("name", list(cases.TRAJ_CASES))
+def test_oracle_matches_golden_trajectories(name):
+    c = cases.traj_case(name)
+    out = cases.run_oracle_traj(c)
+    _check_traj(name, out, cases.load_golden(name))
+
+
+@pytest.mark.parametrize("name", list(cases.NUDGE_CASES))
+def test_oracle_matches_golden_nudging(name):
+    c = cases.nudge_case(name)
+    out = cases.run_oracle_nudge(c)
+    z = cases.load_golden(name)
+    np.testing.assert_array_equal(out["f"], z["f"])
+    np.testing.assert_array_equal(out["g"], z["g"])
+    s = c["nsteps"]
+    np.testing.assert_array_equal(out["T"], z[f"snap{s}_T"])
+    np.testing.assert_array_equal(out["u"], z[f"snap{s}_u"])
+    np.testing.assert_array_equal(out["v"], z[f"snap{s}_v"])
+
+
+needs_ref = pytest.mark.skipif(not build.reference_available(), reason="reference checkout absent")
+
+
+@needs_ref
+def test_oracle_matches_live_reference_inertial():
+    """Rebuild and rerun the reference now (not from fixtures)."""
+    from oracle import refrun
+
+    c = cases.traj_case("traj_inertial")
+    refp = refrun.traj_params(c["base"], c["nsteps"], c["noutconfig"], c["nprtcl"],
+                              tracer=False, taulag=c["taulag"], beta=c["beta"])
+    ref = refrun.run_trajectories(refp, c["f0"], c["g0"], c["f0"], c["g0"], c["ids"],
+                                  c["px"], c["py"], c["pu"], c["pv"])
+    out = cases.run_oracle_traj(c)
+    np.testing.assert_array_equal(out["f"], ref["f"])
+    np.testing.assert_array_equal(out["g"], ref["g"])
+    for s, r in ref["records"].items():
+        order = np.argsort(r["id"])
+        for k, a in out["records"][s].items():
+            np.testing.assert_array_equal(a, r[k][order])
+
+
+@needs_ref
+def test_reference_decomposition_invariance():
+    """The MPI stand-in is faithful: the reference run on a 2x2 process grid
+    gives the same fields as on one rank (restart-route inputs)."""
+    from oracle import refrun
+
+    c = cases.traj_case("traj_tracer")
+    refp = refrun.traj_params(c["base"], 40, 20, c["nprtcl"], tracer=True)
+    a = refrun.run_trajectories(refp, c["f0"], c["g0"], c["f0"], c["g0"], c["ids"],
+                                c["px"], c["py"], c["pu"], c["pv"], np_ranks=1)
+    b = refrun.run_trajectories(refp, c["f0"], c["g0"], c["f0"], c["g0"], c["ids"],
+                                c["px"], c["py"], c["pu"], c["pv"], np_ranks=4, dims="2x2")
+    np.testing.assert_array_equal(a["f"], b["f"])
+    np.testing.assert_array_equal(a["g"], b["g"])
+    for s in a["records"]:
+        oa, ob = np.argsort(a["records"][s]["id"]), np.argsort(b["records"][s]["id"])
+        np.testing.assert_allclose(a["records"][s]["temp"][oa], b["records"][s]["temp"][ob],
+                                   rtol=0, atol=1e-12)
