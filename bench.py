@@ -1,0 +1,550 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 step loop on the production-trajectory workload.
+
+Workload (one GPU): 4096 x 2048 Rayleigh-Benard, Ra = 1e8, Pr = 1, U = 0.05,
+2^17 Lagrangian particles split over Stokes numbers {0 (tracer), 0.1, 0.5, 1,
+2} (26215, 26215, 26214, 26214, 26214), tau_p = St*Ny/U, beta = 0, particle
+record (x, y, u, v, xo, yo, uo, vo, T) every 20 steps.  Synthetic seeded
+initial state: linear conduction + 1e-3 uniform noise; particles uniform.
+
+One "step" = one time step of the whole loop: fused stream/collide kernel,
+particle kernel, and every 20th step a record copied to pinned host memory.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  With N > 1 (torchrun) every rank advances its
+own independent instance (different seed): weak scaling, no per-step
+collective; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NX, NY = 4096, 2048
+RA, PR, U = 1e8, 1.0, 0.05
+ST = [0.0, 0.1, 0.5, 1.0, 2.0]
+NPRTCL = 1 << 17
+NOUTCONFIG = 20
+SEED = 20240531
+WORKLOAD = (f"production trajectories: {NX}x{NY} Ra=1e8 Pr=1 U=0.05, 2^17 particles over "
+            f"St {{0,0.1,0.5,1,2}} (tau_p=St*Ny/U, beta=0), record every {NOUTCONFIG} steps")
+# algorithmic bytes per node and step of the fused kernel: 18 populations read + written
+ALG_BYTES = {"fp32": 144, "fp64": 288}
+FALLBACK_HBM_GBS = 6650.0
+REF_TAG = "bench_c1"
+REF_STEPS_CAP_S = 60.0  # bound on the reference's timed window
+
+
+def st_counts(n: int = NPRTCL) -> list[int]:
+    base, extra = divmod(n, len(ST))
+    return [base + (1 if i < extra else 0) for i in range(len(ST))]
+
+
+def particle_setup(seed: int, n: int = NPRTCL):
+    """Seeded uniform positions in the reference frame, per-particle type and 1/tau_p."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, NX, n)
+    x[x <= 0.0] = 0.5
+    y = rng.uniform(1.0, NY, n)
+    ptype = np.empty(n, np.int32)
+    invtau = np.empty(n)
+    k = 0
+    for st, c in zip(ST, st_counts(n)):
+        ptype[k:k + c] = 0 if st == 0.0 else 1
+        invtau[k:k + c] = 0.0 if st == 0.0 else U / (st * NY)
+        k += c
+    return np.arange(n, dtype=np.int32), x, y, ptype, invtau
+
+
+def bilinear_np(fld: np.ndarray, x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    ny, nx = fld.shape
+    x1 = x.astype(np.int64)
+    y1 = y.astype(np.int64)
+    ix1, ix2 = (x1 - 1) % nx, x1 % nx
+    jy1, jy2 = (y1 - 1) % ny, y1 % ny
+    wx2, wy2 = x - x1, y - y1
+    wx1, wy1 = (x1 + 1) - x, (y1 + 1) - y
+    return (fld[jy1, ix1] * wx1 * wy1 + fld[jy1, ix2] * wx2 * wy1
+            + fld[jy2, ix1] * wx1 * wy2 + fld[jy2, ix2] * wx2 * wy2)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.time(), [c.strip() for c in line.split(",")]))
+
+    def mark(self):
+        return time.time()
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0: float, t1: float) -> dict:
+        rows = [r for t, r in self.rows if t0 <= t <= t1 + 0.1] or [r for _, r in self.rows]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------- our arm
+def make_run(lb, precision: str, seed: int, device: int, slots: int):
+    base = lb.closure(NX, NY, Ra=RA, Pr=PR, U=U)
+    r = lb.Run(**base, precision=precision, twall="dirichlet", nudge="none", beta=0.0,
+               nprtcl=NPRTCL, noutconfig=NOUTCONFIG, record_full=False, record_slots=slots,
+               device=device)
+    return r, base
+
+
+def init_run(r, seed: int):
+    r.init_conduction(seed, 1e-3)
+    m = r.get_moments()
+    ids, x, y, ptype, invtau = particle_setup(seed + 1)
+    u = bilinear_np(m["u"], x, y)
+    v = bilinear_np(m["v"], x, y)
+    r.set_particles(ids, x, y, u, v, ptype, invtau)
+    return m
+
+
+def timed_steps(r, torch, steps: int, warmup: int, dist, device: int, sampler=None):
+    r.step(warmup)
+    r.sync()
+    r.drain_records()
+    stream = torch.cuda.current_stream()
+    r.set_stream(stream.cuda_stream)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    r.set_timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    e0.record(stream)
+    r.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    if dist is not None:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    timing = r.get_timing()
+    r.set_timing(False)
+    r.sync()
+    recs = r.drain_records()
+    return ms, timing, recs, (t0, t1)
+
+
+def max_over_ranks(torch, dist, v: float) -> float:
+    if dist is None:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(precision: str):
+    """DRAM bytes per node of one fused-kernel launch from the committed ncu
+    summary (profiles/lb_step_traffic.json), or None."""
+    p = ROOT / "profiles" / "lb_step_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return float(json.loads(p.read_text())[precision]["bytes_per_node"])
+    except Exception:
+        return None
+
+
+def e2e(lb, torch, precision: str, seed: int, steps: int, device: int, dist):
+    r, base = make_run(lb, precision, seed, device, steps // NOUTCONFIG + 2)
+    w = np.array([16 / 36, 4 / 36, 4 / 36, 4 / 36, 4 / 36, 1 / 36, 1 / 36, 1 / 36, 1 / 36])
+    rng = np.random.default_rng(seed)
+    j = np.arange(NY)
+    Tcol = base["Tdown"] + (base["Tup"] - base["Tdown"]) * ((j + 0.5) / NY)
+
+    def pinned(n, torch_dtype):
+        return torch.empty(n, dtype=torch_dtype, pin_memory=True).numpy()
+
+    nh = (NX + 2) * (NY + 2)
+    f = pinned(nh * 9, torch.float64).reshape(NX + 2, NY + 2, 9)
+    g = pinned(nh * 9, torch.float64).reshape(NX + 2, NY + 2, 9)
+    T = np.empty((NX + 2, NY + 2))
+    T[1:-1, 1:-1] = Tcol[None, :] + 1e-3 * (2.0 * rng.random((NX, NY)) - 1.0)
+    T[0], T[-1] = T[-2], T[1]
+    T[:, 0], T[:, -1] = T[:, -2], T[:, 1]
+    f[:] = w
+    np.multiply(T[:, :, None], w[None, None, :], out=g)
+    rho = pinned(nh, torch.float64).reshape(NX + 2, NY + 2)
+    uu = pinned(nh, torch.float64).reshape(NX + 2, NY + 2)
+    vv = pinned(nh, torch.float64).reshape(NX + 2, NY + 2)
+    Th = pinned(nh, torch.float64).reshape(NX + 2, NY + 2)
+    rho[:] = 1.0
+    uu[:] = 0.0
+    vv[:] = 0.5 * (-base["gravity"]) * T
+    Th[:] = T
+    ids, x, y, ptype, invtau = particle_setup(seed + 1)
+    pu = np.zeros(NPRTCL)
+    pv = bilinear_np(vv[1:-1, 1:-1].T.copy(), x, y)
+    out_m = [pinned(nh, torch.float64).reshape(NX + 2, NY + 2) for _ in range(4)]
+    stream = torch.cuda.current_stream()
+    r.set_stream(stream.cuda_stream)
+    nrec = steps // NOUTCONFIG
+    recbuf = pinned(max(nrec, 1) * 9 * NPRTCL, torch.float64).reshape(max(nrec, 1), 9, NPRTCL)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r.set_populations(f, g, layout="ref")
+    r.set_moments(rho, uu, vv, Th, layout="ref")
+    r.set_particles(ids, x, y, pu, pv, ptype, invtau)
+    r.step(steps)
+    import ctypes as C
+    st = np.empty(max(nrec, 1), np.int32)
+    got = C.c_int()
+    r._ck(lb.lib().lbrb_record_drain(r.h, nrec, lb._ip(st), lb._dp(recbuf), None, C.byref(got)))
+    r._ck(lb.lib().lbrb_get_moments(r.h, *[lb._dp(a) for a in out_m], lb.LAYOUT["ref"]))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    h2d = 2 * f.nbytes + 4 * rho.nbytes + NPRTCL * (4 * 8 + 4 + 4 + 8)
+    d2h = got.value * 9 * NPRTCL * 8 + 4 * rho.nbytes
+    r.close()
+    return ms, h2d, d2h
+
+
+def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | None:
+    import lagrangianrbnudging_b200 as lb
+    from lagrangianrbnudging_b200 import build as b
+
+    if rank == 0:
+        b.build()
+    if dist is not None:
+        dist.barrier()
+    seed = SEED + 7919 * rank
+    K, W = args.steps, args.warmup
+    nodes = NX * NY
+    out = {}
+    # -- headline: FP32 shifted populations
+    r, base = make_run(lb, "fp32", seed, device, K // NOUTCONFIG + W // NOUTCONFIG + 4)
+    init_run(r, seed)
+    with ClockSampler(device) as clk:
+        ms, timing, recs, (t0, t1) = timed_steps(r, torch, K, W, dist, device)
+        clocks = clk.summary(t0, t1)
+    nu32 = r.nusselt()
+    ke32, _ = r.energy()
+    r.close()
+    ms = max_over_ranks(torch, dist, ms)
+    lb_ms, lb_n = timing["lb_step"]
+    pt_ms, pt_n = timing["particles"]
+    # -- FP64 reference-order populations on the same workload
+    K64 = max(K // 2, 10)
+    r64, _ = make_run(lb, "fp64", seed, device, K64 // NOUTCONFIG + W // NOUTCONFIG + 4)
+    init_run(r64, seed)
+    ms64, timing64, _, _ = timed_steps(r64, torch, K64, W, dist, device)
+    r64.step(K - K64)  # same number of steps as the FP32 run for the Nu comparison
+    r64.sync()
+    nu64 = r64.nusselt()
+    ke64, _ = r64.energy()
+    r64.close()
+    ms64 = max_over_ranks(torch, dist, ms64)
+    # -- end to end through the C-ABI with host buffers
+    e2e_ms = e2e_h2d = e2e_d2h = None
+    if not args.no_e2e:
+        e2e_ms, e2e_h2d, e2e_d2h = e2e(lb, torch, "fp32", seed, K, device, dist)
+        e2e_ms = max_over_ranks(torch, dist, e2e_ms)
+    if rank != 0:
+        return None
+    mlups = world * nodes * K / (ms * 1e3)
+    mlups64 = world * nodes * K64 / (ms64 * 1e3)
+    peak, peak_kind = measured_peak()
+    avg_lb = lb_ms / max(lb_n, 1)
+    achieved = ALG_BYTES["fp32"] * nodes / (avg_lb * 1e-3) / 1e9
+    tr = profiled_traffic("fp32")
+    avg_lb64 = timing64["lb_step"][0] / max(timing64["lb_step"][1], 1)
+    achieved64 = ALG_BYTES["fp64"] * nodes / (avg_lb64 * 1e-3) / 1e9
+    out.update({
+        "metric": "MLUPS (lattice updates/s, FP32-shifted populations, whole step incl. particles)",
+        "value": round(mlups, 1),
+        "unit": "MLUPS",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(ms / K, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic (seeded conduction + noise; seeded uniform particles)",
+        "config": {"workload": WORKLOAD, "grid": f"{NX}x{NY}", "particles": NPRTCL,
+                   "precision": "fp32-shifted populations, fp64 particles",
+                   "l2": "state 1.5 GB > 126 MB L2 on every step (no flush needed)",
+                   "parallelism": f"{world} independent instances (replicas), no collective"},
+        "roofline": {"bound": "hbm", "kernel": "lb_step_kernel<float>",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "alg_bytes_per_node": ALG_BYTES["fp32"],
+                     "avg_launch_ms": round(avg_lb, 5),
+                     "traffic": (round(tr * nodes) if tr else None),
+                     "share_of_step": round(lb_ms / ms, 4)},
+        "fp64": {"value": round(mlups64, 1), "unit": "MLUPS", "steps": K64,
+                 "lb_achieved_gbs": round(achieved64, 1),
+                 "lb_frac": round(achieved64 / peak, 4),
+                 "fp32_over_fp64": round(mlups / mlups64, 3)},
+        "accuracy": {"nu_fp32": nu32, "nu_fp64": nu64,
+                     "nu_rel_err": abs(nu32 - nu64) / abs(nu64),
+                     "ke_rel_err": abs(ke32 - ke64) / max(abs(ke64), 1e-300),
+                     "note": f"after {K + W} steps from the same initial state"},
+        "kernels_ms": {k: round(v[0], 3) for k, v in timing.items()},
+        "gpu_launches": int(lb_n + pt_n),
+        "clocks": clocks,
+        "records": len(recs),
+    })
+    if e2e_ms is not None:
+        out["e2e"] = {"value": round(world * nodes * K / (e2e_ms * 1e3), 1), "unit": "MLUPS",
+                      "h2d_bytes_per_step": int(e2e_h2d / K), "d2h_bytes_per_step": int(e2e_d2h / K),
+                      "ms": round(e2e_ms, 2),
+                      "path": "lbrb_set_populations(REF_AOS_HALO fp64) + set_moments + "
+                              "particles_set + lbrb_step(K) + record_drain + get_moments"}
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+# ---------------------------------------------------------- reference arm
+def ref_params() -> dict:
+    nu = U * NY * np.sqrt(PR / RA)
+    kappa = U * NY / np.sqrt(RA * PR)
+    return dict(nx=NX, ny=NY, scratch=1, nstart=0, nsteps=1000000, nout=1000000,
+                noutconfig=NOUTCONFIG, relax=3.0 * nu + 0.5, relaxg=3.0 * kappa + 0.5,
+                Tup=-0.5, Tdown=0.5, gravity=-(U * U) / NY, Particle=1, Particle_scratch=0,
+                Nprtcl=NPRTCL, tracer=0, heavyprtcl=1, taulag=0.5 * NY / U, beta=0.0,
+                Prtcl_Writefull=0)
+
+
+def build_reference_baseline():
+    """Build the reference's own temppart_dump for this workload (needs the
+    reference checkout; the binary travels in oracle/_ref)."""
+    from oracle import build as ob
+
+    return ob.build_ref("temppart_dump", ref_params(), REF_TAG)
+
+
+def ref_exe() -> Path:
+    return ROOT / "oracle" / "_ref" / REF_TAG / "temppart_dump"
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def ref_ranks(cores: int) -> int:
+    p = 1
+    while p * 2 <= min(cores, 128):
+        p *= 2
+    return p
+
+
+def run_reference(steps: int, warmup: int, ranks: int, time_cap: float) -> dict:
+    """Run the reference on `ranks` processes; the per-step time comes from
+    the wall-clock arrival of its per-step stdout line (temppart_dump.c:1698),
+    measured over steps warmup+1 .. warmup+steps, then the run is stopped."""
+    import resource
+
+    exe = ref_exe()
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} missing (built by __graft_entry__.build() where the reference is present)")
+    wd = Path(tempfile.mkdtemp(prefix="lbrb_bench_ref_"))
+    (wd / "Prtcl_Veldata1" / "Particles0.h5.d").mkdir(parents=True)
+    (wd / "Tempfolder").mkdir()
+    ids, x, y, ptype, invtau = particle_setup(SEED + 1)
+    ids.astype(np.int32).tofile(wd / "Prtcl_Veldata1" / "Particles0.h5.d" / "id.bin")
+    rec = np.zeros((NPRTCL, 8))
+    rec[:, 0], rec[:, 1], rec[:, 4], rec[:, 5] = x, y, x, y
+    rec.tofile(wd / "prtcl_dump0.in")
+
+    def pre():
+        for lim in (resource.RLIMIT_STACK,):
+            try:
+                resource.setrlimit(lim, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+            except (ValueError, OSError):
+                pass
+        soft, hard = resource.getrlimit(resource.RLIMIT_NOFILE)
+        try:
+            resource.setrlimit(resource.RLIMIT_NOFILE, (min(hard, 1 << 16), hard))
+        except (ValueError, OSError):
+            pass
+
+    env = dict(os.environ, LBRB_SHIM_NP=str(ranks))
+    env.pop("LBRB_SHIM_DIMS", None)
+    p = subprocess.Popen([str(exe)], cwd=wd, env=env, stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, preexec_fn=pre, start_new_session=True,
+                         text=True, bufsize=1)
+    stamps = {}
+    a, want = warmup, warmup + steps
+    t_start = time.time()
+    try:
+        for line in p.stdout:
+            if line.startswith("Loop "):
+                s = int(line.split()[1])
+                if s == max(a, 1) or s == want or s >= a:
+                    stamps[s] = time.time()
+                if s >= want or (s > a and time.time() - stamps.get(max(a, 1), t_start) > time_cap):
+                    break
+    finally:
+        try:
+            os.killpg(p.pid, signal.SIGKILL)
+        except ProcessLookupError:
+            pass
+        p.wait()
+        import shutil
+        shutil.rmtree(wd, ignore_errors=True)
+    s0 = max(a, 1)
+    s1 = max(stamps)
+    if s1 <= s0:
+        raise RuntimeError("reference produced too few steps")
+    per = (stamps[s1] - stamps[s0]) / (s1 - s0)
+    return {"per_step_s": per, "steps": s1 - s0, "ranks": ranks}
+
+
+def cpu_baseline(args) -> dict:
+    try:
+        cores = host_cores()
+        ranks = ref_ranks(cores)
+        res = run_reference(steps=40, warmup=3, ranks=ranks, time_cap=25.0)
+        return {"value": round(NX * NY / res["per_step_s"] / 1e6, 3), "unit": "MLUPS",
+                "cores": res["ranks"], "kind": "reference",
+                "sample": f"reference temppart_dump (gcc -O2, {res['ranks']} ranks on {cores} host "
+                          f"cores), {NX}x{NY}, 2^17 inertial particles (one St), {res['steps']} "
+                          f"steps timed from its per-step output line"}
+    except Exception as e:  # reported, never fatal for our arm
+        return {"value": None, "unit": "MLUPS", "cores": None, "kind": "reference",
+                "sample": f"unavailable: {e}"}
+
+
+def run_reference_arm(args) -> dict:
+    cores = host_cores()
+    ranks = ref_ranks(cores)
+    res = run_reference(steps=args.steps, warmup=args.warmup, ranks=ranks, time_cap=REF_STEPS_CAP_S)
+    mlups = NX * NY / res["per_step_s"] / 1e6
+    sample = (f"reference temppart_dump (its own C sources, gcc -O2, MPI/HDF5 stand-ins), "
+              f"{res['ranks']} ranks on {cores} host cores, {NX}x{NY}, 2^17 inertial particles "
+              f"(one St: the reference compiles one particle type), {res['steps']} timed steps")
+    return {"impl": "reference", "metric": "MLUPS (lattice updates/s, reference CPU build)",
+            "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": args.gpus,
+            "steps": res["steps"], "warmup": args.warmup,
+            "ms_per_step": round(res["per_step_s"] * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": f"{NX}x{NY}", "particles": NPRTCL},
+            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": res["ranks"],
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=40)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference_arm(args)), flush=True)
+        return
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_mod
+    else:
+        torch.cuda.set_device(0)
+    out = run_ours(args, torch, dist, rank, world, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,201 @@
+/*
+ * lbrb.h -- C-ABI of the B200 thermal lattice-Boltzmann Rayleigh-Benard step
+ * loop with Lagrangian particles and temperature nudging.
+ *
+ * The reference drives its time loop from main() through plain C functions on
+ * host arrays (Trajectories/code/temppart_dump.c:1674-1759,
+ * Nudging/code/tempvel_nudge.c:2346-2411).  This library replaces that loop
+ * body: one opaque handle owns the whole domain in device memory; the caller
+ * hands state in and out through host buffers in the reference's own layouts.
+ *
+ * Conventions
+ *  - Every call returns an int status: LBRB_OK (0) or a negative LBRB_ERR_*;
+ *    lbrb_last_error() returns a message for the last failure on a handle.
+ *  - Host buffers are borrowed for the duration of the call only.
+ *  - A handle has one CUDA stream and must be used from one host thread.
+ *  - Grid: nx, ny interior nodes (the reference's nx, ny); nx % 4 == 0.
+ *  - Reference node (i, j), 1 <= i <= nx, 1 <= j <= ny, has position (i, j):
+ *    particle coordinates use the same frame (walls half-way at y = 0.5 and
+ *    y = ny + 0.5, x periodic with period nx).
+ *
+ * Layouts for populations (9 per node, D2Q9 order of the reference's dellar(),
+ * temppart_dump.c:1363-1401) and scalar fields:
+ *  - LBRB_LAYOUT_REF_AOS_HALO: the reference's own arrays, pop_type[(nx+2)*(ny+2)]
+ *    with node index idx = j + (ny+2)*i (temppart_dump.c:38-40, 1598-1601);
+ *    scalars REAL[(nx+2)*(ny+2)].  On output the halo is filled periodically
+ *    in x and y as pbc() and communication() leave it.
+ *  - LBRB_LAYOUT_SOA: interior only, pops [9][ny][nx], scalars [ny][nx], x fastest.
+ */
+#ifndef LBRB_H
+#define LBRB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBRB_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LBRB_API __attribute__((visibility("default")))
+#else
+#define LBRB_API
+#endif
+
+typedef struct lbrb_s lbrb_t;
+
+enum lbrb_status {
+  LBRB_OK = 0,
+  LBRB_ERR_ARG = -1,        /* invalid argument (reference: silent UB or exit(8)) */
+  LBRB_ERR_CUDA = -2,       /* CUDA runtime failure */
+  LBRB_ERR_NOMEM = -3,      /* device or pinned allocation failed */
+  LBRB_ERR_STATE = -4,      /* call out of order (e.g. nudging data missing) */
+  LBRB_ERR_NONFINITE = -5,  /* NaN/Inf found in the state */
+  LBRB_ERR_RANGE = -6,      /* particle or observation outside the domain */
+  LBRB_ERR_OVERFLOW = -7,   /* record ring full: drain before stepping on */
+  LBRB_ERR_IDS = -8,        /* observation ids do not match particle ids */
+  LBRB_ERR_UNSUPPORTED = -9 /* combination not built */
+};
+
+enum { LBRB_PREC_FP64 = 0, LBRB_PREC_FP32_SHIFTED = 1 };
+enum { LBRB_TWALL_DIRICHLET = 0, LBRB_TWALL_ADIABATIC = 1 };
+enum { LBRB_NUDGE_NONE = 0, LBRB_NUDGE_REFBOX = 1, LBRB_NUDGE_BILINEAR = 2 };
+enum { LBRB_LAYOUT_REF_AOS_HALO = 0, LBRB_LAYOUT_SOA = 1 };
+enum { LBRB_PTYPE_TRACER = 0, LBRB_PTYPE_INERTIAL = 1 };
+
+/* record fields, in the order of the reference's Particles%d.h5 datasets
+ * (temppart_dump.c:1553-1562, then the Prtcl_Writefull block mympi2.h:549-556) */
+enum {
+  LBRB_REC_X = 0, LBRB_REC_Y, LBRB_REC_U, LBRB_REC_V, LBRB_REC_XO, LBRB_REC_YO,
+  LBRB_REC_UO, LBRB_REC_VO, LBRB_REC_TEMP,
+  LBRB_REC_DTU, LBRB_REC_DTV, LBRB_REC_DXU, LBRB_REC_DXV, LBRB_REC_DYU, LBRB_REC_DYV,
+  LBRB_REC_FU, LBRB_REC_FV,
+  LBRB_REC_NBASIC = 9, LBRB_REC_NFULL = 17
+};
+
+/* Run parameters.  Names follow the reference's compile-time #defines
+ * (temppart_dump.c:15-31, Trajectories/code/mympi2.h:14-21,
+ * tempvel_nudge.c:13-31); here they are runtime values. */
+typedef struct {
+  int nx, ny;             /* nx, ny */
+  double relax, relaxg;   /* relax, relaxg (tau of f and g) */
+  double Tup, Tdown;      /* Tup, Tdown */
+  double gravity;         /* gravity (negative; F_y = -gravity*rho*T) */
+  int precision;          /* LBRB_PREC_* */
+  int twall;              /* LBRB_TWALL_*: Trajectories = Dirichlet, Nudging = adiabatic */
+  int nudge;              /* LBRB_NUDGE_* */
+  double alpha;           /* alpha: nudging coefficient */
+  int ntempread;          /* ntempread: observation file interval (box mode) */
+  int nobs;               /* observations per step (box: Nprtcl; bilinear: any) */
+  double beta;            /* beta: Maxey-Riley coefficient */
+  int nprtcl;             /* Nprtcl: Lagrangian particles advanced by the run */
+  int noutconfig;         /* noutconfig: record interval (0 = no records) */
+  int record_full;        /* Prtcl_Writefull: also record the 8 Maxey-Riley terms */
+  int record_slots;       /* records held before lbrb_record_drain() must run */
+  int device;             /* CUDA device ordinal */
+} lbrb_params;
+
+/* Fill *p with defaults (reference values where it has them). */
+LBRB_API void lbrb_params_default(lbrb_params *p);
+
+/* Create / destroy a run.  Replaces myInit + the mallocs of main()
+ * (Trajectories/code/mympi2.h:41-108, temppart_dump.c:1589-1641). */
+LBRB_API int lbrb_create(const lbrb_params *p, lbrb_t **out);
+LBRB_API int lbrb_destroy(lbrb_t *h);
+LBRB_API const char *lbrb_last_error(const lbrb_t *h);
+LBRB_API int lbrb_abi_version(void);
+
+/* ---- state in / out ------------------------------------------------------ */
+/* Post-collision populations f, g.  Replaces restoref/restoreg
+ * (temppart_dump.c:348-507) and dumpf/dumpg (temppart_dump.c:52-141). */
+LBRB_API int lbrb_set_populations(lbrb_t *h, const double *f, const double *g, int layout);
+LBRB_API int lbrb_get_populations(lbrb_t *h, double *f, double *g, int layout);
+/* Moments of the last step (rhopre, upre, vpre, temppre); any pointer may be
+ * NULL on get.  The next step's buoyancy uses rho and T (forcingconstructWW,
+ * temppart_dump.c:744-755). */
+LBRB_API int lbrb_set_moments(lbrb_t *h, const double *rho, const double *u, const double *v,
+                     const double *T, int layout);
+LBRB_API int lbrb_get_moments(lbrb_t *h, double *rho, double *u, double *v, double *T, int layout);
+/* Restart route: moments from the "pre" populations confpre/congpre
+ * (inithydro scratch==0, temppart_dump.c:703-726). */
+LBRB_API int lbrb_moments_from_pre(lbrb_t *h, const double *fpre, const double *gpre, int layout);
+/* Seeded initial state: linear conduction T plus uniform noise of amplitude
+ * `noise` (splitmix64 of seed and node index), f = feq(1,0), g = geq(T,0),
+ * moments by the restart route.  No reference counterpart (the reference's
+ * scratch state uses rand(), inithydro temppart_dump.c:686-701). */
+LBRB_API int lbrb_init_conduction(lbrb_t *h, uint64_t seed, double noise);
+
+/* ---- time loop ----------------------------------------------------------- */
+/* Advance n steps: the loop body temppart_dump.c:1675-1757 (stream, walls,
+ * force, moments, particles, records, collision) or tempvel_nudge.c:2349-2377
+ * (observation update, stream, walls, moments, nudged collision). */
+LBRB_API int lbrb_step(lbrb_t *h, int n);
+/* Wait for all queued work and report device-side status (LBRB_ERR_RANGE,
+ * LBRB_ERR_NONFINITE, ...). */
+LBRB_API int lbrb_sync(lbrb_t *h);
+LBRB_API int lbrb_get_istep(const lbrb_t *h, int *istep);
+LBRB_API int lbrb_set_istep(lbrb_t *h, int istep);
+/* Scan the populations for NaN/Inf (LBRB_ERR_NONFINITE if any). */
+LBRB_API int lbrb_check_finite(lbrb_t *h);
+/* Queue all work of this handle on `cuda_stream` (a cudaStream_t of the
+ * handle's device; NULL restores the handle's own stream).  lbrb_step() joins
+ * its record copies back into this stream before returning, so an event
+ * recorded on it after lbrb_step() covers the whole step. */
+LBRB_API int lbrb_set_stream(lbrb_t *h, void *cuda_stream);
+/* Per-kernel device timing with CUDA events around each launch.  Classes:
+ * 0 fused stream/collide, 1 particles, 2 nudging, 3 record copies.
+ * lbrb_get_timing() waits, returns total milliseconds and launch counts per
+ * class (arrays of length n <= 4) and resets the accumulators. */
+LBRB_API int lbrb_set_timing(lbrb_t *h, int enable);
+LBRB_API int lbrb_get_timing(lbrb_t *h, double *ms, int *launches, int n);
+
+/* ---- particles ------------------------------------------------------------ */
+/* Replaces init_prtcl/restore_prtcl (Trajectories/code/mympi2.h:116-290,
+ * temppart_dump.c:252-346).  Arrays of length n == nprtcl; positions in the
+ * global frame; ptype LBRB_PTYPE_*; invtau = onebytaulag per particle. */
+LBRB_API int lbrb_particles_set(lbrb_t *h, int n, const int *ids, const double *x, const double *y,
+                       const double *u, const double *v, const int *ptype, const double *invtau);
+/* Current particle state (after wrap/reflect, toggle_prtcl mympi2.h:568-760);
+ * any pointer may be NULL. */
+LBRB_API int lbrb_particles_get(lbrb_t *h, int n, int *ids, double *x, double *y, double *u, double *v,
+                       double *xo, double *yo, double *uo, double *vo);
+
+/* ---- trajectory records (prtcl_write, temppart_dump.c:1467-1571) ----------- */
+/* Records are kept on the device and copied to pinned host memory as they
+ * complete.  Drain up to max_records of them, oldest first: steps[r] is the
+ * step of record r and buf holds [r][field][nprtcl] doubles with
+ * LBRB_REC_NBASIC or LBRB_REC_NFULL fields; ids (may be NULL) gets the
+ * particle ids in record order. */
+LBRB_API int lbrb_record_pending(lbrb_t *h, int *count);
+LBRB_API int lbrb_record_drain(lbrb_t *h, int max_records, int *steps, double *buf, int *ids,
+                      int *n_drained);
+
+/* ---- nudging --------------------------------------------------------------- */
+/* Box mode (tempvel_nudge.c): initial observations (set_nudge_vol contin==0,
+ * :2080-2122) and the observation file for step istep+ntempread-1 read by
+ * read_prtcl (:1380-1476), arrays of length nobs in file order. */
+LBRB_API int lbrb_nudge_init(lbrb_t *h, int n, const double *x, const double *y, const double *T,
+                    const int *ids);
+LBRB_API int lbrb_nudge_load(lbrb_t *h, int n, const double *x, const double *y, const int *ids,
+                    const double *T);
+/* Bilinear mode (no reference counterpart): observations for nsteps
+ * consecutive steps starting at step first_step, arrays [nsteps][nobs]. */
+LBRB_API int lbrb_nudge_obs(lbrb_t *h, int first_step, int nsteps, const double *x, const double *y,
+                   const double *T);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+/* Mean kinetic energy and mean temperature over the interior (evolution.dat,
+ * temppart_dump.c:1739-1757), compensated FP64 sums. */
+LBRB_API int lbrb_energy(lbrb_t *h, double *ke_mean, double *t_mean);
+/* Volume Nusselt number 1 + <vT> ny / (kappa (Tdown-Tup)), kappa = (relaxg-1/2)/3. */
+LBRB_API int lbrb_nusselt(lbrb_t *h, double *nu);
+/* Per-row profile [ny][9]: rho, u, v, u^2, v^2, T, vT, dT/dy (profile(),
+ * tempvel_nudge.c:1104-1260), and the row Nusselt number. */
+LBRB_API int lbrb_profile(lbrb_t *h, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

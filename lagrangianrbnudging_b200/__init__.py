@@ -1,0 +1,324 @@
+"""B200-native thermal lattice-Boltzmann Rayleigh-Benard step loop with
+Lagrangian particles and temperature nudging.
+
+The compute path is liblbrb.so (hand-written CUDA for sm_100a behind the
+C-ABI of include/lbrb.h).  This module binds that ABI with ctypes for the
+tests, the benchmark and Python callers; there is no CPU fallback: when the
+library or a CUDA device is missing, calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "liblbrb.so"
+
+OK = 0
+ERRORS = {
+    -1: "LBRB_ERR_ARG", -2: "LBRB_ERR_CUDA", -3: "LBRB_ERR_NOMEM", -4: "LBRB_ERR_STATE",
+    -5: "LBRB_ERR_NONFINITE", -6: "LBRB_ERR_RANGE", -7: "LBRB_ERR_OVERFLOW", -8: "LBRB_ERR_IDS",
+    -9: "LBRB_ERR_UNSUPPORTED",
+}
+PREC = {"fp64": 0, "fp32": 1}
+TWALL = {"dirichlet": 0, "adiabatic": 1}
+NUDGE = {"none": 0, "refbox": 1, "bilinear": 2}
+LAYOUT = {"ref": 0, "soa": 1}
+REC_NAMES = ["x", "y", "u", "v", "xo", "yo", "uo", "vo", "temp",
+             "dtu", "dtv", "dxu", "dxv", "dyu", "dyv", "fu", "fv"]
+
+# every symbol declared in include/lbrb.h
+EXPORTS = [
+    "lbrb_params_default", "lbrb_create", "lbrb_destroy", "lbrb_last_error", "lbrb_abi_version",
+    "lbrb_set_populations", "lbrb_get_populations", "lbrb_set_moments", "lbrb_get_moments",
+    "lbrb_moments_from_pre", "lbrb_init_conduction", "lbrb_step", "lbrb_sync", "lbrb_get_istep",
+    "lbrb_set_istep", "lbrb_check_finite", "lbrb_particles_set", "lbrb_particles_get",
+    "lbrb_record_pending", "lbrb_record_drain", "lbrb_nudge_init", "lbrb_nudge_load",
+    "lbrb_nudge_obs", "lbrb_energy", "lbrb_nusselt", "lbrb_profile", "lbrb_set_stream",
+    "lbrb_set_timing", "lbrb_get_timing",
+]
+
+
+class LbrbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int),
+        ("relax", C.c_double), ("relaxg", C.c_double),
+        ("Tup", C.c_double), ("Tdown", C.c_double), ("gravity", C.c_double),
+        ("precision", C.c_int), ("twall", C.c_int), ("nudge", C.c_int),
+        ("alpha", C.c_double), ("ntempread", C.c_int), ("nobs", C.c_int),
+        ("beta", C.c_double), ("nprtcl", C.c_int), ("noutconfig", C.c_int),
+        ("record_full", C.c_int), ("record_slots", C.c_int), ("device", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load liblbrb.so (built in-tree by lagrangianrbnudging_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(f"{LIB_PATH} is missing: run python -m lagrangianrbnudging_b200.build")
+    L = C.CDLL(str(LIB_PATH))
+    dp, ip, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
+    sig = {
+        "lbrb_params_default": (None, [C.POINTER(Params)]),
+        "lbrb_create": (C.c_int, [C.POINTER(Params), C.POINTER(vp)]),
+        "lbrb_destroy": (C.c_int, [vp]),
+        "lbrb_last_error": (C.c_char_p, [vp]),
+        "lbrb_abi_version": (C.c_int, []),
+        "lbrb_set_populations": (C.c_int, [vp, dp, dp, C.c_int]),
+        "lbrb_get_populations": (C.c_int, [vp, dp, dp, C.c_int]),
+        "lbrb_set_moments": (C.c_int, [vp, dp, dp, dp, dp, C.c_int]),
+        "lbrb_get_moments": (C.c_int, [vp, dp, dp, dp, dp, C.c_int]),
+        "lbrb_moments_from_pre": (C.c_int, [vp, dp, dp, C.c_int]),
+        "lbrb_init_conduction": (C.c_int, [vp, C.c_uint64, C.c_double]),
+        "lbrb_step": (C.c_int, [vp, C.c_int]),
+        "lbrb_sync": (C.c_int, [vp]),
+        "lbrb_get_istep": (C.c_int, [vp, ip]),
+        "lbrb_set_istep": (C.c_int, [vp, C.c_int]),
+        "lbrb_check_finite": (C.c_int, [vp]),
+        "lbrb_particles_set": (C.c_int, [vp, C.c_int, ip, dp, dp, dp, dp, ip, dp]),
+        "lbrb_particles_get": (C.c_int, [vp, C.c_int, ip, dp, dp, dp, dp, dp, dp, dp, dp]),
+        "lbrb_record_pending": (C.c_int, [vp, ip]),
+        "lbrb_record_drain": (C.c_int, [vp, C.c_int, ip, dp, ip, ip]),
+        "lbrb_nudge_init": (C.c_int, [vp, C.c_int, dp, dp, dp, ip]),
+        "lbrb_nudge_load": (C.c_int, [vp, C.c_int, dp, dp, ip, dp]),
+        "lbrb_nudge_obs": (C.c_int, [vp, C.c_int, C.c_int, dp, dp, dp]),
+        "lbrb_energy": (C.c_int, [vp, dp, dp]),
+        "lbrb_nusselt": (C.c_int, [vp, dp]),
+        "lbrb_profile": (C.c_int, [vp, dp]),
+        "lbrb_set_stream": (C.c_int, [vp, vp]),
+        "lbrb_set_timing": (C.c_int, [vp, C.c_int]),
+        "lbrb_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _dp(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous, "float64 C-contiguous array required"
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous, "int32 C-contiguous array required"
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def make_params(**kw) -> Params:
+    p = Params()
+    lib().lbrb_params_default(C.byref(p))
+    for k, v in kw.items():
+        if k == "precision":
+            v = PREC.get(v, v)
+        elif k == "twall":
+            v = TWALL.get(v, v)
+        elif k == "nudge":
+            v = NUDGE.get(v, v)
+        elif k == "record_full":
+            v = int(bool(v))
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class Run:
+    """One whole-domain run on one GPU, through the C-ABI."""
+
+    def __init__(self, **params):
+        self.p = make_params(**params)
+        h = C.c_void_p()
+        rc = lib().lbrb_create(C.byref(self.p), C.byref(h))
+        if rc != OK:
+            raise LbrbError(rc, "lbrb_create failed (arguments, device or memory)")
+        self.h = h
+        self.nx, self.ny, self.np = self.p.nx, self.p.ny, self.p.nprtcl
+        self.nrec = 17 if self.p.record_full else 9
+
+    def _ck(self, rc: int):
+        if rc != OK:
+            msg = lib().lbrb_last_error(self.h)
+            raise LbrbError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lbrb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- state
+    def set_populations(self, f, g, layout="soa"):
+        f, g = _f64(f), _f64(g)
+        self._ck(lib().lbrb_set_populations(self.h, _dp(f), _dp(g), LAYOUT[layout]))
+
+    def get_populations(self, layout="soa"):
+        if layout == "soa":
+            shape = (9, self.ny, self.nx)
+        else:
+            shape = (self.nx + 2, self.ny + 2, 9)
+        f = np.empty(shape)
+        g = np.empty(shape)
+        self._ck(lib().lbrb_get_populations(self.h, _dp(f), _dp(g), LAYOUT[layout]))
+        return f, g
+
+    def set_moments(self, rho, u, v, T, layout="soa"):
+        a = [_f64(x) for x in (rho, u, v, T)]
+        self._ck(lib().lbrb_set_moments(self.h, *[_dp(x) for x in a], LAYOUT[layout]))
+
+    def get_moments(self, layout="soa"):
+        shape = (self.ny, self.nx) if layout == "soa" else (self.nx + 2, self.ny + 2)
+        out = [np.empty(shape) for _ in range(4)]
+        self._ck(lib().lbrb_get_moments(self.h, *[_dp(x) for x in out], LAYOUT[layout]))
+        return dict(zip(("rho", "u", "v", "T"), out))
+
+    def moments_from_pre(self, fpre, gpre, layout="soa"):
+        fpre, gpre = _f64(fpre), _f64(gpre)
+        self._ck(lib().lbrb_moments_from_pre(self.h, _dp(fpre), _dp(gpre), LAYOUT[layout]))
+
+    def init_conduction(self, seed: int, noise: float):
+        self._ck(lib().lbrb_init_conduction(self.h, C.c_uint64(seed), noise))
+
+    # ---- loop
+    def step(self, n: int = 1):
+        self._ck(lib().lbrb_step(self.h, int(n)))
+
+    def sync(self):
+        self._ck(lib().lbrb_sync(self.h))
+
+    @property
+    def istep(self) -> int:
+        s = C.c_int()
+        self._ck(lib().lbrb_get_istep(self.h, C.byref(s)))
+        return s.value
+
+    def check_finite(self):
+        self._ck(lib().lbrb_check_finite(self.h))
+
+    # ---- particles
+    def set_particles(self, ids, x, y, u, v, ptype, invtau):
+        ids, ptype = _i32(ids), _i32(ptype)
+        x, y, u, v, invtau = (_f64(a) for a in (x, y, u, v, invtau))
+        self._ck(lib().lbrb_particles_set(self.h, len(ids), _ip(ids), _dp(x), _dp(y), _dp(u),
+                                          _dp(v), _ip(ptype), _dp(invtau)))
+
+    def get_particles(self):
+        n = self.np
+        ids = np.empty(n, np.int32)
+        arrs = [np.empty(n) for _ in range(8)]
+        self._ck(lib().lbrb_particles_get(self.h, n, _ip(ids), *[_dp(a) for a in arrs]))
+        return dict(id=ids, **dict(zip(["x", "y", "u", "v", "xo", "yo", "uo", "vo"], arrs)))
+
+    def pending_records(self) -> int:
+        c = C.c_int()
+        self._ck(lib().lbrb_record_pending(self.h, C.byref(c)))
+        return c.value
+
+    def drain_records(self, max_records: int | None = None):
+        """Returns {step: {field: array}} for the drained records."""
+        k = self.pending_records() if max_records is None else max_records
+        if k == 0:
+            return {}
+        steps = np.empty(k, np.int32)
+        buf = np.empty((k, self.nrec, self.np))
+        ids = np.empty(self.np, np.int32)
+        got = C.c_int()
+        self._ck(lib().lbrb_record_drain(self.h, k, _ip(steps), _dp(buf), _ip(ids), C.byref(got)))
+        out = {}
+        for r in range(got.value):
+            d = {"id": ids.copy()}
+            for f in range(self.nrec):
+                d[REC_NAMES[f]] = buf[r, f].copy()
+            out[int(steps[r])] = d
+        return out
+
+    # ---- nudging
+    def nudge_init(self, x, y, T, ids):
+        x, y, T, ids = _f64(x), _f64(y), _f64(T), _i32(ids)
+        self._ck(lib().lbrb_nudge_init(self.h, len(x), _dp(x), _dp(y), _dp(T), _ip(ids)))
+
+    def nudge_load(self, x, y, ids, T):
+        x, y, T, ids = _f64(x), _f64(y), _f64(T), _i32(ids)
+        self._ck(lib().lbrb_nudge_load(self.h, len(x), _dp(x), _dp(y), _ip(ids), _dp(T)))
+
+    def nudge_obs(self, first_step: int, x, y, T):
+        x, y, T = _f64(np.atleast_2d(x)), _f64(np.atleast_2d(y)), _f64(np.atleast_2d(T))
+        self._ck(lib().lbrb_nudge_obs(self.h, int(first_step), x.shape[0], _dp(x), _dp(y), _dp(T)))
+
+    # ---- streams and timing
+    def set_stream(self, stream_handle: int | None):
+        self._ck(lib().lbrb_set_stream(self.h, C.c_void_p(stream_handle or 0)))
+
+    def set_timing(self, enable: bool):
+        self._ck(lib().lbrb_set_timing(self.h, int(bool(enable))))
+
+    def get_timing(self):
+        ms = np.zeros(4)
+        cnt = np.zeros(4, np.int32)
+        self._ck(lib().lbrb_get_timing(self.h, _dp(ms), _ip(cnt), 4))
+        names = ["lb_step", "particles", "nudging", "record_copy"]
+        return {n: (float(ms[i]), int(cnt[i])) for i, n in enumerate(names)}
+
+    # ---- diagnostics
+    def energy(self):
+        ke, tm = C.c_double(), C.c_double()
+        self._ck(lib().lbrb_energy(self.h, C.byref(ke), C.byref(tm)))
+        return ke.value, tm.value
+
+    def nusselt(self) -> float:
+        nu = C.c_double()
+        self._ck(lib().lbrb_nusselt(self.h, C.byref(nu)))
+        return nu.value
+
+    def profile(self):
+        out = np.empty((self.ny, 9))
+        self._ck(lib().lbrb_profile(self.h, _dp(out)))
+        return out
+
+
+def closure(nx: int, ny: int, Ra: float, Pr: float, U: float, dT: float = 1.0) -> dict:
+    """Run parameters of the configurations: nu = U*Ny*sqrt(Pr/Ra),
+    kappa = U*Ny/sqrt(Ra*Pr), tau = 3 nu + 1/2, g*beta = U^2/Ny (gravity
+    negative in the reference's sign convention), T_bottom = +dT/2."""
+    nu = U * ny * np.sqrt(Pr / Ra)
+    kappa = U * ny / np.sqrt(Ra * Pr)
+    return dict(nx=nx, ny=ny, relax=3.0 * nu + 0.5, relaxg=3.0 * kappa + 0.5,
+                Tup=-0.5 * dT, Tdown=0.5 * dT, gravity=-(U * U) / ny)

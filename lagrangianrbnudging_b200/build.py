@@ -1,0 +1,61 @@
+"""Build liblbrb.so (the CUDA kernels + C-ABI) in-tree for sm_100a.
+
+    python -m lagrangianrbnudging_b200.build [--verbose-ptxas]
+
+All translation units are compiled with --fmad=false: the FP64 path keeps
+the reference's rounding (no fused multiply-add contraction), which makes
+its results bit-identical to the reference built with gcc -O2 on x86-64.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "liblbrb.so"
+SOURCES = ["lb_kernels.cu", "particle_kernels.cu", "nudge_kernels.cu", "aux_kernels.cu", "capi.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (Path(c).exists() or c == "nvcc"):
+            return c
+    return "nvcc"
+
+
+def _stale() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    deps = [CSRC / s for s in SOURCES] + [CSRC / "lbrb_internal.cuh", ROOT / "include" / "lbrb.h"]
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
+    if not force and not _stale():
+        return LIB
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    objs = []
+    for s in SOURCES:
+        o = objdir / (Path(s).stem + ".o")
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-dc" if False else "-c", str(CSRC / s), "-o", str(o)]
+        if verbose_ptxas:
+            cmd.insert(1, "-Xptxas=-v")
+        subprocess.run(cmd, check=True)
+        objs.append(str(o))
+    tmp = LIB.with_suffix(".so.tmp")
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force=True, verbose_ptxas="--verbose-ptxas" in sys.argv))

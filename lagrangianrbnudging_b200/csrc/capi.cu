@@ -1,0 +1,801 @@
+// capi.cu -- the C-ABI declared in include/lbrb.h.
+//
+// One handle = one whole-domain run on one device.  lbrb_step() queues, per
+// time step, on the handle's stream:
+//   [box nudging: observation interpolation + ordered box means]
+//   fused stream/collide kernel (reads buffer cur, writes cur^1)
+//   [bilinear nudging: innovation scatter + apply on the new g]
+//   particle kernel (+ record into the device ring; a copy stream moves each
+//   finished record into pinned host memory while the next steps run)
+// and returns without waiting; lbrb_sync() waits and reports device flags.
+#include <cstdio>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "lbrb_internal.cuh"
+
+namespace lbrb {
+cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, cudaStream_t s);
+cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s);
+cudaError_t launch_particles(const void* u, const void* v, const void* ub, const void* vb,
+                             const void* T, bool fp32, int nx, int ny, int pitch, double* P,
+                             const int* ptype, int np, double beta, int record, int full,
+                             double* rec, unsigned* dflags, cudaStream_t s);
+cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt, int istep,
+                             int ncx, int ncy, int* cell_count, int* cell_start, int* cell_fill,
+                             int* cell_dirty, int* items, int* nudge_vol, double* tempreadint,
+                             int pitch, unsigned* dflags, cudaStream_t s);
+cudaError_t launch_bilinear_nudge(void* T, void* g, bool fp32, size_t plane, int nx, int ny,
+                                  int pitch, const double* ox, const double* oy, const double* oT,
+                                  int nobs, double alpha, long long* acc, unsigned* dflags,
+                                  cudaStream_t s);
+cudaError_t launch_pops_in(const double* h, int layout, void* d, bool fp32, int nx, int ny,
+                           int pitch, size_t plane, double base, cudaStream_t s);
+cudaError_t launch_pops_out(const void* d, int layout, double* h, bool fp32, int nx, int ny,
+                            int pitch, size_t plane, double base, cudaStream_t s);
+cudaError_t launch_scalar_in(const double* h, int layout, void* d, bool fp32, int nx, int ny,
+                             int pitch, cudaStream_t s);
+cudaError_t launch_scalar_out(const void* d, int layout, double* h, bool fp32, int nx, int ny,
+                              int pitch, cudaStream_t s);
+cudaError_t launch_force(const void* rho, const void* T, void* F, bool fp32, int nx, int ny,
+                         int pitch, double neg_gravity, cudaStream_t s);
+cudaError_t launch_moments_from_pre(const double* fpre, const double* gpre, int layout, void* rho,
+                                    void* u, void* v, void* T, bool fp32, int nx, int ny, int pitch,
+                                    double neg_gravity, cudaStream_t s);
+cudaError_t launch_init_conduction(void* pops, void* rho, void* u, void* v, void* T, bool fp32,
+                                   int nx, int ny, int pitch, size_t plane, double Tup,
+                                   double Tdown, double T0, double neg_gravity, uint64_t seed,
+                                   double noise, cudaStream_t s);
+cudaError_t launch_stats(const void* rho, const void* u, const void* v, const void* T, bool fp32,
+                         int nx, int ny, int pitch, double* part, double* out, cudaStream_t s);
+cudaError_t launch_profile(const void* rho, const void* u, const void* v, const void* T, bool fp32,
+                           int nx, int ny, int pitch, double* out, cudaStream_t s);
+cudaError_t launch_finite(const void* a, size_t n, bool fp32, unsigned* flags, cudaStream_t s);
+int red_blocks();
+}  // namespace lbrb
+
+using namespace lbrb;
+
+struct lbrb_s : public Handle {
+  std::vector<int> h_ids;
+  // timing: event pool and the (class, begin, end) marks of this window
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct Mark { int cls; cudaEvent_t a, b; };
+  std::vector<Mark> marks;
+};
+
+static cudaEvent_t pool_event(lbrb_t* h) {
+  if (h->ev_used == h->ev_pool.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    h->ev_pool.push_back(e);
+  }
+  return h->ev_pool[h->ev_used++];
+}
+
+// begin/end of a timed launch on `s` (no-ops unless timing is enabled)
+static int tmark_begin(lbrb_t* h, int cls, cudaStream_t s) {
+  if (!h->timing) return -1;
+  cudaEvent_t a = pool_event(h), b = pool_event(h);
+  if (!a || !b) return -1;
+  cudaEventRecord(a, s);
+  h->marks.push_back({cls, a, b});
+  return (int)h->marks.size() - 1;
+}
+static void tmark_end(lbrb_t* h, int m, cudaStream_t s) {
+  if (m >= 0) cudaEventRecord(h->marks[m].b, s);
+}
+
+// per-observation arrays of the box mode (see nudge_kernels.cu)
+enum { NB_OX = 0, NB_OY, NB_OT, NB_FX, NB_FY, NB_FT, NB_XINT, NB_YINT, NB_TINT, NB_DX, NB_DY,
+       NB_DT, NB_COUNT };
+enum { NBI_CHK = 0, NBI_BC, NBI_XIDX, NBI_YIDX, NBI_COUNT };
+
+static int fail(lbrb_t* h, int code, const std::string& msg, cudaError_t e = cudaSuccess) {
+  if (h) {
+    h->err = msg;
+    if (e != cudaSuccess) h->err += std::string(": ") + cudaGetErrorString(e);
+  }
+  return code;
+}
+
+#define CK(h, call)                                                   \
+  do {                                                                \
+    cudaError_t e_ = (call);                                          \
+    if (e_ != cudaSuccess) return fail((h), LBRB_ERR_CUDA, #call, e_); \
+  } while (0)
+
+static bool fp32(const lbrb_t* h) { return h->p.precision == LBRB_PREC_FP32_SHIFTED; }
+static double T0_of(const lbrb_t* h) { return 0.5 * (h->p.Tup + h->p.Tdown); }
+
+static char* pop_base(const lbrb_t* h, int buf, int which /*0 f, 1 g*/) {
+  return (char*)h->pops[buf] + (size_t)which * NPOP * h->plane * h->esize;
+}
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e == cudaSuccess) e = cudaMemset(*p, 0, count * sizeof(T));
+  return e;
+}
+
+static size_t host_pops_count(const lbrb_t* h, int layout) {
+  return layout == LBRB_LAYOUT_REF_AOS_HALO ? (size_t)(h->p.nx + 2) * (h->p.ny + 2) * NPOP
+                                            : (size_t)NPOP * h->p.nx * h->p.ny;
+}
+static size_t host_scalar_count(const lbrb_t* h, int layout) {
+  return layout == LBRB_LAYOUT_REF_AOS_HALO ? (size_t)(h->p.nx + 2) * (h->p.ny + 2)
+                                            : (size_t)h->p.nx * h->p.ny;
+}
+
+static int ensure_staging(lbrb_t* h, size_t bytes) {
+  if (h->staging_bytes >= bytes) return LBRB_OK;
+  if (h->staging) cudaFree(h->staging);
+  h->staging = nullptr;
+  h->staging_bytes = 0;
+  cudaError_t e = cudaMalloc(&h->staging, bytes);
+  if (e != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "staging allocation", e);
+  h->staging_bytes = bytes;
+  return LBRB_OK;
+}
+
+extern "C" {
+
+int lbrb_abi_version(void) { return LBRB_ABI_VERSION; }
+
+void lbrb_params_default(lbrb_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  // reference values: temppart_dump.c:16-28, Trajectories/code/mympi2.h:14-19,
+  // tempvel_nudge.c:13, 23
+  p->nx = 1680;
+  p->ny = 840;
+  p->relax = 0.502;
+  p->relaxg = 0.502;
+  p->Tup = -0.01;
+  p->Tdown = 0.01;
+  p->gravity = -0.00004;
+  p->precision = LBRB_PREC_FP64;
+  p->twall = LBRB_TWALL_DIRICHLET;
+  p->nudge = LBRB_NUDGE_NONE;
+  p->alpha = 0.01;
+  p->ntempread = 250;
+  p->nobs = 0;
+  p->beta = 0.1;
+  p->nprtcl = 0;
+  p->noutconfig = 0;
+  p->record_full = 0;
+  p->record_slots = 16;
+  p->device = 0;
+}
+
+const char* lbrb_last_error(const lbrb_t* h) { return h ? h->err.c_str() : "null handle"; }
+
+static void free_all(lbrb_t* h) {
+  auto F = [](void* q) { if (q) cudaFree(q); };
+  F(h->pops[0]); F(h->pops[1]); F(h->F); F(h->rho); F(h->T);
+  for (int a = 0; a < 2; a++) for (int b = 0; b < 2; b++) F(h->uv[a][b]);
+  F(h->px); F(h->pid); F(h->ptype); F(h->d_ring);
+  if (h->h_ring) cudaFreeHost(h->h_ring);
+  delete[] h->h_ring_step;
+  if (h->ring_ev) {
+    for (int s = 0; s < h->p.record_slots; s++) if (h->ring_ev[s]) cudaEventDestroy(h->ring_ev[s]);
+    delete[] h->ring_ev;
+  }
+  F(h->nb); F(h->nbi); F(h->nudge_vol); F(h->tempreadint); F(h->nud_term);
+  F(h->cell_count); F(h->cell_start); F(h->cell_fill); F(h->cell_dirty); F(h->cell_items);
+  delete[] h->h_chk; delete[] h->h_oid;
+  F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
+  if (h->h_flags) cudaFreeHost(h->h_flags);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->join_ev) cudaEventDestroy(h->join_ev);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+}
+
+int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
+  if (!pin || !out) return LBRB_ERR_ARG;
+  *out = nullptr;
+  const lbrb_params& p = *pin;
+  auto bad = [](double x) { return !(x == x) || x > 1e300 || x < -1e300; };
+  if (p.nx < 4 || p.nx % 4 != 0 || p.ny < 3 || bad(p.relax) || bad(p.relaxg) || p.relax <= 0.5 ||
+      p.relaxg <= 0.5 || bad(p.Tup) || bad(p.Tdown) || bad(p.gravity) || bad(p.alpha) ||
+      bad(p.beta) || p.nprtcl < 0 || p.noutconfig < 0 || p.nobs < 0 ||
+      (p.precision != LBRB_PREC_FP64 && p.precision != LBRB_PREC_FP32_SHIFTED) ||
+      (p.twall != LBRB_TWALL_DIRICHLET && p.twall != LBRB_TWALL_ADIABATIC) ||
+      (p.nudge < LBRB_NUDGE_NONE || p.nudge > LBRB_NUDGE_BILINEAR))
+    return LBRB_ERR_ARG;
+  if (p.nudge != LBRB_NUDGE_NONE && p.nobs <= 0) return LBRB_ERR_ARG;
+  if (p.nudge == LBRB_NUDGE_REFBOX && p.ntempread < 2) return LBRB_ERR_ARG;
+  if (p.nudge == LBRB_NUDGE_REFBOX && p.precision != LBRB_PREC_FP64) return LBRB_ERR_UNSUPPORTED;
+  if (p.nprtcl > 0 && p.noutconfig > 0 && p.record_slots < 1) return LBRB_ERR_ARG;
+  if ((long)p.nx * p.ny > (1L << 31) - 1) return LBRB_ERR_ARG;
+
+  lbrb_t* h = new lbrb_t();
+  h->p = p;
+  if (h->p.record_slots < 1) h->p.record_slots = 1;
+  h->dev = p.device;
+  int rc = LBRB_OK;
+  auto done = [&](int code) -> int {
+    if (code != LBRB_OK) {
+      free_all(h);
+      delete h;
+      return code;
+    }
+    *out = h;
+    return (int)LBRB_OK;
+  };
+  cudaError_t e = cudaSetDevice(p.device);
+  if (e != cudaSuccess) return done(LBRB_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess)
+    return done(LBRB_ERR_CUDA);
+  h->stream = h->own_stream;
+  h->pitch = (p.nx + 31) / 32 * 32;
+  h->plane = (size_t)p.ny * h->pitch;
+  h->esize = fp32(h) ? 4 : 8;
+  const size_t pb = 2 * NPOP * h->plane * h->esize;
+  for (int b = 0; b < 2; b++) {
+    if (cudaMalloc(&h->pops[b], pb) != cudaSuccess) return done(LBRB_ERR_NOMEM);
+    cudaMemset(h->pops[b], 0, pb);
+  }
+  void** scal[] = {&h->F, &h->rho, &h->T, &h->uv[0][0], &h->uv[0][1], &h->uv[1][0], &h->uv[1][1]};
+  for (void** s : scal) {
+    if (cudaMalloc(s, h->plane * h->esize) != cudaSuccess) return done(LBRB_ERR_NOMEM);
+    cudaMemset(*s, 0, h->plane * h->esize);
+  }
+  h->np = p.nprtcl;
+  if (h->np > 0) {
+    if (dalloc(&h->px, (size_t)9 * h->np) || dalloc(&h->pid, h->np) || dalloc(&h->ptype, h->np))
+      return done(LBRB_ERR_NOMEM);
+    h->nrec_fields = p.record_full ? LBRB_REC_NFULL : LBRB_REC_NBASIC;
+    if (p.noutconfig > 0) {
+      const size_t rb = (size_t)h->p.record_slots * h->nrec_fields * h->np;
+      if (dalloc(&h->d_ring, rb)) return done(LBRB_ERR_NOMEM);
+      if (cudaMallocHost(&h->h_ring, rb * sizeof(double)) != cudaSuccess) return done(LBRB_ERR_NOMEM);
+      h->h_ring_step = new int[h->p.record_slots]();
+      h->ring_ev = new cudaEvent_t[h->p.record_slots]();
+      for (int s = 0; s < h->p.record_slots; s++)
+        if (cudaEventCreateWithFlags(&h->ring_ev[s], cudaEventDisableTiming) != cudaSuccess)
+          return done(LBRB_ERR_CUDA);
+    }
+  }
+  h->nobs = p.nobs;
+  if (p.nudge == LBRB_NUDGE_REFBOX) {
+    const int n = h->nobs;
+    h->ncx = (p.nx + 7) / 8;
+    h->ncy = (p.ny + 7) / 8;
+    const size_t nc = (size_t)h->ncx * h->ncy;
+    if (dalloc(&h->nb, (size_t)NB_COUNT * n) || dalloc(&h->nbi, (size_t)NBI_COUNT * n) ||
+        dalloc(&h->nudge_vol, h->plane) || dalloc(&h->tempreadint, h->plane) ||
+        dalloc(&h->nud_term, h->plane) || dalloc(&h->cell_count, nc) ||
+        dalloc(&h->cell_start, nc) || dalloc(&h->cell_fill, nc) || dalloc(&h->cell_dirty, nc) ||
+        dalloc(&h->cell_items, (size_t)2 * 12 * n))
+      return done(LBRB_ERR_NOMEM);
+    h->h_chk = new int[n]();
+    h->h_oid = new int[n]();
+  }
+  if (p.nudge == LBRB_NUDGE_BILINEAR) {
+    if (dalloc(&h->acc, h->plane)) return done(LBRB_ERR_NOMEM);
+  }
+  if (dalloc(&h->red, (size_t)red_blocks() * 6 + 8 + (size_t)p.ny * 9)) return done(LBRB_ERR_NOMEM);
+  if (dalloc(&h->dflags, 1)) return done(LBRB_ERR_NOMEM);
+  if (cudaMallocHost(&h->h_flags, sizeof(unsigned)) != cudaSuccess) return done(LBRB_ERR_NOMEM);
+  if (cudaDeviceSynchronize() != cudaSuccess) return done(LBRB_ERR_CUDA);
+  (void)rc;
+  return done(LBRB_OK);
+}
+
+int lbrb_destroy(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  cudaSetDevice(h->dev);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  free_all(h);
+  delete h;
+  return LBRB_OK;
+}
+
+int lbrb_get_istep(const lbrb_t* h, int* istep) {
+  if (!h || !istep) return LBRB_ERR_ARG;
+  *istep = h->istep;
+  return LBRB_OK;
+}
+
+int lbrb_set_istep(lbrb_t* h, int istep) {
+  if (!h || istep < 0) return LBRB_ERR_ARG;
+  h->istep = istep;
+  return LBRB_OK;
+}
+
+// ------------------------------------------------------------- state I/O
+int lbrb_set_populations(lbrb_t* h, const double* f, const double* g, int layout) {
+  if (!h || !f || !g || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
+    return fail(h, LBRB_ERR_ARG, "set_populations: bad arguments");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
+  int rc = ensure_staging(h, 2 * bytes);
+  if (rc) return rc;
+  double* st = (double*)h->staging;
+  CK(h, cudaMemcpyAsync(st, f, bytes, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(st + cnt, g, bytes, cudaMemcpyHostToDevice, h->stream));
+  CK(h, launch_pops_in(st, layout, pop_base(h, h->cur, 0), fp32(h), h->p.nx, h->p.ny, h->pitch,
+                       h->plane, 1.0, h->stream));
+  CK(h, launch_pops_in(st + cnt, layout, pop_base(h, h->cur, 1), fp32(h), h->p.nx, h->p.ny,
+                       h->pitch, h->plane, T0_of(h), h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return LBRB_OK;
+}
+
+int lbrb_get_populations(lbrb_t* h, double* f, double* g, int layout) {
+  if (!h || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
+    return fail(h, LBRB_ERR_ARG, "get_populations: bad arguments");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
+  int rc = ensure_staging(h, 2 * bytes);
+  if (rc) return rc;
+  double* st = (double*)h->staging;
+  if (f) {
+    CK(h, launch_pops_out(pop_base(h, h->cur, 0), layout, st, fp32(h), h->p.nx, h->p.ny, h->pitch,
+                          h->plane, 1.0, h->stream));
+    CK(h, cudaMemcpyAsync(f, st, bytes, cudaMemcpyDeviceToHost, h->stream));
+  }
+  if (g) {
+    CK(h, launch_pops_out(pop_base(h, h->cur, 1), layout, st + cnt, fp32(h), h->p.nx, h->p.ny,
+                          h->pitch, h->plane, T0_of(h), h->stream));
+    CK(h, cudaMemcpyAsync(g, st + cnt, bytes, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  return LBRB_OK;
+}
+
+int lbrb_set_moments(lbrb_t* h, const double* rho, const double* u, const double* v,
+                     const double* T, int layout) {
+  if (!h || !rho || !u || !v || !T || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
+    return fail(h, LBRB_ERR_ARG, "set_moments: bad arguments");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t cnt = host_scalar_count(h, layout), bytes = cnt * sizeof(double);
+  int rc = ensure_staging(h, 4 * bytes);
+  if (rc) return rc;
+  double* st = (double*)h->staging;
+  const double* src[4] = {rho, u, v, T};
+  void* dst[4] = {h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T};
+  for (int a = 0; a < 4; a++) {
+    CK(h, cudaMemcpyAsync(st + a * cnt, src[a], bytes, cudaMemcpyHostToDevice, h->stream));
+    CK(h, launch_scalar_in(st + a * cnt, layout, dst[a], fp32(h), h->p.nx, h->p.ny, h->pitch, h->stream));
+  }
+  CK(h, launch_force(h->rho, h->T, h->F, fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->moments_valid = true;
+  return LBRB_OK;
+}
+
+int lbrb_get_moments(lbrb_t* h, double* rho, double* u, double* v, double* T, int layout) {
+  if (!h || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
+    return fail(h, LBRB_ERR_ARG, "get_moments: bad arguments");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t cnt = host_scalar_count(h, layout), bytes = cnt * sizeof(double);
+  int rc = ensure_staging(h, 4 * bytes);
+  if (rc) return rc;
+  double* st = (double*)h->staging;
+  double* dst[4] = {rho, u, v, T};
+  const void* src[4] = {h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T};
+  for (int a = 0; a < 4; a++) {
+    if (!dst[a]) continue;
+    CK(h, launch_scalar_out(src[a], layout, st + a * cnt, fp32(h), h->p.nx, h->p.ny, h->pitch, h->stream));
+    CK(h, cudaMemcpyAsync(dst[a], st + a * cnt, bytes, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  return LBRB_OK;
+}
+
+int lbrb_moments_from_pre(lbrb_t* h, const double* fpre, const double* gpre, int layout) {
+  if (!h || !fpre || !gpre || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
+    return fail(h, LBRB_ERR_ARG, "moments_from_pre: bad arguments");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
+  int rc = ensure_staging(h, 2 * bytes);
+  if (rc) return rc;
+  double* st = (double*)h->staging;
+  CK(h, cudaMemcpyAsync(st, fpre, bytes, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(st + cnt, gpre, bytes, cudaMemcpyHostToDevice, h->stream));
+  CK(h, launch_moments_from_pre(st, st + cnt, layout, h->rho, h->uv[h->uvcur][0],
+                                h->uv[h->uvcur][1], h->T, fp32(h), h->p.nx, h->p.ny, h->pitch,
+                                -h->p.gravity, h->stream));
+  CK(h, launch_force(h->rho, h->T, h->F, fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->moments_valid = true;
+  return LBRB_OK;
+}
+
+int lbrb_init_conduction(lbrb_t* h, uint64_t seed, double noise) {
+  if (!h || !(noise == noise)) return fail(h, LBRB_ERR_ARG, "init_conduction: bad arguments");
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, launch_init_conduction(h->pops[h->cur], h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1],
+                               h->T, fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->p.Tup,
+                               h->p.Tdown, T0_of(h), -h->p.gravity, seed, noise, h->stream));
+  CK(h, launch_force(h->rho, h->T, h->F, fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->moments_valid = true;
+  return LBRB_OK;
+}
+
+// ------------------------------------------------------------- particles
+int lbrb_particles_set(lbrb_t* h, int n, const int* ids, const double* x, const double* y,
+                       const double* u, const double* v, const int* ptype, const double* invtau) {
+  if (!h || n != h->np || n <= 0 || !ids || !x || !y || !u || !v || !ptype || !invtau)
+    return fail(h, LBRB_ERR_ARG, "particles_set: arguments must cover all nprtcl particles");
+  for (int q = 0; q < n; q++) {
+    if (!(x[q] > -1.0 && x[q] < h->p.nx + 1.0 && y[q] >= 0.0 && y[q] <= h->p.ny + 1.0))
+      return fail(h, LBRB_ERR_RANGE, "particles_set: position outside the domain");
+    if (!(u[q] == u[q]) || !(v[q] == v[q]) || !(invtau[q] >= 0.0) ||
+        (ptype[q] != LBRB_PTYPE_TRACER && ptype[q] != LBRB_PTYPE_INERTIAL))
+      return fail(h, LBRB_ERR_ARG, "particles_set: bad velocity, type or 1/tau");
+  }
+  CK(h, cudaSetDevice(h->dev));
+  std::vector<double> P((size_t)9 * n);
+  std::memcpy(&P[0 * (size_t)n], x, n * sizeof(double));
+  std::memcpy(&P[1 * (size_t)n], y, n * sizeof(double));
+  std::memcpy(&P[2 * (size_t)n], u, n * sizeof(double));
+  std::memcpy(&P[3 * (size_t)n], v, n * sizeof(double));
+  std::memcpy(&P[4 * (size_t)n], x, n * sizeof(double));
+  std::memcpy(&P[5 * (size_t)n], y, n * sizeof(double));
+  std::memcpy(&P[6 * (size_t)n], u, n * sizeof(double));
+  std::memcpy(&P[7 * (size_t)n], v, n * sizeof(double));
+  std::memcpy(&P[8 * (size_t)n], invtau, n * sizeof(double));
+  CK(h, cudaMemcpyAsync(h->px, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->pid, ids, n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->ptype, ptype, n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->h_ids.assign(ids, ids + n);
+  h->particles_set = true;
+  return LBRB_OK;
+}
+
+int lbrb_particles_get(lbrb_t* h, int n, int* ids, double* x, double* y, double* u, double* v,
+                       double* xo, double* yo, double* uo, double* vo) {
+  if (!h || n != h->np || n <= 0) return fail(h, LBRB_ERR_ARG, "particles_get: n must be nprtcl");
+  CK(h, cudaSetDevice(h->dev));
+  std::vector<double> P((size_t)9 * n);
+  CK(h, cudaMemcpyAsync(P.data(), h->px, P.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  double* outs[8] = {x, y, u, v, xo, yo, uo, vo};
+  for (int a = 0; a < 8; a++)
+    if (outs[a]) std::memcpy(outs[a], &P[(size_t)a * n], n * sizeof(double));
+  if (ids) std::memcpy(ids, h->h_ids.data(), n * sizeof(int));
+  return LBRB_OK;
+}
+
+// --------------------------------------------------------------- records
+int lbrb_record_pending(lbrb_t* h, int* count) {
+  if (!h || !count) return LBRB_ERR_ARG;
+  *count = (int)(h->rec_head - h->rec_tail);
+  return LBRB_OK;
+}
+
+int lbrb_record_drain(lbrb_t* h, int max_records, int* steps, double* buf, int* ids, int* n_drained) {
+  if (!h || max_records < 0 || (max_records > 0 && (!steps || !buf)))
+    return fail(h, LBRB_ERR_ARG, "record_drain: bad arguments");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t per = (size_t)h->nrec_fields * h->np;
+  int k = 0;
+  while (k < max_records && h->rec_tail < h->rec_head) {
+    const int slot = (int)(h->rec_tail % h->p.record_slots);
+    CK(h, cudaEventSynchronize(h->ring_ev[slot]));
+    std::memcpy(buf + (size_t)k * per, h->h_ring + (size_t)slot * per, per * sizeof(double));
+    steps[k] = h->h_ring_step[slot];
+    h->rec_tail++;
+    k++;
+  }
+  if (ids && h->np > 0) std::memcpy(ids, h->h_ids.data(), h->np * sizeof(int));
+  if (n_drained) *n_drained = k;
+  return LBRB_OK;
+}
+
+// --------------------------------------------------------------- nudging
+int lbrb_nudge_init(lbrb_t* h, int n, const double* x, const double* y, const double* T,
+                    const int* ids) {
+  if (!h || h->p.nudge != LBRB_NUDGE_REFBOX || n != h->nobs || !x || !y || !T || !ids)
+    return fail(h, LBRB_ERR_ARG, "nudge_init: box nudging with n == nobs required");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t b = n * sizeof(double);
+  double* nb = h->nb;
+  const double* src[6] = {x, y, T, x, y, T};
+  const int dst[6] = {NB_OX, NB_OY, NB_OT, NB_XINT, NB_YINT, NB_TINT};
+  for (int a = 0; a < 6; a++)
+    CK(h, cudaMemcpyAsync(nb + (size_t)dst[a] * n, src[a], b, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemsetAsync(h->nbi, 0, sizeof(int) * NBI_COUNT * (size_t)n, h->stream));
+  CK(h, cudaMemsetAsync(h->nud_term, 0, sizeof(double) * h->plane, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(h->h_oid, ids, n * sizeof(int));
+  std::memset(h->h_chk, 0, n * sizeof(int));
+  h->nudge_init_done = true;
+  return LBRB_OK;
+}
+
+int lbrb_nudge_load(lbrb_t* h, int n, const double* x, const double* y, const int* ids,
+                    const double* T) {
+  if (!h || h->p.nudge != LBRB_NUDGE_REFBOX || n != h->nobs || !x || !y || !T || !ids)
+    return fail(h, LBRB_ERR_ARG, "nudge_load: box nudging with n == nobs required");
+  if (!h->nudge_init_done) return fail(h, LBRB_ERR_STATE, "nudge_load before nudge_init");
+  // read_prtcl matches ids by a first-hit search (tempvel_nudge.c:1480-1487);
+  // the same first occurrence through a hash map
+  std::unordered_map<int, int> first;
+  first.reserve((size_t)n * 2);
+  for (int j = 0; j < n; j++) first.emplace(ids[j], j);
+  for (int i = 0; i < n; i++) {
+    auto it = first.find(h->h_oid[i]);
+    if (it == first.end()) return fail(h, LBRB_ERR_IDS, "nudge_load: an observed id is missing from the file");
+    h->h_chk[i] = it->second;
+  }
+  CK(h, cudaSetDevice(h->dev));
+  const size_t b = n * sizeof(double);
+  CK(h, cudaMemcpyAsync(h->nb + (size_t)NB_FX * n, x, b, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->nb + (size_t)NB_FY * n, y, b, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->nb + (size_t)NB_FT * n, T, b, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->nbi + (size_t)NBI_CHK * n, h->h_chk, n * sizeof(int),
+                        cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->nudge_file_loaded = true;
+  return LBRB_OK;
+}
+
+int lbrb_nudge_obs(lbrb_t* h, int first_step, int nsteps, const double* x, const double* y,
+                   const double* T) {
+  if (!h || h->p.nudge != LBRB_NUDGE_BILINEAR || nsteps < 1 || !x || !y || !T)
+    return fail(h, LBRB_ERR_ARG, "nudge_obs: bilinear nudging required");
+  CK(h, cudaSetDevice(h->dev));
+  const int n = h->nobs;
+  if (nsteps > h->obs_cap_steps) {
+    if (h->obs) cudaFree(h->obs);
+    h->obs = nullptr;
+    h->obs_cap_steps = 0;
+    cudaError_t e = cudaMalloc(&h->obs, (size_t)nsteps * 3 * n * sizeof(double));
+    if (e != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "nudge_obs allocation", e);
+    h->obs_cap_steps = nsteps;
+  }
+  CK(h, cudaStreamSynchronize(h->stream));  // the previous series may still be in use
+  for (int s = 0; s < nsteps; s++) {
+    double* base = h->obs + (size_t)s * 3 * n;
+    CK(h, cudaMemcpyAsync(base, x + (size_t)s * n, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(base + n, y + (size_t)s * n, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(base + 2 * n, T + (size_t)s * n, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->obs_first = first_step;
+  h->obs_nsteps = nsteps;
+  return LBRB_OK;
+}
+
+// ------------------------------------------------------------- time loop
+int lbrb_step(lbrb_t* h, int n) {
+  if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
+  if (n == 0) return LBRB_OK;
+  if (!h->moments_valid)
+    return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
+  if (h->np > 0 && !h->particles_set) return fail(h, LBRB_ERR_STATE, "step: particles not set");
+  if (h->p.nudge == LBRB_NUDGE_REFBOX && !h->nudge_init_done)
+    return fail(h, LBRB_ERR_STATE, "step: nudge_init not called");
+  CK(h, cudaSetDevice(h->dev));
+  const bool f32 = fp32(h);
+  const int nx = h->p.nx, ny = h->p.ny;
+  const int vecn = f32 ? 4 : 2;
+  const int chunks = (nx + WARP * vecn - 1) / (WARP * vecn);
+  for (int s = 0; s < n; s++) {
+    const int istep = h->istep + 1;
+    const bool last = (s == n - 1);
+    const bool rec = h->np > 0 && h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
+    if (rec && (h->rec_head - h->rec_tail) >= h->p.record_slots)
+      return fail(h, LBRB_ERR_OVERFLOW, "step: record ring full, drain records first");
+    const double* obs = nullptr;
+    if (h->p.nudge == LBRB_NUDGE_BILINEAR) {
+      if (!h->obs || istep < h->obs_first || istep >= h->obs_first + h->obs_nsteps)
+        return fail(h, LBRB_ERR_STATE, "step: no bilinear observations for this step");
+      obs = h->obs + (size_t)(istep - h->obs_first) * 3 * h->nobs;
+    }
+    if (h->p.nudge == LBRB_NUDGE_REFBOX) {
+      const int nt = h->p.ntempread;
+      if (istep % nt == 1 && !h->nudge_file_loaded)
+        return fail(h, LBRB_ERR_STATE, "step: observation file for this interval not loaded");
+      const int tm = tmark_begin(h, 2, h->stream);
+      CK(h, launch_box_nudge(h->nb, h->nbi, h->nobs, nx, ny, nt, istep, h->ncx, h->ncy,
+                             h->cell_count, h->cell_start, h->cell_fill, h->cell_dirty,
+                             h->cell_items, h->nudge_vol, h->tempreadint, h->pitch, h->dflags,
+                             h->stream));
+      tmark_end(h, tm, h->stream);
+      if (istep % nt == 1) h->nudge_file_loaded = false;
+    }
+    const int write_uv = (h->np > 0) || last;
+    const int write_rt = last || rec || h->p.nudge == LBRB_NUDGE_BILINEAR;
+    const int uvn = write_uv ? (h->uvcur ^ 1) : h->uvcur;
+    const int src = h->cur, dst = h->cur ^ 1;
+    if (f32) {
+      LBView<float> V{};
+      V.fsrc = (const float*)pop_base(h, src, 0);
+      V.gsrc = (const float*)pop_base(h, src, 1);
+      V.fdst = (float*)pop_base(h, dst, 0);
+      V.gdst = (float*)pop_base(h, dst, 1);
+      V.F = (float*)h->F; V.rho = (float*)h->rho; V.T = (float*)h->T;
+      V.u = (float*)h->uv[uvn][0]; V.v = (float*)h->uv[uvn][1];
+      V.nx = nx; V.ny = ny; V.pitch = h->pitch; V.plane = h->plane;
+      V.omega = 1. / h->p.relax; V.omegag = 1. / h->p.relaxg; V.neg_gravity = -h->p.gravity;
+      V.Tup = h->p.Tup; V.Tdown = h->p.Tdown; V.T0 = T0_of(h);
+      V.write_uv = write_uv; V.write_rt = write_rt;
+      V.chunks_per_row = chunks; V.ntasks = (long)chunks * ny;
+      const int tm = tmark_begin(h, 0, h->stream);
+      CK(h, launch_lb_fp32(V, h->p.twall, h->stream));
+      tmark_end(h, tm, h->stream);
+    } else {
+      LBView<double> V{};
+      V.fsrc = (const double*)pop_base(h, src, 0);
+      V.gsrc = (const double*)pop_base(h, src, 1);
+      V.fdst = (double*)pop_base(h, dst, 0);
+      V.gdst = (double*)pop_base(h, dst, 1);
+      V.F = (double*)h->F; V.rho = (double*)h->rho; V.T = (double*)h->T;
+      V.u = (double*)h->uv[uvn][0]; V.v = (double*)h->uv[uvn][1];
+      V.nx = nx; V.ny = ny; V.pitch = h->pitch; V.plane = h->plane;
+      V.omega = 1. / h->p.relax; V.omegag = 1. / h->p.relaxg; V.neg_gravity = -h->p.gravity;
+      V.Tup = h->p.Tup; V.Tdown = h->p.Tdown; V.T0 = T0_of(h);
+      V.nudge_vol = h->nudge_vol; V.tempreadint = h->tempreadint; V.nud_term = h->nud_term;
+      V.alpha = h->p.alpha;
+      V.write_uv = write_uv; V.write_rt = write_rt;
+      V.chunks_per_row = chunks; V.ntasks = (long)chunks * ny;
+      const int tm = tmark_begin(h, 0, h->stream);
+      CK(h, launch_lb_fp64(V, h->p.twall, h->p.nudge == LBRB_NUDGE_REFBOX, h->stream));
+      tmark_end(h, tm, h->stream);
+    }
+    if (obs) {
+      const int tm = tmark_begin(h, 2, h->stream);
+      CK(h, launch_bilinear_nudge(h->T, pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, obs,
+                                  obs + h->nobs, obs + 2 * (size_t)h->nobs, h->nobs, h->p.alpha,
+                                  h->acc, h->dflags, h->stream));
+      tmark_end(h, tm, h->stream);
+    }
+    if (h->np > 0) {
+      const int slot = rec ? (int)(h->rec_head % h->p.record_slots) : 0;
+      double* rslot = rec ? h->d_ring + (size_t)slot * h->nrec_fields * h->np : nullptr;
+      const int tm = tmark_begin(h, 1, h->stream);
+      CK(h, launch_particles(h->uv[uvn][0], h->uv[uvn][1], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
+                             h->T, f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta,
+                             rec ? 1 : 0, h->p.record_full, rslot, h->dflags, h->stream));
+      tmark_end(h, tm, h->stream);
+      if (rec) {
+        h->h_ring_step[slot] = istep;
+        CK(h, cudaEventRecord(h->ring_ev[slot], h->stream));
+        CK(h, cudaStreamWaitEvent(h->copy_stream, h->ring_ev[slot], 0));
+        const size_t per = (size_t)h->nrec_fields * h->np;
+        const int tc = tmark_begin(h, 3, h->copy_stream);
+        CK(h, cudaMemcpyAsync(h->h_ring + (size_t)slot * per, rslot, per * sizeof(double),
+                              cudaMemcpyDeviceToHost, h->copy_stream));
+        tmark_end(h, tc, h->copy_stream);
+        CK(h, cudaEventRecord(h->ring_ev[slot], h->copy_stream));
+        h->rec_head++;
+        h->join_pending = true;
+      }
+    }
+    h->cur = dst;
+    h->uvcur = uvn;
+    h->istep = istep;
+  }
+  if (h->join_pending) {
+    // the caller's stream sees the record copies as part of the step
+    CK(h, cudaEventRecord(h->join_ev, h->copy_stream));
+    CK(h, cudaStreamWaitEvent(h->stream, h->join_ev, 0));
+    h->join_pending = false;
+  }
+  return LBRB_OK;
+}
+
+int lbrb_set_stream(lbrb_t* h, void* cuda_stream) {
+  if (!h) return LBRB_ERR_ARG;
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+  return LBRB_OK;
+}
+
+int lbrb_set_timing(lbrb_t* h, int enable) {
+  if (!h) return LBRB_ERR_ARG;
+  h->timing = enable != 0;
+  return LBRB_OK;
+}
+
+int lbrb_get_timing(lbrb_t* h, double* ms, int* launches, int n) {
+  if (!h || n < 0 || n > 4) return fail(h, LBRB_ERR_ARG, "get_timing: n must be 0..4");
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaStreamSynchronize(h->copy_stream));
+  double acc[4] = {0, 0, 0, 0};
+  int cnt[4] = {0, 0, 0, 0};
+  for (const auto& m : h->marks) {
+    float t = 0.f;
+    CK(h, cudaEventElapsedTime(&t, m.a, m.b));
+    acc[m.cls] += t;
+    cnt[m.cls]++;
+  }
+  for (int c = 0; c < n; c++) {
+    if (ms) ms[c] = acc[c];
+    if (launches) launches[c] = cnt[c];
+  }
+  h->marks.clear();
+  h->ev_used = 0;
+  return LBRB_OK;
+}
+
+int lbrb_sync(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaStreamSynchronize(h->copy_stream));
+  CK(h, cudaMemcpy(h->h_flags, h->dflags, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  const unsigned f = *h->h_flags;
+  if (f & DFLAG_NONFINITE) return fail(h, LBRB_ERR_NONFINITE, "device: non-finite value seen");
+  if (f & DFLAG_RANGE) return fail(h, LBRB_ERR_RANGE, "device: particle or observation outside the domain");
+  if (f & DFLAG_BOXCAP) return fail(h, LBRB_ERR_STATE, "device: box nudging list inconsistent");
+  return LBRB_OK;
+}
+
+int lbrb_check_finite(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, launch_finite(h->pops[h->cur], 2 * NPOP * h->plane, fp32(h), h->dflags, h->stream));
+  return lbrb_sync(h);
+}
+
+// ------------------------------------------------------------ diagnostics
+static int stats(lbrb_t* h, double out[3]) {
+  if (!h->moments_valid) return fail(h, LBRB_ERR_STATE, "diagnostics: no moments yet");
+  CK(h, cudaSetDevice(h->dev));
+  double* part = h->red;
+  double* res = h->red + (size_t)red_blocks() * 6;
+  CK(h, launch_stats(h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T, fp32(h), h->p.nx,
+                     h->p.ny, h->pitch, part, res, h->stream));
+  CK(h, cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return LBRB_OK;
+}
+
+int lbrb_energy(lbrb_t* h, double* ke_mean, double* t_mean) {
+  if (!h) return LBRB_ERR_ARG;
+  double s[3];
+  int rc = stats(h, s);
+  if (rc) return rc;
+  const double nn = (double)h->p.nx * (double)h->p.ny;
+  if (ke_mean) *ke_mean = s[0] / nn;
+  if (t_mean) *t_mean = s[1] / nn;
+  return LBRB_OK;
+}
+
+int lbrb_nusselt(lbrb_t* h, double* nu) {
+  if (!h || !nu) return LBRB_ERR_ARG;
+  double s[3];
+  int rc = stats(h, s);
+  if (rc) return rc;
+  const double nn = (double)h->p.nx * (double)h->p.ny;
+  const double kappa = (h->p.relaxg - 0.5) / 3.0;
+  *nu = 1.0 + (s[2] / nn) * (double)h->p.ny / (kappa * (h->p.Tdown - h->p.Tup));
+  return LBRB_OK;
+}
+
+int lbrb_profile(lbrb_t* h, double* out) {
+  if (!h || !out) return LBRB_ERR_ARG;
+  if (!h->moments_valid) return fail(h, LBRB_ERR_STATE, "profile: no moments yet");
+  CK(h, cudaSetDevice(h->dev));
+  double* dout = h->red + (size_t)red_blocks() * 6 + 8;
+  CK(h, launch_profile(h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T, fp32(h), h->p.nx,
+                       h->p.ny, h->pitch, dout, h->stream));
+  CK(h, cudaMemcpyAsync(out, dout, (size_t)h->p.ny * 9 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  const double kappa = (h->p.relaxg - 0.5) / 3.0;
+  const double dTw = h->p.Tdown - h->p.Tup;
+  for (int j = 0; j < h->p.ny; j++)
+    out[(size_t)j * 9 + 8] = (out[(size_t)j * 9 + 6] - kappa * out[(size_t)j * 9 + 7]) / (kappa * dTw / (double)h->p.ny);
+  return LBRB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,288 @@
+// lb_kernels.cu -- the fused pull stream + walls + buoyancy + moments +
+// collision kernel: one launch per time step, both populations f and g.
+//
+// Reference semantics (temppart_dump.c, Trajectories):
+//   stream          :781-854   f_k(x) <- f_k(x - c_k) for k = 1..8, same for g
+//   force           :744-755   F_y = -gravity * rho^{n-1} * T^{n-1}, F_x = 0
+//   f walls         :763-777, 859-894   half-way bounce-back from the
+//                              pre-stream wall row: f2,f5,f6(1) <- f4,f7,f8(1);
+//                              f4,f7,f8(NY) <- f2,f5,f6(NY)
+//   g walls (T)     :896-921   g_in = -g_opp(post-stream) + 2 w T_wall
+//   g walls (N)     tempvel_nudge.c:684-702, 783-962: rows 1 and NY hold
+//                              pre-stream copies of rows 2 and NY-1 and are
+//                              not streamed into
+//   moments         :957-987 (tempvel_nudge.c:1069-1102 adds 1/2 nud_term)
+//   collision       :1097-1180, 1314-1341 (tempvel_nudge.c:1917-1945 nudged g)
+//
+// Two arithmetic forms:
+//   Real = double, SHIFT = false: the reference's operation order exactly
+//     (built with --fmad=false), bit-identical to the reference on x86-64.
+//   Real = float, SHIFT = true: populations stored as deviations from their
+//     weights (f_k - w_k rho0, g_k - w_k T0), collision in FP32.
+//
+// Mapping: a warp owns VEC*32 consecutive nodes of one row (VEC = 2 doubles
+// or 4 floats per lane, one 16-byte access per population); the x neighbour
+// values come by warp shuffle, the row ends by periodic scalar loads.  Wall
+// handling is warp-uniform (one row per warp).  Grid-stride over (row, chunk)
+// tasks with a grid sized to fill every SM.
+#include <type_traits>
+
+#include "lbrb_internal.cuh"
+
+namespace lbrb {
+
+template <int K, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (K > 0) {
+    static_for<K - 1>(f);
+    f(std::integral_constant<int, K - 1>{});
+  }
+}
+
+// ---------------------------------------------------------------- pulls
+template <typename Real>
+__device__ __forceinline__ void pull_f(const LBView<Real>& V, int j, int x0, int lane,
+                                       Real (&fs)[NPOP][Vec<Real>::N]) {
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    const int js = j - icy(k);
+    if (js < 0 || js >= V.ny) {
+      // bounce-back: the opposite population of this node, before streaming
+      load_pull_x<0, Real>(V.fsrc + (size_t)opp(k) * V.plane + (size_t)j * V.pitch, x0, lane,
+                           V.nx, fs[k]);
+    } else {
+      load_pull_x<icx(k), Real>(V.fsrc + (size_t)k * V.plane + (size_t)js * V.pitch, x0, lane,
+                                V.nx, fs[k]);
+    }
+  });
+}
+
+template <typename Real, int TWALL>
+__device__ __forceinline__ void pull_g(const LBView<Real>& V, int j, int x0, int lane,
+                                       Real (&gs)[NPOP][Vec<Real>::N]) {
+  constexpr int N = Vec<Real>::N;
+  if (TWALL == LBRB_TWALL_ADIABATIC && (j == 0 || j == V.ny - 1)) {
+    const int jc = (j == 0) ? 1 : V.ny - 2;
+    static_for<NPOP>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      load_pull_x<0, Real>(V.gsrc + (size_t)k * V.plane + (size_t)jc * V.pitch, x0, lane, V.nx,
+                           gs[k]);
+    });
+    return;
+  }
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    int js = j - icy(k);
+    if (TWALL == LBRB_TWALL_ADIABATIC) {
+      if (js == 0) js = 1;
+      else if (js == V.ny - 1) js = V.ny - 2;
+    }
+    if (js < 0 || js >= V.ny) {
+#pragma unroll
+      for (int m = 0; m < N; m++) gs[k][m] = Real(0);
+    } else {
+      load_pull_x<icx(k), Real>(V.gsrc + (size_t)k * V.plane + (size_t)js * V.pitch, x0, lane,
+                                V.nx, gs[k]);
+    }
+  });
+}
+
+// ------------------------------------------------ reference-order FP64 node
+template <bool REFNUDGE>
+__device__ __forceinline__ void node_ref(const LBView<double>& V, size_t idx, double* fs,
+                                         double* gs, double& Fy_io, double& r_out, double& u_out,
+                                         double& v_out, double& t_out) {
+  double r = 0.0, t = 0.0;
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) r = r + fs[k];
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) t = t + gs[k];
+  int nv = 0;
+  if (REFNUDGE) {
+    nv = V.nudge_vol[idx];
+    if (nv > 0) t = (t + 0.5 * V.nud_term[idx]);
+  }
+  const double rhoi = 1. / r;
+  double fl[NPOP];
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) fl[k] = fs[k] * rhoi;
+  const double Fx = 0.0;
+  const double Fy = Fy_io;
+  const double u = fl[1] - fl[3] + fl[5] - fl[6] - fl[7] + fl[8] + 0.5 * rhoi * Fx;
+  const double v = fl[5] + fl[2] + fl[6] - fl[7] - fl[4] - fl[8] + 0.5 * rhoi * Fy;
+  const double omega = V.omega, omegag = V.omegag;
+  double feq[NPOP];
+  equil_ref(r, u, v, feq);
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    double source = (1.0 - 0.5 * omega) * w_of(k);
+    double factor = ((dcx(k) - u) * Fx + (dcy(k) - v) * Fy) / CS2;
+    factor = factor + ((dcx(k) * u + dcy(k) * v) * (dcx(k) * Fx + dcy(k) * Fy)) / (CS2 * CS2);
+    fs[k] = fs[k] * (1. - omega) + omega * feq[k] + source * factor;
+  });
+  equil_ref(t, u, v, feq);
+  if (REFNUDGE && nv > 0) {
+    const double B = 1.0 - 0.5 * omegag;
+    const double Q = V.alpha * (t - V.tempreadint[idx]);
+#pragma unroll
+    for (int k = 0; k < NPOP; k++) gs[k] = gs[k] * (1. - omegag) + omegag * feq[k] - B * w_of(k) * Q;
+    V.nud_term[idx] = -1. * Q;
+  } else {
+#pragma unroll
+    for (int k = 0; k < NPOP; k++) gs[k] = gs[k] * (1. - omegag) + omegag * feq[k];
+  }
+  // buoyancy of the next step from this step's moments (forcingconstructWW)
+  Fy_io = V.neg_gravity * r * (t - 0.0);
+  r_out = r;
+  u_out = u;
+  v_out = v;
+  t_out = t;
+}
+
+// -------------------------------------------------- FP32 shifted-form node
+__device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, float* dg,
+                                           float& Fy_io, float& r_out, float& u_out,
+                                           float& v_out, float& t_out) {
+  float dr = 0.f, dT = 0.f;
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) dr += df[k];
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) dT += dg[k];
+  const float r = 1.f + dr;
+  const float T0 = (float)V.T0;
+  const float t = T0 + dT;
+  const float jx = (df[1] - df[3]) + (df[5] - df[6]) + (df[8] - df[7]);
+  const float jy = (df[2] - df[4]) + (df[5] - df[7]) + (df[6] - df[8]);
+  const float Fy = Fy_io;
+  const float rinv = 1.f / r;
+  const float u = jx * rinv;
+  const float v = (jy + 0.5f * Fy) * rinv;
+  const float om = (float)V.omega, omg = (float)V.omegag;
+  const float srcf = 1.f - 0.5f * om;
+  const float usq15 = 1.5f * (u * u + v * v);
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    constexpr float w = (float)w_of(k);
+    constexpr float cx = (float)icx(k), cy = (float)icy(k);
+    const float cu = cx * u + cy * v;
+    const float P = 3.f * cu + 4.5f * cu * cu - usq15;
+    const float dfeq = w * (dr + r * P);
+    // Guo source with F = (0, Fy): 3 (c - u).F + 9 (c.u)(c.F)
+    const float S = srcf * w * Fy * (3.f * (cy - v) + 9.f * cu * cy);
+    df[k] = df[k] + om * (dfeq - df[k]) + S;
+    const float dgeq = w * (dT + t * P);
+    dg[k] = dg[k] + omg * (dgeq - dg[k]);
+  });
+  Fy_io = (float)V.neg_gravity * r * t;
+  r_out = r;
+  u_out = u;
+  v_out = v;
+  t_out = t;
+}
+
+// ------------------------------------------------------------------ kernel
+template <typename Real, int TWALL, bool REFNUDGE>
+__global__ void __launch_bounds__(256) lb_step_kernel(const LBView<Real> V) {
+  constexpr int N = Vec<Real>::N;
+  const int lane = threadIdx.x & (WARP - 1);
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+  for (long task = gw; task < V.ntasks; task += nw) {
+    const int j = (int)(task / V.chunks_per_row);
+    const int chunk = (int)(task - (long)j * V.chunks_per_row);
+    int x0 = chunk * (WARP * N) + lane * N;
+    const bool active = x0 < V.nx;
+    if (!active) x0 = 0;  // in-bounds loads; results are discarded
+    Real fs[NPOP][N], gs[NPOP][N];
+    pull_f<Real>(V, j, x0, lane, fs);
+    pull_g<Real, TWALL>(V, j, x0, lane, gs);
+    if (TWALL == LBRB_TWALL_DIRICHLET) {
+      const bool top = (j == V.ny - 1), bot = (j == 0);
+      if (top || bot) {
+        const Real twall = top ? (Real)V.Tup : (Real)V.Tdown;
+        const Real tw = std::is_same<Real, double>::value ? twall : (Real)(twall - (Real)V.T0);
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+          if (top) {
+            gs[4][m] = -gs[2][m] + Real(2.0 * w_of(2)) * tw;
+            gs[7][m] = -gs[5][m] + Real(2.0 * w_of(5)) * tw;
+            gs[8][m] = -gs[6][m] + Real(2.0 * w_of(6)) * tw;
+          }
+          if (bot) {
+            gs[2][m] = -gs[4][m] + Real(2.0 * w_of(4)) * tw;
+            gs[5][m] = -gs[7][m] + Real(2.0 * w_of(7)) * tw;
+            gs[6][m] = -gs[8][m] + Real(2.0 * w_of(8)) * tw;
+          }
+        }
+      }
+    }
+    const size_t row = (size_t)j * V.pitch;
+    Real Fv[N], rv[N], uvv[N], vvv[N], tv[N];
+    vload<Real>(V.F + row + x0, Fv);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      Real fn[NPOP], gn[NPOP];
+#pragma unroll
+      for (int k = 0; k < NPOP; k++) { fn[k] = fs[k][m]; gn[k] = gs[k][m]; }
+      if constexpr (std::is_same<Real, double>::value) {
+        node_ref<REFNUDGE>(V, row + x0 + m, fn, gn, Fv[m], rv[m], uvv[m], vvv[m], tv[m]);
+      } else {
+        node_shift(V, fn, gn, Fv[m], rv[m], uvv[m], vvv[m], tv[m]);
+      }
+#pragma unroll
+      for (int k = 0; k < NPOP; k++) { fs[k][m] = fn[k]; gs[k][m] = gn[k]; }
+    }
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < NPOP; k++) {
+        vstore<Real>(V.fdst + (size_t)k * V.plane + row + x0, fs[k]);
+        vstore<Real>(V.gdst + (size_t)k * V.plane + row + x0, gs[k]);
+      }
+      vstore<Real>(V.F + row + x0, Fv);
+      if (V.write_uv) {
+        vstore<Real>(V.u + row + x0, uvv);
+        vstore<Real>(V.v + row + x0, vvv);
+      }
+      if (V.write_rt) {
+        vstore<Real>(V.rho + row + x0, rv);
+        vstore<Real>(V.T + row + x0, tv);
+      }
+    }
+  }
+}
+
+template <typename Real, int TWALL, bool REFNUDGE>
+static cudaError_t launch_lb(const LBView<Real>& V, cudaStream_t s) {
+  static int grid = 0;
+  static int dev_cached = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (grid == 0 || dev != dev_cached) {
+    int nsm = 0, per = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lb_step_kernel<Real, TWALL, REFNUDGE>,
+                                                  256, 0);
+    grid = nsm * (per > 0 ? per : 1);
+    dev_cached = dev;
+  }
+  long need = (V.ntasks * WARP + 255) / 256;
+  int g = (int)(need < grid ? need : grid);
+  if (g < 1) g = 1;
+  lb_step_kernel<Real, TWALL, REFNUDGE><<<g, 256, 0, s>>>(V);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, cudaStream_t s) {
+  if (twall == LBRB_TWALL_DIRICHLET)
+    return refnudge ? launch_lb<double, LBRB_TWALL_DIRICHLET, true>(V, s)
+                    : launch_lb<double, LBRB_TWALL_DIRICHLET, false>(V, s);
+  return refnudge ? launch_lb<double, LBRB_TWALL_ADIABATIC, true>(V, s)
+                  : launch_lb<double, LBRB_TWALL_ADIABATIC, false>(V, s);
+}
+
+cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s) {
+  if (twall == LBRB_TWALL_DIRICHLET) return launch_lb<float, LBRB_TWALL_DIRICHLET, false>(V, s);
+  return launch_lb<float, LBRB_TWALL_ADIABATIC, false>(V, s);
+}
+
+}  // namespace lbrb

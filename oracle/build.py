@@ -71,7 +71,7 @@ def _fmt(v) -> str:
     if isinstance(v, int):
         return str(v)
     if isinstance(v, float):
-        r = repr(v)
+        r = repr(float(v))
         return f"({r})" if v < 0 else r
     return str(v)
 
@@ -97,7 +97,8 @@ def build_ref(program: str, params: dict, tag: str | None = None) -> Path:
     csrc_rel, hdr_rel = PROGRAMS[program]
     csrc = (REFERENCE_ROOT / csrc_rel).read_text()
     hdr = (REFERENCE_ROOT / hdr_rel).read_text()
-    key = hashlib.sha1(repr((program, sorted(params.items()), csrc, hdr)).encode()).hexdigest()[:12]
+    shim = "".join((SHIM / n).read_text() for n in ("mpi.h", "mpi_shim.c", "hdf5.h", "hdf5_shim.c"))
+    key = hashlib.sha1(repr((program, sorted(params.items()), csrc, hdr, shim)).encode()).hexdigest()[:12]
     tag = tag or f"{program}_{key}"
     d = REF_OUT / tag
     exe = d / program
