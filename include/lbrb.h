@@ -195,6 +195,25 @@ LBRB_API int lbrb_nusselt(lbrb_t *h, double *nu);
  * tempvel_nudge.c:1104-1260), and the row Nusselt number. */
 LBRB_API int lbrb_profile(lbrb_t *h, double *out);
 
+/* ---- diagnostics without allocation ----------------------------------------
+ * No counterpart in the reference.  lbrb_stats_noalloc computes what
+ * lbrb_energy() and lbrb_nusselt() give (out3 = mean kinetic energy, mean T,
+ * Nusselt number) from device fields the caller owns -- rho, u, v, T, each
+ * ny rows of `pitch` elements of `precision` (LBRB_PREC_FP64: double,
+ * LBRB_PREC_FP32_SHIFTED: float) -- for callers that cannot allocate device
+ * memory at that point (a framework that keeps all device memory in its own
+ * pool, a loop that must not allocate after start-up).  It allocates
+ * nothing: its scratch is a fixed device array of LBRB_STATS_NOALLOC_MAX_ROWS
+ * row records, so ny above that is rejected with LBRB_ERR_RANGE.  Work runs
+ * on `cuda_stream` (NULL: the default stream) and the call returns after it
+ * finishes.  Calls share the scratch array: calls that overlap on the GPU
+ * race.  The first call on a device looks up the array's address; make it
+ * before any stream capture. */
+#define LBRB_STATS_NOALLOC_MAX_ROWS 16384
+LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, const void *T,
+                                int precision, int nx, int ny, int pitch, double relaxg,
+                                double Tup, double Tdown, void *cuda_stream, double *out3);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,7 +37,7 @@ EXPORTS = [
     "lbrb_set_istep", "lbrb_check_finite", "lbrb_particles_set", "lbrb_particles_get",
     "lbrb_record_pending", "lbrb_record_drain", "lbrb_nudge_init", "lbrb_nudge_load",
     "lbrb_nudge_obs", "lbrb_energy", "lbrb_nusselt", "lbrb_profile", "lbrb_set_stream",
-    "lbrb_set_timing", "lbrb_get_timing",
+    "lbrb_set_timing", "lbrb_get_timing", "lbrb_stats_noalloc",
 ]
 
 
@@ -101,6 +101,8 @@ def lib() -> C.CDLL:
         "lbrb_set_stream": (C.c_int, [vp, vp]),
         "lbrb_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
+        "lbrb_stats_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_double, C.c_double, C.c_double, vp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -17,7 +17,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liblbrb.so"
-SOURCES = ["lb_kernels.cu", "particle_kernels.cu", "nudge_kernels.cu", "aux_kernels.cu", "capi.cu"]
+SOURCES = ["lb_kernels.cu", "particle_kernels.cu", "nudge_kernels.cu", "aux_kernels.cu", "capi.cu",
+           "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
