@@ -161,7 +161,8 @@ def timed_steps(r, torch, steps: int, warmup: int, dist, device: int, sampler=No
     r.step(warmup)
     r.sync()
     r.drain_records()
-    stream = torch.cuda.current_stream()
+    # a real (non-default) stream: the events and all of the handle's work share it
+    stream = torch.cuda.Stream()
     r.set_stream(stream.cuda_stream)
     if dist is not None:
         dist.barrier()
@@ -182,6 +183,7 @@ def timed_steps(r, torch, steps: int, warmup: int, dist, device: int, sampler=No
     r.set_timing(False)
     r.sync()
     recs = r.drain_records()
+    r.set_stream(None)
     return ms, timing, recs, (t0, t1)
 
 
@@ -247,7 +249,7 @@ def e2e(lb, torch, precision: str, seed: int, steps: int, device: int, dist):
     pu = np.zeros(NPRTCL)
     pv = bilinear_np(vv[1:-1, 1:-1].T.copy(), x, y)
     out_m = [pinned(nh, torch.float64).reshape(NX + 2, NY + 2) for _ in range(4)]
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
     r.set_stream(stream.cuda_stream)
     nrec = steps // NOUTCONFIG
     recbuf = pinned(max(nrec, 1) * 9 * NPRTCL, torch.float64).reshape(max(nrec, 1), 9, NPRTCL)
@@ -269,6 +271,7 @@ def e2e(lb, torch, precision: str, seed: int, steps: int, device: int, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    r.set_stream(None)
     h2d = 2 * f.nbytes + 4 * rho.nbytes + NPRTCL * (4 * 8 + 4 + 4 + 8)
     d2h = got.value * 9 * NPRTCL * 8 + 4 * rho.nbytes
     r.close()
@@ -507,6 +510,26 @@ def run_reference_arm(args) -> dict:
                     "d2h_bytes_per_step": 0}}
 
 
+def run_lb_only(args, torch) -> dict:
+    """The fused stream/collide kernel alone on a grid of --grid (no
+    particles): the command used for ncu captures of lb_step_kernel."""
+    import lagrangianrbnudging_b200 as lb
+    from lagrangianrbnudging_b200 import build as b
+
+    b.build()
+    nx, ny = (int(a) for a in args.grid.lower().split("x"))
+    base = lb.closure(nx, ny, Ra=RA, Pr=PR, U=U)
+    with lb.Run(**base, precision=args.precision, device=0) as r:
+        r.init_conduction(SEED, 1e-3)
+        ms, timing, _, _ = timed_steps(r, torch, args.steps, args.warmup, None, 0)
+    lb_ms, n = timing["lb_step"]
+    avg = lb_ms / max(n, 1)
+    gbs = ALG_BYTES[args.precision] * nx * ny / (avg * 1e-3) / 1e9
+    return {"mode": "lb-only", "grid": f"{nx}x{ny}", "precision": args.precision,
+            "steps": args.steps, "avg_lb_ms": round(avg, 5), "alg_gbs": round(gbs, 1),
+            "mlups": round(nx * ny * args.steps / (ms * 1e3), 1)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -515,6 +538,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--lb-only", action="store_true",
+                    help="fused kernel alone on --grid (the ncu capture command)")
+    ap.add_argument("--grid", default="2048x1024")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -527,6 +554,10 @@ def main():
         return
     import torch
 
+    if args.lb_only:
+        torch.cuda.set_device(0)
+        print(json.dumps(run_lb_only(args, torch)), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
