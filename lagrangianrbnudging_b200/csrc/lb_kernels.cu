@@ -25,6 +25,7 @@
 // values come by warp shuffle, the row ends by periodic scalar loads.  Wall
 // handling is warp-uniform (one row per warp).  Grid-stride over (row, chunk)
 // tasks with a grid sized to fill every SM.
+#include <cstdlib>
 #include <type_traits>
 
 #include "lbrb_internal.cuh"
@@ -251,8 +252,100 @@ __global__ void __launch_bounds__(256) lb_step_kernel(const LBView<Real> V) {
   }
 }
 
+// ------------------------------------------------- one node per thread
+// The same step with one node per thread: every population is one plain
+// coalesced load at its pull address (x-1 and x+1 are neighbours in the same
+// 128-byte line, so L1/L2 absorb the shift; DRAM reads each value once).
+// All 18 loads are independent and issue back to back; the register budget
+// is small, so many warps per SM keep enough bytes in flight.
+template <typename Real, int TWALL>
+__device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, Real* fs, Real* gs) {
+  const int xl = (x == 0) ? V.nx - 1 : x - 1;       // source column of c_x = +1
+  const int xr = (x == V.nx - 1) ? 0 : x + 1;       // source column of c_x = -1
+  const bool adia_wall = TWALL == LBRB_TWALL_ADIABATIC && (j == 0 || j == V.ny - 1);
+  const int jc = (j == 0) ? 1 : V.ny - 2;
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
+    const int js = j - icy(k);
+    if (js < 0 || js >= V.ny)
+      fs[k] = __ldcs(V.fsrc + (size_t)opp(k) * V.plane + (size_t)j * V.pitch + x);
+    else
+      fs[k] = __ldcs(V.fsrc + (size_t)k * V.plane + (size_t)js * V.pitch + xs);
+    if (adia_wall) {
+      gs[k] = __ldcs(V.gsrc + (size_t)k * V.plane + (size_t)jc * V.pitch + x);
+    } else {
+      int jg = js;
+      if (TWALL == LBRB_TWALL_ADIABATIC) {
+        if (jg == 0) jg = 1;
+        else if (jg == V.ny - 1) jg = V.ny - 2;
+      }
+      gs[k] = (jg < 0 || jg >= V.ny) ? Real(0)
+                                      : __ldcs(V.gsrc + (size_t)k * V.plane + (size_t)jg * V.pitch + xs);
+    }
+  });
+}
+
+template <typename Real, int TWALL, bool REFNUDGE>
+__global__ void __launch_bounds__(256) lb_node_kernel(const LBView<Real> V) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (x >= V.nx) return;
+  Real fs[NPOP], gs[NPOP];
+  pull_node<Real, TWALL>(V, j, x, fs, gs);
+  if (TWALL == LBRB_TWALL_DIRICHLET) {
+    if (j == V.ny - 1) {
+      const Real tw = std::is_same<Real, double>::value ? (Real)V.Tup : (Real)(V.Tup - V.T0);
+      gs[4] = -gs[2] + Real(2.0 * w_of(2)) * tw;
+      gs[7] = -gs[5] + Real(2.0 * w_of(5)) * tw;
+      gs[8] = -gs[6] + Real(2.0 * w_of(6)) * tw;
+    }
+    if (j == 0) {
+      const Real tw = std::is_same<Real, double>::value ? (Real)V.Tdown : (Real)(V.Tdown - V.T0);
+      gs[2] = -gs[4] + Real(2.0 * w_of(4)) * tw;
+      gs[5] = -gs[7] + Real(2.0 * w_of(7)) * tw;
+      gs[6] = -gs[8] + Real(2.0 * w_of(8)) * tw;
+    }
+  }
+  const size_t o = (size_t)j * V.pitch + x;
+  Real Fy = V.F[o], r, u, v, t;
+  if constexpr (std::is_same<Real, double>::value) {
+    node_ref<REFNUDGE>(V, o, fs, gs, Fy, r, u, v, t);
+  } else {
+    node_shift(V, fs, gs, Fy, r, u, v, t);
+  }
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) {
+    __stcs(V.fdst + (size_t)k * V.plane + o, fs[k]);
+    __stcs(V.gdst + (size_t)k * V.plane + o, gs[k]);
+  }
+  V.F[o] = Fy;
+  if (V.write_uv) {
+    V.u[o] = u;
+    V.v[o] = v;
+  }
+  if (V.write_rt) {
+    V.rho[o] = r;
+    V.T[o] = t;
+  }
+}
+
+static int lb_variant() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("LBRB_LB_VARIANT");
+    v = (e && e[0] == 'w') ? 1 : 0;  // 0: one node per thread, 1: warp-chunk vectors
+  }
+  return v;
+}
+
 template <typename Real, int TWALL, bool REFNUDGE>
 static cudaError_t launch_lb(const LBView<Real>& V, cudaStream_t s) {
+  if (lb_variant() == 0) {
+    dim3 grid((V.nx + 255) / 256, V.ny);
+    lb_node_kernel<Real, TWALL, REFNUDGE><<<grid, 256, 0, s>>>(V);
+    return cudaGetLastError();
+  }
   static int grid = 0;
   static int dev_cached = -1;
   int dev = 0;
