@@ -296,6 +296,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     with ClockSampler(device) as clk:
         ms, timing, recs, (t0, t1) = timed_steps(r, torch, K, W, dist, device)
         clocks = clk.summary(t0, t1)
+    shape32 = r.launch_shape()
     nu32 = r.nusselt()
     ke32, _ = r.energy()
     r.close()
@@ -307,6 +308,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     r64, _ = make_run(lb, "fp64", seed, device, K64 // NOUTCONFIG + W // NOUTCONFIG + 4)
     init_run(r64, seed)
     ms64, timing64, _, _ = timed_steps(r64, torch, K64, W, dist, device)
+    shape64 = r64.launch_shape()
     r64.step(K - K64)  # same number of steps as the FP32 run for the Nu comparison
     r64.sync()
     nu64 = r64.nusselt()
@@ -351,11 +353,13 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
                      "alg_bytes_per_node": ALG_BYTES["fp32"],
                      "avg_launch_ms": round(avg_lb, 5),
                      "traffic": (round(tr * nodes) if tr else None),
-                     "share_of_step": round(lb_ms / ms, 4)},
+                     "share_of_step": round(lb_ms / ms, 4),
+                     "launch_shape": shape32},
         "fp64": {"value": round(mlups64, 1), "unit": "MLUPS", "steps": K64,
                  "lb_achieved_gbs": round(achieved64, 1),
                  "lb_frac": round(achieved64 / peak, 4),
-                 "fp32_over_fp64": round(mlups / mlups64, 3)},
+                 "fp32_over_fp64": round(mlups / mlups64, 3),
+                 "launch_shape": shape64},
         "accuracy": {"nu_fp32": nu32, "nu_fp64": nu64,
                      "nu_rel_err": abs(nu32 - nu64) / abs(nu64),
                      "ke_rel_err": abs(ke32 - ke64) / max(abs(ke64), 1e-300),
@@ -522,12 +526,13 @@ def run_lb_only(args, torch) -> dict:
     with lb.Run(**base, precision=args.precision, device=0) as r:
         r.init_conduction(SEED, 1e-3)
         ms, timing, _, _ = timed_steps(r, torch, args.steps, args.warmup, None, 0)
+        shape = r.launch_shape()
     lb_ms, n = timing["lb_step"]
     avg = lb_ms / max(n, 1)
     gbs = ALG_BYTES[args.precision] * nx * ny / (avg * 1e-3) / 1e9
     return {"mode": "lb-only", "grid": f"{nx}x{ny}", "precision": args.precision,
             "steps": args.steps, "avg_lb_ms": round(avg, 5), "alg_gbs": round(gbs, 1),
-            "mlups": round(nx * ny * args.steps / (ms * 1e3), 1)}
+            "mlups": round(nx * ny * args.steps / (ms * 1e3), 1), "launch_shape": shape}
 
 
 def main():

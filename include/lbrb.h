@@ -95,6 +95,7 @@ typedef struct {
   int record_full;        /* Prtcl_Writefull: also record the 8 Maxey-Riley terms */
   int record_slots;       /* records held before lbrb_record_drain() must run */
   int device;             /* CUDA device ordinal */
+  int autotune;           /* 1: time the fused kernel's launch shapes on the first step */
 } lbrb_params;
 
 /* Fill *p with defaults (reference values where it has them). */
@@ -150,6 +151,10 @@ LBRB_API int lbrb_set_stream(lbrb_t *h, void *cuda_stream);
  * class (arrays of length n <= 4) and resets the accumulators. */
 LBRB_API int lbrb_set_timing(lbrb_t *h, int enable);
 LBRB_API int lbrb_get_timing(lbrb_t *h, double *ms, int *launches, int n);
+/* Launch shape of the fused kernel (threads per block, min blocks per SM)
+ * and its timed milliseconds per launch when the autotuner picked it
+ * (0 before the first step or with autotune off). */
+LBRB_API int lbrb_get_launch_shape(const lbrb_t *h, int *block, int *min_blocks, float *ms);
 
 /* ---- particles ------------------------------------------------------------ */
 /* Replaces init_prtcl/restore_prtcl (Trajectories/code/mympi2.h:116-290,

@@ -37,7 +37,7 @@ EXPORTS = [
     "lbrb_set_istep", "lbrb_check_finite", "lbrb_particles_set", "lbrb_particles_get",
     "lbrb_record_pending", "lbrb_record_drain", "lbrb_nudge_init", "lbrb_nudge_load",
     "lbrb_nudge_obs", "lbrb_energy", "lbrb_nusselt", "lbrb_profile", "lbrb_set_stream",
-    "lbrb_set_timing", "lbrb_get_timing", "lbrb_stats_noalloc",
+    "lbrb_set_timing", "lbrb_get_timing", "lbrb_stats_noalloc", "lbrb_get_launch_shape",
 ]
 
 
@@ -56,6 +56,7 @@ class Params(C.Structure):
         ("alpha", C.c_double), ("ntempread", C.c_int), ("nobs", C.c_int),
         ("beta", C.c_double), ("nprtcl", C.c_int), ("noutconfig", C.c_int),
         ("record_full", C.c_int), ("record_slots", C.c_int), ("device", C.c_int),
+        ("autotune", C.c_int),
     ]
 
 
@@ -101,6 +102,7 @@ def lib() -> C.CDLL:
         "lbrb_set_stream": (C.c_int, [vp, vp]),
         "lbrb_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
+        "lbrb_get_launch_shape": (C.c_int, [vp, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_stats_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_double, C.c_double, C.c_double, vp, dp]),
     }
@@ -298,6 +300,11 @@ class Run:
         self._ck(lib().lbrb_get_timing(self.h, _dp(ms), _ip(cnt), 4))
         names = ["lb_step", "particles", "nudging", "record_copy"]
         return {n: (float(ms[i]), int(cnt[i])) for i, n in enumerate(names)}
+
+    def launch_shape(self):
+        b, m, ms = C.c_int(), C.c_int(), C.c_float()
+        self._ck(lib().lbrb_get_launch_shape(self.h, C.byref(b), C.byref(m), C.byref(ms)))
+        return {"block": b.value, "min_blocks": m.value, "tuned_ms": ms.value}
 
     # ---- diagnostics
     def energy(self):

@@ -16,8 +16,11 @@
 #include "lbrb_internal.cuh"
 
 namespace lbrb {
-cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, cudaStream_t s);
-cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s);
+cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, int shape,
+                           cudaStream_t s);
+cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStream_t s);
+int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best_ms);
+int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_ms);
 cudaError_t launch_particles(const void* u, const void* v, const void* ub, const void* vb,
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,
                              const int* ptype, int np, double beta, int record, int full,
@@ -171,14 +174,16 @@ void lbrb_params_default(lbrb_params* p) {
   p->record_full = 0;
   p->record_slots = 16;
   p->device = 0;
+  p->autotune = 1;
 }
 
 const char* lbrb_last_error(const lbrb_t* h) { return h ? h->err.c_str() : "null handle"; }
 
 static void free_all(lbrb_t* h) {
   auto F = [](void* q) { if (q) cudaFree(q); };
-  F(h->pops[0]); F(h->pops[1]); F(h->F); F(h->rho); F(h->T);
-  for (int a = 0; a < 2; a++) for (int b = 0; b < 2; b++) F(h->uv[a][b]);
+  F(h->pops[0]); F(h->pops[1]); F(h->F[0]); F(h->F[1]);
+  F(h->rho[0]); F(h->rho[1]); F(h->T[0]); F(h->T[1]);
+  for (int a = 0; a < 3; a++) for (int b = 0; b < 2; b++) F(h->uv[a][b]);
   F(h->px); F(h->pid); F(h->ptype); F(h->d_ring);
   if (h->h_ring) cudaFreeHost(h->h_ring);
   delete[] h->h_ring_step;
@@ -194,6 +199,9 @@ static void free_all(lbrb_t* h) {
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->join_ev) cudaEventDestroy(h->join_ev);
+  if (h->pstream) cudaStreamDestroy(h->pstream);
+  cudaEvent_t evs[] = {h->ev_lb, h->ev_uv[0], h->ev_uv[1], h->ev_uv[2], h->ev_T[0], h->ev_T[1], h->ev_pjoin};
+  for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
 }
 
@@ -219,7 +227,6 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
   h->p = p;
   if (h->p.record_slots < 1) h->p.record_slots = 1;
   h->dev = p.device;
-  int rc = LBRB_OK;
   auto done = [&](int code) -> int {
     if (code != LBRB_OK) {
       free_all(h);
@@ -233,8 +240,14 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
   if (e != cudaSuccess) return done(LBRB_ERR_CUDA);
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess)
+      cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->pstream, cudaStreamNonBlocking) != cudaSuccess)
     return done(LBRB_ERR_CUDA);
+  {
+    cudaEvent_t* evs[] = {&h->ev_lb, &h->ev_uv[0], &h->ev_uv[1], &h->ev_uv[2], &h->ev_T[0], &h->ev_T[1], &h->ev_pjoin};
+    for (cudaEvent_t* e : evs)
+      if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return done(LBRB_ERR_CUDA);
+  }
   h->stream = h->own_stream;
   h->pitch = (p.nx + 31) / 32 * 32;
   h->plane = (size_t)p.ny * h->pitch;
@@ -244,7 +257,8 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
     if (cudaMalloc(&h->pops[b], pb) != cudaSuccess) return done(LBRB_ERR_NOMEM);
     cudaMemset(h->pops[b], 0, pb);
   }
-  void** scal[] = {&h->F, &h->rho, &h->T, &h->uv[0][0], &h->uv[0][1], &h->uv[1][0], &h->uv[1][1]};
+  void** scal[] = {&h->F[0], &h->F[1], &h->rho[0], &h->rho[1], &h->T[0], &h->T[1],
+                   &h->uv[0][0], &h->uv[0][1], &h->uv[1][0], &h->uv[1][1], &h->uv[2][0], &h->uv[2][1]};
   for (void** s : scal) {
     if (cudaMalloc(s, h->plane * h->esize) != cudaSuccess) return done(LBRB_ERR_NOMEM);
     cudaMemset(*s, 0, h->plane * h->esize);
@@ -287,7 +301,6 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
   if (dalloc(&h->dflags, 1)) return done(LBRB_ERR_NOMEM);
   if (cudaMallocHost(&h->h_flags, sizeof(unsigned)) != cudaSuccess) return done(LBRB_ERR_NOMEM);
   if (cudaDeviceSynchronize() != cudaSuccess) return done(LBRB_ERR_CUDA);
-  (void)rc;
   return done(LBRB_OK);
 }
 
@@ -295,6 +308,7 @@ int lbrb_destroy(lbrb_t* h) {
   if (!h) return LBRB_ERR_ARG;
   cudaSetDevice(h->dev);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->pstream) cudaStreamSynchronize(h->pstream);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   free_all(h);
   delete h;
@@ -364,12 +378,12 @@ int lbrb_set_moments(lbrb_t* h, const double* rho, const double* u, const double
   if (rc) return rc;
   double* st = (double*)h->staging;
   const double* src[4] = {rho, u, v, T};
-  void* dst[4] = {h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T};
+  void* dst[4] = {h->rho[h->cur], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[h->cur]};
   for (int a = 0; a < 4; a++) {
     CK(h, cudaMemcpyAsync(st + a * cnt, src[a], bytes, cudaMemcpyHostToDevice, h->stream));
     CK(h, launch_scalar_in(st + a * cnt, layout, dst[a], fp32(h), h->p.nx, h->p.ny, h->pitch, h->stream));
   }
-  CK(h, launch_force(h->rho, h->T, h->F, fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
+  CK(h, launch_force(h->rho[h->cur], h->T[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   h->moments_valid = true;
   return LBRB_OK;
@@ -384,7 +398,7 @@ int lbrb_get_moments(lbrb_t* h, double* rho, double* u, double* v, double* T, in
   if (rc) return rc;
   double* st = (double*)h->staging;
   double* dst[4] = {rho, u, v, T};
-  const void* src[4] = {h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T};
+  const void* src[4] = {h->rho[h->cur], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[h->cur]};
   for (int a = 0; a < 4; a++) {
     if (!dst[a]) continue;
     CK(h, launch_scalar_out(src[a], layout, st + a * cnt, fp32(h), h->p.nx, h->p.ny, h->pitch, h->stream));
@@ -404,10 +418,10 @@ int lbrb_moments_from_pre(lbrb_t* h, const double* fpre, const double* gpre, int
   double* st = (double*)h->staging;
   CK(h, cudaMemcpyAsync(st, fpre, bytes, cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(st + cnt, gpre, bytes, cudaMemcpyHostToDevice, h->stream));
-  CK(h, launch_moments_from_pre(st, st + cnt, layout, h->rho, h->uv[h->uvcur][0],
-                                h->uv[h->uvcur][1], h->T, fp32(h), h->p.nx, h->p.ny, h->pitch,
+  CK(h, launch_moments_from_pre(st, st + cnt, layout, h->rho[h->cur], h->uv[h->uvcur][0],
+                                h->uv[h->uvcur][1], h->T[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch,
                                 -h->p.gravity, h->stream));
-  CK(h, launch_force(h->rho, h->T, h->F, fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
+  CK(h, launch_force(h->rho[h->cur], h->T[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   h->moments_valid = true;
   return LBRB_OK;
@@ -416,10 +430,10 @@ int lbrb_moments_from_pre(lbrb_t* h, const double* fpre, const double* gpre, int
 int lbrb_init_conduction(lbrb_t* h, uint64_t seed, double noise) {
   if (!h || !(noise == noise)) return fail(h, LBRB_ERR_ARG, "init_conduction: bad arguments");
   CK(h, cudaSetDevice(h->dev));
-  CK(h, launch_init_conduction(h->pops[h->cur], h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1],
-                               h->T, fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->p.Tup,
+  CK(h, launch_init_conduction(h->pops[h->cur], h->rho[h->cur], h->uv[h->uvcur][0],
+                               h->uv[h->uvcur][1], h->T[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->p.Tup,
                                h->p.Tdown, T0_of(h), -h->p.gravity, seed, noise, h->stream));
-  CK(h, launch_force(h->rho, h->T, h->F, fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
+  CK(h, launch_force(h->rho[h->cur], h->T[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   h->moments_valid = true;
   return LBRB_OK;
@@ -573,6 +587,57 @@ int lbrb_nudge_obs(lbrb_t* h, int first_step, int nsteps, const double* x, const
 }
 
 // ------------------------------------------------------------- time loop
+}  // extern "C"
+
+template <typename Real>
+static LBView<Real> make_view(lbrb_t* h, int src, int dst, int uvslot, int write_uv, int write_rt) {
+  LBView<Real> V{};
+  V.fsrc = (const Real*)pop_base(h, src, 0);
+  V.gsrc = (const Real*)pop_base(h, src, 1);
+  V.fdst = (Real*)pop_base(h, dst, 0);
+  V.gdst = (Real*)pop_base(h, dst, 1);
+  V.Fin = (const Real*)h->F[src];
+  V.Fout = (Real*)h->F[dst];
+  V.rho = (Real*)h->rho[dst];
+  V.T = (Real*)h->T[dst];
+  V.u = (Real*)h->uv[uvslot][0];
+  V.v = (Real*)h->uv[uvslot][1];
+  V.nx = h->p.nx;
+  V.ny = h->p.ny;
+  V.pitch = h->pitch;
+  V.plane = h->plane;
+  V.omega = 1. / h->p.relax;
+  V.omegag = 1. / h->p.relaxg;
+  V.neg_gravity = -h->p.gravity;
+  V.Tup = h->p.Tup;
+  V.Tdown = h->p.Tdown;
+  V.T0 = T0_of(h);
+  V.nudge_vol = h->nudge_vol;
+  V.tempreadint = h->tempreadint;
+  V.nud_term = h->nud_term;
+  V.alpha = h->p.alpha;
+  V.write_uv = write_uv;
+  V.write_rt = write_rt;
+  return V;
+}
+
+// particle kernels on a second stream, overlapping the next fused kernel
+static constexpr bool kParticleStream = false;
+
+static const int SHAPE_BS[] = {256, 256, 256, 128, 128, 512, 512};
+static const int SHAPE_MB[] = {1, 2, 3, 4, 6, 1, 2};
+
+extern "C" {
+
+int lbrb_get_launch_shape(const lbrb_t* h, int* block, int* min_blocks, float* ms) {
+  if (!h) return LBRB_ERR_ARG;
+  const int sh = h->lb_shape < 0 ? 0 : h->lb_shape;
+  if (block) *block = SHAPE_BS[sh];
+  if (min_blocks) *min_blocks = SHAPE_MB[sh];
+  if (ms) *ms = h->lb_shape_ms;
+  return LBRB_OK;
+}
+
 int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   if (n == 0) return LBRB_OK;
@@ -583,9 +648,22 @@ int lbrb_step(lbrb_t* h, int n) {
     return fail(h, LBRB_ERR_STATE, "step: nudge_init not called");
   CK(h, cudaSetDevice(h->dev));
   const bool f32 = fp32(h);
+  const bool refbox = h->p.nudge == LBRB_NUDGE_REFBOX;
   const int nx = h->p.nx, ny = h->p.ny;
-  const int vecn = f32 ? 4 : 2;
-  const int chunks = (nx + WARP * vecn - 1) / (WARP * vecn);
+  if (h->lb_shape < 0) {
+    // autotune the fused kernel's launch shape on this grid (trial launches
+    // write only the buffers the real step overwrites)
+    int sh = 0;
+    float ms = 0.f;
+    if (h->p.autotune && !refbox) {
+      if (f32) sh = tune_lb_fp32(make_view<float>(h, h->cur, h->cur ^ 1, h->uvcur, 0, 0), h->p.twall, h->stream, &ms);
+      else sh = tune_lb_fp64(make_view<double>(h, h->cur, h->cur ^ 1, h->uvcur, 0, 0), h->p.twall, h->stream, &ms);
+    }
+    CK(h, cudaGetLastError());
+    h->lb_shape = sh;
+    h->lb_shape_ms = ms;
+  }
+  bool pt_queued = false;
   for (int s = 0; s < n; s++) {
     const int istep = h->istep + 1;
     const bool last = (s == n - 1);
@@ -598,7 +676,7 @@ int lbrb_step(lbrb_t* h, int n) {
         return fail(h, LBRB_ERR_STATE, "step: no bilinear observations for this step");
       obs = h->obs + (size_t)(istep - h->obs_first) * 3 * h->nobs;
     }
-    if (h->p.nudge == LBRB_NUDGE_REFBOX) {
+    if (refbox) {
       const int nt = h->p.ntempread;
       if (istep % nt == 1 && !h->nudge_file_loaded)
         return fail(h, LBRB_ERR_STATE, "step: observation file for this interval not loaded");
@@ -612,61 +690,52 @@ int lbrb_step(lbrb_t* h, int n) {
     }
     const int write_uv = (h->np > 0) || last;
     const int write_rt = last || rec || h->p.nudge == LBRB_NUDGE_BILINEAR;
-    const int uvn = write_uv ? (h->uvcur ^ 1) : h->uvcur;
     const int src = h->cur, dst = h->cur ^ 1;
-    if (f32) {
-      LBView<float> V{};
-      V.fsrc = (const float*)pop_base(h, src, 0);
-      V.gsrc = (const float*)pop_base(h, src, 1);
-      V.fdst = (float*)pop_base(h, dst, 0);
-      V.gdst = (float*)pop_base(h, dst, 1);
-      V.F = (float*)h->F; V.rho = (float*)h->rho; V.T = (float*)h->T;
-      V.u = (float*)h->uv[uvn][0]; V.v = (float*)h->uv[uvn][1];
-      V.nx = nx; V.ny = ny; V.pitch = h->pitch; V.plane = h->plane;
-      V.omega = 1. / h->p.relax; V.omegag = 1. / h->p.relaxg; V.neg_gravity = -h->p.gravity;
-      V.Tup = h->p.Tup; V.Tdown = h->p.Tdown; V.T0 = T0_of(h);
-      V.write_uv = write_uv; V.write_rt = write_rt;
-      V.chunks_per_row = chunks; V.ntasks = (long)chunks * ny;
+    const int uvn = write_uv ? 3 - h->uvcur - h->uvprev : h->uvcur;
+    // buffers read by an earlier particle kernel must be free before rewriting
+    if (h->np > 0 && kParticleStream) {
+      if (write_uv) CK(h, cudaStreamWaitEvent(h->stream, h->ev_uv[uvn], 0));
+      CK(h, cudaStreamWaitEvent(h->stream, h->ev_T[dst], 0));
+    }
+    {
       const int tm = tmark_begin(h, 0, h->stream);
-      CK(h, launch_lb_fp32(V, h->p.twall, h->stream));
-      tmark_end(h, tm, h->stream);
-    } else {
-      LBView<double> V{};
-      V.fsrc = (const double*)pop_base(h, src, 0);
-      V.gsrc = (const double*)pop_base(h, src, 1);
-      V.fdst = (double*)pop_base(h, dst, 0);
-      V.gdst = (double*)pop_base(h, dst, 1);
-      V.F = (double*)h->F; V.rho = (double*)h->rho; V.T = (double*)h->T;
-      V.u = (double*)h->uv[uvn][0]; V.v = (double*)h->uv[uvn][1];
-      V.nx = nx; V.ny = ny; V.pitch = h->pitch; V.plane = h->plane;
-      V.omega = 1. / h->p.relax; V.omegag = 1. / h->p.relaxg; V.neg_gravity = -h->p.gravity;
-      V.Tup = h->p.Tup; V.Tdown = h->p.Tdown; V.T0 = T0_of(h);
-      V.nudge_vol = h->nudge_vol; V.tempreadint = h->tempreadint; V.nud_term = h->nud_term;
-      V.alpha = h->p.alpha;
-      V.write_uv = write_uv; V.write_rt = write_rt;
-      V.chunks_per_row = chunks; V.ntasks = (long)chunks * ny;
-      const int tm = tmark_begin(h, 0, h->stream);
-      CK(h, launch_lb_fp64(V, h->p.twall, h->p.nudge == LBRB_NUDGE_REFBOX, h->stream));
+      if (f32) CK(h, launch_lb_fp32(make_view<float>(h, src, dst, uvn, write_uv, write_rt), h->p.twall, h->lb_shape, h->stream));
+      else CK(h, launch_lb_fp64(make_view<double>(h, src, dst, uvn, write_uv, write_rt), h->p.twall, refbox, h->lb_shape, h->stream));
       tmark_end(h, tm, h->stream);
     }
+    if (h->np > 0 && kParticleStream) CK(h, cudaEventRecord(h->ev_lb, h->stream));
     if (obs) {
       const int tm = tmark_begin(h, 2, h->stream);
-      CK(h, launch_bilinear_nudge(h->T, pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, obs,
+      CK(h, launch_bilinear_nudge(h->T[dst], pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, obs,
                                   obs + h->nobs, obs + 2 * (size_t)h->nobs, h->nobs, h->p.alpha,
                                   h->acc, h->dflags, h->stream));
       tmark_end(h, tm, h->stream);
     }
     if (h->np > 0) {
+      // Particles of step n.  With kParticleStream they run on their own
+      // stream beside the fused kernel of step n+1 (u, v rotate over three
+      // slots and T over two, ordered by events); measured on B200 the fused
+      // kernel then slows by about the particle kernel's own time, so by
+      // default they run in order on the step stream.
+      const int ub = write_uv ? h->uvcur : h->uvprev;
       const int slot = rec ? (int)(h->rec_head % h->p.record_slots) : 0;
       double* rslot = rec ? h->d_ring + (size_t)slot * h->nrec_fields * h->np : nullptr;
-      const int tm = tmark_begin(h, 1, h->stream);
-      CK(h, launch_particles(h->uv[uvn][0], h->uv[uvn][1], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
-                             h->T, f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta,
-                             rec ? 1 : 0, h->p.record_full, rslot, h->dflags, h->stream));
-      tmark_end(h, tm, h->stream);
+      cudaStream_t ps = kParticleStream ? h->pstream : h->stream;
+      if (kParticleStream) CK(h, cudaStreamWaitEvent(ps, h->ev_lb, 0));
+      const int tm = tmark_begin(h, 1, ps);
+      CK(h, launch_particles(h->uv[uvn][0], h->uv[uvn][1], h->uv[ub][0], h->uv[ub][1],
+                             h->T[dst], f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta,
+                             rec ? 1 : 0, h->p.record_full, rslot, h->dflags, ps));
+      tmark_end(h, tm, ps);
+      if (kParticleStream) {
+        CK(h, cudaEventRecord(h->ev_uv[uvn], ps));
+        CK(h, cudaEventRecord(h->ev_uv[ub], ps));
+        CK(h, cudaEventRecord(h->ev_T[dst], ps));
+        pt_queued = true;
+      }
       if (rec) {
         h->h_ring_step[slot] = istep;
-        CK(h, cudaEventRecord(h->ring_ev[slot], h->stream));
+        CK(h, cudaEventRecord(h->ring_ev[slot], ps));
         CK(h, cudaStreamWaitEvent(h->copy_stream, h->ring_ev[slot], 0));
         const size_t per = (size_t)h->nrec_fields * h->np;
         const int tc = tmark_begin(h, 3, h->copy_stream);
@@ -679,11 +748,19 @@ int lbrb_step(lbrb_t* h, int n) {
       }
     }
     h->cur = dst;
-    h->uvcur = uvn;
+    if (write_uv) {
+      h->uvprev = h->uvcur;
+      h->uvcur = uvn;
+    }
     h->istep = istep;
   }
+  // the caller's stream sees the particle kernels and record copies as part
+  // of the steps
+  if (pt_queued) {
+    CK(h, cudaEventRecord(h->ev_pjoin, h->pstream));
+    CK(h, cudaStreamWaitEvent(h->stream, h->ev_pjoin, 0));
+  }
   if (h->join_pending) {
-    // the caller's stream sees the record copies as part of the step
     CK(h, cudaEventRecord(h->join_ev, h->copy_stream));
     CK(h, cudaStreamWaitEvent(h->stream, h->join_ev, 0));
     h->join_pending = false;
@@ -709,6 +786,7 @@ int lbrb_get_timing(lbrb_t* h, double* ms, int* launches, int n) {
   if (!h || n < 0 || n > 4) return fail(h, LBRB_ERR_ARG, "get_timing: n must be 0..4");
   CK(h, cudaSetDevice(h->dev));
   CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaStreamSynchronize(h->pstream));
   CK(h, cudaStreamSynchronize(h->copy_stream));
   double acc[4] = {0, 0, 0, 0};
   int cnt[4] = {0, 0, 0, 0};
@@ -731,6 +809,7 @@ int lbrb_sync(lbrb_t* h) {
   if (!h) return LBRB_ERR_ARG;
   CK(h, cudaSetDevice(h->dev));
   CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaStreamSynchronize(h->pstream));
   CK(h, cudaStreamSynchronize(h->copy_stream));
   CK(h, cudaMemcpy(h->h_flags, h->dflags, sizeof(unsigned), cudaMemcpyDeviceToHost));
   const unsigned f = *h->h_flags;
@@ -753,7 +832,7 @@ static int stats(lbrb_t* h, double out[3]) {
   CK(h, cudaSetDevice(h->dev));
   double* part = h->red;
   double* res = h->red + (size_t)red_blocks() * 6;
-  CK(h, launch_stats(h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T, fp32(h), h->p.nx,
+  CK(h, launch_stats(h->rho[h->cur], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[h->cur], fp32(h), h->p.nx,
                      h->p.ny, h->pitch, part, res, h->stream));
   CK(h, cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
@@ -787,7 +866,7 @@ int lbrb_profile(lbrb_t* h, double* out) {
   if (!h->moments_valid) return fail(h, LBRB_ERR_STATE, "profile: no moments yet");
   CK(h, cudaSetDevice(h->dev));
   double* dout = h->red + (size_t)red_blocks() * 6 + 8;
-  CK(h, launch_profile(h->rho, h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T, fp32(h), h->p.nx,
+  CK(h, launch_profile(h->rho[h->cur], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[h->cur], fp32(h), h->p.nx,
                        h->p.ny, h->pitch, dout, h->stream));
   CK(h, cudaMemcpyAsync(out, dout, (size_t)h->p.ny * 9 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));

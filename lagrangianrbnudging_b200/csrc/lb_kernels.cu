@@ -15,16 +15,21 @@
 //   collision       :1097-1180, 1314-1341 (tempvel_nudge.c:1917-1945 nudged g)
 //
 // Two arithmetic forms:
-//   Real = double, SHIFT = false: the reference's operation order exactly
-//     (built with --fmad=false), bit-identical to the reference on x86-64.
-//   Real = float, SHIFT = true: populations stored as deviations from their
-//     weights (f_k - w_k rho0, g_k - w_k T0), collision in FP32.
+//   Real = double: the reference's operation order exactly (built with
+//     --fmad=false), bit-identical to the reference on x86-64.
+//   Real = float: populations stored as deviations from their weights
+//     (f_k - w_k rho0, g_k - w_k T0), collision in FP32.
 //
-// Mapping: a warp owns VEC*32 consecutive nodes of one row (VEC = 2 doubles
-// or 4 floats per lane, one 16-byte access per population); the x neighbour
-// values come by warp shuffle, the row ends by periodic scalar loads.  Wall
-// handling is warp-uniform (one row per warp).  Grid-stride over (row, chunk)
-// tasks with a grid sized to fill every SM.
+// Mapping: one node per thread, a block covers BS consecutive nodes of one
+// row (wall handling is block-uniform).  Every population is one plain
+// coalesced load at its pull address: x-1 and x+1 fall in the same 128-byte
+// lines as the neighbouring threads' loads, so L1/L2 absorb the shift and
+// DRAM reads each value once.  All 18 loads are independent and issue back to
+// back; the small register budget keeps many warps per SM and enough bytes in
+// flight for HBM3e.  The buoyancy F of the next step is written to the other
+// of two buffers, so a launch is a pure function of its sources: the launch
+// shape (block size, blocks per SM) is picked by timing the candidates on the
+// run's own grid (tune_lb).
 #include <cstdlib>
 #include <type_traits>
 
@@ -38,54 +43,6 @@ __device__ __forceinline__ void static_for(F&& f) {
     static_for<K - 1>(f);
     f(std::integral_constant<int, K - 1>{});
   }
-}
-
-// ---------------------------------------------------------------- pulls
-template <typename Real>
-__device__ __forceinline__ void pull_f(const LBView<Real>& V, int j, int x0, int lane,
-                                       Real (&fs)[NPOP][Vec<Real>::N]) {
-  static_for<NPOP>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    const int js = j - icy(k);
-    if (js < 0 || js >= V.ny) {
-      // bounce-back: the opposite population of this node, before streaming
-      load_pull_x<0, Real>(V.fsrc + (size_t)opp(k) * V.plane + (size_t)j * V.pitch, x0, lane,
-                           V.nx, fs[k]);
-    } else {
-      load_pull_x<icx(k), Real>(V.fsrc + (size_t)k * V.plane + (size_t)js * V.pitch, x0, lane,
-                                V.nx, fs[k]);
-    }
-  });
-}
-
-template <typename Real, int TWALL>
-__device__ __forceinline__ void pull_g(const LBView<Real>& V, int j, int x0, int lane,
-                                       Real (&gs)[NPOP][Vec<Real>::N]) {
-  constexpr int N = Vec<Real>::N;
-  if (TWALL == LBRB_TWALL_ADIABATIC && (j == 0 || j == V.ny - 1)) {
-    const int jc = (j == 0) ? 1 : V.ny - 2;
-    static_for<NPOP>([&](auto kc) {
-      constexpr int k = decltype(kc)::value;
-      load_pull_x<0, Real>(V.gsrc + (size_t)k * V.plane + (size_t)jc * V.pitch, x0, lane, V.nx,
-                           gs[k]);
-    });
-    return;
-  }
-  static_for<NPOP>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    int js = j - icy(k);
-    if (TWALL == LBRB_TWALL_ADIABATIC) {
-      if (js == 0) js = 1;
-      else if (js == V.ny - 1) js = V.ny - 2;
-    }
-    if (js < 0 || js >= V.ny) {
-#pragma unroll
-      for (int m = 0; m < N; m++) gs[k][m] = Real(0);
-    } else {
-      load_pull_x<icx(k), Real>(V.gsrc + (size_t)k * V.plane + (size_t)js * V.pitch, x0, lane,
-                                V.nx, gs[k]);
-    }
-  });
 }
 
 // ------------------------------------------------ reference-order FP64 node
@@ -182,82 +139,6 @@ __device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, fl
 }
 
 // ------------------------------------------------------------------ kernel
-template <typename Real, int TWALL, bool REFNUDGE>
-__global__ void __launch_bounds__(256) lb_step_kernel(const LBView<Real> V) {
-  constexpr int N = Vec<Real>::N;
-  const int lane = threadIdx.x & (WARP - 1);
-  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long nw = ((long)gridDim.x * blockDim.x) >> 5;
-  for (long task = gw; task < V.ntasks; task += nw) {
-    const int j = (int)(task / V.chunks_per_row);
-    const int chunk = (int)(task - (long)j * V.chunks_per_row);
-    int x0 = chunk * (WARP * N) + lane * N;
-    const bool active = x0 < V.nx;
-    if (!active) x0 = 0;  // in-bounds loads; results are discarded
-    Real fs[NPOP][N], gs[NPOP][N];
-    pull_f<Real>(V, j, x0, lane, fs);
-    pull_g<Real, TWALL>(V, j, x0, lane, gs);
-    if (TWALL == LBRB_TWALL_DIRICHLET) {
-      const bool top = (j == V.ny - 1), bot = (j == 0);
-      if (top || bot) {
-        const Real twall = top ? (Real)V.Tup : (Real)V.Tdown;
-        const Real tw = std::is_same<Real, double>::value ? twall : (Real)(twall - (Real)V.T0);
-#pragma unroll
-        for (int m = 0; m < N; m++) {
-          if (top) {
-            gs[4][m] = -gs[2][m] + Real(2.0 * w_of(2)) * tw;
-            gs[7][m] = -gs[5][m] + Real(2.0 * w_of(5)) * tw;
-            gs[8][m] = -gs[6][m] + Real(2.0 * w_of(6)) * tw;
-          }
-          if (bot) {
-            gs[2][m] = -gs[4][m] + Real(2.0 * w_of(4)) * tw;
-            gs[5][m] = -gs[7][m] + Real(2.0 * w_of(7)) * tw;
-            gs[6][m] = -gs[8][m] + Real(2.0 * w_of(8)) * tw;
-          }
-        }
-      }
-    }
-    const size_t row = (size_t)j * V.pitch;
-    Real Fv[N], rv[N], uvv[N], vvv[N], tv[N];
-    vload<Real>(V.F + row + x0, Fv);
-#pragma unroll
-    for (int m = 0; m < N; m++) {
-      Real fn[NPOP], gn[NPOP];
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) { fn[k] = fs[k][m]; gn[k] = gs[k][m]; }
-      if constexpr (std::is_same<Real, double>::value) {
-        node_ref<REFNUDGE>(V, row + x0 + m, fn, gn, Fv[m], rv[m], uvv[m], vvv[m], tv[m]);
-      } else {
-        node_shift(V, fn, gn, Fv[m], rv[m], uvv[m], vvv[m], tv[m]);
-      }
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) { fs[k][m] = fn[k]; gs[k][m] = gn[k]; }
-    }
-    if (active) {
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) {
-        vstore<Real>(V.fdst + (size_t)k * V.plane + row + x0, fs[k]);
-        vstore<Real>(V.gdst + (size_t)k * V.plane + row + x0, gs[k]);
-      }
-      vstore<Real>(V.F + row + x0, Fv);
-      if (V.write_uv) {
-        vstore<Real>(V.u + row + x0, uvv);
-        vstore<Real>(V.v + row + x0, vvv);
-      }
-      if (V.write_rt) {
-        vstore<Real>(V.rho + row + x0, rv);
-        vstore<Real>(V.T + row + x0, tv);
-      }
-    }
-  }
-}
-
-// ------------------------------------------------- one node per thread
-// The same step with one node per thread: every population is one plain
-// coalesced load at its pull address (x-1 and x+1 are neighbours in the same
-// 128-byte line, so L1/L2 absorb the shift; DRAM reads each value once).
-// All 18 loads are independent and issue back to back; the register budget
-// is small, so many warps per SM keep enough bytes in flight.
 template <typename Real, int TWALL>
 __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, Real* fs, Real* gs) {
   const int xl = (x == 0) ? V.nx - 1 : x - 1;       // source column of c_x = +1
@@ -286,8 +167,8 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
   });
 }
 
-template <typename Real, int TWALL, bool REFNUDGE>
-__global__ void __launch_bounds__(256) lb_node_kernel(const LBView<Real> V) {
+template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (x >= V.nx) return;
@@ -308,7 +189,7 @@ __global__ void __launch_bounds__(256) lb_node_kernel(const LBView<Real> V) {
     }
   }
   const size_t o = (size_t)j * V.pitch + x;
-  Real Fy = V.F[o], r, u, v, t;
+  Real Fy = V.Fin[o], r, u, v, t;
   if constexpr (std::is_same<Real, double>::value) {
     node_ref<REFNUDGE>(V, o, fs, gs, Fy, r, u, v, t);
   } else {
@@ -319,7 +200,7 @@ __global__ void __launch_bounds__(256) lb_node_kernel(const LBView<Real> V) {
     __stcs(V.fdst + (size_t)k * V.plane + o, fs[k]);
     __stcs(V.gdst + (size_t)k * V.plane + o, gs[k]);
   }
-  V.F[o] = Fy;
+  V.Fout[o] = Fy;
   if (V.write_uv) {
     V.u[o] = u;
     V.v[o] = v;
@@ -330,52 +211,90 @@ __global__ void __launch_bounds__(256) lb_node_kernel(const LBView<Real> V) {
   }
 }
 
-static int lb_variant() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("LBRB_LB_VARIANT");
-    v = (e && e[0] == 'w') ? 1 : 0;  // 0: one node per thread, 1: warp-chunk vectors
-  }
-  return v;
-}
+// --------------------------------------------------------------- launch
+// launch shapes tried by tune_lb: (threads per block, min blocks per SM)
+struct Shape { int bs, minb; };
+constexpr Shape SHAPES[] = {{256, 1}, {256, 2}, {256, 3}, {128, 4}, {128, 6}, {512, 1}, {512, 2}};
+constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 
-template <typename Real, int TWALL, bool REFNUDGE>
-static cudaError_t launch_lb(const LBView<Real>& V, cudaStream_t s) {
-  if (lb_variant() == 0) {
-    dim3 grid((V.nx + 255) / 256, V.ny);
-    lb_node_kernel<Real, TWALL, REFNUDGE><<<grid, 256, 0, s>>>(V);
-    return cudaGetLastError();
-  }
-  static int grid = 0;
-  static int dev_cached = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (grid == 0 || dev != dev_cached) {
-    int nsm = 0, per = 0;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lb_step_kernel<Real, TWALL, REFNUDGE>,
-                                                  256, 0);
-    grid = nsm * (per > 0 ? per : 1);
-    dev_cached = dev;
-  }
-  long need = (V.ntasks * WARP + 255) / 256;
-  int g = (int)(need < grid ? need : grid);
-  if (g < 1) g = 1;
-  lb_step_kernel<Real, TWALL, REFNUDGE><<<g, 256, 0, s>>>(V);
+template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB>
+static cudaError_t launch_shape(const LBView<Real>& V, cudaStream_t s) {
+  dim3 grid((V.nx + BS - 1) / BS, V.ny);
+  lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB><<<grid, BS, 0, s>>>(V);
   return cudaGetLastError();
 }
 
-cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, cudaStream_t s) {
-  if (twall == LBRB_TWALL_DIRICHLET)
-    return refnudge ? launch_lb<double, LBRB_TWALL_DIRICHLET, true>(V, s)
-                    : launch_lb<double, LBRB_TWALL_DIRICHLET, false>(V, s);
-  return refnudge ? launch_lb<double, LBRB_TWALL_ADIABATIC, true>(V, s)
-                  : launch_lb<double, LBRB_TWALL_ADIABATIC, false>(V, s);
+template <typename Real, int TWALL, bool REFNUDGE>
+static cudaError_t launch_lb(const LBView<Real>& V, int shape, cudaStream_t s) {
+  switch (shape) {
+    case 1: return launch_shape<Real, TWALL, REFNUDGE, 256, 2>(V, s);
+    case 2: return launch_shape<Real, TWALL, REFNUDGE, 256, 3>(V, s);
+    case 3: return launch_shape<Real, TWALL, REFNUDGE, 128, 4>(V, s);
+    case 4: return launch_shape<Real, TWALL, REFNUDGE, 128, 6>(V, s);
+    case 5: return launch_shape<Real, TWALL, REFNUDGE, 512, 1>(V, s);
+    case 6: return launch_shape<Real, TWALL, REFNUDGE, 512, 2>(V, s);
+    default: return launch_shape<Real, TWALL, REFNUDGE, 256, 1>(V, s);
+  }
 }
 
-cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s) {
-  if (twall == LBRB_TWALL_DIRICHLET) return launch_lb<float, LBRB_TWALL_DIRICHLET, false>(V, s);
-  return launch_lb<float, LBRB_TWALL_ADIABATIC, false>(V, s);
+cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, int shape,
+                           cudaStream_t s) {
+  if (twall == LBRB_TWALL_DIRICHLET)
+    return refnudge ? launch_lb<double, LBRB_TWALL_DIRICHLET, true>(V, shape, s)
+                    : launch_lb<double, LBRB_TWALL_DIRICHLET, false>(V, shape, s);
+  return refnudge ? launch_lb<double, LBRB_TWALL_ADIABATIC, true>(V, shape, s)
+                  : launch_lb<double, LBRB_TWALL_ADIABATIC, false>(V, shape, s);
+}
+
+cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStream_t s) {
+  if (twall == LBRB_TWALL_DIRICHLET) return launch_lb<float, LBRB_TWALL_DIRICHLET, false>(V, shape, s);
+  return launch_lb<float, LBRB_TWALL_ADIABATIC, false>(V, shape, s);
+}
+
+// Autotuner: time every launch shape on this run's grid (CUDA events, `reps`
+// launches after one warm-up launch each) and return the fastest.  A trial
+// launch reads the current state and writes only the other population
+// buffer and the other F buffer, which the real step overwrites; moments
+// are not written.  Box-nudged FP64 steps update nud_term in place and are
+// not tuned (shape 0).
+template <typename Real>
+static int tune(const LBView<Real>& Vin, int twall, bool refnudge, cudaStream_t s, int reps,
+                float* best_ms) {
+  LBView<Real> V = Vin;
+  V.write_uv = 0;
+  V.write_rt = 0;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int best = 0;
+  float bt = 1e30f;
+  for (int sh = 0; sh < NSHAPES; sh++) {
+    cudaError_t e;
+    auto go = [&]() {
+      if constexpr (std::is_same<Real, double>::value) return launch_lb_fp64(V, twall, refnudge, sh, s);
+      else return launch_lb_fp32(V, twall, sh, s);
+    };
+    e = go();
+    if (e != cudaSuccess) { cudaGetLastError(); continue; }
+    cudaEventRecord(a, s);
+    for (int r = 0; r < reps; r++) go();
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < bt) { bt = ms; best = sh; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (best_ms) *best_ms = bt / reps;
+  return best;
+}
+
+int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best_ms) {
+  return tune<double>(V, twall, false, s, 3, best_ms);
+}
+int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_ms) {
+  return tune<float>(V, twall, false, s, 3, best_ms);
 }
 
 }  // namespace lbrb

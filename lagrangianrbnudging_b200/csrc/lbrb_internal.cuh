@@ -79,67 +79,6 @@ enum : unsigned {
   DFLAG_BOXCAP = 4u,     // box nudging cell list inconsistent
 };
 
-// ---------------------------------------------------------------- vectors
-template <typename Real>
-struct Vec;
-template <>
-struct Vec<double> {
-  static constexpr int N = 2;
-  using T = double2;
-  __device__ static inline void unpack(const T& v, double* o) { o[0] = v.x; o[1] = v.y; }
-  __device__ static inline T pack(const double* a) { return make_double2(a[0], a[1]); }
-};
-template <>
-struct Vec<float> {
-  static constexpr int N = 4;
-  using T = float4;
-  __device__ static inline void unpack(const T& v, float* o) {
-    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
-  }
-  __device__ static inline T pack(const float* a) { return make_float4(a[0], a[1], a[2], a[3]); }
-};
-
-template <typename Real>
-__device__ __forceinline__ void vload(const Real* __restrict__ p, Real* o) {
-  using V = Vec<Real>;
-  typename V::T v = __ldcs(reinterpret_cast<const typename V::T*>(p));
-  V::unpack(v, o);
-}
-template <typename Real>
-__device__ __forceinline__ void vstore(Real* __restrict__ p, const Real* a) {
-  using V = Vec<Real>;
-  __stcs(reinterpret_cast<typename V::T*>(p), V::pack(a));
-}
-
-// Load VEC consecutive values of `row` pulled along x by `cx`:
-//   out[m] = row[(x0 + m - cx) mod nx].
-// Lanes own aligned chunks [x0, x0+VEC); the one value that lies in the
-// neighbour lane's chunk comes by shuffle, and lanes at the warp or row edge
-// fetch it with a scalar load (periodic wrap).
-template <int CX, typename Real>
-__device__ __forceinline__ void load_pull_x(const Real* __restrict__ row, int x0, int lane,
-                                            int nx, Real* out) {
-  constexpr int N = Vec<Real>::N;
-  Real v[N];
-  vload<Real>(row + x0, v);
-  if (CX == 0) {
-#pragma unroll
-    for (int m = 0; m < N; m++) out[m] = v[m];
-  } else if (CX == 1) {
-    Real left = __shfl_up_sync(0xffffffffu, v[N - 1], 1);
-    if (lane == 0 || x0 == 0) left = __ldcs(row + (x0 == 0 ? nx - 1 : x0 - 1));
-    out[0] = left;
-#pragma unroll
-    for (int m = 1; m < N; m++) out[m] = v[m - 1];
-  } else {
-    Real right = __shfl_down_sync(0xffffffffu, v[0], 1);
-    if (lane == WARP - 1 || x0 + N >= nx) right = __ldcs(row + (x0 + N >= nx ? 0 : x0 + N));
-#pragma unroll
-    for (int m = 0; m < N - 1; m++) out[m] = v[m + 1];
-    out[N - 1] = right;
-  }
-}
-
 // ------------------------------------------------------------ kernel views
 template <typename Real>
 struct LBView {
@@ -147,7 +86,8 @@ struct LBView {
   const Real* __restrict__ gsrc;
   Real* __restrict__ fdst;
   Real* __restrict__ gdst;
-  Real* __restrict__ F;    // buoyancy F_y of the NEXT step; read then rewritten in place
+  const Real* __restrict__ Fin;  // buoyancy F_y of this step (from step n-1 moments)
+  Real* __restrict__ Fout;       // buoyancy of the next step (this step's moments)
   Real* __restrict__ rho;
   Real* __restrict__ u;
   Real* __restrict__ v;
@@ -163,8 +103,6 @@ struct LBView {
   double* __restrict__ nud_term;
   double alpha;
   int write_uv, write_rt;
-  int chunks_per_row;
-  long ntasks;
 };
 
 // --------------------------------------------------------------- handle
@@ -187,11 +125,22 @@ struct Handle {
   void* pops[2] = {nullptr, nullptr};
   int cur = 0;        // buffer holding the current post-collision state
   // scalar fields (Real)
-  void* F = nullptr;
-  void* rho = nullptr;
-  void* uv[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [slot][u/v]
-  int uvcur = 0;      // slot of the current u, v (the other holds u^{n-1})
-  void* T = nullptr;
+  void* F[2] = {nullptr, nullptr};  // buoyancy for the step after the state in pops[cur] is F[cur]
+  int lb_shape = -1;                // launch shape picked by the autotuner (-1: not tuned yet)
+  float lb_shape_ms = 0.f;
+  // moments: rho and T of the state in pops[cur] are rho[cur], T[cur];
+  // u, v rotate over three slots: u^n in uvcur, u^{n-1} in uvprev, so the
+  // particle kernel of step n can run beside the fused kernel of step n+1
+  void* rho[2] = {nullptr, nullptr};
+  void* T[2] = {nullptr, nullptr};
+  void* uv[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  int uvcur = 0, uvprev = 1;
+  // particle stream and the events that order it against the fused kernel
+  cudaStream_t pstream = nullptr;
+  cudaEvent_t ev_lb = nullptr;       // fused kernel of the last queued step done
+  cudaEvent_t ev_uv[3] = {nullptr, nullptr, nullptr};  // last particle kernel reading slot done
+  cudaEvent_t ev_T[2] = {nullptr, nullptr};            // last particle kernel reading T[b] done
+  cudaEvent_t ev_pjoin = nullptr;
   bool moments_valid = false;
   // particles (FP64)
   int np = 0;
