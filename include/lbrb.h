@@ -113,6 +113,11 @@ LBRB_API int lbrb_abi_version(void);
  * (temppart_dump.c:348-507) and dumpf/dumpg (temppart_dump.c:52-141). */
 LBRB_API int lbrb_set_populations(lbrb_t *h, const double *f, const double *g, int layout);
 LBRB_API int lbrb_get_populations(lbrb_t *h, double *f, double *g, int layout);
+/* Post-stream (pre-collision) populations of the last step, walls applied:
+ * what dumpfpre/dumpgpre write (temppart_dump.c:143-232, called at
+ * :1702-1710).  Rebuilt from the state before the last step, which the
+ * ping-pong layout keeps; any pointer may be NULL. */
+LBRB_API int lbrb_get_poststream(lbrb_t *h, double *f, double *g, int layout);
 /* Moments of the last step (rhopre, upre, vpre, temppre); any pointer may be
  * NULL on get.  The next step's buoyancy uses rho and T (forcingconstructWW,
  * temppart_dump.c:744-755). */

@@ -38,6 +38,7 @@ EXPORTS = [
     "lbrb_record_pending", "lbrb_record_drain", "lbrb_nudge_init", "lbrb_nudge_load",
     "lbrb_nudge_obs", "lbrb_energy", "lbrb_nusselt", "lbrb_profile", "lbrb_set_stream",
     "lbrb_set_timing", "lbrb_get_timing", "lbrb_stats_noalloc", "lbrb_get_launch_shape",
+    "lbrb_get_poststream",
 ]
 
 
@@ -102,6 +103,7 @@ def lib() -> C.CDLL:
         "lbrb_set_stream": (C.c_int, [vp, vp]),
         "lbrb_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
+        "lbrb_get_poststream": (C.c_int, [vp, dp, dp, C.c_int]),
         "lbrb_get_launch_shape": (C.c_int, [vp, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_stats_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_double, C.c_double, C.c_double, vp, dp]),
@@ -202,6 +204,14 @@ class Run:
         f = np.empty(shape)
         g = np.empty(shape)
         self._ck(lib().lbrb_get_populations(self.h, _dp(f), _dp(g), LAYOUT[layout]))
+        return f, g
+
+    def get_poststream(self, layout="soa"):
+        """post-stream populations of the last step (dumpfpre/dumpgpre)"""
+        shape = (9, self.ny, self.nx) if layout == "soa" else (self.nx + 2, self.ny + 2, 9)
+        f = np.empty(shape)
+        g = np.empty(shape)
+        self._ck(lib().lbrb_get_poststream(self.h, _dp(f), _dp(g), LAYOUT[layout]))
         return f, g
 
     def set_moments(self, rho, u, v, T, layout="soa"):

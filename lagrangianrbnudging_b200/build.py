@@ -17,6 +17,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liblbrb.so"
+HOST = PKG / "lbrb_host"
 SOURCES = ["lb_kernels.cu", "particle_kernels.cu", "nudge_kernels.cu", "aux_kernels.cu", "capi.cu",
            "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -32,7 +33,9 @@ def nvcc() -> str:
 
 
 def _stale() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not HOST.exists():
+        return True
+    if (PKG / "host" / "lbrb_host.c").stat().st_mtime > HOST.stat().st_mtime:
         return True
     t = LIB.stat().st_mtime
     deps = [CSRC / s for s in SOURCES] + [CSRC / "lbrb_internal.cuh", ROOT / "include" / "lbrb.h"]
@@ -55,6 +58,11 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
+    # the host program, linked against the library next to it
+    tmp = HOST.with_suffix(".tmp")
+    subprocess.run(["gcc", "-std=c99", "-O2", "-Wall", "-o", str(tmp), str(PKG / "host" / "lbrb_host.c"),
+                    f"-L{PKG}", "-llbrb", "-Wl,-rpath,$ORIGIN", "-lm"], check=True)
+    os.replace(tmp, HOST)
     return LIB
 
 

@@ -20,6 +20,8 @@ cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, in
                            cudaStream_t s);
 cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStream_t s);
 int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best_ms);
+cudaError_t launch_pull_fp64(const LBView<double>& V, int twall, void* outf, void* outg, cudaStream_t s);
+cudaError_t launch_pull_fp32(const LBView<float>& V, int twall, void* outf, void* outg, cudaStream_t s);
 int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_ms);
 cudaError_t launch_particles(const void* u, const void* v, const void* ub, const void* vb,
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,
@@ -343,6 +345,7 @@ int lbrb_set_populations(lbrb_t* h, const double* f, const double* g, int layout
   CK(h, launch_pops_in(st + cnt, layout, pop_base(h, h->cur, 1), fp32(h), h->p.nx, h->p.ny,
                        h->pitch, h->plane, T0_of(h), h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
+  h->prev_valid = false;
   return LBRB_OK;
 }
 
@@ -638,6 +641,34 @@ int lbrb_get_launch_shape(const lbrb_t* h, int* block, int* min_blocks, float* m
   return LBRB_OK;
 }
 
+int lbrb_get_poststream(lbrb_t* h, double* f, double* g, int layout) {
+  if (!h || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
+    return fail(h, LBRB_ERR_ARG, "get_poststream: bad arguments");
+  if (!h->prev_valid)
+    return fail(h, LBRB_ERR_STATE, "get_poststream: no step since the populations were set");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t tmp = 2 * NPOP * h->plane * h->esize;
+  const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
+  int rc = ensure_staging(h, tmp + 2 * bytes);
+  if (rc) return rc;
+  char* t = (char*)h->staging;
+  double* st = (double*)(t + tmp);
+  const int prev = h->cur ^ 1;
+  if (fp32(h)) CK(h, launch_pull_fp32(make_view<float>(h, prev, h->cur, h->uvcur, 0, 0), h->p.twall, t, t + tmp / 2, h->stream));
+  else CK(h, launch_pull_fp64(make_view<double>(h, prev, h->cur, h->uvcur, 0, 0), h->p.twall, t, t + tmp / 2, h->stream));
+  if (f) {
+    CK(h, launch_pops_out(t, layout, st, fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, 1.0, h->stream));
+    CK(h, cudaMemcpyAsync(f, st, bytes, cudaMemcpyDeviceToHost, h->stream));
+  }
+  if (g) {
+    CK(h, launch_pops_out(t + tmp / 2, layout, st + cnt, fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane,
+                          T0_of(h), h->stream));
+    CK(h, cudaMemcpyAsync(g, st + cnt, bytes, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  return LBRB_OK;
+}
+
 int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   if (n == 0) return LBRB_OK;
@@ -748,6 +779,7 @@ int lbrb_step(lbrb_t* h, int n) {
       }
     }
     h->cur = dst;
+    h->prev_valid = true;
     if (write_uv) {
       h->uvprev = h->uvcur;
       h->uvcur = uvn;

@@ -167,6 +167,42 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
   });
 }
 
+// anti-bounce-back with the post-stream opposite population
+// (temppart_dump.c:896-921): g_in = -g_opp + 2 w T_wall (shifted form: T_wall - T0)
+template <typename Real>
+__device__ __forceinline__ void dirichlet_walls(const LBView<Real>& V, int j, Real* gs) {
+  if (j == V.ny - 1) {
+    const Real tw = std::is_same<Real, double>::value ? (Real)V.Tup : (Real)(V.Tup - V.T0);
+    gs[4] = -gs[2] + Real(2.0 * w_of(2)) * tw;
+    gs[7] = -gs[5] + Real(2.0 * w_of(5)) * tw;
+    gs[8] = -gs[6] + Real(2.0 * w_of(6)) * tw;
+  }
+  if (j == 0) {
+    const Real tw = std::is_same<Real, double>::value ? (Real)V.Tdown : (Real)(V.Tdown - V.T0);
+    gs[2] = -gs[4] + Real(2.0 * w_of(4)) * tw;
+    gs[5] = -gs[7] + Real(2.0 * w_of(7)) * tw;
+    gs[6] = -gs[8] + Real(2.0 * w_of(8)) * tw;
+  }
+}
+
+// post-stream populations only (walls applied): dumpfpre/dumpgpre
+template <typename Real, int TWALL>
+__global__ void __launch_bounds__(128) lb_pull_kernel(const LBView<Real> V, Real* __restrict__ outf,
+                                                      Real* __restrict__ outg) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (x >= V.nx) return;
+  Real fs[NPOP], gs[NPOP];
+  pull_node<Real, TWALL>(V, j, x, fs, gs);
+  if (TWALL == LBRB_TWALL_DIRICHLET) dirichlet_walls(V, j, gs);
+  const size_t o = (size_t)j * V.pitch + x;
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) {
+    outf[(size_t)k * V.plane + o] = fs[k];
+    outg[(size_t)k * V.plane + o] = gs[k];
+  }
+}
+
 template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB>
 __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -174,20 +210,7 @@ __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V)
   if (x >= V.nx) return;
   Real fs[NPOP], gs[NPOP];
   pull_node<Real, TWALL>(V, j, x, fs, gs);
-  if (TWALL == LBRB_TWALL_DIRICHLET) {
-    if (j == V.ny - 1) {
-      const Real tw = std::is_same<Real, double>::value ? (Real)V.Tup : (Real)(V.Tup - V.T0);
-      gs[4] = -gs[2] + Real(2.0 * w_of(2)) * tw;
-      gs[7] = -gs[5] + Real(2.0 * w_of(5)) * tw;
-      gs[8] = -gs[6] + Real(2.0 * w_of(6)) * tw;
-    }
-    if (j == 0) {
-      const Real tw = std::is_same<Real, double>::value ? (Real)V.Tdown : (Real)(V.Tdown - V.T0);
-      gs[2] = -gs[4] + Real(2.0 * w_of(4)) * tw;
-      gs[5] = -gs[7] + Real(2.0 * w_of(7)) * tw;
-      gs[6] = -gs[8] + Real(2.0 * w_of(8)) * tw;
-    }
-  }
+  if (TWALL == LBRB_TWALL_DIRICHLET) dirichlet_walls(V, j, gs);
   const size_t o = (size_t)j * V.pitch + x;
   Real Fy = V.Fin[o], r, u, v, t;
   if constexpr (std::is_same<Real, double>::value) {
@@ -288,6 +311,23 @@ static int tune(const LBView<Real>& Vin, int twall, bool refnudge, cudaStream_t 
   cudaEventDestroy(b);
   if (best_ms) *best_ms = bt / reps;
   return best;
+}
+
+template <typename Real>
+static cudaError_t launch_pull_t(const LBView<Real>& V, int twall, void* outf, void* outg,
+                                 cudaStream_t s) {
+  dim3 grid((V.nx + 127) / 128, V.ny);
+  if (twall == LBRB_TWALL_DIRICHLET)
+    lb_pull_kernel<Real, LBRB_TWALL_DIRICHLET><<<grid, 128, 0, s>>>(V, (Real*)outf, (Real*)outg);
+  else
+    lb_pull_kernel<Real, LBRB_TWALL_ADIABATIC><<<grid, 128, 0, s>>>(V, (Real*)outf, (Real*)outg);
+  return cudaGetLastError();
+}
+cudaError_t launch_pull_fp64(const LBView<double>& V, int twall, void* outf, void* outg, cudaStream_t s) {
+  return launch_pull_t<double>(V, twall, outf, outg, s);
+}
+cudaError_t launch_pull_fp32(const LBView<float>& V, int twall, void* outf, void* outg, cudaStream_t s) {
+  return launch_pull_t<float>(V, twall, outf, outg, s);
 }
 
 int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best_ms) {

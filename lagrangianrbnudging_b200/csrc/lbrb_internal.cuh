@@ -124,6 +124,7 @@ struct Handle {
   // populations: pops[buf] holds f (9 planes) then g (9 planes)
   void* pops[2] = {nullptr, nullptr};
   int cur = 0;        // buffer holding the current post-collision state
+  bool prev_valid = false;  // pops[cur^1] holds the state before the last step
   // scalar fields (Real)
   void* F[2] = {nullptr, nullptr};  // buoyancy for the step after the state in pops[cur] is F[cur]
   int lb_shape = -1;                // launch shape picked by the autotuner (-1: not tuned yet)

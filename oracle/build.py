@@ -8,7 +8,7 @@
   ``#define`` blocks at Trajectories/code/temppart_dump.c:15-31,
   Trajectories/code/mympi2.h:14-21, Nudging/code/tempvel_nudge.c:13-31) and
   hard-coded input paths (temppart_dump.c:374,454,535,615;
-  tempvel_nudge.c:1415,2086-2101,2151) are rewritten.  The patched copies and
+  tempvel_nudge.c:282,361,441,520,1415,2086-2101,2151) are rewritten.  The patched copies and
   the binaries go to ``oracle/_ref/<tag>/`` only (git-ignored; never
   committed).  Compiler: ``gcc -std=c99 -O2`` as the reference makefiles use.
 """
@@ -39,6 +39,7 @@ PATH_PATCHES = [
     ("/mnt/petaStor/agasthya/LagrangianNudging/High_Ra/St0.5/beta1/", "obs/"),
     ("/mnt/petaStor/agasthya/LagrangianNudging/High_Ra/", ""),
     ("../../St0.5/beta1/", "obs/"),
+    ("../dump_Guo2/", ""),
 ]
 
 
@@ -98,7 +99,7 @@ def build_ref(program: str, params: dict, tag: str | None = None) -> Path:
     csrc = (REFERENCE_ROOT / csrc_rel).read_text()
     hdr = (REFERENCE_ROOT / hdr_rel).read_text()
     shim = "".join((SHIM / n).read_text() for n in ("mpi.h", "mpi_shim.c", "hdf5.h", "hdf5_shim.c"))
-    key = hashlib.sha1(repr((program, sorted(params.items()), csrc, hdr, shim)).encode()).hexdigest()[:12]
+    key = hashlib.sha1(repr((program, sorted(params.items()), csrc, hdr, shim, PATH_PATCHES)).encode()).hexdigest()[:12]
     tag = tag or f"{program}_{key}"
     d = REF_OUT / tag
     exe = d / program

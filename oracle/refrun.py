@@ -81,6 +81,34 @@ def traj_params(base: dict, nsteps: int, noutconfig: int, nprtcl: int, tracer: b
     )
 
 
+def run_trajectories_scratch(refp: dict, workdir: Path | None = None, tag: str | None = None) -> dict:
+    """Run temppart_dump with scratch=1, Particle_scratch=1 on one rank."""
+    exe = build.build_ref("temppart_dump", refp, tag)
+    nx, ny, nsteps, nout_c = refp["nx"], refp["ny"], refp["nsteps"], refp["noutconfig"]
+    wd = Path(tempfile.mkdtemp(prefix="lbrb_refs_")) if workdir is None else Path(workdir)
+    (wd / "Prtcl_Veldata1").mkdir(parents=True, exist_ok=True)
+    (wd / "Tempfolder").mkdir(exist_ok=True)
+    run_exe(exe, wd, 1, None)
+    out = {"workdir": wd}
+    last = nsteps + 1
+    out["f"] = _from_ref_pops(np.fromfile(wd / f"confnew{last}.h5.d" / "f.bin"), nx, ny)
+    out["g"] = _from_ref_pops(np.fromfile(wd / f"congnew{last}.h5.d" / "g.bin"), nx, ny)
+    out["fpre"] = _from_ref_pops(np.fromfile(wd / f"confpre{nsteps}.h5.d" / "f.bin"), nx, ny)
+    out["gpre"] = _from_ref_pops(np.fromfile(wd / f"congpre{nsteps}.h5.d" / "g.bin"), nx, ny)
+    recs = {}
+    for s in range(nout_c, nsteps + 1, nout_c):
+        d = wd / "Prtcl_Veldata1" / f"Particles{s}.h5.d"
+        r = {"id": np.fromfile(d / "id.bin", dtype=np.int32)}
+        for name in REC_FIELDS:
+            if (d / f"{name}.bin").exists():
+                r[name] = np.fromfile(d / f"{name}.bin")
+        recs[s] = r
+    out["records"] = recs
+    out["init_x"] = np.fromfile(wd / "init_prtclx0.in")
+    out["init_y"] = np.fromfile(wd / "init_prtcly0.in")
+    return out
+
+
 def run_trajectories(refp: dict, f0, g0, fpre0, gpre0, ids, px, py, pu, pv,
                      np_ranks: int = 1, dims: str | None = None, workdir: Path | None = None,
                      tag: str | None = None) -> dict:
@@ -125,10 +153,10 @@ def run_trajectories(refp: dict, f0, g0, fpre0, gpre0, ids, px, py, pu, pv,
 
 
 def nudge_params(base: dict, nsteps: int, ntempread: int, alpha: float, noutconfig: int,
-                 nout: int) -> dict:
+                 nout: int, scratch: int = 1) -> dict:
     """compile-time parameters of tempvel_nudge.c (Nprtcl stays 40*40)"""
     return dict(
-        nx=int(base["nx"]), ny=int(base["ny"]), scratch=1, contin=0, nstart=0,
+        nx=int(base["nx"]), ny=int(base["ny"]), scratch=int(scratch), contin=0, nstart=0,
         nsteps=int(nsteps), nout=int(nout), noutconfig=int(noutconfig),
         ntempread=int(ntempread), relax=float(base["relax"]), relaxg=float(base["relaxg"]),
         Tup=float(base["Tup"]), Tdown=float(base["Tdown"]), gravity=float(base["gravity"]),
@@ -161,7 +189,7 @@ def scratch_ic_T(nx: int, ny: int, Tup: float, Tdown: float, npy: int) -> np.nda
 
 
 def run_nudging(refp: dict, init_obs: dict, files: dict, np_ranks: int = 2, dims: str = "1x2",
-                workdir: Path | None = None, tag: str | None = None) -> dict:
+                workdir: Path | None = None, tag: str | None = None, restart: dict | None = None) -> dict:
     """Run tempvel_nudge (scratch IC, contin=0).  init_obs: x,y,T,id arrays
     (init_prtcl*0.in); files: {step: dict(x,y,id,temp)} observation files."""
     exe = build.build_ref("tempvel_nudge", refp, tag)
@@ -175,6 +203,12 @@ def run_nudging(refp: dict, init_obs: dict, files: dict, np_ranks: int = 2, dims
     np.asarray(init_obs["y"], np.float64).tofile(obs / "init_prtcly0.in")
     np.asarray(init_obs["T"], np.float64).tofile(obs / "init_prtclT0.in")
     np.asarray(init_obs["id"], np.int32).tofile(obs / "init_prtcl_id0.in")
+    if restart is not None:
+        # restart route (scratch=0): conf/cong/confpre/congpre in the run directory
+        _write_ds(wd / "conf.h5.d" / "f.bin", _to_ref_pops(restart["f"]))
+        _write_ds(wd / "cong.h5.d" / "g.bin", _to_ref_pops(restart["g"]))
+        _write_ds(wd / "confpre.h5.d" / "f.bin", _to_ref_pops(restart["fpre"]))
+        _write_ds(wd / "congpre.h5.d" / "g.bin", _to_ref_pops(restart["gpre"]))
     for s, d in files.items():
         base = obs / "Prtcl_Veldata1" / f"Particles{s}.h5.d"
         _write_ds(base / "x.bin", np.asarray(d["x"], np.float64))

@@ -10,7 +10,7 @@ from pathlib import Path
 
 import numpy as np
 
-from oracle.oracle import Oracle, closure
+from oracle.oracle import Oracle, closure  # noqa: F401  (closure re-exported for the generator)
 
 GOLDEN = Path(__file__).resolve().parent
 W = np.array([16 / 36, 4 / 36, 4 / 36, 4 / 36, 4 / 36, 1 / 36, 1 / 36, 1 / 36, 1 / 36])
@@ -35,9 +35,20 @@ TRAJ_CASES = {
                       inertial=True, taulag=30.0, beta=0.1, nsteps=120, noutconfig=40),
 }
 
+# runs of the host program against the reference's own scratch / restart paths
+SCRATCH_TRAJ_CASES = {
+    # the reference's scratch state (tanh + rand(), one rank) and its 40x40
+    # particle lattice, which places 2 particles on a 48x24 grid
+    "traj_scratch": dict(nx=48, ny=24, Ra=1e5, U=0.1, nprtcl=2, tracer=True, taulag=50.0,
+                         beta=0.0, nsteps=100, noutconfig=25),
+}
+
 NUDGE_CASES = {
     "nudge_box": dict(nx=64, ny=32, Ra=1e5, U=0.1, nsteps=30, ntempread=5, alpha=0.1,
                       nprtcl=1600, seed=11, npy=2),
+    # restart route of the nudging program (scratch=0, contin=0)
+    "nudge_restart": dict(nx=64, ny=32, Ra=1e5, U=0.1, nsteps=30, ntempread=5, alpha=0.1,
+                          nprtcl=1600, seed=13, npy=2, restart=True),
 }
 
 
@@ -105,15 +116,61 @@ def nudge_case(name: str) -> dict:
     params = dict(base, twall="adiabatic", nudge="refbox", alpha=c["alpha"], ntempread=nt)
     c.update(base=base, params=params, Tic=Tic,
              init_obs=dict(x=x0, y=y0, T=T0, id=ids0), files=files)
+    if c.get("restart"):
+        # positive restart populations (restore* abort on an exact zero)
+        rr = np.random.default_rng(c["seed"] + 500)
+        Tr = rr.uniform(-0.5, 0.5, (ny, nx))
+        Tr[np.abs(Tr) < 1e-3] = 1e-3
+        c["restart_pops"] = dict(
+            f=W[:, None, None] * (1.0 + 1e-3 * rr.uniform(-1, 1, (9, ny, nx))),
+            g=Tr[None] * W[:, None, None] * (1.0 + 1e-3 * rr.uniform(-1, 1, (9, ny, nx))),
+            fpre=W[:, None, None] * (1.0 + 1e-3 * rr.uniform(-1, 1, (9, ny, nx))),
+            gpre=Tr[None] * W[:, None, None] * (1.0 + 1e-3 * rr.uniform(-1, 1, (9, ny, nx))))
     return c
+
+
+def initial_box_mask(nx: int, ny: int) -> np.ndarray:
+    """nudge_vol of set_nudge_vol (contin==0, tempvel_nudge.c:2054-2079): the
+    7x7 boxes around the 40x40 particle lattice of a 1680x840 run"""
+    xs = [5]
+    for i in range(1, 40):
+        xs.append(xs[-1] + 42 + (i % 2))
+    xs[-1] += 3
+    ys = [10 + 21 * i for i in range(40)]
+    i = np.arange(1, nx + 1)[None, :]
+    j = np.arange(1, ny + 1)[:, None]
+    m = np.zeros((ny, nx), bool)
+    for a in xs:
+        for b in ys:
+            m |= (np.abs(i - a) < 4) & (np.abs(j - b) < 4)
+    return m
+
+
+def nudge_initial_state(c: dict) -> dict:
+    """f, g, rho, u, v, T at the start of the nudging run (interior arrays)"""
+    ny, nx = c["ny"], c["nx"]
+    if c.get("restart"):
+        rp = c["restart_pops"]
+        T = np.zeros((ny, nx))
+        m = initial_box_mask(nx, ny)
+        # inithydro contin==0 (tempvel_nudge.c:598-617): sum of congpre in k order
+        t = np.zeros((ny, nx))
+        for k in range(9):
+            t = t + rp["gpre"][k]
+        T[m] = t[m]
+        return dict(f=W[:, None, None] * np.ones((1, ny, nx)), g=rp["g"].copy(),
+                    rho=np.ones((ny, nx)), u=np.zeros((ny, nx)), v=np.zeros((ny, nx)), T=T)
+    return dict(f=W[:, None, None] * np.ones((1, ny, nx)), g=c["Tic"][None] * W[:, None, None],
+                rho=np.ones((ny, nx)), u=np.zeros((ny, nx)), v=np.zeros((ny, nx)), T=c["Tic"].copy())
 
 
 def run_oracle_nudge(c: dict) -> dict:
     o = Oracle(c["params"], c["nprtcl"])
-    o.f[:] = W[:, None, None] * 1.0
-    o.g[:] = c["Tic"][None] * W[:, None, None]
-    o.rho[:] = 1.0
-    o.T[:] = c["Tic"]
+    st = nudge_initial_state(c)
+    o.f[:] = st["f"]
+    o.g[:] = st["g"]
+    o.rho[:] = st["rho"]
+    o.T[:] = st["T"]
     o.u[:] = 0.0
     o.v[:] = 0.0
     io = c["init_obs"]

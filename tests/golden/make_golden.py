@@ -32,6 +32,26 @@ def make_traj(name: str) -> dict:
     out = refrun.run_trajectories(refp, c["f0"], c["g0"], c["f0"], c["g0"], c["ids"],
                                   c["px"], c["py"], c["pu"], c["pv"])
     z = {"f": out["f"], "g": out["g"], "evolution": out["evolution"]}
+    if name == "traj_inertial":
+        z["fpre"], z["gpre"] = out["fpre"], out["gpre"]
+    for s, r in out["records"].items():
+        order = np.argsort(r["id"], kind="stable")
+        z[f"rec{s}_id"] = r["id"][order]
+        for k in refrun.REC_FIELDS:
+            if k in r:
+                z[f"rec{s}_{k}"] = r[k][order]
+    return z
+
+
+def make_scratch(name: str) -> dict:
+    c = dict(cases.SCRATCH_TRAJ_CASES[name])
+    base = cases.closure(c["nx"], c["ny"], Ra=c["Ra"], Pr=1.0, U=c["U"])
+    refp = refrun.traj_params(base, c["nsteps"], c["noutconfig"], c["nprtcl"], tracer=c["tracer"],
+                              taulag=c["taulag"], beta=c["beta"])
+    refp.update(scratch=1, Particle_scratch=1)
+    out = refrun.run_trajectories_scratch(refp)
+    z = {"f": out["f"], "g": out["g"], "fpre": out["fpre"], "gpre": out["gpre"],
+         "init_x": out["init_x"], "init_y": out["init_y"]}
     for s, r in out["records"].items():
         order = np.argsort(r["id"], kind="stable")
         z[f"rec{s}_id"] = r["id"][order]
@@ -44,9 +64,9 @@ def make_traj(name: str) -> dict:
 def make_nudge(name: str) -> dict:
     c = cases.nudge_case(name)
     refp = refrun.nudge_params(c["base"], c["nsteps"], c["ntempread"], c["alpha"],
-                               noutconfig=10, nout=10**6)
+                               noutconfig=10, nout=10**6, scratch=0 if c.get("restart") else 1)
     out = refrun.run_nudging(refp, c["init_obs"], c["files"], np_ranks=c["npy"],
-                             dims=f"1x{c['npy']}")
+                             dims=f"1x{c['npy']}", restart=c.get("restart_pops"))
     z = {"f": out["f"], "g": out["g"]}
     for s, d in out["snaps"].items():
         for k, a in d.items():
@@ -57,6 +77,10 @@ def make_nudge(name: str) -> dict:
 def main():
     for name in cases.TRAJ_CASES:
         z = make_traj(name)
+        np.savez_compressed(cases.golden_path(name), **z)
+        print("wrote", cases.golden_path(name))
+    for name in cases.SCRATCH_TRAJ_CASES:
+        z = make_scratch(name)
         np.savez_compressed(cases.golden_path(name), **z)
         print("wrote", cases.golden_path(name))
     for name in cases.NUDGE_CASES:

@@ -63,3 +63,14 @@ def test_box_nudging_needs_fp64(L):
     p = lb.make_params(nx=64, ny=32, precision="fp32", nudge="refbox", nobs=16, ntempread=5)
     h = C.c_void_p()
     assert L.lbrb_create(C.byref(p), C.byref(h)) == -9
+
+
+def test_host_program_rejects_bad_usage():
+    import subprocess
+
+    host = Path(build.__file__).resolve().parent / "lbrb_host"
+    build.build()
+    assert subprocess.run([str(host)], capture_output=True).returncode == 2
+    assert subprocess.run([str(host), "trajectories", "nosuchparam=1"], capture_output=True).returncode == 2
+    # the reference's contin=1 restart reads an uninitialised value; refused
+    assert subprocess.run([str(host), "nudging", "contin=1"], capture_output=True).returncode == 2

@@ -74,16 +74,15 @@ def test_fp64_moments_particles_energy_match_oracle():
     assert abs(nu - oo.nusselt()) <= 1e-12 * abs(oo.nusselt())
 
 
-def test_fp64_box_nudging_bit_exact_vs_reference():
-    c = cases.nudge_case("nudge_box")
-    z = cases.load_golden("nudge_box")
-    W = cases.W
+@pytest.mark.parametrize("name", list(cases.NUDGE_CASES))
+def test_fp64_box_nudging_bit_exact_vs_reference(name):
+    c = cases.nudge_case(name)
+    z = cases.load_golden(name)
+    st = cases.nudge_initial_state(c)
     with lb.Run(**c["base"], precision="fp64", twall="adiabatic", nudge="refbox",
                 alpha=c["alpha"], ntempread=c["ntempread"], nobs=c["nprtcl"]) as r:
-        r.set_populations(W[:, None, None] * np.ones((1, c["ny"], c["nx"])),
-                          c["Tic"][None] * W[:, None, None])
-        r.set_moments(np.ones_like(c["Tic"]), np.zeros_like(c["Tic"]), np.zeros_like(c["Tic"]),
-                      c["Tic"])
+        r.set_populations(st["f"], st["g"])
+        r.set_moments(st["rho"], st["u"], st["v"], st["T"])
         io = c["init_obs"]
         r.nudge_init(io["x"], io["y"], io["T"], io["id"])
         nt = c["ntempread"]
