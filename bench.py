@@ -523,7 +523,8 @@ def run_lb_only(args, torch) -> dict:
     b.build()
     nx, ny = (int(a) for a in args.grid.lower().split("x"))
     base = lb.closure(nx, ny, Ra=RA, Pr=PR, U=U)
-    with lb.Run(**base, precision=args.precision, device=0) as r:
+    fixed = dict(autotune=0, launch_shape=args.shape) if args.shape >= 0 else {}
+    with lb.Run(**base, precision=args.precision, device=0, **fixed) as r:
         r.init_conduction(SEED, 1e-3)
         ms, timing, _, _ = timed_steps(r, torch, args.steps, args.warmup, None, 0)
         shape = r.launch_shape()
@@ -547,6 +548,8 @@ def main():
                     help="fused kernel alone on --grid (the ncu capture command)")
     ap.add_argument("--grid", default="2048x1024")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--shape", type=int, default=-1,
+                    help="lb-only: fixed launch shape index instead of the autotuner")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

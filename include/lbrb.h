@@ -96,6 +96,9 @@ typedef struct {
   int record_slots;       /* records held before lbrb_record_drain() must run */
   int device;             /* CUDA device ordinal */
   int autotune;           /* 1: time the fused kernel's launch shapes on the first step */
+  int launch_shape;       /* with autotune 0: the shape used, an index into
+                           * (threads per block, min blocks per SM) =
+                           * (256,1) (256,2) (256,3) (128,4) (128,6) (512,1) (512,2) */
 } lbrb_params;
 
 /* Fill *p with defaults (reference values where it has them). */

@@ -57,7 +57,7 @@ class Params(C.Structure):
         ("alpha", C.c_double), ("ntempread", C.c_int), ("nobs", C.c_int),
         ("beta", C.c_double), ("nprtcl", C.c_int), ("noutconfig", C.c_int),
         ("record_full", C.c_int), ("record_slots", C.c_int), ("device", C.c_int),
-        ("autotune", C.c_int),
+        ("autotune", C.c_int), ("launch_shape", C.c_int),
     ]
 
 

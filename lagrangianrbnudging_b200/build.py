@@ -35,8 +35,9 @@ def nvcc() -> str:
 def _stale() -> bool:
     if not LIB.exists() or not HOST.exists():
         return True
-    if (PKG / "host" / "lbrb_host.c").stat().st_mtime > HOST.stat().st_mtime:
-        return True
+    for dep in (PKG / "host" / "lbrb_host.c", ROOT / "include" / "lbrb.h"):
+        if dep.stat().st_mtime > HOST.stat().st_mtime:
+            return True
     t = LIB.stat().st_mtime
     deps = [CSRC / s for s in SOURCES] + [CSRC / "lbrb_internal.cuh", ROOT / "include" / "lbrb.h"]
     return any(d.stat().st_mtime > t for d in deps)

@@ -244,15 +244,30 @@ __global__ void __launch_bounds__(256) stats_partial_kernel(const Real* __restri
   }
 }
 
-__global__ void stats_final_kernel(const double* __restrict__ part, int nblocks,
-                                   double* __restrict__ out) {
-  if (threadIdx.x >= RED_Q) return;
-  KSum b;
-  for (int k = 0; k < nblocks; k++) {
-    b.add(part[(size_t)k * 2 * RED_Q + 2 * threadIdx.x]);
-    b.add(part[(size_t)k * 2 * RED_Q + 2 * threadIdx.x + 1]);
+// one block: every thread folds a strided share of the block partials, then
+// thread 0 folds the per-thread results (all compensated)
+__global__ void __launch_bounds__(256) stats_final_kernel(const double* __restrict__ part,
+                                                          int nblocks, double* __restrict__ out) {
+  __shared__ double sh[RED_Q][2][256];
+  KSum a[RED_Q];
+  for (int k = threadIdx.x; k < nblocks; k += blockDim.x)
+    for (int q = 0; q < RED_Q; q++) {
+      a[q].add(part[(size_t)k * 2 * RED_Q + 2 * q]);
+      a[q].add(part[(size_t)k * 2 * RED_Q + 2 * q + 1]);
+    }
+  for (int q = 0; q < RED_Q; q++) {
+    sh[q][0][threadIdx.x] = a[q].s;
+    sh[q][1][threadIdx.x] = a[q].c;
   }
-  out[threadIdx.x] = b.val();
+  __syncthreads();
+  if (threadIdx.x < RED_Q) {
+    KSum b;
+    for (int t = 0; t < (int)blockDim.x; t++) {
+      b.add(sh[threadIdx.x][0][t]);
+      b.add(sh[threadIdx.x][1][t]);
+    }
+    out[threadIdx.x] = b.val();
+  }
 }
 
 // per-row sums, one block per row
@@ -382,7 +397,7 @@ cudaError_t launch_stats(const void* rho, const void* u, const void* v, const vo
     stats_partial_kernel<double><<<RED_BLOCKS, 256, 0, s>>>((const double*)rho, (const double*)u,
                                                             (const double*)v, (const double*)T, nx,
                                                             ny, pitch, part);
-  stats_final_kernel<<<1, 32, 0, s>>>(part, RED_BLOCKS, out);
+  stats_final_kernel<<<1, 256, 0, s>>>(part, RED_BLOCKS, out);
   return cudaGetLastError();
 }
 

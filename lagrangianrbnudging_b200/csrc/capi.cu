@@ -223,6 +223,7 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
   if (p.nudge == LBRB_NUDGE_REFBOX && p.ntempread < 2) return LBRB_ERR_ARG;
   if (p.nudge == LBRB_NUDGE_REFBOX && p.precision != LBRB_PREC_FP64) return LBRB_ERR_UNSUPPORTED;
   if (p.nprtcl > 0 && p.noutconfig > 0 && p.record_slots < 1) return LBRB_ERR_ARG;
+  if (p.launch_shape < 0 || p.launch_shape > 6) return LBRB_ERR_ARG;
   if ((long)p.nx * p.ny > (1L << 31) - 1) return LBRB_ERR_ARG;
 
   lbrb_t* h = new lbrb_t();
@@ -684,7 +685,7 @@ int lbrb_step(lbrb_t* h, int n) {
   if (h->lb_shape < 0) {
     // autotune the fused kernel's launch shape on this grid (trial launches
     // write only the buffers the real step overwrites)
-    int sh = 0;
+    int sh = h->p.launch_shape;
     float ms = 0.f;
     if (h->p.autotune && !refbox) {
       if (f32) sh = tune_lb_fp32(make_view<float>(h, h->cur, h->cur ^ 1, h->uvcur, 0, 0), h->p.twall, h->stream, &ms);

@@ -21,7 +21,7 @@ def _built():
 
 
 def run_host(program: str, params: dict, wd: Path):
-    args = [str(HOST), program] + [f"{k}={v!r}" if isinstance(v, float) else f"{k}={v}"
+    args = [str(HOST), program] + [f"{k}={float(v)!r}" if isinstance(v, float) else f"{k}={v}"
                                    for k, v in params.items()] + [f"dir={wd}"]
     r = subprocess.run(args, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
