@@ -208,6 +208,23 @@ LBRB_API int lbrb_nusselt(lbrb_t *h, double *nu);
  * tempvel_nudge.c:1104-1260), and the row Nusselt number. */
 LBRB_API int lbrb_profile(lbrb_t *h, double *out);
 
+/* ---- adjoint (no counterpart in the reference) ----------------------------- */
+/* Observations of an assimilation window: nobs_steps window steps
+ * (1-based, increasing), each with nobs observations -- positions x, y in
+ * the reference frame and temperatures T, arrays [nobs_steps][nobs]. */
+LBRB_API int lbrb_adjoint_set_obs(lbrb_t *h, int nobs_steps, const int *steps, int nobs,
+                                  const double *x, const double *y, const double *T);
+/* Run the window from the initial temperature field T0 ([ny][nx]: f =
+ * feq(1,0), g = geq(T0,0), moments by the restart route) for nsteps steps and
+ * return the misfit J = sum over the observations of (T(x,t) - T_obs)^2,
+ * T(x,t) the bilinear interpolation of the step's temperature.  If dJdT0 is
+ * not NULL, also its gradient with respect to T0 ([ny][nx]) by the adjoint
+ * of the time step, recomputing the forward from checkpoints taken every
+ * `checkpoint_every` steps.  Dirichlet walls, no nudging; the handle's state
+ * ends at the end of the window; particles are not advanced. */
+LBRB_API int lbrb_adjoint_window(lbrb_t *h, const double *T0, int nsteps, int checkpoint_every,
+                                 double *J, double *dJdT0);
+
 /* ---- diagnostics without allocation ----------------------------------------
  * No counterpart in the reference.  lbrb_stats_noalloc computes what
  * lbrb_energy() and lbrb_nusselt() give (out3 = mean kinetic energy, mean T,

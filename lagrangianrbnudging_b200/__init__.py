@@ -38,7 +38,7 @@ EXPORTS = [
     "lbrb_record_pending", "lbrb_record_drain", "lbrb_nudge_init", "lbrb_nudge_load",
     "lbrb_nudge_obs", "lbrb_energy", "lbrb_nusselt", "lbrb_profile", "lbrb_set_stream",
     "lbrb_set_timing", "lbrb_get_timing", "lbrb_stats_noalloc", "lbrb_get_launch_shape",
-    "lbrb_get_poststream",
+    "lbrb_get_poststream", "lbrb_adjoint_set_obs", "lbrb_adjoint_window",
 ]
 
 
@@ -104,6 +104,8 @@ def lib() -> C.CDLL:
         "lbrb_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
         "lbrb_get_poststream": (C.c_int, [vp, dp, dp, C.c_int]),
+        "lbrb_adjoint_set_obs": (C.c_int, [vp, C.c_int, ip, C.c_int, dp, dp, dp]),
+        "lbrb_adjoint_window": (C.c_int, [vp, dp, C.c_int, C.c_int, dp, dp]),
         "lbrb_get_launch_shape": (C.c_int, [vp, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_stats_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_double, C.c_double, C.c_double, vp, dp]),
@@ -296,6 +298,21 @@ class Run:
     def nudge_obs(self, first_step: int, x, y, T):
         x, y, T = _f64(np.atleast_2d(x)), _f64(np.atleast_2d(y)), _f64(np.atleast_2d(T))
         self._ck(lib().lbrb_nudge_obs(self.h, int(first_step), x.shape[0], _dp(x), _dp(y), _dp(T)))
+
+    # ---- adjoint
+    def adjoint_set_obs(self, steps, x, y, T):
+        steps = _i32(steps)
+        x, y, T = _f64(np.atleast_2d(x)), _f64(np.atleast_2d(y)), _f64(np.atleast_2d(T))
+        self._ck(lib().lbrb_adjoint_set_obs(self.h, len(steps), _ip(steps), x.shape[1], _dp(x),
+                                            _dp(y), _dp(T)))
+
+    def adjoint_window(self, T0, nsteps: int, checkpoint_every: int, gradient: bool = True):
+        T0 = _f64(T0)
+        J = C.c_double()
+        g = np.empty((self.ny, self.nx)) if gradient else None
+        self._ck(lib().lbrb_adjoint_window(self.h, _dp(T0), int(nsteps), int(checkpoint_every),
+                                           C.byref(J), _dp(g)))
+        return (J.value, g) if gradient else J.value
 
     # ---- streams and timing
     def set_stream(self, stream_handle: int | None):

@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "liblbrb.so"
 HOST = PKG / "lbrb_host"
 SOURCES = ["lb_kernels.cu", "particle_kernels.cu", "nudge_kernels.cu", "aux_kernels.cu", "capi.cu",
-           "noalloc.cu"]
+           "adjoint_kernels.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]

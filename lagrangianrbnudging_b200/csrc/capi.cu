@@ -8,6 +8,7 @@
 //   particle kernel (+ record into the device ring; a copy stream moves each
 //   finished record into pinned host memory while the next steps run)
 // and returns without waiting; lbrb_sync() waits and reports device flags.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <unordered_map>
@@ -58,6 +59,21 @@ cudaError_t launch_profile(const void* rho, const void* u, const void* v, const 
                            int nx, int ny, int pitch, double* out, cudaStream_t s);
 cudaError_t launch_finite(const void* a, size_t n, bool fp32, unsigned* flags, cudaStream_t s);
 int red_blocks();
+cudaError_t launch_adjoint_step(bool fp32, const void* fsrc, const void* gsrc, const void* Fin,
+                                const double* lf_out, const double* lg_out, double* lf_in,
+                                double* lg_in, double* lF, long long* lT, int nx, int ny, int pitch,
+                                size_t plane, double omega, double omegag, double gbeta, double T0,
+                                double Tup, double Tdown, cudaStream_t s);
+cudaError_t launch_adj_obs_scatter(const double* ox, const double* oy, const double* res, int nobs,
+                                   int nx, int ny, int pitch, long long* acc, cudaStream_t s);
+cudaError_t launch_obs_residual(const void* T, bool fp32, int nx, int ny, int pitch, const double* ox,
+                                const double* oy, const double* oT, int nobs, double* res,
+                                cudaStream_t s);
+cudaError_t launch_init_from_T0(const double* T0f, void* pops, void* rho, void* u, void* v, void* T,
+                                void* F, bool fp32, int nx, int ny, int pitch, size_t plane,
+                                double Tref, double neg_gravity, cudaStream_t s);
+cudaError_t launch_adj_initial(const double* lg, const double* lF, int nx, int ny, int pitch,
+                               size_t plane, double gbeta, double* out, cudaStream_t s);
 }  // namespace lbrb
 
 using namespace lbrb;
@@ -197,6 +213,8 @@ static void free_all(lbrb_t* h) {
   F(h->cell_count); F(h->cell_start); F(h->cell_fill); F(h->cell_dirty); F(h->cell_items);
   delete[] h->h_chk; delete[] h->h_oid;
   F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
+  F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
+  delete[] h->adj_steps;
   if (h->h_flags) cudaFreeHost(h->h_flags);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
@@ -628,6 +646,23 @@ static LBView<Real> make_view(lbrb_t* h, int src, int dst, int uvslot, int write
 // particle kernels on a second stream, overlapping the next fused kernel
 static constexpr bool kParticleStream = false;
 
+// view of one step from state buffers (pops: 18 planes, then F) to others;
+// moments written into the handle's rho/T/u/v of buffer 0 when asked
+template <typename Real>
+static LBView<Real> seg_view(lbrb_t* h, const char* src, char* dst, int write_rt) {
+  LBView<Real> V = make_view<Real>(h, 0, 1, h->uvcur, 0, write_rt);
+  const size_t pb = NPOP * h->plane * sizeof(Real);
+  V.fsrc = (const Real*)src;
+  V.gsrc = (const Real*)(src + pb);
+  V.Fin = (const Real*)(src + 2 * pb);
+  V.fdst = (Real*)dst;
+  V.gdst = (Real*)(dst + pb);
+  V.Fout = (Real*)(dst + 2 * pb);
+  V.rho = (Real*)h->rho[0];
+  V.T = (Real*)h->T[0];
+  return V;
+}
+
 static const int SHAPE_BS[] = {256, 256, 256, 128, 128, 512, 512};
 static const int SHAPE_MB[] = {1, 2, 3, 4, 6, 1, 2};
 
@@ -798,6 +833,174 @@ int lbrb_step(lbrb_t* h, int n) {
     CK(h, cudaStreamWaitEvent(h->stream, h->join_ev, 0));
     h->join_pending = false;
   }
+  return LBRB_OK;
+}
+
+int lbrb_adjoint_set_obs(lbrb_t* h, int nobs_steps, const int* steps, int nobs, const double* x,
+                         const double* y, const double* T) {
+  if (!h || nobs_steps < 1 || nobs < 1 || !steps || !x || !y || !T)
+    return fail(h, LBRB_ERR_ARG, "adjoint_set_obs: bad arguments");
+  for (int a = 0; a < nobs_steps; a++)
+    if (steps[a] < 1 || (a > 0 && steps[a] <= steps[a - 1]))
+      return fail(h, LBRB_ERR_ARG, "adjoint_set_obs: steps must be >= 1 and increasing");
+  CK(h, cudaSetDevice(h->dev));
+  if (h->adj_obs) cudaFree(h->adj_obs);
+  if (h->adj_res) cudaFree(h->adj_res);
+  h->adj_obs = nullptr;
+  h->adj_res = nullptr;
+  delete[] h->adj_steps;
+  h->adj_steps = nullptr;
+  const size_t n = (size_t)nobs_steps * nobs;
+  if (cudaMalloc(&h->adj_obs, 3 * n * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->adj_res, n * sizeof(double)) != cudaSuccess)
+    return fail(h, LBRB_ERR_NOMEM, "adjoint_set_obs: allocation");
+  for (int a = 0; a < nobs_steps; a++) {
+    double* b = h->adj_obs + (size_t)a * 3 * nobs;
+    CK(h, cudaMemcpyAsync(b, x + (size_t)a * nobs, nobs * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(b + nobs, y + (size_t)a * nobs, nobs * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(b + 2 * nobs, T + (size_t)a * nobs, nobs * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->adj_steps = new int[nobs_steps];
+  std::memcpy(h->adj_steps, steps, nobs_steps * sizeof(int));
+  h->adj_nobs = nobs;
+  h->adj_nsteps_obs = nobs_steps;
+  return LBRB_OK;
+}
+
+static int grow(lbrb_t* h, void** p, size_t* have, size_t need) {
+  if (*have >= need) return LBRB_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc(p, need);
+  if (e != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "adjoint buffers", e);
+  *have = need;
+  return LBRB_OK;
+}
+
+int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* J, double* dJdT0) {
+  if (!h || !T0 || nsteps < 1 || K < 1 || !J) return fail(h, LBRB_ERR_ARG, "adjoint_window: bad arguments");
+  if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE)
+    return fail(h, LBRB_ERR_UNSUPPORTED, "adjoint_window: Dirichlet walls without nudging only");
+  if (!h->adj_obs) return fail(h, LBRB_ERR_STATE, "adjoint_window: no observations set");
+  CK(h, cudaSetDevice(h->dev));
+  const bool f32 = fp32(h);
+  const int nx = h->p.nx, ny = h->p.ny, pitch = h->pitch;
+  const size_t plane = h->plane, es = h->esize;
+  const size_t sb = (2 * NPOP + 1) * plane * es;  // one state: pops + F
+  const size_t nn = (size_t)nx * ny;
+  if (K > nsteps) K = nsteps;
+  const int nchk = (nsteps + K - 1) / K;
+  int rc;
+  if ((rc = grow(h, &h->adj_chk, &h->adj_chk_bytes, (size_t)nchk * sb))) return rc;
+  if (!h->adj_T0 && cudaMalloc(&h->adj_T0, nn * sizeof(double)) != cudaSuccess)
+    return fail(h, LBRB_ERR_NOMEM, "adjoint T0");
+  CK(h, cudaMemcpyAsync(h->adj_T0, T0, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const double T0ref = T0_of(h), ng = -h->p.gravity;
+  const double om = 1. / h->p.relax, omg = 1. / h->p.relaxg;
+  const int shape = h->lb_shape < 0 ? h->p.launch_shape : h->lb_shape;
+  // observation step lookup
+  std::vector<int> obs_at(nsteps + 1, -1);
+  for (int a = 0; a < h->adj_nsteps_obs; a++)
+    if (h->adj_steps[a] <= nsteps) obs_at[h->adj_steps[a]] = a;
+  const int nob = h->adj_nobs;
+  auto launch_fwd = [&](const char* src, char* dst, int write_rt) -> cudaError_t {
+    if (f32) return launch_lb_fp32(seg_view<float>(h, src, dst, write_rt), h->p.twall, shape, h->stream);
+    return launch_lb_fp64(seg_view<double>(h, src, dst, write_rt), h->p.twall, false, shape, h->stream);
+  };
+  // ---- forward pass: checkpoints, residuals
+  char* chk = (char*)h->adj_chk;
+  // the window's initial state is built in checkpoint 0 (pops + F), moments in buffer 0
+  CK(h, launch_init_from_T0(h->adj_T0, chk, h->rho[0], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
+                            h->T[0], chk + 2 * NPOP * plane * es, f32, nx, ny, pitch, plane, T0ref,
+                            ng, h->stream));
+  // ping-pong through the handle's two population buffers (pops + F contiguous views)
+  std::vector<char> dummy;
+  const size_t pb = 2 * NPOP * plane * es;
+  (void)pb;
+  // state buffers for the forward: use the segment buffer's first two slots
+  if ((rc = grow(h, &h->adj_seg, &h->adj_seg_bytes, (size_t)(K + 1) * sb))) return rc;
+  char* seg = (char*)h->adj_seg;
+  CK(h, cudaMemcpyAsync(seg, chk, sb, cudaMemcpyDeviceToDevice, h->stream));
+  int a_cur = 0;
+  for (int s = 1; s <= nsteps; s++) {
+    if ((s - 1) % K == 0 && s > 1)
+      CK(h, cudaMemcpyAsync(chk + (size_t)((s - 1) / K) * sb, seg + (size_t)a_cur * sb, sb,
+                            cudaMemcpyDeviceToDevice, h->stream));
+    const int oi = obs_at[s];
+    CK(h, launch_fwd(seg + (size_t)a_cur * sb, seg + (size_t)(a_cur ^ 1) * sb, oi >= 0));
+    if (oi >= 0) {
+      const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
+      CK(h, launch_obs_residual(h->T[0], f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob, nob,
+                                h->adj_res + (size_t)oi * nob, h->stream));
+    }
+    a_cur ^= 1;
+  }
+  // misfit (compensated sum on the host)
+  std::vector<double> res((size_t)h->adj_nsteps_obs * nob);
+  CK(h, cudaMemcpyAsync(res.data(), h->adj_res, res.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  {
+    double sum = 0.0, c = 0.0;
+    for (int a = 0; a < h->adj_nsteps_obs; a++) {
+      if (h->adj_steps[a] > nsteps) continue;
+      for (int p = 0; p < nob; p++) {
+        const double r = res[(size_t)a * nob + p];
+        const double y = r * r - c, t = sum + y;
+        c = (t - sum) - y;
+        sum = t;
+      }
+    }
+    *J = sum;
+  }
+  // the handle's state: end of the window
+  {
+    const size_t popb = 2 * NPOP * plane * es;
+    CK(h, cudaMemcpyAsync(h->pops[h->cur], seg + (size_t)a_cur * sb, popb, cudaMemcpyDeviceToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->F[h->cur], seg + (size_t)a_cur * sb + popb, plane * es, cudaMemcpyDeviceToDevice, h->stream));
+    h->prev_valid = false;
+  }
+  if (!dJdT0) {
+    CK(h, cudaStreamSynchronize(h->stream));
+    return LBRB_OK;
+  }
+  // ---- backward pass
+  const size_t lp = NPOP * plane;  // one lambda population set (doubles)
+  if (!h->adj_lam && cudaMalloc((void**)&h->adj_lam, (4 * lp + plane) * sizeof(double)) != cudaSuccess)
+    return fail(h, LBRB_ERR_NOMEM, "adjoint lambda");
+  if (!h->adj_lT && cudaMalloc((void**)&h->adj_lT, plane * sizeof(long long)) != cudaSuccess)
+    return fail(h, LBRB_ERR_NOMEM, "adjoint lambda T");
+  double* lam[2][2] = {{h->adj_lam, h->adj_lam + lp}, {h->adj_lam + 2 * lp, h->adj_lam + 3 * lp}};
+  double* lF = h->adj_lam + 4 * lp;
+  CK(h, cudaMemsetAsync(h->adj_lam, 0, (4 * lp + plane) * sizeof(double), h->stream));
+  CK(h, cudaMemsetAsync(h->adj_lT, 0, plane * sizeof(long long), h->stream));
+  int lc = 0;  // lam[lc] holds the adjoint of the current state
+  for (int c = nchk - 1; c >= 0; c--) {
+    const int s0 = c * K, s1 = std::min(s0 + K, nsteps);
+    // recompute the segment: slot i holds the input state of step s0+1+i
+    CK(h, cudaMemcpyAsync(seg, chk + (size_t)c * sb, sb, cudaMemcpyDeviceToDevice, h->stream));
+    for (int i = 0; i + 1 < s1 - s0; i++)
+      CK(h, launch_fwd(seg + (size_t)i * sb, seg + (size_t)(i + 1) * sb, 0));
+    for (int s = s1; s > s0; s--) {
+      const int i = s - s0 - 1;
+      const char* st = seg + (size_t)i * sb;
+      const int oi = obs_at[s];
+      if (oi >= 0) {
+        const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
+        CK(h, launch_adj_obs_scatter(ob, ob + nob, h->adj_res + (size_t)oi * nob, nob, nx, ny, pitch,
+                                     h->adj_lT, h->stream));
+      }
+      CK(h, launch_adjoint_step(f32, st, st + NPOP * plane * es, st + 2 * NPOP * plane * es,
+                                lam[lc][0], lam[lc][1], lam[lc ^ 1][0], lam[lc ^ 1][1], lF,
+                                oi >= 0 ? h->adj_lT : nullptr, nx, ny, pitch, plane, om, omg, ng,
+                                T0ref, h->p.Tup, h->p.Tdown, h->stream));
+      lc ^= 1;
+    }
+  }
+  CK(h, launch_adj_initial(lam[lc][1], lF, nx, ny, pitch, plane, ng, h->adj_T0, h->stream));
+  CK(h, cudaMemcpyAsync(dJdT0, h->adj_T0, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
   return LBRB_OK;
 }
 

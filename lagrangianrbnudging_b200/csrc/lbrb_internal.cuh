@@ -177,6 +177,18 @@ struct Handle {
   double* obs = nullptr;    // [nsteps][3][nobs]
   int obs_first = 0, obs_nsteps = 0, obs_cap_steps = 0;
   long long* acc = nullptr;
+  // adjoint window
+  double* adj_obs = nullptr;         // [nobs_steps][3][nobs]
+  int adj_nobs = 0, adj_nsteps_obs = 0;
+  int* adj_steps = nullptr;          // host
+  double* adj_res = nullptr;         // residuals [nobs_steps][nobs]
+  void* adj_chk = nullptr;           // checkpoints: 19 planes each (pops + F)
+  size_t adj_chk_bytes = 0;
+  void* adj_seg = nullptr;           // recomputed segment states
+  size_t adj_seg_bytes = 0;
+  double* adj_lam = nullptr;         // 2 x 18 planes + lambda F plane
+  long long* adj_lT = nullptr;       // fixed-point lambda T plane
+  double* adj_T0 = nullptr;          // [ny*nx] initial temperature / gradient
   // scratch / staging
   void* staging = nullptr;
   size_t staging_bytes = 0;

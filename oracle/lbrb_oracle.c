@@ -717,3 +717,113 @@ double orc_nusselt(orc_t *s) {
   double mean = sum / ((double)nx * (double)ny);
   return 1.0 + mean * (double)ny / (kappa * dTw);
 }
+
+/* ------------------------------------------------- tangent-linear model */
+/* Tangent of one step, applied after orc_step() computed the values: the
+ * post-stream values fs, gs, the buoyancy Fy used and the moments are in
+ * the state.  Tangents: tf, tg (post-collision, 9 planes each), tF (the
+ * buoyancy of the next step); updated in place through the scratch tfs/tgs.
+ * Differentiates the shifted-form mathematics of the step (see the CUDA
+ * adjoint for the formulas); the pull moves tangents like values, and the
+ * anti-bounce-back drops its constant. */
+static void tlm_step(orc_t *s, double *tf, double *tg, double *tF, double *tfs, double *tgs,
+                     double *tT) {
+  const int nx = s->p.nx, ny = s->p.ny;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+      for (int k = 0; k < NPOP; k++) {
+        int js = j - ICY[k], is = wrap(i - ICX[k], nx);
+        tfs[pidx(s, k, i, j)] = (js < 0 || js >= ny) ? tf[pidx(s, OPP[k], i, j)] : tf[pidx(s, k, is, js)];
+        tgs[pidx(s, k, i, j)] = (js < 0 || js >= ny) ? 0.0 : tg[pidx(s, k, is, js)];
+      }
+  for (int i = 0; i < nx; i++) {
+    int j = ny - 1;
+    tgs[pidx(s, 4, i, j)] = -tgs[pidx(s, 2, i, j)];
+    tgs[pidx(s, 7, i, j)] = -tgs[pidx(s, 5, i, j)];
+    tgs[pidx(s, 8, i, j)] = -tgs[pidx(s, 6, i, j)];
+    j = 0;
+    tgs[pidx(s, 2, i, j)] = -tgs[pidx(s, 4, i, j)];
+    tgs[pidx(s, 5, i, j)] = -tgs[pidx(s, 7, i, j)];
+    tgs[pidx(s, 6, i, j)] = -tgs[pidx(s, 8, i, j)];
+  }
+  const double om = 1. / s->p.relax, omg = 1. / s->p.relaxg, srcf = 1.0 - 0.5 * om;
+  const double gb = -s->p.gravity;
+  const double *rho = s->fld[ORC_RHO], *u = s->fld[ORC_U], *v = s->fld[ORC_V], *T = s->fld[ORC_T];
+  const double *Fy = s->fld[ORC_FY];
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      size_t q = sidx(s, i, j);
+      double r = rho[q], uu = u[q], vv = v[q], t = T[q], F = Fy[q];
+      double rd = 0, jxd = 0, jyd = 0, td = 0;
+      for (int k = 0; k < NPOP; k++) {
+        double a = tfs[pidx(s, k, i, j)];
+        rd += a;
+        jxd += ICX[k] * a;
+        jyd += ICY[k] * a;
+        td += tgs[pidx(s, k, i, j)];
+      }
+      double Fd = tF[q];
+      double ud = (jxd - uu * rd) / r, vd = (jyd + 0.5 * Fd - vv * rd) / r;
+      for (int k = 0; k < NPOP; k++) {
+        double w = WW[k], cx = ICX[k], cy = ICY[k];
+        double cu = cx * uu + cy * vv, cud = cx * ud + cy * vd;
+        double P = 3.0 * cu + 4.5 * cu * cu - 1.5 * (uu * uu + vv * vv);
+        double Pd = (3.0 + 9.0 * cu) * cud - 3.0 * (uu * ud + vv * vd);
+        double feqd = w * (rd + rd * P + r * Pd);
+        double Sd = srcf * w * (Fd * (3.0 * (cy - vv) + 9.0 * cu * cy) + F * (-3.0 * vd + 9.0 * cud * cy));
+        tf[pidx(s, k, i, j)] = (1.0 - om) * tfs[pidx(s, k, i, j)] + om * feqd + Sd;
+        double geqd = w * (td + td * P + t * Pd);
+        tg[pidx(s, k, i, j)] = (1.0 - omg) * tgs[pidx(s, k, i, j)] + omg * geqd;
+      }
+      tF[q] = gb * (rd * t + r * td);
+      tT[q] = td;
+    }
+}
+
+void orc_tlm_window(orc_t *s, const double *T0, const double *dT0, int nsteps, int nobs_steps,
+                    const int *steps, int nobs, const double *ox, const double *oy,
+                    const double *oT, double *J, double *dJ) {
+  const int nx = s->p.nx, ny = s->p.ny;
+  const size_t n = (size_t)nx * ny;
+  double *f = s->fld[ORC_F], *g = s->fld[ORC_G];
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      double feq[NPOP], geq[NPOP];
+      equil(1.0, 0.0, 0.0, feq);
+      equil(T0[sidx(s, i, j)], 0.0, 0.0, geq);
+      for (int k = 0; k < NPOP; k++) {
+        f[pidx(s, k, i, j)] = feq[k];
+        g[pidx(s, k, i, j)] = geq[k];
+      }
+    }
+  orc_moments_from_pre(s, f, g);
+  double *tf = (double *)calloc(NPOP * n, sizeof(double)), *tg = (double *)calloc(NPOP * n, sizeof(double));
+  double *tfs = (double *)calloc(NPOP * n, sizeof(double)), *tgs = (double *)calloc(NPOP * n, sizeof(double));
+  double *tF = (double *)calloc(n, sizeof(double)), *tT = (double *)calloc(n, sizeof(double));
+  double sw = 0.0;
+  for (int k = 0; k < NPOP; k++) sw += WW[k];
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      size_t q = sidx(s, i, j);
+      for (int k = 0; k < NPOP; k++) tg[pidx(s, k, i, j)] = WW[k] * dT0[q];
+      tF[q] = -s->p.gravity * s->fld[ORC_RHO][q] * sw * dT0[q];
+    }
+  double Js = 0.0, dJs = 0.0;
+  int a = 0;
+  for (int st = 1; st <= nsteps; st++) {
+    orc_step(s, st);
+    tlm_step(s, tf, tg, tF, tfs, tgs, tT);
+    while (a < nobs_steps && steps[a] < st) a++;
+    if (a < nobs_steps && steps[a] == st) {
+      for (int p = 0; p < nobs; p++) {
+        size_t o = (size_t)a * nobs + p;
+        double r = bilinear(s, s->fld[ORC_T], ox[o], oy[o]) - oT[o];
+        Js += r * r;
+        dJs += 2.0 * r * bilinear(s, tT, ox[o], oy[o]);
+      }
+    }
+  }
+  *J = Js;
+  *dJ = dJs;
+  free(tf); free(tg); free(tfs); free(tgs); free(tF); free(tT);
+}

@@ -100,6 +100,17 @@ void orc_energy(orc_t *s, double *ke_mean, double *t_mean);
 void orc_profile(orc_t *s, double *out);
 double orc_nusselt(orc_t *s);
 
+/* FP64 tangent-linear model of an assimilation window (no counterpart in the
+ * reference): from the initial temperature T0 ([ny][nx]; f = feq(1,0),
+ * g = geq(T0,0), moments by the restart route) and a direction dT0, run
+ * nsteps reference steps (Dirichlet walls, no particles, no nudging) and
+ * return the misfit J = sum over observations of (T(x,t) - T_obs)^2 and its
+ * directional derivative dJ = <grad J, dT0>.  Observations: nobs_steps steps
+ * (1-based, increasing), nobs each, arrays [nobs_steps][nobs]. */
+void orc_tlm_window(orc_t *s, const double *T0, const double *dT0, int nsteps, int nobs_steps,
+                    const int *steps, int nobs, const double *ox, const double *oy,
+                    const double *oT, double *J, double *dJ);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,8 @@ def lib():
         L.orc_profile.argtypes = [C.c_void_p, dp]
         L.orc_nusselt.restype = C.c_double
         L.orc_nusselt.argtypes = [C.c_void_p]
+        L.orc_tlm_window.argtypes = [C.c_void_p, dp, dp, C.c_int, C.c_int, ip, C.c_int, dp, dp,
+                                     dp, dp, dp]
         _lib = L
     return _lib
 
@@ -190,6 +192,16 @@ class Oracle:
 
     def nusselt(self) -> float:
         return lib().orc_nusselt(self._h)
+
+    def tlm_window(self, T0, dT0, nsteps, steps, ox, oy, oT):
+        """misfit J and its directional derivative along dT0 (FP64 tangent-linear model)"""
+        T0, dT0 = np.ascontiguousarray(T0, np.float64), np.ascontiguousarray(dT0, np.float64)
+        steps = np.ascontiguousarray(steps, np.int32)
+        ox, oy, oT = (np.ascontiguousarray(np.atleast_2d(a), np.float64) for a in (ox, oy, oT))
+        J, dJ = C.c_double(), C.c_double()
+        lib().orc_tlm_window(self._h, _dp(T0), _dp(dT0), int(nsteps), len(steps), _ip(steps),
+                             ox.shape[1], _dp(ox), _dp(oy), _dp(oT), C.byref(J), C.byref(dJ))
+        return J.value, dJ.value
 
 
 def splitmix_uniform(seed: int, index: int) -> float:

@@ -192,3 +192,44 @@ def golden_path(name: str) -> Path:
 def load_golden(name: str) -> dict:
     z = np.load(golden_path(name), allow_pickle=False)
     return {k: z[k] for k in z.files}
+
+
+def adjoint_case(seed: int, nx: int = 48, ny: int = 24, nsteps: int = 40, every: int = 4,
+                 nobs: int = 30) -> dict:
+    """Assimilation window: observations of a truth run (seeded conduction
+    state with its own noise) at fixed random positions every `every` steps;
+    the window starts from another seeded state."""
+    base = closure(nx, ny, Ra=1e5, Pr=1.0, U=0.1)
+    params = dict(base, twall="dirichlet", nudge="none")
+    rng = np.random.default_rng(seed)
+    j = np.arange(ny)
+    Tcol = base["Tdown"] + (base["Tup"] - base["Tdown"]) * ((j + 0.5) / ny)
+    T_truth = Tcol[:, None] + 2e-2 * rng.uniform(-1, 1, (ny, nx))
+    T0 = Tcol[:, None] + 2e-2 * rng.uniform(-1, 1, (ny, nx))
+    steps = np.arange(every, nsteps + 1, every, dtype=np.int32)
+    ox = rng.uniform(0.5, nx - 0.5, (len(steps), nobs))
+    oy = rng.uniform(1.0, ny, (len(steps), nobs))
+    oT = truth_obs(params, T_truth, nsteps, steps, ox, oy)
+    return dict(params=params, base=base, nx=nx, ny=ny, nsteps=nsteps, steps=steps, ox=ox, oy=oy,
+                oT=oT, T0=T0, T_truth=T_truth)
+
+
+def truth_obs(params: dict, T_truth: np.ndarray, nsteps: int, steps, ox, oy) -> np.ndarray:
+    """temperatures of the truth run at the observation points"""
+    nx, ny = int(params["nx"]), int(params["ny"])
+    o = Oracle(params, 0)
+    f = W[:, None, None] * np.ones((1, ny, nx))
+    g = np.empty((9, ny, nx))
+    for k in range(9):
+        g[k] = T_truth * W[k]
+    o.f[:] = f
+    o.g[:] = g
+    o.moments_from_pre(o.f.copy(), o.g.copy())
+    out = np.zeros((len(steps), ox.shape[1]))
+    a = 0
+    for s in range(1, nsteps + 1):
+        o.step(s)
+        if a < len(steps) and steps[a] == s:
+            out[a] = [bilinear_np(o.T, x, y) for x, y in zip(ox[a], oy[a])]
+            a += 1
+    return out

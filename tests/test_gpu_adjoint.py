@@ -1,0 +1,72 @@
+"""The CUDA adjoint of the time step (lbrb_adjoint_window) against the FP64
+tangent-linear model of the oracle, against central finite differences of the
+GPU's own FP64 forward, and across checkpoint intervals and precisions."""
+import numpy as np
+import pytest
+
+import lagrangianrbnudging_b200 as lb
+from lagrangianrbnudging_b200 import build
+from oracle.oracle import Oracle
+from tests.golden.cases import adjoint_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    build.build()
+    return adjoint_case(seed=3)
+
+
+def gpu_window(c, precision, K, gradient=True, T0=None):
+    with lb.Run(**c["base"], precision=precision) as r:
+        r.adjoint_set_obs(c["steps"], c["ox"], c["oy"], c["oT"])
+        return r.adjoint_window(c["T0"] if T0 is None else T0, c["nsteps"], K, gradient=gradient)
+
+
+def test_fp64_adjoint_matches_tangent_linear_model(case):
+    c = case
+    J, grad = gpu_window(c, "fp64", K=8)
+    o = Oracle(c["params"], 0)
+    rng = np.random.default_rng(23)
+    for _ in range(3):
+        d = rng.standard_normal(c["T0"].shape)
+        Jt, dJ = o.tlm_window(c["T0"], d, c["nsteps"], c["steps"], c["ox"], c["oy"], c["oT"])
+        assert abs(J - Jt) <= 1e-12 * Jt
+        # <grad J, d> from the adjoint against the tangent-linear derivative
+        assert abs(np.sum(grad * d) - dJ) <= 1e-9 * abs(dJ), (np.sum(grad * d), dJ)
+
+
+def test_fp64_adjoint_matches_gpu_finite_differences(case):
+    """central differences h = 1e-6 of the FP64 GPU forward (64x fewer
+    directions than the configuration's 64, same tolerance 1e-4)"""
+    c = case
+    _, grad = gpu_window(c, "fp64", K=8)
+    rng = np.random.default_rng(29)
+    h = 1e-6
+    for _ in range(2):
+        d = rng.standard_normal(c["T0"].shape)
+        Jp = gpu_window(c, "fp64", K=8, gradient=False, T0=c["T0"] + h * d)
+        Jm = gpu_window(c, "fp64", K=8, gradient=False, T0=c["T0"] - h * d)
+        fd = (Jp - Jm) / (2 * h)
+        ad = np.sum(grad * d)
+        assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(case):
+    c = case
+    g1 = gpu_window(c, "fp64", K=1)[1]
+    g7 = gpu_window(c, "fp64", K=7)[1]
+    gall = gpu_window(c, "fp64", K=c["nsteps"])[1]
+    np.testing.assert_array_equal(g1, g7)
+    np.testing.assert_array_equal(g1, gall)
+
+
+def test_fp32_forward_adjoint_close_to_fp64(case):
+    """FP32 shifted forward with FP64 adjoint accumulation: gradient within
+    1e-3 (relative L2) of the FP64 one"""
+    c = case
+    J64, g64 = gpu_window(c, "fp64", K=8)
+    J32, g32 = gpu_window(c, "fp32", K=8)
+    assert abs(J32 - J64) <= 1e-4 * J64
+    assert np.linalg.norm(g32 - g64) <= 1e-3 * np.linalg.norm(g64)
