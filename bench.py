@@ -369,6 +369,8 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
         "clocks": clocks,
         "records": len(recs),
     })
+    if world == 1 and not args.no_adjoint:
+        out["adjoint"] = run_adjoint_bench(lb, torch, device)
     if e2e_ms is not None:
         out["e2e"] = {"value": round(world * nodes * K / (e2e_ms * 1e3), 1), "unit": "MLUPS",
                       "h2d_bytes_per_step": int(e2e_h2d / K), "d2h_bytes_per_step": int(e2e_d2h / K),
@@ -378,6 +380,102 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
+
+
+# ------------------------------------------------------------- adjoint
+ADJ_NX, ADJ_NY, ADJ_STEPS, ADJ_K, ADJ_EVERY, ADJ_NOBS = 1024, 512, 2000, 100, 10, 4096
+
+
+def adjoint_problem(lb, device: int, seed: int = 31):
+    """Assimilation window of the adjoint configuration: 1024x512, Ra=1e6,
+    Pr=1, U=0.1; observations = T along 4096 tracer trajectories of a seeded
+    truth run, every 10 steps over 2000 steps; the window starts from an
+    initial state with other noise."""
+    base = lb.closure(ADJ_NX, ADJ_NY, Ra=1e6, Pr=1.0, U=0.1)
+    nrec = ADJ_STEPS // ADJ_EVERY
+    with lb.Run(**base, precision="fp64", nprtcl=ADJ_NOBS, noutconfig=ADJ_EVERY, record_slots=nrec + 1,
+                device=device) as r:
+        r.init_conduction(seed, 1e-2)
+        m = r.get_moments()
+        rng = np.random.default_rng(seed)
+        x = rng.uniform(0.5, ADJ_NX - 0.5, ADJ_NOBS)
+        y = rng.uniform(1.0, ADJ_NY, ADJ_NOBS)
+        r.set_particles(np.arange(ADJ_NOBS, dtype=np.int32), x, y, bilinear_np(m["u"], x, y),
+                        bilinear_np(m["v"], x, y), np.zeros(ADJ_NOBS, np.int32), np.zeros(ADJ_NOBS))
+        r.step(ADJ_STEPS)
+        recs = r.drain_records()
+    steps = np.array(sorted(recs), np.int32)
+    ox = np.stack([recs[s]["x"] for s in steps])
+    oy = np.stack([recs[s]["y"] for s in steps])
+    oT = np.stack([recs[s]["temp"] for s in steps])
+    rng = np.random.default_rng(seed + 1)
+    j = np.arange(ADJ_NY)
+    T0 = (base["Tdown"] + (base["Tup"] - base["Tdown"]) * ((j + 0.5) / ADJ_NY))[:, None] \
+        + 1e-2 * rng.uniform(-1, 1, (ADJ_NY, ADJ_NX))
+    return base, steps, ox, oy, oT, T0
+
+
+def run_adjoint_bench(lb, torch, device: int) -> dict:
+    base, steps, ox, oy, oT, T0 = adjoint_problem(lb, device)
+    out = {}
+    for prec in ("fp32",):
+        with lb.Run(**base, precision=prec, device=device) as w:
+            w.adjoint_set_obs(steps, ox, oy, oT)
+            stream = torch.cuda.Stream()
+            w.set_stream(stream.cuda_stream)
+            w.adjoint_window(T0, 20, 10)  # warm-up (allocations, autotune)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+            ev[0].record(stream)
+            Jf = w.adjoint_window(T0, ADJ_STEPS, ADJ_K, gradient=False)
+            ev[1].record(stream)
+            ev[2].record(stream)
+            J, grad = w.adjoint_window(T0, ADJ_STEPS, ADJ_K, gradient=True)
+            ev[3].record(stream)
+            # plain forward steps of the same grid, for the cost ratio
+            w.init_conduction(1, 1e-3)
+            w.step(10)
+            ev[4].record(stream)
+            w.step(ADJ_STEPS)
+            ev[5].record(stream)
+            torch.cuda.synchronize()
+            t_fwd_window = ev[0].elapsed_time(ev[1])
+            t_adj = ev[2].elapsed_time(ev[3])
+            t_step = ev[4].elapsed_time(ev[5]) / ADJ_STEPS
+            w.set_stream(None)
+        out = {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": ADJ_STEPS, "checkpoint_every": ADJ_K,
+               "observations": f"{ADJ_NOBS} tracers every {ADJ_EVERY} steps (seeded truth run)",
+               "precision": "fp32 forward, fp64 adjoint", "J": J,
+               "grad_norm": float(np.linalg.norm(grad)),
+               "adjoint_steps_per_s": round(ADJ_STEPS / (t_adj * 1e-3), 1),
+               "ms_gradient_window": round(t_adj, 2), "ms_misfit_window": round(t_fwd_window, 2),
+               "ms_forward_step": round(t_step, 5),
+               "cost_vs_forward_steps": round(t_adj / (ADJ_STEPS * t_step), 2)}
+    return out
+
+
+def run_adjoint_check(lb, torch, device: int, ndir: int = 64, h: float = 1e-6) -> dict:
+    """gradient of the FP64 forward against central differences (h = 1e-6) on
+    seeded random directions, and the FP32-forward gradient against the FP64 one"""
+    base, steps, ox, oy, oT, T0 = adjoint_problem(lb, device)
+    with lb.Run(**base, precision="fp64", device=device) as w:
+        w.adjoint_set_obs(steps, ox, oy, oT)
+        J, g64 = w.adjoint_window(T0, ADJ_STEPS, ADJ_K)
+        rng = np.random.default_rng(2024)
+        errs = []
+        for _ in range(ndir):
+            d = rng.standard_normal(T0.shape)
+            Jp = w.adjoint_window(T0 + h * d, ADJ_STEPS, ADJ_K, gradient=False)
+            Jm = w.adjoint_window(T0 - h * d, ADJ_STEPS, ADJ_K, gradient=False)
+            fd = (Jp - Jm) / (2 * h)
+            ad = float(np.sum(g64 * d))
+            errs.append(abs(fd - ad) / abs(ad))
+    with lb.Run(**base, precision="fp32", device=device) as w:
+        w.adjoint_set_obs(steps, ox, oy, oT)
+        J32, g32 = w.adjoint_window(T0, ADJ_STEPS, ADJ_K)
+    return {"mode": "adjoint-check", "grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": ADJ_STEPS,
+            "directions": ndir, "h": h, "J_fp64": J, "J_fp32": J32,
+            "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)),
+            "fp32_grad_rel_l2_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))}
 
 
 # ---------------------------------------------------------- reference arm
@@ -544,6 +642,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-check", action="store_true",
+                    help="FD check of the adjoint gradient at the adjoint configuration")
     ap.add_argument("--lb-only", action="store_true",
                     help="fused kernel alone on --grid (the ncu capture command)")
     ap.add_argument("--grid", default="2048x1024")
@@ -565,6 +666,14 @@ def main():
     if args.lb_only:
         torch.cuda.set_device(0)
         print(json.dumps(run_lb_only(args, torch)), flush=True)
+        return
+    if args.adjoint_check:
+        import lagrangianrbnudging_b200 as lb
+        from lagrangianrbnudging_b200 import build as b
+
+        b.build()
+        torch.cuda.set_device(0)
+        print(json.dumps(run_adjoint_check(lb, torch, 0)), flush=True)
         return
     dist = None
     if world > 1:
