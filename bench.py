@@ -347,7 +347,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
                    "precision": "fp32-shifted populations, fp64 particles",
                    "l2": "state 1.5 GB > 126 MB L2 on every step (no flush needed)",
                    "parallelism": f"{world} independent instances (replicas), no collective"},
-        "roofline": {"bound": "hbm", "kernel": "lb_step_kernel<float>",
+        "roofline": {"bound": "hbm", "kernel": "lb_node_kernel<float>",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "alg_bytes_per_node": ALG_BYTES["fp32"],
@@ -371,6 +371,8 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     })
     if world == 1 and not args.no_adjoint:
         out["adjoint"] = run_adjoint_bench(lb, torch, device)
+    if world == 1 and not args.no_ensemble:
+        out["ensemble"] = run_ensemble_bench(lb, torch, device, args.ensemble_steps)
     if e2e_ms is not None:
         out["e2e"] = {"value": round(world * nodes * K / (e2e_ms * 1e3), 1), "unit": "MLUPS",
                       "h2d_bytes_per_step": int(e2e_h2d / K), "d2h_bytes_per_step": int(e2e_d2h / K),
@@ -476,6 +478,101 @@ def run_adjoint_check(lb, torch, device: int, ndir: int = 64, h: float = 1e-6) -
             "directions": ndir, "h": h, "J_fp64": J, "J_fp32": J32,
             "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)),
             "fp32_grad_rel_l2_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))}
+
+
+# ------------------------------------------------------------- ensemble
+ENS_N, ENS_STEPS, ENS_TRACERS, ENS_OBS_ROWS = 64, 10000, 1024, 100
+
+
+def ensemble_members(lb, device: int, seed: int = 41):
+    """The uneven ensemble: 64 members with Nx x Ny drawn from {256x128,
+    512x256, 1024x512} and Ra log-uniform in [1e5, 1e7] (Pr=1, U=0.1), each
+    with 1024 tracers and a nudging alpha drawn from {0, 0.1}; FP32-shifted
+    populations.  Nudged members relax T toward synthetic observations at
+    1024 seeded positions (a repeating series of 100 rows; T = conduction
+    profile + 0.01 seeded noise)."""
+    rng = np.random.default_rng(seed)
+    sizes = [(256, 128), (512, 256), (1024, 512)]
+    members, desc = [], []
+    for i in range(ENS_N):
+        nx, ny = sizes[int(rng.integers(3))]
+        Ra = float(10 ** rng.uniform(5, 7))
+        alpha = [0.0, 0.1][int(rng.integers(2))]
+        kw = dict(**lb.closure(nx, ny, Ra=Ra, Pr=1.0, U=0.1), precision="fp32", nprtcl=ENS_TRACERS,
+                  device=device)
+        if alpha:
+            kw.update(nudge="bilinear", alpha=alpha, nobs=ENS_TRACERS, obs_cycle=1)
+        r = lb.Run(**kw)
+        r.init_conduction(seed * 1000 + i, 1e-3)
+        x = rng.uniform(0.5, nx + 0.5, ENS_TRACERS)
+        y = rng.uniform(1.0, ny, ENS_TRACERS)
+        z = np.zeros(ENS_TRACERS)
+        r.set_particles(np.arange(ENS_TRACERS, dtype=np.int32), x, y, z, z,
+                        np.zeros(ENS_TRACERS, np.int32), z)
+        if alpha:
+            ox = rng.uniform(0.5, nx + 0.5, (ENS_OBS_ROWS, ENS_TRACERS))
+            oy = rng.uniform(1.0, ny, (ENS_OBS_ROWS, ENS_TRACERS))
+            oT = 0.5 - (oy - 0.5) / ny + 0.01 * rng.standard_normal(oy.shape)
+            r.nudge_obs(1, ox, oy, oT)
+        members.append(r)
+        desc.append((nx, ny, Ra, alpha))
+    return members, desc
+
+
+def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS) -> dict:
+    members, desc = ensemble_members(lb, device)
+    nodes = sum(nx * ny for nx, ny, _, _ in desc)
+    out = {}
+    with lb.Ensemble(members) as ens:
+        stream = torch.cuda.Stream()
+        ens.set_stream(stream.cuda_stream)
+        ens.step(12)  # autotune + graph capture + warm-up
+        ens.sync()
+        sched = ens.schedule()
+        # per-launch timing of the phases (direct launches, no graph)
+        ens.set_timing(True)
+        ens.step(60)
+        t = ens.get_timing()
+        ens.set_timing(False)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ens.sync()
+        ens.set_stream(None)
+    def is_finite(r):
+        try:
+            r.check_finite()
+            return True
+        except lb.LbrbError:
+            return False
+
+    finite = all(is_finite(r) for r in members)
+    nus = [r.nusselt() for r in members]
+    for r in members:
+        r.close()
+    peak, _ = measured_peak()
+    lb_ms = t["lb_step"][0] / max(t["lb_step"][1], 1)
+    agg = nodes * ALG_BYTES["fp32"] * steps / (ms * 1e-3) / 1e9
+    lb_gbs = nodes * ALG_BYTES["fp32"] / (lb_ms * 1e-3) / 1e9
+    nudged = sum(1 for d in desc if d[3] > 0)
+    out = {"members": ENS_N, "nodes": nodes, "steps": steps, "ms": round(ms, 2),
+           "mlups": round(nodes * steps / (ms * 1e3), 1),
+           "aggregate_gbs": round(agg, 1), "aggregate_frac": round(agg / peak, 4),
+           "lb_phase_ms": round(lb_ms, 5), "lb_phase_gbs": round(lb_gbs, 1),
+           "lb_phase_frac": round(lb_gbs / peak, 4),
+           "phase_share": {k: round(v[0] / sum(x[0] for x in t.values()), 4) for k, v in t.items()},
+           "launches_per_step": 3, "schedule": sched, "finite": bool(finite),
+           "nu_range": [round(min(nus), 3), round(max(nus), 3)],
+           "config": f"{ENS_N} members from {{256x128, 512x256, 1024x512}}, Ra log-uniform "
+                     f"[1e5,1e7], Pr=1, U=0.1, {ENS_TRACERS} tracers each, alpha in {{0,0.1}} "
+                     f"({nudged} nudged), fp32-shifted; {steps} steps in CUDA-graph replays",
+           "alg_bytes": "sum of nodes x 144 B per step"}
+    return out
 
 
 # ---------------------------------------------------------- reference arm
@@ -614,7 +711,7 @@ def run_reference_arm(args) -> dict:
 
 def run_lb_only(args, torch) -> dict:
     """The fused stream/collide kernel alone on a grid of --grid (no
-    particles): the command used for ncu captures of lb_step_kernel."""
+    particles): the command used for ncu captures of lb_node_kernel."""
     import lagrangianrbnudging_b200 as lb
     from lagrangianrbnudging_b200 import build as b
 
@@ -643,6 +740,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-steps", type=int, default=ENS_STEPS)
     ap.add_argument("--adjoint-check", action="store_true",
                     help="FD check of the adjoint gradient at the adjoint configuration")
     ap.add_argument("--lb-only", action="store_true",

@@ -99,6 +99,9 @@ typedef struct {
   int launch_shape;       /* with autotune 0: the shape used, an index into
                            * (threads per block, min blocks per SM) =
                            * (256,1) (256,2) (256,3) (128,4) (128,6) (512,1) (512,2) */
+  int obs_cycle;          /* bilinear nudging: 1 = the series given to lbrb_nudge_obs repeats
+                           * (step s uses row (s - first_step) mod nsteps); 0 = a step
+                           * outside the series is an error (LBRB_ERR_STATE) */
 } lbrb_params;
 
 /* Fill *p with defaults (reference values where it has them). */
@@ -224,6 +227,41 @@ LBRB_API int lbrb_adjoint_set_obs(lbrb_t *h, int nobs_steps, const int *steps, i
  * ends at the end of the window; particles are not advanced. */
 LBRB_API int lbrb_adjoint_window(lbrb_t *h, const double *T0, int nsteps, int checkpoint_every,
                                  double *J, double *dJdT0);
+
+/* ---- ensemble (no counterpart in the reference) ---------------------------
+ * Independent runs ("members": handles made by lbrb_create, of any grid size
+ * and closure) advanced together.  Per time step one launch covers the fused
+ * stream/collide step of every member (a persistent kernel over a work list
+ * of equal tiles), one advances every member's particles and scatters its
+ * bilinear observations, and one applies the nudging of all members; the
+ * steps are replayed from a CUDA graph.  A member's state stays in its
+ * handle: every per-handle call (get_moments, particles_get, energy, ...)
+ * works between ensemble steps, and a member advanced by the ensemble ends
+ * bit-identical to the same handle advanced by lbrb_step.
+ * Members: one device, one precision, one wall mode, nudging none or
+ * bilinear, no trajectory records (noutconfig 0 when nprtcl > 0).  The
+ * ensemble borrows the handles: destroy it before them. */
+typedef struct lbrb_ensemble_s lbrb_ensemble_t;
+LBRB_API int lbrb_ensemble_create(lbrb_t *const *members, int n, lbrb_ensemble_t **out);
+LBRB_API int lbrb_ensemble_destroy(lbrb_ensemble_t *e);
+LBRB_API const char *lbrb_ensemble_last_error(const lbrb_ensemble_t *e);
+/* Advance every member by n steps (queued, like lbrb_step). */
+LBRB_API int lbrb_ensemble_step(lbrb_ensemble_t *e, int n);
+/* Wait; return the first member status that is not LBRB_OK. */
+LBRB_API int lbrb_ensemble_sync(lbrb_ensemble_t *e);
+LBRB_API int lbrb_ensemble_set_stream(lbrb_ensemble_t *e, void *cuda_stream);
+/* Launch variant of the fused phase (threads per tile row, rows per tile,
+ * schedule: 0 one block per tile, 1 persistent grid stride, 2 persistent
+ * atomic tile counter).  -1 (the default): the autotuner times every variant
+ * on the members' state at the next step and keeps the fastest. */
+LBRB_API int lbrb_ensemble_nvariants(void);
+LBRB_API int lbrb_ensemble_set_schedule(lbrb_ensemble_t *e, int variant);
+LBRB_API int lbrb_ensemble_get_schedule(const lbrb_ensemble_t *e, int *variant, int *block,
+                                        int *rows, int *schedule, float *ms);
+/* Per-launch device timing (steps then launch directly, without the graph).
+ * Classes: 0 fused step, 1 particles + innovation scatter, 2 nudging apply. */
+LBRB_API int lbrb_ensemble_set_timing(lbrb_ensemble_t *e, int enable);
+LBRB_API int lbrb_ensemble_get_timing(lbrb_ensemble_t *e, double *ms, int *launches, int n);
 
 /* ---- diagnostics without allocation ----------------------------------------
  * No counterpart in the reference.  lbrb_stats_noalloc computes what

@@ -39,6 +39,10 @@ EXPORTS = [
     "lbrb_nudge_obs", "lbrb_energy", "lbrb_nusselt", "lbrb_profile", "lbrb_set_stream",
     "lbrb_set_timing", "lbrb_get_timing", "lbrb_stats_noalloc", "lbrb_get_launch_shape",
     "lbrb_get_poststream", "lbrb_adjoint_set_obs", "lbrb_adjoint_window",
+    "lbrb_ensemble_create", "lbrb_ensemble_destroy", "lbrb_ensemble_last_error",
+    "lbrb_ensemble_step", "lbrb_ensemble_sync", "lbrb_ensemble_set_stream",
+    "lbrb_ensemble_nvariants", "lbrb_ensemble_set_schedule", "lbrb_ensemble_get_schedule",
+    "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
 ]
 
 
@@ -57,7 +61,7 @@ class Params(C.Structure):
         ("alpha", C.c_double), ("ntempread", C.c_int), ("nobs", C.c_int),
         ("beta", C.c_double), ("nprtcl", C.c_int), ("noutconfig", C.c_int),
         ("record_full", C.c_int), ("record_slots", C.c_int), ("device", C.c_int),
-        ("autotune", C.c_int), ("launch_shape", C.c_int),
+        ("autotune", C.c_int), ("launch_shape", C.c_int), ("obs_cycle", C.c_int),
     ]
 
 
@@ -109,6 +113,17 @@ def lib() -> C.CDLL:
         "lbrb_get_launch_shape": (C.c_int, [vp, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_stats_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_double, C.c_double, C.c_double, vp, dp]),
+        "lbrb_ensemble_create": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(vp)]),
+        "lbrb_ensemble_destroy": (C.c_int, [vp]),
+        "lbrb_ensemble_last_error": (C.c_char_p, [vp]),
+        "lbrb_ensemble_step": (C.c_int, [vp, C.c_int]),
+        "lbrb_ensemble_sync": (C.c_int, [vp]),
+        "lbrb_ensemble_set_stream": (C.c_int, [vp, vp]),
+        "lbrb_ensemble_nvariants": (C.c_int, []),
+        "lbrb_ensemble_set_schedule": (C.c_int, [vp, C.c_int]),
+        "lbrb_ensemble_get_schedule": (C.c_int, [vp, ip, ip, ip, ip, C.POINTER(C.c_float)]),
+        "lbrb_ensemble_set_timing": (C.c_int, [vp, C.c_int]),
+        "lbrb_ensemble_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -348,6 +363,79 @@ class Run:
         out = np.empty((self.ny, 9))
         self._ck(lib().lbrb_profile(self.h, _dp(out)))
         return out
+
+
+class Ensemble:
+    """Independent runs advanced together (lbrb_ensemble_*): one launch per
+    phase of the step covers every member, replayed from a CUDA graph.  The
+    members are Run objects; their state stays theirs, so every Run method
+    works between ensemble steps.  Close the ensemble before its members."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.h for m in self.members])
+        e = C.c_void_p()
+        rc = lib().lbrb_ensemble_create(arr, len(self.members), C.byref(e))
+        if rc != OK:
+            raise LbrbError(rc, "lbrb_ensemble_create: members must share device, precision and "
+                                "wall mode; no box nudging; no trajectory records")
+        self.e = e
+
+    def _ck(self, rc: int):
+        if rc != OK:
+            msg = lib().lbrb_ensemble_last_error(self.e)
+            raise LbrbError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "e", None):
+            lib().lbrb_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def step(self, n: int):
+        self._ck(lib().lbrb_ensemble_step(self.e, int(n)))
+
+    def sync(self):
+        self._ck(lib().lbrb_ensemble_sync(self.e))
+
+    def set_stream(self, cuda_stream):
+        self._ck(lib().lbrb_ensemble_set_stream(self.e, C.c_void_p(cuda_stream or 0)))
+
+    @staticmethod
+    def nvariants() -> int:
+        return lib().lbrb_ensemble_nvariants()
+
+    def set_schedule(self, variant: int):
+        self._ck(lib().lbrb_ensemble_set_schedule(self.e, int(variant)))
+
+    def schedule(self) -> dict:
+        v, b, r, s, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        self._ck(lib().lbrb_ensemble_get_schedule(self.e, C.byref(v), C.byref(b), C.byref(r),
+                                                  C.byref(s), C.byref(ms)))
+        return {"variant": v.value, "block": b.value, "rows": r.value,
+                "schedule": ["one block per tile", "persistent grid stride",
+                             "persistent atomic counter"][s.value] if s.value >= 0 else None,
+                "tuned_ms": ms.value}
+
+    def set_timing(self, enable: bool):
+        self._ck(lib().lbrb_ensemble_set_timing(self.e, int(bool(enable))))
+
+    def get_timing(self) -> dict:
+        ms = np.zeros(3)
+        cnt = np.zeros(3, dtype=np.int32)
+        self._ck(lib().lbrb_ensemble_get_timing(self.e, _dp(ms), _ip(cnt), 3))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("lb_step", "aux", "apply"))}
 
 
 def closure(nx: int, ny: int, Ra: float, Pr: float, U: float, dT: float = 1.0) -> dict:

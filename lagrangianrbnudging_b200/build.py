@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "liblbrb.so"
 HOST = PKG / "lbrb_host"
 SOURCES = ["lb_kernels.cu", "particle_kernels.cu", "nudge_kernels.cu", "aux_kernels.cu", "capi.cu",
-           "adjoint_kernels.cu", "noalloc.cu"]
+           "adjoint_kernels.cu", "noalloc.cu", "ensemble_kernels.cu", "ensemble.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
@@ -39,7 +39,7 @@ def _stale() -> bool:
         if dep.stat().st_mtime > HOST.stat().st_mtime:
             return True
     t = LIB.stat().st_mtime
-    deps = [CSRC / s for s in SOURCES] + [CSRC / "lbrb_internal.cuh", ROOT / "include" / "lbrb.h"]
+    deps = [CSRC / s for s in SOURCES] + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "lbrb.h"]
     return any(d.stat().st_mtime > t for d in deps)
 
 
@@ -48,14 +48,24 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
         return LIB
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for s in SOURCES:
         o = objdir / (Path(s).stem + ".o")
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-dc" if False else "-c", str(CSRC / s), "-o", str(o)]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(CSRC / s), "-o", str(o)]
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(o))
+    # translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+            if verbose_ptxas:
+                sys.stderr.write(r.stderr)
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)

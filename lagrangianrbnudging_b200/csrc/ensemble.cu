@@ -1,0 +1,496 @@
+// ensemble.cu -- C-ABI of the ensemble: many independent runs (handles made by
+// lbrb_create) advanced together, one launch per phase of the step for all
+// of them, replayed from a CUDA graph.  No counterpart in the reference.
+//
+// A member's state stays in its handle.  Every call of lbrb_ensemble_step
+// rebuilds the members' step views for the six phases of the buffer cycle
+// (populations and F alternate over 2 buffers, u and v over 3 slots, so the
+// buffer assignment repeats every 6 steps) and one view set for the last
+// step (which also writes the moments, as lbrb_step does), uploads them,
+// and queues the steps: 6-step graph replays, then single steps.  The views
+// follow lbrb_step's own buffer bookkeeping step by step, so a member
+// advanced by the ensemble ends bit-identical to the same handle advanced by
+// lbrb_step.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "capi_internal.cuh"
+#include "ensemble.cuh"
+
+using namespace lbrb;
+
+struct lbrb_ensemble_s {
+  std::vector<lbrb_t*> m;
+  std::string err;
+  int dev = 0, nsm = 148;
+  bool f32 = true;
+  int twall = LBRB_TWALL_DIRICHLET;
+  size_t vsize = 0, asize = 0;  // bytes of one LBView / EnsAux
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  void* d_views = nullptr;      // [7][n]: phases 0..5, then the last step
+  void* d_aux = nullptr;        // [7][n]
+  int4* d_items = nullptr;
+  int nitems = 0, items_variant = -1;
+  int2* d_pch = nullptr;
+  int npch = 0;
+  int2* d_och = nullptr;
+  int noch = 0;
+  int* d_ctr = nullptr;
+  int variant = -1;             // -1: tune at the next step
+  float variant_ms = 0.f;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_variant = -1;
+  bool timing = false;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+  struct Mark { int cls; cudaEvent_t a, b; };
+  std::vector<Mark> marks;
+};
+
+static int efail(lbrb_ensemble_t* e, int code, const std::string& msg, cudaError_t ce = cudaSuccess) {
+  if (e) {
+    e->err = msg;
+    if (ce != cudaSuccess) e->err += std::string(": ") + cudaGetErrorString(ce);
+  }
+  return code;
+}
+
+#define EK(e, call)                                                     \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) return efail((e), LBRB_ERR_CUDA, #call, e_); \
+  } while (0)
+
+namespace {
+
+// buffer bookkeeping of one member, as lbrb_step advances it
+struct MState {
+  int cur, uvcur, uvprev;
+};
+
+struct StepBufs {
+  int src, dst, uvn, ub, write_uv, write_rt;
+};
+
+StepBufs step_bufs(const lbrb_t* h, MState& s, bool last) {
+  StepBufs b;
+  b.write_uv = (h->np > 0) || last;
+  b.write_rt = last || h->p.nudge == LBRB_NUDGE_BILINEAR;
+  b.src = s.cur;
+  b.dst = s.cur ^ 1;
+  b.uvn = b.write_uv ? 3 - s.uvcur - s.uvprev : s.uvcur;
+  b.ub = b.write_uv ? s.uvcur : s.uvprev;
+  s.cur = b.dst;
+  if (b.write_uv) {
+    s.uvprev = s.uvcur;
+    s.uvcur = b.uvn;
+  }
+  return b;
+}
+
+template <typename Real>
+void fill_views(lbrb_t* h, const StepBufs& b, LBView<Real>* V, EnsAux<Real>* A) {
+  *V = make_view<Real>(h, b.src, b.dst, b.uvn, b.write_uv, b.write_rt);
+  EnsAux<Real> a{};
+  a.P = PView<Real>{(const Real*)h->uv[b.uvn][0], (const Real*)h->uv[b.uvn][1],
+                    (const Real*)h->uv[b.ub][0], (const Real*)h->uv[b.ub][1],
+                    (const Real*)h->T[b.dst], h->p.nx, h->p.ny, h->pitch, h->px, h->ptype, h->np,
+                    h->p.beta, 0, 0, nullptr, h->dflags};
+  a.T = (const Real*)h->T[b.dst];
+  a.g = (Real*)pop_base(h, b.dst, 1);
+  a.plane = h->plane;
+  a.nx = h->p.nx;
+  a.ny = h->p.ny;
+  a.pitch = h->pitch;
+  if (h->p.nudge == LBRB_NUDGE_BILINEAR) {
+    a.obs = h->obs;
+    a.nobs = h->nobs;
+    a.obs_first = h->obs_first;
+    a.obs_nsteps = h->obs_nsteps;
+    a.obs_cycle = h->p.obs_cycle;
+    a.alpha = h->p.alpha;
+    a.acc = reinterpret_cast<unsigned long long*>(h->acc);
+  }
+  a.istep0 = h->istep;
+  a.dflags = h->dflags;
+  *A = a;
+}
+
+// views of phases 0..5 and of the last step (n steps in this call)
+template <typename Real>
+void build_views(lbrb_ensemble_t* e, int n, std::vector<char>& vbuf, std::vector<char>& abuf) {
+  const size_t nm = e->m.size();
+  vbuf.assign(7 * nm * sizeof(LBView<Real>), 0);
+  abuf.assign(7 * nm * sizeof(EnsAux<Real>), 0);
+  LBView<Real>* V = reinterpret_cast<LBView<Real>*>(vbuf.data());
+  EnsAux<Real>* A = reinterpret_cast<EnsAux<Real>*>(abuf.data());
+  for (size_t i = 0; i < nm; i++) {
+    lbrb_t* h = e->m[i];
+    MState s{h->cur, h->uvcur, h->uvprev};
+    for (int ph = 0; ph < 6; ph++) {
+      StepBufs b = step_bufs(h, s, false);
+      fill_views<Real>(h, b, V + ph * nm + i, A + ph * nm + i);
+    }
+    MState l{h->cur, h->uvcur, h->uvprev};
+    for (int t = 0; t < (n - 1) % 6; t++) step_bufs(h, l, false);
+    StepBufs b = step_bufs(h, l, true);
+    fill_views<Real>(h, b, V + 6 * nm + i, A + 6 * nm + i);
+  }
+}
+
+// the handle state lbrb_step(n) would leave
+void advance_members(lbrb_ensemble_t* e, int n) {
+  for (lbrb_t* h : e->m) {
+    MState s{h->cur, h->uvcur, h->uvprev};
+    for (int t = 0; t < (n - 1) % 6; t++) step_bufs(h, s, false);
+    step_bufs(h, s, true);
+    h->cur = s.cur;
+    h->uvcur = s.uvcur;
+    h->uvprev = s.uvprev;
+    h->istep += n;
+    h->prev_valid = true;
+  }
+}
+
+std::vector<int4> make_items(const lbrb_ensemble_t* e, int bs, int rows) {
+  std::vector<int4> it;
+  for (size_t i = 0; i < e->m.size(); i++) {
+    const lbrb_t* h = e->m[i];
+    for (int j = 0; j < h->p.ny; j += rows)
+      for (int x = 0; x < h->p.nx; x += bs) it.push_back(make_int4((int)i, j, x, 0));
+  }
+  return it;
+}
+
+cudaEvent_t pool_ev(lbrb_ensemble_t* e) {
+  if (e->evused == e->evpool.size()) {
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+    e->evpool.push_back(ev);
+  }
+  return e->evpool[e->evused++];
+}
+
+int mark_begin(lbrb_ensemble_t* e, int cls) {
+  if (!e->timing) return -1;
+  cudaEvent_t a = pool_ev(e), b = pool_ev(e);
+  if (!a || !b) return -1;
+  cudaEventRecord(a, e->stream);
+  e->marks.push_back({cls, a, b});
+  return (int)e->marks.size() - 1;
+}
+void mark_end(lbrb_ensemble_t* e, int k) {
+  if (k >= 0) cudaEventRecord(e->marks[k].b, e->stream);
+}
+
+const char* view_at(const lbrb_ensemble_t* e, int ph) {
+  return (const char*)e->d_views + (size_t)ph * e->m.size() * e->vsize;
+}
+const char* aux_at(const lbrb_ensemble_t* e, int ph) {
+  return (const char*)e->d_aux + (size_t)ph * e->m.size() * e->asize;
+}
+
+// one step of every member, phase ph (0..5) or the last step (6)
+cudaError_t launch_step(lbrb_ensemble_t* e, int ph) {
+  int k = mark_begin(e, 0);
+  cudaError_t c = launch_ens_lb(e->f32, e->twall, e->variant, view_at(e, ph), e->d_items, e->nitems,
+                                e->d_ctr, e->nsm, e->stream);
+  mark_end(e, k);
+  if (c != cudaSuccess) return c;
+  k = mark_begin(e, 1);
+  c = launch_ens_aux(e->f32, aux_at(e, ph), e->d_pch, e->npch, e->d_och, e->noch, e->d_ctr, e->stream);
+  mark_end(e, k);
+  if (c != cudaSuccess) return c;
+  if (e->noch > 0) {
+    k = mark_begin(e, 2);
+    c = launch_ens_apply(e->f32, aux_at(e, ph), e->d_och, e->noch, e->d_ctr, e->stream);
+    mark_end(e, k);
+  }
+  return c;
+}
+
+int set_items(lbrb_ensemble_t* e, int variant) {
+  if (e->items_variant >= 0 && ENS_TABLE[e->items_variant].bs == ENS_TABLE[variant].bs &&
+      ENS_TABLE[e->items_variant].rows == ENS_TABLE[variant].rows) {
+    e->items_variant = variant;
+    EK(e, launch_ens_lb(e->f32, e->twall, variant, e->d_views, e->d_items, 0, e->d_ctr, e->nsm, e->stream));
+    return LBRB_OK;
+  }
+  std::vector<int4> it = make_items(e, ENS_TABLE[variant].bs, ENS_TABLE[variant].rows);
+  if (e->d_items) cudaFree(e->d_items);
+  e->d_items = nullptr;
+  EK(e, cudaMalloc(&e->d_items, it.size() * sizeof(int4)));
+  EK(e, cudaMemcpyAsync(e->d_items, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+  EK(e, cudaStreamSynchronize(e->stream));
+  e->nitems = (int)it.size();
+  e->items_variant = variant;
+  // the variant's occupancy query runs here, never inside a graph capture
+  EK(e, launch_ens_lb(e->f32, e->twall, variant, e->d_views, e->d_items, 0, e->d_ctr, e->nsm, e->stream));
+  return LBRB_OK;
+}
+
+// Autotuner: time each variant's phase-A launch on the members' current state
+// (a trial reads the current buffers and writes only buffers the real step
+// overwrites), 3 timed launches after a warm-up, and keep the fastest.
+int tune(lbrb_ensemble_t* e) {
+  cudaEvent_t a, b;
+  EK(e, cudaEventCreate(&a));
+  EK(e, cudaEventCreate(&b));
+  int best = 0;
+  float bt = 1e30f;
+  for (int v = 0; v < ENS_NVARIANTS; v++) {
+    int rc = set_items(e, v);
+    if (rc) return rc;
+    float tot = 0.f;
+    bool ok = true;
+    for (int r = 0; r < 4 && ok; r++) {
+      EK(e, cudaMemsetAsync(e->d_ctr, 0, 2 * sizeof(int), e->stream));
+      EK(e, cudaEventRecord(a, e->stream));
+      cudaError_t c = launch_ens_lb(e->f32, e->twall, v, view_at(e, 0), e->d_items, e->nitems, e->d_ctr,
+                                    e->nsm, e->stream);
+      if (c != cudaSuccess) {
+        cudaGetLastError();
+        ok = false;
+        break;
+      }
+      EK(e, cudaEventRecord(b, e->stream));
+      EK(e, cudaEventSynchronize(b));
+      float ms = 0.f;
+      EK(e, cudaEventElapsedTime(&ms, a, b));
+      if (r > 0) tot += ms;
+    }
+    if (ok && tot / 3 < bt) {
+      bt = tot / 3;
+      best = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  EK(e, cudaMemsetAsync(e->d_ctr, 0, 2 * sizeof(int), e->stream));
+  e->variant = best;
+  e->variant_ms = bt;
+  return set_items(e, best);
+}
+
+int ensure_graph(lbrb_ensemble_t* e) {
+  if (e->gexec && e->graph_variant == e->variant) return LBRB_OK;
+  if (e->gexec) cudaGraphExecDestroy(e->gexec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->gexec = nullptr;
+  e->graph = nullptr;
+  EK(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t c = cudaSuccess;
+  for (int ph = 0; ph < 6 && c == cudaSuccess; ph++) c = launch_step(e, ph);
+  cudaGraph_t g = nullptr;
+  cudaError_t c2 = cudaStreamEndCapture(e->stream, &g);
+  if (c != cudaSuccess) return efail(e, LBRB_ERR_CUDA, "ensemble graph capture", c);
+  if (c2 != cudaSuccess) return efail(e, LBRB_ERR_CUDA, "ensemble graph capture", c2);
+  e->graph = g;
+  EK(e, cudaGraphInstantiate(&e->gexec, g, 0));
+  e->graph_variant = e->variant;
+  return LBRB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbrb_ensemble_nvariants(void) { return ENS_NVARIANTS; }
+
+int lbrb_ensemble_create(lbrb_t* const* members, int n, lbrb_ensemble_t** out) {
+  if (!out) return LBRB_ERR_ARG;
+  *out = nullptr;
+  if (!members || n < 1) return LBRB_ERR_ARG;
+  for (int i = 0; i < n; i++) {
+    const lbrb_t* h = members[i];
+    if (!h) return LBRB_ERR_ARG;
+    for (int k = 0; k < i; k++)
+      if (members[k] == h) return LBRB_ERR_ARG;  // a handle appears once
+    const lbrb_t* h0 = members[0];
+    if (h->dev != h0->dev || h->p.precision != h0->p.precision || h->p.twall != h0->p.twall)
+      return LBRB_ERR_ARG;
+    if (h->p.nudge == LBRB_NUDGE_REFBOX) return LBRB_ERR_UNSUPPORTED;
+    if (h->np > 0 && h->p.noutconfig > 0) return LBRB_ERR_UNSUPPORTED;
+  }
+  lbrb_ensemble_t* e = new lbrb_ensemble_t();
+  e->m.assign(members, members + n);
+  e->dev = members[0]->dev;
+  e->f32 = fp32(members[0]);
+  e->twall = members[0]->p.twall;
+  e->vsize = e->f32 ? sizeof(LBView<float>) : sizeof(LBView<double>);
+  e->asize = e->f32 ? sizeof(EnsAux<float>) : sizeof(EnsAux<double>);
+  auto bad = [&](cudaError_t c) {
+    lbrb_ensemble_destroy(e);
+    return c == cudaErrorMemoryAllocation ? LBRB_ERR_NOMEM : LBRB_ERR_CUDA;
+  };
+  cudaError_t c = cudaSetDevice(e->dev);
+  if (c == cudaSuccess) c = cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, e->dev);
+  if (c == cudaSuccess) c = cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking);
+  if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->ev, cudaEventDisableTiming);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_views, 7 * (size_t)n * e->vsize);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_aux, 7 * (size_t)n * e->asize);
+  if (c == cudaSuccess) c = cudaMalloc((void**)&e->d_ctr, 4 * sizeof(int));
+  if (c != cudaSuccess) return bad(c);
+  e->stream = e->own_stream;
+  std::vector<int2> pch, och;
+  for (int i = 0; i < n; i++) {
+    const lbrb_t* h = members[i];
+    for (int p = 0; p < h->np; p += ENS_PCHUNK) pch.push_back(make_int2(i, p));
+    if (h->p.nudge == LBRB_NUDGE_BILINEAR)
+      for (int o = 0; o < h->nobs; o += ENS_OCHUNK) och.push_back(make_int2(i, o));
+  }
+  e->npch = (int)pch.size();
+  e->noch = (int)och.size();
+  c = cudaMalloc((void**)&e->d_pch, std::max<size_t>(1, pch.size()) * sizeof(int2));
+  if (c == cudaSuccess) c = cudaMalloc((void**)&e->d_och, std::max<size_t>(1, och.size()) * sizeof(int2));
+  if (c == cudaSuccess && !pch.empty())
+    c = cudaMemcpy(e->d_pch, pch.data(), pch.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  if (c == cudaSuccess && !och.empty())
+    c = cudaMemcpy(e->d_och, och.data(), och.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  if (c == cudaSuccess) c = cudaMemset(e->d_ctr, 0, 4 * sizeof(int));
+  if (c != cudaSuccess) return bad(c);
+  *out = e;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_destroy(lbrb_ensemble_t* e) {
+  if (!e) return LBRB_ERR_ARG;
+  cudaSetDevice(e->dev);
+  if (e->own_stream) cudaStreamSynchronize(e->own_stream);
+  if (e->stream && e->stream != e->own_stream) cudaStreamSynchronize(e->stream);
+  if (e->gexec) cudaGraphExecDestroy(e->gexec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  for (void* p : {(void*)e->d_views, (void*)e->d_aux, (void*)e->d_items, (void*)e->d_pch, (void*)e->d_och,
+                  (void*)e->d_ctr})
+    if (p) cudaFree(p);
+  for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
+  if (e->ev) cudaEventDestroy(e->ev);
+  if (e->own_stream) cudaStreamDestroy(e->own_stream);
+  delete e;
+  return LBRB_OK;
+}
+
+const char* lbrb_ensemble_last_error(const lbrb_ensemble_t* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int lbrb_ensemble_set_stream(lbrb_ensemble_t* e, void* cuda_stream) {
+  if (!e) return LBRB_ERR_ARG;
+  EK(e, cudaSetDevice(e->dev));
+  EK(e, cudaStreamSynchronize(e->stream));
+  e->stream = cuda_stream ? (cudaStream_t)cuda_stream : e->own_stream;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_set_schedule(lbrb_ensemble_t* e, int variant) {
+  if (!e || variant < -1 || variant >= ENS_NVARIANTS)
+    return efail(e, LBRB_ERR_ARG, "ensemble_set_schedule: variant out of range");
+  EK(e, cudaSetDevice(e->dev));
+  e->variant = variant;
+  e->variant_ms = 0.f;
+  if (variant >= 0) return set_items(e, variant);
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_get_schedule(const lbrb_ensemble_t* e, int* variant, int* block, int* rows,
+                               int* schedule, float* ms) {
+  if (!e) return LBRB_ERR_ARG;
+  const int v = e->variant;
+  if (variant) *variant = v;
+  if (block) *block = v >= 0 ? ENS_TABLE[v].bs : 0;
+  if (rows) *rows = v >= 0 ? ENS_TABLE[v].rows : 0;
+  if (schedule) *schedule = v >= 0 ? ENS_TABLE[v].sched : -1;
+  if (ms) *ms = e->variant_ms;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_set_timing(lbrb_ensemble_t* e, int enable) {
+  if (!e) return LBRB_ERR_ARG;
+  e->timing = enable != 0;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_get_timing(lbrb_ensemble_t* e, double* ms, int* launches, int n) {
+  if (!e || n < 0 || n > 3) return efail(e, LBRB_ERR_ARG, "ensemble_get_timing: n must be 0..3");
+  EK(e, cudaSetDevice(e->dev));
+  EK(e, cudaStreamSynchronize(e->stream));
+  double acc[3] = {0, 0, 0};
+  int cnt[3] = {0, 0, 0};
+  for (const auto& mk : e->marks) {
+    float t = 0.f;
+    EK(e, cudaEventElapsedTime(&t, mk.a, mk.b));
+    acc[mk.cls] += t;
+    cnt[mk.cls]++;
+  }
+  for (int c = 0; c < n; c++) {
+    if (ms) ms[c] = acc[c];
+    if (launches) launches[c] = cnt[c];
+  }
+  e->marks.clear();
+  e->evused = 0;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_step(lbrb_ensemble_t* e, int n) {
+  if (!e || n < 0) return efail(e, LBRB_ERR_ARG, "ensemble_step: bad arguments");
+  if (n == 0) return LBRB_OK;
+  for (size_t i = 0; i < e->m.size(); i++) {
+    const lbrb_t* h = e->m[i];
+    const std::string who = "ensemble_step: member " + std::to_string(i) + ": ";
+    if (!h->moments_valid) return efail(e, LBRB_ERR_STATE, who + "moments not set");
+    if (h->np > 0 && !h->particles_set) return efail(e, LBRB_ERR_STATE, who + "particles not set");
+    if (h->p.nudge == LBRB_NUDGE_BILINEAR) {
+      const int first = h->istep + 1, last = h->istep + n;
+      if (!h->obs || first < h->obs_first ||
+          (!h->p.obs_cycle && last >= h->obs_first + h->obs_nsteps))
+        return efail(e, LBRB_ERR_STATE, who + "no bilinear observations for every step");
+    }
+  }
+  EK(e, cudaSetDevice(e->dev));
+  // after the work already queued on the members' own streams
+  for (lbrb_t* h : e->m) {
+    EK(e, cudaEventRecord(e->ev, h->stream));
+    EK(e, cudaStreamWaitEvent(e->stream, e->ev, 0));
+  }
+  std::vector<char> vb, ab;
+  if (e->f32) build_views<float>(e, n, vb, ab);
+  else build_views<double>(e, n, vb, ab);
+  EK(e, cudaMemcpyAsync(e->d_views, vb.data(), vb.size(), cudaMemcpyHostToDevice, e->stream));
+  EK(e, cudaMemcpyAsync(e->d_aux, ab.data(), ab.size(), cudaMemcpyHostToDevice, e->stream));
+  EK(e, cudaMemsetAsync(e->d_ctr, 0, 2 * sizeof(int), e->stream));
+  if (e->variant < 0) {
+    int rc = tune(e);
+    if (rc) return rc;
+  } else if (e->items_variant != e->variant) {
+    int rc = set_items(e, e->variant);
+    if (rc) return rc;
+  }
+  int t = 0;
+  if (!e->timing && n - 1 >= 6) {
+    int rc = ensure_graph(e);
+    if (rc) return rc;
+    for (; t + 6 <= n - 1; t += 6) EK(e, cudaGraphLaunch(e->gexec, e->stream));
+  }
+  for (; t < n - 1; t++) EK(e, launch_step(e, t % 6));
+  EK(e, launch_step(e, 6));
+  advance_members(e, n);
+  // the members' own streams see the ensemble's steps
+  EK(e, cudaEventRecord(e->ev, e->stream));
+  for (lbrb_t* h : e->m) EK(e, cudaStreamWaitEvent(h->stream, e->ev, 0));
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_sync(lbrb_ensemble_t* e) {
+  if (!e) return LBRB_ERR_ARG;
+  EK(e, cudaSetDevice(e->dev));
+  EK(e, cudaStreamSynchronize(e->stream));
+  for (size_t i = 0; i < e->m.size(); i++) {
+    const int rc = lbrb_sync(e->m[i]);
+    if (rc != LBRB_OK)
+      return efail(e, rc, "member " + std::to_string(i) + ": " + lbrb_last_error(e->m[i]));
+  }
+  return LBRB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,50 @@
+// ensemble.cuh -- per-member views of the ensemble kernels and their launchers.
+#pragma once
+
+#include "lbrb_internal.cuh"
+#include "particle_dev.cuh"
+
+namespace lbrb {
+
+// everything phases B and C need of one member for one step
+template <typename Real>
+struct EnsAux {
+  PView<Real> P;            // particles of the step (np = 0: none)
+  const Real* T;            // T of the new state (innovations)
+  Real* g;                  // g planes of the new state (nudging apply)
+  size_t plane;
+  int nx, ny, pitch;
+  const double* obs;        // bilinear observations [rows][3][nobs], or null
+  int nobs, obs_first, obs_nsteps, obs_cycle, istep0;
+  double alpha;
+  unsigned long long* acc;  // fixed-point innovation sums
+  unsigned* dflags;
+};
+
+// observation row of the member's step istep0 + t + 1 (t counts the steps of
+// the current call from 0); coverage is checked on the host before launch
+template <typename Real>
+__device__ __forceinline__ const double* ens_obs_row(const EnsAux<Real>& A, int t) {
+  int row = A.istep0 + t + 1 - A.obs_first;
+  if (A.obs_cycle) row %= A.obs_nsteps;
+  return A.obs + (size_t)row * 3 * A.nobs;
+}
+
+// a launch variant of phase A: threads per tile row, rows per tile,
+// schedule (0 one block per tile, 1 persistent grid-stride, 2 persistent
+// atomic counter), min blocks per SM of the launch bounds
+struct EnsVariant { int bs, rows, sched, minb; };
+extern const EnsVariant ENS_TABLE[];
+extern const int ENS_NVARIANTS;
+
+constexpr int ENS_PCHUNK = 128;  // particles per block of phase B
+constexpr int ENS_OCHUNK = 128;  // observations per block of phases B and C
+
+cudaError_t launch_ens_lb(bool f32, int twall, int variant, const void* views, const int4* items,
+                          int nitems, int* ctr, int nsm, cudaStream_t s);
+cudaError_t launch_ens_aux(bool f32, const void* aux, const int2* pchunks, int npchunks,
+                           const int2* ochunks, int nochunks, int* ctr, cudaStream_t s);
+cudaError_t launch_ens_apply(bool f32, const void* aux, const int2* ochunks, int nochunks,
+                             const int* ctr, cudaStream_t s);
+
+}  // namespace lbrb

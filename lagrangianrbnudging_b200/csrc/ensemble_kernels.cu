@@ -1,0 +1,196 @@
+// ensemble_kernels.cu -- kernels that advance many independent runs
+// ("members", of uneven grid size and closure) in one launch per phase of the
+// time step.  No counterpart in the reference.
+//
+// Phase A, the fused stream/collide step of every member: a work list of
+// equal tiles (member, first row, first column; BS columns x ROWS rows) is
+// processed either one block per tile, or by a persistent grid of
+// (SMs x resident blocks) walking the list statically (grid stride) or
+// dynamically (an atomic tile counter).  A block copies its tile's member
+// view into shared memory when the member changes, then runs lb_update_node
+// -- the same per-node function as the single-run kernel, so a member's
+// result is bit-identical to the same run advanced alone.
+// Phase B: every member's particles (one block per 128-particle chunk) and
+// the innovation scatter of its bilinear observations.
+// Phase C: the nudging apply of every member.
+//
+// ctr[0] counts the steps of the current lbrb_ensemble_step call (phase A's
+// first block increments it; B and C read it to pick observation rows);
+// ctr[1] is the dynamic schedule's tile counter (cleared by phase B).
+#include "capi_internal.cuh"
+#include "ensemble.cuh"
+#include "lb_node.cuh"
+#include "nudge_dev.cuh"
+#include "particle_dev.cuh"
+
+namespace lbrb {
+
+template <typename Real, int TWALL, int BS, int ROWS, int SCHED, int MINB>
+__global__ void __launch_bounds__(BS, MINB)
+    ens_lb_kernel(const LBView<Real>* __restrict__ views, const int4* __restrict__ items, int nitems,
+                  int* __restrict__ ctr) {
+  __shared__ LBView<Real> sV;
+  __shared__ int s_item[2];
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ctr[0], 1);
+  constexpr int WORDS = (int)(sizeof(LBView<Real>) / sizeof(int));
+  static_assert(sizeof(LBView<Real>) % sizeof(int) == 0, "view size");
+  int cur_m = -1;
+  int it = blockIdx.x;
+  int par = 0;
+  for (;;) {
+    int item;
+    if (SCHED == 2) {
+      if (threadIdx.x == 0) s_item[par] = atomicAdd(&ctr[1], 1);
+      __syncthreads();
+      item = s_item[par];
+      par ^= 1;
+    } else {
+      item = it;
+      it += gridDim.x;
+    }
+    if (item >= nitems) break;
+    const int4 w = items[item];
+    if (w.x != cur_m) {
+      __syncthreads();  // every thread is done with the previous member's view
+      const int* src = reinterpret_cast<const int*>(views + w.x);
+      int* dst = reinterpret_cast<int*>(&sV);
+      for (int i = threadIdx.x; i < WORDS; i += BS) dst[i] = src[i];
+      __syncthreads();
+      cur_m = w.x;
+    }
+    const int x = w.z + threadIdx.x;
+    if (x < sV.nx) {
+      const int j1 = min(w.y + ROWS, sV.ny);
+      for (int j = w.y; j < j1; j++) lb_update_node<Real, TWALL, false>(sV, j, x);
+    }
+    if (SCHED == 0) break;
+  }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(128)
+    ens_aux_kernel(const EnsAux<Real>* __restrict__ aux, const int2* __restrict__ pchunks, int npchunks,
+                   const int2* __restrict__ ochunks, int nochunks, int* __restrict__ ctr) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctr[1] = 0;
+  int b = blockIdx.x;
+  if (b < npchunks) {
+    const int2 c = pchunks[b];
+    const EnsAux<Real>& A = aux[c.x];
+    const int p = c.y + threadIdx.x;
+    if (p < A.P.np) particle_update(A.P, p);
+    return;
+  }
+  b -= npchunks;
+  if (b < nochunks) {
+    const int2 c = ochunks[b];
+    const EnsAux<Real>& A = aux[c.x];
+    const int o = c.y + threadIdx.x;
+    if (o >= A.nobs) return;
+    const double* ob = ens_obs_row(A, ctr[0] - 1);
+    obs_scatter_one(A.T, A.nx, A.ny, A.pitch, ob[o], ob[A.nobs + o], ob[2 * A.nobs + o], A.alpha,
+                    A.acc, A.dflags);
+  }
+}
+
+// 4 threads per observation (its cell corners), 128 observations per block
+template <typename Real>
+__global__ void __launch_bounds__(512)
+    ens_apply_kernel(const EnsAux<Real>* __restrict__ aux, const int2* __restrict__ ochunks,
+                     const int* __restrict__ ctr) {
+  const int2 c = ochunks[blockIdx.x];
+  const EnsAux<Real>& A = aux[c.x];
+  const int o = c.y + (threadIdx.x >> 2);
+  if (o >= A.nobs) return;
+  const double* ob = ens_obs_row(A, ctr[0] - 1);
+  obs_apply_one(A.g, A.plane, A.nx, A.ny, A.pitch, ob[o], ob[A.nobs + o], threadIdx.x & 3, A.acc);
+}
+
+// ------------------------------------------------------------ variants
+// (threads per tile row, rows per tile, schedule, min blocks per SM)
+template <typename Real, int TWALL, int BS, int ROWS, int SCHED, int MINB>
+static cudaError_t ens_lb_launch(const LBView<Real>* views, const int4* items, int nitems, int* ctr,
+                                 int nsm, cudaStream_t s) {
+  auto k = ens_lb_kernel<Real, TWALL, BS, ROWS, SCHED, MINB>;
+  int grid = nitems;
+  if (SCHED != 0) {
+    // resident blocks per SM of this variant, queried once (outside any
+    // stream capture: the first launch of a variant is a tuning or direct one)
+    static int per = 0;
+    if (per <= 0) {
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, BS, 0);
+      if (e != cudaSuccess) return e;
+      if (per <= 0) return cudaErrorInvalidConfiguration;
+    }
+    grid = std::max(1, std::min(nitems, per * nsm));
+  }
+  if (nitems <= 0) return cudaSuccess;
+  k<<<grid, BS, 0, s>>>(views, items, nitems, ctr);
+  return cudaGetLastError();
+}
+
+#define ENS_VARIANTS(X)  \
+  X(0, 128, 1, 0, 6)     \
+  X(1, 128, 2, 0, 6)     \
+  X(2, 128, 1, 0, 8)     \
+  X(3, 128, 2, 0, 8)     \
+  X(4, 128, 1, 1, 6)     \
+  X(5, 128, 2, 1, 6)     \
+  X(6, 128, 1, 1, 8)     \
+  X(7, 128, 4, 1, 8)     \
+  X(8, 128, 1, 2, 6)     \
+  X(9, 128, 2, 2, 8)     \
+  X(10, 256, 1, 0, 3)    \
+  X(11, 256, 2, 1, 4)
+
+const EnsVariant ENS_TABLE[] = {
+#define X(i, bs, rows, sched, minb) {bs, rows, sched, minb},
+    ENS_VARIANTS(X)
+#undef X
+};
+const int ENS_NVARIANTS = sizeof(ENS_TABLE) / sizeof(ENS_TABLE[0]);
+
+template <typename Real, int TWALL>
+static cudaError_t ens_lb_dispatch(int variant, const LBView<Real>* views, const int4* items,
+                                   int nitems, int* ctr, int nsm, cudaStream_t s) {
+  switch (variant) {
+#define X(i, bs, rows, sched, minb) \
+  case i: return ens_lb_launch<Real, TWALL, bs, rows, sched, minb>(views, items, nitems, ctr, nsm, s);
+    ENS_VARIANTS(X)
+#undef X
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_ens_lb(bool f32, int twall, int variant, const void* views, const int4* items,
+                          int nitems, int* ctr, int nsm, cudaStream_t s) {
+  if (f32) {
+    if (twall == LBRB_TWALL_DIRICHLET)
+      return ens_lb_dispatch<float, LBRB_TWALL_DIRICHLET>(variant, (const LBView<float>*)views, items, nitems, ctr, nsm, s);
+    return ens_lb_dispatch<float, LBRB_TWALL_ADIABATIC>(variant, (const LBView<float>*)views, items, nitems, ctr, nsm, s);
+  }
+  if (twall == LBRB_TWALL_DIRICHLET)
+    return ens_lb_dispatch<double, LBRB_TWALL_DIRICHLET>(variant, (const LBView<double>*)views, items, nitems, ctr, nsm, s);
+  return ens_lb_dispatch<double, LBRB_TWALL_ADIABATIC>(variant, (const LBView<double>*)views, items, nitems, ctr, nsm, s);
+}
+
+cudaError_t launch_ens_aux(bool f32, const void* aux, const int2* pchunks, int npchunks,
+                           const int2* ochunks, int nochunks, int* ctr, cudaStream_t s) {
+  const int grid = std::max(1, npchunks + nochunks);
+  if (f32)
+    ens_aux_kernel<float><<<grid, 128, 0, s>>>((const EnsAux<float>*)aux, pchunks, npchunks, ochunks, nochunks, ctr);
+  else
+    ens_aux_kernel<double><<<grid, 128, 0, s>>>((const EnsAux<double>*)aux, pchunks, npchunks, ochunks, nochunks, ctr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ens_apply(bool f32, const void* aux, const int2* ochunks, int nochunks, const int* ctr,
+                             cudaStream_t s) {
+  if (nochunks <= 0) return cudaSuccess;
+  if (f32)
+    ens_apply_kernel<float><<<nochunks, 512, 0, s>>>((const EnsAux<float>*)aux, ochunks, ctr);
+  else
+    ens_apply_kernel<double><<<nochunks, 512, 0, s>>>((const EnsAux<double>*)aux, ochunks, ctr);
+  return cudaGetLastError();
+}
+
+}  // namespace lbrb

@@ -33,157 +33,9 @@
 #include <cstdlib>
 #include <type_traits>
 
-#include "lbrb_internal.cuh"
+#include "lb_node.cuh"
 
 namespace lbrb {
-
-template <int K, typename F>
-__device__ __forceinline__ void static_for(F&& f) {
-  if constexpr (K > 0) {
-    static_for<K - 1>(f);
-    f(std::integral_constant<int, K - 1>{});
-  }
-}
-
-// ------------------------------------------------ reference-order FP64 node
-template <bool REFNUDGE>
-__device__ __forceinline__ void node_ref(const LBView<double>& V, size_t idx, double* fs,
-                                         double* gs, double& Fy_io, double& r_out, double& u_out,
-                                         double& v_out, double& t_out) {
-  double r = 0.0, t = 0.0;
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) r = r + fs[k];
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) t = t + gs[k];
-  int nv = 0;
-  if (REFNUDGE) {
-    nv = V.nudge_vol[idx];
-    if (nv > 0) t = (t + 0.5 * V.nud_term[idx]);
-  }
-  const double rhoi = 1. / r;
-  double fl[NPOP];
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) fl[k] = fs[k] * rhoi;
-  const double Fx = 0.0;
-  const double Fy = Fy_io;
-  const double u = fl[1] - fl[3] + fl[5] - fl[6] - fl[7] + fl[8] + 0.5 * rhoi * Fx;
-  const double v = fl[5] + fl[2] + fl[6] - fl[7] - fl[4] - fl[8] + 0.5 * rhoi * Fy;
-  const double omega = V.omega, omegag = V.omegag;
-  double feq[NPOP];
-  equil_ref(r, u, v, feq);
-  static_for<NPOP>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    double source = (1.0 - 0.5 * omega) * w_of(k);
-    double factor = ((dcx(k) - u) * Fx + (dcy(k) - v) * Fy) / CS2;
-    factor = factor + ((dcx(k) * u + dcy(k) * v) * (dcx(k) * Fx + dcy(k) * Fy)) / (CS2 * CS2);
-    fs[k] = fs[k] * (1. - omega) + omega * feq[k] + source * factor;
-  });
-  equil_ref(t, u, v, feq);
-  if (REFNUDGE && nv > 0) {
-    const double B = 1.0 - 0.5 * omegag;
-    const double Q = V.alpha * (t - V.tempreadint[idx]);
-#pragma unroll
-    for (int k = 0; k < NPOP; k++) gs[k] = gs[k] * (1. - omegag) + omegag * feq[k] - B * w_of(k) * Q;
-    V.nud_term[idx] = -1. * Q;
-  } else {
-#pragma unroll
-    for (int k = 0; k < NPOP; k++) gs[k] = gs[k] * (1. - omegag) + omegag * feq[k];
-  }
-  // buoyancy of the next step from this step's moments (forcingconstructWW)
-  Fy_io = V.neg_gravity * r * (t - 0.0);
-  r_out = r;
-  u_out = u;
-  v_out = v;
-  t_out = t;
-}
-
-// -------------------------------------------------- FP32 shifted-form node
-__device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, float* dg,
-                                           float& Fy_io, float& r_out, float& u_out,
-                                           float& v_out, float& t_out) {
-  float dr = 0.f, dT = 0.f;
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) dr += df[k];
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) dT += dg[k];
-  const float r = 1.f + dr;
-  const float T0 = (float)V.T0;
-  const float t = T0 + dT;
-  const float jx = (df[1] - df[3]) + (df[5] - df[6]) + (df[8] - df[7]);
-  const float jy = (df[2] - df[4]) + (df[5] - df[7]) + (df[6] - df[8]);
-  const float Fy = Fy_io;
-  const float rinv = 1.f / r;
-  const float u = jx * rinv;
-  const float v = (jy + 0.5f * Fy) * rinv;
-  const float om = (float)V.omega, omg = (float)V.omegag;
-  const float srcf = 1.f - 0.5f * om;
-  const float usq15 = 1.5f * (u * u + v * v);
-  static_for<NPOP>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    constexpr float w = (float)w_of(k);
-    constexpr float cx = (float)icx(k), cy = (float)icy(k);
-    const float cu = cx * u + cy * v;
-    const float P = 3.f * cu + 4.5f * cu * cu - usq15;
-    const float dfeq = w * (dr + r * P);
-    // Guo source with F = (0, Fy): 3 (c - u).F + 9 (c.u)(c.F)
-    const float S = srcf * w * Fy * (3.f * (cy - v) + 9.f * cu * cy);
-    df[k] = df[k] + om * (dfeq - df[k]) + S;
-    const float dgeq = w * (dT + t * P);
-    dg[k] = dg[k] + omg * (dgeq - dg[k]);
-  });
-  Fy_io = (float)V.neg_gravity * r * t;
-  r_out = r;
-  u_out = u;
-  v_out = v;
-  t_out = t;
-}
-
-// ------------------------------------------------------------------ kernel
-template <typename Real, int TWALL>
-__device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, Real* fs, Real* gs) {
-  const int xl = (x == 0) ? V.nx - 1 : x - 1;       // source column of c_x = +1
-  const int xr = (x == V.nx - 1) ? 0 : x + 1;       // source column of c_x = -1
-  const bool adia_wall = TWALL == LBRB_TWALL_ADIABATIC && (j == 0 || j == V.ny - 1);
-  const int jc = (j == 0) ? 1 : V.ny - 2;
-  static_for<NPOP>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
-    const int js = j - icy(k);
-    if (js < 0 || js >= V.ny)
-      fs[k] = __ldcs(V.fsrc + (size_t)opp(k) * V.plane + (size_t)j * V.pitch + x);
-    else
-      fs[k] = __ldcs(V.fsrc + (size_t)k * V.plane + (size_t)js * V.pitch + xs);
-    if (adia_wall) {
-      gs[k] = __ldcs(V.gsrc + (size_t)k * V.plane + (size_t)jc * V.pitch + x);
-    } else {
-      int jg = js;
-      if (TWALL == LBRB_TWALL_ADIABATIC) {
-        if (jg == 0) jg = 1;
-        else if (jg == V.ny - 1) jg = V.ny - 2;
-      }
-      gs[k] = (jg < 0 || jg >= V.ny) ? Real(0)
-                                      : __ldcs(V.gsrc + (size_t)k * V.plane + (size_t)jg * V.pitch + xs);
-    }
-  });
-}
-
-// anti-bounce-back with the post-stream opposite population
-// (temppart_dump.c:896-921): g_in = -g_opp + 2 w T_wall (shifted form: T_wall - T0)
-template <typename Real>
-__device__ __forceinline__ void dirichlet_walls(const LBView<Real>& V, int j, Real* gs) {
-  if (j == V.ny - 1) {
-    const Real tw = std::is_same<Real, double>::value ? (Real)V.Tup : (Real)(V.Tup - V.T0);
-    gs[4] = -gs[2] + Real(2.0 * w_of(2)) * tw;
-    gs[7] = -gs[5] + Real(2.0 * w_of(5)) * tw;
-    gs[8] = -gs[6] + Real(2.0 * w_of(6)) * tw;
-  }
-  if (j == 0) {
-    const Real tw = std::is_same<Real, double>::value ? (Real)V.Tdown : (Real)(V.Tdown - V.T0);
-    gs[2] = -gs[4] + Real(2.0 * w_of(4)) * tw;
-    gs[5] = -gs[7] + Real(2.0 * w_of(7)) * tw;
-    gs[6] = -gs[8] + Real(2.0 * w_of(8)) * tw;
-  }
-}
 
 // post-stream populations only (walls applied): dumpfpre/dumpgpre
 template <typename Real, int TWALL>
@@ -208,30 +60,7 @@ __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V)
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (x >= V.nx) return;
-  Real fs[NPOP], gs[NPOP];
-  pull_node<Real, TWALL>(V, j, x, fs, gs);
-  if (TWALL == LBRB_TWALL_DIRICHLET) dirichlet_walls(V, j, gs);
-  const size_t o = (size_t)j * V.pitch + x;
-  Real Fy = V.Fin[o], r, u, v, t;
-  if constexpr (std::is_same<Real, double>::value) {
-    node_ref<REFNUDGE>(V, o, fs, gs, Fy, r, u, v, t);
-  } else {
-    node_shift(V, fs, gs, Fy, r, u, v, t);
-  }
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    __stcs(V.fdst + (size_t)k * V.plane + o, fs[k]);
-    __stcs(V.gdst + (size_t)k * V.plane + o, gs[k]);
-  }
-  V.Fout[o] = Fy;
-  if (V.write_uv) {
-    V.u[o] = u;
-    V.v[o] = v;
-  }
-  if (V.write_rt) {
-    V.rho[o] = r;
-    V.T[o] = t;
-  }
+  lb_update_node<Real, TWALL, REFNUDGE>(V, j, x);
 }
 
 // --------------------------------------------------------------- launch

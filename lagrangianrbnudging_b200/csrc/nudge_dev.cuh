@@ -1,0 +1,80 @@
+// nudge_dev.cuh -- bilinear-4 nudging of one observation, shared by the
+// single-run kernels (nudge_kernels.cu) and the ensemble kernels
+// (ensemble_kernels.cu).  The innovation alpha (T_obs - T(x_p)) uses the
+// reference's bilinear() form (Trajectories/code/mympi2.h:292-311) and is
+// scattered to the 4 cell corners with 2^-40 fixed-point int64 atomics:
+// integer sums do not depend on the order of the atomics, so the result is
+// deterministic.  The apply pass takes each touched node's sum once (atomic
+// exchange, leaving the accumulator cleared) and adds w_k * sum to its g.
+#pragma once
+
+#include <type_traits>
+
+#include "lbrb_internal.cuh"
+
+namespace lbrb {
+
+constexpr double FIX_SCALE = 1099511627776.0;  // 2^40
+
+__device__ __forceinline__ void obs_cell(double xx, double yy, int nx, int ny, int& x1, int& y1,
+                                         int& ix1, int& ix2, int& jy1, int& jy2) {
+  x1 = (int)xx;
+  y1 = (int)yy;
+  ix1 = (x1 - 1) % nx; if (ix1 < 0) ix1 += nx;
+  ix2 = x1 % nx; if (ix2 < 0) ix2 += nx;
+  jy1 = (y1 - 1) % ny; if (jy1 < 0) jy1 += ny;
+  jy2 = y1 % ny; if (jy2 < 0) jy2 += ny;
+}
+
+template <typename Real>
+__device__ __forceinline__ void obs_scatter_one(const Real* __restrict__ T, int nx, int ny, int pitch,
+                                                double xx, double yy, double Tobs, double alpha,
+                                                unsigned long long* __restrict__ acc,
+                                                unsigned* dflags) {
+  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) {
+    atomicOr(dflags, DFLAG_RANGE);
+    return;
+  }
+  int x1, y1, ix1, ix2, jy1, jy2;
+  obs_cell(xx, yy, nx, ny, x1, y1, ix1, ix2, jy1, jy2);
+  const int x2 = x1 + 1, y2 = y1 + 1;
+  const double u11 = (double)T[(size_t)jy1 * pitch + ix1];
+  const double u12 = (double)T[(size_t)jy2 * pitch + ix1];
+  const double u21 = (double)T[(size_t)jy1 * pitch + ix2];
+  const double u22 = (double)T[(size_t)jy2 * pitch + ix2];
+  const double val1 = u11 * ((double)x2 - xx) * ((double)y2 - yy);
+  const double val2 = u21 * (xx - (double)x1) * ((double)y2 - yy);
+  const double val3 = u12 * ((double)x2 - xx) * (yy - (double)y1);
+  const double val4 = u22 * (xx - (double)x1) * (yy - (double)y1);
+  const double tm = val1 + val2 + val3 + val4;
+  const double dlt = alpha * (Tobs - tm);
+  const double wx1 = (double)x2 - xx, wx2 = xx - (double)x1;
+  const double wy1 = (double)y2 - yy, wy2 = yy - (double)y1;
+  atomicAdd(&acc[(size_t)jy1 * pitch + ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy1) * FIX_SCALE));
+  atomicAdd(&acc[(size_t)jy1 * pitch + ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy1) * FIX_SCALE));
+  atomicAdd(&acc[(size_t)jy2 * pitch + ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy2) * FIX_SCALE));
+  atomicAdd(&acc[(size_t)jy2 * pitch + ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy2) * FIX_SCALE));
+}
+
+// corner `corner` (0..3) of the observation at (xx, yy)
+template <typename Real>
+__device__ __forceinline__ void obs_apply_one(Real* __restrict__ g, size_t plane, int nx, int ny,
+                                              int pitch, double xx, double yy, int corner,
+                                              unsigned long long* __restrict__ acc) {
+  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
+  const int x1 = (int)xx + (corner & 1), y1 = (int)yy + (corner >> 1);
+  int ix = (x1 - 1) % nx; if (ix < 0) ix += nx;
+  int jy = (y1 - 1) % ny; if (jy < 0) jy += ny;
+  const size_t q = (size_t)jy * pitch + ix;
+  const long long sfix = (long long)atomicExch(&acc[q], 0ull);
+  if (sfix == 0) return;
+  const double sv = (double)sfix * (1.0 / FIX_SCALE);
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) {
+    Real* a = g + (size_t)k * plane + q;
+    if constexpr (std::is_same<Real, double>::value) *a = *a + w_of(k) * sv;
+    else *a = *a + (float)(w_of(k) * sv);
+  }
+}
+
+}  // namespace lbrb

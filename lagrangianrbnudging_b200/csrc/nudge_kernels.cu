@@ -20,6 +20,7 @@
 //   atomics, so the result does not depend on their order, then added to the
 //   post-collision g as w_k * S.
 #include "lbrb_internal.cuh"
+#include "nudge_dev.cuh"
 
 namespace lbrb {
 
@@ -270,8 +271,6 @@ cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt
 }
 
 // ------------------------------------------------------------ bilinear mode
-constexpr double FIX_SCALE = 1099511627776.0;  // 2^40
-
 template <typename Real>
 __global__ void obs_scatter_kernel(const Real* __restrict__ T, int nx, int ny, int pitch,
                                    const double* __restrict__ ox, const double* __restrict__ oy,
@@ -279,58 +278,17 @@ __global__ void obs_scatter_kernel(const Real* __restrict__ T, int nx, int ny, i
                                    unsigned long long* __restrict__ acc, unsigned* dflags) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nobs) return;
-  double xx = ox[p], yy = oy[p];
-  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) {
-    atomicOr(dflags, DFLAG_RANGE);
-    return;
-  }
-  const int x1 = (int)xx, y1 = (int)yy, x2 = x1 + 1, y2 = y1 + 1;
-  int ix1 = (x1 - 1) % nx; if (ix1 < 0) ix1 += nx;
-  int ix2 = (x2 - 1) % nx; if (ix2 < 0) ix2 += nx;
-  int jy1 = (y1 - 1) % ny; if (jy1 < 0) jy1 += ny;
-  int jy2 = (y2 - 1) % ny; if (jy2 < 0) jy2 += ny;
-  const double u11 = (double)T[(size_t)jy1 * pitch + ix1];
-  const double u12 = (double)T[(size_t)jy2 * pitch + ix1];
-  const double u21 = (double)T[(size_t)jy1 * pitch + ix2];
-  const double u22 = (double)T[(size_t)jy2 * pitch + ix2];
-  const double val1 = u11 * ((double)x2 - xx) * ((double)y2 - yy);
-  const double val2 = u21 * (xx - (double)x1) * ((double)y2 - yy);
-  const double val3 = u12 * ((double)x2 - xx) * (yy - (double)y1);
-  const double val4 = u22 * (xx - (double)x1) * (yy - (double)y1);
-  const double tm = val1 + val2 + val3 + val4;
-  const double dlt = alpha * (oT[p] - tm);
-  const double wx1 = (double)x2 - xx, wx2 = xx - (double)x1;
-  const double wy1 = (double)y2 - yy, wy2 = yy - (double)y1;
-  atomicAdd(&acc[(size_t)jy1 * pitch + ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy1) * FIX_SCALE));
-  atomicAdd(&acc[(size_t)jy1 * pitch + ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy1) * FIX_SCALE));
-  atomicAdd(&acc[(size_t)jy2 * pitch + ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy2) * FIX_SCALE));
-  atomicAdd(&acc[(size_t)jy2 * pitch + ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy2) * FIX_SCALE));
+  obs_scatter_one(T, nx, ny, pitch, ox[p], oy[p], oT[p], alpha, acc, dflags);
 }
 
-// one thread per (observation, corner): the first to reach a node takes its
-// whole sum (atomic exchange) and adds w_k S to the 9 populations
 template <typename Real>
 __global__ void obs_apply_kernel(Real* __restrict__ g, size_t plane, int nx, int ny, int pitch,
                                  const double* __restrict__ ox, const double* __restrict__ oy,
                                  int nobs, unsigned long long* __restrict__ acc) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 4 * nobs) return;
-  const int p = t >> 2, corner = t & 3;
-  const double xx = ox[p], yy = oy[p];
-  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
-  const int x1 = (int)xx + (corner & 1), y1 = (int)yy + (corner >> 1);
-  int ix = (x1 - 1) % nx; if (ix < 0) ix += nx;
-  int jy = (y1 - 1) % ny; if (jy < 0) jy += ny;
-  const size_t q = (size_t)jy * pitch + ix;
-  const long long sfix = (long long)atomicExch(&acc[q], 0ull);
-  if (sfix == 0) return;
-  const double sv = (double)sfix * (1.0 / FIX_SCALE);
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    Real* a = g + (size_t)k * plane + q;
-    if constexpr (std::is_same<Real, double>::value) *a = *a + w_of(k) * sv;
-    else *a = *a + (float)(w_of(k) * sv);
-  }
+  const int p = t >> 2;
+  obs_apply_one(g, plane, nx, ny, pitch, ox[p], oy[p], t & 3, acc);
 }
 
 cudaError_t launch_bilinear_nudge(void* T, void* g, bool fp32, size_t plane, int nx, int ny,

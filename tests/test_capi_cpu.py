@@ -74,3 +74,12 @@ def test_host_program_rejects_bad_usage():
     assert subprocess.run([str(host), "trajectories", "nosuchparam=1"], capture_output=True).returncode == 2
     # the reference's contin=1 restart reads an uninitialised value; refused
     assert subprocess.run([str(host), "nudging", "contin=1"], capture_output=True).returncode == 2
+
+
+def test_ensemble_create_rejects_bad_arguments(L):
+    e = C.c_void_p()
+    assert L.lbrb_ensemble_create(None, 0, C.byref(e)) == -1
+    assert not e.value
+    empty = (C.c_void_p * 1)(None)
+    assert L.lbrb_ensemble_create(empty, 1, C.byref(e)) == -1
+    assert L.lbrb_ensemble_nvariants() >= 1
