@@ -188,11 +188,23 @@ def timed_steps(r, torch, steps: int, warmup: int, dist, device: int, sampler=No
 
 
 def max_over_ranks(torch, dist, v: float) -> float:
+    """the slowest rank's time: one all-reduce (NCCL on the GPUs, gloo on CPU)"""
     if dist is None:
         return v
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_seed(rank: int) -> int:
+    """each replica's own seed (independent instances, no shared state)"""
+    return SEED + 7919 * rank
+
+
+def whole_job_mlups(world: int, nodes: int, steps: int, ms_max: float) -> float:
+    """lattice updates of all ranks over the slowest rank's time"""
+    return world * nodes * steps / (ms_max * 1e3)
 
 
 def measured_peak():
@@ -286,7 +298,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
         b.build()
     if dist is not None:
         dist.barrier()
-    seed = SEED + 7919 * rank
+    seed = rank_seed(rank)
     K, W = args.steps, args.warmup
     nodes = NX * NY
     out = {}
@@ -322,8 +334,8 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
         e2e_ms = max_over_ranks(torch, dist, e2e_ms)
     if rank != 0:
         return None
-    mlups = world * nodes * K / (ms * 1e3)
-    mlups64 = world * nodes * K64 / (ms64 * 1e3)
+    mlups = whole_job_mlups(world, nodes, K, ms)
+    mlups64 = whole_job_mlups(world, nodes, K64, ms64)
     peak, peak_kind = measured_peak()
     avg_lb = lb_ms / max(lb_n, 1)
     achieved = ALG_BYTES["fp32"] * nodes / (avg_lb * 1e-3) / 1e9
@@ -742,6 +754,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=ENS_STEPS)
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="only the ensemble section (the command used for ncu captures of ens_lb_kernel)")
     ap.add_argument("--adjoint-check", action="store_true",
                     help="FD check of the adjoint gradient at the adjoint configuration")
     ap.add_argument("--lb-only", action="store_true",
@@ -765,6 +779,15 @@ def main():
     if args.lb_only:
         torch.cuda.set_device(0)
         print(json.dumps(run_lb_only(args, torch)), flush=True)
+        return
+    if args.ensemble_only:
+        import lagrangianrbnudging_b200 as lb
+        from lagrangianrbnudging_b200 import build as b
+
+        b.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"mode": "ensemble-only", **run_ensemble_bench(lb, torch, 0, args.ensemble_steps)}),
+              flush=True)
         return
     if args.adjoint_check:
         import lagrangianrbnudging_b200 as lb
