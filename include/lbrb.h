@@ -98,7 +98,9 @@ typedef struct {
   int autotune;           /* 1: time the fused kernel's launch shapes on the first step */
   int launch_shape;       /* with autotune 0: the shape used, an index into
                            * (threads per block, min blocks per SM) =
-                           * (256,1) (256,2) (256,3) (128,4) (128,6) (512,1) (512,2) */
+                           * (256,1) (256,2) (256,3) (128,4) (128,6) (512,1) (512,2)
+                           * with interior rows pulled without wall logic, then
+                           * (256,3) (128,4) (128,6) with the general pull on every row */
   int obs_cycle;          /* bilinear nudging: 1 = the series given to lbrb_nudge_obs repeats
                            * (step s uses row (s - first_step) mod nsteps); 0 = a step
                            * outside the series is an error (LBRB_ERR_STATE) */
@@ -162,10 +164,12 @@ LBRB_API int lbrb_set_stream(lbrb_t *h, void *cuda_stream);
  * class (arrays of length n <= 4) and resets the accumulators. */
 LBRB_API int lbrb_set_timing(lbrb_t *h, int enable);
 LBRB_API int lbrb_get_timing(lbrb_t *h, double *ms, int *launches, int n);
-/* Launch shape of the fused kernel (threads per block, min blocks per SM)
- * and its timed milliseconds per launch when the autotuner picked it
- * (0 before the first step or with autotune off). */
-LBRB_API int lbrb_get_launch_shape(const lbrb_t *h, int *block, int *min_blocks, float *ms);
+/* Launch shape of the fused kernel (index into the launch_shape list,
+ * threads per block, min blocks per SM) and its timed milliseconds per
+ * launch when the autotuner picked it (0 before the first step or with
+ * autotune off). */
+LBRB_API int lbrb_get_launch_shape(const lbrb_t *h, int *shape, int *block, int *min_blocks,
+                                   float *ms);
 
 /* ---- particles ------------------------------------------------------------ */
 /* Replaces init_prtcl/restore_prtcl (Trajectories/code/mympi2.h:116-290,
@@ -252,12 +256,13 @@ LBRB_API int lbrb_ensemble_sync(lbrb_ensemble_t *e);
 LBRB_API int lbrb_ensemble_set_stream(lbrb_ensemble_t *e, void *cuda_stream);
 /* Launch variant of the fused phase (threads per tile row, rows per tile,
  * schedule: 0 one block per tile, 1 persistent grid stride, 2 persistent
- * atomic tile counter).  -1 (the default): the autotuner times every variant
- * on the members' state at the next step and keeps the fastest. */
+ * atomic tile counter; pull form: 1 interior rows without wall logic, 0 the
+ * general pull).  -1 (the default): the autotuner times every variant on
+ * the members' state at the next step and keeps the fastest. */
 LBRB_API int lbrb_ensemble_nvariants(void);
 LBRB_API int lbrb_ensemble_set_schedule(lbrb_ensemble_t *e, int variant);
 LBRB_API int lbrb_ensemble_get_schedule(const lbrb_ensemble_t *e, int *variant, int *block,
-                                        int *rows, int *schedule, float *ms);
+                                        int *rows, int *schedule, int *fast_pull, float *ms);
 /* Per-launch device timing (steps then launch directly, without the graph).
  * Classes: 0 fused step, 1 particles + innovation scatter, 2 nudging apply. */
 LBRB_API int lbrb_ensemble_set_timing(lbrb_ensemble_t *e, int enable);

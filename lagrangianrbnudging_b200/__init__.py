@@ -110,7 +110,7 @@ def lib() -> C.CDLL:
         "lbrb_get_poststream": (C.c_int, [vp, dp, dp, C.c_int]),
         "lbrb_adjoint_set_obs": (C.c_int, [vp, C.c_int, ip, C.c_int, dp, dp, dp]),
         "lbrb_adjoint_window": (C.c_int, [vp, dp, C.c_int, C.c_int, dp, dp]),
-        "lbrb_get_launch_shape": (C.c_int, [vp, ip, ip, C.POINTER(C.c_float)]),
+        "lbrb_get_launch_shape": (C.c_int, [vp, ip, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_stats_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_double, C.c_double, C.c_double, vp, dp]),
         "lbrb_ensemble_create": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(vp)]),
@@ -121,7 +121,7 @@ def lib() -> C.CDLL:
         "lbrb_ensemble_set_stream": (C.c_int, [vp, vp]),
         "lbrb_ensemble_nvariants": (C.c_int, []),
         "lbrb_ensemble_set_schedule": (C.c_int, [vp, C.c_int]),
-        "lbrb_ensemble_get_schedule": (C.c_int, [vp, ip, ip, ip, ip, C.POINTER(C.c_float)]),
+        "lbrb_ensemble_get_schedule": (C.c_int, [vp, ip, ip, ip, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_ensemble_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_ensemble_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
     }
@@ -344,9 +344,11 @@ class Run:
         return {n: (float(ms[i]), int(cnt[i])) for i, n in enumerate(names)}
 
     def launch_shape(self):
-        b, m, ms = C.c_int(), C.c_int(), C.c_float()
-        self._ck(lib().lbrb_get_launch_shape(self.h, C.byref(b), C.byref(m), C.byref(ms)))
-        return {"block": b.value, "min_blocks": m.value, "tuned_ms": ms.value}
+        sh, b, m, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        self._ck(lib().lbrb_get_launch_shape(self.h, C.byref(sh), C.byref(b), C.byref(m), C.byref(ms)))
+        return {"shape": sh.value, "block": b.value, "min_blocks": m.value,
+                "pull": "interior fast path" if sh.value <= 6 else "general",
+                "tuned_ms": ms.value}
 
     # ---- diagnostics
     def energy(self):
@@ -420,12 +422,13 @@ class Ensemble:
         self._ck(lib().lbrb_ensemble_set_schedule(self.e, int(variant)))
 
     def schedule(self) -> dict:
-        v, b, r, s, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        v, b, r, s, f, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()
         self._ck(lib().lbrb_ensemble_get_schedule(self.e, C.byref(v), C.byref(b), C.byref(r),
-                                                  C.byref(s), C.byref(ms)))
+                                                  C.byref(s), C.byref(f), C.byref(ms)))
         return {"variant": v.value, "block": b.value, "rows": r.value,
                 "schedule": ["one block per tile", "persistent grid stride",
                              "persistent atomic counter"][s.value] if s.value >= 0 else None,
+                "pull": {1: "interior fast path", 0: "general"}.get(f.value),
                 "tuned_ms": ms.value}
 
     def set_timing(self, enable: bool):

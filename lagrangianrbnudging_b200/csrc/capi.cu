@@ -122,7 +122,7 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
   if (p.nudge == LBRB_NUDGE_REFBOX && p.ntempread < 2) return LBRB_ERR_ARG;
   if (p.nudge == LBRB_NUDGE_REFBOX && p.precision != LBRB_PREC_FP64) return LBRB_ERR_UNSUPPORTED;
   if (p.nprtcl > 0 && p.noutconfig > 0 && p.record_slots < 1) return LBRB_ERR_ARG;
-  if (p.launch_shape < 0 || p.launch_shape > 6) return LBRB_ERR_ARG;
+  if (p.launch_shape < 0 || p.launch_shape > 9) return LBRB_ERR_ARG;
   if ((long)p.nx * p.ny > (1L << 31) - 1) return LBRB_ERR_ARG;
 
   lbrb_t* h = new lbrb_t();
@@ -512,14 +512,15 @@ static LBView<Real> seg_view(lbrb_t* h, const char* src, char* dst, int write_rt
   return V;
 }
 
-static const int SHAPE_BS[] = {256, 256, 256, 128, 128, 512, 512};
-static const int SHAPE_MB[] = {1, 2, 3, 4, 6, 1, 2};
+static const int SHAPE_BS[] = {256, 256, 256, 128, 128, 512, 512, 256, 128, 128};
+static const int SHAPE_MB[] = {1, 2, 3, 4, 6, 1, 2, 3, 4, 6};
 
 extern "C" {
 
-int lbrb_get_launch_shape(const lbrb_t* h, int* block, int* min_blocks, float* ms) {
+int lbrb_get_launch_shape(const lbrb_t* h, int* shape, int* block, int* min_blocks, float* ms) {
   if (!h) return LBRB_ERR_ARG;
-  const int sh = h->lb_shape < 0 ? 0 : h->lb_shape;
+  const int sh = h->lb_shape < 0 ? h->p.launch_shape : h->lb_shape;
+  if (shape) *shape = sh;
   if (block) *block = SHAPE_BS[sh];
   if (min_blocks) *min_blocks = SHAPE_MB[sh];
   if (ms) *ms = h->lb_shape_ms;

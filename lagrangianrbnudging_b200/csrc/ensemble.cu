@@ -26,6 +26,7 @@ struct lbrb_ensemble_s {
   int dev = 0, nsm = 148;
   bool f32 = true;
   int twall = LBRB_TWALL_DIRICHLET;
+  bool off32 = true;            // 32-bit element offsets for every member
   size_t vsize = 0, asize = 0;  // bytes of one LBView / EnsAux
   cudaStream_t stream = nullptr, own_stream = nullptr;
   cudaEvent_t ev = nullptr;
@@ -196,7 +197,7 @@ const char* aux_at(const lbrb_ensemble_t* e, int ph) {
 // one step of every member, phase ph (0..5) or the last step (6)
 cudaError_t launch_step(lbrb_ensemble_t* e, int ph) {
   int k = mark_begin(e, 0);
-  cudaError_t c = launch_ens_lb(e->f32, e->twall, e->variant, view_at(e, ph), e->d_items, e->nitems,
+  cudaError_t c = launch_ens_lb(e->f32, e->off32, e->twall, e->variant, view_at(e, ph), e->d_items, e->nitems,
                                 e->d_ctr, e->nsm, e->stream);
   mark_end(e, k);
   if (c != cudaSuccess) return c;
@@ -216,7 +217,7 @@ int set_items(lbrb_ensemble_t* e, int variant) {
   if (e->items_variant >= 0 && ENS_TABLE[e->items_variant].bs == ENS_TABLE[variant].bs &&
       ENS_TABLE[e->items_variant].rows == ENS_TABLE[variant].rows) {
     e->items_variant = variant;
-    EK(e, launch_ens_lb(e->f32, e->twall, variant, e->d_views, e->d_items, 0, e->d_ctr, e->nsm, e->stream));
+    EK(e, launch_ens_lb(e->f32, e->off32, e->twall, variant, e->d_views, e->d_items, 0, e->d_ctr, e->nsm, e->stream));
     return LBRB_OK;
   }
   std::vector<int4> it = make_items(e, ENS_TABLE[variant].bs, ENS_TABLE[variant].rows);
@@ -228,7 +229,7 @@ int set_items(lbrb_ensemble_t* e, int variant) {
   e->nitems = (int)it.size();
   e->items_variant = variant;
   // the variant's occupancy query runs here, never inside a graph capture
-  EK(e, launch_ens_lb(e->f32, e->twall, variant, e->d_views, e->d_items, 0, e->d_ctr, e->nsm, e->stream));
+  EK(e, launch_ens_lb(e->f32, e->off32, e->twall, variant, e->d_views, e->d_items, 0, e->d_ctr, e->nsm, e->stream));
   return LBRB_OK;
 }
 
@@ -249,7 +250,7 @@ int tune(lbrb_ensemble_t* e) {
     for (int r = 0; r < 4 && ok; r++) {
       EK(e, cudaMemsetAsync(e->d_ctr, 0, 2 * sizeof(int), e->stream));
       EK(e, cudaEventRecord(a, e->stream));
-      cudaError_t c = launch_ens_lb(e->f32, e->twall, v, view_at(e, 0), e->d_items, e->nitems, e->d_ctr,
+      cudaError_t c = launch_ens_lb(e->f32, e->off32, e->twall, v, view_at(e, 0), e->d_items, e->nitems, e->d_ctr,
                                     e->nsm, e->stream);
       if (c != cudaSuccess) {
         cudaGetLastError();
@@ -320,6 +321,7 @@ int lbrb_ensemble_create(lbrb_t* const* members, int n, lbrb_ensemble_t** out) {
   e->dev = members[0]->dev;
   e->f32 = fp32(members[0]);
   e->twall = members[0]->p.twall;
+  for (int i = 0; i < n; i++) e->off32 = e->off32 && off32_ok(members[i]->plane);
   e->vsize = e->f32 ? sizeof(LBView<float>) : sizeof(LBView<double>);
   e->asize = e->f32 ? sizeof(EnsAux<float>) : sizeof(EnsAux<double>);
   auto bad = [&](cudaError_t c) {
@@ -394,13 +396,14 @@ int lbrb_ensemble_set_schedule(lbrb_ensemble_t* e, int variant) {
 }
 
 int lbrb_ensemble_get_schedule(const lbrb_ensemble_t* e, int* variant, int* block, int* rows,
-                               int* schedule, float* ms) {
+                               int* schedule, int* fast_pull, float* ms) {
   if (!e) return LBRB_ERR_ARG;
   const int v = e->variant;
   if (variant) *variant = v;
   if (block) *block = v >= 0 ? ENS_TABLE[v].bs : 0;
   if (rows) *rows = v >= 0 ? ENS_TABLE[v].rows : 0;
   if (schedule) *schedule = v >= 0 ? ENS_TABLE[v].sched : -1;
+  if (fast_pull) *fast_pull = v >= 0 ? ENS_TABLE[v].fast : -1;
   if (ms) *ms = e->variant_ms;
   return LBRB_OK;
 }

@@ -32,16 +32,19 @@ __device__ __forceinline__ const double* ens_obs_row(const EnsAux<Real>& A, int 
 
 // a launch variant of phase A: threads per tile row, rows per tile,
 // schedule (0 one block per tile, 1 persistent grid-stride, 2 persistent
-// atomic counter), min blocks per SM of the launch bounds
-struct EnsVariant { int bs, rows, sched, minb; };
+// atomic counter), min blocks per SM of the launch bounds, pull form (1
+// interior rows without wall logic and 32-bit offsets where they fit, 0 the
+// general pull with 64-bit offsets)
+struct EnsVariant { int bs, rows, sched, minb, fast; };
 extern const EnsVariant ENS_TABLE[];
 extern const int ENS_NVARIANTS;
 
 constexpr int ENS_PCHUNK = 128;  // particles per block of phase B
 constexpr int ENS_OCHUNK = 128;  // observations per block of phases B and C
 
-cudaError_t launch_ens_lb(bool f32, int twall, int variant, const void* views, const int4* items,
-                          int nitems, int* ctr, int nsm, cudaStream_t s);
+// off32: every member's population buffer holds fewer than 2^32 elements
+cudaError_t launch_ens_lb(bool f32, bool off32, int twall, int variant, const void* views,
+                          const int4* items, int nitems, int* ctr, int nsm, cudaStream_t s);
 cudaError_t launch_ens_aux(bool f32, const void* aux, const int2* pchunks, int npchunks,
                            const int2* ochunks, int nochunks, int* ctr, cudaStream_t s);
 cudaError_t launch_ens_apply(bool f32, const void* aux, const int2* ochunks, int nochunks,

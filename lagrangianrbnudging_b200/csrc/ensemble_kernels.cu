@@ -25,7 +25,7 @@
 
 namespace lbrb {
 
-template <typename Real, int TWALL, int BS, int ROWS, int SCHED, int MINB>
+template <typename Real, int TWALL, int BS, int ROWS, int SCHED, int MINB, typename Off, bool FAST>
 __global__ void __launch_bounds__(BS, MINB)
     ens_lb_kernel(const LBView<Real>* __restrict__ views, const int4* __restrict__ items, int nitems,
                   int* __restrict__ ctr) {
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(BS, MINB)
     const int x = w.z + threadIdx.x;
     if (x < sV.nx) {
       const int j1 = min(w.y + ROWS, sV.ny);
-      for (int j = w.y; j < j1; j++) lb_update_node<Real, TWALL, false>(sV, j, x);
+      for (int j = w.y; j < j1; j++) lb_update_node<Real, TWALL, false, Off, FAST>(sV, j, x);
     }
     if (SCHED == 0) break;
   }
@@ -107,10 +107,10 @@ __global__ void __launch_bounds__(512)
 
 // ------------------------------------------------------------ variants
 // (threads per tile row, rows per tile, schedule, min blocks per SM)
-template <typename Real, int TWALL, int BS, int ROWS, int SCHED, int MINB>
+template <typename Real, int TWALL, int BS, int ROWS, int SCHED, int MINB, typename Off, bool FAST>
 static cudaError_t ens_lb_launch(const LBView<Real>* views, const int4* items, int nitems, int* ctr,
                                  int nsm, cudaStream_t s) {
-  auto k = ens_lb_kernel<Real, TWALL, BS, ROWS, SCHED, MINB>;
+  auto k = ens_lb_kernel<Real, TWALL, BS, ROWS, SCHED, MINB, Off, FAST>;
   int grid = nitems;
   if (SCHED != 0) {
     // resident blocks per SM of this variant, queried once (outside any
@@ -128,49 +128,58 @@ static cudaError_t ens_lb_launch(const LBView<Real>* views, const int4* items, i
   return cudaGetLastError();
 }
 
-#define ENS_VARIANTS(X)  \
-  X(0, 128, 1, 0, 6)     \
-  X(1, 128, 2, 0, 6)     \
-  X(2, 128, 1, 0, 8)     \
-  X(3, 128, 2, 0, 8)     \
-  X(4, 128, 1, 1, 6)     \
-  X(5, 128, 2, 1, 6)     \
-  X(6, 128, 1, 1, 8)     \
-  X(7, 128, 4, 1, 8)     \
-  X(8, 128, 1, 2, 6)     \
-  X(9, 128, 2, 2, 8)     \
-  X(10, 256, 1, 0, 3)    \
-  X(11, 256, 2, 1, 4)
+// (threads per tile row, rows per tile, schedule, min blocks per SM, pull
+// form: 1 interior rows without wall logic + 32-bit offsets, 0 general)
+#define ENS_VARIANTS(X)    \
+  X(0, 128, 1, 0, 8, 1)    \
+  X(1, 128, 2, 0, 8, 1)    \
+  X(2, 128, 1, 0, 6, 1)    \
+  X(3, 128, 2, 1, 8, 1)    \
+  X(4, 128, 4, 1, 8, 1)    \
+  X(5, 128, 2, 2, 8, 1)    \
+  X(6, 256, 1, 0, 4, 1)    \
+  X(7, 256, 2, 1, 4, 1)    \
+  X(8, 128, 1, 0, 6, 0)    \
+  X(9, 128, 2, 0, 6, 0)    \
+  X(10, 256, 1, 0, 3, 0)   \
+  X(11, 128, 2, 1, 6, 0)
 
 const EnsVariant ENS_TABLE[] = {
-#define X(i, bs, rows, sched, minb) {bs, rows, sched, minb},
+#define X(i, bs, rows, sched, minb, fast) {bs, rows, sched, minb, fast},
     ENS_VARIANTS(X)
 #undef X
 };
 const int ENS_NVARIANTS = sizeof(ENS_TABLE) / sizeof(ENS_TABLE[0]);
 
-template <typename Real, int TWALL>
+template <typename Real, int TWALL, typename Off>
 static cudaError_t ens_lb_dispatch(int variant, const LBView<Real>* views, const int4* items,
                                    int nitems, int* ctr, int nsm, cudaStream_t s) {
   switch (variant) {
-#define X(i, bs, rows, sched, minb) \
-  case i: return ens_lb_launch<Real, TWALL, bs, rows, sched, minb>(views, items, nitems, ctr, nsm, s);
+#define X(i, bs, rows, sched, minb, fast)                                                       \
+  case i:                                                                                       \
+    if (fast && std::is_same<Off, uint32_t>::value)                                             \
+      return ens_lb_launch<Real, TWALL, bs, rows, sched, minb, uint32_t, true>(views, items, nitems, ctr, nsm, s); \
+    return ens_lb_launch<Real, TWALL, bs, rows, sched, minb, size_t, (bool)fast>(views, items, nitems, ctr, nsm, s);
     ENS_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_ens_lb(bool f32, int twall, int variant, const void* views, const int4* items,
-                          int nitems, int* ctr, int nsm, cudaStream_t s) {
-  if (f32) {
-    if (twall == LBRB_TWALL_DIRICHLET)
-      return ens_lb_dispatch<float, LBRB_TWALL_DIRICHLET>(variant, (const LBView<float>*)views, items, nitems, ctr, nsm, s);
-    return ens_lb_dispatch<float, LBRB_TWALL_ADIABATIC>(variant, (const LBView<float>*)views, items, nitems, ctr, nsm, s);
-  }
+template <typename Real>
+static cudaError_t ens_lb_walls(bool off32, int twall, int variant, const LBView<Real>* views,
+                                const int4* items, int nitems, int* ctr, int nsm, cudaStream_t s) {
   if (twall == LBRB_TWALL_DIRICHLET)
-    return ens_lb_dispatch<double, LBRB_TWALL_DIRICHLET>(variant, (const LBView<double>*)views, items, nitems, ctr, nsm, s);
-  return ens_lb_dispatch<double, LBRB_TWALL_ADIABATIC>(variant, (const LBView<double>*)views, items, nitems, ctr, nsm, s);
+    return off32 ? ens_lb_dispatch<Real, LBRB_TWALL_DIRICHLET, uint32_t>(variant, views, items, nitems, ctr, nsm, s)
+                 : ens_lb_dispatch<Real, LBRB_TWALL_DIRICHLET, size_t>(variant, views, items, nitems, ctr, nsm, s);
+  return off32 ? ens_lb_dispatch<Real, LBRB_TWALL_ADIABATIC, uint32_t>(variant, views, items, nitems, ctr, nsm, s)
+               : ens_lb_dispatch<Real, LBRB_TWALL_ADIABATIC, size_t>(variant, views, items, nitems, ctr, nsm, s);
+}
+
+cudaError_t launch_ens_lb(bool f32, bool off32, int twall, int variant, const void* views,
+                          const int4* items, int nitems, int* ctr, int nsm, cudaStream_t s) {
+  if (f32) return ens_lb_walls<float>(off32, twall, variant, (const LBView<float>*)views, items, nitems, ctr, nsm, s);
+  return ens_lb_walls<double>(off32, twall, variant, (const LBView<double>*)views, items, nitems, ctr, nsm, s);
 }
 
 cudaError_t launch_ens_aux(bool f32, const void* aux, const int2* pchunks, int npchunks,

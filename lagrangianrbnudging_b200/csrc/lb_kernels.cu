@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(128) lb_pull_kernel(const LBView<Real> V, Real
   const int j = blockIdx.y;
   if (x >= V.nx) return;
   Real fs[NPOP], gs[NPOP];
-  pull_node<Real, TWALL>(V, j, x, fs, gs);
+  pull_node<Real, TWALL, size_t>(V, j, x, fs, gs);
   if (TWALL == LBRB_TWALL_DIRICHLET) dirichlet_walls(V, j, gs);
   const size_t o = (size_t)j * V.pitch + x;
 #pragma unroll
@@ -55,37 +55,46 @@ __global__ void __launch_bounds__(128) lb_pull_kernel(const LBView<Real> V, Real
   }
 }
 
-template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB>
+template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB, typename Off, bool FAST>
 __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (x >= V.nx) return;
-  lb_update_node<Real, TWALL, REFNUDGE>(V, j, x);
+  lb_update_node<Real, TWALL, REFNUDGE, Off, FAST>(V, j, x);
 }
 
 // --------------------------------------------------------------- launch
-// launch shapes tried by tune_lb: (threads per block, min blocks per SM)
-struct Shape { int bs, minb; };
-constexpr Shape SHAPES[] = {{256, 1}, {256, 2}, {256, 3}, {128, 4}, {128, 6}, {512, 1}, {512, 2}};
+// launch shapes tried by tune_lb: (threads per block, min blocks per SM,
+// pull form: 1 = interior rows without wall logic and 32-bit offsets where
+// they fit, 0 = the general pull with 64-bit offsets on every row)
+struct Shape { int bs, minb, fast; };
+constexpr Shape SHAPES[] = {{256, 1, 1}, {256, 2, 1}, {256, 3, 1}, {128, 4, 1}, {128, 6, 1},
+                            {512, 1, 1}, {512, 2, 1}, {256, 3, 0}, {128, 4, 0}, {128, 6, 0}};
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 
-template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB>
+template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB, bool FAST>
 static cudaError_t launch_shape(const LBView<Real>& V, cudaStream_t s) {
   dim3 grid((V.nx + BS - 1) / BS, V.ny);
-  lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB><<<grid, BS, 0, s>>>(V);
+  if (FAST && off32_ok(V.plane))
+    lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB, uint32_t, true><<<grid, BS, 0, s>>>(V);
+  else
+    lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB, size_t, FAST><<<grid, BS, 0, s>>>(V);
   return cudaGetLastError();
 }
 
 template <typename Real, int TWALL, bool REFNUDGE>
 static cudaError_t launch_lb(const LBView<Real>& V, int shape, cudaStream_t s) {
   switch (shape) {
-    case 1: return launch_shape<Real, TWALL, REFNUDGE, 256, 2>(V, s);
-    case 2: return launch_shape<Real, TWALL, REFNUDGE, 256, 3>(V, s);
-    case 3: return launch_shape<Real, TWALL, REFNUDGE, 128, 4>(V, s);
-    case 4: return launch_shape<Real, TWALL, REFNUDGE, 128, 6>(V, s);
-    case 5: return launch_shape<Real, TWALL, REFNUDGE, 512, 1>(V, s);
-    case 6: return launch_shape<Real, TWALL, REFNUDGE, 512, 2>(V, s);
-    default: return launch_shape<Real, TWALL, REFNUDGE, 256, 1>(V, s);
+    case 1: return launch_shape<Real, TWALL, REFNUDGE, 256, 2, true>(V, s);
+    case 2: return launch_shape<Real, TWALL, REFNUDGE, 256, 3, true>(V, s);
+    case 3: return launch_shape<Real, TWALL, REFNUDGE, 128, 4, true>(V, s);
+    case 4: return launch_shape<Real, TWALL, REFNUDGE, 128, 6, true>(V, s);
+    case 5: return launch_shape<Real, TWALL, REFNUDGE, 512, 1, true>(V, s);
+    case 6: return launch_shape<Real, TWALL, REFNUDGE, 512, 2, true>(V, s);
+    case 7: return launch_shape<Real, TWALL, REFNUDGE, 256, 3, false>(V, s);
+    case 8: return launch_shape<Real, TWALL, REFNUDGE, 128, 4, false>(V, s);
+    case 9: return launch_shape<Real, TWALL, REFNUDGE, 128, 6, false>(V, s);
+    default: return launch_shape<Real, TWALL, REFNUDGE, 256, 1, true>(V, s);
   }
 }
 

@@ -80,6 +80,26 @@ __device__ __forceinline__ void node_ref(const LBView<double>& V, size_t idx, do
 }
 
 // -------------------------------------------------- FP32 shifted-form node
+// Shifted variables df_k = f_k - w_k, dg_k = g_k - w_k T0 and
+//   dr = sum df, r = 1 + dr, u = jx / r, v = (jy + Fy/2) / r, t = T0 + sum dg
+//   P_k = 3 c.u + 4.5 (c.u)^2 - 1.5 |u|^2
+//   df_k' = df_k + om (w_k (dr + r P_k) - df_k) + (1 - om/2) w_k Fy (3 (cy - v) + 9 (c.u) cy)
+//   dg_k' = dg_k + omg (w_k (dT + t P_k) - dg_k)
+// the same BGK + Guo collision as the reference, written with explicit fused
+// multiply-adds (this translation unit is otherwise built without FMA
+// contraction, which the FP64 reference-order form needs); c.u is picked per
+// direction at compile time, so no multiplication by a zero lattice
+// component is issued.
+template <int K>
+__device__ __forceinline__ float cdotu(float u, float v, float upv, float umv) {
+  constexpr int cx = icx(K), cy = icy(K);
+  if constexpr (cx == 0 && cy == 0) return 0.f;
+  else if constexpr (cy == 0) return cx > 0 ? u : -u;
+  else if constexpr (cx == 0) return cy > 0 ? v : -v;
+  else if constexpr (cx == cy) return cx > 0 ? upv : -upv;
+  else return cx > 0 ? umv : -umv;
+}
+
 __device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, float* dg,
                                            float& Fy_io, float& r_out, float& u_out,
                                            float& v_out, float& t_out) {
@@ -96,22 +116,26 @@ __device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, fl
   const float Fy = Fy_io;
   const float rinv = 1.f / r;
   const float u = jx * rinv;
-  const float v = (jy + 0.5f * Fy) * rinv;
+  const float v = fmaf(0.5f, Fy, jy) * rinv;
   const float om = (float)V.omega, omg = (float)V.omegag;
-  const float srcf = 1.f - 0.5f * om;
-  const float usq15 = 1.5f * (u * u + v * v);
+  const float srcFy = (1.f - 0.5f * om) * Fy;
+  const float usq15 = 1.5f * fmaf(u, u, v * v);
+  const float v3 = 3.f * v;
+  const float upv = u + v, umv = u - v;
   static_for<NPOP>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     constexpr float w = (float)w_of(k);
-    constexpr float cx = (float)icx(k), cy = (float)icy(k);
-    const float cu = cx * u + cy * v;
-    const float P = 3.f * cu + 4.5f * cu * cu - usq15;
-    const float dfeq = w * (dr + r * P);
-    // Guo source with F = (0, Fy): 3 (c - u).F + 9 (c.u)(c.F)
-    const float S = srcf * w * Fy * (3.f * (cy - v) + 9.f * cu * cy);
-    df[k] = df[k] + om * (dfeq - df[k]) + S;
-    const float dgeq = w * (dT + t * P);
-    dg[k] = dg[k] + omg * (dgeq - dg[k]);
+    constexpr int cy = icy(k);
+    const float cu = cdotu<k>(u, v, upv, umv);
+    const float P = (k == 0) ? -usq15 : fmaf(cu, fmaf(4.5f, cu, 3.f), -usq15);
+    // Guo source factor 3 (cy - v) + 9 (c.u) cy
+    float G;
+    if constexpr (cy == 0) G = -v3;
+    else G = fmaf(cu, 9.f * cy, 3.f * cy - v3);
+    const float dfeq = w * fmaf(r, P, dr);
+    df[k] = fmaf(w * srcFy, G, fmaf(om, dfeq - df[k], df[k]));
+    const float dgeq = w * fmaf(t, P, dT);
+    dg[k] = fmaf(omg, dgeq - dg[k], dg[k]);
   });
   Fy_io = (float)V.neg_gravity * r * t;
   r_out = r;
@@ -121,10 +145,31 @@ __device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, fl
 }
 
 // ------------------------------------------------------------------ kernel
-template <typename Real, int TWALL>
+// Element offsets: Off = uint32_t when a population buffer (18 planes) holds
+// fewer than 2^32 elements (off32_ok), else size_t.
+
+// the 9 f and 9 g values streaming into node (x, j), walls applied for f
+// (bounce-back) and for adiabatic g; Dirichlet g walls follow in dirichlet_walls
+template <typename Real, int TWALL, typename Off, bool FAST = true>
 __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, Real* fs, Real* gs) {
   const int xl = (x == 0) ? V.nx - 1 : x - 1;       // source column of c_x = +1
   const int xr = (x == V.nx - 1) ? 0 : x + 1;       // source column of c_x = -1
+  const Off pl = (Off)V.plane, pitch = (Off)V.pitch;
+  const Off oc = (Off)j * pitch;
+  // rows whose sources all lie inside the domain (for adiabatic g also off
+  // the copy rows): no wall logic; the row is uniform over a block
+  const bool interior = TWALL == LBRB_TWALL_ADIABATIC ? (j > 1 && j < V.ny - 2) : (j > 0 && j < V.ny - 1);
+  if (FAST && interior) {
+    static_for<NPOP>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
+      const Off row = icy(k) == 1 ? oc - pitch : (icy(k) == -1 ? oc + pitch : oc);
+      const Off o = (Off)k * pl + row + (Off)xs;
+      fs[k] = __ldcs(V.fsrc + o);
+      gs[k] = __ldcs(V.gsrc + o);
+    });
+    return;
+  }
   const bool adia_wall = TWALL == LBRB_TWALL_ADIABATIC && (j == 0 || j == V.ny - 1);
   const int jc = (j == 0) ? 1 : V.ny - 2;
   static_for<NPOP>([&](auto kc) {
@@ -132,11 +177,11 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
     const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
     const int js = j - icy(k);
     if (js < 0 || js >= V.ny)
-      fs[k] = __ldcs(V.fsrc + (size_t)opp(k) * V.plane + (size_t)j * V.pitch + x);
+      fs[k] = __ldcs(V.fsrc + ((Off)opp(k) * pl + oc + (Off)x));
     else
-      fs[k] = __ldcs(V.fsrc + (size_t)k * V.plane + (size_t)js * V.pitch + xs);
+      fs[k] = __ldcs(V.fsrc + ((Off)k * pl + (Off)js * pitch + (Off)xs));
     if (adia_wall) {
-      gs[k] = __ldcs(V.gsrc + (size_t)k * V.plane + (size_t)jc * V.pitch + x);
+      gs[k] = __ldcs(V.gsrc + ((Off)k * pl + (Off)jc * pitch + (Off)x));
     } else {
       int jg = js;
       if (TWALL == LBRB_TWALL_ADIABATIC) {
@@ -144,7 +189,7 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
         else if (jg == V.ny - 1) jg = V.ny - 2;
       }
       gs[k] = (jg < 0 || jg >= V.ny) ? Real(0)
-                                      : __ldcs(V.gsrc + (size_t)k * V.plane + (size_t)jg * V.pitch + xs);
+                                      : __ldcs(V.gsrc + ((Off)k * pl + (Off)jg * pitch + (Off)xs));
     }
   });
 }
@@ -169,22 +214,25 @@ __device__ __forceinline__ void dirichlet_walls(const LBView<Real>& V, int j, Re
 
 
 // one node of one step: pull (walls applied), moments, collision, stores
-template <typename Real, int TWALL, bool REFNUDGE>
+// FAST: interior rows take the pull without wall logic (else every row takes
+// the general pull)
+template <typename Real, int TWALL, bool REFNUDGE, typename Off = size_t, bool FAST = true>
 __device__ __forceinline__ void lb_update_node(const LBView<Real>& V, int j, int x) {
   Real fs[NPOP], gs[NPOP];
-  pull_node<Real, TWALL>(V, j, x, fs, gs);
+  pull_node<Real, TWALL, Off, FAST>(V, j, x, fs, gs);
   if (TWALL == LBRB_TWALL_DIRICHLET) dirichlet_walls(V, j, gs);
-  const size_t o = (size_t)j * V.pitch + x;
+  const Off pl = (Off)V.plane;
+  const Off o = (Off)j * (Off)V.pitch + (Off)x;
   Real Fy = V.Fin[o], r, u, v, t;
   if constexpr (std::is_same<Real, double>::value) {
-    node_ref<REFNUDGE>(V, o, fs, gs, Fy, r, u, v, t);
+    node_ref<REFNUDGE>(V, (size_t)o, fs, gs, Fy, r, u, v, t);
   } else {
     node_shift(V, fs, gs, Fy, r, u, v, t);
   }
 #pragma unroll
   for (int k = 0; k < NPOP; k++) {
-    __stcs(V.fdst + (size_t)k * V.plane + o, fs[k]);
-    __stcs(V.gdst + (size_t)k * V.plane + o, gs[k]);
+    __stcs(V.fdst + ((Off)k * pl + o), fs[k]);
+    __stcs(V.gdst + ((Off)k * pl + o), gs[k]);
   }
   V.Fout[o] = Fy;
   if (V.write_uv) {

@@ -48,6 +48,9 @@ static_assert(opp(5) == 7 && opp(6) == 8 && opp(7) == 5 && opp(8) == 6, "opp");
 
 constexpr double CS2 = 1.0 / 3.0;
 
+// element offsets of a population buffer (18 planes) fit in 32 bits
+inline bool off32_ok(size_t plane) { return plane * 2 * NPOP < (size_t(1) << 32); }
+
 // equilif / equilig in the reference's operation order
 // (temppart_dump.c:1097-1180): r1 is rho for f and T for g.
 __device__ __forceinline__ void equil_ref(double r1, double u, double v, double feq[NPOP]) {
