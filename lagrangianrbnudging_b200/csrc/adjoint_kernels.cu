@@ -46,7 +46,9 @@ struct AdjView {
 constexpr double ADJ_FIX = 1099511627776.0;  // 2^40
 
 template <typename Real>
-__device__ __forceinline__ void adj_pull(const AdjView<Real>& V, int j, int x, double* df, double* dg) {
+__device__ __forceinline__ void adj_pull(const AdjView<Real>& V, const Real* __restrict__ fsrc,
+                                         const Real* __restrict__ gsrc, int j, int x, double* df,
+                                         double* dg) {
   const int xl = (x == 0) ? V.nx - 1 : x - 1;
   const int xr = (x == V.nx - 1) ? 0 : x + 1;
 #pragma unroll
@@ -55,11 +57,11 @@ __device__ __forceinline__ void adj_pull(const AdjView<Real>& V, int j, int x, d
     const int js = j - icy(k);
     double fv, gv;
     if (js < 0 || js >= V.ny) {
-      fv = (double)V.fsrc[(size_t)opp(k) * V.plane + (size_t)j * V.pitch + x];
+      fv = (double)fsrc[(size_t)opp(k) * V.plane + (size_t)j * V.pitch + x];
       gv = 0.0;
     } else {
-      fv = (double)V.fsrc[(size_t)k * V.plane + (size_t)js * V.pitch + xs];
-      gv = (double)V.gsrc[(size_t)k * V.plane + (size_t)js * V.pitch + xs];
+      fv = (double)fsrc[(size_t)k * V.plane + (size_t)js * V.pitch + xs];
+      gv = (double)gsrc[(size_t)k * V.plane + (size_t)js * V.pitch + xs];
     }
     if constexpr (std::is_same<Real, double>::value) {
       // reference-order storage holds f, g themselves: go to the shifted form
@@ -85,71 +87,121 @@ __device__ __forceinline__ void adj_pull(const AdjView<Real>& V, int j, int x, d
   }
 }
 
+// The adjoint of one step at one node: from the adjoints of the node's
+// outputs (post-collision lfo(k), lgo(k); the next step's buoyancy lFo; the
+// observation term lt on T) to the adjoints of the values the node pulled
+// (outf(k, .), outg(k, .); anti-bounce-back folded in) and of the step's
+// buoyancy (lFin).  fsrc/gsrc/Fin: the state before the step.
+// Two passes over the directions: the first accumulates the adjoints of the
+// node's scalars (u, v, rho, T, F), the second forms the outputs; lfo and
+// lgo are read again there rather than held, which keeps the register count
+// (and so the number of resident warps) in reach of a latency-bound kernel.
+// The arithmetic uses explicit fused multiply-adds and one reciprocal of rho.
+template <int K>
+__device__ __forceinline__ double adj_cu(double u, double v, double upv, double umv) {
+  constexpr int cx = icx(K), cy = icy(K);
+  if constexpr (cx == 0 && cy == 0) return 0.0;
+  else if constexpr (cy == 0) return cx > 0 ? u : -u;
+  else if constexpr (cx == 0) return cy > 0 ? v : -v;
+  else if constexpr (cx == cy) return cx > 0 ? upv : -upv;
+  else return cx > 0 ? umv : -umv;
+}
+
+template <int K, typename F>
+__device__ __forceinline__ void adj_for(F&& f) {
+  if constexpr (K > 0) {
+    adj_for<K - 1>(f);
+    f(std::integral_constant<int, K - 1>{});
+  }
+}
+
+// forward quantities of a node at the step: rho, T, u, v and the buoyancy F
+struct AdjLoc {
+  double r, t, u, v, F;
+};
+
 template <typename Real>
-__global__ void __launch_bounds__(128) adjoint_step_kernel(const AdjView<Real> V) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
-  if (x >= V.nx) return;
-  const size_t o = (size_t)j * V.pitch + x;
+__device__ __forceinline__ AdjLoc adj_locals(const AdjView<Real>& V, const Real* __restrict__ fsrc,
+                                             const Real* __restrict__ gsrc, const Real* __restrict__ Fin,
+                                             int j, int x) {
   double df[NPOP], dg[NPOP];
-  adj_pull(V, j, x, df, dg);
-  // forward local quantities
-  double dr = 0.0, dT = 0.0, jx = 0.0, jy = 0.0;
+  adj_pull(V, fsrc, gsrc, j, x, df, dg);
+  double dr = 0.0, dT = 0.0;
 #pragma unroll
   for (int k = 0; k < NPOP; k++) {
     dr += df[k];
     dT += dg[k];
-    jx += icx(k) * df[k];
-    jy += icy(k) * df[k];
   }
-  const double r = 1.0 + dr, t = V.T0 + dT;
-  const double F = (double)V.Fin[o];
-  const double u = jx / r, v = (jy + 0.5 * F) / r;
+  const double jx = (df[1] - df[3]) + (df[5] - df[6]) + (df[8] - df[7]);
+  const double jy = (df[2] - df[4]) + (df[5] - df[7]) + (df[6] - df[8]);
+  AdjLoc L;
+  L.r = 1.0 + dr;
+  L.t = V.T0 + dT;
+  L.F = (double)Fin[(size_t)j * V.pitch + x];
+  const double rinv = 1.0 / L.r;
+  L.u = jx * rinv;
+  L.v = fma(0.5, L.F, jy) * rinv;
+  return L;
+}
+
+template <typename Real, typename LF, typename LG, typename OF, typename OG>
+__device__ __forceinline__ void adj_local(const AdjView<Real>& V, const AdjLoc& L, int j, LF&& lfo,
+                                          LG&& lgo, double lFo, double lt, OF&& outf, OG&& outg,
+                                          double& lFin) {
+  const double r = L.r, t = L.t, u = L.u, v = L.v, F = L.F;
+  const double rinv = 1.0 / r;
   const double om = V.omega, omg = V.omegag, srcf = 1.0 - 0.5 * om;
-  // adjoints of the outputs
-  double lfo[NPOP], lgo[NPOP];
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    lfo[k] = V.lf_out[(size_t)k * V.plane + o];
-    lgo[k] = V.lg_out[(size_t)k * V.plane + o];
-  }
-  const double lFo = V.lF[o];
-  double lt = 0.0;
-  if (V.lT) {
-    const long long q = V.lT[o];
-    lt = (double)q * (1.0 / ADJ_FIX);
-    if (q != 0) V.lT[o] = 0;
-  }
-  // transposed local Jacobian
-  double lu = 0.0, lv = 0.0, ldr = 0.0, ldT = 0.0, lFin = 0.0;
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    const double w = w_of(k), cx = icx(k), cy = icy(k);
-    const double cu = cx * u + cy * v;
-    const double P = 3.0 * cu + 4.5 * cu * cu - 1.5 * (u * u + v * v);
-    const double A = om * lfo[k];   // lambda of df_eq
-    const double B = omg * lgo[k];  // lambda of dg_eq
-    const double lP = A * w * r + B * w * t;
-    const double lS = lfo[k] * srcf * w;  // lambda of S / (srcf w) scale folded
-    const double lcu = lP * (3.0 + 9.0 * cu) + lS * F * 9.0 * cy;
-    lu += lcu * cx - lP * 3.0 * u;
-    lv += lcu * cy - lP * 3.0 * v - lS * F * 3.0;
-    ldr += A * w * (1.0 + P);
-    ldT += B * w * (1.0 + P);
-    lFin += lS * (3.0 * (cy - v) + 9.0 * cu * cy);
-  }
-  lFin += lv * 0.5 / r;
-  const double lt_tot = lt + lFo * V.gbeta * r;
-  const double lr = lFo * V.gbeta * t - (lu * u + lv * v) / r;
-  const double ljx = lu / r, ljy = lv / r;
-  ldr += lr;
-  ldT += lt_tot;
-  double lfs[NPOP], lgs[NPOP];
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    lfs[k] = (1.0 - om) * lfo[k] + ldr + icx(k) * ljx + icy(k) * ljy;
-    lgs[k] = (1.0 - omg) * lgo[k] + ldT;
-  }
+  const double usq15 = 1.5 * fma(u, u, v * v);
+  const double upv = u + v, umv = u - v, v3 = 3.0 * v, F9 = 9.0 * F;
+  // pass 1: adjoints of the scalars
+  double lu = 0.0, lv = 0.0, ldr = 0.0, ldT = 0.0, lF = 0.0, slP = 0.0, slS = 0.0;
+  adj_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    constexpr double w = w_of(k);
+    constexpr int cx = icx(k), cy = icy(k);
+    const double cu = adj_cu<k>(u, v, upv, umv);
+    const double P = fma(cu, fma(4.5, cu, 3.0), -usq15);
+    const double lf = lfo(k), lg = lgo(k);
+    const double Aw = (om * w) * lf;   // lambda of df_eq, times w
+    const double Bw = (omg * w) * lg;  // lambda of dg_eq, times w
+    const double lP = fma(Aw, r, Bw * t);
+    const double lS = (srcf * w) * lf;
+    double lcu = lP * fma(9.0, cu, 3.0);
+    if constexpr (cy != 0) lcu = fma(lS, cy * F9, lcu);
+    if constexpr (cx == 1) lu += lcu;
+    if constexpr (cx == -1) lu -= lcu;
+    if constexpr (cy == 1) lv += lcu;
+    if constexpr (cy == -1) lv -= lcu;
+    slP += lP;
+    slS += lS;
+    const double onep = 1.0 + P;
+    ldr = fma(Aw, onep, ldr);
+    ldT = fma(Bw, onep, ldT);
+    // Guo source factor 3 (cy - v) + 9 (c.u) cy
+    double G;
+    if constexpr (cy == 0) G = -v3;
+    else G = fma(9.0 * cy, cu, 3.0 * cy - v3);
+    lF = fma(lS, G, lF);
+  });
+  lu = fma(-3.0 * u, slP, lu);
+  lv = fma(-3.0 * v, slP, fma(-3.0 * F, slS, lv));
+  lF = fma(lv * 0.5, rinv, lF);
+  ldr += fma(lFo * V.gbeta, t, -fma(lu, u, lv * v) * rinv);
+  ldT += fma(lFo * V.gbeta, r, lt);
+  const double ljx = lu * rinv, ljy = lv * rinv;
+  // pass 2: outputs
+  double lgs[NPOP];
+  adj_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    constexpr int cx = icx(k), cy = icy(k);
+    double o = fma(1.0 - om, lfo(k), ldr);
+    if constexpr (cx == 1) o += ljx;
+    if constexpr (cx == -1) o -= ljx;
+    if constexpr (cy == 1) o += ljy;
+    if constexpr (cy == -1) o -= ljy;
+    outf(k, o);
+    lgs[k] = fma(1.0 - omg, lgo(k), ldT);
+  });
   // anti-bounce-back transpose: the replaced population feeds its opposite
   if (j == V.ny - 1) {
     lgs[2] -= lgs[4]; lgs[4] = 0.0;
@@ -161,23 +213,138 @@ __global__ void __launch_bounds__(128) adjoint_step_kernel(const AdjView<Real> V
     lgs[7] -= lgs[5]; lgs[5] = 0.0;
     lgs[8] -= lgs[6]; lgs[6] = 0.0;
   }
-  // transpose of the pull
-  const int xl = (x == 0) ? V.nx - 1 : x - 1;
-  const int xr = (x == V.nx - 1) ? 0 : x + 1;
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) outg(k, lgs[k]);
+  lFin = lF;
+}
+
+// transpose of the pull for one direction: the node's pulled adjoint of
+// population k goes to the node the forward pulled it from (bounce-back:
+// this node's opposite population; g streaming out of the domain gets zero).
+// Every (population, node) of the output receives exactly one write.
+__device__ __forceinline__ void adj_push_one(int k, bool is_g, double val, int nx, int ny, int pitch,
+                                             size_t plane, int j, int x, double* __restrict__ out) {
+  const int xs = icx(k) == 1 ? (x == 0 ? nx - 1 : x - 1) : (icx(k) == -1 ? (x == nx - 1 ? 0 : x + 1) : x);
+  const int js = j - icy(k);
+  if (js < 0 || js >= ny) out[(size_t)opp(k) * plane + (size_t)j * pitch + x] = is_g ? 0.0 : val;
+  else out[(size_t)k * plane + (size_t)js * pitch + xs] = val;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(128) adjoint_step_kernel(const AdjView<Real> V) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (x >= V.nx) return;
+  const size_t o = (size_t)j * V.pitch + x;
+  // every load of the node issued before the arithmetic
+  double lf[NPOP], lg[NPOP];
 #pragma unroll
   for (int k = 0; k < NPOP; k++) {
-    const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
-    const int js = j - icy(k);
-    if (js < 0 || js >= V.ny) {
-      V.lf_in[(size_t)opp(k) * V.plane + o] = lfs[k];  // bounce-back source
-      V.lg_in[(size_t)opp(k) * V.plane + o] = 0.0;     // streams out, never read
-    } else {
-      const size_t os = (size_t)js * V.pitch + xs;
-      V.lf_in[(size_t)k * V.plane + os] = lfs[k];
-      V.lg_in[(size_t)k * V.plane + os] = lgs[k];
-    }
+    lf[k] = V.lf_out[(size_t)k * V.plane + o];
+    lg[k] = V.lg_out[(size_t)k * V.plane + o];
   }
+  const double lFo = V.lF[o];
+  const double lt = V.lT ? (double)V.lT[o] * (1.0 / ADJ_FIX) : 0.0;
+  const AdjLoc L = adj_locals(V, V.fsrc, V.gsrc, V.Fin, j, x);
+  double lFin;
+  adj_local(
+      V, L, j, [&](int k) { return lf[k]; }, [&](int k) { return lg[k]; }, lFo, lt,
+      [&](int k, double val) { adj_push_one(k, false, val, V.nx, V.ny, V.pitch, V.plane, j, x, V.lf_in); },
+      [&](int k, double val) { adj_push_one(k, true, val, V.nx, V.ny, V.pitch, V.plane, j, x, V.lg_in); },
+      lFin);
   V.lF[o] = lFin;
+}
+
+// Two adjoint steps (n, then n-1) in one launch.  A block owns a TX x TY
+// tile.  Phase 1 computes step n's pulled adjoints (18 values and lambda F^n)
+// at the tile and a one-node ring around it, from lambda^n in HBM, into
+// shared memory.  Phase 2 gathers step n-1's output adjoints of each tile
+// node from shared memory -- the value the push of step n would have written
+// there -- and pushes step n-1's pulled adjoints to lambda^{n-2} in HBM.  The
+// FP64 lambda crosses HBM once per two steps instead of once per step.
+// lambda F is read from lF (step n+1) and written to lF_out (step n-1), and
+// the observation terms lT_a (step n) and lT_b (step n-1) are only read
+// (cleared afterwards), since neighbouring blocks read the ring nodes too.
+template <typename Real>
+struct AdjPairView {
+  AdjView<Real> a;                      // step n: state before it, lambda^n, lambda F^{n+1}, lambda T^n
+  const Real* __restrict__ fsrc_b;      // state before step n-1
+  const Real* __restrict__ gsrc_b;
+  const Real* __restrict__ Fin_b;
+  const long long* __restrict__ lT_b;   // lambda T^{n-1} or null
+  double* __restrict__ lf_in;           // lambda^{n-2}
+  double* __restrict__ lg_in;
+  double* __restrict__ lF_out;          // lambda F^{n-1}
+};
+
+constexpr int ADJ_TX = 32;
+
+template <typename Real, int TY, int MINB>
+__global__ void __launch_bounds__(ADJ_TX * TY, MINB) adjoint_pair_kernel(const AdjPairView<Real> P) {
+  extern __shared__ double sm[];
+  constexpr int HX = ADJ_TX + 2, HY = TY + 2, NH = HX * HY;
+  const AdjView<Real>& V = P.a;
+  const int nx = V.nx, ny = V.ny;
+  const int x0 = blockIdx.x * ADJ_TX, j0 = blockIdx.y * TY;
+  // the forward quantities of this thread's phase-2 node do not depend on
+  // phase 1: their loads go out first and overlap it
+  const int tx = threadIdx.x % ADJ_TX, ty = threadIdx.x / ADJ_TX;
+  const int x = x0 + tx, j = j0 + ty;
+  const bool mine = x < nx && j < ny;
+  AdjLoc L2{};
+  double lt2 = 0.0;
+  if (mine) {
+    L2 = adj_locals(V, P.fsrc_b, P.gsrc_b, P.Fin_b, j, x);
+    if (P.lT_b) lt2 = (double)P.lT_b[(size_t)j * V.pitch + x] * (1.0 / ADJ_FIX);
+  }
+  // phase 1: step n at the tile and its ring
+  for (int h = threadIdx.x; h < NH; h += blockDim.x) {
+    const int hx = h % HX, hy = h / HX;
+    int xh = x0 - 1 + hx;
+    const int jh = j0 - 1 + hy;
+    if (xh == -1) xh = nx - 1;
+    else if (xh == nx) xh = 0;
+    if (jh < 0 || jh >= ny || xh >= nx) continue;  // no node there
+    const size_t o = (size_t)jh * V.pitch + xh;
+    double lf[NPOP], lg[NPOP];
+#pragma unroll
+    for (int k = 0; k < NPOP; k++) {
+      lf[k] = V.lf_out[(size_t)k * V.plane + o];
+      lg[k] = V.lg_out[(size_t)k * V.plane + o];
+    }
+    const double lFo = V.lF[o];
+    const double lt = V.lT ? (double)V.lT[o] * (1.0 / ADJ_FIX) : 0.0;
+    const AdjLoc L = adj_locals(V, V.fsrc, V.gsrc, V.Fin, jh, xh);
+    double lFin;
+    adj_local(
+        V, L, jh, [&](int k) { return lf[k]; }, [&](int k) { return lg[k]; }, lFo, lt,
+        [&](int k, double val) { sm[k * NH + h] = val; },
+        [&](int k, double val) { sm[(NPOP + k) * NH + h] = val; }, lFin);
+    sm[2 * NPOP * NH + h] = lFin;
+  }
+  __syncthreads();
+  // phase 2: step n-1 at the tile
+  if (!mine) return;
+  const int hs = (tx + 1) + (ty + 1) * HX;  // this node in the ring layout
+  // output m of step n-1 at this node went to node (x, j) + c_m (pulled there
+  // by step n); at a wall it was bounced back into opp(m) here (f) or left
+  // the domain (g)
+  auto lfo = [&](int m) {
+    const int sj = j + icy(m);
+    return (sj < 0 || sj >= ny) ? sm[opp(m) * NH + hs] : sm[m * NH + hs + icx(m) + icy(m) * HX];
+  };
+  auto lgo = [&](int m) {
+    const int sj = j + icy(m);
+    return (sj < 0 || sj >= ny) ? 0.0 : sm[(NPOP + m) * NH + hs + icx(m) + icy(m) * HX];
+  };
+  const size_t o = (size_t)j * V.pitch + x;
+  double lFin;
+  adj_local(
+      V, L2, j, lfo, lgo, sm[2 * NPOP * NH + hs], lt2,
+      [&](int k, double val) { adj_push_one(k, false, val, nx, ny, V.pitch, V.plane, j, x, P.lf_in); },
+      [&](int k, double val) { adj_push_one(k, true, val, nx, ny, V.pitch, V.plane, j, x, P.lg_in); },
+      lFin);
+  P.lF_out[o] = lFin;
 }
 
 // observation adjoint of step n: lambda T += 2 r_p w_corner, fixed point
@@ -285,7 +452,111 @@ __global__ void adj_initial_kernel(const double* __restrict__ lg, const double* 
   }
 }
 
+// clear the observation adjoint of one step after its consumer kernel ran
+// (the corners the scatter touched)
+__global__ void adj_obs_clear_kernel(const double* __restrict__ ox, const double* __restrict__ oy,
+                                     int nobs, int nx, int ny, int pitch, long long* __restrict__ acc) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nobs) return;
+  const double xx = ox[p], yy = oy[p];
+  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
+  const int x1 = (int)xx, y1 = (int)yy, x2 = x1 + 1, y2 = y1 + 1;
+  int ix1 = (x1 - 1) % nx; if (ix1 < 0) ix1 += nx;
+  int ix2 = (x2 - 1) % nx; if (ix2 < 0) ix2 += nx;
+  int jy1 = (y1 - 1) % ny; if (jy1 < 0) jy1 += ny;
+  int jy2 = (y2 - 1) % ny; if (jy2 < 0) jy2 += ny;
+  acc[(size_t)jy1 * pitch + ix1] = 0;
+  acc[(size_t)jy1 * pitch + ix2] = 0;
+  acc[(size_t)jy2 * pitch + ix1] = 0;
+  acc[(size_t)jy2 * pitch + ix2] = 0;
+}
+
+// misfit J = sum of squared residuals: per-thread Neumaier sums in a fixed
+// order, combined by a tree of error-free additions (deterministic)
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bp = s - a;
+  e = (a - (s - bp)) + (b - bp);
+}
+
+__global__ void __launch_bounds__(1024) misfit_kernel(const double* __restrict__ res, long n,
+                                                      double* __restrict__ out) {
+  __shared__ double ss[1024], sc[1024];
+  double sum = 0.0, comp = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) {
+    const double x = res[i] * res[i];
+    double t, e;
+    two_sum(sum, x, t, e);
+    sum = t;
+    comp += e;
+  }
+  ss[threadIdx.x] = sum;
+  sc[threadIdx.x] = comp;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      double t, e;
+      two_sum(ss[threadIdx.x], ss[threadIdx.x + w], t, e);
+      ss[threadIdx.x] = t;
+      sc[threadIdx.x] += sc[threadIdx.x + w] + e;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = ss[0] + sc[0];
+}
+
 // ---------------------------------------------------------------- launchers
+template <typename Real, int TY, int MINB>
+static cudaError_t launch_pair_t(const AdjPairView<Real>& P, cudaStream_t s) {
+  constexpr int NH = (ADJ_TX + 2) * (TY + 2);
+  constexpr size_t smem = (size_t)(2 * NPOP + 1) * NH * sizeof(double);
+  static cudaError_t attr = cudaFuncSetAttribute(adjoint_pair_kernel<Real, TY, MINB>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr != cudaSuccess) return attr;
+  dim3 grid((P.a.nx + ADJ_TX - 1) / ADJ_TX, (P.a.ny + TY - 1) / TY);
+  adjoint_pair_kernel<Real, TY, MINB><<<grid, ADJ_TX * TY, smem, s>>>(P);
+  return cudaGetLastError();
+}
+
+// launch variants of the pair kernel: tile rows (TY, 32 columns) and min
+// blocks per SM
+constexpr int ADJ_NPAIR_VARIANTS = 4;
+int adjoint_pair_variants() { return ADJ_NPAIR_VARIANTS; }
+
+// steps n and n-1: state_a before step n, state_b before step n-1 (18 pop
+// planes then F), lambda^n in (lf_out, lg_out), lambda^{n-2} out (lf_in,
+// lg_in), lambda F^{n+1} in (lF_in), lambda F^{n-1} out (lF_out)
+cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, const void* state_b,
+                                const double* lf_out, const double* lg_out, double* lf_in,
+                                double* lg_in, double* lF_in, double* lF_out, const long long* lT_a,
+                                const long long* lT_b, int nx, int ny, int pitch, size_t plane,
+                                double omega, double omegag, double gbeta, double T0, double Tup,
+                                double Tdown, cudaStream_t s) {
+  auto go = [&](auto zero) -> cudaError_t {
+    using Real = decltype(zero);
+    const Real* a = (const Real*)state_a;
+    const Real* b = (const Real*)state_b;
+    AdjPairView<Real> P{};
+    P.a = AdjView<Real>{a, a + NPOP * plane, a + 2 * NPOP * plane, lf_out, lg_out, nullptr, nullptr,
+                        lF_in, const_cast<long long*>(lT_a), nx, ny, pitch, plane, omega, omegag,
+                        gbeta, T0, Tup, Tdown};
+    P.fsrc_b = b;
+    P.gsrc_b = b + NPOP * plane;
+    P.Fin_b = b + 2 * NPOP * plane;
+    P.lT_b = lT_b;
+    P.lf_in = lf_in;
+    P.lg_in = lg_in;
+    P.lF_out = lF_out;
+    switch (variant) {
+      case 1: return launch_pair_t<Real, 4, 6>(P, s);
+      case 2: return launch_pair_t<Real, 8, 2>(P, s);
+      case 3: return launch_pair_t<Real, 8, 3>(P, s);
+      default: return launch_pair_t<Real, 4, 4>(P, s);
+    }
+  };
+  return fp32 ? go(0.f) : go(0.0);
+}
+
 template <typename Real>
 static cudaError_t launch_adj_t(const AdjView<Real>& V, cudaStream_t s) {
   dim3 grid((V.nx + 127) / 128, V.ny);
@@ -306,6 +577,18 @@ cudaError_t launch_adjoint_step(bool fp32, const void* fsrc, const void* gsrc, c
   AdjView<double> V{(const double*)fsrc, (const double*)gsrc, (const double*)Fin, lf_out, lg_out, lf_in,
                     lg_in, lF, lT, nx, ny, pitch, plane, omega, omegag, gbeta, T0, Tup, Tdown};
   return launch_adj_t(V, s);
+}
+
+cudaError_t launch_misfit(const double* res, long n, double* out, cudaStream_t s) {
+  misfit_kernel<<<1, 1024, 0, s>>>(res, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_obs_clear(const double* ox, const double* oy, int nobs, int nx, int ny, int pitch,
+                                 long long* acc, cudaStream_t s) {
+  if (nobs <= 0) return cudaSuccess;
+  adj_obs_clear_kernel<<<(nobs + 127) / 128, 128, 0, s>>>(ox, oy, nobs, nx, ny, pitch, acc);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_adj_obs_scatter(const double* ox, const double* oy, const double* res, int nobs,

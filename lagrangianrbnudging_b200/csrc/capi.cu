@@ -97,6 +97,7 @@ static void free_all(lbrb_t* h) {
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
   delete[] h->adj_steps;
   if (h->h_flags) cudaFreeHost(h->h_flags);
+  if (h->h_scalar) cudaFreeHost(h->h_scalar);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->join_ev) cudaEventDestroy(h->join_ev);
@@ -202,6 +203,7 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
   if (dalloc(&h->red, (size_t)red_blocks() * 6 + 8 + (size_t)p.ny * 9)) return done(LBRB_ERR_NOMEM);
   if (dalloc(&h->dflags, 1)) return done(LBRB_ERR_NOMEM);
   if (cudaMallocHost(&h->h_flags, sizeof(unsigned)) != cudaSuccess) return done(LBRB_ERR_NOMEM);
+  if (cudaMallocHost(&h->h_scalar, sizeof(double)) != cudaSuccess) return done(LBRB_ERR_NOMEM);
   if (cudaDeviceSynchronize() != cudaSuccess) return done(LBRB_ERR_CUDA);
   return done(LBRB_OK);
 }
@@ -732,6 +734,16 @@ static int grow(lbrb_t* h, void** p, size_t* have, size_t need) {
   return LBRB_OK;
 }
 
+// Assimilation window with checkpoints every K steps.
+// Forward: step i of segment c reads its input state from checkpoint c (i = 0)
+// or segment slot i, and writes its output to slot i+1 -- or, for the
+// segment's last step, to checkpoint c+1 (the window's end state: slot K).
+// The last segment's states are therefore still in the slots when the
+// backward pass starts and need no recompute.
+// Backward: segments last to first; each is recomputed into the slots (all
+// but the last), then its steps run in reverse, two at a time through the
+// pair kernel (lambda crosses HBM once per two steps) and one at a time for
+// an odd leftover.  Results do not depend on K.
 int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* J, double* dJdT0) {
   if (!h || !T0 || nsteps < 1 || K < 1 || !J) return fail(h, LBRB_ERR_ARG, "adjoint_window: bad arguments");
   if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE)
@@ -747,113 +759,165 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   const int nchk = (nsteps + K - 1) / K;
   int rc;
   if ((rc = grow(h, &h->adj_chk, &h->adj_chk_bytes, (size_t)nchk * sb))) return rc;
+  if ((rc = grow(h, &h->adj_seg, &h->adj_seg_bytes, (size_t)(K + 1) * sb))) return rc;
   if (!h->adj_T0 && cudaMalloc(&h->adj_T0, nn * sizeof(double)) != cudaSuccess)
     return fail(h, LBRB_ERR_NOMEM, "adjoint T0");
   CK(h, cudaMemcpyAsync(h->adj_T0, T0, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   const double T0ref = T0_of(h), ng = -h->p.gravity;
   const double om = 1. / h->p.relax, omg = 1. / h->p.relaxg;
-  const int shape = h->lb_shape < 0 ? h->p.launch_shape : h->lb_shape;
   // observation step lookup
   std::vector<int> obs_at(nsteps + 1, -1);
   for (int a = 0; a < h->adj_nsteps_obs; a++)
     if (h->adj_steps[a] <= nsteps) obs_at[h->adj_steps[a]] = a;
   const int nob = h->adj_nobs;
+  char* chk = (char*)h->adj_chk;
+  char* seg = (char*)h->adj_seg;
+  auto state_in = [&](int c, int i) -> char* { return i == 0 ? chk + (size_t)c * sb : seg + (size_t)i * sb; };
+  // the window's initial state in checkpoint 0 (pops + F), moments in buffer 0
+  CK(h, launch_init_from_T0(h->adj_T0, chk, h->rho[0], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
+                            h->T[0], chk + 2 * NPOP * plane * es, f32, nx, ny, pitch, plane, T0ref,
+                            ng, h->stream));
+  if (h->lb_shape < 0) {
+    // the fused kernel's launch shape, timed on this window's initial state
+    int sh = h->p.launch_shape;
+    float ms = 0.f;
+    if (h->p.autotune) {
+      if (f32) sh = tune_lb_fp32(seg_view<float>(h, chk, seg + sb, 0), h->p.twall, h->stream, &ms);
+      else sh = tune_lb_fp64(seg_view<double>(h, chk, seg + sb, 0), h->p.twall, h->stream, &ms);
+    }
+    CK(h, cudaGetLastError());
+    h->lb_shape = sh;
+    h->lb_shape_ms = ms;
+  }
+  const int shape = h->lb_shape;
   auto launch_fwd = [&](const char* src, char* dst, int write_rt) -> cudaError_t {
     if (f32) return launch_lb_fp32(seg_view<float>(h, src, dst, write_rt), h->p.twall, shape, h->stream);
     return launch_lb_fp64(seg_view<double>(h, src, dst, write_rt), h->p.twall, false, shape, h->stream);
   };
   // ---- forward pass: checkpoints, residuals
-  char* chk = (char*)h->adj_chk;
-  // the window's initial state is built in checkpoint 0 (pops + F), moments in buffer 0
-  CK(h, launch_init_from_T0(h->adj_T0, chk, h->rho[0], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
-                            h->T[0], chk + 2 * NPOP * plane * es, f32, nx, ny, pitch, plane, T0ref,
-                            ng, h->stream));
-  // ping-pong through the handle's two population buffers (pops + F contiguous views)
-  std::vector<char> dummy;
-  const size_t pb = 2 * NPOP * plane * es;
-  (void)pb;
-  // state buffers for the forward: use the segment buffer's first two slots
-  if ((rc = grow(h, &h->adj_seg, &h->adj_seg_bytes, (size_t)(K + 1) * sb))) return rc;
-  char* seg = (char*)h->adj_seg;
-  CK(h, cudaMemcpyAsync(seg, chk, sb, cudaMemcpyDeviceToDevice, h->stream));
-  int a_cur = 0;
-  for (int s = 1; s <= nsteps; s++) {
-    if ((s - 1) % K == 0 && s > 1)
-      CK(h, cudaMemcpyAsync(chk + (size_t)((s - 1) / K) * sb, seg + (size_t)a_cur * sb, sb,
-                            cudaMemcpyDeviceToDevice, h->stream));
-    const int oi = obs_at[s];
-    CK(h, launch_fwd(seg + (size_t)a_cur * sb, seg + (size_t)(a_cur ^ 1) * sb, oi >= 0));
-    if (oi >= 0) {
-      const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
-      CK(h, launch_obs_residual(h->T[0], f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob, nob,
-                                h->adj_res + (size_t)oi * nob, h->stream));
-    }
-    a_cur ^= 1;
-  }
-  // misfit (compensated sum on the host)
-  std::vector<double> res((size_t)h->adj_nsteps_obs * nob);
-  CK(h, cudaMemcpyAsync(res.data(), h->adj_res, res.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaStreamSynchronize(h->stream));
-  {
-    double sum = 0.0, c = 0.0;
-    for (int a = 0; a < h->adj_nsteps_obs; a++) {
-      if (h->adj_steps[a] > nsteps) continue;
-      for (int p = 0; p < nob; p++) {
-        const double r = res[(size_t)a * nob + p];
-        const double y = r * r - c, t = sum + y;
-        c = (t - sum) - y;
-        sum = t;
+  char* end_state = nullptr;
+  for (int c = 0; c < nchk; c++) {
+    const int s0 = c * K, len = std::min(K, nsteps - s0);
+    for (int i = 0; i < len; i++) {
+      const int s = s0 + i + 1;
+      char* dst = (i + 1 < len) ? seg + (size_t)(i + 1) * sb
+                                : (c + 1 < nchk ? chk + (size_t)(c + 1) * sb : seg + (size_t)K * sb);
+      const int oi = obs_at[s];
+      CK(h, launch_fwd(state_in(c, i), dst, oi >= 0));
+      if (oi >= 0) {
+        const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
+        CK(h, launch_obs_residual(h->T[0], f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob, nob,
+                                  h->adj_res + (size_t)oi * nob, h->stream));
       }
+      end_state = dst;
     }
-    *J = sum;
   }
+  // misfit on the device (observation steps inside the window: a prefix)
+  int nused = 0;
+  while (nused < h->adj_nsteps_obs && h->adj_steps[nused] <= nsteps) nused++;
+  double* dJ = h->red;  // reduction scratch of the handle
+  CK(h, launch_misfit(h->adj_res, (long)nused * nob, dJ, h->stream));
+  CK(h, cudaMemcpyAsync(h->h_scalar, dJ, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   // the handle's state: end of the window
   {
     const size_t popb = 2 * NPOP * plane * es;
-    CK(h, cudaMemcpyAsync(h->pops[h->cur], seg + (size_t)a_cur * sb, popb, cudaMemcpyDeviceToDevice, h->stream));
-    CK(h, cudaMemcpyAsync(h->F[h->cur], seg + (size_t)a_cur * sb + popb, plane * es, cudaMemcpyDeviceToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->pops[h->cur], end_state, popb, cudaMemcpyDeviceToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->F[h->cur], end_state + popb, plane * es, cudaMemcpyDeviceToDevice, h->stream));
     h->prev_valid = false;
   }
   if (!dJdT0) {
     CK(h, cudaStreamSynchronize(h->stream));
+    *J = *h->h_scalar;
     return LBRB_OK;
   }
   // ---- backward pass
   const size_t lp = NPOP * plane;  // one lambda population set (doubles)
-  if (!h->adj_lam && cudaMalloc((void**)&h->adj_lam, (4 * lp + plane) * sizeof(double)) != cudaSuccess)
+  if (!h->adj_lam && cudaMalloc((void**)&h->adj_lam, (4 * lp + 2 * plane) * sizeof(double)) != cudaSuccess)
     return fail(h, LBRB_ERR_NOMEM, "adjoint lambda");
-  if (!h->adj_lT && cudaMalloc((void**)&h->adj_lT, plane * sizeof(long long)) != cudaSuccess)
+  if (!h->adj_lT && cudaMalloc((void**)&h->adj_lT, 2 * plane * sizeof(long long)) != cudaSuccess)
     return fail(h, LBRB_ERR_NOMEM, "adjoint lambda T");
   double* lam[2][2] = {{h->adj_lam, h->adj_lam + lp}, {h->adj_lam + 2 * lp, h->adj_lam + 3 * lp}};
-  double* lF = h->adj_lam + 4 * lp;
-  CK(h, cudaMemsetAsync(h->adj_lam, 0, (4 * lp + plane) * sizeof(double), h->stream));
-  CK(h, cudaMemsetAsync(h->adj_lT, 0, plane * sizeof(long long), h->stream));
-  int lc = 0;  // lam[lc] holds the adjoint of the current state
+  double* lF[2] = {h->adj_lam + 4 * lp, h->adj_lam + 4 * lp + plane};
+  long long* lT[2] = {h->adj_lT, h->adj_lT + plane};
+  CK(h, cudaMemsetAsync(h->adj_lam, 0, (4 * lp + 2 * plane) * sizeof(double), h->stream));
+  CK(h, cudaMemsetAsync(h->adj_lT, 0, 2 * plane * sizeof(long long), h->stream));
+  int lc = 0, fc = 0;  // lam[lc]: adjoint of the current state; lF[fc]: lambda F of the next step
+  auto scatter = [&](int s, long long* acc) -> cudaError_t {
+    const int oi = obs_at[s];
+    if (oi < 0) return cudaSuccess;
+    const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
+    return launch_adj_obs_scatter(ob, ob + nob, h->adj_res + (size_t)oi * nob, nob, nx, ny, pitch, acc, h->stream);
+  };
+  auto unscatter = [&](int s, long long* acc) -> cudaError_t {
+    const int oi = obs_at[s];
+    if (oi < 0) return cudaSuccess;
+    const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
+    return launch_adj_obs_clear(ob, ob + nob, nob, nx, ny, pitch, acc, h->stream);
+  };
   for (int c = nchk - 1; c >= 0; c--) {
-    const int s0 = c * K, s1 = std::min(s0 + K, nsteps);
-    // recompute the segment: slot i holds the input state of step s0+1+i
-    CK(h, cudaMemcpyAsync(seg, chk + (size_t)c * sb, sb, cudaMemcpyDeviceToDevice, h->stream));
-    for (int i = 0; i + 1 < s1 - s0; i++)
-      CK(h, launch_fwd(seg + (size_t)i * sb, seg + (size_t)(i + 1) * sb, 0));
-    for (int s = s1; s > s0; s--) {
+    const int s0 = c * K, len = std::min(K, nsteps - s0), s1 = s0 + len;
+    // recompute the segment's states (the last segment kept them)
+    if (c < nchk - 1)
+      for (int i = 0; i + 1 < len; i++) CK(h, launch_fwd(state_in(c, i), seg + (size_t)(i + 1) * sb, 0));
+    int s = s1;
+    while (s > s0) {
       const int i = s - s0 - 1;
-      const char* st = seg + (size_t)i * sb;
-      const int oi = obs_at[s];
-      if (oi >= 0) {
-        const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
-        CK(h, launch_adj_obs_scatter(ob, ob + nob, h->adj_res + (size_t)oi * nob, nob, nx, ny, pitch,
-                                     h->adj_lT, h->stream));
+      if (s - 1 > s0) {
+        // steps s and s-1 in one launch
+        CK(h, scatter(s, lT[0]));
+        CK(h, scatter(s - 1, lT[1]));
+        auto pair = [&](int variant) {
+          return launch_adjoint_pair(f32, variant, state_in(c, i), state_in(c, i - 1), lam[lc][0], lam[lc][1],
+                                     lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc], lF[fc ^ 1],
+                                     obs_at[s] >= 0 ? lT[0] : nullptr, obs_at[s - 1] >= 0 ? lT[1] : nullptr,
+                                     nx, ny, pitch, plane, om, omg, ng, T0ref, h->p.Tup, h->p.Tdown,
+                                     h->stream);
+        };
+        if (h->adj_pair_variant < 0) {
+          // launch variants of the pair kernel, timed on this pair: each
+          // writes the same values into the same outputs from unchanged inputs
+          cudaEvent_t ea, eb;
+          CK(h, cudaEventCreate(&ea));
+          CK(h, cudaEventCreate(&eb));
+          float best = 1e30f;
+          int bv = 0;
+          for (int v = 0; v < adjoint_pair_variants(); v++) {
+            CK(h, pair(v));
+            CK(h, cudaEventRecord(ea, h->stream));
+            CK(h, pair(v));
+            CK(h, cudaEventRecord(eb, h->stream));
+            CK(h, cudaEventSynchronize(eb));
+            float ms = 0.f;
+            CK(h, cudaEventElapsedTime(&ms, ea, eb));
+            if (ms < best) best = ms, bv = v;
+          }
+          cudaEventDestroy(ea);
+          cudaEventDestroy(eb);
+          h->adj_pair_variant = bv;
+        }
+        CK(h, pair(h->adj_pair_variant));
+        CK(h, unscatter(s, lT[0]));
+        CK(h, unscatter(s - 1, lT[1]));
+        lc ^= 1;
+        fc ^= 1;
+        s -= 2;
+      } else {
+        const char* st = state_in(c, i);
+        CK(h, scatter(s, lT[0]));
+        CK(h, launch_adjoint_step(f32, st, st + NPOP * plane * es, st + 2 * NPOP * plane * es,
+                                  lam[lc][0], lam[lc][1], lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc],
+                                  obs_at[s] >= 0 ? lT[0] : nullptr, nx, ny, pitch, plane, om, omg, ng,
+                                  T0ref, h->p.Tup, h->p.Tdown, h->stream));
+        CK(h, unscatter(s, lT[0]));
+        lc ^= 1;
+        s -= 1;
       }
-      CK(h, launch_adjoint_step(f32, st, st + NPOP * plane * es, st + 2 * NPOP * plane * es,
-                                lam[lc][0], lam[lc][1], lam[lc ^ 1][0], lam[lc ^ 1][1], lF,
-                                oi >= 0 ? h->adj_lT : nullptr, nx, ny, pitch, plane, om, omg, ng,
-                                T0ref, h->p.Tup, h->p.Tdown, h->stream));
-      lc ^= 1;
     }
   }
-  CK(h, launch_adj_initial(lam[lc][1], lF, nx, ny, pitch, plane, ng, h->adj_T0, h->stream));
+  CK(h, launch_adj_initial(lam[lc][1], lF[fc], nx, ny, pitch, plane, ng, h->adj_T0, h->stream));
   CK(h, cudaMemcpyAsync(dJdT0, h->adj_T0, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
+  *J = *h->h_scalar;
   return LBRB_OK;
 }
 

@@ -56,6 +56,16 @@ cudaError_t launch_adjoint_step(bool fp32, const void* fsrc, const void* gsrc, c
                                 double* lg_in, double* lF, long long* lT, int nx, int ny, int pitch,
                                 size_t plane, double omega, double omegag, double gbeta, double T0,
                                 double Tup, double Tdown, cudaStream_t s);
+int adjoint_pair_variants();
+cudaError_t launch_misfit(const double* res, long n, double* out, cudaStream_t s);
+cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, const void* state_b,
+                                const double* lf_out, const double* lg_out, double* lf_in,
+                                double* lg_in, double* lF_in, double* lF_out, const long long* lT_a,
+                                const long long* lT_b, int nx, int ny, int pitch, size_t plane,
+                                double omega, double omegag, double gbeta, double T0, double Tup,
+                                double Tdown, cudaStream_t s);
+cudaError_t launch_adj_obs_clear(const double* ox, const double* oy, int nobs, int nx, int ny, int pitch,
+                                 long long* acc, cudaStream_t s);
 cudaError_t launch_adj_obs_scatter(const double* ox, const double* oy, const double* res, int nobs,
                                    int nx, int ny, int pitch, long long* acc, cudaStream_t s);
 cudaError_t launch_obs_residual(const void* T, bool fp32, int nx, int ny, int pitch, const double* ox,

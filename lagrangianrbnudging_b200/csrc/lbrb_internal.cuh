@@ -192,12 +192,14 @@ struct Handle {
   double* adj_lam = nullptr;         // 2 x 18 planes + lambda F plane
   long long* adj_lT = nullptr;       // fixed-point lambda T plane
   double* adj_T0 = nullptr;          // [ny*nx] initial temperature / gradient
+  int adj_pair_variant = -1;         // launch variant of the pair kernel (-1: tune at first use)
   // scratch / staging
   void* staging = nullptr;
   size_t staging_bytes = 0;
   double* red = nullptr;    // reduction partials
   unsigned* dflags = nullptr;
   unsigned* h_flags = nullptr;
+  double* h_scalar = nullptr;  // pinned: one device scalar read back (the misfit)
 };
 
 }  // namespace lbrb
