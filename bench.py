@@ -383,6 +383,8 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     })
     if world == 1 and not args.no_adjoint:
         out["adjoint"] = run_adjoint_bench(lb, torch, device)
+    if world == 1 and not args.no_nudging:
+        out["nudging"] = run_nudging_bench(lb, torch, device, args.nudging_steps)
     if world == 1 and not args.no_ensemble:
         out["ensemble"] = run_ensemble_bench(lb, torch, device, args.ensemble_steps)
     if e2e_ms is not None:
@@ -494,6 +496,88 @@ def run_adjoint_check(lb, torch, device: int, ndir: int = 64, h: float = 1e-6) -
             "directions": ndir, "h": h, "J_fp64": J, "J_fp32": J32,
             "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)),
             "fp32_grad_rel_l2_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))}
+
+
+# ------------------------------------------------------------- nudging twin
+NUD_NX, NUD_NY, NUD_RA, NUD_TRACERS, NUD_STEPS, NUD_CHUNK = 2048, 1024, 1e7, 1 << 14, 50000, 250
+NUD_ALPHAS = (0.01, 0.1, 1.0)
+
+
+def run_nudging_bench(lb, torch, device: int, steps: int = NUD_STEPS, chunk: int = NUD_CHUNK) -> dict:
+    """Twin experiment: run A (seed A, 2^14 tracers) records T along the
+    trajectories every step; runs from seed B relax T toward those records at
+    the recorded positions (bilinear, alpha in {0.01, 0.1, 1} per step), beside
+    a free run (alpha = 0) from seed B.  All FP32-shifted populations, FP64
+    positions; the L2 error of T against run A is sampled along the way."""
+    base = lb.closure(NUD_NX, NUD_NY, Ra=NUD_RA, Pr=1.0, U=0.1)
+    seed_a, seed_b = 1001, 2002
+    rng = np.random.default_rng(seed_a)
+    n = NUD_TRACERS
+    x = rng.uniform(0.5, NUD_NX + 0.5, n)
+    y = rng.uniform(1.0, NUD_NY, n)
+    truth = lb.Run(**base, precision="fp32", nprtcl=n, noutconfig=1, record_slots=chunk + 1,
+                   device=device)
+    truth.init_conduction(seed_a, 1e-3)
+    m = truth.get_moments()
+    truth.set_particles(np.arange(n, dtype=np.int32), x, y, bilinear_np(m["u"], x, y),
+                        bilinear_np(m["v"], x, y), np.zeros(n, np.int32), np.zeros(n))
+    runs = {}
+    for a in (0.0,) + NUD_ALPHAS:
+        kw = dict(base, precision="fp32", device=device)
+        if a > 0:
+            kw.update(nudge="bilinear", alpha=a, nobs=n)
+        r = lb.Run(**kw)
+        r.init_conduction(seed_b, 1e-3)
+        runs[a] = r
+    stream = torch.cuda.Stream()
+    ms = {a: 0.0 for a in runs}
+    ms_truth = 0.0
+    samples = {a: [] for a in runs}
+    sample_every = max(steps // 20, chunk)
+
+    def l2(ra, rb):
+        ta = ra.get_moments()["T"]
+        tb = rb.get_moments()["T"]
+        return float(np.sqrt(np.mean((tb - ta) ** 2)))
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for r in [truth, *runs.values()]:
+        r.set_stream(stream.cuda_stream)
+    done = 0
+    while done < steps:
+        c = min(chunk, steps - done)
+        e0.record(stream)
+        truth.step(c)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_truth += e0.elapsed_time(e1)
+        st, buf = truth.drain_records_array()
+        ox, oy, oT = buf[:, 0, :], buf[:, 1, :], buf[:, 8, :]
+        for a, r in runs.items():
+            if a > 0:
+                r.nudge_obs(int(st[0]), ox, oy, oT)
+            e0.record(stream)
+            r.step(c)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms[a] += e0.elapsed_time(e1)
+        done += c
+        if done % sample_every == 0 or done == steps:
+            for a, r in runs.items():
+                samples[a].append((done, round(l2(truth, r), 6)))
+    for r in [truth, *runs.values()]:
+        r.set_stream(None)
+    nodes = NUD_NX * NUD_NY
+    out = {"grid": f"{NUD_NX}x{NUD_NY}", "Ra": NUD_RA, "tracers": n, "steps": steps,
+           "obs": "run A's records (x, y, T) every step, fed in chunks of %d steps" % chunk,
+           "truth_mlups_with_records": round(nodes * steps / (ms_truth * 1e3), 1),
+           "free_run": {"l2_final": samples[0.0][-1][1], "l2": samples[0.0]},
+           "nudged": {str(a): {"l2_final": samples[a][-1][1], "l2": samples[a],
+                               "mlups": round(nodes * steps / (ms[a] * 1e3), 1)} for a in NUD_ALPHAS},
+           "metric": "L2 T-field error vs run A, sqrt(mean((T_B - T_A)^2))"}
+    for r in [truth, *runs.values()]:
+        r.close()
+    return out
 
 
 # ------------------------------------------------------------- ensemble
@@ -757,6 +841,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-nudging", action="store_true")
+    ap.add_argument("--nudging-steps", type=int, default=NUD_STEPS)
+    ap.add_argument("--nudging-only", action="store_true",
+                    help="only the nudging twin experiment")
     ap.add_argument("--ensemble-steps", type=int, default=ENS_STEPS)
     ap.add_argument("--ensemble-only", action="store_true",
                     help="only the ensemble section (the command used for ncu captures of ens_lb_kernel)")
@@ -783,6 +871,15 @@ def main():
     if args.lb_only:
         torch.cuda.set_device(0)
         print(json.dumps(run_lb_only(args, torch)), flush=True)
+        return
+    if args.nudging_only:
+        import lagrangianrbnudging_b200 as lb
+        from lagrangianrbnudging_b200 import build as b
+
+        b.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"mode": "nudging-only", **run_nudging_bench(lb, torch, 0, args.nudging_steps)}),
+              flush=True)
         return
     if args.ensemble_only:
         import lagrangianrbnudging_b200 as lb

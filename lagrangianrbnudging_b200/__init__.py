@@ -301,6 +301,17 @@ class Run:
             out[int(steps[r])] = d
         return out
 
+    def drain_records_array(self):
+        """All pending records as (steps[k], buf[k][field][nprtcl]), particles in id order."""
+        k = self.pending_records()
+        steps = np.empty(k, np.int32)
+        buf = np.empty((k, self.nrec, self.np))
+        if k == 0:
+            return steps, buf
+        got = C.c_int()
+        self._ck(lib().lbrb_record_drain(self.h, k, _ip(steps), _dp(buf), None, C.byref(got)))
+        return steps[: got.value], buf[: got.value]
+
     # ---- nudging
     def nudge_init(self, x, y, T, ids):
         x, y, T, ids = _f64(x), _f64(y), _f64(T), _i32(ids)
