@@ -431,44 +431,46 @@ def adjoint_problem(lb, device: int, seed: int = 31):
     return base, steps, ox, oy, oT, T0
 
 
-def run_adjoint_bench(lb, torch, device: int) -> dict:
+def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS) -> dict:
     base, steps, ox, oy, oT, T0 = adjoint_problem(lb, device)
+    keep = steps <= nsteps
+    steps, ox, oy, oT = steps[keep], ox[keep], oy[keep], oT[keep]
     with lb.Run(**base, precision="fp32", device=device) as w:
         w.adjoint_set_obs(steps, ox, oy, oT)
         stream = torch.cuda.Stream()
         w.set_stream(stream.cuda_stream)
         # warm-up at the window's own size: checkpoint and segment buffers,
         # launch-shape and pair-kernel autotuning happen here, untimed
-        w.adjoint_window(T0, ADJ_STEPS, ADJ_K, gradient=True)
+        w.adjoint_window(T0, nsteps, ADJ_K, gradient=True)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         ev[0].record(stream)
-        w.adjoint_window(T0, ADJ_STEPS, ADJ_K, gradient=False)
+        w.adjoint_window(T0, nsteps, ADJ_K, gradient=False)
         ev[1].record(stream)
         ev[2].record(stream)
-        J, grad = w.adjoint_window(T0, ADJ_STEPS, ADJ_K, gradient=True)
+        J, grad = w.adjoint_window(T0, nsteps, ADJ_K, gradient=True)
         ev[3].record(stream)
         # plain forward steps of the same grid, for the cost ratio
         w.init_conduction(1, 1e-3)
         w.step(10)
         ev[4].record(stream)
-        w.step(ADJ_STEPS)
+        w.step(nsteps)
         ev[5].record(stream)
         torch.cuda.synchronize()
         t_fwd_window = ev[0].elapsed_time(ev[1])
         t_adj = ev[2].elapsed_time(ev[3])
-        t_step = ev[4].elapsed_time(ev[5]) / ADJ_STEPS
+        t_step = ev[4].elapsed_time(ev[5]) / nsteps
         w.set_stream(None)
-    return {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": ADJ_STEPS, "checkpoint_every": ADJ_K,
+    return {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": nsteps, "checkpoint_every": ADJ_K,
             "observations": f"{ADJ_NOBS} tracers every {ADJ_EVERY} steps (seeded truth run)",
             "precision": "fp32 forward, fp64 adjoint", "J": J,
             "grad_norm": float(np.linalg.norm(grad)),
-            "adjoint_steps_per_s": round(ADJ_STEPS / (t_adj * 1e-3), 1),
+            "adjoint_steps_per_s": round(nsteps / (t_adj * 1e-3), 1),
             "ms_gradient_window": round(t_adj, 2), "ms_misfit_window": round(t_fwd_window, 2),
             "ms_forward_step": round(t_step, 5),
             # gradient (forward + recompute + backward) per window step, in plain forward steps
-            "cost_vs_forward_steps": round(t_adj / (ADJ_STEPS * t_step), 2),
+            "cost_vs_forward_steps": round(t_adj / (nsteps * t_step), 2),
             # the backward sweep alone (recompute + adjoint) per step, in plain forward steps
-            "backward_sweep_vs_forward_steps": round((t_adj - t_fwd_window) / (ADJ_STEPS * t_step), 2),
+            "backward_sweep_vs_forward_steps": round((t_adj - t_fwd_window) / (nsteps * t_step), 2),
             # gradient over function: the gradient window against the misfit window
             "gradient_over_misfit": round(t_adj / t_fwd_window, 2)}
 
@@ -564,7 +566,7 @@ def run_nudging_bench(lb, torch, device: int, steps: int = NUD_STEPS, chunk: int
         done += c
         if done % sample_every == 0 or done == steps:
             for a, r in runs.items():
-                samples[a].append((done, round(l2(truth, r), 6)))
+                samples[a].append((done, float(f"{l2(truth, r):.4g}")))
     for r in [truth, *runs.values()]:
         r.set_stream(None)
     nodes = NUD_NX * NUD_NY
@@ -619,11 +621,13 @@ def ensemble_members(lb, device: int, seed: int = 41):
     return members, desc
 
 
-def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS) -> dict:
+def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: int = -1) -> dict:
     members, desc = ensemble_members(lb, device)
     nodes = sum(nx * ny for nx, ny, _, _ in desc)
     out = {}
     with lb.Ensemble(members) as ens:
+        if variant >= 0:
+            ens.set_schedule(variant)
         stream = torch.cuda.Stream()
         ens.set_stream(stream.cuda_stream)
         ens.step(12)  # autotune + graph capture + warm-up
@@ -846,6 +850,11 @@ def main():
     ap.add_argument("--nudging-only", action="store_true",
                     help="only the nudging twin experiment")
     ap.add_argument("--ensemble-steps", type=int, default=ENS_STEPS)
+    ap.add_argument("--ensemble-variant", type=int, default=-1,
+                    help="fixed launch variant of the ensemble's fused phase (-1: autotune)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="only the adjoint window (the command used for ncu captures of the adjoint kernels)")
+    ap.add_argument("--adjoint-steps", type=int, default=ADJ_STEPS)
     ap.add_argument("--ensemble-only", action="store_true",
                     help="only the ensemble section (the command used for ncu captures of ens_lb_kernel)")
     ap.add_argument("--adjoint-check", action="store_true",
@@ -872,6 +881,15 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps(run_lb_only(args, torch)), flush=True)
         return
+    if args.adjoint_only:
+        import lagrangianrbnudging_b200 as lb
+        from lagrangianrbnudging_b200 import build as b
+
+        b.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"mode": "adjoint-only", **run_adjoint_bench(lb, torch, 0, args.adjoint_steps)}),
+              flush=True)
+        return
     if args.nudging_only:
         import lagrangianrbnudging_b200 as lb
         from lagrangianrbnudging_b200 import build as b
@@ -887,7 +905,8 @@ def main():
 
         b.build()
         torch.cuda.set_device(0)
-        print(json.dumps({"mode": "ensemble-only", **run_ensemble_bench(lb, torch, 0, args.ensemble_steps)}),
+        print(json.dumps({"mode": "ensemble-only",
+                          **run_ensemble_bench(lb, torch, 0, args.ensemble_steps, args.ensemble_variant)}),
               flush=True)
         return
     if args.adjoint_check:
