@@ -87,26 +87,7 @@ __device__ __forceinline__ void adj_pull(const AdjView<Real>& V, const Real* __r
   }
 }
 
-// The adjoint of one step at one node: from the adjoints of the node's
-// outputs (post-collision lfo(k), lgo(k); the next step's buoyancy lFo; the
-// observation term lt on T) to the adjoints of the values the node pulled
-// (outf(k, .), outg(k, .); anti-bounce-back folded in) and of the step's
-// buoyancy (lFin).  fsrc/gsrc/Fin: the state before the step.
-// Two passes over the directions: the first accumulates the adjoints of the
-// node's scalars (u, v, rho, T, F), the second forms the outputs; lfo and
-// lgo are read again there rather than held, which keeps the register count
-// (and so the number of resident warps) in reach of a latency-bound kernel.
-// The arithmetic uses explicit fused multiply-adds and one reciprocal of rho.
-template <int K>
-__device__ __forceinline__ double adj_cu(double u, double v, double upv, double umv) {
-  constexpr int cx = icx(K), cy = icy(K);
-  if constexpr (cx == 0 && cy == 0) return 0.0;
-  else if constexpr (cy == 0) return cx > 0 ? u : -u;
-  else if constexpr (cx == 0) return cy > 0 ? v : -v;
-  else if constexpr (cx == cy) return cx > 0 ? upv : -upv;
-  else return cx > 0 ? umv : -umv;
-}
-
+// compile-time loop over the directions
 template <int K, typename F>
 __device__ __forceinline__ void adj_for(F&& f) {
   if constexpr (K > 0) {
@@ -144,52 +125,74 @@ __device__ __forceinline__ AdjLoc adj_locals(const AdjView<Real>& V, const Real*
   return L;
 }
 
+// weighted moments of 9 adjoint values X_k: sum w_k X_k {1, cx, cy, cx^2,
+// cy^2, cx cy}, as tree sums over the D2Q9 directions
+struct AdjMom {
+  double m0, mx, my, mxx, myy, mxy;
+};
+
+template <typename LX>
+__device__ __forceinline__ AdjMom adj_moments(LX&& X) {
+  constexpr double w0 = w_of(0), w1 = w_of(1), w5 = w_of(5);
+  const double s13 = X(1) + X(3), d13 = X(1) - X(3);
+  const double s24 = X(2) + X(4), d24 = X(2) - X(4);
+  const double c57 = X(5) + X(7), c68 = X(6) + X(8);
+  const double e57 = X(5) - X(7), e68 = X(6) - X(8);
+  const double cs = c57 + c68;
+  AdjMom M;
+  M.mxx = fma(w1, s13, w5 * cs);
+  M.myy = fma(w1, s24, w5 * cs);
+  M.m0 = fma(w0, X(0), fma(w1, s13 + s24, w5 * cs));
+  M.mx = fma(w1, d13, w5 * (e57 - e68));
+  M.my = fma(w1, d24, w5 * (e57 + e68));
+  M.mxy = w5 * (c57 - c68);
+  return M;
+}
+
+// The adjoint of one step at one node: from the adjoints of the node's
+// outputs (post-collision lfo(k), lgo(k); the next step's buoyancy lFo; the
+// observation term lt on T) to the adjoints of the values the node pulled
+// (outf(k, .), outg(k, .); anti-bounce-back folded in) and of the step's
+// buoyancy (lFin).  L: the node's forward quantities at the step.
+// The equilibria and the Guo source depend on the populations only through
+// rho, u, v (and T), so the transposed Jacobian needs the adjoints only
+// through their six weighted moments (M for f, N for g):
+//   Phi = om r M + omg t N
+//   l_u = 3 Phi_x + 9u Phi_xx + 9v Phi_xy - 3u Phi_0 + 9 s F M_xy
+//   l_v = 3 Phi_y + 9u Phi_xy + 9v Phi_yy - 3v Phi_0 + s F (9 M_yy - 3 M_0)
+//   Q(X) = X_0 (1 - 1.5|u|^2) + 3(u X_x + v X_y) + 4.5(u^2 X_xx + 2uv X_xy + v^2 X_yy)
+//   l_rho = om Q(M) + lFo gb t - (l_u u + l_v v) / r,   l_T = omg Q(N) + lt + lFo gb r
+//   l_F = s (3 M_y - 3v M_0 + 9u M_xy + 9v M_yy) + l_v / (2r)
+//   out_f_k = (1 - om) lfo_k + l_rho + cx_k l_u / r + cy_k l_v / r
+//   out_g_k = (1 - omg) lgo_k + l_T
+// with s = 1 - om/2 (om = 1/tau, omg = 1/tau_g, gb = g beta).
 template <typename Real, typename LF, typename LG, typename OF, typename OG>
 __device__ __forceinline__ void adj_local(const AdjView<Real>& V, const AdjLoc& L, int j, LF&& lfo,
                                           LG&& lgo, double lFo, double lt, OF&& outf, OG&& outg,
                                           double& lFin) {
   const double r = L.r, t = L.t, u = L.u, v = L.v, F = L.F;
   const double rinv = 1.0 / r;
-  const double om = V.omega, omg = V.omegag, srcf = 1.0 - 0.5 * om;
-  const double usq15 = 1.5 * fma(u, u, v * v);
-  const double upv = u + v, umv = u - v, v3 = 3.0 * v, F9 = 9.0 * F;
-  // pass 1: adjoints of the scalars
-  double lu = 0.0, lv = 0.0, ldr = 0.0, ldT = 0.0, lF = 0.0, slP = 0.0, slS = 0.0;
-  adj_for<NPOP>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    constexpr double w = w_of(k);
-    constexpr int cx = icx(k), cy = icy(k);
-    const double cu = adj_cu<k>(u, v, upv, umv);
-    const double P = fma(cu, fma(4.5, cu, 3.0), -usq15);
-    const double lf = lfo(k), lg = lgo(k);
-    const double Aw = (om * w) * lf;   // lambda of df_eq, times w
-    const double Bw = (omg * w) * lg;  // lambda of dg_eq, times w
-    const double lP = fma(Aw, r, Bw * t);
-    const double lS = (srcf * w) * lf;
-    double lcu = lP * fma(9.0, cu, 3.0);
-    if constexpr (cy != 0) lcu = fma(lS, cy * F9, lcu);
-    if constexpr (cx == 1) lu += lcu;
-    if constexpr (cx == -1) lu -= lcu;
-    if constexpr (cy == 1) lv += lcu;
-    if constexpr (cy == -1) lv -= lcu;
-    slP += lP;
-    slS += lS;
-    const double onep = 1.0 + P;
-    ldr = fma(Aw, onep, ldr);
-    ldT = fma(Bw, onep, ldT);
-    // Guo source factor 3 (cy - v) + 9 (c.u) cy
-    double G;
-    if constexpr (cy == 0) G = -v3;
-    else G = fma(9.0 * cy, cu, 3.0 * cy - v3);
-    lF = fma(lS, G, lF);
-  });
-  lu = fma(-3.0 * u, slP, lu);
-  lv = fma(-3.0 * v, slP, fma(-3.0 * F, slS, lv));
-  lF = fma(lv * 0.5, rinv, lF);
-  ldr += fma(lFo * V.gbeta, t, -fma(lu, u, lv * v) * rinv);
-  ldT += fma(lFo * V.gbeta, r, lt);
+  const double om = V.omega, omg = V.omegag, sf = 1.0 - 0.5 * om;
+  const AdjMom M = adj_moments(lfo);
+  const AdjMom N = adj_moments(lgo);
+  const double al = om * r, be = omg * t;
+  const double P0 = fma(al, M.m0, be * N.m0), Px = fma(al, M.mx, be * N.mx);
+  const double Py = fma(al, M.my, be * N.my), Pxx = fma(al, M.mxx, be * N.mxx);
+  const double Pyy = fma(al, M.myy, be * N.myy), Pxy = fma(al, M.mxy, be * N.mxy);
+  const double sF = sf * F;
+  const double lu = fma(3.0, Px, fma(9.0 * u, Pxx, fma(9.0 * v, Pxy, fma(-3.0 * u, P0, 9.0 * sF * M.mxy))));
+  const double lv = fma(3.0, Py, fma(9.0 * u, Pxy, fma(9.0 * v, Pyy,
+                        fma(-3.0 * v, P0, sF * fma(9.0, M.myy, -3.0 * M.m0)))));
+  const double q15 = 1.0 - 1.5 * fma(u, u, v * v);
+  const double uu45 = 4.5 * u * u, vv45 = 4.5 * v * v, uv9 = 9.0 * u * v, u3 = 3.0 * u, v3 = 3.0 * v;
+  auto Q = [&](const AdjMom& X) {
+    return fma(X.m0, q15, fma(u3, X.mx, fma(v3, X.my, fma(uu45, X.mxx, fma(uv9, X.mxy, vv45 * X.myy)))));
+  };
+  const double ldr = fma(om, Q(M), fma(lFo * V.gbeta, t, -fma(lu, u, lv * v) * rinv));
+  const double ldT = fma(omg, Q(N), fma(lFo * V.gbeta, r, lt));
+  lFin = fma(sf, fma(3.0, M.my, fma(-v3, M.m0, fma(9.0 * u, M.mxy, 9.0 * v * M.myy))), 0.5 * lv * rinv);
   const double ljx = lu * rinv, ljy = lv * rinv;
-  // pass 2: outputs
+  // outputs
   double lgs[NPOP];
   adj_for<NPOP>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
@@ -215,7 +218,6 @@ __device__ __forceinline__ void adj_local(const AdjView<Real>& V, const AdjLoc& 
   }
 #pragma unroll
   for (int k = 0; k < NPOP; k++) outg(k, lgs[k]);
-  lFin = lF;
 }
 
 // transpose of the pull for one direction: the node's pulled adjoint of
