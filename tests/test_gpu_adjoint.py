@@ -70,3 +70,21 @@ def test_fp32_forward_adjoint_close_to_fp64(case):
     J32, g32 = gpu_window(c, "fp32", K=8)
     assert abs(J32 - J64) <= 1e-4 * J64
     assert np.linalg.norm(g32 - g64) <= 1e-3 * np.linalg.norm(g64)
+
+
+def test_autograd_wrapper_passes_gradcheck():
+    """torch.autograd.gradcheck (central differences, FP64) through the
+    C-ABI adjoint on a 16x8 window of 12 steps"""
+    import torch
+    from tests.adjoint_function import WindowMisfit
+
+    c = adjoint_case(seed=5, nx=16, ny=8, nsteps=12, every=3, nobs=12)
+    with lb.Run(**c["base"], precision="fp64") as r:
+        r.adjoint_set_obs(c["steps"], c["ox"], c["oy"], c["oT"])
+        T0 = torch.tensor(c["T0"], dtype=torch.float64, requires_grad=True)
+        assert torch.autograd.gradcheck(lambda t: WindowMisfit.apply(t, r, c["nsteps"], 4), (T0,),
+                                        eps=1e-6, atol=1e-9, rtol=1e-6)
+        J = WindowMisfit.apply(T0, r, c["nsteps"], 4)
+        J.backward()
+        _, g = r.adjoint_window(c["T0"], c["nsteps"], 4)
+        np.testing.assert_array_equal(T0.grad.numpy(), g)
