@@ -372,7 +372,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
                  "lb_frac": round(achieved64 / peak, 4),
                  "fp32_over_fp64": round(mlups / mlups64, 3),
                  "launch_shape": shape64},
-        "accuracy": {"nu_fp32": nu32, "nu_fp64": nu64,
+        "accuracy_end_of_timed_run": {"nu_fp32": nu32, "nu_fp64": nu64,
                      "nu_rel_err": abs(nu32 - nu64) / abs(nu64),
                      "ke_rel_err": abs(ke32 - ke64) / max(abs(ke64), 1e-300),
                      "note": f"after {K + W} steps from the same initial state"},
@@ -383,6 +383,8 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     })
     if world == 1 and not args.no_adjoint:
         out["adjoint"] = run_adjoint_bench(lb, torch, device)
+    if world == 1 and not args.no_accuracy:
+        out["accuracy"] = run_accuracy(lb, device)
     if world == 1 and not args.no_nudging:
         out["nudging"] = run_nudging_bench(lb, torch, device, args.nudging_steps)
     if world == 1 and not args.no_ensemble:
@@ -460,8 +462,10 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS) -> dict:
         t_adj = ev[2].elapsed_time(ev[3])
         t_step = ev[4].elapsed_time(ev[5]) / nsteps
         w.set_stream(None)
+    fd = adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir=8)
     return {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": nsteps, "checkpoint_every": ADJ_K,
             "observations": f"{ADJ_NOBS} tracers every {ADJ_EVERY} steps (seeded truth run)",
+            "fd_check": fd,
             "precision": "fp32 forward, fp64 adjoint", "J": J,
             "grad_norm": float(np.linalg.norm(grad)),
             "adjoint_steps_per_s": round(nsteps / (t_adj * 1e-3), 1),
@@ -475,29 +479,66 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS) -> dict:
             "gradient_over_misfit": round(t_adj / t_fwd_window, 2)}
 
 
-def run_adjoint_check(lb, torch, device: int, ndir: int = 64, h: float = 1e-6) -> dict:
-    """gradient of the FP64 forward against central differences (h = 1e-6) on
-    seeded random directions, and the FP32-forward gradient against the FP64 one"""
-    base, steps, ox, oy, oT, T0 = adjoint_problem(lb, device)
+def adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir, h=1e-6, seed=2024) -> dict:
+    """<gradient, d> of the FP64 adjoint against central differences (h) of the
+    FP64 forward on ndir seeded directions; FP32-forward gradient against it"""
     with lb.Run(**base, precision="fp64", device=device) as w:
         w.adjoint_set_obs(steps, ox, oy, oT)
-        J, g64 = w.adjoint_window(T0, ADJ_STEPS, ADJ_K)
-        rng = np.random.default_rng(2024)
+        J, g64 = w.adjoint_window(T0, nsteps, ADJ_K)
+        rng = np.random.default_rng(seed)
         errs = []
         for _ in range(ndir):
             d = rng.standard_normal(T0.shape)
-            Jp = w.adjoint_window(T0 + h * d, ADJ_STEPS, ADJ_K, gradient=False)
-            Jm = w.adjoint_window(T0 - h * d, ADJ_STEPS, ADJ_K, gradient=False)
+            Jp = w.adjoint_window(T0 + h * d, nsteps, ADJ_K, gradient=False)
+            Jm = w.adjoint_window(T0 - h * d, nsteps, ADJ_K, gradient=False)
             fd = (Jp - Jm) / (2 * h)
             ad = float(np.sum(g64 * d))
             errs.append(abs(fd - ad) / abs(ad))
     with lb.Run(**base, precision="fp32", device=device) as w:
         w.adjoint_set_obs(steps, ox, oy, oT)
-        J32, g32 = w.adjoint_window(T0, ADJ_STEPS, ADJ_K)
-    return {"mode": "adjoint-check", "grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": ADJ_STEPS,
-            "directions": ndir, "h": h, "J_fp64": J, "J_fp32": J32,
-            "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)),
+        J32, g32 = w.adjoint_window(T0, nsteps, ADJ_K)
+    return {"directions": ndir, "h": h, "fd_rel_err_max": float(max(errs)),
+            "fd_rel_err_median": float(np.median(errs)), "tolerance": 1e-4,
+            "J_fp64": J, "J_fp32": J32,
             "fp32_grad_rel_l2_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))}
+
+
+def run_adjoint_check(lb, torch, device: int, ndir: int = 64, h: float = 1e-6) -> dict:
+    """the adjoint configuration's full check: 64 seeded directions"""
+    base, steps, ox, oy, oT, T0 = adjoint_problem(lb, device)
+    return {"mode": "adjoint-check", "grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": ADJ_STEPS,
+            **adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, ADJ_STEPS, device, ndir, h)}
+
+
+# ------------------------------------------------------------- accuracy
+ACC_STEPS, ACC_EVERY = 8000, 100
+
+
+def run_accuracy(lb, device: int, steps: int = ACC_STEPS, every: int = ACC_EVERY) -> dict:
+    """FP32-shifted against FP64 (reference operation order) on the headline
+    grid from the same seeded state: time-averaged Nu and <u^2> over the
+    run (sampled every `every` steps) and the T-field error at its end."""
+    base = lb.closure(NX, NY, Ra=RA, Pr=PR, U=U)
+    res = {}
+    for prec in ("fp32", "fp64"):
+        with lb.Run(**base, precision=prec, device=device) as r:
+            r.init_conduction(SEED, 1e-3)
+            nus, kes = [], []
+            for _ in range(steps // every):
+                r.step(every)
+                nus.append(r.nusselt())
+                kes.append(r.energy()[0])
+            res[prec] = (np.array(nus), np.array(kes), r.get_moments()["T"])
+    n32, k32, T32 = res["fp32"]
+    n64, k64, T64 = res["fp64"]
+    dT = T32 - T64
+    return {"grid": f"{NX}x{NY}", "steps": steps, "sampled_every": every,
+            "nu_avg_fp32": float(n32.mean()), "nu_avg_fp64": float(n64.mean()),
+            "nu_avg_rel_err": float(abs(n32.mean() - n64.mean()) / abs(n64.mean())),
+            "nu_final_rel_err": float(abs(n32[-1] - n64[-1]) / abs(n64[-1])),
+            "u2_avg_rel_err": float(abs(k32.mean() - k64.mean()) / abs(k64.mean())),
+            "T_max_abs_err": float(np.abs(dT).max()), "T_l2_err": float(np.sqrt(np.mean(dT ** 2))),
+            "bar": "time-averaged Nu within 0.5% of FP64"}
 
 
 # ------------------------------------------------------------- nudging twin
@@ -846,6 +887,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-nudging", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--nudging-steps", type=int, default=NUD_STEPS)
     ap.add_argument("--nudging-only", action="store_true",
                     help="only the nudging twin experiment")

@@ -33,6 +33,9 @@ TRAJ_CASES = {
                           inertial=True, taulag=50.0, beta=0.1, nsteps=200, noutconfig=50),
     "traj_wide": dict(nx=136, ny=20, Ra=3e5, U=0.1, seed=21, noise=2e-2, nprtcl=300,
                       inertial=True, taulag=30.0, beta=0.1, nsteps=120, noutconfig=40),
+    # the 1000-step window: f, g, u, T and every record bit for bit
+    "traj_long": dict(nx=64, ny=32, Ra=1e6, U=0.1, seed=31, noise=2e-2, nprtcl=128,
+                      inertial=True, taulag=40.0, beta=0.1, nsteps=1000, noutconfig=250),
 }
 
 # runs of the host program against the reference's own scratch / restart paths

@@ -74,20 +74,18 @@ def make_nudge(name: str) -> dict:
     return z
 
 
-def main():
-    for name in cases.TRAJ_CASES:
-        z = make_traj(name)
-        np.savez_compressed(cases.golden_path(name), **z)
-        print("wrote", cases.golden_path(name))
-    for name in cases.SCRATCH_TRAJ_CASES:
-        z = make_scratch(name)
-        np.savez_compressed(cases.golden_path(name), **z)
-        print("wrote", cases.golden_path(name))
-    for name in cases.NUDGE_CASES:
-        z = make_nudge(name)
-        np.savez_compressed(cases.golden_path(name), **z)
-        print("wrote", cases.golden_path(name))
+def main(only=()):
+    """all fixtures, or only the named ones (command-line arguments)"""
+    makers = [(cases.TRAJ_CASES, make_traj), (cases.SCRATCH_TRAJ_CASES, make_scratch),
+              (cases.NUDGE_CASES, make_nudge)]
+    for table, make in makers:
+        for name in table:
+            if only and name not in only:
+                continue
+            z = make(name)
+            np.savez_compressed(cases.golden_path(name), **z)
+            print("wrote", cases.golden_path(name))
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))
