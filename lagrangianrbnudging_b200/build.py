@@ -71,8 +71,12 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     os.replace(tmp, LIB)
     # the host program, linked against the library next to it
     tmp = HOST.with_suffix(".tmp")
-    subprocess.run(["gcc", "-std=c99", "-O2", "-Wall", "-o", str(tmp), str(PKG / "host" / "lbrb_host.c"),
-                    f"-L{PKG}", "-llbrb", "-Wl,-rpath,$ORIGIN", "-lm"], check=True)
+    import shutil
+
+    cuda_inc = Path(shutil.which(nvcc()) or nvcc()).resolve().parent.parent / "include"
+    subprocess.run(["gcc", "-std=gnu99", "-O2", "-Wall", f"-I{cuda_inc}", "-o", str(tmp),
+                    str(PKG / "host" / "lbrb_host.c"), f"-L{PKG}", "-llbrb", "-Wl,-rpath,$ORIGIN",
+                    "-lm", "-ldl"], check=True)
     os.replace(tmp, HOST)
     return LIB
 

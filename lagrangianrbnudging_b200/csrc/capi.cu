@@ -559,6 +559,7 @@ int lbrb_get_poststream(lbrb_t* h, double* f, double* g, int layout) {
 
 int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
+  NvtxRange nvtx("lbrb_step");
   if (n == 0) return LBRB_OK;
   if (!h->moments_valid)
     return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
@@ -746,6 +747,7 @@ static int grow(lbrb_t* h, void** p, size_t* have, size_t need) {
 // an odd leftover.  Results do not depend on K.
 int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* J, double* dJdT0) {
   if (!h || !T0 || nsteps < 1 || K < 1 || !J) return fail(h, LBRB_ERR_ARG, "adjoint_window: bad arguments");
+  NvtxRange nvtx("lbrb_adjoint_window");
   if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE)
     return fail(h, LBRB_ERR_UNSUPPORTED, "adjoint_window: Dirichlet walls without nudging only");
   if (!h->adj_obs) return fail(h, LBRB_ERR_STATE, "adjoint_window: no observations set");

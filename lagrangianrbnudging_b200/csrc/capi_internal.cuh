@@ -6,7 +6,17 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "lbrb_internal.cuh"
+
+namespace lbrb {
+// an NVTX range over a C-ABI call (free when no tool is attached)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+}  // namespace lbrb
 
 namespace lbrb {
 cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, int shape,

@@ -437,6 +437,7 @@ int lbrb_ensemble_get_timing(lbrb_ensemble_t* e, double* ms, int* launches, int 
 
 int lbrb_ensemble_step(lbrb_ensemble_t* e, int n) {
   if (!e || n < 0) return efail(e, LBRB_ERR_ARG, "ensemble_step: bad arguments");
+  NvtxRange nvtx("lbrb_ensemble_step");
   if (n == 0) return LBRB_OK;
   for (size_t i = 0; i < e->m.size(); i++) {
     const lbrb_t* h = e->m[i];

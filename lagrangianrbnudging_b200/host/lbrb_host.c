@@ -43,6 +43,8 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/lbrb.h"
 
 #define NPOP 9
@@ -376,6 +378,13 @@ static void prtcl_dump(lbrb_t *h, const cfg_t *c, int istep) {
 static void evolution(lbrb_t *h, const cfg_t *c, FILE *f, int istep) {
   double ke = 0, tm = 0;
   (void)c;
+  /* NaN/Inf sentinel over the populations at every evolution line */
+  const int fin = lbrb_check_finite(h);
+  if (fin == LBRB_ERR_NONFINITE) {
+    fprintf(stderr, "lbrb_host: non-finite populations at step %d\n", istep);
+    exit(7);
+  }
+  if (fin != LBRB_OK) die("lbrb_check_finite", h);
   CALL(h, lbrb_energy(h, &ke, &tm));
   fprintf(f, "%d %e %e\n", istep, ke, tm);
   fflush(f);
@@ -624,9 +633,12 @@ int main(int argc, char **argv) {
     }
     int target = next_event(&c, istep, last);
     if (target <= istep) target = istep + 1;
+    nvtxRangePushA("lbrb_host steps");
     CALL(h, lbrb_step(h, target - istep));
     istep = target;
     CALL(h, lbrb_sync(h));
+    nvtxRangePop();
+    nvtxRangePushA("lbrb_host output");
     if (np > 0) write_records(h, &c, nrec_fields);
     /* post-stream populations of this step (dumpfpre/dumpgpre) */
     if (istep == last || istep % 2000000 == 0) {
@@ -653,6 +665,7 @@ int main(int argc, char **argv) {
       dump_pops(h, &c, "confnew", "congnew", istep);
       if (np > 0) prtcl_dump(h, &c, istep);
     }
+    nvtxRangePop();
   }
   fclose(fevo);
   /* final dumps (temppart_dump.c:1763-1767): the reference's loop counter is

@@ -38,3 +38,24 @@ def test_nudging_toward_trajectory_records_tracks_the_truth():
     print(f"L2 error free {e_free:.3e} nudged {e_nud:.3e}")
     assert e_free > 0
     assert e_nud < 0.5 * e_free
+
+
+def test_bilinear_nudging_is_deterministic():
+    """the fixed-point innovation atomics make two identical nudged runs
+    bit-identical whatever the order in which the atomics land"""
+    build.build()
+    nx, ny, n = 96, 48, 2048
+    base = lb.closure(nx, ny, Ra=1e6, Pr=1.0, U=0.1)
+    rng = np.random.default_rng(8)
+    ox = rng.uniform(0.5, nx + 0.5, (50, n))
+    oy = rng.uniform(1.0, ny, (50, n))
+    oT = 0.5 - (oy - 0.5) / ny + 0.1 * rng.standard_normal((50, n))
+    out = []
+    for _ in range(2):
+        with lb.Run(**base, precision="fp32", nudge="bilinear", alpha=0.5, nobs=n) as r:
+            r.init_conduction(4, 1e-2)
+            r.nudge_obs(1, ox, oy, oT)
+            r.step(50)
+            out.append(r.get_populations())
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
