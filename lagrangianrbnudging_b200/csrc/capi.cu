@@ -761,7 +761,9 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   const int nchk = (nsteps + K - 1) / K;
   int rc;
   if ((rc = grow(h, &h->adj_chk, &h->adj_chk_bytes, (size_t)nchk * sb))) return rc;
-  if ((rc = grow(h, &h->adj_seg, &h->adj_seg_bytes, (size_t)(K + 1) * sb))) return rc;
+  // two segment buffers: the backward sweep of one segment reads one while
+  // the recompute of the segment before it fills the other
+  if ((rc = grow(h, &h->adj_seg, &h->adj_seg_bytes, 2 * (size_t)(K + 1) * sb))) return rc;
   if (!h->adj_T0 && cudaMalloc(&h->adj_T0, nn * sizeof(double)) != cudaSuccess)
     return fail(h, LBRB_ERR_NOMEM, "adjoint T0");
   CK(h, cudaMemcpyAsync(h->adj_T0, T0, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -774,7 +776,10 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   const int nob = h->adj_nobs;
   char* chk = (char*)h->adj_chk;
   char* seg = (char*)h->adj_seg;
-  auto state_in = [&](int c, int i) -> char* { return i == 0 ? chk + (size_t)c * sb : seg + (size_t)i * sb; };
+  // segment c's states live in buffer (nchk-1-c) % 2: the last segment, which
+  // the forward pass leaves in place, in buffer 0
+  auto segbuf = [&](int c) -> char* { return seg + (size_t)((nchk - 1 - c) & 1) * (K + 1) * sb; };
+  auto state_in = [&](int c, int i) -> char* { return i == 0 ? chk + (size_t)c * sb : segbuf(c) + (size_t)i * sb; };
   // the window's initial state in checkpoint 0 (pops + F), moments in buffer 0
   CK(h, launch_init_from_T0(h->adj_T0, chk, h->rho[0], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
                             h->T[0], chk + 2 * NPOP * plane * es, f32, nx, ny, pitch, plane, T0ref,
@@ -792,18 +797,19 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     h->lb_shape_ms = ms;
   }
   const int shape = h->lb_shape;
-  auto launch_fwd = [&](const char* src, char* dst, int write_rt) -> cudaError_t {
-    if (f32) return launch_lb_fp32(seg_view<float>(h, src, dst, write_rt), h->p.twall, shape, h->stream);
-    return launch_lb_fp64(seg_view<double>(h, src, dst, write_rt), h->p.twall, false, shape, h->stream);
+  auto launch_fwd_on = [&](const char* src, char* dst, int write_rt, cudaStream_t st) -> cudaError_t {
+    if (f32) return launch_lb_fp32(seg_view<float>(h, src, dst, write_rt), h->p.twall, shape, st);
+    return launch_lb_fp64(seg_view<double>(h, src, dst, write_rt), h->p.twall, false, shape, st);
   };
+  auto launch_fwd = [&](const char* src, char* dst, int write_rt) { return launch_fwd_on(src, dst, write_rt, h->stream); };
   // ---- forward pass: checkpoints, residuals
   char* end_state = nullptr;
   for (int c = 0; c < nchk; c++) {
     const int s0 = c * K, len = std::min(K, nsteps - s0);
     for (int i = 0; i < len; i++) {
       const int s = s0 + i + 1;
-      char* dst = (i + 1 < len) ? seg + (size_t)(i + 1) * sb
-                                : (c + 1 < nchk ? chk + (size_t)(c + 1) * sb : seg + (size_t)K * sb);
+      char* dst = (i + 1 < len) ? segbuf(c) + (size_t)(i + 1) * sb
+                                : (c + 1 < nchk ? chk + (size_t)(c + 1) * sb : segbuf(c) + (size_t)K * sb);
       const int oi = obs_at[s];
       CK(h, launch_fwd(state_in(c, i), dst, oi >= 0));
       if (oi >= 0) {
@@ -856,11 +862,35 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
     return launch_adj_obs_clear(ob, ob + nob, nob, nx, ny, pitch, acc, h->stream);
   };
+  // The recompute of segment c-1 runs on the second stream while the
+  // backward sweep of segment c runs on the handle's stream: the sweep is
+  // latency-bound and leaves HBM bandwidth for the recompute.  Events order
+  // each buffer's reuse (a recompute waits for the sweep that last read its
+  // buffer; a sweep waits for its recompute).
+  cudaEvent_t ev_fwd = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_bwd[2] = {nullptr, nullptr};
+  struct EvGuard {
+    cudaEvent_t* e[5];
+    ~EvGuard() {
+      for (cudaEvent_t* p : e)
+        if (*p) cudaEventDestroy(*p);
+    }
+  } ev_guard{{&ev_fwd, &ev_rec[0], &ev_rec[1], &ev_bwd[0], &ev_bwd[1]}};
+  for (cudaEvent_t* p : ev_guard.e) CK(h, cudaEventCreateWithFlags(p, cudaEventDisableTiming));
+  cudaStream_t rs = h->pstream;
+  CK(h, cudaEventRecord(ev_fwd, h->stream));
+  CK(h, cudaStreamWaitEvent(rs, ev_fwd, 0));
   for (int c = nchk - 1; c >= 0; c--) {
     const int s0 = c * K, len = std::min(K, nsteps - s0), s1 = s0 + len;
-    // recompute the segment's states (the last segment kept them)
-    if (c < nchk - 1)
-      for (int i = 0; i + 1 < len; i++) CK(h, launch_fwd(state_in(c, i), seg + (size_t)(i + 1) * sb, 0));
+    const int b = (nchk - 1 - c) & 1;
+    if (c >= 1) {
+      // recompute segment c-1 into the other buffer, after the sweep that read it
+      const int cp = c - 1, lenp = std::min(K, nsteps - cp * K);
+      CK(h, cudaStreamWaitEvent(rs, ev_bwd[b ^ 1], 0));
+      for (int i = 0; i + 1 < lenp; i++)
+        CK(h, launch_fwd_on(state_in(cp, i), segbuf(cp) + (size_t)(i + 1) * sb, 0, rs));
+      CK(h, cudaEventRecord(ev_rec[b ^ 1], rs));
+    }
+    if (c < nchk - 1) CK(h, cudaStreamWaitEvent(h->stream, ev_rec[b], 0));
     int s = s1;
     while (s > s0) {
       const int i = s - s0 - 1;
@@ -915,6 +945,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
         s -= 1;
       }
     }
+    CK(h, cudaEventRecord(ev_bwd[b], h->stream));
   }
   CK(h, launch_adj_initial(lam[lc][1], lF[fc], nx, ny, pitch, plane, ng, h->adj_T0, h->stream));
   CK(h, cudaMemcpyAsync(dJdT0, h->adj_T0, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
