@@ -20,7 +20,8 @@
 // fold the anti-bounce-back transpose, and push the results to the nodes the
 // forward pulled from (the transpose of streaming: bounce-back sends the
 // adjoint to the opposite population of the same node; populations that
-// stream out of the domain get zero).  Adjoints are FP64.
+// stream out of the domain get zero).  Adjoints are FP64.  adjoint_pair_kernel
+// runs two such steps per launch through shared memory (see there).
 #include <type_traits>
 
 #include "lbrb_internal.cuh"
@@ -37,7 +38,8 @@ struct AdjView {
   double* __restrict__ lf_in;     // lambda of the step's input (pushed)
   double* __restrict__ lg_in;
   double* __restrict__ lF;        // in: lambda F^{n+1}; out: lambda F^n (same node)
-  long long* __restrict__ lT;     // fixed-point lambda T of this step, or null; cleared
+  long long* __restrict__ lT;     // fixed-point lambda T of this step, or null (read only;
+                                  // adj_obs_clear_kernel clears it after the launch)
   int nx, ny, pitch;
   size_t plane;
   double omega, omegag, gbeta, T0, Tup, Tdown;

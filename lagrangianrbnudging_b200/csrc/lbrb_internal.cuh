@@ -139,7 +139,8 @@ struct Handle {
   void* T[2] = {nullptr, nullptr};
   void* uv[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
   int uvcur = 0, uvprev = 1;
-  // particle stream and the events that order it against the fused kernel
+  // second stream: particle kernels beside the fused kernel (when enabled) and
+  // the adjoint window's segment recompute; events order it against `stream`
   cudaStream_t pstream = nullptr;
   cudaEvent_t ev_lb = nullptr;       // fused kernel of the last queued step done
   cudaEvent_t ev_uv[3] = {nullptr, nullptr, nullptr};  // last particle kernel reading slot done
@@ -187,10 +188,10 @@ struct Handle {
   double* adj_res = nullptr;         // residuals [nobs_steps][nobs]
   void* adj_chk = nullptr;           // checkpoints: 19 planes each (pops + F)
   size_t adj_chk_bytes = 0;
-  void* adj_seg = nullptr;           // recomputed segment states
+  void* adj_seg = nullptr;           // two buffers of K+1 segment states
   size_t adj_seg_bytes = 0;
-  double* adj_lam = nullptr;         // 2 x 18 planes + lambda F plane
-  long long* adj_lT = nullptr;       // fixed-point lambda T plane
+  double* adj_lam = nullptr;         // 2 x 18 lambda planes (ping-pong) + 2 lambda F planes
+  long long* adj_lT = nullptr;       // 2 fixed-point lambda T planes (the steps of a pair)
   double* adj_T0 = nullptr;          // [ny*nx] initial temperature / gradient
   int adj_pair_variant = -1;         // launch variant of the pair kernel (-1: tune at first use)
   // scratch / staging
