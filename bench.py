@@ -732,11 +732,84 @@ def ref_params() -> dict:
 
 
 def build_reference_baseline():
-    """Build the reference's own temppart_dump for this workload (needs the
-    reference checkout; the binary travels in oracle/_ref)."""
+    """Build the reference's own temppart_dump for the production-trajectory
+    workload and for the 512x256 case (needs the reference checkout; the
+    binaries travel in oracle/_ref)."""
     from oracle import build as ob
 
+    ob.build_ref("temppart_dump", c0_ref_params(), C0_REF_TAG)
     return ob.build_ref("temppart_dump", ref_params(), REF_TAG)
+
+
+# ------------------------------------------------------ 512x256 tracer case
+C0_NX, C0_NY, C0_RA, C0_U, C0_TRACERS, C0_EVERY, C0_STEPS = 512, 256, 1e6, 0.1, 4096, 10, 20000
+C0_REF_TAG = "bench_c0"
+
+
+def c0_ref_params() -> dict:
+    nu = C0_U * C0_NY * np.sqrt(1.0 / C0_RA)
+    return dict(nx=C0_NX, ny=C0_NY, scratch=1, nstart=0, nsteps=1000000, nout=1000000,
+                noutconfig=C0_EVERY, relax=3.0 * nu + 0.5, relaxg=3.0 * nu + 0.5, Tup=-0.5, Tdown=0.5,
+                gravity=-(C0_U * C0_U) / C0_NY, Particle=1, Particle_scratch=0, Nprtcl=C0_TRACERS,
+                tracer=1, heavyprtcl=0, taulag=1.0, beta=0.0, Prtcl_Writefull=0)
+
+
+def run_config0(lb, torch, device: int, steps: int = C0_STEPS) -> dict:
+    """The reference's CPU-runnable case: 512x256, Ra=1e6, U=0.1, 4096 seeded
+    uniform tracers, records (x, y, u, v, T, ...) every 10 steps, drained to
+    the host every 1000 steps.  GPU FP32-shifted and FP64, and the
+    reference's own build on the host cores at several rank counts."""
+    base = lb.closure(C0_NX, C0_NY, Ra=C0_RA, Pr=1.0, U=C0_U)
+    rng = np.random.default_rng(SEED + 5)
+    n = C0_TRACERS
+    x = rng.uniform(0.5, C0_NX + 0.5, n)
+    y = rng.uniform(1.0, C0_NY, n)
+    ids = np.arange(n, dtype=np.int32)
+    out = {"grid": f"{C0_NX}x{C0_NY}", "tracers": n, "records_every": C0_EVERY, "steps": steps}
+    chunk = 1000
+    for prec in ("fp32", "fp64"):
+        with lb.Run(**base, precision=prec, nprtcl=n, noutconfig=C0_EVERY, record_slots=chunk // C0_EVERY + 2,
+                    device=device) as r:
+            r.init_conduction(SEED, 1e-3)
+            m = r.get_moments()
+            r.set_particles(ids, x, y, bilinear_np(m["u"], x, y), bilinear_np(m["v"], x, y),
+                            np.zeros(n, np.int32), np.zeros(n))
+            r.step(chunk)
+            r.sync()
+            r.drain_records_array()
+            stream = torch.cuda.Stream()
+            r.set_stream(stream.cuda_stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            dev_ms = 0.0
+            nrec = 0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(steps // chunk):
+                e0.record(stream)
+                r.step(chunk)
+                e1.record(stream)
+                r.sync()
+                dev_ms += e0.elapsed_time(e1)
+                nrec += len(r.drain_records_array()[0])
+            wall = time.perf_counter() - t0
+            r.set_stream(None)
+        out[prec] = {"mlups_device": round(C0_NX * C0_NY * steps / (dev_ms * 1e3), 1),
+                     "mlups_with_record_drains": round(C0_NX * C0_NY * steps / (wall * 1e6), 1),
+                     "records": nrec}
+    cpu = {}
+    exe = ROOT / "oracle" / "_ref" / C0_REF_TAG / "temppart_dump"
+    cores = host_cores()
+    np_list = [p for p in (1, 2, 4, 8, 16, 32, 64) if p <= cores]
+    for p in np_list:
+        try:
+            res = run_reference(steps=200, warmup=5, ranks=p, time_cap=8.0, exe=exe, particles=(ids, x, y))
+            cpu[str(p)] = round(C0_NX * C0_NY / res["per_step_s"] / 1e6, 3)
+        except Exception as e:  # reported, never fatal
+            cpu[str(p)] = f"unavailable: {e}"
+    out["reference_cpu_mlups_by_ranks"] = cpu
+    out["reference_note"] = ("the reference's own temppart_dump (tracers, records every 10 steps, "
+                             "scratch tanh+rand initial state) timed from its per-step output line")
+    return out
 
 
 def ref_exe() -> Path:
@@ -757,21 +830,27 @@ def ref_ranks(cores: int) -> int:
     return p
 
 
-def run_reference(steps: int, warmup: int, ranks: int, time_cap: float) -> dict:
+def run_reference(steps: int, warmup: int, ranks: int, time_cap: float, exe: Path | None = None,
+                  particles=None) -> dict:
     """Run the reference on `ranks` processes; the per-step time comes from
     the wall-clock arrival of its per-step stdout line (temppart_dump.c:1698),
-    measured over steps warmup+1 .. warmup+steps, then the run is stopped."""
+    measured over steps warmup+1 .. warmup+steps, then the run is stopped.
+    exe: a reference build (default: the production-trajectory one);
+    particles: (ids, x, y) of its restart particle files."""
     import resource
 
-    exe = ref_exe()
+    exe = exe or ref_exe()
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing (built by __graft_entry__.build() where the reference is present)")
     wd = Path(tempfile.mkdtemp(prefix="lbrb_bench_ref_"))
     (wd / "Prtcl_Veldata1" / "Particles0.h5.d").mkdir(parents=True)
     (wd / "Tempfolder").mkdir()
-    ids, x, y, ptype, invtau = particle_setup(SEED + 1)
+    if particles is None:
+        ids, x, y, _, _ = particle_setup(SEED + 1)
+    else:
+        ids, x, y = particles
     ids.astype(np.int32).tofile(wd / "Prtcl_Veldata1" / "Particles0.h5.d" / "id.bin")
-    rec = np.zeros((NPRTCL, 8))
+    rec = np.zeros((len(ids), 8))
     rec[:, 0], rec[:, 1], rec[:, 4], rec[:, 5] = x, y, x, y
     rec.tofile(wd / "prtcl_dump0.in")
 
@@ -894,6 +973,8 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=ENS_STEPS)
     ap.add_argument("--ensemble-variant", type=int, default=-1,
                     help="fixed launch variant of the ensemble's fused phase (-1: autotune)")
+    ap.add_argument("--config0", action="store_true",
+                    help="the 512x256 tracer case on the GPU and the reference CPU build")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="only the adjoint window (the command used for ncu captures of the adjoint kernels)")
     ap.add_argument("--adjoint-steps", type=int, default=ADJ_STEPS)
@@ -922,6 +1003,14 @@ def main():
     if args.lb_only:
         torch.cuda.set_device(0)
         print(json.dumps(run_lb_only(args, torch)), flush=True)
+        return
+    if args.config0:
+        import lagrangianrbnudging_b200 as lb
+        from lagrangianrbnudging_b200 import build as b
+
+        b.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"mode": "config0", **run_config0(lb, torch, 0)}), flush=True)
         return
     if args.adjoint_only:
         import lagrangianrbnudging_b200 as lb
