@@ -435,6 +435,18 @@ int main(int argc, char **argv) {
     fprintf(stderr, "contin=1 is not supported\n");
     return 2;
   }
+  /* the run directory and its missing parents are created (mkdir -p) */
+  {
+    char path[1024];
+    snprintf(path, sizeof(path), "%s", c.dir);
+    for (char *q = path + 1; *q; q++)
+      if (*q == '/') {
+        *q = '\0';
+        if (mkdir(path, 0755) != 0 && errno != EEXIST) break;
+        *q = '/';
+      }
+    if (mkdir(path, 0755) != 0 && errno != EEXIST) { /* chdir below reports it */ }
+  }
   if (chdir(c.dir) != 0) { fprintf(stderr, "cannot enter %s\n", c.dir); return 2; }
   ensure_dir("Prtcl_Veldata1");
   ensure_dir("Tempfolder");
