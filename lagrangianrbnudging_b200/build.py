@@ -67,7 +67,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
             if verbose_ptxas:
                 sys.stderr.write(r.stderr)
     tmp = LIB.with_suffix(".so.tmp")
-    subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart", "-lpthread"], check=True)
     os.replace(tmp, LIB)
     # the host program, linked against the library next to it
     tmp = HOST.with_suffix(".tmp")

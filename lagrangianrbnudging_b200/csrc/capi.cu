@@ -9,8 +9,10 @@
 //   finished record into pinned host memory while the next steps run)
 // and returns without waiting; lbrb_sync() waits and reports device flags.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -43,6 +45,41 @@ static int ensure_staging(lbrb_t* h, size_t bytes) {
   if (e != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "staging allocation", e);
   h->staging_bytes = bytes;
   return LBRB_OK;
+}
+
+// Host copies out of the pinned record ring.  A large drain (hundreds of MB
+// at the production size) is split over host threads: one thread's memcpy
+// runs at a fraction of the host memory bandwidth.
+struct CopyJob {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
+static void parallel_copy(const std::vector<CopyJob>& jobs) {
+  size_t total = 0;
+  for (const CopyJob& j : jobs) total += j.bytes;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = std::min(hw, 16u);
+  if (total < ((size_t)32 << 20) || nt == 1) {
+    for (const CopyJob& j : jobs) std::memcpy(j.dst, j.src, j.bytes);
+    return;
+  }
+  // pieces of about total / (4 nt) bytes, at least 1 MB, handed out in order
+  const size_t piece = std::max(total / (4 * nt), (size_t)1 << 20);
+  std::vector<CopyJob> pieces;
+  for (const CopyJob& j : jobs)
+    for (size_t o = 0; o < j.bytes; o += piece)
+      pieces.push_back({(char*)j.dst + o, (const char*)j.src + o, std::min(piece, j.bytes - o)});
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    for (size_t i; (i = next.fetch_add(1)) < pieces.size();)
+      std::memcpy(pieces[i].dst, pieces[i].src, pieces[i].bytes);
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
+  work();
+  for (std::thread& t : pool) t.join();
 }
 
 extern "C" {
@@ -403,14 +440,16 @@ int lbrb_record_drain(lbrb_t* h, int max_records, int* steps, double* buf, int* 
   CK(h, cudaSetDevice(h->dev));
   const size_t per = (size_t)h->nrec_fields * h->np;
   int k = 0;
+  std::vector<CopyJob> jobs;
   while (k < max_records && h->rec_tail < h->rec_head) {
     const int slot = (int)(h->rec_tail % h->p.record_slots);
     CK(h, cudaEventSynchronize(h->ring_ev[slot]));
-    std::memcpy(buf + (size_t)k * per, h->h_ring + (size_t)slot * per, per * sizeof(double));
+    jobs.push_back({buf + (size_t)k * per, h->h_ring + (size_t)slot * per, per * sizeof(double)});
     steps[k] = h->h_ring_step[slot];
     h->rec_tail++;
     k++;
   }
+  parallel_copy(jobs);
   if (ids && h->np > 0) std::memcpy(ids, h->h_ids.data(), h->np * sizeof(int));
   if (n_drained) *n_drained = k;
   return LBRB_OK;
