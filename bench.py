@@ -444,6 +444,7 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS) -> dict:
         # warm-up at the window's own size: checkpoint and segment buffers,
         # launch-shape and pair-kernel autotuning happen here, untimed
         w.adjoint_window(T0, nsteps, ADJ_K, gradient=True)
+        pair_variant = w.adjoint_variant()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         ev[0].record(stream)
         w.adjoint_window(T0, nsteps, ADJ_K, gradient=False)
@@ -465,7 +466,7 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS) -> dict:
     fd = adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir=8)
     return {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": nsteps, "checkpoint_every": ADJ_K,
             "observations": f"{ADJ_NOBS} tracers every {ADJ_EVERY} steps (seeded truth run)",
-            "fd_check": fd,
+            "fd_check": fd, "pair_kernel_variant": pair_variant,
             "precision": "fp32 forward, fp64 adjoint", "J": J,
             "grad_norm": float(np.linalg.norm(grad)),
             "adjoint_steps_per_s": round(nsteps / (t_adj * 1e-3), 1),

@@ -43,6 +43,7 @@ EXPORTS = [
     "lbrb_ensemble_step", "lbrb_ensemble_sync", "lbrb_ensemble_set_stream",
     "lbrb_ensemble_nvariants", "lbrb_ensemble_set_schedule", "lbrb_ensemble_get_schedule",
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
+    "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
 ]
 
 
@@ -124,6 +125,9 @@ def lib() -> C.CDLL:
         "lbrb_ensemble_get_schedule": (C.c_int, [vp, ip, ip, ip, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_ensemble_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_ensemble_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
+        "lbrb_adjoint_variants": (C.c_int, []),
+        "lbrb_adjoint_set_variant": (C.c_int, [vp, C.c_int]),
+        "lbrb_adjoint_get_variant": (C.c_int, [vp, ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -326,6 +330,18 @@ class Run:
         self._ck(lib().lbrb_nudge_obs(self.h, int(first_step), x.shape[0], _dp(x), _dp(y), _dp(T)))
 
     # ---- adjoint
+    @staticmethod
+    def adjoint_variants() -> int:
+        return lib().lbrb_adjoint_variants()
+
+    def adjoint_set_variant(self, variant: int):
+        self._ck(lib().lbrb_adjoint_set_variant(self.h, int(variant)))
+
+    def adjoint_variant(self) -> int:
+        v = C.c_int()
+        self._ck(lib().lbrb_adjoint_get_variant(self.h, C.byref(v)))
+        return v.value
+
     def adjoint_set_obs(self, steps, x, y, T):
         steps = _i32(steps)
         x, y, T = _f64(np.atleast_2d(x)), _f64(np.atleast_2d(y)), _f64(np.atleast_2d(T))

@@ -281,20 +281,23 @@ struct AdjPairView {
   double* __restrict__ lF_out;          // lambda F^{n-1}
 };
 
-constexpr int ADJ_TX = 32;
-
-template <typename Real, int TY, int MINB>
-__global__ void __launch_bounds__(ADJ_TX * TY, MINB) adjoint_pair_kernel(const AdjPairView<Real> P) {
+// TX x TY tile, NT threads; the ring of (TX+2)(TY+2) nodes takes a second,
+// partial round of phase 1 when it has more nodes than the block threads
+// (tiles with (TX+2)(TY+2) == NT, e.g. 30x6 on 256 threads, measured slower
+// on B200: unaligned rows and more blocks)
+template <typename Real, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) adjoint_pair_kernel(const AdjPairView<Real> P) {
   extern __shared__ double sm[];
-  constexpr int HX = ADJ_TX + 2, HY = TY + 2, NH = HX * HY;
+  constexpr int HX = TX + 2, HY = TY + 2, NH = HX * HY;
+  static_assert(NT >= TX * TY, "one thread per tile node");
   const AdjView<Real>& V = P.a;
   const int nx = V.nx, ny = V.ny;
-  const int x0 = blockIdx.x * ADJ_TX, j0 = blockIdx.y * TY;
+  const int x0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   // the forward quantities of this thread's phase-2 node do not depend on
   // phase 1: their loads go out first and overlap it
-  const int tx = threadIdx.x % ADJ_TX, ty = threadIdx.x / ADJ_TX;
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   const int x = x0 + tx, j = j0 + ty;
-  const bool mine = x < nx && j < ny;
+  const bool mine = (int)threadIdx.x < TX * TY && x < nx && j < ny;
   AdjLoc L2{};
   double lt2 = 0.0;
   if (mine) {
@@ -510,20 +513,19 @@ __global__ void __launch_bounds__(1024) misfit_kernel(const double* __restrict__
 }
 
 // ---------------------------------------------------------------- launchers
-template <typename Real, int TY, int MINB>
+template <typename Real, int TX, int TY, int NT, int MINB>
 static cudaError_t launch_pair_t(const AdjPairView<Real>& P, cudaStream_t s) {
-  constexpr int NH = (ADJ_TX + 2) * (TY + 2);
+  constexpr int NH = (TX + 2) * (TY + 2);
   constexpr size_t smem = (size_t)(2 * NPOP + 1) * NH * sizeof(double);
-  static cudaError_t attr = cudaFuncSetAttribute(adjoint_pair_kernel<Real, TY, MINB>,
+  static cudaError_t attr = cudaFuncSetAttribute(adjoint_pair_kernel<Real, TX, TY, NT, MINB>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (attr != cudaSuccess) return attr;
-  dim3 grid((P.a.nx + ADJ_TX - 1) / ADJ_TX, (P.a.ny + TY - 1) / TY);
-  adjoint_pair_kernel<Real, TY, MINB><<<grid, ADJ_TX * TY, smem, s>>>(P);
+  dim3 grid((P.a.nx + TX - 1) / TX, (P.a.ny + TY - 1) / TY);
+  adjoint_pair_kernel<Real, TX, TY, NT, MINB><<<grid, NT, smem, s>>>(P);
   return cudaGetLastError();
 }
 
-// launch variants of the pair kernel: tile rows (TY, 32 columns) and min
-// blocks per SM
+// launch variants of the pair kernel: tile (TX x TY), threads, min blocks per SM
 constexpr int ADJ_NPAIR_VARIANTS = 4;
 int adjoint_pair_variants() { return ADJ_NPAIR_VARIANTS; }
 
@@ -552,10 +554,10 @@ cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, con
     P.lg_in = lg_in;
     P.lF_out = lF_out;
     switch (variant) {
-      case 1: return launch_pair_t<Real, 4, 6>(P, s);
-      case 2: return launch_pair_t<Real, 8, 2>(P, s);
-      case 3: return launch_pair_t<Real, 8, 3>(P, s);
-      default: return launch_pair_t<Real, 4, 4>(P, s);
+      case 1: return launch_pair_t<Real, 32, 4, 128, 6>(P, s);
+      case 2: return launch_pair_t<Real, 32, 8, 256, 2>(P, s);
+      case 3: return launch_pair_t<Real, 32, 8, 256, 3>(P, s);
+      default: return launch_pair_t<Real, 32, 4, 128, 4>(P, s);
     }
   };
   return fp32 ? go(0.f) : go(0.0);

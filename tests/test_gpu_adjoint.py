@@ -62,6 +62,19 @@ def test_checkpoint_interval_does_not_change_the_gradient(case):
     np.testing.assert_array_equal(g1, gall)
 
 
+def test_every_pair_kernel_variant_gives_the_same_gradient(case):
+    c = case
+    grads = []
+    for v in range(lb.Run.adjoint_variants()):
+        with lb.Run(**c["base"], precision="fp64") as r:
+            r.adjoint_set_variant(v)
+            r.adjoint_set_obs(c["steps"], c["ox"], c["oy"], c["oT"])
+            grads.append(r.adjoint_window(c["T0"], c["nsteps"], 8)[1])
+            assert r.adjoint_variant() == v
+    for g in grads[1:]:
+        np.testing.assert_array_equal(g, grads[0])
+
+
 def test_fp32_forward_adjoint_close_to_fp64(case):
     """FP32 shifted forward with FP64 adjoint accumulation: gradient within
     1e-3 (relative L2) of the FP64 one"""
