@@ -615,8 +615,11 @@ int lbrb_step(lbrb_t* h, int n) {
     int sh = h->p.launch_shape;
     float ms = 0.f;
     if (h->p.autotune && !refbox) {
-      if (f32) sh = tune_lb_fp32(make_view<float>(h, h->cur, h->cur ^ 1, h->uvcur, 0, 0), h->p.twall, h->stream, &ms);
-      else sh = tune_lb_fp64(make_view<double>(h, h->cur, h->cur ^ 1, h->uvcur, 0, 0), h->p.twall, h->stream, &ms);
+      // trials store u, v as the steps will (particles need them every step),
+      // into the slot the first step overwrites
+      const int tuv = h->np > 0 ? 3 - h->uvcur - h->uvprev : h->uvcur;
+      if (f32) sh = tune_lb_fp32(make_view<float>(h, h->cur, h->cur ^ 1, tuv, h->np > 0, 0), h->p.twall, h->stream, &ms);
+      else sh = tune_lb_fp64(make_view<double>(h, h->cur, h->cur ^ 1, tuv, h->np > 0, 0), h->p.twall, h->stream, &ms);
     }
     CK(h, cudaGetLastError());
     h->lb_shape = sh;

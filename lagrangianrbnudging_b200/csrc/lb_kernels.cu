@@ -114,15 +114,15 @@ cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStr
 
 // Autotuner: time every launch shape on this run's grid (CUDA events, `reps`
 // launches after one warm-up launch each) and return the fastest.  A trial
-// launch reads the current state and writes only the other population
-// buffer and the other F buffer, which the real step overwrites; moments
-// are not written.  Box-nudged FP64 steps update nud_term in place and are
-// not tuned (shape 0).
+// launch reads the current state and writes only buffers the real step
+// overwrites: the other population buffer, the other F buffer and, when the
+// caller's view stores u, v (runs with particles), the u, v slot of the next
+// step; rho and T are not written.  Box-nudged FP64 steps update nud_term in
+// place and are not tuned (shape 0).
 template <typename Real>
 static int tune(const LBView<Real>& Vin, int twall, bool refnudge, cudaStream_t s, int reps,
                 float* best_ms) {
-  LBView<Real> V = Vin;
-  V.write_uv = 0;
+  LBView<Real> V = Vin;  // u, v stores as the caller's view has them
   V.write_rt = 0;
   cudaEvent_t a, b;
   cudaEventCreate(&a);
@@ -169,10 +169,10 @@ cudaError_t launch_pull_fp32(const LBView<float>& V, int twall, void* outf, void
 }
 
 int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best_ms) {
-  return tune<double>(V, twall, false, s, 3, best_ms);
+  return tune<double>(V, twall, false, s, 6, best_ms);
 }
 int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_ms) {
-  return tune<float>(V, twall, false, s, 3, best_ms);
+  return tune<float>(V, twall, false, s, 6, best_ms);
 }
 
 }  // namespace lbrb
