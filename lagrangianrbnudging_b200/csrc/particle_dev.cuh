@@ -113,7 +113,9 @@ __device__ __forceinline__ void bilin_derivs(const PView<Real>& V, const Cell& c
 }
 
 // one particle of one step: interpolate, advance, record, wrap/reflect
-template <typename Real>
+// DERIVS = false: the run needs no Maxey-Riley derivative terms (beta == 0
+// and no full records), so the 4x4 derivative stencil is not compiled in
+template <typename Real, bool DERIVS = true>
 __device__ __forceinline__ void particle_update(const PView<Real>& V, int p) {
   const int n = V.np;
   double* X = V.P;
@@ -128,7 +130,7 @@ __device__ __forceinline__ void particle_update(const PView<Real>& V, int p) {
   const bool tracer = V.ptype[p] == LBRB_PTYPE_TRACER;
   const bool need_d = (!tracer && V.beta != 0.0) || (V.record && V.full);
   double dd[6] = {0, 0, 0, 0, 0, 0};
-  if (need_d) bilin_derivs(V, c, xx, yy, dd);
+  if (DERIVS && need_d) bilin_derivs(V, c, xx, yy, dd);
   double xn, yn, un, vn;
   if (tracer) {
     xn = xx + 1.5 * delta_t * tempup - 0.5 * delta_t * uold;

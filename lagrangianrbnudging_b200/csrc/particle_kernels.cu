@@ -20,17 +20,21 @@
 
 namespace lbrb {
 
-template <typename Real>
+template <typename Real, bool DERIVS>
 __global__ void __launch_bounds__(128) particle_kernel(const PView<Real> V) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= V.np) return;
-  particle_update(V, p);
+  particle_update<Real, DERIVS>(V, p);
 }
 
 template <typename Real>
 cudaError_t launch_particles_t(const PView<Real>& V, cudaStream_t s) {
   if (V.np <= 0) return cudaSuccess;
-  particle_kernel<Real><<<(V.np + 127) / 128, 128, 0, s>>>(V);
+  // the derivative stencil only where beta != 0 or full records need it
+  if (V.beta != 0.0 || V.full)
+    particle_kernel<Real, true><<<(V.np + 127) / 128, 128, 0, s>>>(V);
+  else
+    particle_kernel<Real, false><<<(V.np + 127) / 128, 128, 0, s>>>(V);
   return cudaGetLastError();
 }
 
