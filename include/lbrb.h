@@ -231,10 +231,11 @@ LBRB_API int lbrb_adjoint_set_obs(lbrb_t *h, int nobs_steps, const int *steps, i
  * ends at the end of the window; particles are not advanced. */
 LBRB_API int lbrb_adjoint_window(lbrb_t *h, const double *T0, int nsteps, int checkpoint_every,
                                  double *J, double *dJdT0);
-/* Launch variant of the two-step adjoint kernel (tile shape, threads, blocks
- * per SM), 0 .. lbrb_adjoint_variants()-1; -1 (the default): timed on the
- * first step pair of the next window and the fastest kept.  Every variant
- * gives the same gradient, bit for bit. */
+/* Launch variant of the two-step adjoint kernel, 0 .. lbrb_adjoint_variants()-1:
+ * 0-3 the tiled kernel (tile shape, threads, blocks per SM), 4 and up the
+ * marching kernel (rows per group, blocks per SM, register prefetch, waves).
+ * -1 (the default): timed on the first step pair of the next window and the
+ * fastest kept.  Every variant gives the same gradient, bit for bit. */
 LBRB_API int lbrb_adjoint_variants(void);
 LBRB_API int lbrb_adjoint_set_variant(lbrb_t *h, int variant);
 LBRB_API int lbrb_adjoint_get_variant(const lbrb_t *h, int *variant);

@@ -47,31 +47,43 @@ struct AdjView {
 
 constexpr double ADJ_FIX = 1099511627776.0;  // 2^40
 
+// the stored values the forward step pulls into node (x, j): fv[k], gv[k]
+// (bounce-back at the walls: f from the node's opposite population, g left
+// zero for the anti-bounce-back below)
 template <typename Real>
-__device__ __forceinline__ void adj_pull(const AdjView<Real>& V, const Real* __restrict__ fsrc,
-                                         const Real* __restrict__ gsrc, int j, int x, double* df,
-                                         double* dg) {
-  const int xl = (x == 0) ? V.nx - 1 : x - 1;
-  const int xr = (x == V.nx - 1) ? 0 : x + 1;
+__device__ __forceinline__ void adj_pull_raw(const Real* __restrict__ fsrc, const Real* __restrict__ gsrc,
+                                             int nx, int ny, int pitch, size_t plane, int j, int x,
+                                             Real* fv, Real* gv) {
+  const int xl = (x == 0) ? nx - 1 : x - 1;
+  const int xr = (x == nx - 1) ? 0 : x + 1;
 #pragma unroll
   for (int k = 0; k < NPOP; k++) {
     const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
     const int js = j - icy(k);
-    double fv, gv;
-    if (js < 0 || js >= V.ny) {
-      fv = (double)fsrc[(size_t)opp(k) * V.plane + (size_t)j * V.pitch + x];
-      gv = 0.0;
+    if (js < 0 || js >= ny) {
+      fv[k] = fsrc[(size_t)opp(k) * plane + (size_t)j * pitch + x];
+      gv[k] = Real(0);
     } else {
-      fv = (double)fsrc[(size_t)k * V.plane + (size_t)js * V.pitch + xs];
-      gv = (double)gsrc[(size_t)k * V.plane + (size_t)js * V.pitch + xs];
+      fv[k] = fsrc[(size_t)k * plane + (size_t)js * pitch + xs];
+      gv[k] = gsrc[(size_t)k * plane + (size_t)js * pitch + xs];
     }
+  }
+}
+
+// pulled values in the shifted form, walls applied
+template <typename Real>
+__device__ __forceinline__ void adj_shift_pulled(const AdjView<Real>& V, int j, const Real* fv,
+                                                 const Real* gv, double* df, double* dg) {
+#pragma unroll
+  for (int k = 0; k < NPOP; k++) {
+    const int js = j - icy(k);
     if constexpr (std::is_same<Real, double>::value) {
       // reference-order storage holds f, g themselves: go to the shifted form
-      df[k] = fv - w_of(k);
-      dg[k] = (js < 0 || js >= V.ny) ? 0.0 : gv - w_of(k) * V.T0;
+      df[k] = fv[k] - w_of(k);
+      dg[k] = (js < 0 || js >= V.ny) ? 0.0 : gv[k] - w_of(k) * V.T0;
     } else {
-      df[k] = fv;
-      dg[k] = gv;
+      df[k] = (double)fv[k];
+      dg[k] = (double)gv[k];
     }
   }
   // anti-bounce-back on the shifted form: dg_in = -dg_opp + 2 w (Twall - T0)
@@ -103,12 +115,12 @@ struct AdjLoc {
   double r, t, u, v, F;
 };
 
+// from the raw pulled values fv, gv and the step's buoyancy F at the node
 template <typename Real>
-__device__ __forceinline__ AdjLoc adj_locals(const AdjView<Real>& V, const Real* __restrict__ fsrc,
-                                             const Real* __restrict__ gsrc, const Real* __restrict__ Fin,
-                                             int j, int x) {
+__device__ __forceinline__ AdjLoc adj_locals_raw(const AdjView<Real>& V, const Real* fv, const Real* gv,
+                                                 Real Fnode, int j) {
   double df[NPOP], dg[NPOP];
-  adj_pull(V, fsrc, gsrc, j, x, df, dg);
+  adj_shift_pulled(V, j, fv, gv, df, dg);
   double dr = 0.0, dT = 0.0;
 #pragma unroll
   for (int k = 0; k < NPOP; k++) {
@@ -120,11 +132,20 @@ __device__ __forceinline__ AdjLoc adj_locals(const AdjView<Real>& V, const Real*
   AdjLoc L;
   L.r = 1.0 + dr;
   L.t = V.T0 + dT;
-  L.F = (double)Fin[(size_t)j * V.pitch + x];
+  L.F = (double)Fnode;
   const double rinv = 1.0 / L.r;
   L.u = jx * rinv;
   L.v = fma(0.5, L.F, jy) * rinv;
   return L;
+}
+
+template <typename Real>
+__device__ __forceinline__ AdjLoc adj_locals(const AdjView<Real>& V, const Real* __restrict__ fsrc,
+                                             const Real* __restrict__ gsrc, const Real* __restrict__ Fin,
+                                             int j, int x) {
+  Real fv[NPOP], gv[NPOP];
+  adj_pull_raw(fsrc, gsrc, V.nx, V.ny, V.pitch, V.plane, j, x, fv, gv);
+  return adj_locals_raw(V, fv, gv, Fin[(size_t)j * V.pitch + x], j);
 }
 
 // weighted moments of 9 adjoint values X_k: sum w_k X_k {1, cx, cy, cx^2,
@@ -354,6 +375,191 @@ __global__ void __launch_bounds__(NT, MINB) adjoint_pair_kernel(const AdjPairVie
   P.lF_out[o] = lFin;
 }
 
+// Marching form of the two steps.  The domain is cut into strips of 32
+// columns and groups of RB rows; a unit is one (strip, group).  Block b walks
+// down strip b % nstrips over one chunk of `chunk` consecutive groups (chunk
+// b / nstrips): the blocks of one chunk run together on neighbouring strips,
+// so the halo columns and the pushes across strip edges meet in L2.
+// Per unit, phase 1 computes step n's pulled adjoints of the group's next RB
+// rows (rows r+1 .. r+RB, 34 columns with the two halo columns) into a ring
+// of 2 RB + 2 rows in shared memory, and phase 2 computes step n-1 at rows
+// r .. r+RB-1 from the ring.  Rows r-1 and r come from the previous unit, or
+// from a prologue step (phase 1 alone, those two rows) where a run starts.
+// Phase 1 of one unit writes ring rows that phase 2 of the previous unit
+// does not read, so one barrier per unit orders them.  Each thread loads the
+// next unit's inputs (lambda^n and the state of its phase-1 node, the state
+// of its phase-2 node) into registers before computing the current unit, so
+// the loads are in flight during the FP64 arithmetic.  Results are those of
+// two adjoint_step_kernel launches, bit for bit.
+template <typename Real>
+struct MarchIn {
+  double lf[NPOP], lg[NPOP], lFo;  // lambda^n and lambda F^{n+1} at the phase-1 node
+  long long lt;                    // lambda T^n (fixed point)
+  Real fa[NPOP], ga[NPOP], Fa;     // state before step n, pulled into the phase-1 node
+  Real fb[NPOP], gb[NPOP], Fb;     // state before step n-1, pulled into the phase-2 node
+  long long ltb;                   // lambda T^{n-1}
+};
+
+template <int RB>
+struct MarchStep {
+  int u;     // unit
+  bool pro;  // prologue: phase 1 of rows r-1, r only
+};
+
+// PRE: the next unit's inputs go to registers before the current unit's
+// arithmetic (one block per SM: about 240 registers); without it the blocks
+// per SM (MINB) hide each other's loads.
+template <typename Real, int RB, int MINB, bool PRE>
+__global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjPairView<Real> P, int chunk) {
+  extern __shared__ double sm[];
+  constexpr int HX = 34, S = 2 * RB + 2;  // ring: S rows of HX columns, 2*NPOP+1 values
+  const AdjView<Real>& V = P.a;
+  const int nx = V.nx, ny = V.ny, pitch = V.pitch;
+  const size_t plane = V.plane;
+  const int ngroups = (ny + RB - 1) / RB;
+  const int nstrips = (nx + 31) / 32;
+  const int g0 = (blockIdx.x / nstrips) * chunk;
+  const int ub = (blockIdx.x % nstrips) * ngroups + g0;
+  const int ue = ub + min(chunk, ngroups - g0);
+  if (g0 >= ngroups) return;
+  const int t = threadIdx.x;
+  const int hx = t % HX, hy = t / HX;  // phase-1 node in the group
+  const int px = t % 32, py = t / 32;  // phase-2 node in the group
+  auto ring = [&](int v, int row, int col) -> double& { return sm[(v * S + row % S) * HX + col]; };
+  // node coordinates of a step for this thread (phase 1: xh, j1; phase 2: x2, j2)
+  auto coords = [&](const MarchStep<RB>& st, int& xh, int& j1, bool& a1, int& x2, int& j2, bool& a2) {
+    const int s = st.u / ngroups, r = (st.u % ngroups) * RB, x0 = 32 * s;
+    j1 = (st.pro ? r - RB : r) + 1 + hy;
+    xh = x0 - 1 + hx;
+    if (xh == -1) xh = nx - 1;
+    else if (xh == nx) xh = 0;
+    a1 = j1 >= 0 && j1 < ny && xh < nx && (!st.pro || hy >= RB - 2);
+    j2 = r + py;
+    x2 = x0 + px;
+    a2 = !st.pro && t < 32 * RB && j2 < ny && x2 < nx;
+  };
+  auto load = [&](const MarchStep<RB>& st, MarchIn<Real>& in) {
+    int xh, j1, x2, j2;
+    bool a1, a2;
+    coords(st, xh, j1, a1, x2, j2, a2);
+    if (a1) {
+      const size_t o = (size_t)j1 * pitch + xh;
+#pragma unroll
+      for (int k = 0; k < NPOP; k++) {
+        in.lf[k] = V.lf_out[(size_t)k * plane + o];
+        in.lg[k] = V.lg_out[(size_t)k * plane + o];
+      }
+      in.lFo = V.lF[o];
+      in.lt = V.lT ? V.lT[o] : 0ll;
+      adj_pull_raw(V.fsrc, V.gsrc, nx, ny, pitch, plane, j1, xh, in.fa, in.ga);
+      in.Fa = V.Fin[o];
+    }
+    if (a2) {
+      const size_t o = (size_t)j2 * pitch + x2;
+      adj_pull_raw(P.fsrc_b, P.gsrc_b, nx, ny, pitch, plane, j2, x2, in.fb, in.gb);
+      in.Fb = P.Fin_b[o];
+      in.ltb = P.lT_b ? P.lT_b[o] : 0ll;
+    }
+  };
+  auto next = [&](const MarchStep<RB>& st) {
+    if (st.pro) return MarchStep<RB>{st.u, false};
+    return MarchStep<RB>{st.u + 1, (st.u + 1) % ngroups == 0};  // a new strip starts with a prologue
+  };
+  auto phase1 = [&](int j1, const MarchIn<Real>& cur) {
+    const AdjLoc L = adj_locals_raw(V, cur.fa, cur.ga, cur.Fa, j1);
+    double lFin;
+    adj_local(
+        V, L, j1, [&](int k) { return cur.lf[k]; }, [&](int k) { return cur.lg[k]; }, cur.lFo,
+        (double)cur.lt * (1.0 / ADJ_FIX), [&](int k, double val) { ring(k, j1, hx) = val; },
+        [&](int k, double val) { ring(NPOP + k, j1, hx) = val; }, lFin);
+    ring(2 * NPOP, j1, hx) = lFin;
+  };
+  auto phase2 = [&](int j2, int x2, const MarchIn<Real>& cur) {
+    // output m of step n-1 at this node went to node (x2, j2) + c_m; at a
+    // wall it was bounced back into opp(m) here (f) or left the domain (g)
+    const int c = px + 1;
+    auto lfo = [&](int m) {
+      const int sj = j2 + icy(m);
+      return (sj < 0 || sj >= ny) ? ring(opp(m), j2, c) : ring(m, sj, c + icx(m));
+    };
+    auto lgo = [&](int m) {
+      const int sj = j2 + icy(m);
+      return (sj < 0 || sj >= ny) ? 0.0 : ring(NPOP + m, sj, c + icx(m));
+    };
+    const AdjLoc L = adj_locals_raw(V, cur.fb, cur.gb, cur.Fb, j2);
+    double lFin;
+    adj_local(
+        V, L, j2, lfo, lgo, ring(2 * NPOP, j2, c), (double)cur.ltb * (1.0 / ADJ_FIX),
+        [&](int k, double val) { adj_push_one(k, false, val, nx, ny, pitch, plane, j2, x2, P.lf_in); },
+        [&](int k, double val) { adj_push_one(k, true, val, nx, ny, pitch, plane, j2, x2, P.lg_in); },
+        lFin);
+    P.lF_out[(size_t)j2 * pitch + x2] = lFin;
+  };
+  auto compute = [&](const MarchStep<RB>& st, const MarchIn<Real>& cur) {
+    int xh, j1, x2, j2;
+    bool a1, a2;
+    coords(st, xh, j1, a1, x2, j2, a2);
+    // a prologue inside the run: the previous unit's phase 2 may still read
+    // the ring rows it writes
+    if (st.pro && st.u != ub) __syncthreads();
+    if (a1) phase1(j1, cur);
+    if (!st.pro) {
+      __syncthreads();
+      if (a2) phase2(j2, x2, cur);
+    }
+  };
+  MarchStep<RB> st{ub, true};
+  if constexpr (PRE) {
+    // the next step's loads go out before the current step's arithmetic
+    MarchIn<Real> cur;
+    load(st, cur);
+    for (;;) {
+      const MarchStep<RB> nst = next(st);
+      const bool more = nst.u < ue;
+      MarchIn<Real> nxt;
+      if (more) load(nst, nxt);
+      compute(st, cur);
+      if (!more) break;
+      cur = nxt;
+      st = nst;
+    }
+  } else {
+    // each phase loads its own inputs (fewer live registers)
+    for (;;) {
+      MarchIn<Real> cur;
+      int xh, j1, x2, j2;
+      bool a1, a2;
+      coords(st, xh, j1, a1, x2, j2, a2);
+      if (st.pro && st.u != ub) __syncthreads();
+      if (a1) {
+        const size_t o = (size_t)j1 * pitch + xh;
+#pragma unroll
+        for (int k = 0; k < NPOP; k++) {
+          cur.lf[k] = V.lf_out[(size_t)k * plane + o];
+          cur.lg[k] = V.lg_out[(size_t)k * plane + o];
+        }
+        cur.lFo = V.lF[o];
+        cur.lt = V.lT ? V.lT[o] : 0ll;
+        adj_pull_raw(V.fsrc, V.gsrc, nx, ny, pitch, plane, j1, xh, cur.fa, cur.ga);
+        cur.Fa = V.Fin[o];
+        phase1(j1, cur);
+      }
+      if (!st.pro) {
+        __syncthreads();
+        if (a2) {
+          const size_t o = (size_t)j2 * pitch + x2;
+          adj_pull_raw(P.fsrc_b, P.gsrc_b, nx, ny, pitch, plane, j2, x2, cur.fb, cur.gb);
+          cur.Fb = P.Fin_b[o];
+          cur.ltb = P.lT_b ? P.lT_b[o] : 0ll;
+          phase2(j2, x2, cur);
+        }
+      }
+      st = next(st);
+      if (st.u >= ue) break;
+    }
+  }
+}
+
 // observation adjoint of step n: lambda T += 2 r_p w_corner, fixed point
 __global__ void adj_obs_scatter_kernel(const double* __restrict__ ox, const double* __restrict__ oy,
                                        const double* __restrict__ res, int nobs, int nx, int ny,
@@ -525,8 +731,37 @@ static cudaError_t launch_pair_t(const AdjPairView<Real>& P, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// launch variants of the pair kernel: tile (TX x TY), threads, min blocks per SM
-constexpr int ADJ_NPAIR_VARIANTS = 4;
+// marching kernel: strips x chunks blocks, the chunk length chosen so that
+// the grid fills about `waves` waves of resident blocks
+template <typename Real, int RB, int MINB, bool PRE>
+static cudaError_t launch_march_t(const AdjPairView<Real>& P, int waves, cudaStream_t s) {
+  constexpr int NT = 34 * RB;
+  constexpr size_t smem = (size_t)(2 * NPOP + 1) * (2 * RB + 2) * 34 * sizeof(double);
+  auto kern = adjoint_march_kernel<Real, RB, MINB, PRE>;
+  static cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr != cudaSuccess) return attr;
+  static int occ = 0;
+  if (occ == 0) {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+  }
+  int dev = 0, nsm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int nstrips = (P.a.nx + 31) / 32, ngroups = (P.a.ny + RB - 1) / RB;
+  const int target = std::max(1, nsm * occ * waves / nstrips);  // chunks per strip
+  const int chunk = (ngroups + target - 1) / target;
+  const int nchunks = (ngroups + chunk - 1) / chunk;
+  kern<<<nstrips * nchunks, NT, smem, s>>>(P, chunk);
+  return cudaGetLastError();
+}
+
+// launch variants of the two-step adjoint: 0-3 the tiled pair kernel (tile
+// TX x TY, threads, min blocks per SM), 4-9 the marching kernel (rows per
+// group, blocks per SM, register prefetch; waves of blocks)
+constexpr int ADJ_NPAIR_VARIANTS = 10;
 int adjoint_pair_variants() { return ADJ_NPAIR_VARIANTS; }
 
 // steps n and n-1: state_a before step n, state_b before step n-1 (18 pop
@@ -557,6 +792,12 @@ cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, con
       case 1: return launch_pair_t<Real, 32, 4, 128, 6>(P, s);
       case 2: return launch_pair_t<Real, 32, 8, 256, 2>(P, s);
       case 3: return launch_pair_t<Real, 32, 8, 256, 3>(P, s);
+      case 4: return launch_march_t<Real, 7, 1, true>(P, 2, s);
+      case 5: return launch_march_t<Real, 6, 1, true>(P, 2, s);
+      case 6: return launch_march_t<Real, 7, 2, false>(P, 1, s);
+      case 7: return launch_march_t<Real, 7, 2, false>(P, 2, s);
+      case 8: return launch_march_t<Real, 4, 3, false>(P, 2, s);
+      case 9: return launch_march_t<Real, 6, 2, false>(P, 2, s);
       default: return launch_pair_t<Real, 32, 4, 128, 4>(P, s);
     }
   };

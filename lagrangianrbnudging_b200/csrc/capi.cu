@@ -848,12 +848,21 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   char* end_state = nullptr;
   for (int c = 0; c < nchk; c++) {
     const int s0 = c * K, len = std::min(K, nsteps - s0);
+    const bool last = c + 1 == nchk;
+    // the last two segments keep every state for the backward pass (one in
+    // each segment buffer); inside a segment that the backward pass
+    // recomputes, the states alternate between slots 1 and 2 (a footprint
+    // that stays in L2)
+    const bool keep = c + 2 >= nchk;
+    auto fslot = [&](int i) -> char* {
+      if (i == 0) return state_in(c, 0);
+      return segbuf(c) + (size_t)(keep ? i : 1 + ((i - 1) & 1)) * sb;
+    };
     for (int i = 0; i < len; i++) {
       const int s = s0 + i + 1;
-      char* dst = (i + 1 < len) ? segbuf(c) + (size_t)(i + 1) * sb
-                                : (c + 1 < nchk ? chk + (size_t)(c + 1) * sb : segbuf(c) + (size_t)K * sb);
+      char* dst = (i + 1 < len) ? fslot(i + 1) : (last ? segbuf(c) + (size_t)K * sb : chk + (size_t)(c + 1) * sb);
       const int oi = obs_at[s];
-      CK(h, launch_fwd(state_in(c, i), dst, oi >= 0));
+      CK(h, launch_fwd(fslot(i), dst, oi >= 0));
       if (oi >= 0) {
         const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
         CK(h, launch_obs_residual(h->T[0], f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob, nob,
@@ -957,15 +966,16 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   for (int c = nchk - 1; c >= 0; c--) {
     const int s0 = c * K, len = std::min(K, nsteps - s0), s1 = s0 + len;
     const int b = (nchk - 1 - c) & 1;
-    if (c >= 1) {
-      // recompute segment c-1 into the other buffer, after the sweep that read it
+    if (c >= 1 && c + 1 < nchk) {
+      // recompute segment c-1 into the other buffer, after the sweep that
+      // read it (segment nchk-2 is still there from the forward pass)
       const int cp = c - 1, lenp = std::min(K, nsteps - cp * K);
       CK(h, cudaStreamWaitEvent(rs, ev_bwd[b ^ 1], 0));
       for (int i = 0; i + 1 < lenp; i++)
         CK(h, launch_fwd_on(state_in(cp, i), segbuf(cp) + (size_t)(i + 1) * sb, 0, rs));
       CK(h, cudaEventRecord(ev_rec[b ^ 1], rs));
     }
-    if (c < nchk - 1) CK(h, cudaStreamWaitEvent(h->stream, ev_rec[b], 0));
+    if (c + 2 < nchk) CK(h, cudaStreamWaitEvent(h->stream, ev_rec[b], 0));
     int s = s1;
     while (s > s0) {
       const int i = s - s0 - 1;

@@ -62,11 +62,16 @@ def test_checkpoint_interval_does_not_change_the_gradient(case):
     np.testing.assert_array_equal(g1, gall)
 
 
-def test_every_pair_kernel_variant_gives_the_same_gradient(case):
-    c = case
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [None, (40, 13)])
+def test_every_pair_kernel_variant_gives_the_same_gradient(case, precision, shape):
+    """the tiled and the marching two-step kernels, every launch variant, on
+    the 48x24 case and on a grid of partial strips and row groups"""
+    c = case if shape is None else adjoint_case(seed=9, nx=shape[0], ny=shape[1], nsteps=17, every=3,
+                                                nobs=11)
     grads = []
     for v in range(lb.Run.adjoint_variants()):
-        with lb.Run(**c["base"], precision="fp64") as r:
+        with lb.Run(**c["base"], precision=precision) as r:
             r.adjoint_set_variant(v)
             r.adjoint_set_obs(c["steps"], c["ox"], c["oy"], c["oT"])
             grads.append(r.adjoint_window(c["T0"], c["nsteps"], 8)[1])
