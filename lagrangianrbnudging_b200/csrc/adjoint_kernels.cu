@@ -50,7 +50,8 @@ constexpr double ADJ_FIX = 1099511627776.0;  // 2^40
 // the stored values the forward step pulls into node (x, j): fv[k], gv[k]
 // (bounce-back at the walls: f from the node's opposite population, g left
 // zero for the anti-bounce-back below)
-template <typename Real>
+// (Off: element offset type, uint32_t where the buffers allow it)
+template <typename Real, typename Off = size_t>
 __device__ __forceinline__ void adj_pull_raw(const Real* __restrict__ fsrc, const Real* __restrict__ gsrc,
                                              int nx, int ny, int pitch, size_t plane, int j, int x,
                                              Real* fv, Real* gv) {
@@ -61,11 +62,11 @@ __device__ __forceinline__ void adj_pull_raw(const Real* __restrict__ fsrc, cons
     const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
     const int js = j - icy(k);
     if (js < 0 || js >= ny) {
-      fv[k] = fsrc[(size_t)opp(k) * plane + (size_t)j * pitch + x];
+      fv[k] = fsrc[(Off)opp(k) * (Off)plane + (Off)j * (Off)pitch + (Off)x];
       gv[k] = Real(0);
     } else {
-      fv[k] = fsrc[(size_t)k * plane + (size_t)js * pitch + xs];
-      gv[k] = gsrc[(size_t)k * plane + (size_t)js * pitch + xs];
+      fv[k] = fsrc[(Off)k * (Off)plane + (Off)js * (Off)pitch + (Off)xs];
+      gv[k] = gsrc[(Off)k * (Off)plane + (Off)js * (Off)pitch + (Off)xs];
     }
   }
 }
@@ -247,12 +248,13 @@ __device__ __forceinline__ void adj_local(const AdjView<Real>& V, const AdjLoc& 
 // population k goes to the node the forward pulled it from (bounce-back:
 // this node's opposite population; g streaming out of the domain gets zero).
 // Every (population, node) of the output receives exactly one write.
+template <typename Off = size_t>
 __device__ __forceinline__ void adj_push_one(int k, bool is_g, double val, int nx, int ny, int pitch,
                                              size_t plane, int j, int x, double* __restrict__ out) {
   const int xs = icx(k) == 1 ? (x == 0 ? nx - 1 : x - 1) : (icx(k) == -1 ? (x == nx - 1 ? 0 : x + 1) : x);
   const int js = j - icy(k);
-  if (js < 0 || js >= ny) out[(size_t)opp(k) * plane + (size_t)j * pitch + x] = is_g ? 0.0 : val;
-  else out[(size_t)k * plane + (size_t)js * pitch + xs] = val;
+  if (js < 0 || js >= ny) out[(Off)opp(k) * (Off)plane + (Off)j * (Off)pitch + (Off)x] = is_g ? 0.0 : val;
+  else out[(Off)k * (Off)plane + (Off)js * (Off)pitch + (Off)xs] = val;
 }
 
 template <typename Real>
@@ -406,10 +408,12 @@ struct MarchStep {
   bool pro;  // prologue: phase 1 of rows r-1, r only
 };
 
-// PRE: the next unit's inputs go to registers before the current unit's
-// arithmetic (one block per SM: about 240 registers); without it the blocks
-// per SM (MINB) hide each other's loads.
-template <typename Real, int RB, int MINB, bool PRE>
+// PRE = 1: the next unit's inputs go to registers before the current unit's
+// arithmetic (one block per SM: about 240 registers); PRE = 2: half a unit
+// ahead (phase 2's inputs during phase 1, the next phase 1's during phase 2);
+// PRE = 0: each phase loads its own inputs and the blocks per SM (MINB) hide
+// each other's loads.
+template <typename Real, int RB, int MINB, int PRE, typename Off>
 __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjPairView<Real> P, int chunk) {
   extern __shared__ double sm[];
   constexpr int HX = 34, S = 2 * RB + 2;  // ring: S rows of HX columns, 2*NPOP+1 values
@@ -438,28 +442,32 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
     x2 = x0 + px;
     a2 = !st.pro && t < 32 * RB && j2 < ny && x2 < nx;
   };
+  // inputs of phase 1 (lambda^n and the state before step n at xh, j1) and
+  // of phase 2 (the state before step n-1 at x2, j2)
+  auto load1 = [&](int xh, int j1, MarchIn<Real>& in) {
+    const Off o = (Off)j1 * (Off)pitch + (Off)xh;
+#pragma unroll
+    for (int k = 0; k < NPOP; k++) {
+      in.lf[k] = V.lf_out[(Off)k * (Off)plane + o];
+      in.lg[k] = V.lg_out[(Off)k * (Off)plane + o];
+    }
+    in.lFo = V.lF[o];
+    in.lt = V.lT ? V.lT[o] : 0ll;
+    adj_pull_raw<Real, Off>(V.fsrc, V.gsrc, nx, ny, pitch, plane, j1, xh, in.fa, in.ga);
+    in.Fa = V.Fin[o];
+  };
+  auto load2 = [&](int x2, int j2, MarchIn<Real>& in) {
+    const Off o = (Off)j2 * (Off)pitch + (Off)x2;
+    adj_pull_raw<Real, Off>(P.fsrc_b, P.gsrc_b, nx, ny, pitch, plane, j2, x2, in.fb, in.gb);
+    in.Fb = P.Fin_b[o];
+    in.ltb = P.lT_b ? P.lT_b[o] : 0ll;
+  };
   auto load = [&](const MarchStep<RB>& st, MarchIn<Real>& in) {
     int xh, j1, x2, j2;
     bool a1, a2;
     coords(st, xh, j1, a1, x2, j2, a2);
-    if (a1) {
-      const size_t o = (size_t)j1 * pitch + xh;
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) {
-        in.lf[k] = V.lf_out[(size_t)k * plane + o];
-        in.lg[k] = V.lg_out[(size_t)k * plane + o];
-      }
-      in.lFo = V.lF[o];
-      in.lt = V.lT ? V.lT[o] : 0ll;
-      adj_pull_raw(V.fsrc, V.gsrc, nx, ny, pitch, plane, j1, xh, in.fa, in.ga);
-      in.Fa = V.Fin[o];
-    }
-    if (a2) {
-      const size_t o = (size_t)j2 * pitch + x2;
-      adj_pull_raw(P.fsrc_b, P.gsrc_b, nx, ny, pitch, plane, j2, x2, in.fb, in.gb);
-      in.Fb = P.Fin_b[o];
-      in.ltb = P.lT_b ? P.lT_b[o] : 0ll;
-    }
+    if (a1) load1(xh, j1, in);
+    if (a2) load2(x2, j2, in);
   };
   auto next = [&](const MarchStep<RB>& st) {
     if (st.pro) return MarchStep<RB>{st.u, false};
@@ -490,10 +498,10 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
     double lFin;
     adj_local(
         V, L, j2, lfo, lgo, ring(2 * NPOP, j2, c), (double)cur.ltb * (1.0 / ADJ_FIX),
-        [&](int k, double val) { adj_push_one(k, false, val, nx, ny, pitch, plane, j2, x2, P.lf_in); },
-        [&](int k, double val) { adj_push_one(k, true, val, nx, ny, pitch, plane, j2, x2, P.lg_in); },
+        [&](int k, double val) { adj_push_one<Off>(k, false, val, nx, ny, pitch, plane, j2, x2, P.lf_in); },
+        [&](int k, double val) { adj_push_one<Off>(k, true, val, nx, ny, pitch, plane, j2, x2, P.lg_in); },
         lFin);
-    P.lF_out[(size_t)j2 * pitch + x2] = lFin;
+    P.lF_out[(Off)j2 * (Off)pitch + (Off)x2] = lFin;
   };
   auto compute = [&](const MarchStep<RB>& st, const MarchIn<Real>& cur) {
     int xh, j1, x2, j2;
@@ -509,7 +517,7 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
     }
   };
   MarchStep<RB> st{ub, true};
-  if constexpr (PRE) {
+  if constexpr (PRE == 1) {
     // the next step's loads go out before the current step's arithmetic
     MarchIn<Real> cur;
     load(st, cur);
@@ -523,8 +531,36 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
       cur = nxt;
       st = nst;
     }
+  } else if constexpr (PRE == 2) {
+    // half a step ahead: phase 2's loads go out before phase 1's arithmetic,
+    // the next step's phase-1 loads before phase 2's arithmetic
+    MarchIn<Real> in1, in2;
+    int xh, j1, x2, j2;
+    bool a1, a2;
+    coords(st, xh, j1, a1, x2, j2, a2);
+    if (a1) load1(xh, j1, in1);
+    for (;;) {
+      if (a2) load2(x2, j2, in2);
+      if (st.pro && st.u != ub) __syncthreads();
+      if (a1) phase1(j1, in1);
+      const MarchStep<RB> nst = next(st);
+      const bool more = nst.u < ue;
+      int nxh, nj1, nx2, nj2;
+      bool na1 = false, na2 = false;
+      if (more) {
+        coords(nst, nxh, nj1, na1, nx2, nj2, na2);
+        if (na1) load1(nxh, nj1, in1);
+      }
+      if (!st.pro) {
+        __syncthreads();
+        if (a2) phase2(j2, x2, in2);
+      }
+      if (!more) break;
+      st = nst;
+      xh = nxh, j1 = nj1, a1 = na1, x2 = nx2, j2 = nj2, a2 = na2;
+    }
   } else {
-    // each phase loads its own inputs (fewer live registers)
+    // each phase loads its own inputs
     for (;;) {
       MarchIn<Real> cur;
       int xh, j1, x2, j2;
@@ -532,25 +568,13 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
       coords(st, xh, j1, a1, x2, j2, a2);
       if (st.pro && st.u != ub) __syncthreads();
       if (a1) {
-        const size_t o = (size_t)j1 * pitch + xh;
-#pragma unroll
-        for (int k = 0; k < NPOP; k++) {
-          cur.lf[k] = V.lf_out[(size_t)k * plane + o];
-          cur.lg[k] = V.lg_out[(size_t)k * plane + o];
-        }
-        cur.lFo = V.lF[o];
-        cur.lt = V.lT ? V.lT[o] : 0ll;
-        adj_pull_raw(V.fsrc, V.gsrc, nx, ny, pitch, plane, j1, xh, cur.fa, cur.ga);
-        cur.Fa = V.Fin[o];
+        load1(xh, j1, cur);
         phase1(j1, cur);
       }
       if (!st.pro) {
         __syncthreads();
         if (a2) {
-          const size_t o = (size_t)j2 * pitch + x2;
-          adj_pull_raw(P.fsrc_b, P.gsrc_b, nx, ny, pitch, plane, j2, x2, cur.fb, cur.gb);
-          cur.Fb = P.Fin_b[o];
-          cur.ltb = P.lT_b ? P.lT_b[o] : 0ll;
+          load2(x2, j2, cur);
           phase2(j2, x2, cur);
         }
       }
@@ -733,11 +757,11 @@ static cudaError_t launch_pair_t(const AdjPairView<Real>& P, cudaStream_t s) {
 
 // marching kernel: strips x chunks blocks, the chunk length chosen so that
 // the grid fills about `waves` waves of resident blocks
-template <typename Real, int RB, int MINB, bool PRE>
-static cudaError_t launch_march_t(const AdjPairView<Real>& P, int waves, cudaStream_t s) {
+template <typename Real, int RB, int MINB, int PRE, typename Off>
+static cudaError_t launch_march_o(const AdjPairView<Real>& P, int waves, cudaStream_t s) {
   constexpr int NT = 34 * RB;
   constexpr size_t smem = (size_t)(2 * NPOP + 1) * (2 * RB + 2) * 34 * sizeof(double);
-  auto kern = adjoint_march_kernel<Real, RB, MINB, PRE>;
+  auto kern = adjoint_march_kernel<Real, RB, MINB, PRE, Off>;
   static cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (attr != cudaSuccess) return attr;
   static int occ = 0;
@@ -756,6 +780,13 @@ static cudaError_t launch_march_t(const AdjPairView<Real>& P, int waves, cudaStr
   const int nchunks = (ngroups + chunk - 1) / chunk;
   kern<<<nstrips * nchunks, NT, smem, s>>>(P, chunk);
   return cudaGetLastError();
+}
+
+// 32-bit element offsets where 36 planes of the grid fit below 2^32
+template <typename Real, int RB, int MINB, int PRE>
+static cudaError_t launch_march_t(const AdjPairView<Real>& P, int waves, cudaStream_t s) {
+  if (off32_ok(P.a.plane)) return launch_march_o<Real, RB, MINB, PRE, uint32_t>(P, waves, s);
+  return launch_march_o<Real, RB, MINB, PRE, size_t>(P, waves, s);
 }
 
 // launch variants of the two-step adjoint: 0-3 the tiled pair kernel (tile
@@ -792,12 +823,12 @@ cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, con
       case 1: return launch_pair_t<Real, 32, 4, 128, 6>(P, s);
       case 2: return launch_pair_t<Real, 32, 8, 256, 2>(P, s);
       case 3: return launch_pair_t<Real, 32, 8, 256, 3>(P, s);
-      case 4: return launch_march_t<Real, 7, 1, true>(P, 2, s);
-      case 5: return launch_march_t<Real, 6, 1, true>(P, 2, s);
-      case 6: return launch_march_t<Real, 7, 2, false>(P, 1, s);
-      case 7: return launch_march_t<Real, 7, 2, false>(P, 2, s);
-      case 8: return launch_march_t<Real, 4, 3, false>(P, 2, s);
-      case 9: return launch_march_t<Real, 6, 2, false>(P, 2, s);
+      case 4: return launch_march_t<Real, 7, 1, 1>(P, 2, s);
+      case 5: return launch_march_t<Real, 6, 1, 1>(P, 2, s);
+      case 6: return launch_march_t<Real, 7, 1, 2>(P, 2, s);
+      case 7: return launch_march_t<Real, 5, 2, 2>(P, 2, s);
+      case 8: return launch_march_t<Real, 5, 2, 2>(P, 1, s);
+      case 9: return launch_march_t<Real, 3, 3, 2>(P, 2, s);
       default: return launch_pair_t<Real, 32, 4, 128, 4>(P, s);
     }
   };
