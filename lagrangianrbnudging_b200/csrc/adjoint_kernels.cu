@@ -122,12 +122,9 @@ __device__ __forceinline__ AdjLoc adj_locals_raw(const AdjView<Real>& V, const R
                                                  Real Fnode, int j) {
   double df[NPOP], dg[NPOP];
   adj_shift_pulled(V, j, fv, gv, df, dg);
-  double dr = 0.0, dT = 0.0;
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    dr += df[k];
-    dT += dg[k];
-  }
+  // tree sums (short dependency chains)
+  const double dr = ((df[0] + df[1]) + (df[2] + df[3])) + ((df[4] + df[5]) + (df[6] + df[7])) + df[8];
+  const double dT = ((dg[0] + dg[1]) + (dg[2] + dg[3])) + ((dg[4] + dg[5]) + (dg[6] + dg[7])) + dg[8];
   const double jx = (df[1] - df[3]) + (df[5] - df[6]) + (df[8] - df[7]);
   const double jy = (df[2] - df[4]) + (df[5] - df[7]) + (df[6] - df[8]);
   AdjLoc L;
@@ -204,13 +201,14 @@ __device__ __forceinline__ void adj_local(const AdjView<Real>& V, const AdjLoc& 
   const double Py = fma(al, M.my, be * N.my), Pxx = fma(al, M.mxx, be * N.mxx);
   const double Pyy = fma(al, M.myy, be * N.myy), Pxy = fma(al, M.mxy, be * N.mxy);
   const double sF = sf * F;
-  const double lu = fma(3.0, Px, fma(9.0 * u, Pxx, fma(9.0 * v, Pxy, fma(-3.0 * u, P0, 9.0 * sF * M.mxy))));
-  const double lv = fma(3.0, Py, fma(9.0 * u, Pxy, fma(9.0 * v, Pyy,
-                        fma(-3.0 * v, P0, sF * fma(9.0, M.myy, -3.0 * M.m0)))));
+  // each sum as two independent halves (short dependency chains)
+  const double lu = fma(3.0, Px, fma(-3.0 * u, P0, 9.0 * sF * M.mxy)) + fma(9.0 * u, Pxx, 9.0 * v * Pxy);
+  const double lv = fma(3.0, Py, fma(-3.0 * v, P0, sF * fma(9.0, M.myy, -3.0 * M.m0))) +
+                    fma(9.0 * u, Pxy, 9.0 * v * Pyy);
   const double q15 = 1.0 - 1.5 * fma(u, u, v * v);
   const double uu45 = 4.5 * u * u, vv45 = 4.5 * v * v, uv9 = 9.0 * u * v, u3 = 3.0 * u, v3 = 3.0 * v;
   auto Q = [&](const AdjMom& X) {
-    return fma(X.m0, q15, fma(u3, X.mx, fma(v3, X.my, fma(uu45, X.mxx, fma(uv9, X.mxy, vv45 * X.myy)))));
+    return fma(X.m0, q15, fma(u3, X.mx, v3 * X.my)) + fma(uu45, X.mxx, fma(uv9, X.mxy, vv45 * X.myy));
   };
   const double ldr = fma(om, Q(M), fma(lFo * V.gbeta, t, -fma(lu, u, lv * v) * rinv));
   const double ldT = fma(omg, Q(N), fma(lFo * V.gbeta, r, lt));
