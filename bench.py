@@ -433,24 +433,27 @@ def adjoint_problem(lb, device: int, seed: int = 31):
     return base, steps, ox, oy, oT, T0
 
 
-def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS) -> dict:
+def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = ADJ_K,
+                      variant: int = -1) -> dict:
     base, steps, ox, oy, oT, T0 = adjoint_problem(lb, device)
     keep = steps <= nsteps
     steps, ox, oy, oT = steps[keep], ox[keep], oy[keep], oT[keep]
     with lb.Run(**base, precision="fp32", device=device) as w:
         w.adjoint_set_obs(steps, ox, oy, oT)
+        if variant >= 0:
+            w.adjoint_set_variant(variant)
         stream = torch.cuda.Stream()
         w.set_stream(stream.cuda_stream)
         # warm-up at the window's own size: checkpoint and segment buffers,
         # launch-shape and pair-kernel autotuning happen here, untimed
-        w.adjoint_window(T0, nsteps, ADJ_K, gradient=True)
+        w.adjoint_window(T0, nsteps, K, gradient=True)
         pair_variant = w.adjoint_variant()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         ev[0].record(stream)
-        w.adjoint_window(T0, nsteps, ADJ_K, gradient=False)
+        w.adjoint_window(T0, nsteps, K, gradient=False)
         ev[1].record(stream)
         ev[2].record(stream)
-        J, grad = w.adjoint_window(T0, nsteps, ADJ_K, gradient=True)
+        J, grad = w.adjoint_window(T0, nsteps, K, gradient=True)
         ev[3].record(stream)
         # plain forward steps of the same grid, for the cost ratio
         w.init_conduction(1, 1e-3)
@@ -464,7 +467,7 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS) -> dict:
         t_step = ev[4].elapsed_time(ev[5]) / nsteps
         w.set_stream(None)
     fd = adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir=8)
-    return {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": nsteps, "checkpoint_every": ADJ_K,
+    return {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": nsteps, "checkpoint_every": K,
             "observations": f"{ADJ_NOBS} tracers every {ADJ_EVERY} steps (seeded truth run)",
             "fd_check": fd, "pair_kernel_variant": pair_variant,
             "precision": "fp32 forward, fp64 adjoint", "J": J,
@@ -979,6 +982,9 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true",
                     help="only the adjoint window (the command used for ncu captures of the adjoint kernels)")
     ap.add_argument("--adjoint-steps", type=int, default=ADJ_STEPS)
+    ap.add_argument("--adjoint-k", type=int, default=ADJ_K, help="checkpoint interval of the adjoint window")
+    ap.add_argument("--adjoint-variant", type=int, default=-1,
+                    help="fixed launch variant of the two-step adjoint kernel (-1: autotune)")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="only the ensemble section (the command used for ncu captures of ens_lb_kernel)")
     ap.add_argument("--adjoint-check", action="store_true",
@@ -1019,7 +1025,8 @@ def main():
 
         b.build()
         torch.cuda.set_device(0)
-        print(json.dumps({"mode": "adjoint-only", **run_adjoint_bench(lb, torch, 0, args.adjoint_steps)}),
+        print(json.dumps({"mode": "adjoint-only", **run_adjoint_bench(lb, torch, 0, args.adjoint_steps,
+                                                                      args.adjoint_k, args.adjoint_variant)}),
               flush=True)
         return
     if args.nudging_only:
