@@ -332,6 +332,19 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     if not args.no_e2e:
         e2e_ms, e2e_h2d, e2e_d2h = e2e(lb, torch, "fp32", seed, K, device, dist)
         e2e_ms = max_over_ranks(torch, dist, e2e_ms)
+    # sections with independent units: every rank takes its share (replicas
+    # for the adjoint window's timing), results gathered once
+    sec = {}
+    if not args.no_adjoint:
+        sec["adjoint"] = run_adjoint_bench(lb, torch, device, dist=dist, rank=rank, world=world)
+    if world == 1 and not args.no_accuracy:
+        sec["accuracy"] = run_accuracy(lb, device)
+    if not args.no_nudging:
+        sec["nudging"] = run_nudging_bench(lb, torch, device, args.nudging_steps, dist=dist, rank=rank,
+                                           world=world)
+    if not args.no_ensemble:
+        sec["ensemble"] = run_ensemble_bench(lb, torch, device, args.ensemble_steps, dist=dist, rank=rank,
+                                             world=world)
     if rank != 0:
         return None
     mlups = whole_job_mlups(world, nodes, K, ms)
@@ -381,14 +394,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
         "clocks": clocks,
         "records": len(recs),
     })
-    if world == 1 and not args.no_adjoint:
-        out["adjoint"] = run_adjoint_bench(lb, torch, device)
-    if world == 1 and not args.no_accuracy:
-        out["accuracy"] = run_accuracy(lb, device)
-    if world == 1 and not args.no_nudging:
-        out["nudging"] = run_nudging_bench(lb, torch, device, args.nudging_steps)
-    if world == 1 and not args.no_ensemble:
-        out["ensemble"] = run_ensemble_bench(lb, torch, device, args.ensemble_steps)
+    out.update(sec)
     if e2e_ms is not None:
         out["e2e"] = {"value": round(world * nodes * K / (e2e_ms * 1e3), 1), "unit": "MLUPS",
                       "h2d_bytes_per_step": int(e2e_h2d / K), "d2h_bytes_per_step": int(e2e_d2h / K),
@@ -433,8 +439,18 @@ def adjoint_problem(lb, device: int, seed: int = 31):
     return base, steps, ox, oy, oT, T0
 
 
+def sync_ranks(torch, dist):
+    """all ranks at the same point with their GPU work done"""
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+
+
 def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = ADJ_K,
-                      variant: int = -1) -> dict:
+                      variant: int = -1, dist=None, rank: int = 0, world: int = 1) -> dict:
+    """The adjoint window's cost (every rank times the same window: replicas,
+    the slowest rank's times) and the FD check (directions split over the
+    ranks)."""
     base, steps, ox, oy, oT, T0 = adjoint_problem(lb, device)
     keep = steps <= nsteps
     steps, ox, oy, oT = steps[keep], ox[keep], oy[keep], oT[keep]
@@ -448,6 +464,7 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = 
         # launch-shape and pair-kernel autotuning happen here, untimed
         w.adjoint_window(T0, nsteps, K, gradient=True)
         pair_variant = w.adjoint_variant()
+        sync_ranks(torch, dist)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         ev[0].record(stream)
         w.adjoint_window(T0, nsteps, K, gradient=False)
@@ -462,17 +479,20 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = 
         w.step(nsteps)
         ev[5].record(stream)
         torch.cuda.synchronize()
-        t_fwd_window = ev[0].elapsed_time(ev[1])
-        t_adj = ev[2].elapsed_time(ev[3])
-        t_step = ev[4].elapsed_time(ev[5]) / nsteps
+        t_fwd_window = max_over_ranks(torch, dist, ev[0].elapsed_time(ev[1]))
+        t_adj = max_over_ranks(torch, dist, ev[2].elapsed_time(ev[3]))
+        t_step = max_over_ranks(torch, dist, ev[4].elapsed_time(ev[5]) / nsteps)
         w.set_stream(None)
-    fd = adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir=8)
+    fd = adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir=8, dist=dist, rank=rank,
+                          world=world)
     return {"grid": f"{ADJ_NX}x{ADJ_NY}", "window_steps": nsteps, "checkpoint_every": K,
+            "ranks": world,
             "observations": f"{ADJ_NOBS} tracers every {ADJ_EVERY} steps (seeded truth run)",
             "fd_check": fd, "pair_kernel_variant": pair_variant,
             "precision": "fp32 forward, fp64 adjoint", "J": J,
             "grad_norm": float(np.linalg.norm(grad)),
-            "adjoint_steps_per_s": round(nsteps / (t_adj * 1e-3), 1),
+            # all ranks' adjoint steps over the slowest rank's window
+            "adjoint_steps_per_s": round(world * nsteps / (t_adj * 1e-3), 1),
             "ms_gradient_window": round(t_adj, 2), "ms_misfit_window": round(t_fwd_window, 2),
             "ms_forward_step": round(t_step, 5),
             # gradient (forward + recompute + backward) per window step, in plain forward steps
@@ -483,21 +503,32 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = 
             "gradient_over_misfit": round(t_adj / t_fwd_window, 2)}
 
 
-def adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir, h=1e-6, seed=2024) -> dict:
+def adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir, h=1e-6, seed=2024,
+                     dist=None, rank: int = 0, world: int = 1) -> dict:
     """<gradient, d> of the FP64 adjoint against central differences (h) of the
-    FP64 forward on ndir seeded directions; FP32-forward gradient against it"""
+    FP64 forward on ndir seeded directions, split over the ranks (each rank
+    its own gradient and its directions; the errors gathered once);
+    FP32-forward gradient against it"""
+    from lagrangianrbnudging_b200 import shard
+
+    mine = set(shard.my_units([1.0] * ndir, rank, world))
+    errs = {}
     with lb.Run(**base, precision="fp64", device=device) as w:
         w.adjoint_set_obs(steps, ox, oy, oT)
         J, g64 = w.adjoint_window(T0, nsteps, ADJ_K)
         rng = np.random.default_rng(seed)
-        errs = []
-        for _ in range(ndir):
-            d = rng.standard_normal(T0.shape)
+        for k in range(ndir):
+            d = rng.standard_normal(T0.shape)  # every rank draws every direction, in order
+            if k not in mine:
+                continue
             Jp = w.adjoint_window(T0 + h * d, nsteps, ADJ_K, gradient=False)
             Jm = w.adjoint_window(T0 - h * d, nsteps, ADJ_K, gradient=False)
             fd = (Jp - Jm) / (2 * h)
             ad = float(np.sum(g64 * d))
-            errs.append(abs(fd - ad) / abs(ad))
+            errs[k] = abs(fd - ad) / abs(ad)
+    for part in shard.gather(dist, errs):
+        errs.update(part)
+    errs = [errs[k] for k in range(ndir)]
     with lb.Run(**base, precision="fp32", device=device) as w:
         w.adjoint_set_obs(steps, ox, oy, oT)
         J32, g32 = w.adjoint_window(T0, nsteps, ADJ_K)
@@ -550,71 +581,89 @@ NUD_NX, NUD_NY, NUD_RA, NUD_TRACERS, NUD_STEPS, NUD_CHUNK = 2048, 1024, 1e7, 1 <
 NUD_ALPHAS = (0.01, 0.1, 1.0)
 
 
-def run_nudging_bench(lb, torch, device: int, steps: int = NUD_STEPS, chunk: int = NUD_CHUNK) -> dict:
+def run_nudging_bench(lb, torch, device: int, steps: int = NUD_STEPS, chunk: int = NUD_CHUNK,
+                      dist=None, rank: int = 0, world: int = 1) -> dict:
     """Twin experiment: run A (seed A, 2^14 tracers) records T along the
     trajectories every step; runs from seed B relax T toward those records at
     the recorded positions (bilinear, alpha in {0.01, 0.1, 1} per step), beside
     a free run (alpha = 0) from seed B.  All FP32-shifted populations, FP64
-    positions; the L2 error of T against run A is sampled along the way."""
+    positions; the L2 error of T against run A is sampled along the way.
+    With several ranks the four runs from seed B are split over them; each
+    rank with runs computes run A itself (deterministic), and the results are
+    gathered once."""
+    from lagrangianrbnudging_b200 import shard
+
+    alphas_all = (0.0,) + NUD_ALPHAS
+    mine = [alphas_all[i] for i in shard.my_units([1.0] * len(alphas_all), rank, world)]
     base = lb.closure(NUD_NX, NUD_NY, Ra=NUD_RA, Pr=1.0, U=0.1)
     seed_a, seed_b = 1001, 2002
-    rng = np.random.default_rng(seed_a)
     n = NUD_TRACERS
-    x = rng.uniform(0.5, NUD_NX + 0.5, n)
-    y = rng.uniform(1.0, NUD_NY, n)
-    truth = lb.Run(**base, precision="fp32", nprtcl=n, noutconfig=1, record_slots=chunk + 1,
-                   device=device)
-    truth.init_conduction(seed_a, 1e-3)
-    m = truth.get_moments()
-    truth.set_particles(np.arange(n, dtype=np.int32), x, y, bilinear_np(m["u"], x, y),
-                        bilinear_np(m["v"], x, y), np.zeros(n, np.int32), np.zeros(n))
-    runs = {}
-    for a in (0.0,) + NUD_ALPHAS:
-        kw = dict(base, precision="fp32", device=device)
-        if a > 0:
-            kw.update(nudge="bilinear", alpha=a, nobs=n)
-        r = lb.Run(**kw)
-        r.init_conduction(seed_b, 1e-3)
-        runs[a] = r
-    stream = torch.cuda.Stream()
-    ms = {a: 0.0 for a in runs}
-    ms_truth = 0.0
-    samples = {a: [] for a in runs}
-    sample_every = max(steps // 20, chunk)
-
-    def l2(ra, rb):
-        ta = ra.get_moments()["T"]
-        tb = rb.get_moments()["T"]
-        return float(np.sqrt(np.mean((tb - ta) ** 2)))
-
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for r in [truth, *runs.values()]:
-        r.set_stream(stream.cuda_stream)
-    done = 0
-    while done < steps:
-        c = min(chunk, steps - done)
-        e0.record(stream)
-        truth.step(c)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms_truth += e0.elapsed_time(e1)
-        st, buf = truth.drain_records_array()
-        ox, oy, oT = buf[:, 0, :], buf[:, 1, :], buf[:, 8, :]
-        for a, r in runs.items():
+    nodes = NUD_NX * NUD_NY
+    part = {"ms_truth": None, "runs": {}}
+    if mine:
+        rng = np.random.default_rng(seed_a)
+        x = rng.uniform(0.5, NUD_NX + 0.5, n)
+        y = rng.uniform(1.0, NUD_NY, n)
+        truth = lb.Run(**base, precision="fp32", nprtcl=n, noutconfig=1, record_slots=chunk + 1,
+                       device=device)
+        truth.init_conduction(seed_a, 1e-3)
+        m = truth.get_moments()
+        truth.set_particles(np.arange(n, dtype=np.int32), x, y, bilinear_np(m["u"], x, y),
+                            bilinear_np(m["v"], x, y), np.zeros(n, np.int32), np.zeros(n))
+        runs = {}
+        for a in mine:
+            kw = dict(base, precision="fp32", device=device)
             if a > 0:
-                r.nudge_obs(int(st[0]), ox, oy, oT)
+                kw.update(nudge="bilinear", alpha=a, nobs=n)
+            r = lb.Run(**kw)
+            r.init_conduction(seed_b, 1e-3)
+            runs[a] = r
+        stream = torch.cuda.Stream()
+        ms = {a: 0.0 for a in runs}
+        ms_truth = 0.0
+        samples = {a: [] for a in runs}
+        sample_every = max(steps // 20, chunk)
+
+        def l2(ra, rb):
+            ta = ra.get_moments()["T"]
+            tb = rb.get_moments()["T"]
+            return float(np.sqrt(np.mean((tb - ta) ** 2)))
+
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for r in [truth, *runs.values()]:
+            r.set_stream(stream.cuda_stream)
+        done = 0
+        while done < steps:
+            c = min(chunk, steps - done)
             e0.record(stream)
-            r.step(c)
+            truth.step(c)
             e1.record(stream)
             torch.cuda.synchronize()
-            ms[a] += e0.elapsed_time(e1)
-        done += c
-        if done % sample_every == 0 or done == steps:
+            ms_truth += e0.elapsed_time(e1)
+            st, buf = truth.drain_records_array()
+            ox, oy, oT = buf[:, 0, :], buf[:, 1, :], buf[:, 8, :]
             for a, r in runs.items():
-                samples[a].append((done, float(f"{l2(truth, r):.4g}")))
-    for r in [truth, *runs.values()]:
-        r.set_stream(None)
-    nodes = NUD_NX * NUD_NY
+                if a > 0:
+                    r.nudge_obs(int(st[0]), ox, oy, oT)
+                e0.record(stream)
+                r.step(c)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms[a] += e0.elapsed_time(e1)
+            done += c
+            if done % sample_every == 0 or done == steps:
+                for a, r in runs.items():
+                    samples[a].append((done, float(f"{l2(truth, r):.4g}")))
+        for r in [truth, *runs.values()]:
+            r.set_stream(None)
+            r.close()
+        part = {"ms_truth": ms_truth, "runs": {a: (samples[a], ms[a]) for a in runs}}
+    parts = shard.gather(dist, part)
+    ms_truth = next(p["ms_truth"] for p in parts if p["ms_truth"] is not None)
+    samples, ms = {}, {}
+    for p in parts:
+        for a, (sm, m_) in p["runs"].items():
+            samples[a], ms[a] = sm, m_
     out = {"grid": f"{NUD_NX}x{NUD_NY}", "Ra": NUD_RA, "tracers": n, "steps": steps,
            "obs": "run A's records (x, y, T) every step, fed in chunks of %d steps" % chunk,
            "truth_mlups_with_records": round(nodes * steps / (ms_truth * 1e3), 1),
@@ -622,8 +671,9 @@ def run_nudging_bench(lb, torch, device: int, steps: int = NUD_STEPS, chunk: int
            "nudged": {str(a): {"l2_final": samples[a][-1][1], "l2": samples[a],
                                "mlups": round(nodes * steps / (ms[a] * 1e3), 1)} for a in NUD_ALPHAS},
            "metric": "L2 T-field error vs run A, sqrt(mean((T_B - T_A)^2))"}
-    for r in [truth, *runs.values()]:
-        r.close()
+    if world > 1:
+        out["ranks"] = world
+        out["split"] = "the four runs from seed B over the ranks (longest processing time first)"
     return out
 
 
@@ -631,13 +681,15 @@ def run_nudging_bench(lb, torch, device: int, steps: int = NUD_STEPS, chunk: int
 ENS_N, ENS_STEPS, ENS_TRACERS, ENS_OBS_ROWS = 64, 10000, 1024, 100
 
 
-def ensemble_members(lb, device: int, seed: int = 41):
+def ensemble_members(lb, device: int, seed: int = 41, keep=None):
     """The uneven ensemble: 64 members with Nx x Ny drawn from {256x128,
     512x256, 1024x512} and Ra log-uniform in [1e5, 1e7] (Pr=1, U=0.1), each
     with 1024 tracers and a nudging alpha drawn from {0, 0.1}; FP32-shifted
     populations.  Nudged members relax T toward synthetic observations at
     1024 seeded positions (a repeating series of 100 rows; T = conduction
-    profile + 0.01 seeded noise)."""
+    profile + 0.01 seeded noise).  Every member's draws are taken in order;
+    only the members in `keep` (all when None) are built.  Returns the built
+    members and the description of all 64."""
     rng = np.random.default_rng(seed)
     sizes = [(256, 128), (512, 256), (1024, 512)]
     members, desc = [], []
@@ -645,32 +697,52 @@ def ensemble_members(lb, device: int, seed: int = 41):
         nx, ny = sizes[int(rng.integers(3))]
         Ra = float(10 ** rng.uniform(5, 7))
         alpha = [0.0, 0.1][int(rng.integers(2))]
+        x = rng.uniform(0.5, nx + 0.5, ENS_TRACERS)
+        y = rng.uniform(1.0, ny, ENS_TRACERS)
+        if alpha:
+            ox = rng.uniform(0.5, nx + 0.5, (ENS_OBS_ROWS, ENS_TRACERS))
+            oy = rng.uniform(1.0, ny, (ENS_OBS_ROWS, ENS_TRACERS))
+            oT = 0.5 - (oy - 0.5) / ny + 0.01 * rng.standard_normal(oy.shape)
+        desc.append((nx, ny, Ra, alpha))
+        if keep is not None and i not in keep:
+            continue
         kw = dict(**lb.closure(nx, ny, Ra=Ra, Pr=1.0, U=0.1), precision="fp32", nprtcl=ENS_TRACERS,
                   device=device)
         if alpha:
             kw.update(nudge="bilinear", alpha=alpha, nobs=ENS_TRACERS, obs_cycle=1)
         r = lb.Run(**kw)
         r.init_conduction(seed * 1000 + i, 1e-3)
-        x = rng.uniform(0.5, nx + 0.5, ENS_TRACERS)
-        y = rng.uniform(1.0, ny, ENS_TRACERS)
         z = np.zeros(ENS_TRACERS)
         r.set_particles(np.arange(ENS_TRACERS, dtype=np.int32), x, y, z, z,
                         np.zeros(ENS_TRACERS, np.int32), z)
         if alpha:
-            ox = rng.uniform(0.5, nx + 0.5, (ENS_OBS_ROWS, ENS_TRACERS))
-            oy = rng.uniform(1.0, ny, (ENS_OBS_ROWS, ENS_TRACERS))
-            oT = 0.5 - (oy - 0.5) / ny + 0.01 * rng.standard_normal(oy.shape)
             r.nudge_obs(1, ox, oy, oT)
         members.append(r)
-        desc.append((nx, ny, Ra, alpha))
     return members, desc
 
 
-def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: int = -1) -> dict:
-    members, desc = ensemble_members(lb, device)
-    nodes = sum(nx * ny for nx, ny, _, _ in desc)
-    out = {}
-    with lb.Ensemble(members) as ens:
+def ensemble_desc(seed: int = 41):
+    """the 64 members' (nx, ny, Ra, alpha) without building any"""
+    return ensemble_members(None, 0, seed, keep=())[1]
+
+
+def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: int = -1, dist=None,
+                       rank: int = 0, world: int = 1) -> dict:
+    """The 64-member ensemble under its CUDA graph.  With several ranks the
+    members are split over them by node count (longest processing time
+    first), each rank runs its share as one ensemble, and the aggregate is
+    all nodes x steps over the slowest rank's time."""
+    from lagrangianrbnudging_b200 import shard
+
+    desc = ensemble_desc()
+    costs = [nx * ny for nx, ny, _, _ in desc]
+    keep = shard.my_units(costs, rank, world)
+    members, _ = ensemble_members(lb, device, keep=set(keep))
+    nodes = sum(costs)
+    my_nodes = sum(costs[i] for i in keep)
+    ms_mine, sched, t = 0.0, None, None
+    ens = lb.Ensemble(members) if members else None
+    if ens is not None:
         if variant >= 0:
             ens.set_schedule(variant)
         stream = torch.cuda.Stream()
@@ -683,16 +755,20 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
         ens.step(60)
         t = ens.get_timing()
         ens.set_timing(False)
-        torch.cuda.synchronize()
+    sync_ranks(torch, dist)
+    if ens is not None:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         ens.step(steps)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms_mine = e0.elapsed_time(e1)
         ens.sync()
         ens.set_stream(None)
+        ens.close()
+    ms = max_over_ranks(torch, dist, ms_mine)
+
     def is_finite(r):
         try:
             r.check_finite()
@@ -700,18 +776,23 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
         except lb.LbrbError:
             return False
 
-    finite = all(is_finite(r) for r in members)
-    nus = [r.nusselt() for r in members]
+    mine = {"members": len(keep), "nodes": my_nodes, "ms": ms_mine, "schedule": sched, "timing": t,
+            "finite": all(is_finite(r) for r in members), "nus": [r.nusselt() for r in members]}
     for r in members:
         r.close()
+    parts = shard.gather(dist, mine)
+    finite = all(p["finite"] for p in parts)
+    nus = [v for p in parts for v in p["nus"]]
+    t = parts[0]["timing"]
+    sched = parts[0]["schedule"]
     peak, _ = measured_peak()
     lb_ms = t["lb_step"][0] / max(t["lb_step"][1], 1)
     agg = nodes * ALG_BYTES["fp32"] * steps / (ms * 1e-3) / 1e9
-    lb_gbs = nodes * ALG_BYTES["fp32"] / (lb_ms * 1e-3) / 1e9
+    lb_gbs = parts[0]["nodes"] * ALG_BYTES["fp32"] / (lb_ms * 1e-3) / 1e9
     nudged = sum(1 for d in desc if d[3] > 0)
     out = {"members": ENS_N, "nodes": nodes, "steps": steps, "ms": round(ms, 2),
            "mlups": round(nodes * steps / (ms * 1e3), 1),
-           "aggregate_gbs": round(agg, 1), "aggregate_frac": round(agg / peak, 4),
+           "aggregate_gbs": round(agg, 1), "aggregate_frac": round(agg / (peak * world), 4),
            "lb_phase_ms": round(lb_ms, 5), "lb_phase_gbs": round(lb_gbs, 1),
            "lb_phase_frac": round(lb_gbs / peak, 4),
            "phase_share": {k: round(v[0] / sum(x[0] for x in t.values()), 4) for k, v in t.items()},
@@ -721,6 +802,11 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
                      f"[1e5,1e7], Pr=1, U=0.1, {ENS_TRACERS} tracers each, alpha in {{0,0.1}} "
                      f"({nudged} nudged), fp32-shifted; {steps} steps in CUDA-graph replays",
            "alg_bytes": "sum of nodes x 144 B per step"}
+    if world > 1:
+        out["ranks"] = [{"members": p["members"], "nodes": p["nodes"], "ms": round(p["ms"], 2)}
+                        for p in parts]
+        out["split"] = "members over the ranks by node count (longest processing time first)"
+        out["lb_phase"] = "rank 0's share"
     return out
 
 
