@@ -295,6 +295,40 @@ LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, c
                                 int precision, int nx, int ny, int pitch, double relaxg,
                                 double Tup, double Tdown, void *cuda_stream, double *out3);
 
+/* ---- One domain over several GPUs: y-slabs ------------------------------
+ * Replaces the reference's domain decomposition over MPI ranks and its halo
+ * refresh of the populations around the stream (pbc, temppart_dump.c:234-250,
+ * called in the loop at temppart_dump.c:1674-1759) for a split in y.
+ * A handle created with ny rows becomes rows [j0, j0 + ny) of a domain of
+ * ny_total rows.  Only the slab at j0 = 0 has the bottom wall and only the
+ * slab ending at ny_total the top wall.  Across an inner boundary a step
+ * pulls the three f and three g populations that cross it from the
+ * handle's ghost rows, which must hold the neighbour slab's boundary row
+ * after its previous step.  The slabs of one domain then advance exactly as
+ * the whole domain in one handle would, bit for bit.
+ * lbrb_init_conduction on a slab gives the whole domain's profile and noise
+ * at its rows; lbrb_nusselt gives the slab's mean of v T at the whole
+ * domain's height (the domain's Nu is the slabs' values weighted by ny).
+ * Supported: Dirichlet walls, no nudging, no particles. */
+LBRB_API int lbrb_slab_set(lbrb_t *h, int j0, int ny_total);
+/* bytes of one packed boundary row set: 6 rows (f then g) of nx values */
+LBRB_API size_t lbrb_slab_ghost_bytes(const lbrb_t *h);
+/* device buffers of a slab: `up` and `down` receive lbrb_slab_pack's output
+ * (the top row's upward populations f2 f5 f6 g2 g5 g6 for the slab above;
+ * the bottom row's downward f4 f7 f8 g4 g7 g8 for the slab below);
+ * `ghost_lo` / `ghost_hi` are the rows below row 0 / above row ny-1 (NULL at
+ * a wall).  One process per GPU: after lbrb_slab_pack, send `up` to the slab
+ * above's ghost_lo and `down` to the slab below's ghost_hi (NCCL send/recv
+ * of lbrb_slab_ghost_bytes on the handle's stream), then lbrb_step(h, 1). */
+LBRB_API int lbrb_slab_buffers(lbrb_t *h, void **up, void **down, void **ghost_lo, void **ghost_hi);
+LBRB_API int lbrb_slab_pack(lbrb_t *h);
+/* nsteps steps of a whole domain whose slabs this process holds (one or
+ * several GPUs), slabs in order of j0: per step, every slab packs and copies
+ * its boundary rows into its neighbours' ghost rows (peer copies across
+ * GPUs), then steps; events order the copies against the neighbours' steps.
+ * The moments (rho, u, v, T) are written on the last of the nsteps. */
+LBRB_API int lbrb_slab_step(lbrb_t *const *slabs, int nslabs, int nsteps);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,7 @@ EXPORTS = [
     "lbrb_ensemble_nvariants", "lbrb_ensemble_set_schedule", "lbrb_ensemble_get_schedule",
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
+    "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
 ]
 
 
@@ -128,6 +129,11 @@ def lib() -> C.CDLL:
         "lbrb_adjoint_variants": (C.c_int, []),
         "lbrb_adjoint_set_variant": (C.c_int, [vp, C.c_int]),
         "lbrb_adjoint_get_variant": (C.c_int, [vp, ip]),
+        "lbrb_slab_set": (C.c_int, [vp, C.c_int, C.c_int]),
+        "lbrb_slab_ghost_bytes": (C.c_size_t, [vp]),
+        "lbrb_slab_buffers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "lbrb_slab_pack": (C.c_int, [vp]),
+        "lbrb_slab_step": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -392,6 +398,90 @@ class Run:
         out = np.empty((self.ny, 9))
         self._ck(lib().lbrb_profile(self.h, _dp(out)))
         return out
+
+
+class SlabDomain:
+    """One domain of nx x ny_total nodes cut into y-slabs, one handle each
+    (on one or several GPUs of this process): lbrb_slab_set on each slab and
+    lbrb_slab_step for the whole domain.  The slabs advance exactly as the
+    whole domain in one handle would.
+
+    heights: rows per slab, bottom to top; devices: one CUDA device per slab
+    (default: all on `device`); params as for Run, with ny the whole
+    domain's rows (each slab gets its own height)."""
+
+    def __init__(self, heights, devices=None, **params):
+        ny_total = int(params["ny"])
+        heights = [int(h) for h in heights]
+        if sum(heights) != ny_total or min(heights) < 3:
+            raise ValueError("slab heights must be >= 3 (a handle's minimum) and add up to ny")
+        devices = list(devices) if devices is not None else [params.get("device", 0)] * len(heights)
+        if len(devices) != len(heights):
+            raise ValueError("one device per slab")
+        self.nx, self.ny = int(params["nx"]), ny_total
+        self.heights = heights
+        self.slabs = []
+        j0 = 0
+        try:
+            for hgt, dev in zip(heights, devices):
+                r = Run(**dict(params, ny=hgt, device=dev))
+                self.slabs.append(r)
+                r._ck(lib().lbrb_slab_set(r.h, j0, ny_total))
+                j0 += hgt
+        except Exception:
+            self.close()
+            raise
+        self._arr = (C.c_void_p * len(self.slabs))(*[r.h for r in self.slabs])
+
+    def close(self):
+        for r in self.slabs:
+            r.close()
+        self.slabs = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def init_conduction(self, seed: int, noise: float):
+        """the whole domain's seeded conduction state, each slab its rows"""
+        for r in self.slabs:
+            r.init_conduction(seed, noise)
+
+    def step(self, n: int):
+        rc = lib().lbrb_slab_step(self._arr, len(self.slabs), int(n))
+        if rc:
+            for r in self.slabs:
+                msg = lib().lbrb_last_error(r.h)
+                if msg:
+                    raise LbrbError(rc, msg.decode())
+            raise LbrbError(rc, "slab_step")
+
+    def set_populations(self, f, g):
+        """whole-domain populations, SoA (9, ny, nx) each"""
+        j0 = 0
+        for r, hgt in zip(self.slabs, self.heights):
+            r.set_populations(f[:, j0:j0 + hgt], g[:, j0:j0 + hgt])
+            j0 += hgt
+
+    def set_moments(self, rho, u, v, T):
+        j0 = 0
+        for r, hgt in zip(self.slabs, self.heights):
+            r.set_moments(rho[j0:j0 + hgt], u[j0:j0 + hgt], v[j0:j0 + hgt], T[j0:j0 + hgt])
+            j0 += hgt
+
+    def get_populations(self):
+        parts = [r.get_populations() for r in self.slabs]
+        return np.concatenate([p[0] for p in parts], axis=1), np.concatenate([p[1] for p in parts], axis=1)
+
+    def get_moments(self):
+        parts = [r.get_moments() for r in self.slabs]
+        return {k: np.concatenate([p[k] for p in parts], axis=0) for k in ("rho", "u", "v", "T")}
+
+    def nusselt(self) -> float:
+        """the slabs' values weighted by their heights"""
+        return float(sum(hgt * r.nusselt() for r, hgt in zip(self.slabs, self.heights)) / self.ny)
 
 
 class Ensemble:

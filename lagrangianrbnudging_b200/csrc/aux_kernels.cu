@@ -157,14 +157,18 @@ __global__ void init_conduction_kernel(Real* __restrict__ pops, Real* __restrict
                                        Real* __restrict__ u, Real* __restrict__ v,
                                        Real* __restrict__ T, int nx, int ny, int pitch,
                                        size_t plane, double Tup, double Tdown, double T0,
-                                       double neg_gravity, uint64_t seed, double noise) {
+                                       double neg_gravity, uint64_t seed, double noise, int j0,
+                                       int ny_total) {
+  // rows [j0, j0 + ny) of a domain of ny_total rows (a y-slab; j0 = 0 and
+  // ny_total = ny for a whole domain): profile and noise by global node
   const long n = (long)nx * ny;
   const double dT = Tup - Tdown;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const int i = (int)(q % nx), j = (int)(q / nx);
-    const uint64_t z = splitmix64(seed + ((uint64_t)q + 1ULL) * 0x9E3779B97F4A7C15ULL);
+    const long qg = q + (long)j0 * nx;
+    const uint64_t z = splitmix64(seed + ((uint64_t)qg + 1ULL) * 0x9E3779B97F4A7C15ULL);
     const double un = (double)(z >> 11) * (1.0 / 9007199254740992.0);
-    const double t = Tdown + dT * (((double)j + 0.5) / (double)ny) + noise * (2.0 * un - 1.0);
+    const double t = Tdown + dT * (((double)(j0 + j) + 0.5) / (double)ny_total) + noise * (2.0 * un - 1.0);
     double feq[NPOP], geq[NPOP];
     equil_ref(1.0, 0.0, 0.0, feq);
     equil_ref(t, 0.0, 0.0, geq);
@@ -372,16 +376,45 @@ cudaError_t launch_moments_from_pre(const double* fpre, const double* gpre, int 
 cudaError_t launch_init_conduction(void* pops, void* rho, void* u, void* v, void* T, bool fp32,
                                    int nx, int ny, int pitch, size_t plane, double Tup,
                                    double Tdown, double T0, double neg_gravity, uint64_t seed,
-                                   double noise, cudaStream_t s) {
+                                   double noise, int j0, int ny_total, cudaStream_t s) {
   const int g = grid_for((long)nx * ny);
   if (fp32)
     init_conduction_kernel<float><<<g, 256, 0, s>>>((float*)pops, (float*)rho, (float*)u, (float*)v,
                                                     (float*)T, nx, ny, pitch, plane, Tup, Tdown, T0,
-                                                    neg_gravity, seed, noise);
+                                                    neg_gravity, seed, noise, j0, ny_total);
   else
     init_conduction_kernel<double><<<g, 256, 0, s>>>((double*)pops, (double*)rho, (double*)u,
                                                      (double*)v, (double*)T, nx, ny, pitch, plane,
-                                                     Tup, Tdown, T0, neg_gravity, seed, noise);
+                                                     Tup, Tdown, T0, neg_gravity, seed, noise, j0,
+                                                     ny_total);
+  return cudaGetLastError();
+}
+
+// y-slab exchange: this slab's top row's upward populations (f2, f5, f6,
+// g2, g5, g6) into `up` and its bottom row's downward ones (f4, f7, f8, g4,
+// g7, g8) into `down`, each 6 rows of nx values: the neighbours' ghost rows
+template <typename Real>
+__global__ void slab_pack_kernel(const Real* __restrict__ pops, int nx, int ny, int pitch, size_t plane,
+                                 Real* __restrict__ up, Real* __restrict__ down) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;  // 0..5: f then g, three populations each
+  if (x >= nx) return;
+  const int g = r / 3, m = r % 3;
+  const int kup = m == 0 ? 2 : (m == 1 ? 5 : 6), kdn = m == 0 ? 4 : (m == 1 ? 7 : 8);
+  const Real* base = pops + (size_t)g * NPOP * plane;
+  up[(size_t)r * nx + x] = base[(size_t)kup * plane + (size_t)(ny - 1) * pitch + x];
+  down[(size_t)r * nx + x] = base[(size_t)kdn * plane + x];
+}
+
+cudaError_t launch_slab_pack(const void* pops, bool fp32, int nx, int ny, int pitch, size_t plane, void* up,
+                             void* down, cudaStream_t s) {
+  dim3 grid((nx + 127) / 128, 6);
+  if (fp32)
+    slab_pack_kernel<float><<<grid, 128, 0, s>>>((const float*)pops, nx, ny, pitch, plane, (float*)up,
+                                                 (float*)down);
+  else
+    slab_pack_kernel<double><<<grid, 128, 0, s>>>((const double*)pops, nx, ny, pitch, plane, (double*)up,
+                                                  (double*)down);
   return cudaGetLastError();
 }
 

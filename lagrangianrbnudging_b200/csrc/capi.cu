@@ -132,6 +132,9 @@ static void free_all(lbrb_t* h) {
   delete[] h->h_chk; delete[] h->h_oid;
   F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
+  F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down);
+  if (h->slab_ev_xfer) cudaEventDestroy(h->slab_ev_xfer);
+  if (h->slab_ev_done) cudaEventDestroy(h->slab_ev_done);
   delete[] h->adj_steps;
   if (h->h_flags) cudaFreeHost(h->h_flags);
   if (h->h_scalar) cudaFreeHost(h->h_scalar);
@@ -374,7 +377,8 @@ int lbrb_init_conduction(lbrb_t* h, uint64_t seed, double noise) {
   CK(h, cudaSetDevice(h->dev));
   CK(h, launch_init_conduction(h->pops[h->cur], h->rho[h->cur], h->uv[h->uvcur][0],
                                h->uv[h->uvcur][1], h->T[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->p.Tup,
-                               h->p.Tdown, T0_of(h), -h->p.gravity, seed, noise, h->stream));
+                               h->p.Tdown, T0_of(h), -h->p.gravity, seed, noise, h->slab ? h->slab_j0 : 0,
+                               h->slab ? h->slab_ny_total : h->p.ny, h->stream));
   CK(h, launch_force(h->rho[h->cur], h->T[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   h->moments_valid = true;
@@ -600,6 +604,8 @@ int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
   if (n == 0) return LBRB_OK;
+  if (h->slab && n != 1)
+    return fail(h, LBRB_ERR_ARG, "step: a y-slab takes one step per boundary exchange (lbrb_slab_step)");
   if (!h->moments_valid)
     return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
   if (h->np > 0 && !h->particles_set) return fail(h, LBRB_ERR_STATE, "step: particles not set");
@@ -628,7 +634,7 @@ int lbrb_step(lbrb_t* h, int n) {
   bool pt_queued = false;
   for (int s = 0; s < n; s++) {
     const int istep = h->istep + 1;
-    const bool last = (s == n - 1);
+    const bool last = (s == n - 1) && !h->slab_defer_moments;
     const bool rec = h->np > 0 && h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
     if (rec && (h->rec_head - h->rec_tail) >= h->p.record_slots)
       return fail(h, LBRB_ERR_OVERFLOW, "step: record ring full, drain records first");
@@ -792,6 +798,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   NvtxRange nvtx("lbrb_adjoint_window");
   if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE)
     return fail(h, LBRB_ERR_UNSUPPORTED, "adjoint_window: Dirichlet walls without nudging only");
+  if (h->slab) return fail(h, LBRB_ERR_UNSUPPORTED, "adjoint_window: whole domains only, not a y-slab");
   if (!h->adj_obs) return fail(h, LBRB_ERR_STATE, "adjoint_window: no observations set");
   CK(h, cudaSetDevice(h->dev));
   const bool f32 = fp32(h);
@@ -1032,6 +1039,114 @@ int lbrb_adjoint_get_variant(const lbrb_t* h, int* variant) {
   return LBRB_OK;
 }
 
+// ------------------------------------------------------------ y-slabs
+// One domain over several GPUs, cut into slabs of rows.  The reference cuts
+// its domain over MPI ranks and refreshes halo rows of the populations by
+// message passing (pbc, temppart_dump.c:234-250, called around the stream in
+// the loop, temppart_dump.c:1674-1759); here a slab's step pulls
+// the three f and three g populations that cross an inner boundary from
+// ghost rows filled from the neighbour's boundary row (lbrb_slab_pack), and
+// the walls apply only at the domain's own bottom and top.
+int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
+  if (!h) return LBRB_ERR_ARG;
+  if (j0 < 0 || ny_total < 2 || j0 + h->p.ny > ny_total)
+    return fail(h, LBRB_ERR_ARG, "slab_set: rows [j0, j0 + ny) must lie in [0, ny_total)");
+  if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE || h->np > 0)
+    return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls, no nudging and no particles");
+  CK(h, cudaSetDevice(h->dev));
+  const size_t gb = lbrb_slab_ghost_bytes(h);
+  void** bufs[] = {&h->slab_ghost_lo, &h->slab_ghost_hi, &h->slab_up, &h->slab_down};
+  for (void** b : bufs) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+  }
+  // ghost rows only across inner boundaries (none at a wall of the domain)
+  if (j0 > 0 && cudaMalloc(&h->slab_ghost_lo, gb) != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "slab ghosts");
+  if (j0 + h->p.ny < ny_total && cudaMalloc(&h->slab_ghost_hi, gb) != cudaSuccess)
+    return fail(h, LBRB_ERR_NOMEM, "slab ghosts");
+  if (cudaMalloc(&h->slab_up, gb) != cudaSuccess || cudaMalloc(&h->slab_down, gb) != cudaSuccess)
+    return fail(h, LBRB_ERR_NOMEM, "slab boundary rows");
+  for (void* b : {h->slab_ghost_lo, h->slab_ghost_hi, h->slab_up, h->slab_down})
+    if (b) CK(h, cudaMemsetAsync(b, 0, gb, h->stream));
+  if (!h->slab_ev_xfer) CK(h, cudaEventCreateWithFlags(&h->slab_ev_xfer, cudaEventDisableTiming));
+  if (!h->slab_ev_done) CK(h, cudaEventCreateWithFlags(&h->slab_ev_done, cudaEventDisableTiming));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->slab = true;
+  h->slab_j0 = j0;
+  h->slab_ny_total = ny_total;
+  return LBRB_OK;
+}
+
+size_t lbrb_slab_ghost_bytes(const lbrb_t* h) { return h ? 6 * (size_t)h->p.nx * h->esize : 0; }
+
+int lbrb_slab_buffers(lbrb_t* h, void** up, void** down, void** ghost_lo, void** ghost_hi) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->slab) return fail(h, LBRB_ERR_STATE, "slab_buffers: not a y-slab (lbrb_slab_set)");
+  if (up) *up = h->slab_up;
+  if (down) *down = h->slab_down;
+  if (ghost_lo) *ghost_lo = h->slab_ghost_lo;
+  if (ghost_hi) *ghost_hi = h->slab_ghost_hi;
+  return LBRB_OK;
+}
+
+int lbrb_slab_pack(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->slab) return fail(h, LBRB_ERR_STATE, "slab_pack: not a y-slab (lbrb_slab_set)");
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, launch_slab_pack(h->pops[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->slab_up,
+                         h->slab_down, h->stream));
+  return LBRB_OK;
+}
+
+int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
+  if (!slabs || n < 1 || nsteps < 0) return LBRB_ERR_ARG;
+  for (int s = 0; s < n; s++) {
+    const lbrb_t* h = slabs[s];
+    if (!h || !h->slab) return LBRB_ERR_ARG;
+    const lbrb_t* h0 = slabs[0];
+    if (h->p.nx != h0->p.nx || h->esize != h0->esize || h->slab_ny_total != h0->slab_ny_total)
+      return LBRB_ERR_ARG;
+    // slabs in order, each starting where the previous ends
+    if (h->slab_j0 != (s == 0 ? 0 : slabs[s - 1]->slab_j0 + slabs[s - 1]->p.ny)) return LBRB_ERR_ARG;
+  }
+  if (slabs[n - 1]->slab_j0 + slabs[n - 1]->p.ny != slabs[0]->slab_ny_total) return LBRB_ERR_ARG;
+  const size_t gb = lbrb_slab_ghost_bytes(slabs[0]);
+  for (int it = 0; it < nsteps; it++) {
+    // 1. each slab packs its boundary rows and copies them into its
+    //    neighbours' ghost rows, once the neighbours' previous step (which
+    //    read those ghost rows) is done
+    for (int s = 0; s < n; s++) {
+      lbrb_t* h = slabs[s];
+      CK(h, cudaSetDevice(h->dev));
+      if (it > 0) {
+        if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_done, 0));
+        if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_done, 0));
+      }
+      int rc = lbrb_slab_pack(h);
+      if (rc) return rc;
+      if (s + 1 < n)
+        CK(h, cudaMemcpyPeerAsync(slabs[s + 1]->slab_ghost_lo, slabs[s + 1]->dev, h->slab_up, h->dev, gb, h->stream));
+      if (s > 0)
+        CK(h, cudaMemcpyPeerAsync(slabs[s - 1]->slab_ghost_hi, slabs[s - 1]->dev, h->slab_down, h->dev, gb, h->stream));
+      CK(h, cudaEventRecord(h->slab_ev_xfer, h->stream));
+    }
+    // 2. each slab steps once its ghost rows are filled
+    for (int s = 0; s < n; s++) {
+      lbrb_t* h = slabs[s];
+      CK(h, cudaSetDevice(h->dev));
+      if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_xfer, 0));
+      if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_xfer, 0));
+      // the moments (rho, u, v, T) are written on the last step only
+      h->slab_defer_moments = it + 1 < nsteps;
+      int rc = lbrb_step(h, 1);
+      h->slab_defer_moments = false;
+      if (rc) return rc;
+      CK(h, cudaEventRecord(h->slab_ev_done, h->stream));
+    }
+  }
+  return LBRB_OK;
+}
+
 int lbrb_set_stream(lbrb_t* h, void* cuda_stream) {
   if (!h) return LBRB_ERR_ARG;
   CK(h, cudaSetDevice(h->dev));
@@ -1121,7 +1236,10 @@ int lbrb_nusselt(lbrb_t* h, double* nu) {
   if (rc) return rc;
   const double nn = (double)h->p.nx * (double)h->p.ny;
   const double kappa = (h->p.relaxg - 0.5) / 3.0;
-  *nu = 1.0 + (s[2] / nn) * (double)h->p.ny / (kappa * (h->p.Tdown - h->p.Tup));
+  // (a y-slab: its mean of v T at the whole domain's height; the domain's Nu
+  // is the slabs' values weighted by their heights)
+  const double H = h->slab ? (double)h->slab_ny_total : (double)h->p.ny;
+  *nu = 1.0 + (s[2] / nn) * H / (kappa * (h->p.Tdown - h->p.Tup));
   return LBRB_OK;
 }
 

@@ -54,7 +54,9 @@ cudaError_t launch_moments_from_pre(const double* fpre, const double* gpre, int 
 cudaError_t launch_init_conduction(void* pops, void* rho, void* u, void* v, void* T, bool fp32,
                                    int nx, int ny, int pitch, size_t plane, double Tup,
                                    double Tdown, double T0, double neg_gravity, uint64_t seed,
-                                   double noise, cudaStream_t s);
+                                   double noise, int j0, int ny_total, cudaStream_t s);
+cudaError_t launch_slab_pack(const void* pops, bool fp32, int nx, int ny, int pitch, size_t plane, void* up,
+                             void* down, cudaStream_t s);
 cudaError_t launch_stats(const void* rho, const void* u, const void* v, const void* T, bool fp32,
                          int nx, int ny, int pitch, double* part, double* out, cudaStream_t s);
 cudaError_t launch_profile(const void* rho, const void* u, const void* v, const void* T, bool fp32,
@@ -177,5 +179,7 @@ inline LBView<Real> make_view(lbrb_t* h, int src, int dst, int uvslot, int write
   V.alpha = h->p.alpha;
   V.write_uv = write_uv;
   V.write_rt = write_rt;
+  V.ghost_lo = (const Real*)h->slab_ghost_lo;
+  V.ghost_hi = (const Real*)h->slab_ghost_hi;
   return V;
 }

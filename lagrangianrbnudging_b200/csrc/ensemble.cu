@@ -315,6 +315,7 @@ int lbrb_ensemble_create(lbrb_t* const* members, int n, lbrb_ensemble_t** out) {
       return LBRB_ERR_ARG;
     if (h->p.nudge == LBRB_NUDGE_REFBOX) return LBRB_ERR_UNSUPPORTED;
     if (h->np > 0 && h->p.noutconfig > 0) return LBRB_ERR_UNSUPPORTED;
+    if (h->slab) return LBRB_ERR_UNSUPPORTED;  // members are whole domains
   }
   lbrb_ensemble_t* e = new lbrb_ensemble_t();
   e->m.assign(members, members + n);

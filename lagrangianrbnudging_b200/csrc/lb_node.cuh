@@ -176,6 +176,14 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
     constexpr int k = decltype(kc)::value;
     const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
     const int js = j - icy(k);
+    // y-slab boundary inside the domain: the neighbour's boundary row
+    const Real* gh = js < 0 ? V.ghost_lo : (js >= V.ny ? V.ghost_hi : nullptr);
+    if (gh) {
+      constexpr int slot = (k == 2 || k == 4) ? 0 : ((k == 5 || k == 7) ? 1 : 2);
+      fs[k] = gh[(size_t)slot * V.nx + xs];
+      gs[k] = gh[(size_t)(3 + slot) * V.nx + xs];
+      return;
+    }
     if (js < 0 || js >= V.ny)
       fs[k] = __ldcs(V.fsrc + ((Off)opp(k) * pl + oc + (Off)x));
     else
@@ -198,13 +206,13 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
 // (temppart_dump.c:896-921): g_in = -g_opp + 2 w T_wall (shifted form: T_wall - T0)
 template <typename Real>
 __device__ __forceinline__ void dirichlet_walls(const LBView<Real>& V, int j, Real* gs) {
-  if (j == V.ny - 1) {
+  if (j == V.ny - 1 && !V.ghost_hi) {
     const Real tw = std::is_same<Real, double>::value ? (Real)V.Tup : (Real)(V.Tup - V.T0);
     gs[4] = -gs[2] + Real(2.0 * w_of(2)) * tw;
     gs[7] = -gs[5] + Real(2.0 * w_of(5)) * tw;
     gs[8] = -gs[6] + Real(2.0 * w_of(6)) * tw;
   }
-  if (j == 0) {
+  if (j == 0 && !V.ghost_lo) {
     const Real tw = std::is_same<Real, double>::value ? (Real)V.Tdown : (Real)(V.Tdown - V.T0);
     gs[2] = -gs[4] + Real(2.0 * w_of(4)) * tw;
     gs[5] = -gs[7] + Real(2.0 * w_of(7)) * tw;

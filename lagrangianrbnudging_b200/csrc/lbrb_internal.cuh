@@ -106,6 +106,11 @@ struct LBView {
   double* __restrict__ nud_term;
   double alpha;
   int write_uv, write_rt;
+  // y-slab of a larger domain: the rows below row 0 / above row ny-1 (the
+  // neighbour slab's boundary row after its collision), 6 rows of nx values:
+  // f then g of the three populations crossing the boundary; null = wall
+  const Real* __restrict__ ghost_lo;
+  const Real* __restrict__ ghost_hi;
 };
 
 // --------------------------------------------------------------- handle
@@ -123,6 +128,18 @@ struct Handle {
   int istep = 0;  // steps done (the reference's istep of the last step)
   int pitch = 0;
   size_t plane = 0;   // ny * pitch
+  // y-slab mode: rows [slab_j0, slab_j0 + ny) of ny_total; ghost rows below
+  // and above (null at a wall), this slab's packed boundary rows (up: the top
+  // row's upward populations, down: the bottom row's downward ones), events
+  // ordering the exchange between neighbours
+  bool slab = false;
+  int slab_j0 = 0, slab_ny_total = 0;
+  void* slab_ghost_lo = nullptr;
+  void* slab_ghost_hi = nullptr;
+  void* slab_up = nullptr;
+  void* slab_down = nullptr;
+  cudaEvent_t slab_ev_xfer = nullptr, slab_ev_done = nullptr;
+  bool slab_defer_moments = false;  // inside lbrb_slab_step: moments on its last step only
   size_t esize = 8;   // bytes per population value
   // populations: pops[buf] holds f (9 planes) then g (9 planes)
   void* pops[2] = {nullptr, nullptr};
