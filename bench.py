@@ -345,6 +345,8 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     if not args.no_ensemble:
         sec["ensemble"] = run_ensemble_bench(lb, torch, device, args.ensemble_steps, dist=dist, rank=rank,
                                              world=world)
+    if world == 1 and not args.no_slab:
+        sec["slab"] = run_slab_bench(lb, torch, device)
     if rank != 0:
         return None
     mlups = whole_job_mlups(world, nodes, K, ms)
@@ -810,6 +812,50 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
     return out
 
 
+# ------------------------------------------------------------- y-slabs
+SLAB_STEPS = 200
+
+
+def run_slab_bench(lb, torch, device: int, steps: int = SLAB_STEPS, devices=None) -> dict:
+    """The headline grid (FP32-shifted, no particles) as one handle and as a
+    domain of 2 and 4 y-slabs (lbrb_slab_step: per step a pack kernel and
+    peer copies of the crossing populations, then the fused kernel per slab).
+    With one GPU the slabs share it (all on one stream), which measures the
+    exchange's cost; the end states must equal the single handle's bit for
+    bit (T and u compared)."""
+    base = dict(**lb.closure(NX, NY, Ra=RA, Pr=PR, U=U), precision="fp32")
+    stream = torch.cuda.Stream()
+
+    def timed(obj, set_stream):
+        set_stream(stream.cuda_stream)
+        obj.init_conduction(SEED, 1e-3)
+        obj.step(20)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        obj.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        m = obj.get_moments()
+        return e0.elapsed_time(e1), m
+
+    nodes = NX * NY
+    with lb.Run(**base, device=device) as whole:
+        ms1, m1 = timed(whole, whole.set_stream)
+    out = {"grid": f"{NX}x{NY}", "steps": steps, "single_handle_mlups": round(nodes * steps / (ms1 * 1e3), 1)}
+    for n in (2, 4):
+        with lb.SlabDomain([NY // n] * n, devices=devices, **base, device=device) as dom:
+            ms, m = timed(dom, lambda st: [r.set_stream(st) for r in dom.slabs])
+            exact = all(np.array_equal(m[k], m1[k]) for k in ("T", "u"))
+            for r in dom.slabs:
+                r.set_stream(None)
+        out[f"slabs_{n}"] = {"mlups": round(nodes * steps / (ms * 1e3), 1),
+                             "vs_single_handle": round(ms1 / ms, 4), "bit_exact_T_u": bool(exact)}
+    out["note"] = ("slabs on one GPU and one stream: the figure is the exchange's overhead; "
+                   "across GPUs each slab runs on its own device")
+    return out
+
+
 # ---------------------------------------------------------- reference arm
 def ref_params() -> dict:
     nu = U * NY * np.sqrt(PR / RA)
@@ -1065,6 +1111,9 @@ def main():
                     help="fixed launch variant of the ensemble's fused phase (-1: autotune)")
     ap.add_argument("--config0", action="store_true",
                     help="the 512x256 tracer case on the GPU and the reference CPU build")
+    ap.add_argument("--no-slab", action="store_true", help="skip the y-slab section")
+    ap.add_argument("--slab-only", action="store_true",
+                    help="only the y-slab section (one domain as 2 and 4 slabs against one handle)")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="only the adjoint window (the command used for ncu captures of the adjoint kernels)")
     ap.add_argument("--adjoint-steps", type=int, default=ADJ_STEPS)
@@ -1104,6 +1153,14 @@ def main():
         b.build()
         torch.cuda.set_device(0)
         print(json.dumps({"mode": "config0", **run_config0(lb, torch, 0)}), flush=True)
+        return
+    if args.slab_only:
+        import lagrangianrbnudging_b200 as lb
+        from lagrangianrbnudging_b200 import build as b
+
+        b.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"mode": "slab-only", **run_slab_bench(lb, torch, 0)}), flush=True)
         return
     if args.adjoint_only:
         import lagrangianrbnudging_b200 as lb
