@@ -28,10 +28,12 @@ __device__ __forceinline__ void static_for(F&& f) {
 }
 
 // ------------------------------------------------ reference-order FP64 node
-template <bool REFNUDGE>
+// SF(k, value), SG(k, value): store a post-collision population as soon as
+// it is computed (short live ranges; the operation order is unchanged)
+template <bool REFNUDGE, typename SF, typename SG>
 __device__ __forceinline__ void node_ref(const LBView<double>& V, size_t idx, double* fs,
                                          double* gs, double& Fy_io, double& r_out, double& u_out,
-                                         double& v_out, double& t_out) {
+                                         double& v_out, double& t_out, SF&& store_f, SG&& store_g) {
   double r = 0.0, t = 0.0;
 #pragma unroll
   for (int k = 0; k < NPOP; k++) r = r + fs[k];
@@ -59,17 +61,24 @@ __device__ __forceinline__ void node_ref(const LBView<double>& V, size_t idx, do
     double factor = ((dcx(k) - u) * Fx + (dcy(k) - v) * Fy) / CS2;
     factor = factor + ((dcx(k) * u + dcy(k) * v) * (dcx(k) * Fx + dcy(k) * Fy)) / (CS2 * CS2);
     fs[k] = fs[k] * (1. - omega) + omega * feq[k] + source * factor;
+    store_f(k, fs[k]);
   });
   equil_ref(t, u, v, feq);
   if (REFNUDGE && nv > 0) {
     const double B = 1.0 - 0.5 * omegag;
     const double Q = V.alpha * (t - V.tempreadint[idx]);
 #pragma unroll
-    for (int k = 0; k < NPOP; k++) gs[k] = gs[k] * (1. - omegag) + omegag * feq[k] - B * w_of(k) * Q;
+    for (int k = 0; k < NPOP; k++) {
+      gs[k] = gs[k] * (1. - omegag) + omegag * feq[k] - B * w_of(k) * Q;
+      store_g(k, gs[k]);
+    }
     V.nud_term[idx] = -1. * Q;
   } else {
 #pragma unroll
-    for (int k = 0; k < NPOP; k++) gs[k] = gs[k] * (1. - omegag) + omegag * feq[k];
+    for (int k = 0; k < NPOP; k++) {
+      gs[k] = gs[k] * (1. - omegag) + omegag * feq[k];
+      store_g(k, gs[k]);
+    }
   }
   // buoyancy of the next step from this step's moments (forcingconstructWW)
   Fy_io = V.neg_gravity * r * (t - 0.0);
@@ -233,14 +242,17 @@ __device__ __forceinline__ void lb_update_node(const LBView<Real>& V, int j, int
   const Off o = (Off)j * (Off)V.pitch + (Off)x;
   Real Fy = V.Fin[o], r, u, v, t;
   if constexpr (std::is_same<Real, double>::value) {
-    node_ref<REFNUDGE>(V, (size_t)o, fs, gs, Fy, r, u, v, t);
+    node_ref<REFNUDGE>(
+        V, (size_t)o, fs, gs, Fy, r, u, v, t,
+        [&](int k, double val) { __stcs(V.fdst + ((Off)k * pl + o), val); },
+        [&](int k, double val) { __stcs(V.gdst + ((Off)k * pl + o), val); });
   } else {
     node_shift(V, fs, gs, Fy, r, u, v, t);
-  }
 #pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    __stcs(V.fdst + ((Off)k * pl + o), fs[k]);
-    __stcs(V.gdst + ((Off)k * pl + o), gs[k]);
+    for (int k = 0; k < NPOP; k++) {
+      __stcs(V.fdst + ((Off)k * pl + o), fs[k]);
+      __stcs(V.gdst + ((Off)k * pl + o), gs[k]);
+    }
   }
   V.Fout[o] = Fy;
   if (V.write_uv) {
