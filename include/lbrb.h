@@ -158,6 +158,14 @@ LBRB_API int lbrb_check_finite(lbrb_t *h);
  * its record copies back into this stream before returning, so an event
  * recorded on it after lbrb_step() covers the whole step. */
 LBRB_API int lbrb_set_stream(lbrb_t *h, void *cuda_stream);
+/* CUDA-graph replay inside lbrb_step: runs of 3 steps without a record
+ * replay a graph of the same launches (one graph per buffer phase, captured
+ * on first use), so small grids are not bound by the host's per-launch
+ * enqueue.  Results are identical either way.  -1 (the default): grids of
+ * at most 2^20 nodes; 0: off; 1: every grid.  Not used with nudging,
+ * per-kernel timing, a y-slab or the legacy default stream.  No counterpart
+ * in the reference. */
+LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
 /* Per-kernel device timing with CUDA events around each launch.  Classes:
  * 0 fused stream/collide, 1 particles, 2 nudging, 3 record copies.
  * lbrb_get_timing() waits, returns total milliseconds and launch counts per

@@ -45,6 +45,7 @@ EXPORTS = [
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
+    "lbrb_set_graph",
 ]
 
 
@@ -134,6 +135,7 @@ def lib() -> C.CDLL:
         "lbrb_slab_buffers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
         "lbrb_slab_pack": (C.c_int, [vp]),
         "lbrb_slab_step": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int]),
+        "lbrb_set_graph": (C.c_int, [vp, C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -365,6 +367,10 @@ class Run:
     # ---- streams and timing
     def set_stream(self, stream_handle: int | None):
         self._ck(lib().lbrb_set_stream(self.h, C.c_void_p(stream_handle or 0)))
+
+    def set_graph(self, mode: int):
+        """CUDA-graph replay of plain steps: -1 small grids (default), 0 off, 1 on"""
+        self._ck(lib().lbrb_set_graph(self.h, int(mode)))
 
     def set_timing(self, enable: bool):
         self._ck(lib().lbrb_set_timing(self.h, int(bool(enable))))

@@ -133,6 +133,8 @@ static void free_all(lbrb_t* h) {
   F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
   F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down);
+  for (cudaGraphExec_t& g : h->graph_exec)
+    if (g) cudaGraphExecDestroy(g);
   if (h->slab_ev_xfer) cudaEventDestroy(h->slab_ev_xfer);
   if (h->slab_ev_done) cudaEventDestroy(h->slab_ev_done);
   delete[] h->adj_steps;
@@ -600,6 +602,17 @@ int lbrb_get_poststream(lbrb_t* h, double* f, double* g, int layout) {
   return LBRB_OK;
 }
 
+// CUDA-graph replay of plain steps: grids up to GRAPH_MAX_NODES nodes (where
+// the host's per-launch enqueue is comparable to the step), a capturable
+// stream (not the legacy default stream), no nudging, no per-kernel timing,
+// particle kernels on the step stream, not a y-slab
+constexpr int GRAPH_STEPS = 3;
+constexpr long GRAPH_MAX_NODES = 1L << 20;
+static bool graph_ok(const lbrb_t* h) {
+  return h->graph_mode != 0 && (h->graph_mode == 1 || (long)h->p.nx * h->p.ny <= GRAPH_MAX_NODES) &&
+         h->stream != nullptr && h->p.nudge == LBRB_NUDGE_NONE && !h->timing && !kParticleStream && !h->slab;
+}
+
 int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
@@ -632,9 +645,9 @@ int lbrb_step(lbrb_t* h, int n) {
     h->lb_shape_ms = ms;
   }
   bool pt_queued = false;
-  for (int s = 0; s < n; s++) {
+  // one step's launches; `last` writes the moments
+  auto one = [&](bool last) -> int {
     const int istep = h->istep + 1;
-    const bool last = (s == n - 1) && !h->slab_defer_moments;
     const bool rec = h->np > 0 && h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
     if (rec && (h->rec_head - h->rec_tail) >= h->p.record_slots)
       return fail(h, LBRB_ERR_OVERFLOW, "step: record ring full, drain records first");
@@ -725,6 +738,60 @@ int lbrb_step(lbrb_t* h, int n) {
       h->uvcur = uvn;
     }
     h->istep = istep;
+    return LBRB_OK;
+  };
+  // Small grids: a run of GRAPH_STEPS plain steps (no record, not the call's
+  // last step) replays a CUDA graph of exactly the launches `one` would
+  // issue.  Those launches depend only on the buffer phase (cur, uvcur,
+  // uvprev), so one graph per phase is captured on first use.
+  const bool graphs = graph_ok(h);
+  int s = 0;
+  while (s < n) {
+    if (graphs && n - 1 - s >= GRAPH_STEPS) {
+      bool plain = true;
+      if (h->np > 0 && h->p.noutconfig > 0)
+        for (int q = 1; q <= GRAPH_STEPS; q++) plain = plain && (h->istep + q) % h->p.noutconfig != 0;
+      if (plain) {
+        const int key = h->cur * 9 + h->uvcur * 3 + h->uvprev;
+        if (!h->graph_exec[key]) {
+          const int cur0 = h->cur, uvc0 = h->uvcur, uvp0 = h->uvprev, ist0 = h->istep;
+          cudaGraph_t g = nullptr;
+          CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+          int rc = LBRB_OK;
+          for (int q = 0; q < GRAPH_STEPS && rc == LBRB_OK; q++) rc = one(false);
+          const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+          h->cur = cur0, h->uvcur = uvc0, h->uvprev = uvp0, h->istep = ist0;  // captured, not run
+          if (rc != LBRB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+          }
+          if (ec != cudaSuccess) return fail(h, LBRB_ERR_CUDA, "step: graph capture", ec);
+          const cudaError_t ei = cudaGraphInstantiate(&h->graph_exec[key], g, 0);
+          cudaGraphDestroy(g);
+          if (ei != cudaSuccess) {
+            h->graph_exec[key] = nullptr;
+            return fail(h, LBRB_ERR_CUDA, "step: graph instantiate", ei);
+          }
+        }
+        CK(h, cudaGraphLaunch(h->graph_exec[key], h->stream));
+        // the state after the replayed steps, as `one` leaves it
+        for (int q = 0; q < GRAPH_STEPS; q++) {
+          h->cur ^= 1;
+          if (h->np > 0) {
+            const int uvn = 3 - h->uvcur - h->uvprev;
+            h->uvprev = h->uvcur;
+            h->uvcur = uvn;
+          }
+        }
+        h->prev_valid = true;
+        h->istep += GRAPH_STEPS;
+        s += GRAPH_STEPS;
+        continue;
+      }
+    }
+    const int rc = one(s == n - 1 && !h->slab_defer_moments);
+    if (rc) return rc;
+    s++;
   }
   // the caller's stream sees the particle kernels and record copies as part
   // of the steps
@@ -1144,6 +1211,12 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
       CK(h, cudaEventRecord(h->slab_ev_done, h->stream));
     }
   }
+  return LBRB_OK;
+}
+
+int lbrb_set_graph(lbrb_t* h, int mode) {
+  if (!h || mode < -1 || mode > 1) return fail(h, LBRB_ERR_ARG, "set_graph: mode must be -1, 0 or 1");
+  h->graph_mode = mode;
   return LBRB_OK;
 }
 

@@ -140,6 +140,10 @@ struct Handle {
   void* slab_down = nullptr;
   cudaEvent_t slab_ev_xfer = nullptr, slab_ev_done = nullptr;
   bool slab_defer_moments = false;  // inside lbrb_slab_step: moments on its last step only
+  // CUDA graphs of plain steps, one per buffer phase (cur * 9 + uvcur * 3 +
+  // uvprev); graph_mode -1: small grids only, 0: off, 1: on
+  cudaGraphExec_t graph_exec[18] = {};
+  int graph_mode = -1;
   size_t esize = 8;   // bytes per population value
   // populations: pops[buf] holds f (9 planes) then g (9 planes)
   void* pops[2] = {nullptr, nullptr};
