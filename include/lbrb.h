@@ -163,8 +163,8 @@ LBRB_API int lbrb_set_stream(lbrb_t *h, void *cuda_stream);
  * on first use), so small grids are not bound by the host's per-launch
  * enqueue.  Results are identical either way.  -1 (the default): grids of
  * at most 2^20 nodes; 0: off; 1: every grid.  Not used with nudging,
- * per-kernel timing, a y-slab or the legacy default stream.  No counterpart
- * in the reference. */
+ * per-kernel timing, a y-slab, the legacy default stream, or while the
+ * caller captures the handle's stream.  No counterpart in the reference. */
 LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
 /* Per-kernel device timing with CUDA events around each launch.  Classes:
  * 0 fused stream/collide, 1 particles, 2 nudging, 3 record copies.

@@ -744,7 +744,13 @@ int lbrb_step(lbrb_t* h, int n) {
   // last step) replays a CUDA graph of exactly the launches `one` would
   // issue.  Those launches depend only on the buffer phase (cur, uvcur,
   // uvprev), so one graph per phase is captured on first use.
-  const bool graphs = graph_ok(h);
+  bool graphs = graph_ok(h);
+  if (graphs) {
+    // a caller capturing this stream gets the launches themselves
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(h, cudaStreamIsCapturing(h->stream, &cs));
+    graphs = cs == cudaStreamCaptureStatusNone;
+  }
   int s = 0;
   while (s < n) {
     if (graphs && n - 1 - s >= GRAPH_STEPS) {

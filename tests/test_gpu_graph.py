@@ -63,3 +63,28 @@ def test_graph_mode_argument_checked():
     with lb.Run(**lb.closure(NX, NY, Ra=1e6, Pr=1.0, U=0.1), precision="fp32") as r:
         with pytest.raises(lb.LbrbError):
             r.set_graph(2)
+
+
+def test_steps_inside_a_callers_capture():
+    """a caller that captures lbrb_step into its own graph gets the launches
+    themselves (no nested capture): 6 steps without particles return the
+    buffer phase, so three replays equal 18 direct steps"""
+    import torch
+
+    with make("fp32", -1, 0) as a, make("fp32", -1, 0) as b:
+        s = torch.cuda.Stream()
+        a.set_stream(s.cuda_stream)
+        a.step(1)  # launch-shape tuning before the capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s, capture_error_mode="thread_local"):
+            a.step(6)
+        for _ in range(3):
+            g.replay()
+        torch.cuda.synchronize()
+        a.set_stream(None)
+        b.step(19)
+        fa, ga = a.get_populations()
+        fb, gb = b.get_populations()
+        np.testing.assert_array_equal(fa, fb)
+        np.testing.assert_array_equal(ga, gb)
