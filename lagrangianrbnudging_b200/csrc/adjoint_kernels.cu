@@ -14,9 +14,11 @@
 //   df'_k = (1-w) df_k + w w_k (dr + r P_k) + (1-w/2) w_k F (3 (cy_k - v) + 9 cu_k cy_k)
 //   dg'_k = (1-wg) dg_k + wg w_k (dT + t P_k)
 //   F' = g*beta r t
-// The adjoint kernel of step n, one thread per node x: re-pull the forward
-// state at x, apply the transposed local Jacobian to the adjoints of the
-// step's outputs at x (lambda df', dg', F', plus the observation term on T),
+// The adjoint kernel of step n, one thread per node x: read the moments the
+// forward step formed at x (stored beside the state after the step; they are
+// the step's linearisation point) and F^n, apply the transposed local
+// Jacobian to the adjoints of the step's outputs at x (lambda df', dg', F',
+// plus the observation term on T),
 // fold the anti-bounce-back transpose, and push the results to the nodes the
 // forward pulled from (the transpose of streaming: bounce-back sends the
 // adjoint to the opposite population of the same node; populations that
@@ -30,9 +32,9 @@ namespace lbrb {
 
 template <typename Real>
 struct AdjView {
-  const Real* __restrict__ fsrc;  // forward state before the step (18 planes)
-  const Real* __restrict__ gsrc;
-  const Real* __restrict__ Fin;   // F of the step
+  const Real* __restrict__ mom;   // the step's moments as the forward formed them: rho, u, v, T
+                                  // planes (the moment planes of the state after the step)
+  const Real* __restrict__ Fin;   // F of the step (the state before the step)
   const double* __restrict__ lf_out;  // lambda of the step's post-collision output
   const double* __restrict__ lg_out;
   double* __restrict__ lf_in;     // lambda of the step's input (pushed)
@@ -46,61 +48,6 @@ struct AdjView {
 };
 
 constexpr double ADJ_FIX = 1099511627776.0;  // 2^40
-
-// the stored values the forward step pulls into node (x, j): fv[k], gv[k]
-// (bounce-back at the walls: f from the node's opposite population, g left
-// zero for the anti-bounce-back below)
-// (Off: element offset type, uint32_t where the buffers allow it)
-template <typename Real, typename Off = size_t>
-__device__ __forceinline__ void adj_pull_raw(const Real* __restrict__ fsrc, const Real* __restrict__ gsrc,
-                                             int nx, int ny, int pitch, size_t plane, int j, int x,
-                                             Real* fv, Real* gv) {
-  const int xl = (x == 0) ? nx - 1 : x - 1;
-  const int xr = (x == nx - 1) ? 0 : x + 1;
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
-    const int js = j - icy(k);
-    if (js < 0 || js >= ny) {
-      fv[k] = fsrc[(Off)opp(k) * (Off)plane + (Off)j * (Off)pitch + (Off)x];
-      gv[k] = Real(0);
-    } else {
-      fv[k] = fsrc[(Off)k * (Off)plane + (Off)js * (Off)pitch + (Off)xs];
-      gv[k] = gsrc[(Off)k * (Off)plane + (Off)js * (Off)pitch + (Off)xs];
-    }
-  }
-}
-
-// pulled values in the shifted form, walls applied
-template <typename Real>
-__device__ __forceinline__ void adj_shift_pulled(const AdjView<Real>& V, int j, const Real* fv,
-                                                 const Real* gv, double* df, double* dg) {
-#pragma unroll
-  for (int k = 0; k < NPOP; k++) {
-    const int js = j - icy(k);
-    if constexpr (std::is_same<Real, double>::value) {
-      // reference-order storage holds f, g themselves: go to the shifted form
-      df[k] = fv[k] - w_of(k);
-      dg[k] = (js < 0 || js >= V.ny) ? 0.0 : gv[k] - w_of(k) * V.T0;
-    } else {
-      df[k] = (double)fv[k];
-      dg[k] = (double)gv[k];
-    }
-  }
-  // anti-bounce-back on the shifted form: dg_in = -dg_opp + 2 w (Twall - T0)
-  if (j == V.ny - 1) {
-    const double tw = V.Tup - V.T0;
-    dg[4] = -dg[2] + 2.0 * w_of(2) * tw;
-    dg[7] = -dg[5] + 2.0 * w_of(5) * tw;
-    dg[8] = -dg[6] + 2.0 * w_of(6) * tw;
-  }
-  if (j == 0) {
-    const double tw = V.Tdown - V.T0;
-    dg[2] = -dg[4] + 2.0 * w_of(4) * tw;
-    dg[5] = -dg[7] + 2.0 * w_of(7) * tw;
-    dg[6] = -dg[8] + 2.0 * w_of(8) * tw;
-  }
-}
 
 // compile-time loop over the directions
 template <int K, typename F>
@@ -116,34 +63,19 @@ struct AdjLoc {
   double r, t, u, v, F;
 };
 
-// from the raw pulled values fv, gv and the step's buoyancy F at the node
-template <typename Real>
-__device__ __forceinline__ AdjLoc adj_locals_raw(const AdjView<Real>& V, const Real* fv, const Real* gv,
-                                                 Real Fnode, int j) {
-  double df[NPOP], dg[NPOP];
-  adj_shift_pulled(V, j, fv, gv, df, dg);
-  // tree sums (short dependency chains)
-  const double dr = ((df[0] + df[1]) + (df[2] + df[3])) + ((df[4] + df[5]) + (df[6] + df[7])) + df[8];
-  const double dT = ((dg[0] + dg[1]) + (dg[2] + dg[3])) + ((dg[4] + dg[5]) + (dg[6] + dg[7])) + dg[8];
-  const double jx = (df[1] - df[3]) + (df[5] - df[6]) + (df[8] - df[7]);
-  const double jy = (df[2] - df[4]) + (df[5] - df[7]) + (df[6] - df[8]);
+// The step's linearisation point at node offset o: the moments the forward
+// step formed there (rho, u, v, T, stored beside the state after the step)
+// and the step's buoyancy F.  (Off: element offset type.)
+template <typename Real, typename Off = size_t>
+__device__ __forceinline__ AdjLoc adj_locals(const Real* __restrict__ mom, const Real* __restrict__ Fin,
+                                             size_t plane, Off o) {
   AdjLoc L;
-  L.r = 1.0 + dr;
-  L.t = V.T0 + dT;
-  L.F = (double)Fnode;
-  const double rinv = 1.0 / L.r;
-  L.u = jx * rinv;
-  L.v = fma(0.5, L.F, jy) * rinv;
+  L.r = (double)mom[o];
+  L.u = (double)mom[(Off)plane + o];
+  L.v = (double)mom[(Off)(2 * plane) + o];
+  L.t = (double)mom[(Off)(3 * plane) + o];
+  L.F = (double)Fin[o];
   return L;
-}
-
-template <typename Real>
-__device__ __forceinline__ AdjLoc adj_locals(const AdjView<Real>& V, const Real* __restrict__ fsrc,
-                                             const Real* __restrict__ gsrc, const Real* __restrict__ Fin,
-                                             int j, int x) {
-  Real fv[NPOP], gv[NPOP];
-  adj_pull_raw(fsrc, gsrc, V.nx, V.ny, V.pitch, V.plane, j, x, fv, gv);
-  return adj_locals_raw(V, fv, gv, Fin[(size_t)j * V.pitch + x], j);
 }
 
 // weighted moments of 9 adjoint values X_k: sum w_k X_k {1, cx, cy, cx^2,
@@ -257,6 +189,7 @@ __device__ __forceinline__ void adj_push_one(int k, bool is_g, double val, int n
 
 template <typename Real>
 __global__ void __launch_bounds__(128) adjoint_step_kernel(const AdjView<Real> V) {
+  pdl_wait();
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (x >= V.nx) return;
@@ -270,7 +203,7 @@ __global__ void __launch_bounds__(128) adjoint_step_kernel(const AdjView<Real> V
   }
   const double lFo = V.lF[o];
   const double lt = V.lT ? (double)V.lT[o] * (1.0 / ADJ_FIX) : 0.0;
-  const AdjLoc L = adj_locals(V, V.fsrc, V.gsrc, V.Fin, j, x);
+  const AdjLoc L = adj_locals(V.mom, V.Fin, V.plane, o);
   double lFin;
   adj_local(
       V, L, j, [&](int k) { return lf[k]; }, [&](int k) { return lg[k]; }, lFo, lt,
@@ -292,10 +225,9 @@ __global__ void __launch_bounds__(128) adjoint_step_kernel(const AdjView<Real> V
 // (cleared afterwards), since neighbouring blocks read the ring nodes too.
 template <typename Real>
 struct AdjPairView {
-  AdjView<Real> a;                      // step n: state before it, lambda^n, lambda F^{n+1}, lambda T^n
-  const Real* __restrict__ fsrc_b;      // state before step n-1
-  const Real* __restrict__ gsrc_b;
-  const Real* __restrict__ Fin_b;
+  AdjView<Real> a;                      // step n: its moments and F, lambda^n, lambda F^{n+1}, lambda T^n
+  const Real* __restrict__ mom_b;       // moments of step n-1
+  const Real* __restrict__ Fin_b;       // F of step n-1
   const long long* __restrict__ lT_b;   // lambda T^{n-1} or null
   double* __restrict__ lf_in;           // lambda^{n-2}
   double* __restrict__ lg_in;
@@ -308,6 +240,7 @@ struct AdjPairView {
 // on B200: unaligned rows and more blocks)
 template <typename Real, int TX, int TY, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) adjoint_pair_kernel(const AdjPairView<Real> P) {
+  pdl_wait();
   extern __shared__ double sm[];
   constexpr int HX = TX + 2, HY = TY + 2, NH = HX * HY;
   static_assert(NT >= TX * TY, "one thread per tile node");
@@ -322,7 +255,7 @@ __global__ void __launch_bounds__(NT, MINB) adjoint_pair_kernel(const AdjPairVie
   AdjLoc L2{};
   double lt2 = 0.0;
   if (mine) {
-    L2 = adj_locals(V, P.fsrc_b, P.gsrc_b, P.Fin_b, j, x);
+    L2 = adj_locals(P.mom_b, P.Fin_b, V.plane, (size_t)j * V.pitch + x);
     if (P.lT_b) lt2 = (double)P.lT_b[(size_t)j * V.pitch + x] * (1.0 / ADJ_FIX);
   }
   // phase 1: step n at the tile and its ring
@@ -342,7 +275,7 @@ __global__ void __launch_bounds__(NT, MINB) adjoint_pair_kernel(const AdjPairVie
     }
     const double lFo = V.lF[o];
     const double lt = V.lT ? (double)V.lT[o] * (1.0 / ADJ_FIX) : 0.0;
-    const AdjLoc L = adj_locals(V, V.fsrc, V.gsrc, V.Fin, jh, xh);
+    const AdjLoc L = adj_locals(V.mom, V.Fin, V.plane, o);
     double lFin;
     adj_local(
         V, L, jh, [&](int k) { return lf[k]; }, [&](int k) { return lg[k]; }, lFo, lt,
@@ -395,8 +328,8 @@ template <typename Real>
 struct MarchIn {
   double lf[NPOP], lg[NPOP], lFo;  // lambda^n and lambda F^{n+1} at the phase-1 node
   long long lt;                    // lambda T^n (fixed point)
-  Real fa[NPOP], ga[NPOP], Fa;     // state before step n, pulled into the phase-1 node
-  Real fb[NPOP], gb[NPOP], Fb;     // state before step n-1, pulled into the phase-2 node
+  Real ma[4], Fa;                  // moments (rho, u, v, T) and F of step n at the phase-1 node
+  Real mb[4], Fb;                  // moments and F of step n-1 at the phase-2 node
   long long ltb;                   // lambda T^{n-1}
 };
 
@@ -413,6 +346,7 @@ struct MarchStep {
 // each other's loads.
 template <typename Real, int RB, int MINB, int PRE, typename Off>
 __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjPairView<Real> P, int chunk) {
+  pdl_wait();
   extern __shared__ double sm[];
   constexpr int HX = 34, S = 2 * RB + 2;  // ring: S rows of HX columns, 2*NPOP+1 values
   const AdjView<Real>& V = P.a;
@@ -451,12 +385,14 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
     }
     in.lFo = V.lF[o];
     in.lt = V.lT ? V.lT[o] : 0ll;
-    adj_pull_raw<Real, Off>(V.fsrc, V.gsrc, nx, ny, pitch, plane, j1, xh, in.fa, in.ga);
+#pragma unroll
+    for (int q = 0; q < 4; q++) in.ma[q] = V.mom[(Off)q * (Off)plane + o];
     in.Fa = V.Fin[o];
   };
   auto load2 = [&](int x2, int j2, MarchIn<Real>& in) {
     const Off o = (Off)j2 * (Off)pitch + (Off)x2;
-    adj_pull_raw<Real, Off>(P.fsrc_b, P.gsrc_b, nx, ny, pitch, plane, j2, x2, in.fb, in.gb);
+#pragma unroll
+    for (int q = 0; q < 4; q++) in.mb[q] = P.mom_b[(Off)q * (Off)plane + o];
     in.Fb = P.Fin_b[o];
     in.ltb = P.lT_b ? P.lT_b[o] : 0ll;
   };
@@ -472,7 +408,7 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
     return MarchStep<RB>{st.u + 1, (st.u + 1) % ngroups == 0};  // a new strip starts with a prologue
   };
   auto phase1 = [&](int j1, const MarchIn<Real>& cur) {
-    const AdjLoc L = adj_locals_raw(V, cur.fa, cur.ga, cur.Fa, j1);
+    const AdjLoc L{(double)cur.ma[0], (double)cur.ma[3], (double)cur.ma[1], (double)cur.ma[2], (double)cur.Fa};
     double lFin;
     adj_local(
         V, L, j1, [&](int k) { return cur.lf[k]; }, [&](int k) { return cur.lg[k]; }, cur.lFo,
@@ -492,7 +428,7 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
       const int sj = j2 + icy(m);
       return (sj < 0 || sj >= ny) ? 0.0 : ring(NPOP + m, sj, c + icx(m));
     };
-    const AdjLoc L = adj_locals_raw(V, cur.fb, cur.gb, cur.Fb, j2);
+    const AdjLoc L{(double)cur.mb[0], (double)cur.mb[3], (double)cur.mb[1], (double)cur.mb[2], (double)cur.Fb};
     double lFin;
     adj_local(
         V, L, j2, lfo, lgo, ring(2 * NPOP, j2, c), (double)cur.ltb * (1.0 / ADJ_FIX),
@@ -586,6 +522,7 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
 __global__ void adj_obs_scatter_kernel(const double* __restrict__ ox, const double* __restrict__ oy,
                                        const double* __restrict__ res, int nobs, int nx, int ny,
                                        int pitch, unsigned long long* __restrict__ acc) {
+  pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nobs) return;
   const double xx = ox[p], yy = oy[p];
@@ -609,6 +546,7 @@ template <typename Real>
 __global__ void obs_residual_kernel(const Real* __restrict__ T, int nx, int ny, int pitch,
                                     const double* __restrict__ ox, const double* __restrict__ oy,
                                     const double* __restrict__ oT, int nobs, double* __restrict__ res) {
+  pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nobs) return;
   const double xx = ox[p], yy = oy[p];
@@ -691,6 +629,7 @@ __global__ void adj_initial_kernel(const double* __restrict__ lg, const double* 
 // (the corners the scatter touched)
 __global__ void adj_obs_clear_kernel(const double* __restrict__ ox, const double* __restrict__ oy,
                                      int nobs, int nx, int ny, int pitch, long long* __restrict__ acc) {
+  pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nobs) return;
   const double xx = ox[p], yy = oy[p];
@@ -716,6 +655,7 @@ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e
 
 __global__ void __launch_bounds__(1024) misfit_kernel(const double* __restrict__ res, long n,
                                                       double* __restrict__ out) {
+  pdl_wait();
   __shared__ double ss[1024], sc[1024];
   double sum = 0.0, comp = 0.0;
   for (long i = threadIdx.x; i < n; i += blockDim.x) {
@@ -749,8 +689,7 @@ static cudaError_t launch_pair_t(const AdjPairView<Real>& P, cudaStream_t s) {
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (attr != cudaSuccess) return attr;
   dim3 grid((P.a.nx + TX - 1) / TX, (P.a.ny + TY - 1) / TY);
-  adjoint_pair_kernel<Real, TX, TY, NT, MINB><<<grid, NT, smem, s>>>(P);
-  return cudaGetLastError();
+  return launch_k(adjoint_pair_kernel<Real, TX, TY, NT, MINB>, grid, NT, smem, s, true, P);
 }
 
 // marching kernel: strips x chunks blocks, the chunk length chosen so that
@@ -776,8 +715,7 @@ static cudaError_t launch_march_o(const AdjPairView<Real>& P, int waves, cudaStr
   const int target = std::max(1, nsm * occ * waves / nstrips);  // chunks per strip
   const int chunk = (ngroups + target - 1) / target;
   const int nchunks = (ngroups + chunk - 1) / chunk;
-  kern<<<nstrips * nchunks, NT, smem, s>>>(P, chunk);
-  return cudaGetLastError();
+  return launch_k(kern, nstrips * nchunks, NT, smem, s, true, P, chunk);
 }
 
 // 32-bit element offsets where 36 planes of the grid fit below 2^32
@@ -793,26 +731,28 @@ static cudaError_t launch_march_t(const AdjPairView<Real>& P, int waves, cudaStr
 constexpr int ADJ_NPAIR_VARIANTS = 10;
 int adjoint_pair_variants() { return ADJ_NPAIR_VARIANTS; }
 
-// steps n and n-1: state_a before step n, state_b before step n-1 (18 pop
-// planes then F), lambda^n in (lf_out, lg_out), lambda^{n-2} out (lf_in,
-// lg_in), lambda F^{n+1} in (lF_in), lambda F^{n-1} out (lF_out)
-cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, const void* state_b,
-                                const double* lf_out, const double* lg_out, double* lf_in,
-                                double* lg_in, double* lF_in, double* lF_out, const long long* lT_a,
-                                const long long* lT_b, int nx, int ny, int pitch, size_t plane,
-                                double omega, double omegag, double gbeta, double T0, double Tup,
-                                double Tdown, cudaStream_t s) {
+// steps n and n-1 from three state slots: after_a (the state after step n:
+// its moment planes are step n's linearisation point), state_a (before step
+// n: F^n, and in its moment planes step n-1's), state_b (before step n-1:
+// F^{n-1}); lambda^n in (lf_out, lg_out), lambda^{n-2} out (lf_in, lg_in),
+// lambda F^{n+1} in (lF_in), lambda F^{n-1} out (lF_out)
+cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* after_a, const void* state_a,
+                                const void* state_b, const double* lf_out, const double* lg_out,
+                                double* lf_in, double* lg_in, double* lF_in, double* lF_out,
+                                const long long* lT_a, const long long* lT_b, int nx, int ny, int pitch,
+                                size_t plane, double omega, double omegag, double gbeta, double T0,
+                                double Tup, double Tdown, cudaStream_t s) {
   auto go = [&](auto zero) -> cudaError_t {
     using Real = decltype(zero);
+    const Real* n1 = (const Real*)after_a;
     const Real* a = (const Real*)state_a;
     const Real* b = (const Real*)state_b;
     AdjPairView<Real> P{};
-    P.a = AdjView<Real>{a, a + NPOP * plane, a + 2 * NPOP * plane, lf_out, lg_out, nullptr, nullptr,
+    P.a = AdjView<Real>{n1 + SLOT_MOM * plane, a + SLOT_F * plane, lf_out, lg_out, nullptr, nullptr,
                         lF_in, const_cast<long long*>(lT_a), nx, ny, pitch, plane, omega, omegag,
                         gbeta, T0, Tup, Tdown};
-    P.fsrc_b = b;
-    P.gsrc_b = b + NPOP * plane;
-    P.Fin_b = b + 2 * NPOP * plane;
+    P.mom_b = a + SLOT_MOM * plane;
+    P.Fin_b = b + SLOT_F * plane;
     P.lT_b = lT_b;
     P.lf_in = lf_in;
     P.lg_in = lg_in;
@@ -836,43 +776,43 @@ cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, con
 template <typename Real>
 static cudaError_t launch_adj_t(const AdjView<Real>& V, cudaStream_t s) {
   dim3 grid((V.nx + 127) / 128, V.ny);
-  adjoint_step_kernel<Real><<<grid, 128, 0, s>>>(V);
-  return cudaGetLastError();
+  return launch_k(adjoint_step_kernel<Real>, grid, 128, 0, s, true, V);
 }
 
-cudaError_t launch_adjoint_step(bool fp32, const void* fsrc, const void* gsrc, const void* Fin,
-                                const double* lf_out, const double* lg_out, double* lf_in,
-                                double* lg_in, double* lF, long long* lT, int nx, int ny, int pitch,
-                                size_t plane, double omega, double omegag, double gbeta, double T0,
-                                double Tup, double Tdown, cudaStream_t s) {
+// one step from two state slots: `after` (its moments: the step's
+// linearisation point) and `state` (before the step: F)
+cudaError_t launch_adjoint_step(bool fp32, const void* after, const void* state, const double* lf_out,
+                                const double* lg_out, double* lf_in, double* lg_in, double* lF,
+                                long long* lT, int nx, int ny, int pitch, size_t plane, double omega,
+                                double omegag, double gbeta, double T0, double Tup, double Tdown,
+                                cudaStream_t s) {
   if (fp32) {
-    AdjView<float> V{(const float*)fsrc, (const float*)gsrc, (const float*)Fin, lf_out, lg_out, lf_in,
-                     lg_in, lF, lT, nx, ny, pitch, plane, omega, omegag, gbeta, T0, Tup, Tdown};
+    AdjView<float> V{(const float*)after + SLOT_MOM * plane, (const float*)state + SLOT_F * plane, lf_out,
+                     lg_out, lf_in, lg_in, lF, lT, nx, ny, pitch, plane, omega, omegag, gbeta, T0, Tup,
+                     Tdown};
     return launch_adj_t(V, s);
   }
-  AdjView<double> V{(const double*)fsrc, (const double*)gsrc, (const double*)Fin, lf_out, lg_out, lf_in,
-                    lg_in, lF, lT, nx, ny, pitch, plane, omega, omegag, gbeta, T0, Tup, Tdown};
+  AdjView<double> V{(const double*)after + SLOT_MOM * plane, (const double*)state + SLOT_F * plane, lf_out,
+                    lg_out, lf_in, lg_in, lF, lT, nx, ny, pitch, plane, omega, omegag, gbeta, T0, Tup,
+                    Tdown};
   return launch_adj_t(V, s);
 }
 
 cudaError_t launch_misfit(const double* res, long n, double* out, cudaStream_t s) {
-  misfit_kernel<<<1, 1024, 0, s>>>(res, n, out);
-  return cudaGetLastError();
+  return launch_k(misfit_kernel, 1, 1024, 0, s, true, res, n, out);
 }
 
 cudaError_t launch_adj_obs_clear(const double* ox, const double* oy, int nobs, int nx, int ny, int pitch,
                                  long long* acc, cudaStream_t s) {
   if (nobs <= 0) return cudaSuccess;
-  adj_obs_clear_kernel<<<(nobs + 127) / 128, 128, 0, s>>>(ox, oy, nobs, nx, ny, pitch, acc);
-  return cudaGetLastError();
+  return launch_k(adj_obs_clear_kernel, (nobs + 127) / 128, 128, 0, s, true, ox, oy, nobs, nx, ny, pitch, acc);
 }
 
 cudaError_t launch_adj_obs_scatter(const double* ox, const double* oy, const double* res, int nobs,
                                    int nx, int ny, int pitch, long long* acc, cudaStream_t s) {
   if (nobs <= 0) return cudaSuccess;
-  adj_obs_scatter_kernel<<<(nobs + 127) / 128, 128, 0, s>>>(ox, oy, res, nobs, nx, ny, pitch,
-                                                            reinterpret_cast<unsigned long long*>(acc));
-  return cudaGetLastError();
+  return launch_k(adj_obs_scatter_kernel, (nobs + 127) / 128, 128, 0, s, true, ox, oy, res, nobs, nx, ny, pitch,
+                  reinterpret_cast<unsigned long long*>(acc));
 }
 
 cudaError_t launch_obs_residual(const void* T, bool fp32, int nx, int ny, int pitch, const double* ox,
@@ -880,10 +820,10 @@ cudaError_t launch_obs_residual(const void* T, bool fp32, int nx, int ny, int pi
                                 cudaStream_t s) {
   if (nobs <= 0) return cudaSuccess;
   if (fp32)
-    obs_residual_kernel<float><<<(nobs + 127) / 128, 128, 0, s>>>((const float*)T, nx, ny, pitch, ox, oy, oT, nobs, res);
-  else
-    obs_residual_kernel<double><<<(nobs + 127) / 128, 128, 0, s>>>((const double*)T, nx, ny, pitch, ox, oy, oT, nobs, res);
-  return cudaGetLastError();
+    return launch_k(obs_residual_kernel<float>, (nobs + 127) / 128, 128, 0, s, true, (const float*)T, nx, ny,
+                    pitch, ox, oy, oT, nobs, res);
+  return launch_k(obs_residual_kernel<double>, (nobs + 127) / 128, 128, 0, s, true, (const double*)T, nx, ny,
+                  pitch, ox, oy, oT, nobs, res);
 }
 
 cudaError_t launch_init_from_T0(const double* T0f, void* pops, void* rho, void* u, void* v, void* T,

@@ -542,20 +542,25 @@ int lbrb_nudge_obs(lbrb_t* h, int first_step, int nsteps, const double* x, const
 // particle kernels on a second stream, overlapping the next fused kernel
 static constexpr bool kParticleStream = false;
 
-// view of one step from state buffers (pops: 18 planes, then F) to others;
-// moments written into the handle's rho/T/u/v of buffer 0 when asked
+// view of one step from one state slot (SLOT_PLANES planes: pops, F,
+// moments) to another; with `mom` the step's moments go to the destination
+// slot's moment planes
 template <typename Real>
-static LBView<Real> seg_view(lbrb_t* h, const char* src, char* dst, int write_rt) {
-  LBView<Real> V = make_view<Real>(h, 0, 1, h->uvcur, 0, write_rt);
-  const size_t pb = NPOP * h->plane * sizeof(Real);
-  V.fsrc = (const Real*)src;
-  V.gsrc = (const Real*)(src + pb);
-  V.Fin = (const Real*)(src + 2 * pb);
-  V.fdst = (Real*)dst;
-  V.gdst = (Real*)(dst + pb);
-  V.Fout = (Real*)(dst + 2 * pb);
-  V.rho = (Real*)h->rho[0];
-  V.T = (Real*)h->T[0];
+static LBView<Real> seg_view(lbrb_t* h, const char* src, char* dst, int mom) {
+  LBView<Real> V = make_view<Real>(h, 0, 1, h->uvcur, mom, mom);
+  const size_t pl = h->plane;
+  const Real* a = (const Real*)src;
+  Real* b = (Real*)dst;
+  V.fsrc = a;
+  V.gsrc = a + NPOP * pl;
+  V.Fin = a + SLOT_F * pl;
+  V.fdst = b;
+  V.gdst = b + NPOP * pl;
+  V.Fout = b + SLOT_F * pl;
+  V.rho = b + SLOT_MOM * pl;
+  V.u = b + (SLOT_MOM + 1) * pl;
+  V.v = b + (SLOT_MOM + 2) * pl;
+  V.T = b + (SLOT_MOM + 3) * pl;
   return V;
 }
 
@@ -877,7 +882,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   const bool f32 = fp32(h);
   const int nx = h->p.nx, ny = h->p.ny, pitch = h->pitch;
   const size_t plane = h->plane, es = h->esize;
-  const size_t sb = (2 * NPOP + 1) * plane * es;  // one state: pops + F
+  const size_t sb = SLOT_PLANES * plane * es;  // one state slot: pops, F, moments
   const size_t nn = (size_t)nx * ny;
   if (K > nsteps) K = nsteps;
   const int nchk = (nsteps + K - 1) / K;
@@ -902,6 +907,12 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   // the forward pass leaves in place, in buffer 0
   auto segbuf = [&](int c) -> char* { return seg + (size_t)((nchk - 1 - c) & 1) * (K + 1) * sb; };
   auto state_in = [&](int c, int i) -> char* { return i == 0 ? chk + (size_t)c * sb : segbuf(c) + (size_t)i * sb; };
+  // the state after i steps of segment c (its last step writes the next
+  // checkpoint; the last segment's, slot K)
+  auto after = [&](int c, int i) -> char* {
+    if (i < std::min(K, nsteps - c * K)) return state_in(c, i);
+    return c + 1 < nchk ? chk + (size_t)(c + 1) * sb : segbuf(c) + (size_t)K * sb;
+  };
   // the window's initial state in checkpoint 0 (pops + F), moments in buffer 0
   CK(h, launch_init_from_T0(h->adj_T0, chk, h->rho[0], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
                             h->T[0], chk + 2 * NPOP * plane * es, f32, nx, ny, pitch, plane, T0ref,
@@ -919,11 +930,13 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     h->lb_shape_ms = ms;
   }
   const int shape = h->lb_shape;
-  auto launch_fwd_on = [&](const char* src, char* dst, int write_rt, cudaStream_t st) -> cudaError_t {
-    if (f32) return launch_lb_fp32(seg_view<float>(h, src, dst, write_rt), h->p.twall, shape, st);
-    return launch_lb_fp64(seg_view<double>(h, src, dst, write_rt), h->p.twall, false, shape, st);
+  auto launch_fwd_on = [&](const char* src, char* dst, int mom, cudaStream_t st) -> cudaError_t {
+    // programmatic dependent launch: each step may start while the one
+    // before it in the stream finishes (the kernel waits for it first)
+    if (f32) return launch_lb_fp32(seg_view<float>(h, src, dst, mom), h->p.twall, shape, st, true);
+    return launch_lb_fp64(seg_view<double>(h, src, dst, mom), h->p.twall, false, shape, st, true);
   };
-  auto launch_fwd = [&](const char* src, char* dst, int write_rt) { return launch_fwd_on(src, dst, write_rt, h->stream); };
+  auto launch_fwd = [&](const char* src, char* dst, int mom) { return launch_fwd_on(src, dst, mom, h->stream); };
   // ---- forward pass: checkpoints, residuals
   char* end_state = nullptr;
   for (int c = 0; c < nchk; c++) {
@@ -942,11 +955,13 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
       const int s = s0 + i + 1;
       char* dst = (i + 1 < len) ? fslot(i + 1) : (last ? segbuf(c) + (size_t)K * sb : chk + (size_t)(c + 1) * sb);
       const int oi = obs_at[s];
-      CK(h, launch_fwd(fslot(i), dst, oi >= 0));
+      // moments into every state the backward pass reads (and at observation
+      // steps, for the residual's T)
+      CK(h, launch_fwd(fslot(i), dst, (dJdT0 && (keep || i + 1 == len)) || oi >= 0));
       if (oi >= 0) {
         const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
-        CK(h, launch_obs_residual(h->T[0], f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob, nob,
-                                  h->adj_res + (size_t)oi * nob, h->stream));
+        CK(h, launch_obs_residual(dst + (SLOT_MOM + 3) * plane * es, f32, nx, ny, pitch, ob, ob + nob,
+                                  ob + 2 * nob, nob, h->adj_res + (size_t)oi * nob, h->stream));
       }
       end_state = dst;
     }
@@ -1006,7 +1021,8 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
       float best = 1e30f;
       for (int v = 0; v < adjoint_pair_variants(); v++) {
         auto trial = [&]() {
-          return launch_adjoint_pair(f32, v, state_in(nchk - 1, il), state_in(nchk - 1, il - 1),
+          return launch_adjoint_pair(f32, v, after(nchk - 1, il + 1), state_in(nchk - 1, il),
+                                     state_in(nchk - 1, il - 1),
                                      lam[lc][0], lam[lc][1], lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc],
                                      lF[fc ^ 1], nullptr, nullptr, nx, ny, pitch, plane, om, omg, ng, T0ref,
                                      h->p.Tup, h->p.Tdown, h->stream);
@@ -1052,7 +1068,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
       const int cp = c - 1, lenp = std::min(K, nsteps - cp * K);
       CK(h, cudaStreamWaitEvent(rs, ev_bwd[b ^ 1], 0));
       for (int i = 0; i + 1 < lenp; i++)
-        CK(h, launch_fwd_on(state_in(cp, i), segbuf(cp) + (size_t)(i + 1) * sb, 0, rs));
+        CK(h, launch_fwd_on(state_in(cp, i), segbuf(cp) + (size_t)(i + 1) * sb, 1, rs));
       CK(h, cudaEventRecord(ev_rec[b ^ 1], rs));
     }
     if (c + 2 < nchk) CK(h, cudaStreamWaitEvent(h->stream, ev_rec[b], 0));
@@ -1064,7 +1080,8 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
         CK(h, scatter(s, lT[0]));
         CK(h, scatter(s - 1, lT[1]));
         auto pair = [&](int variant) {
-          return launch_adjoint_pair(f32, variant, state_in(c, i), state_in(c, i - 1), lam[lc][0], lam[lc][1],
+          return launch_adjoint_pair(f32, variant, after(c, i + 1), state_in(c, i), state_in(c, i - 1),
+                                     lam[lc][0], lam[lc][1],
                                      lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc], lF[fc ^ 1],
                                      obs_at[s] >= 0 ? lT[0] : nullptr, obs_at[s - 1] >= 0 ? lT[1] : nullptr,
                                      nx, ny, pitch, plane, om, omg, ng, T0ref, h->p.Tup, h->p.Tdown,
@@ -1077,9 +1094,8 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
         fc ^= 1;
         s -= 2;
       } else {
-        const char* st = state_in(c, i);
         CK(h, scatter(s, lT[0]));
-        CK(h, launch_adjoint_step(f32, st, st + NPOP * plane * es, st + 2 * NPOP * plane * es,
+        CK(h, launch_adjoint_step(f32, after(c, i + 1), state_in(c, i),
                                   lam[lc][0], lam[lc][1], lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc],
                                   obs_at[s] >= 0 ? lT[0] : nullptr, nx, ny, pitch, plane, om, omg, ng,
                                   T0ref, h->p.Tup, h->p.Tdown, h->stream));

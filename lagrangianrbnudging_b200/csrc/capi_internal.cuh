@@ -20,8 +20,8 @@ struct NvtxRange {
 
 namespace lbrb {
 cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, int shape,
-                           cudaStream_t s);
-cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStream_t s);
+                           cudaStream_t s, bool pdl = false);
+cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStream_t s, bool pdl = false);
 int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best_ms);
 cudaError_t launch_pull_fp64(const LBView<double>& V, int twall, void* outf, void* outg, cudaStream_t s);
 cudaError_t launch_pull_fp32(const LBView<float>& V, int twall, void* outf, void* outg, cudaStream_t s);
@@ -63,19 +63,19 @@ cudaError_t launch_profile(const void* rho, const void* u, const void* v, const 
                            int nx, int ny, int pitch, double* out, cudaStream_t s);
 cudaError_t launch_finite(const void* a, size_t n, bool fp32, unsigned* flags, cudaStream_t s);
 int red_blocks();
-cudaError_t launch_adjoint_step(bool fp32, const void* fsrc, const void* gsrc, const void* Fin,
-                                const double* lf_out, const double* lg_out, double* lf_in,
-                                double* lg_in, double* lF, long long* lT, int nx, int ny, int pitch,
-                                size_t plane, double omega, double omegag, double gbeta, double T0,
-                                double Tup, double Tdown, cudaStream_t s);
+cudaError_t launch_adjoint_step(bool fp32, const void* after, const void* state, const double* lf_out,
+                                const double* lg_out, double* lf_in, double* lg_in, double* lF,
+                                long long* lT, int nx, int ny, int pitch, size_t plane, double omega,
+                                double omegag, double gbeta, double T0, double Tup, double Tdown,
+                                cudaStream_t s);
 int adjoint_pair_variants();
 cudaError_t launch_misfit(const double* res, long n, double* out, cudaStream_t s);
-cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* state_a, const void* state_b,
-                                const double* lf_out, const double* lg_out, double* lf_in,
-                                double* lg_in, double* lF_in, double* lF_out, const long long* lT_a,
-                                const long long* lT_b, int nx, int ny, int pitch, size_t plane,
-                                double omega, double omegag, double gbeta, double T0, double Tup,
-                                double Tdown, cudaStream_t s);
+cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* after_a, const void* state_a,
+                                const void* state_b, const double* lf_out, const double* lg_out,
+                                double* lf_in, double* lg_in, double* lF_in, double* lF_out,
+                                const long long* lT_a, const long long* lT_b, int nx, int ny, int pitch,
+                                size_t plane, double omega, double omegag, double gbeta, double T0,
+                                double Tup, double Tdown, cudaStream_t s);
 cudaError_t launch_adj_obs_clear(const double* ox, const double* oy, int nobs, int nx, int ny, int pitch,
                                  long long* acc, cudaStream_t s);
 cudaError_t launch_adj_obs_scatter(const double* ox, const double* oy, const double* res, int nobs,

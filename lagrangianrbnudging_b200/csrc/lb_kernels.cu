@@ -57,6 +57,7 @@ __global__ void __launch_bounds__(128) lb_pull_kernel(const LBView<Real> V, Real
 
 template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB, typename Off, bool FAST>
 __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V) {
+  pdl_wait();
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (x >= V.nx) return;
@@ -73,43 +74,41 @@ constexpr Shape SHAPES[] = {{256, 1, 1}, {256, 2, 1}, {256, 3, 1}, {128, 4, 1}, 
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 
 template <typename Real, int TWALL, bool REFNUDGE, int BS, int MINB, bool FAST>
-static cudaError_t launch_shape(const LBView<Real>& V, cudaStream_t s) {
+static cudaError_t launch_shape(const LBView<Real>& V, cudaStream_t s, bool pdl) {
   dim3 grid((V.nx + BS - 1) / BS, V.ny);
   if (FAST && off32_ok(V.plane))
-    lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB, uint32_t, true><<<grid, BS, 0, s>>>(V);
-  else
-    lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB, size_t, FAST><<<grid, BS, 0, s>>>(V);
-  return cudaGetLastError();
+    return launch_k(lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB, uint32_t, true>, grid, BS, 0, s, pdl, V);
+  return launch_k(lb_node_kernel<Real, TWALL, REFNUDGE, BS, MINB, size_t, FAST>, grid, BS, 0, s, pdl, V);
 }
 
 template <typename Real, int TWALL, bool REFNUDGE>
-static cudaError_t launch_lb(const LBView<Real>& V, int shape, cudaStream_t s) {
+static cudaError_t launch_lb(const LBView<Real>& V, int shape, cudaStream_t s, bool pdl) {
   switch (shape) {
-    case 1: return launch_shape<Real, TWALL, REFNUDGE, 256, 2, true>(V, s);
-    case 2: return launch_shape<Real, TWALL, REFNUDGE, 256, 3, true>(V, s);
-    case 3: return launch_shape<Real, TWALL, REFNUDGE, 128, 4, true>(V, s);
-    case 4: return launch_shape<Real, TWALL, REFNUDGE, 128, 6, true>(V, s);
-    case 5: return launch_shape<Real, TWALL, REFNUDGE, 512, 1, true>(V, s);
-    case 6: return launch_shape<Real, TWALL, REFNUDGE, 512, 2, true>(V, s);
-    case 7: return launch_shape<Real, TWALL, REFNUDGE, 256, 3, false>(V, s);
-    case 8: return launch_shape<Real, TWALL, REFNUDGE, 128, 4, false>(V, s);
-    case 9: return launch_shape<Real, TWALL, REFNUDGE, 128, 6, false>(V, s);
-    default: return launch_shape<Real, TWALL, REFNUDGE, 256, 1, true>(V, s);
+    case 1: return launch_shape<Real, TWALL, REFNUDGE, 256, 2, true>(V, s, pdl);
+    case 2: return launch_shape<Real, TWALL, REFNUDGE, 256, 3, true>(V, s, pdl);
+    case 3: return launch_shape<Real, TWALL, REFNUDGE, 128, 4, true>(V, s, pdl);
+    case 4: return launch_shape<Real, TWALL, REFNUDGE, 128, 6, true>(V, s, pdl);
+    case 5: return launch_shape<Real, TWALL, REFNUDGE, 512, 1, true>(V, s, pdl);
+    case 6: return launch_shape<Real, TWALL, REFNUDGE, 512, 2, true>(V, s, pdl);
+    case 7: return launch_shape<Real, TWALL, REFNUDGE, 256, 3, false>(V, s, pdl);
+    case 8: return launch_shape<Real, TWALL, REFNUDGE, 128, 4, false>(V, s, pdl);
+    case 9: return launch_shape<Real, TWALL, REFNUDGE, 128, 6, false>(V, s, pdl);
+    default: return launch_shape<Real, TWALL, REFNUDGE, 256, 1, true>(V, s, pdl);
   }
 }
 
 cudaError_t launch_lb_fp64(const LBView<double>& V, int twall, bool refnudge, int shape,
-                           cudaStream_t s) {
+                           cudaStream_t s, bool pdl) {
   if (twall == LBRB_TWALL_DIRICHLET)
-    return refnudge ? launch_lb<double, LBRB_TWALL_DIRICHLET, true>(V, shape, s)
-                    : launch_lb<double, LBRB_TWALL_DIRICHLET, false>(V, shape, s);
-  return refnudge ? launch_lb<double, LBRB_TWALL_ADIABATIC, true>(V, shape, s)
-                  : launch_lb<double, LBRB_TWALL_ADIABATIC, false>(V, shape, s);
+    return refnudge ? launch_lb<double, LBRB_TWALL_DIRICHLET, true>(V, shape, s, pdl)
+                    : launch_lb<double, LBRB_TWALL_DIRICHLET, false>(V, shape, s, pdl);
+  return refnudge ? launch_lb<double, LBRB_TWALL_ADIABATIC, true>(V, shape, s, pdl)
+                  : launch_lb<double, LBRB_TWALL_ADIABATIC, false>(V, shape, s, pdl);
 }
 
-cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStream_t s) {
-  if (twall == LBRB_TWALL_DIRICHLET) return launch_lb<float, LBRB_TWALL_DIRICHLET, false>(V, shape, s);
-  return launch_lb<float, LBRB_TWALL_ADIABATIC, false>(V, shape, s);
+cudaError_t launch_lb_fp32(const LBView<float>& V, int twall, int shape, cudaStream_t s, bool pdl) {
+  if (twall == LBRB_TWALL_DIRICHLET) return launch_lb<float, LBRB_TWALL_DIRICHLET, false>(V, shape, s, pdl);
+  return launch_lb<float, LBRB_TWALL_ADIABATIC, false>(V, shape, s, pdl);
 }
 
 // Autotuner: time every launch shape on this run's grid (CUDA events, `reps`
@@ -132,8 +131,8 @@ static int tune(const LBView<Real>& Vin, int twall, bool refnudge, cudaStream_t 
   for (int sh = 0; sh < NSHAPES; sh++) {
     cudaError_t e;
     auto go = [&]() {
-      if constexpr (std::is_same<Real, double>::value) return launch_lb_fp64(V, twall, refnudge, sh, s);
-      else return launch_lb_fp32(V, twall, sh, s);
+      if constexpr (std::is_same<Real, double>::value) return launch_lb_fp64(V, twall, refnudge, sh, s, false);
+      else return launch_lb_fp32(V, twall, sh, s, false);
     };
     e = go();
     if (e != cudaSuccess) { cudaGetLastError(); continue; }

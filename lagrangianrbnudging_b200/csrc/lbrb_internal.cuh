@@ -9,6 +9,7 @@
 // device node (x = i-1, y = j-1).  The reference's periodic halos (pbc,
 // communication) become index wrap.
 #pragma once
+#include <utility>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -50,6 +51,35 @@ constexpr double CS2 = 1.0 / 3.0;
 
 // element offsets of a population buffer (18 planes) fit in 32 bits
 inline bool off32_ok(size_t plane) { return plane * 2 * NPOP < (size_t(1) << 32); }
+
+// Programmatic dependent launch: a kernel launched with the attribute may
+// start while the kernel before it in the stream finishes; it waits here,
+// before touching memory, until that kernel has completed and its writes are
+// visible.  For a kernel launched without the attribute this returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// launch k<<<grid, block, smem, s>>>(args...), with programmatic dependent
+// launch when `pdl` (the kernel must call pdl_wait() first)
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl,
+                            Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
+// a state slot of the adjoint window (planes of `plane` elements): the 18
+// populations, F, then the moments the step that produced the state formed
+// (rho, u, v, T; the next step's adjoint linearises around them)
+constexpr int SLOT_F = 2 * NPOP, SLOT_MOM = 2 * NPOP + 1, SLOT_PLANES = 2 * NPOP + 5;
 
 // equilif / equilig in the reference's operation order
 // (temppart_dump.c:1097-1180): r1 is rho for f and T for g.
