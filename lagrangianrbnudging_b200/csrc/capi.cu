@@ -651,6 +651,7 @@ int lbrb_step(lbrb_t* h, int n) {
   }
   bool pt_queued = false;
   // one step's launches; `last` writes the moments
+  const bool pdl_ok = !h->timing;  // (per-kernel timing keeps plain launches)
   auto one = [&](bool last) -> int {
     const int istep = h->istep + 1;
     const bool rec = h->np > 0 && h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
@@ -688,8 +689,10 @@ int lbrb_step(lbrb_t* h, int n) {
     }
     {
       const int tm = tmark_begin(h, 0, h->stream);
-      if (f32) CK(h, launch_lb_fp32(make_view<float>(h, src, dst, uvn, write_uv, write_rt), h->p.twall, h->lb_shape, h->stream));
-      else CK(h, launch_lb_fp64(make_view<double>(h, src, dst, uvn, write_uv, write_rt), h->p.twall, refbox, h->lb_shape, h->stream));
+      // programmatic dependent launch when the kernel before it is this
+      // loop's own (the fused kernel waits for it before touching memory)
+      if (f32) CK(h, launch_lb_fp32(make_view<float>(h, src, dst, uvn, write_uv, write_rt), h->p.twall, h->lb_shape, h->stream, pdl_ok));
+      else CK(h, launch_lb_fp64(make_view<double>(h, src, dst, uvn, write_uv, write_rt), h->p.twall, refbox, h->lb_shape, h->stream, pdl_ok));
       tmark_end(h, tm, h->stream);
     }
     if (h->np > 0 && kParticleStream) CK(h, cudaEventRecord(h->ev_lb, h->stream));
@@ -714,7 +717,7 @@ int lbrb_step(lbrb_t* h, int n) {
       const int tm = tmark_begin(h, 1, ps);
       CK(h, launch_particles(h->uv[uvn][0], h->uv[uvn][1], h->uv[ub][0], h->uv[ub][1],
                              h->T[dst], f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta,
-                             rec ? 1 : 0, h->p.record_full, rslot, h->dflags, ps));
+                             rec ? 1 : 0, h->p.record_full, rslot, h->dflags, ps, pdl_ok && !kParticleStream));
       tmark_end(h, tm, ps);
       if (kParticleStream) {
         CK(h, cudaEventRecord(h->ev_uv[uvn], ps));

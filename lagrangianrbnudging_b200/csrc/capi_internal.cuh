@@ -29,7 +29,7 @@ int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_
 cudaError_t launch_particles(const void* u, const void* v, const void* ub, const void* vb,
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,
                              const int* ptype, int np, double beta, int record, int full,
-                             double* rec, unsigned* dflags, cudaStream_t s);
+                             double* rec, unsigned* dflags, cudaStream_t s, bool pdl = false);
 cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt, int istep,
                              int ncx, int ncy, int* cell_count, int* cell_start, int* cell_fill,
                              int* cell_dirty, int* items, int* nudge_vol, double* tempreadint,

@@ -22,35 +22,33 @@ namespace lbrb {
 
 template <typename Real, bool DERIVS>
 __global__ void __launch_bounds__(128) particle_kernel(const PView<Real> V) {
+  pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= V.np) return;
   particle_update<Real, DERIVS>(V, p);
 }
 
 template <typename Real>
-cudaError_t launch_particles_t(const PView<Real>& V, cudaStream_t s) {
+cudaError_t launch_particles_t(const PView<Real>& V, cudaStream_t s, bool pdl) {
   if (V.np <= 0) return cudaSuccess;
   // the derivative stencil only where beta != 0 or full records need it
-  if (V.beta != 0.0 || V.full)
-    particle_kernel<Real, true><<<(V.np + 127) / 128, 128, 0, s>>>(V);
-  else
-    particle_kernel<Real, false><<<(V.np + 127) / 128, 128, 0, s>>>(V);
-  return cudaGetLastError();
+  if (V.beta != 0.0 || V.full) return launch_k(particle_kernel<Real, true>, (V.np + 127) / 128, 128, 0, s, pdl, V);
+  return launch_k(particle_kernel<Real, false>, (V.np + 127) / 128, 128, 0, s, pdl, V);
 }
 
 // explicit views built by the host side
 cudaError_t launch_particles(const void* u, const void* v, const void* ub, const void* vb,
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,
                              const int* ptype, int np, double beta, int record, int full,
-                             double* rec, unsigned* dflags, cudaStream_t s) {
+                             double* rec, unsigned* dflags, cudaStream_t s, bool pdl) {
   if (fp32) {
     PView<float> V{(const float*)u, (const float*)v, (const float*)ub, (const float*)vb,
                    (const float*)T, nx, ny, pitch, P, ptype, np, beta, record, full, rec, dflags};
-    return launch_particles_t(V, s);
+    return launch_particles_t(V, s, pdl);
   }
   PView<double> V{(const double*)u, (const double*)v, (const double*)ub, (const double*)vb,
                   (const double*)T, nx, ny, pitch, P, ptype, np, beta, record, full, rec, dflags};
-  return launch_particles_t(V, s);
+  return launch_particles_t(V, s, pdl);
 }
 
 }  // namespace lbrb
