@@ -340,10 +340,8 @@ struct MarchStep {
 };
 
 // PRE = 1: the next unit's inputs go to registers before the current unit's
-// arithmetic (one block per SM: about 240 registers); PRE = 2: half a unit
-// ahead (phase 2's inputs during phase 1, the next phase 1's during phase 2);
-// PRE = 0: each phase loads its own inputs and the blocks per SM (MINB) hide
-// each other's loads.
+// arithmetic; PRE = 2: half a unit ahead (phase 2's inputs during phase 1,
+// the next phase 1's during phase 2), which holds fewer registers.
 template <typename Real, int RB, int MINB, int PRE, typename Off>
 __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjPairView<Real> P, int chunk) {
   pdl_wait();
@@ -465,7 +463,8 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
       cur = nxt;
       st = nst;
     }
-  } else if constexpr (PRE == 2) {
+  } else {
+    static_assert(PRE == 2, "prefetch form");
     // half a step ahead: phase 2's loads go out before phase 1's arithmetic,
     // the next step's phase-1 loads before phase 2's arithmetic
     MarchIn<Real> in1, in2;
@@ -492,28 +491,6 @@ __global__ void __launch_bounds__(34 * RB, MINB) adjoint_march_kernel(const AdjP
       if (!more) break;
       st = nst;
       xh = nxh, j1 = nj1, a1 = na1, x2 = nx2, j2 = nj2, a2 = na2;
-    }
-  } else {
-    // each phase loads its own inputs
-    for (;;) {
-      MarchIn<Real> cur;
-      int xh, j1, x2, j2;
-      bool a1, a2;
-      coords(st, xh, j1, a1, x2, j2, a2);
-      if (st.pro && st.u != ub) __syncthreads();
-      if (a1) {
-        load1(xh, j1, cur);
-        phase1(j1, cur);
-      }
-      if (!st.pro) {
-        __syncthreads();
-        if (a2) {
-          load2(x2, j2, cur);
-          phase2(j2, x2, cur);
-        }
-      }
-      st = next(st);
-      if (st.u >= ue) break;
     }
   }
 }
