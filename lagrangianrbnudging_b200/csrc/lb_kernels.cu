@@ -167,11 +167,16 @@ cudaError_t launch_pull_fp32(const LBView<float>& V, int twall, void* outf, void
   return launch_pull_t<float>(V, twall, outf, outg, s);
 }
 
+// launches timed per shape: enough that each shape's timed span is well above
+// the event resolution and launch jitter on small grids
+static int tune_reps(const LBView<float>& V) { return (long)V.nx * V.ny >= (1L << 21) ? 6 : 30; }
+static int tune_reps(const LBView<double>& V) { return (long)V.nx * V.ny >= (1L << 21) ? 6 : 30; }
+
 int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best_ms) {
-  return tune<double>(V, twall, false, s, 6, best_ms);
+  return tune<double>(V, twall, false, s, tune_reps(V), best_ms);
 }
 int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_ms) {
-  return tune<float>(V, twall, false, s, 6, best_ms);
+  return tune<float>(V, twall, false, s, tune_reps(V), best_ms);
 }
 
 }  // namespace lbrb
