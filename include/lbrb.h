@@ -317,7 +317,10 @@ LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, c
  * lbrb_init_conduction on a slab gives the whole domain's profile and noise
  * at its rows; lbrb_nusselt gives the slab's mean of v T at the whole
  * domain's height (the domain's Nu is the slabs' values weighted by ny).
- * Supported: Dirichlet walls, no nudging, no particles. */
+ * Supported: Dirichlet walls, no nudging.  Particles: every slab of the
+ * domain holds all of them (lbrb_particles_set on each, positions in the
+ * whole domain) and lbrb_slab_step moves them; a slab with particles steps
+ * only through lbrb_slab_step. */
 LBRB_API int lbrb_slab_set(lbrb_t *h, int j0, int ny_total);
 /* bytes of one packed boundary row set: 6 rows (f then g) of nx values */
 LBRB_API size_t lbrb_slab_ghost_bytes(const lbrb_t *h);
@@ -334,7 +337,16 @@ LBRB_API int lbrb_slab_pack(lbrb_t *h);
  * several GPUs), slabs in order of j0: per step, every slab packs and copies
  * its boundary rows into its neighbours' ghost rows (peer copies across
  * GPUs), then steps; events order the copies against the neighbours' steps.
- * The moments (rho, u, v, T) are written on the last of the nsteps. */
+ * The moments (rho, u, v, T) are written on the last of the nsteps.
+ * With particles (the reference advances each rank's own particles,
+ * propagate_prtcl at Trajectories/code/mympi2.h:350, and hands those that
+ * leave its rows to the neighbour rank, toggle_prtcl at mympi2.h:568-760):
+ * after every slab's step, the slab whose
+ * rows hold a particle's cell advances it, reading the fields of the other
+ * slabs through peer access (their GPUs must allow it); every slab then
+ * copies in the particles it did not advance, and slab 0 their records, so
+ * each slab's particle array and slab 0's record ring are the whole
+ * domain's, bit for bit.  Drain the records from slab 0. */
 LBRB_API int lbrb_slab_step(lbrb_t *const *slabs, int nslabs, int nsteps);
 
 #ifdef __cplusplus

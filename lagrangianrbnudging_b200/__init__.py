@@ -489,6 +489,32 @@ class SlabDomain:
         """the slabs' values weighted by their heights"""
         return float(sum(hgt * r.nusselt() for r, hgt in zip(self.slabs, self.heights)) / self.ny)
 
+    # ---- particles: every slab holds all of them (the slab that holds a
+    # particle's cell advances it each step); slab 0 keeps the records
+    @property
+    def istep(self) -> int:
+        return self.slabs[0].istep
+
+    def set_particles(self, ids, x, y, u, v, ptype, invtau):
+        for r in self.slabs:
+            r.set_particles(ids, x, y, u, v, ptype, invtau)
+
+    def get_particles(self):
+        return self.slabs[0].get_particles()
+
+    def pending_records(self) -> int:
+        return self.slabs[0].pending_records()
+
+    def drain_records(self, max_records: int | None = None):
+        return self.slabs[0].drain_records(max_records)
+
+    def drain_records_array(self):
+        return self.slabs[0].drain_records_array()
+
+    def check_finite(self):
+        for r in self.slabs:
+            r.check_finite()
+
 
 class Ensemble:
     """Independent runs advanced together (lbrb_ensemble_*): one launch per

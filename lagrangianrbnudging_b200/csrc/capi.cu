@@ -132,11 +132,12 @@ static void free_all(lbrb_t* h) {
   delete[] h->h_chk; delete[] h->h_oid;
   F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
-  F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down);
+  F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down); F(h->slab_own); F(h->slab_tab);
   for (cudaGraphExec_t& g : h->graph_exec)
     if (g) cudaGraphExecDestroy(g);
   if (h->slab_ev_xfer) cudaEventDestroy(h->slab_ev_xfer);
   if (h->slab_ev_done) cudaEventDestroy(h->slab_ev_done);
+  if (h->slab_ev_part) cudaEventDestroy(h->slab_ev_part);
   delete[] h->adj_steps;
   if (h->h_flags) cudaFreeHost(h->h_flags);
   if (h->h_scalar) cudaFreeHost(h->h_scalar);
@@ -392,8 +393,9 @@ int lbrb_particles_set(lbrb_t* h, int n, const int* ids, const double* x, const 
                        const double* u, const double* v, const int* ptype, const double* invtau) {
   if (!h || n != h->np || n <= 0 || !ids || !x || !y || !u || !v || !ptype || !invtau)
     return fail(h, LBRB_ERR_ARG, "particles_set: arguments must cover all nprtcl particles");
+  const int nyd = h->slab ? h->slab_ny_total : h->p.ny;  // (a y-slab: the whole domain's rows)
   for (int q = 0; q < n; q++) {
-    if (!(x[q] > -1.0 && x[q] < h->p.nx + 1.0 && y[q] >= 0.0 && y[q] <= h->p.ny + 1.0))
+    if (!(x[q] > -1.0 && x[q] < h->p.nx + 1.0 && y[q] >= 0.0 && y[q] <= nyd + 1.0))
       return fail(h, LBRB_ERR_RANGE, "particles_set: position outside the domain");
     if (!(u[q] == u[q]) || !(v[q] == v[q]) || !(invtau[q] >= 0.0) ||
         (ptype[q] != LBRB_PTYPE_TRACER && ptype[q] != LBRB_PTYPE_INERTIAL))
@@ -622,7 +624,7 @@ int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
   if (n == 0) return LBRB_OK;
-  if (h->slab && n != 1)
+  if (h->slab && (n != 1 || (h->np > 0 && !h->slab_stepping)))
     return fail(h, LBRB_ERR_ARG, "step: a y-slab takes one step per boundary exchange (lbrb_slab_step)");
   if (!h->moments_valid)
     return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
@@ -655,7 +657,7 @@ int lbrb_step(lbrb_t* h, int n) {
   auto one = [&](bool last) -> int {
     const int istep = h->istep + 1;
     const bool rec = h->np > 0 && h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
-    if (rec && (h->rec_head - h->rec_tail) >= h->p.record_slots)
+    if (rec && !h->slab && (h->rec_head - h->rec_tail) >= h->p.record_slots)
       return fail(h, LBRB_ERR_OVERFLOW, "step: record ring full, drain records first");
     const double* obs = nullptr;
     if (h->p.nudge == LBRB_NUDGE_BILINEAR) {
@@ -703,7 +705,7 @@ int lbrb_step(lbrb_t* h, int n) {
                                   h->acc, h->dflags, h->stream));
       tmark_end(h, tm, h->stream);
     }
-    if (h->np > 0) {
+    if (h->np > 0 && !h->slab) {  // (y-slabs: lbrb_slab_step moves the particles)
       // Particles of step n.  With kParticleStream they run on their own
       // stream beside the fused kernel of step n+1 (u, v rotate over three
       // slots and T over two, ordered by events); measured on B200 the fused
@@ -1143,8 +1145,8 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
   if (!h) return LBRB_ERR_ARG;
   if (j0 < 0 || ny_total < 2 || j0 + h->p.ny > ny_total)
     return fail(h, LBRB_ERR_ARG, "slab_set: rows [j0, j0 + ny) must lie in [0, ny_total)");
-  if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE || h->np > 0)
-    return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls, no nudging and no particles");
+  if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE)
+    return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls and no nudging");
   CK(h, cudaSetDevice(h->dev));
   const size_t gb = lbrb_slab_ghost_bytes(h);
   void** bufs[] = {&h->slab_ghost_lo, &h->slab_ghost_hi, &h->slab_up, &h->slab_down};
@@ -1162,6 +1164,11 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
     if (b) CK(h, cudaMemsetAsync(b, 0, gb, h->stream));
   if (!h->slab_ev_xfer) CK(h, cudaEventCreateWithFlags(&h->slab_ev_xfer, cudaEventDisableTiming));
   if (!h->slab_ev_done) CK(h, cudaEventCreateWithFlags(&h->slab_ev_done, cudaEventDisableTiming));
+  if (h->np > 0) {
+    if (!h->slab_own && dalloc(&h->slab_own, h->np)) return fail(h, LBRB_ERR_NOMEM, "slab particle owners");
+    if (!h->slab_ev_part) CK(h, cudaEventCreateWithFlags(&h->slab_ev_part, cudaEventDisableTiming));
+  }
+  h->slab_sig.clear();  // (tables rebuilt on the next slab step)
   CK(h, cudaStreamSynchronize(h->stream));
   h->slab = true;
   h->slab_j0 = j0;
@@ -1190,6 +1197,127 @@ int lbrb_slab_pack(lbrb_t* h) {
   return LBRB_OK;
 }
 
+// Tables for the particles of a slab domain, one copy on each slab's device
+// (addresses are unified, so the copies are equal): for every global row a
+// pointer to that row of u and v (3 slots each) and T (2 buffers) in the slab
+// that holds it, then each slab's particle array and record ring, then the
+// slab of each row.  Kernels on one device read the other slabs' rows through
+// peer access.
+static size_t tab_rows(int ny_total) { return (size_t)8 * ny_total; }
+static int slab_particle_tables(lbrb_t* const* slabs, int n) {
+  lbrb_t* h0 = slabs[0];
+  std::vector<const void*> sig;
+  for (int s = 0; s < n; s++) {
+    sig.push_back(slabs[s]);
+    sig.push_back(slabs[s]->px);
+  }
+  bool fresh = true;
+  for (int s = 0; s < n; s++) fresh = fresh && slabs[s]->slab_sig == sig;
+  if (fresh) return LBRB_OK;
+  for (int s = 0; s < n; s++)
+    for (int t = 0; t < n; t++) {
+      const int a = slabs[s]->dev, b = slabs[t]->dev;
+      if (a == b) continue;
+      int ok = 0;
+      CK(slabs[s], cudaDeviceCanAccessPeer(&ok, a, b));
+      if (!ok) return fail(slabs[s], LBRB_ERR_UNSUPPORTED, "slab_step: particles need peer access between the slabs' GPUs");
+      CK(slabs[s], cudaSetDevice(a));
+      const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
+      if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
+      else if (e != cudaSuccess) return fail(slabs[s], LBRB_ERR_CUDA, "slab_step: peer access", e);
+    }
+  const int nyT = h0->slab_ny_total;
+  const size_t nptr = tab_rows(nyT) + 2 * (size_t)n;
+  std::vector<unsigned char> tab(nptr * sizeof(void*) + (size_t)nyT * sizeof(int));
+  const void** ptr = (const void**)tab.data();
+  int* sor = (int*)(tab.data() + nptr * sizeof(void*));
+  for (int t = 0; t < n; t++) {
+    const lbrb_t* h = slabs[t];
+    const size_t rowb = (size_t)h->pitch * h->esize;
+    for (int jl = 0; jl < h->p.ny; jl++) {
+      const int j = h->slab_j0 + jl;
+      for (int a = 0; a < 3; a++) {
+        ptr[(size_t)a * nyT + j] = (const char*)h->uv[a][0] + jl * rowb;
+        ptr[(size_t)(3 + a) * nyT + j] = (const char*)h->uv[a][1] + jl * rowb;
+      }
+      for (int b = 0; b < 2; b++) ptr[(size_t)(6 + b) * nyT + j] = (const char*)h->T[b] + jl * rowb;
+      sor[j] = t;
+    }
+    ptr[tab_rows(nyT) + t] = h->px;
+    ptr[tab_rows(nyT) + n + t] = h->d_ring;
+  }
+  for (int s = 0; s < n; s++) {
+    lbrb_t* h = slabs[s];
+    CK(h, cudaSetDevice(h->dev));
+    if (h->slab_tab_bytes < tab.size()) {
+      if (h->slab_tab) cudaFree(h->slab_tab);
+      h->slab_tab = nullptr;
+      h->slab_tab_bytes = 0;
+      if (cudaMalloc(&h->slab_tab, tab.size()) != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "slab particle tables");
+      h->slab_tab_bytes = tab.size();
+    }
+    CK(h, cudaMemcpyAsync(h->slab_tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->slab_sig = sig;
+  }
+  return LBRB_OK;
+}
+
+// Particles of one step of a slab domain, after every slab's fused kernel:
+// each slab advances the particles whose cell lies in its rows (fields read
+// through the row tables, records into its own ring slot), then each slab
+// takes the particles it did not advance from their owners, and slab 0 their
+// records, which it copies to the host like a whole domain's.
+static int slab_particles(lbrb_t* const* slabs, int n) {
+  lbrb_t* h0 = slabs[0];
+  const int np = h0->np, nyT = h0->slab_ny_total;
+  const int istep = h0->istep;  // (the step just taken)
+  const bool rec = h0->p.noutconfig > 0 && istep % h0->p.noutconfig == 0;
+  const int slot = rec ? (int)(h0->rec_head % h0->p.record_slots) : 0;
+  const size_t per = (size_t)h0->nrec_fields * np;
+  const size_t rec_off = (size_t)slot * per;
+  for (int s = 0; s < n; s++) {
+    lbrb_t* h = slabs[s];
+    CK(h, cudaSetDevice(h->dev));
+    for (int t = 0; t < n; t++)
+      if (t != s) CK(h, cudaStreamWaitEvent(h->stream, slabs[t]->slab_ev_done, 0));
+    const void* const* rows = (const void* const*)h->slab_tab;
+    // after the step: u, v in slot uvcur, the step's input in uvprev, T in cur
+    const void* rows5[5] = {rows + (size_t)h->uvcur * nyT, rows + (size_t)(3 + h->uvcur) * nyT,
+                            rows + (size_t)h->uvprev * nyT, rows + (size_t)(3 + h->uvprev) * nyT,
+                            rows + (size_t)(6 + h->cur) * nyT};
+    const int* sor = (const int*)(rows + tab_rows(nyT) + 2 * (size_t)n);
+    const bool f32 = fp32(h);
+    CK(h, launch_particles_slab(h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->uv[h->uvprev][0], h->uv[h->uvprev][1],
+                                h->T[h->cur], rows5, f32, h->p.nx, nyT, h->pitch, h->px, h->ptype, np, h->p.beta,
+                                rec ? 1 : 0, h->p.record_full, rec ? h->d_ring + rec_off : nullptr, h->dflags, sor,
+                                s, h->slab_own, h->stream));
+    CK(h, cudaEventRecord(h->slab_ev_part, h->stream));
+  }
+  for (int s = 0; s < n; s++) {
+    lbrb_t* h = slabs[s];
+    CK(h, cudaSetDevice(h->dev));
+    for (int t = 0; t < n; t++)
+      if (t != s) CK(h, cudaStreamWaitEvent(h->stream, slabs[t]->slab_ev_part, 0));
+    const void* const* rows = (const void* const*)h->slab_tab;
+    const double* const* Ps = (const double* const*)(rows + tab_rows(nyT));
+    CK(h, launch_particles_merge(h->px, np, h->slab_own, s, Ps, s == 0 && rec ? h->d_ring + rec_off : nullptr,
+                                 Ps + n, rec_off, h0->nrec_fields, h->stream));
+  }
+  if (rec) {
+    CK(h0, cudaSetDevice(h0->dev));
+    h0->h_ring_step[slot] = istep;
+    CK(h0, cudaEventRecord(h0->ring_ev[slot], h0->stream));
+    CK(h0, cudaStreamWaitEvent(h0->copy_stream, h0->ring_ev[slot], 0));
+    CK(h0, cudaMemcpyAsync(h0->h_ring + rec_off, h0->d_ring + rec_off, per * sizeof(double), cudaMemcpyDeviceToHost,
+                           h0->copy_stream));
+    CK(h0, cudaEventRecord(h0->ring_ev[slot], h0->copy_stream));
+    h0->rec_head++;
+    h0->join_pending = true;
+  }
+  return LBRB_OK;
+}
+
 int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
   if (!slabs || n < 1 || nsteps < 0) return LBRB_ERR_ARG;
   for (int s = 0; s < n; s++) {
@@ -1202,18 +1330,34 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
     if (h->slab_j0 != (s == 0 ? 0 : slabs[s - 1]->slab_j0 + slabs[s - 1]->p.ny)) return LBRB_ERR_ARG;
   }
   if (slabs[n - 1]->slab_j0 + slabs[n - 1]->p.ny != slabs[0]->slab_ny_total) return LBRB_ERR_ARG;
-  const size_t gb = lbrb_slab_ghost_bytes(slabs[0]);
+  lbrb_t* h0 = slabs[0];
+  const bool parts = h0->np > 0;
+  for (int s = 0; s < n; s++) {
+    lbrb_t* h = slabs[s];
+    if (h->np != h0->np) return fail(h, LBRB_ERR_ARG, "slab_step: every slab holds all particles");
+    if (!parts) continue;
+    if (!h->particles_set) return fail(h, LBRB_ERR_STATE, "slab_step: particles not set");
+    if (h->p.noutconfig != h0->p.noutconfig || h->p.record_full != h0->p.record_full || h->p.beta != h0->p.beta ||
+        h->istep != h0->istep || h->cur != h0->cur || h->uvcur != h0->uvcur || h->uvprev != h0->uvprev)
+      return fail(h, LBRB_ERR_ARG, "slab_step: slabs differ in particle settings or step");
+  }
+  if (parts) {
+    const int rc = slab_particle_tables(slabs, n);
+    if (rc) return rc;
+  }
+  const size_t gb = lbrb_slab_ghost_bytes(h0);
   for (int it = 0; it < nsteps; it++) {
+    if (parts && h0->p.noutconfig > 0 && (h0->istep + 1) % h0->p.noutconfig == 0 &&
+        h0->rec_head - h0->rec_tail >= h0->p.record_slots)
+      return fail(h0, LBRB_ERR_OVERFLOW, "slab_step: record ring full, drain records first");
     // 1. each slab packs its boundary rows and copies them into its
     //    neighbours' ghost rows, once the neighbours' previous step (which
-    //    read those ghost rows) is done
+    //    read those ghost rows, possibly in an earlier call) is done
     for (int s = 0; s < n; s++) {
       lbrb_t* h = slabs[s];
       CK(h, cudaSetDevice(h->dev));
-      if (it > 0) {
-        if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_done, 0));
-        if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_done, 0));
-      }
+      if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_done, 0));
+      if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_done, 0));
       int rc = lbrb_slab_pack(h);
       if (rc) return rc;
       if (s + 1 < n)
@@ -1230,11 +1374,27 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
       if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_xfer, 0));
       // the moments (rho, u, v, T) are written on the last step only
       h->slab_defer_moments = it + 1 < nsteps;
+      h->slab_stepping = true;
       int rc = lbrb_step(h, 1);
       h->slab_defer_moments = false;
+      h->slab_stepping = false;
       if (rc) return rc;
       CK(h, cudaEventRecord(h->slab_ev_done, h->stream));
     }
+    // 3. the particles of the step (next step's fused kernels run after them:
+    //    each slab's stream holds its merge, which waited for every slab's
+    //    particle kernel)
+    if (parts) {
+      const int rc = slab_particles(slabs, n);
+      if (rc) return rc;
+    }
+  }
+  if (h0->join_pending) {
+    // the record copies are part of the steps for slab 0's stream
+    CK(h0, cudaSetDevice(h0->dev));
+    CK(h0, cudaEventRecord(h0->join_ev, h0->copy_stream));
+    CK(h0, cudaStreamWaitEvent(h0->stream, h0->join_ev, 0));
+    h0->join_pending = false;
   }
   return LBRB_OK;
 }

@@ -30,6 +30,16 @@ cudaError_t launch_particles(const void* u, const void* v, const void* ub, const
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,
                              const int* ptype, int np, double beta, int record, int full,
                              double* rec, unsigned* dflags, cudaStream_t s, bool pdl = false);
+// y-slabs: rows5 = device tables of row pointers (u, v, ub, vb, T), one
+// entry per global row
+cudaError_t launch_particles_slab(const void* u, const void* v, const void* ub, const void* vb, const void* T,
+                                  const void* const* rows5, bool fp32, int nx, int ny_total, int pitch,
+                                  double* P, const int* ptype, int np, double beta, int record, int full,
+                                  double* rec, unsigned* dflags, const int* slab_of_row, int me, int* own,
+                                  cudaStream_t s);
+cudaError_t launch_particles_merge(double* P, int np, const int* own, int me, const double* const* Ps,
+                                   double* rec, const double* const* recs, size_t rec_off, int nrec,
+                                   cudaStream_t s);
 cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt, int istep,
                              int ncx, int ncy, int* cell_count, int* cell_start, int* cell_fill,
                              int* cell_dirty, int* items, int* nudge_vol, double* tempreadint,

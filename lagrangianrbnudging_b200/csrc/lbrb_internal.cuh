@@ -10,6 +10,7 @@
 // communication) become index wrap.
 #pragma once
 #include <utility>
+#include <vector>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -170,6 +171,17 @@ struct Handle {
   void* slab_down = nullptr;
   cudaEvent_t slab_ev_xfer = nullptr, slab_ev_done = nullptr;
   bool slab_defer_moments = false;  // inside lbrb_slab_step: moments on its last step only
+  bool slab_stepping = false;       // inside lbrb_slab_step
+  // particles of a slab domain: every slab holds all of them; slab_own: the
+  // owner slab of each particle in the last step; slab_tab: device tables
+  // (row pointers of u, v for 3 slots and T for 2 buffers, then every slab's
+  // particle array and record ring, then the slab of each row) built for the
+  // slab list slab_sig
+  int* slab_own = nullptr;
+  void* slab_tab = nullptr;
+  size_t slab_tab_bytes = 0;
+  std::vector<const void*> slab_sig;
+  cudaEvent_t slab_ev_part = nullptr;
   // CUDA graphs of plain steps, one per buffer phase (cur * 9 + uvcur * 3 +
   // uvprev); graph_mode -1: small grids only, 0: off, 1: on
   cudaGraphExec_t graph_exec[18] = {};

@@ -23,7 +23,24 @@ struct PView {
   int full;                // also the 8 Writefull fields
   double* __restrict__ rec;  // ring slot base, [fields][np]
   unsigned* dflags;
+  // y-slabs of one domain: for each global row, a pointer to that row of u,
+  // v, ub, vb and T in the slab that holds it (nx, ny are then the whole
+  // domain's); null for a whole domain in one handle
+  const Real* const* __restrict__ urow;
+  const Real* const* __restrict__ vrow;
+  const Real* const* __restrict__ ubrow;
+  const Real* const* __restrict__ vbrow;
+  const Real* const* __restrict__ Trow;
 };
+
+// value of a field at row j, column i: one plane (ROWS = false) or a table of
+// row pointers (ROWS = true, a domain held as y-slabs)
+template <bool ROWS, typename Real>
+__device__ __forceinline__ Real fat(const Real* __restrict__ f, const Real* const* __restrict__ rows, int pitch,
+                                    int j, int i) {
+  if constexpr (ROWS) return rows[j][i];
+  else return f[(size_t)j * pitch + i];
+}
 
 __device__ __forceinline__ int wrapi(int a, int n) {
   int r = a % n;
@@ -65,57 +82,59 @@ __device__ __forceinline__ double bil_combine(const Cell& c, double xx, double y
   return val1 + val2 + val3 + val4;
 }
 
-template <typename Real>
-__device__ __forceinline__ double bilin(const Real* __restrict__ f, int pitch, const Cell& c,
-                                        double xx, double yy) {
-  double u11 = (double)f[(size_t)c.jy[0] * pitch + c.ix[0]];
-  double u12 = (double)f[(size_t)c.jy[1] * pitch + c.ix[0]];
-  double u21 = (double)f[(size_t)c.jy[0] * pitch + c.ix[1]];
-  double u22 = (double)f[(size_t)c.jy[1] * pitch + c.ix[1]];
+template <bool ROWS = false, typename Real>
+__device__ __forceinline__ double bilin(const Real* __restrict__ f, const Real* const* rows, int pitch,
+                                        const Cell& c, double xx, double yy) {
+  double u11 = (double)fat<ROWS>(f, rows, pitch, c.jy[0], c.ix[0]);
+  double u12 = (double)fat<ROWS>(f, rows, pitch, c.jy[1], c.ix[0]);
+  double u21 = (double)fat<ROWS>(f, rows, pitch, c.jy[0], c.ix[1]);
+  double u22 = (double)fat<ROWS>(f, rows, pitch, c.jy[1], c.ix[1]);
   return bil_combine(c, xx, yy, u11, u12, u21, u22);
 }
 
 // derivative terms at one device node (i, j): dt, dx, dy of u and v
-template <typename Real>
+template <bool ROWS = false, typename Real>
 __device__ __forceinline__ void node_derivs(const PView<Real>& V, int i, int j, double d[6]) {
   const int nx = V.nx, ny = V.ny, pitch = V.pitch;
-  const size_t q = (size_t)j * pitch + i;
-  const size_t qr = (size_t)j * pitch + wrapi(i + 1, nx), ql = (size_t)j * pitch + wrapi(i - 1, nx);
-  const size_t qt = (size_t)wrapi(j + 1, ny) * pitch + i, qb = (size_t)wrapi(j - 1, ny) * pitch + i;
-  const double uq = (double)V.u[q], vq = (double)V.v[q];
-  d[0] = uq - (double)V.ub[q];
-  d[1] = vq - (double)V.vb[q];
-  d[2] = ((double)V.u[qr] - (double)V.u[ql]) * 0.5;
-  d[3] = ((double)V.v[qr] - (double)V.v[ql]) * 0.5;
+  auto U = [&](int jj, int ii) { return (double)fat<ROWS>(V.u, V.urow, pitch, jj, ii); };
+  auto W = [&](int jj, int ii) { return (double)fat<ROWS>(V.v, V.vrow, pitch, jj, ii); };
+  const int ir = wrapi(i + 1, nx), il = wrapi(i - 1, nx);
+  const int jt = wrapi(j + 1, ny), jb = wrapi(j - 1, ny);
+  const double uq = U(j, i), vq = W(j, i);
+  d[0] = uq - (double)fat<ROWS>(V.ub, V.ubrow, pitch, j, i);
+  d[1] = vq - (double)fat<ROWS>(V.vb, V.vbrow, pitch, j, i);
+  d[2] = (U(j, ir) - U(j, il)) * 0.5;
+  d[3] = (W(j, ir) - W(j, il)) * 0.5;
   if (j == 0) {
-    d[4] = ((double)V.u[qt] - uq);
-    d[5] = ((double)V.v[qt] - vq);
+    d[4] = (U(jt, i) - uq);
+    d[5] = (W(jt, i) - vq);
   } else if (j == ny - 1) {
-    d[4] = (uq - (double)V.u[qb]);
-    d[5] = (vq - (double)V.v[qb]);
+    d[4] = (uq - U(jb, i));
+    d[5] = (vq - W(jb, i));
   } else {
-    d[4] = ((double)V.u[qt] - (double)V.u[qb]) * 0.5;
-    d[5] = ((double)V.v[qt] - (double)V.v[qb]) * 0.5;
+    d[4] = (U(jt, i) - U(jb, i)) * 0.5;
+    d[5] = (W(jt, i) - W(jb, i)) * 0.5;
   }
 }
 
 // bilinear of the six derivative fields over one cell
-template <typename Real>
+template <bool ROWS = false, typename Real>
 __device__ __forceinline__ void bilin_derivs(const PView<Real>& V, const Cell& c, double xx,
                                              double yy, double out[6]) {
   double d11[6], d12[6], d21[6], d22[6];
-  node_derivs(V, c.ix[0], c.jy[0], d11);
-  node_derivs(V, c.ix[0], c.jy[1], d12);
-  node_derivs(V, c.ix[1], c.jy[0], d21);
-  node_derivs(V, c.ix[1], c.jy[1], d22);
+  node_derivs<ROWS>(V, c.ix[0], c.jy[0], d11);
+  node_derivs<ROWS>(V, c.ix[0], c.jy[1], d12);
+  node_derivs<ROWS>(V, c.ix[1], c.jy[0], d21);
+  node_derivs<ROWS>(V, c.ix[1], c.jy[1], d22);
 #pragma unroll
   for (int w = 0; w < 6; w++) out[w] = bil_combine(c, xx, yy, d11[w], d12[w], d21[w], d22[w]);
 }
 
 // one particle of one step: interpolate, advance, record, wrap/reflect
 // DERIVS = false: the run needs no Maxey-Riley derivative terms (beta == 0
-// and no full records), so the 4x4 derivative stencil is not compiled in
-template <typename Real, bool DERIVS = true>
+// and no full records), so the 4x4 derivative stencil is not compiled in.
+// ROWS: the fields are read through the view's row tables (y-slabs).
+template <typename Real, bool DERIVS = true, bool ROWS = false>
 __device__ __forceinline__ void particle_update(const PView<Real>& V, int p) {
   const int n = V.np;
   double* X = V.P;
@@ -125,12 +144,12 @@ __device__ __forceinline__ void particle_update(const PView<Real>& V, int p) {
   const double invtau = X[8 * n + p];
   Cell c;
   make_cell(xx, yy, V.nx, V.ny, c, V.dflags);
-  const double tempup = bilin(V.u, V.pitch, c, xx, yy);
-  const double tempvp = bilin(V.v, V.pitch, c, xx, yy);
+  const double tempup = bilin<ROWS>(V.u, V.urow, V.pitch, c, xx, yy);
+  const double tempvp = bilin<ROWS>(V.v, V.vrow, V.pitch, c, xx, yy);
   const bool tracer = V.ptype[p] == LBRB_PTYPE_TRACER;
   const bool need_d = (!tracer && V.beta != 0.0) || (V.record && V.full);
   double dd[6] = {0, 0, 0, 0, 0, 0};
-  if (DERIVS && need_d) bilin_derivs(V, c, xx, yy, dd);
+  if (DERIVS && need_d) bilin_derivs<ROWS>(V, c, xx, yy, dd);
   double xn, yn, un, vn;
   if (tracer) {
     xn = xx + 1.5 * delta_t * tempup - 0.5 * delta_t * uold;
@@ -156,7 +175,7 @@ __device__ __forceinline__ void particle_update(const PView<Real>& V, int p) {
     r[LBRB_REC_VO * n + p] = vold;
     Cell cn;
     make_cell(xn, yn, V.nx, V.ny, cn, V.dflags);
-    r[LBRB_REC_TEMP * n + p] = bilin(V.T, V.pitch, cn, xn, yn);
+    r[LBRB_REC_TEMP * n + p] = bilin<ROWS>(V.T, V.Trow, V.pitch, cn, xn, yn);
     if (V.full) {
       // Writefull terms at (xo, yo): the cell this step started in
       r[LBRB_REC_DTU * n + p] = dd[0];

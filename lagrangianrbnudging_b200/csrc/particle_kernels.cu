@@ -36,6 +36,76 @@ cudaError_t launch_particles_t(const PView<Real>& V, cudaStream_t s, bool pdl) {
   return launch_k(particle_kernel<Real, false>, (V.np + 127) / 128, 128, 0, s, pdl, V);
 }
 
+// ------------------------------------------------------------- y-slabs
+// A domain held as y-slabs: every slab holds all particles.  Each step, the
+// slab whose rows hold a particle's cell (its position before the step)
+// advances it, reading the fields through the view's row tables; every slab
+// notes that owner.  The merge then copies each particle it did not own (and,
+// on record steps, its record) from its owner.  (The reference keeps each
+// rank's particles in that rank and sends those that leave its rows to the
+// neighbour, toggle_prtcl in Trajectories/code/mympi2.h:568-760; replicated
+// arrays need no compaction and keep the whole domain's particle order.)
+__device__ __forceinline__ int cell_row(double yy, int ny) {
+  if (!(yy > -2.0 && yy < ny + 2.0)) return 0;  // (flagged by make_cell)
+  return wrapi((int)yy - 1, ny);
+}
+
+template <typename Real, bool DERIVS>
+__global__ void __launch_bounds__(128)
+    particle_slab_kernel(const PView<Real> V, const int* __restrict__ slab_of_row, int me, int* __restrict__ own) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= V.np) return;
+  const int o = slab_of_row[cell_row(V.P[V.np + p], V.ny)];
+  own[p] = o;
+  if (o != me) return;
+  particle_update<Real, DERIVS, true>(V, p);
+}
+
+__global__ void __launch_bounds__(128)
+    particle_merge_kernel(double* __restrict__ P, int np, const int* __restrict__ own, int me,
+                          const double* const* __restrict__ Ps, double* __restrict__ rec,
+                          const double* const* __restrict__ recs, size_t rec_off, int nrec) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int o = own[p];
+  if (o == me) return;
+  const double* Q = Ps[o];
+#pragma unroll
+  for (int k = 0; k < 8; k++) P[(size_t)k * np + p] = Q[(size_t)k * np + p];
+  if (rec) {
+    const double* R = recs[o] + rec_off;
+    for (int f = 0; f < nrec; f++) rec[(size_t)f * np + p] = R[(size_t)f * np + p];
+  }
+}
+
+cudaError_t launch_particles_slab(const void* u, const void* v, const void* ub, const void* vb, const void* T,
+                                  const void* const* rows5, bool fp32, int nx, int ny_total, int pitch,
+                                  double* P, const int* ptype, int np, double beta, int record, int full,
+                                  double* rec, unsigned* dflags, const int* slab_of_row, int me, int* own,
+                                  cudaStream_t s) {
+  if (np <= 0) return cudaSuccess;
+  const int g = (np + 127) / 128;
+  auto go = [&](auto zero) -> cudaError_t {
+    using Real = decltype(zero);
+    using Rows = const Real* const*;
+    PView<Real> V{(const Real*)u, (const Real*)v, (const Real*)ub, (const Real*)vb, (const Real*)T, nx, ny_total,
+                  pitch, P, ptype, np, beta, record, full, rec, dflags, (Rows)rows5[0], (Rows)rows5[1],
+                  (Rows)rows5[2], (Rows)rows5[3], (Rows)rows5[4]};
+    if (beta != 0.0 || full) particle_slab_kernel<Real, true><<<g, 128, 0, s>>>(V, slab_of_row, me, own);
+    else particle_slab_kernel<Real, false><<<g, 128, 0, s>>>(V, slab_of_row, me, own);
+    return cudaGetLastError();
+  };
+  return fp32 ? go(0.f) : go(0.0);
+}
+
+cudaError_t launch_particles_merge(double* P, int np, const int* own, int me, const double* const* Ps,
+                                   double* rec, const double* const* recs, size_t rec_off, int nrec,
+                                   cudaStream_t s) {
+  if (np <= 0) return cudaSuccess;
+  particle_merge_kernel<<<(np + 127) / 128, 128, 0, s>>>(P, np, own, me, Ps, rec, recs, rec_off, nrec);
+  return cudaGetLastError();
+}
+
 // explicit views built by the host side
 cudaError_t launch_particles(const void* u, const void* v, const void* ub, const void* vb,
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,

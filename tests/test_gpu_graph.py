@@ -50,8 +50,9 @@ def test_graph_replay_is_bit_identical(precision, nprtcl, beta, full):
                 np.testing.assert_array_equal(ma[k], mb[k])
             if nprtcl:
                 pa, pb = a.get_particles(), b.get_particles()
-                for xa, xb in zip(pa, pb):
-                    np.testing.assert_array_equal(xa, xb)
+                assert pa.keys() == pb.keys()
+                for k in pa:
+                    np.testing.assert_array_equal(pa[k], pb[k])
                 sa, ra = a.drain_records_array()
                 sb, rb = b.drain_records_array()
                 np.testing.assert_array_equal(sa, sb)

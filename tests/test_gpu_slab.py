@@ -1,7 +1,8 @@
 """One domain cut into y-slabs (lbrb_slab_set / lbrb_slab_step): the slabs
 advance exactly as the whole domain in one handle, bit for bit, in both
-precisions and with uneven slab heights; the slabs' initial state is the
-whole domain's; the height-weighted Nu is the whole domain's.  On one GPU the
+precisions and with uneven slab heights, particles and their records
+included; the slabs' initial state is the whole domain's; the
+height-weighted Nu is the whole domain's.  On one GPU the
 slabs are handles on the same device: the exchange is the same peer copy as
 across GPUs (cudaMemcpyPeerAsync), ordered by the same events."""
 import numpy as np
@@ -75,12 +76,85 @@ def test_slab_mode_rejects_what_it_does_not_cover():
         r.init_conduction(1, 1e-3)
         with pytest.raises(lb.LbrbError):
             r.step(2)  # one step per boundary exchange
-    with lb.Run(**dict(params("fp32"), ny=24, nprtcl=8)) as r:
+    with lb.Run(**dict(params("fp32"), ny=24, twall="adiabatic")) as r:
         with pytest.raises(lb.LbrbError):
-            r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # particles are not covered
+            r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # adiabatic walls are not covered
+    with lb.Run(**dict(params("fp32"), ny=24, nprtcl=8)) as r:
+        r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))
+        r.init_conduction(1, 1e-3)
+        r.set_particles(np.arange(8, dtype=np.int32), np.full(8, 5.0), np.full(8, 40.0), np.zeros(8),
+                        np.zeros(8), np.zeros(8, np.int32), np.zeros(8))  # (y in the whole domain)
+        with pytest.raises(lb.LbrbError):
+            r.step(1)  # particles move through lbrb_slab_step only
     with pytest.raises(ValueError):
         lb.SlabDomain((20, 20), **params("fp32"))  # heights must add up to ny
     with lb.SlabDomain((24, 24), **params("fp32")) as dom:
         dom.init_conduction(1, 1e-3)
         rev = (lb.C.c_void_p * 2)(dom.slabs[1].h, dom.slabs[0].h)
         assert lb.ERRORS[lb.lib().lbrb_slab_step(rev, 2, 1)] == "LBRB_ERR_ARG"  # slabs out of order
+
+
+def seed_particles(run, n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.5, NX + 0.5, n)
+    y = rng.uniform(1.0, NY, n)
+    y[:6] = [1.0, 20.5, 21.0, 36.99, 37.0, NY - 0.01]  # on and beside the slab boundaries and walls
+    ptype = (np.arange(n) % 2).astype(np.int32)  # tracers and inertial particles
+    invtau = np.where(ptype == 1, 1.0 / 40.0, 0.0)
+    u0 = rng.uniform(-0.01, 0.01, n)
+    run.set_particles(np.arange(n, dtype=np.int32)[::-1].copy(), x, y, u0, -u0, ptype, invtau)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("beta,full", [(0.0, 0), (0.5, 1)])
+def test_slab_particles_and_records_match_the_whole_domain(precision, beta, full):
+    """particles cross the inner boundaries of three uneven slabs; states and
+    records equal the whole domain's bit for bit"""
+    npart = 300
+    kw = dict(params(precision), nprtcl=npart, noutconfig=7, record_slots=64, beta=beta, record_full=full)
+    with lb.Run(**params(precision)) as dev:  # a developed flow (no particles)
+        dev.init_conduction(23, 5e-2)
+        dev.step(3000)
+        f, g = dev.get_populations()
+        m = dev.get_moments()
+    with lb.Run(**kw) as whole, lb.SlabDomain((20, 17, 11), **kw) as dom:
+        for d in (whole, dom):
+            d.set_populations(f, g)
+            d.set_moments(m["rho"], m["u"], m["v"], m["T"])
+        seed_particles(whole, npart, 4)
+        seed_particles(dom, npart, 4)
+        y0 = whole.get_particles()["y"]
+        for n in (1, 6, 90, 300):
+            whole.step(n)
+            dom.step(n)
+            pw, ps = whole.get_particles(), dom.get_particles()
+            for k in pw:
+                np.testing.assert_array_equal(ps[k], pw[k])
+            sw, rw = whole.drain_records_array()
+            ss, rs = dom.drain_records_array()
+            np.testing.assert_array_equal(ss, sw)
+            np.testing.assert_array_equal(rs, rw)
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+        assert dom.istep == whole.istep
+        # the particles did change slabs
+        edges = np.array([20, 37])
+        moved = np.searchsorted(edges, y0 - 1, side="right") != np.searchsorted(edges, pw["y"] - 1, side="right")
+        assert moved.sum() > 10
+
+
+def test_slab_particle_record_ring_overflow_is_reported():
+    kw = dict(params("fp32"), nprtcl=16, noutconfig=2, record_slots=2)
+    with lb.SlabDomain((24, 24), **kw) as dom:
+        dom.init_conduction(3, 1e-2)
+        seed_particles(dom, 16, 1)
+        dom.step(4)
+        assert dom.pending_records() == 2
+        with pytest.raises(lb.LbrbError):
+            dom.step(2)
+        steps, _ = dom.drain_records_array()
+        assert list(steps) == [2, 4]
+        dom.step(2)
+        assert dom.pending_records() == 1
