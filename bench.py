@@ -851,6 +851,34 @@ def run_slab_bench(lb, torch, device: int, steps: int = SLAB_STEPS, devices=None
                 r.set_stream(None)
         out[f"slabs_{n}"] = {"mlups": round(nodes * steps / (ms * 1e3), 1),
                              "vs_single_handle": round(ms1 / ms, 4), "bit_exact_T_u": bool(exact)}
+    # the production workload with its 2^17 particles and records: one handle
+    # against 2 slabs (owner slab advances, the others copy in)
+    pk = dict(base, nprtcl=NPRTCL, noutconfig=NOUTCONFIG, record_slots=steps // NOUTCONFIG + 4)
+
+    def timed_p(obj, set_stream):
+        set_stream(stream.cuda_stream)
+        init_run(obj, SEED)
+        obj.step(20)
+        obj.drain_records_array()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        obj.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), obj.get_particles(), obj.drain_records_array()
+
+    with lb.Run(**pk, device=device) as whole:
+        ms1, p1, r1 = timed_p(whole, whole.set_stream)
+    with lb.SlabDomain([NY // 2] * 2, devices=devices, **pk, device=device) as dom:
+        ms, p2, r2 = timed_p(dom, lambda st: [r.set_stream(st) for r in dom.slabs])
+        for r in dom.slabs:
+            r.set_stream(None)
+    exact = all(np.array_equal(p1[k], p2[k]) for k in p1) and all(np.array_equal(a, b) for a, b in zip(r1, r2))
+    out["particles_2_slabs"] = {"nprtcl": NPRTCL, "records_every": NOUTCONFIG,
+                                "single_handle_mlups": round(nodes * steps / (ms1 * 1e3), 1),
+                                "mlups": round(nodes * steps / (ms * 1e3), 1), "vs_single_handle": round(ms1 / ms, 4),
+                                "bit_exact_particles_records": bool(exact)}
     out["note"] = ("slabs on one GPU and one stream: the figure is the exchange's overhead; "
                    "across GPUs each slab runs on its own device")
     return out
