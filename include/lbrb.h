@@ -317,10 +317,11 @@ LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, c
  * lbrb_init_conduction on a slab gives the whole domain's profile and noise
  * at its rows; lbrb_nusselt gives the slab's mean of v T at the whole
  * domain's height (the domain's Nu is the slabs' values weighted by ny).
- * Supported: Dirichlet walls, no nudging.  Particles: every slab of the
- * domain holds all of them (lbrb_particles_set on each, positions in the
- * whole domain) and lbrb_slab_step moves them; a slab with particles steps
- * only through lbrb_slab_step. */
+ * Supported: Dirichlet walls; particles; bilinear nudging (not box
+ * nudging).  Every slab of the domain holds all particles and all
+ * observations (lbrb_particles_set / lbrb_nudge_obs on each, in the whole
+ * domain's coordinates) and lbrb_slab_step moves and applies them; a slab
+ * with particles or nudging steps only through lbrb_slab_step. */
 LBRB_API int lbrb_slab_set(lbrb_t *h, int j0, int ny_total);
 /* bytes of one packed boundary row set: 6 rows (f then g) of nx values */
 LBRB_API size_t lbrb_slab_ghost_bytes(const lbrb_t *h);
@@ -346,7 +347,10 @@ LBRB_API int lbrb_slab_pack(lbrb_t *h);
  * slabs through peer access (their GPUs must allow it); every slab then
  * copies in the particles it did not advance, and slab 0 their records, so
  * each slab's particle array and slab 0's record ring are the whole
- * domain's, bit for bit.  Drain the records from slab 0. */
+ * domain's, bit for bit.  Drain the records from slab 0.
+ * With bilinear nudging, after every slab's step each slab scatters the
+ * innovations of the observations to the cell corners in its own rows
+ * (order-free fixed-point sums, so g is the whole domain's bit for bit). */
 LBRB_API int lbrb_slab_step(lbrb_t *const *slabs, int nslabs, int nsteps);
 
 #ifdef __cplusplus

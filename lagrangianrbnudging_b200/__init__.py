@@ -515,6 +515,12 @@ class SlabDomain:
         for r in self.slabs:
             r.check_finite()
 
+    def nudge_obs(self, first_step: int, x, y, T):
+        """bilinear observations in the whole domain's coordinates, given to
+        every slab (each nudges the corners in its own rows)"""
+        for r in self.slabs:
+            r.nudge_obs(first_step, x, y, T)
+
 
 class Ensemble:
     """Independent runs advanced together (lbrb_ensemble_*): one launch per

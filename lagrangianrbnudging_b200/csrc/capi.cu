@@ -624,7 +624,7 @@ int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
   if (n == 0) return LBRB_OK;
-  if (h->slab && (n != 1 || (h->np > 0 && !h->slab_stepping)))
+  if (h->slab && (n != 1 || ((h->np > 0 || h->p.nudge != LBRB_NUDGE_NONE) && !h->slab_stepping)))
     return fail(h, LBRB_ERR_ARG, "step: a y-slab takes one step per boundary exchange (lbrb_slab_step)");
   if (!h->moments_valid)
     return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
@@ -698,7 +698,8 @@ int lbrb_step(lbrb_t* h, int n) {
       tmark_end(h, tm, h->stream);
     }
     if (h->np > 0 && kParticleStream) CK(h, cudaEventRecord(h->ev_lb, h->stream));
-    if (obs) {
+    if (h->slab) h->slab_obs = obs;  // (y-slabs: lbrb_slab_step nudges once every slab has stepped)
+    if (obs && !h->slab) {
       const int tm = tmark_begin(h, 2, h->stream);
       CK(h, launch_bilinear_nudge(h->T[dst], pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, obs,
                                   obs + h->nobs, obs + 2 * (size_t)h->nobs, h->nobs, h->p.alpha,
@@ -1145,8 +1146,8 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
   if (!h) return LBRB_ERR_ARG;
   if (j0 < 0 || ny_total < 2 || j0 + h->p.ny > ny_total)
     return fail(h, LBRB_ERR_ARG, "slab_set: rows [j0, j0 + ny) must lie in [0, ny_total)");
-  if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge != LBRB_NUDGE_NONE)
-    return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls and no nudging");
+  if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge == LBRB_NUDGE_REFBOX)
+    return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls, no box nudging");
   CK(h, cudaSetDevice(h->dev));
   const size_t gb = lbrb_slab_ghost_bytes(h);
   void** bufs[] = {&h->slab_ghost_lo, &h->slab_ghost_hi, &h->slab_up, &h->slab_down};
@@ -1220,7 +1221,9 @@ static int slab_particle_tables(lbrb_t* const* slabs, int n) {
       if (a == b) continue;
       int ok = 0;
       CK(slabs[s], cudaDeviceCanAccessPeer(&ok, a, b));
-      if (!ok) return fail(slabs[s], LBRB_ERR_UNSUPPORTED, "slab_step: particles need peer access between the slabs' GPUs");
+      if (!ok)
+        return fail(slabs[s], LBRB_ERR_UNSUPPORTED,
+                    "slab_step: particles and nudging need peer access between the slabs' GPUs");
       CK(slabs[s], cudaSetDevice(a));
       const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
       if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
@@ -1332,16 +1335,19 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
   if (slabs[n - 1]->slab_j0 + slabs[n - 1]->p.ny != slabs[0]->slab_ny_total) return LBRB_ERR_ARG;
   lbrb_t* h0 = slabs[0];
   const bool parts = h0->np > 0;
+  const bool nudge = h0->p.nudge == LBRB_NUDGE_BILINEAR;
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
     if (h->np != h0->np) return fail(h, LBRB_ERR_ARG, "slab_step: every slab holds all particles");
+    if (h->p.nudge != h0->p.nudge || h->p.alpha != h0->p.alpha || h->nobs != h0->nobs)
+      return fail(h, LBRB_ERR_ARG, "slab_step: slabs differ in nudging");
     if (!parts) continue;
     if (!h->particles_set) return fail(h, LBRB_ERR_STATE, "slab_step: particles not set");
     if (h->p.noutconfig != h0->p.noutconfig || h->p.record_full != h0->p.record_full || h->p.beta != h0->p.beta ||
         h->istep != h0->istep || h->cur != h0->cur || h->uvcur != h0->uvcur || h->uvprev != h0->uvprev)
       return fail(h, LBRB_ERR_ARG, "slab_step: slabs differ in particle settings or step");
   }
-  if (parts) {
+  if (parts || nudge) {
     const int rc = slab_particle_tables(slabs, n);
     if (rc) return rc;
   }
@@ -1381,7 +1387,24 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
       if (rc) return rc;
       CK(h, cudaEventRecord(h->slab_ev_done, h->stream));
     }
-    // 3. the particles of the step (next step's fused kernels run after them:
+    // 3. bilinear nudging: each slab's innovations read T of every slab and
+    //    go to the corners in its own rows (g of the step's output)
+    if (nudge) {
+      for (int s = 0; s < n; s++) {
+        lbrb_t* h = slabs[s];
+        CK(h, cudaSetDevice(h->dev));
+        for (int t = 0; t < n; t++)
+          if (t != s) CK(h, cudaStreamWaitEvent(h->stream, slabs[t]->slab_ev_done, 0));
+        const double* obs = h->slab_obs;
+        const void* const* Trows = (const void* const*)h->slab_tab + (size_t)(6 + h->cur) * h->slab_ny_total;
+        const int tm = tmark_begin(h, 2, h->stream);
+        CK(h, launch_bilinear_nudge_slab(Trows, pop_base(h, h->cur, 1), fp32(h), h->plane, h->p.nx, h->slab_ny_total,
+                                         h->slab_j0, h->p.ny, h->pitch, obs, obs + h->nobs, obs + 2 * (size_t)h->nobs,
+                                         h->nobs, h->p.alpha, h->acc, h->dflags, h->stream));
+        tmark_end(h, tm, h->stream);
+      }
+    }
+    // 4. the particles of the step (next step's fused kernels run after them:
     //    each slab's stream holds its merge, which waited for every slab's
     //    particle kernel)
     if (parts) {

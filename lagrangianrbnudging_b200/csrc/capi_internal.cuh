@@ -40,6 +40,11 @@ cudaError_t launch_particles_slab(const void* u, const void* v, const void* ub, 
 cudaError_t launch_particles_merge(double* P, int np, const int* own, int me, const double* const* Ps,
                                    double* rec, const double* const* recs, size_t rec_off, int nrec,
                                    cudaStream_t s);
+// y-slabs: Trows = device table of T row pointers, one per global row
+cudaError_t launch_bilinear_nudge_slab(const void* Trows, void* g, bool fp32, size_t plane, int nx, int ny_total,
+                                       int j0, int nyl, int pitch, const double* ox, const double* oy,
+                                       const double* oT, int nobs, double alpha, long long* acc, unsigned* dflags,
+                                       cudaStream_t s);
 cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt, int istep,
                              int ncx, int ncy, int* cell_count, int* cell_start, int* cell_fill,
                              int* cell_dirty, int* items, int* nudge_vol, double* tempreadint,

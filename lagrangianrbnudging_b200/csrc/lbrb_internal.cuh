@@ -182,6 +182,7 @@ struct Handle {
   size_t slab_tab_bytes = 0;
   std::vector<const void*> slab_sig;
   cudaEvent_t slab_ev_part = nullptr;
+  const double* slab_obs = nullptr;  // bilinear observations of the step just taken (lbrb_slab_step applies them)
   // CUDA graphs of plain steps, one per buffer phase (cur * 9 + uvcur * 3 +
   // uvprev); graph_mode -1: small grids only, 0: off, 1: on
   cudaGraphExec_t graph_exec[18] = {};

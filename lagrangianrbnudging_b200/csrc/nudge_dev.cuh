@@ -26,22 +26,27 @@ __device__ __forceinline__ void obs_cell(double xx, double yy, int nx, int ny, i
   jy2 = y1 % ny; if (jy2 < 0) jy2 += ny;
 }
 
-template <typename Real>
-__device__ __forceinline__ void obs_scatter_one(const Real* __restrict__ T, int nx, int ny, int pitch,
-                                                double xx, double yy, double Tobs, double alpha,
-                                                unsigned long long* __restrict__ acc,
-                                                unsigned* dflags) {
+// Innovation of one observation, scattered to those of its 4 cell corners
+// whose rows lie in [j0, j0 + nyl) of the accumulator (a whole domain: j0 =
+// 0, nyl = ny; a y-slab: its own rows, indexed from j0).  Tat(j, i) is the
+// temperature at global row j, column i.
+template <typename TAt>
+__device__ __forceinline__ void obs_scatter_rows(TAt Tat, int nx, int ny, int pitch, double xx, double yy,
+                                                 double Tobs, double alpha, unsigned long long* __restrict__ acc,
+                                                 unsigned* dflags, int j0, int nyl) {
   if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) {
     atomicOr(dflags, DFLAG_RANGE);
     return;
   }
   int x1, y1, ix1, ix2, jy1, jy2;
   obs_cell(xx, yy, nx, ny, x1, y1, ix1, ix2, jy1, jy2);
+  const bool in1 = (unsigned)(jy1 - j0) < (unsigned)nyl, in2 = (unsigned)(jy2 - j0) < (unsigned)nyl;
+  if (!in1 && !in2) return;
   const int x2 = x1 + 1, y2 = y1 + 1;
-  const double u11 = (double)T[(size_t)jy1 * pitch + ix1];
-  const double u12 = (double)T[(size_t)jy2 * pitch + ix1];
-  const double u21 = (double)T[(size_t)jy1 * pitch + ix2];
-  const double u22 = (double)T[(size_t)jy2 * pitch + ix2];
+  const double u11 = (double)Tat(jy1, ix1);
+  const double u12 = (double)Tat(jy2, ix1);
+  const double u21 = (double)Tat(jy1, ix2);
+  const double u22 = (double)Tat(jy2, ix2);
   const double val1 = u11 * ((double)x2 - xx) * ((double)y2 - yy);
   const double val2 = u21 * (xx - (double)x1) * ((double)y2 - yy);
   const double val3 = u12 * ((double)x2 - xx) * (yy - (double)y1);
@@ -50,22 +55,39 @@ __device__ __forceinline__ void obs_scatter_one(const Real* __restrict__ T, int 
   const double dlt = alpha * (Tobs - tm);
   const double wx1 = (double)x2 - xx, wx2 = xx - (double)x1;
   const double wy1 = (double)y2 - yy, wy2 = yy - (double)y1;
-  atomicAdd(&acc[(size_t)jy1 * pitch + ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy1) * FIX_SCALE));
-  atomicAdd(&acc[(size_t)jy1 * pitch + ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy1) * FIX_SCALE));
-  atomicAdd(&acc[(size_t)jy2 * pitch + ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy2) * FIX_SCALE));
-  atomicAdd(&acc[(size_t)jy2 * pitch + ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy2) * FIX_SCALE));
+  if (in1) {
+    unsigned long long* r = acc + (size_t)(jy1 - j0) * pitch;
+    atomicAdd(&r[ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy1) * FIX_SCALE));
+    atomicAdd(&r[ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy1) * FIX_SCALE));
+  }
+  if (in2) {
+    unsigned long long* r = acc + (size_t)(jy2 - j0) * pitch;
+    atomicAdd(&r[ix1], (unsigned long long)__double2ll_rn(dlt * (wx1 * wy2) * FIX_SCALE));
+    atomicAdd(&r[ix2], (unsigned long long)__double2ll_rn(dlt * (wx2 * wy2) * FIX_SCALE));
+  }
 }
 
-// corner `corner` (0..3) of the observation at (xx, yy)
+template <typename Real>
+__device__ __forceinline__ void obs_scatter_one(const Real* __restrict__ T, int nx, int ny, int pitch,
+                                                double xx, double yy, double Tobs, double alpha,
+                                                unsigned long long* __restrict__ acc,
+                                                unsigned* dflags) {
+  obs_scatter_rows([&](int j, int i) { return T[(size_t)j * pitch + i]; }, nx, ny, pitch, xx, yy, Tobs, alpha,
+                   acc, dflags, 0, ny);
+}
+
+// corner `corner` (0..3) of the observation at (xx, yy), when its row lies
+// in [j0, j0 + nyl) (rows of g and acc indexed from j0)
 template <typename Real>
 __device__ __forceinline__ void obs_apply_one(Real* __restrict__ g, size_t plane, int nx, int ny,
                                               int pitch, double xx, double yy, int corner,
-                                              unsigned long long* __restrict__ acc) {
+                                              unsigned long long* __restrict__ acc, int j0 = 0, int nyl = -1) {
   if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
   const int x1 = (int)xx + (corner & 1), y1 = (int)yy + (corner >> 1);
   int ix = (x1 - 1) % nx; if (ix < 0) ix += nx;
   int jy = (y1 - 1) % ny; if (jy < 0) jy += ny;
-  const size_t q = (size_t)jy * pitch + ix;
+  if (nyl >= 0 && (unsigned)(jy - j0) >= (unsigned)nyl) return;
+  const size_t q = (size_t)(jy - j0) * pitch + ix;
   const long long sfix = (long long)atomicExch(&acc[q], 0ull);
   if (sfix == 0) return;
   const double sv = (double)sfix * (1.0 / FIX_SCALE);

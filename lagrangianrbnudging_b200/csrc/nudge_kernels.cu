@@ -291,6 +291,49 @@ __global__ void obs_apply_kernel(Real* __restrict__ g, size_t plane, int nx, int
   obs_apply_one(g, plane, nx, ny, pitch, ox[p], oy[p], t & 3, acc);
 }
 
+// y-slab: the observations' innovations read T of the whole domain through
+// a table of row pointers (one per global row); the slab scatters to and
+// applies at the corners in its own rows only
+template <typename Real>
+__global__ void obs_scatter_slab_kernel(const Real* const* __restrict__ Trow, int nx, int ny_total, int pitch,
+                                        const double* __restrict__ ox, const double* __restrict__ oy,
+                                        const double* __restrict__ oT, int nobs, double alpha,
+                                        unsigned long long* __restrict__ acc, unsigned* dflags, int j0, int nyl) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nobs) return;
+  obs_scatter_rows([&](int j, int i) { return Trow[j][i]; }, nx, ny_total, pitch, ox[p], oy[p], oT[p], alpha, acc,
+                   dflags, j0, nyl);
+}
+
+template <typename Real>
+__global__ void obs_apply_slab_kernel(Real* __restrict__ g, size_t plane, int nx, int ny_total, int pitch,
+                                      const double* __restrict__ ox, const double* __restrict__ oy, int nobs,
+                                      unsigned long long* __restrict__ acc, int j0, int nyl) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 4 * nobs) return;
+  const int p = t >> 2;
+  obs_apply_one(g, plane, nx, ny_total, pitch, ox[p], oy[p], t & 3, acc, j0, nyl);
+}
+
+cudaError_t launch_bilinear_nudge_slab(const void* Trows, void* g, bool fp32, size_t plane, int nx, int ny_total,
+                                       int j0, int nyl, int pitch, const double* ox, const double* oy,
+                                       const double* oT, int nobs, double alpha, long long* acc, unsigned* dflags,
+                                       cudaStream_t s) {
+  if (nobs <= 0) return cudaSuccess;
+  const int tb = 128;
+  unsigned long long* a = reinterpret_cast<unsigned long long*>(acc);
+  auto go = [&](auto zero) {
+    using Real = decltype(zero);
+    obs_scatter_slab_kernel<Real><<<(nobs + tb - 1) / tb, tb, 0, s>>>(
+        (const Real* const*)Trows, nx, ny_total, pitch, ox, oy, oT, nobs, alpha, a, dflags, j0, nyl);
+    obs_apply_slab_kernel<Real><<<(4 * nobs + tb - 1) / tb, tb, 0, s>>>((Real*)g, plane, nx, ny_total, pitch, ox,
+                                                                       oy, nobs, a, j0, nyl);
+  };
+  if (fp32) go(0.f);
+  else go(0.0);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_bilinear_nudge(void* T, void* g, bool fp32, size_t plane, int nx, int ny,
                                   int pitch, const double* ox, const double* oy, const double* oT,
                                   int nobs, double alpha, long long* acc, unsigned* dflags,

@@ -1,7 +1,7 @@
 """One domain cut into y-slabs (lbrb_slab_set / lbrb_slab_step): the slabs
 advance exactly as the whole domain in one handle, bit for bit, in both
-precisions and with uneven slab heights, particles and their records
-included; the slabs' initial state is the whole domain's; the
+precisions and with uneven slab heights, particles, their records and
+bilinear nudging included; the slabs' initial state is the whole domain's; the
 height-weighted Nu is the whole domain's.  On one GPU the
 slabs are handles on the same device: the exchange is the same peer copy as
 across GPUs (cudaMemcpyPeerAsync), ordered by the same events."""
@@ -79,6 +79,9 @@ def test_slab_mode_rejects_what_it_does_not_cover():
     with lb.Run(**dict(params("fp32"), ny=24, twall="adiabatic")) as r:
         with pytest.raises(lb.LbrbError):
             r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # adiabatic walls are not covered
+    with lb.Run(**dict(params("fp64"), ny=24, nudge="refbox", nobs=4, ntempread=10)) as r:
+        with pytest.raises(lb.LbrbError):
+            r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # box nudging is not covered
     with lb.Run(**dict(params("fp32"), ny=24, nprtcl=8)) as r:
         r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))
         r.init_conduction(1, 1e-3)
@@ -158,3 +161,49 @@ def test_slab_particle_record_ring_overflow_is_reported():
         assert list(steps) == [2, 4]
         dom.step(2)
         assert dom.pending_records() == 1
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("npart", [0, 120])
+def test_slab_bilinear_nudging_matches_the_whole_domain(precision, npart):
+    """observations cycling over 5 steps, cells straddling the inner
+    boundaries among them; with and without particles"""
+    nobs, nst = 90, 5
+    rng = np.random.default_rng(31)
+    ox = rng.uniform(0.0, NX + 1.0, (nst, nobs))
+    oy = rng.uniform(0.5, NY + 0.5, (nst, nobs))
+    oy[:, :8] = [19.5, 20.0, 20.5, 21.0, 36.2, 37.0, 37.9, 0.7]  # cells across the slab edges and the wall
+    oT = rng.uniform(-0.5, 0.5, (nst, nobs))
+    kw = dict(params(precision), nudge="bilinear", alpha=0.3, nobs=nobs, obs_cycle=1, nprtcl=npart,
+              noutconfig=5 if npart else 0, record_slots=64)
+    with lb.Run(**kw) as whole, lb.SlabDomain((20, 17, 11), **kw) as dom:
+        for d in (whole, dom):
+            d.init_conduction(41, 2e-2)
+            d.nudge_obs(1, ox, oy, oT)
+            if npart:
+                seed_particles(d, npart, 8)
+        for n in (1, 4, 60):
+            whole.step(n)
+            dom.step(n)
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+            mw, ms = whole.get_moments(), dom.get_moments()
+            for k in ("rho", "u", "v", "T"):
+                np.testing.assert_array_equal(ms[k], mw[k])
+            if npart:
+                pw, ps = whole.get_particles(), dom.get_particles()
+                for k in pw:
+                    np.testing.assert_array_equal(ps[k], pw[k])
+                sw, rw = whole.drain_records_array()
+                ss, rs = dom.drain_records_array()
+                np.testing.assert_array_equal(ss, sw)
+                np.testing.assert_array_equal(rs, rw)
+        # the nudging did act: without it the state differs
+        with lb.Run(**dict(kw, nudge="none", nobs=0)) as free:
+            free.init_conduction(41, 2e-2)
+            if npart:
+                seed_particles(free, npart, 8)
+            free.step(65)
+            assert not np.array_equal(free.get_moments()["T"], mw["T"])
