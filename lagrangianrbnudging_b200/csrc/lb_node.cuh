@@ -58,8 +58,8 @@ __device__ __forceinline__ void node_ref(const LBView<double>& V, size_t idx, do
   static_for<NPOP>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     double source = (1.0 - 0.5 * omega) * w_of(k);
-    double factor = ((dcx(k) - u) * Fx + (dcy(k) - v) * Fy) / CS2;
-    factor = factor + ((dcx(k) * u + dcy(k) * v) * (dcx(k) * Fx + dcy(k) * Fy)) / (CS2 * CS2);
+    double factor = div_const((dcx(k) - u) * Fx + (dcy(k) - v) * Fy, CS2, RCP_CS2);
+    factor = factor + div_const((dcx(k) * u + dcy(k) * v) * (dcx(k) * Fx + dcy(k) * Fy), DIV_CS4, RCP_CS4);
     fs[k] = fs[k] * (1. - omega) + omega * feq[k] + source * factor;
     store_f(k, fs[k]);
   });

@@ -82,17 +82,38 @@ inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t s
 // (rho, u, v, T; the next step's adjoint linearises around them)
 constexpr int SLOT_F = 2 * NPOP, SLOT_MOM = 2 * NPOP + 1, SLOT_PLANES = 2 * NPOP + 5;
 
+// x / c for a divisor c fixed at compile time, equal to the IEEE quotient
+// RN(x / c) without a division: with rc = RN(1 / c), q0 = RN(x rc) is within
+// one ulp of x / c, the remainder r = x - q0 c is exact in one fused
+// multiply-add, and RN(q0 + r rc) is RN(x / c) (Markstein's correction step,
+// P. Markstein, IBM J. Res. Dev. 34(1), 1990, the basis of correctly rounded
+// division on fused multiply-add hardware).  Holds for quotients in the
+// normal range, which the state's values are far from leaving; r == 0 means
+// q0 is exact (and keeps the sign of a zero x).  tests/test_div_const.py
+// checks it against exact rational quotients, including binade edges.
+__device__ __forceinline__ double div_const(double x, double c, double rc) {
+  const double q0 = __dmul_rn(x, rc);
+  const double r = __fma_rn(-q0, c, x);
+  return r == 0.0 ? q0 : __fma_rn(r, rc, q0);
+}
+// the reference's divisors and their rounded reciprocals
+constexpr double DIV_2CS2 = 2. * CS2, RCP_2CS2 = 1. / (2. * CS2);
+constexpr double RCP_CS2 = 1. / CS2;
+constexpr double DIV_2_9 = 2. / 9., RCP_2_9 = 1. / (2. / 9.);
+constexpr double DIV_CS4 = CS2 * CS2, RCP_CS4 = 1. / (CS2 * CS2);
+
 // equilif / equilig in the reference's operation order
-// (temppart_dump.c:1097-1180): r1 is rho for f and T for g.
+// (temppart_dump.c:1097-1180): r1 is rho for f and T for g; the divisions by
+// lattice constants go through div_const (the same quotients)
 __device__ __forceinline__ void equil_ref(double r1, double u, double v, double feq[NPOP]) {
   double usq = u * u;
   double vsq = v * v;
-  double sumsq = (usq + vsq) / (2. * CS2);
-  double sumsq2 = sumsq * (1. - CS2) / CS2;
-  double u2 = usq / (2. / 9.);
-  double v2 = vsq / (2. / 9.);
-  double ui = u / CS2;
-  double vi = v / CS2;
+  double sumsq = div_const(usq + vsq, DIV_2CS2, RCP_2CS2);
+  double sumsq2 = div_const(sumsq * (1. - CS2), CS2, RCP_CS2);
+  double u2 = div_const(usq, DIV_2_9, RCP_2_9);
+  double v2 = div_const(vsq, DIV_2_9, RCP_2_9);
+  double ui = div_const(u, CS2, RCP_CS2);
+  double vi = div_const(v, CS2, RCP_CS2);
   double uv = ui * vi;
   feq[0] = r1 * w_of(0) * (1. - sumsq);
   feq[1] = r1 * w_of(1) * (1. - sumsq + u2 + ui);
