@@ -230,17 +230,12 @@ __device__ __forceinline__ void dirichlet_walls(const LBView<Real>& V, int j, Re
 }
 
 
-// one node of one step: pull (walls applied), moments, collision, stores
-// FAST: interior rows take the pull without wall logic (else every row takes
-// the general pull)
-template <typename Real, int TWALL, bool REFNUDGE, typename Off = size_t, bool FAST = true>
-__device__ __forceinline__ void lb_update_node(const LBView<Real>& V, int j, int x) {
-  Real fs[NPOP], gs[NPOP];
-  pull_node<Real, TWALL, Off, FAST>(V, j, x, fs, gs);
-  if (TWALL == LBRB_TWALL_DIRICHLET) dirichlet_walls(V, j, gs);
+// moments, collision and stores of node o from its pulled populations and
+// this step's buoyancy Fy
+template <typename Real, bool REFNUDGE, typename Off>
+__device__ __forceinline__ void lb_finish_node(const LBView<Real>& V, Off o, Real* fs, Real* gs, Real Fy) {
   const Off pl = (Off)V.plane;
-  const Off o = (Off)j * (Off)V.pitch + (Off)x;
-  Real Fy = V.Fin[o], r, u, v, t;
+  Real r, u, v, t;
   if constexpr (std::is_same<Real, double>::value) {
     node_ref<REFNUDGE>(
         V, (size_t)o, fs, gs, Fy, r, u, v, t,
@@ -263,6 +258,18 @@ __device__ __forceinline__ void lb_update_node(const LBView<Real>& V, int j, int
     V.rho[o] = r;
     V.T[o] = t;
   }
+}
+
+// one node of one step: pull (walls applied), moments, collision, stores
+// FAST: interior rows take the pull without wall logic (else every row takes
+// the general pull)
+template <typename Real, int TWALL, bool REFNUDGE, typename Off = size_t, bool FAST = true>
+__device__ __forceinline__ void lb_update_node(const LBView<Real>& V, int j, int x) {
+  Real fs[NPOP], gs[NPOP];
+  pull_node<Real, TWALL, Off, FAST>(V, j, x, fs, gs);
+  if (TWALL == LBRB_TWALL_DIRICHLET) dirichlet_walls(V, j, gs);
+  const Off o = (Off)j * (Off)V.pitch + (Off)x;
+  lb_finish_node<Real, REFNUDGE, Off>(V, o, fs, gs, V.Fin[o]);
 }
 
 }  // namespace lbrb
