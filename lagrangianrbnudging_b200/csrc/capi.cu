@@ -549,7 +549,7 @@ static constexpr bool kParticleStream = false;
 // slot's moment planes
 template <typename Real>
 static LBView<Real> seg_view(lbrb_t* h, const char* src, char* dst, int mom) {
-  LBView<Real> V = make_view<Real>(h, 0, 1, h->uvcur, mom, mom);
+  LBView<Real> V = make_view<Real>(h, 0, 1, h->uvcur, mom, mom ? 3 : 0);
   const size_t pl = h->plane;
   const Real* a = (const Real*)src;
   Real* b = (Real*)dst;
@@ -681,7 +681,8 @@ int lbrb_step(lbrb_t* h, int n) {
       if (istep % nt == 1) h->nudge_file_loaded = false;
     }
     const int write_uv = (h->np > 0) || last;
-    const int write_rt = last || rec || h->p.nudge == LBRB_NUDGE_BILINEAR;
+    // T for the records and the nudging scatter; rho only for the call's end
+    const int write_rt = last ? 3 : ((rec || h->p.nudge == LBRB_NUDGE_BILINEAR) ? 1 : 0);
     const int src = h->cur, dst = h->cur ^ 1;
     const int uvn = write_uv ? 3 - h->uvcur - h->uvprev : h->uvcur;
     // buffers read by an earlier particle kernel must be free before rewriting

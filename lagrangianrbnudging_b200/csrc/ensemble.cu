@@ -79,7 +79,7 @@ struct StepBufs {
 StepBufs step_bufs(const lbrb_t* h, MState& s, bool last) {
   StepBufs b;
   b.write_uv = (h->np > 0) || last;
-  b.write_rt = last || h->p.nudge == LBRB_NUDGE_BILINEAR;
+  b.write_rt = last ? 3 : (h->p.nudge == LBRB_NUDGE_BILINEAR ? 1 : 0);  // (as lbrb_step)
   b.src = s.cur;
   b.dst = s.cur ^ 1;
   b.uvn = b.write_uv ? 3 - s.uvcur - s.uvprev : s.uvcur;

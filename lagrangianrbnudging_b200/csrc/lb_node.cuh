@@ -254,10 +254,8 @@ __device__ __forceinline__ void lb_finish_node(const LBView<Real>& V, Off o, Rea
     V.u[o] = u;
     V.v[o] = v;
   }
-  if (V.write_rt) {
-    V.rho[o] = r;
-    V.T[o] = t;
-  }
+  if (V.write_rt & 1) V.T[o] = t;
+  if (V.write_rt & 2) V.rho[o] = r;
 }
 
 // one node of one step: pull (walls applied), moments, collision, stores

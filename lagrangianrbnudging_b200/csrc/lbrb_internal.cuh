@@ -157,7 +157,8 @@ struct LBView {
   const double* __restrict__ tempreadint;
   double* __restrict__ nud_term;
   double alpha;
-  int write_uv, write_rt;
+  int write_uv;
+  int write_rt;  // bit 0: store T (records, nudging), bit 1: also rho (a call's last step)
   // y-slab of a larger domain: the rows below row 0 / above row ny-1 (the
   // neighbour slab's boundary row after its collision), 6 rows of nx values:
   // f then g of the three populations crossing the boundary; null = wall
