@@ -704,7 +704,7 @@ int lbrb_step(lbrb_t* h, int n) {
       const int tm = tmark_begin(h, 2, h->stream);
       CK(h, launch_bilinear_nudge(h->T[dst], pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, obs,
                                   obs + h->nobs, obs + 2 * (size_t)h->nobs, h->nobs, h->p.alpha,
-                                  h->acc, h->dflags, h->stream));
+                                  h->acc, h->dflags, h->stream, pdl_ok));
       tmark_end(h, tm, h->stream);
     }
     if (h->np > 0 && !h->slab) {  // (y-slabs: lbrb_slab_step moves the particles)

@@ -52,7 +52,7 @@ cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt
 cudaError_t launch_bilinear_nudge(void* T, void* g, bool fp32, size_t plane, int nx, int ny,
                                   int pitch, const double* ox, const double* oy, const double* oT,
                                   int nobs, double alpha, long long* acc, unsigned* dflags,
-                                  cudaStream_t s);
+                                  cudaStream_t s, bool pdl = false);
 cudaError_t launch_pops_in(const double* h, int layout, void* d, bool fp32, int nx, int ny,
                            int pitch, size_t plane, double base, cudaStream_t s);
 cudaError_t launch_pops_out(const void* d, int layout, double* h, bool fp32, int nx, int ny,

@@ -17,6 +17,9 @@
 // ctr[0] counts the steps of the current lbrb_ensemble_step call (phase A's
 // first block increments it; B and C read it to pick observation rows);
 // ctr[1] is the dynamic schedule's tile counter (cleared by phase B).
+// The three kernels are launched with programmatic dependent launch (also
+// inside the ensemble's CUDA graph) and wait for the previous phase before
+// touching memory, so each launch overlaps only the previous one's drain.
 #include "capi_internal.cuh"
 #include "ensemble.cuh"
 #include "lb_node.cuh"
@@ -31,6 +34,7 @@ __global__ void __launch_bounds__(BS, MINB)
                   int* __restrict__ ctr) {
   __shared__ LBView<Real> sV;
   __shared__ int s_item[2];
+  pdl_wait();
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ctr[0], 1);
   constexpr int WORDS = (int)(sizeof(LBView<Real>) / sizeof(int));
   static_assert(sizeof(LBView<Real>) % sizeof(int) == 0, "view size");
@@ -71,6 +75,7 @@ template <typename Real>
 __global__ void __launch_bounds__(128)
     ens_aux_kernel(const EnsAux<Real>* __restrict__ aux, const int2* __restrict__ pchunks, int npchunks,
                    const int2* __restrict__ ochunks, int nochunks, int* __restrict__ ctr) {
+  pdl_wait();
   if (blockIdx.x == 0 && threadIdx.x == 0) ctr[1] = 0;
   int b = blockIdx.x;
   if (b < npchunks) {
@@ -97,6 +102,7 @@ template <typename Real>
 __global__ void __launch_bounds__(512)
     ens_apply_kernel(const EnsAux<Real>* __restrict__ aux, const int2* __restrict__ ochunks,
                      const int* __restrict__ ctr) {
+  pdl_wait();
   const int2 c = ochunks[blockIdx.x];
   const EnsAux<Real>& A = aux[c.x];
   const int o = c.y + (threadIdx.x >> 2);
@@ -124,8 +130,7 @@ static cudaError_t ens_lb_launch(const LBView<Real>* views, const int4* items, i
     grid = std::max(1, std::min(nitems, per * nsm));
   }
   if (nitems <= 0) return cudaSuccess;
-  k<<<grid, BS, 0, s>>>(views, items, nitems, ctr);
-  return cudaGetLastError();
+  return launch_k(k, grid, BS, 0, s, true, views, items, nitems, ctr);
 }
 
 // (threads per tile row, rows per tile, schedule, min blocks per SM, pull
@@ -186,20 +191,17 @@ cudaError_t launch_ens_aux(bool f32, const void* aux, const int2* pchunks, int n
                            const int2* ochunks, int nochunks, int* ctr, cudaStream_t s) {
   const int grid = std::max(1, npchunks + nochunks);
   if (f32)
-    ens_aux_kernel<float><<<grid, 128, 0, s>>>((const EnsAux<float>*)aux, pchunks, npchunks, ochunks, nochunks, ctr);
-  else
-    ens_aux_kernel<double><<<grid, 128, 0, s>>>((const EnsAux<double>*)aux, pchunks, npchunks, ochunks, nochunks, ctr);
-  return cudaGetLastError();
+    return launch_k(ens_aux_kernel<float>, grid, 128, 0, s, true, (const EnsAux<float>*)aux, pchunks, npchunks,
+                    ochunks, nochunks, ctr);
+  return launch_k(ens_aux_kernel<double>, grid, 128, 0, s, true, (const EnsAux<double>*)aux, pchunks, npchunks,
+                  ochunks, nochunks, ctr);
 }
 
 cudaError_t launch_ens_apply(bool f32, const void* aux, const int2* ochunks, int nochunks, const int* ctr,
                              cudaStream_t s) {
   if (nochunks <= 0) return cudaSuccess;
-  if (f32)
-    ens_apply_kernel<float><<<nochunks, 512, 0, s>>>((const EnsAux<float>*)aux, ochunks, ctr);
-  else
-    ens_apply_kernel<double><<<nochunks, 512, 0, s>>>((const EnsAux<double>*)aux, ochunks, ctr);
-  return cudaGetLastError();
+  if (f32) return launch_k(ens_apply_kernel<float>, nochunks, 512, 0, s, true, (const EnsAux<float>*)aux, ochunks, ctr);
+  return launch_k(ens_apply_kernel<double>, nochunks, 512, 0, s, true, (const EnsAux<double>*)aux, ochunks, ctr);
 }
 
 }  // namespace lbrb

@@ -276,6 +276,7 @@ __global__ void obs_scatter_kernel(const Real* __restrict__ T, int nx, int ny, i
                                    const double* __restrict__ ox, const double* __restrict__ oy,
                                    const double* __restrict__ oT, int nobs, double alpha,
                                    unsigned long long* __restrict__ acc, unsigned* dflags) {
+  pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nobs) return;
   obs_scatter_one(T, nx, ny, pitch, ox[p], oy[p], oT[p], alpha, acc, dflags);
@@ -285,6 +286,7 @@ template <typename Real>
 __global__ void obs_apply_kernel(Real* __restrict__ g, size_t plane, int nx, int ny, int pitch,
                                  const double* __restrict__ ox, const double* __restrict__ oy,
                                  int nobs, unsigned long long* __restrict__ acc) {
+  pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 4 * nobs) return;
   const int p = t >> 2;
@@ -337,22 +339,19 @@ cudaError_t launch_bilinear_nudge_slab(const void* Trows, void* g, bool fp32, si
 cudaError_t launch_bilinear_nudge(void* T, void* g, bool fp32, size_t plane, int nx, int ny,
                                   int pitch, const double* ox, const double* oy, const double* oT,
                                   int nobs, double alpha, long long* acc, unsigned* dflags,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, bool pdl) {
   if (nobs <= 0) return cudaSuccess;
   const int tb = 128;
   unsigned long long* a = reinterpret_cast<unsigned long long*>(acc);
-  if (fp32) {
-    obs_scatter_kernel<float><<<(nobs + tb - 1) / tb, tb, 0, s>>>((const float*)T, nx, ny, pitch,
-                                                                 ox, oy, oT, nobs, alpha, a, dflags);
-    obs_apply_kernel<float><<<(4 * nobs + tb - 1) / tb, tb, 0, s>>>((float*)g, plane, nx, ny,
-                                                                   pitch, ox, oy, nobs, a);
-  } else {
-    obs_scatter_kernel<double><<<(nobs + tb - 1) / tb, tb, 0, s>>>((const double*)T, nx, ny, pitch,
-                                                                  ox, oy, oT, nobs, alpha, a, dflags);
-    obs_apply_kernel<double><<<(4 * nobs + tb - 1) / tb, tb, 0, s>>>((double*)g, plane, nx, ny,
-                                                                    pitch, ox, oy, nobs, a);
-  }
-  return cudaGetLastError();
+  auto go = [&](auto zero) -> cudaError_t {
+    using Real = decltype(zero);
+    cudaError_t e = launch_k(obs_scatter_kernel<Real>, (nobs + tb - 1) / tb, tb, 0, s, pdl, (const Real*)T, nx, ny,
+                             pitch, ox, oy, oT, nobs, alpha, a, dflags);
+    if (e != cudaSuccess) return e;
+    return launch_k(obs_apply_kernel<Real>, (4 * nobs + tb - 1) / tb, tb, 0, s, pdl, (Real*)g, plane, nx, ny, pitch,
+                    ox, oy, nobs, a);
+  };
+  return fp32 ? go(0.f) : go(0.0);
 }
 
 }  // namespace lbrb
