@@ -166,6 +166,23 @@ LBRB_API int lbrb_set_stream(lbrb_t *h, void *cuda_stream);
  * per-kernel timing, a y-slab, the legacy default stream, or while the
  * caller captures the handle's stream.  No counterpart in the reference. */
 LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
+/* Two steps per launch inside lbrb_step: the fused kernel computes step n
+ * at a tile and a one-node ring into shared memory and step n+1 from there,
+ * so populations and F cross HBM once per two steps (u, v, and T on record
+ * steps, are still stored for every step; the particle kernels run after
+ * the launch for each step).  Results are identical to single steps.
+ * -1 (the default) and 1: pairs of steps that do not replay graphs; 0: off.
+ * Used with Dirichlet walls, without nudging, not on a y-slab, and never for
+ * the last step of a call (so lbrb_get_poststream keeps its meaning).
+ * The tile shape is timed on first use; lbrb_get_pair_shape reports it
+ * (shape index, tile columns and rows, ms per launch; shape -1 before).
+ * Replaces, for two steps at a time, the reference's per-step sweeps
+ * (stream, moments, collide: temppart_dump.c:1674-1759). */
+LBRB_API int lbrb_set_pairs(lbrb_t *h, int mode);
+/* fix the tile shape (0: 32x8, 1: 32x4, 2: 32x16, 3: 64x4) instead of timing
+ * the shapes on first use (-1) */
+LBRB_API int lbrb_set_pair_shape(lbrb_t *h, int shape);
+LBRB_API int lbrb_get_pair_shape(const lbrb_t *h, int *shape, int *tile_x, int *tile_y, float *ms);
 /* Per-kernel device timing with CUDA events around each launch.  Classes:
  * 0 fused stream/collide, 1 particles, 2 nudging, 3 record copies.
  * lbrb_get_timing() waits, returns total milliseconds and launch counts per

@@ -45,7 +45,7 @@ EXPORTS = [
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
-    "lbrb_set_graph",
+    "lbrb_set_graph", "lbrb_set_pairs", "lbrb_set_pair_shape", "lbrb_get_pair_shape",
 ]
 
 
@@ -136,6 +136,9 @@ def lib() -> C.CDLL:
         "lbrb_slab_pack": (C.c_int, [vp]),
         "lbrb_slab_step": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int]),
         "lbrb_set_graph": (C.c_int, [vp, C.c_int]),
+        "lbrb_set_pairs": (C.c_int, [vp, C.c_int]),
+        "lbrb_set_pair_shape": (C.c_int, [vp, C.c_int]),
+        "lbrb_get_pair_shape": (C.c_int, [vp, ip, ip, ip, C.POINTER(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -371,6 +374,19 @@ class Run:
     def set_graph(self, mode: int):
         """CUDA-graph replay of plain steps: -1 small grids (default), 0 off, 1 on"""
         self._ck(lib().lbrb_set_graph(self.h, int(mode)))
+
+    def set_pairs(self, mode: int):
+        """two steps per fused launch: -1 (default) and 1 where eligible, 0 off"""
+        self._ck(lib().lbrb_set_pairs(self.h, int(mode)))
+
+    def set_pair_shape(self, shape: int):
+        """fixed tile shape of the two-step launch (0..3), or -1: timed on first use"""
+        self._ck(lib().lbrb_set_pair_shape(self.h, int(shape)))
+
+    def pair_shape(self):
+        sh, tx, ty, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        self._ck(lib().lbrb_get_pair_shape(self.h, C.byref(sh), C.byref(tx), C.byref(ty), C.byref(ms)))
+        return {"shape": sh.value, "tile": [tx.value, ty.value], "tuned_ms": ms.value}
 
     def set_timing(self, enable: bool):
         self._ck(lib().lbrb_set_timing(self.h, int(bool(enable))))

@@ -620,6 +620,13 @@ static bool graph_ok(const lbrb_t* h) {
          h->stream != nullptr && h->p.nudge == LBRB_NUDGE_NONE && !h->timing && !kParticleStream && !h->slab;
 }
 
+// two steps per launch: Dirichlet walls, no nudging (it acts between the
+// steps), not a y-slab (ghost rows are exchanged every step)
+static bool pairs_ok(const lbrb_t* h) {
+  return h->pair_mode != 0 && h->p.twall == LBRB_TWALL_DIRICHLET && h->p.nudge == LBRB_NUDGE_NONE && !h->slab &&
+         !kParticleStream;
+}
+
 int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
@@ -651,6 +658,22 @@ int lbrb_step(lbrb_t* h, int n) {
     h->lb_shape = sh;
     h->lb_shape_ms = ms;
   }
+  // the record of step istep in ring slot `slot`, written by a particle
+  // kernel on stream ps: copied to the host ring on the copy stream
+  auto record_copy = [&](int istep, int slot, double* rslot, cudaStream_t ps) -> int {
+    h->h_ring_step[slot] = istep;
+    CK(h, cudaEventRecord(h->ring_ev[slot], ps));
+    CK(h, cudaStreamWaitEvent(h->copy_stream, h->ring_ev[slot], 0));
+    const size_t per = (size_t)h->nrec_fields * h->np;
+    const int tc = tmark_begin(h, 3, h->copy_stream);
+    CK(h, cudaMemcpyAsync(h->h_ring + (size_t)slot * per, rslot, per * sizeof(double), cudaMemcpyDeviceToHost,
+                          h->copy_stream));
+    tmark_end(h, tc, h->copy_stream);
+    CK(h, cudaEventRecord(h->ring_ev[slot], h->copy_stream));
+    h->rec_head++;
+    h->join_pending = true;
+    return LBRB_OK;
+  };
   bool pt_queued = false;
   // one step's launches; `last` writes the moments
   const bool pdl_ok = !h->timing;  // (per-kernel timing keeps plain launches)
@@ -730,17 +753,8 @@ int lbrb_step(lbrb_t* h, int n) {
         pt_queued = true;
       }
       if (rec) {
-        h->h_ring_step[slot] = istep;
-        CK(h, cudaEventRecord(h->ring_ev[slot], ps));
-        CK(h, cudaStreamWaitEvent(h->copy_stream, h->ring_ev[slot], 0));
-        const size_t per = (size_t)h->nrec_fields * h->np;
-        const int tc = tmark_begin(h, 3, h->copy_stream);
-        CK(h, cudaMemcpyAsync(h->h_ring + (size_t)slot * per, rslot, per * sizeof(double),
-                              cudaMemcpyDeviceToHost, h->copy_stream));
-        tmark_end(h, tc, h->copy_stream);
-        CK(h, cudaEventRecord(h->ring_ev[slot], h->copy_stream));
-        h->rec_head++;
-        h->join_pending = true;
+        const int rc = record_copy(istep, slot, rslot, ps);
+        if (rc) return rc;
       }
     }
     h->cur = dst;
@@ -752,6 +766,97 @@ int lbrb_step(lbrb_t* h, int n) {
     h->istep = istep;
     return LBRB_OK;
   };
+  // Two plain steps n, n+1 in one launch (lb_pair_kernel), then the particles
+  // of each.  Step n's T goes to the source buffer T[cur] (its particle
+  // records read it there), step n+1's to T[cur ^ 1]; u, v of step n go to
+  // the free slot and of step n+1 to the slot of u^{n-2}, as two `one` calls
+  // would rotate them.  The intermediate populations stay in shared memory,
+  // so get_poststream needs the call's last step, which is never in a pair.
+  auto two = [&]() -> int {
+    const int i1 = h->istep + 1, i2 = h->istep + 2;
+    const bool parts = h->np > 0;
+    const bool rec1 = parts && h->p.noutconfig > 0 && i1 % h->p.noutconfig == 0;
+    const bool rec2 = parts && h->p.noutconfig > 0 && i2 % h->p.noutconfig == 0;
+    const int src = h->cur, dst = h->cur ^ 1;
+    const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;  // u^n
+    const int B = parts ? h->uvprev : h->uvcur;                 // u^{n+1}
+    const int wuv = parts ? 1 : 0;
+    {
+      const int tm = tmark_begin(h, 0, h->stream);
+      if (f32) {
+        LBView<float> V1 = make_view<float>(h, src, dst, A, wuv, rec1 ? 1 : 0);
+        V1.T = (float*)h->T[src];
+        V1.rho = (float*)h->rho[src];
+        CK(h, launch_pair_fp32(V1, make_view<float>(h, dst, dst, B, wuv, rec2 ? 1 : 0), h->pair_shape, h->stream,
+                               pdl_ok));
+      } else {
+        LBView<double> V1 = make_view<double>(h, src, dst, A, wuv, rec1 ? 1 : 0);
+        V1.T = (double*)h->T[src];
+        V1.rho = (double*)h->rho[src];
+        CK(h, launch_pair_fp64(V1, make_view<double>(h, dst, dst, B, wuv, rec2 ? 1 : 0), h->pair_shape, h->stream,
+                               pdl_ok));
+      }
+      tmark_end(h, tm, h->stream);
+    }
+    if (parts) {
+      const int ubs[2] = {h->uvcur, A}, us[2] = {A, B}, ts[2] = {src, dst}, isteps[2] = {i1, i2};
+      const bool recs[2] = {rec1, rec2};
+      for (int q = 0; q < 2; q++) {
+        const int slot = recs[q] ? (int)(h->rec_head % h->p.record_slots) : 0;
+        double* rslot = recs[q] ? h->d_ring + (size_t)slot * h->nrec_fields * h->np : nullptr;
+        const int tm = tmark_begin(h, 1, h->stream);
+        CK(h, launch_particles(h->uv[us[q]][0], h->uv[us[q]][1], h->uv[ubs[q]][0], h->uv[ubs[q]][1], h->T[ts[q]],
+                               f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta, recs[q] ? 1 : 0,
+                               h->p.record_full, rslot, h->dflags, h->stream, pdl_ok));
+        tmark_end(h, tm, h->stream);
+        if (recs[q]) {
+          const int rc = record_copy(isteps[q], slot, rslot, h->stream);
+          if (rc) return rc;
+        }
+      }
+      h->uvprev = A;
+      h->uvcur = B;
+    }
+    h->cur = dst;
+    h->prev_valid = false;
+    h->istep = i2;
+    return LBRB_OK;
+  };
+  auto tune_pairs = [&]() -> int {
+    const int src = h->cur, dst = h->cur ^ 1;
+    const bool parts = h->np > 0;
+    const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;
+    const int B = parts ? h->uvprev : h->uvcur;
+    const int wuv = parts ? 1 : 0;
+    {
+      float ms = 0.f;
+      int sh = 0;
+      if (f32) {
+        LBView<float> t1 = make_view<float>(h, src, dst, A, wuv, 0), t2 = make_view<float>(h, dst, dst, B, wuv, 0);
+        sh = tune_pair_fp32(t1, t2, h->stream, &ms);
+      } else {
+        LBView<double> t1 = make_view<double>(h, src, dst, A, wuv, 0), t2 = make_view<double>(h, dst, dst, B, wuv, 0);
+        sh = tune_pair_fp64(t1, t2, h->stream, &ms);
+      }
+      CK(h, cudaGetLastError());
+      h->pair_shape = sh;
+      h->pair_ms = ms;
+      // automatic mode keeps pairs only where one beats two tuned single launches
+      if (h->pair_mode < 0 && h->lb_shape_ms > 0.f && ms >= 2.f * h->lb_shape_ms) h->pair_mode = 0;
+    }
+    return LBRB_OK;
+  };
+  bool graphs_on = graph_ok(h);  // (refined below for a caller's capture)
+  if (pairs_ok(h) && h->pair_shape < 0 && n >= 3) {
+    // the pair shape is timed on the first call that can use pairs (trial
+    // launches write only what the steps overwrite)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(h, cudaStreamIsCapturing(h->stream, &cs));
+    if (cs == cudaStreamCaptureStatusNone && !(graphs_on && n - 1 >= GRAPH_STEPS)) {
+      const int rc = tune_pairs();
+      if (rc) return rc;
+    }
+  }
   // Small grids: a run of GRAPH_STEPS plain steps (no record, not the call's
   // last step) replays a CUDA graph of exactly the launches `one` would
   // issue.  Those launches depend only on the buffer phase (cur, uvcur,
@@ -804,6 +909,20 @@ int lbrb_step(lbrb_t* h, int n) {
         h->prev_valid = true;
         h->istep += GRAPH_STEPS;
         s += GRAPH_STEPS;
+        continue;
+      }
+    }
+    if (!graphs && h->pair_shape >= 0 && pairs_ok(h) && n - 1 - s >= 2) {
+      // two steps per launch, never the call's last step; a pair whose
+      // records would not fit in the ring runs as single steps (which report
+      // the overflow at the same step)
+      int need = 0;
+      for (int q = 1; q <= 2; q++)
+        need += h->np > 0 && h->p.noutconfig > 0 && (h->istep + q) % h->p.noutconfig == 0;
+      if (h->rec_head - h->rec_tail + need <= h->p.record_slots) {
+        const int rc = two();
+        if (rc) return rc;
+        s += 2;
         continue;
       }
     }
@@ -1426,6 +1545,30 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
 int lbrb_set_graph(lbrb_t* h, int mode) {
   if (!h || mode < -1 || mode > 1) return fail(h, LBRB_ERR_ARG, "set_graph: mode must be -1, 0 or 1");
   h->graph_mode = mode;
+  return LBRB_OK;
+}
+
+int lbrb_set_pairs(lbrb_t* h, int mode) {
+  if (!h || mode < -1 || mode > 1) return fail(h, LBRB_ERR_ARG, "set_pairs: mode must be -1, 0 or 1");
+  h->pair_mode = mode;
+  return LBRB_OK;
+}
+
+int lbrb_set_pair_shape(lbrb_t* h, int shape) {
+  if (!h || shape < -1 || shape > 3) return fail(h, LBRB_ERR_ARG, "set_pair_shape: shape must be -1 (tune) or 0..3");
+  h->pair_shape = shape;
+  h->pair_ms = 0.f;
+  return LBRB_OK;
+}
+
+int lbrb_get_pair_shape(const lbrb_t* h, int* shape, int* tile_x, int* tile_y, float* ms) {
+  if (!h) return LBRB_ERR_ARG;
+  static const int TXS[] = {32, 32, 32, 64}, TYS[] = {8, 4, 16, 4};  // (lb_kernels.cu: PAIR_SHAPES)
+  const int sh = h->pair_shape;
+  if (shape) *shape = sh;
+  if (tile_x) *tile_x = sh < 0 ? 0 : TXS[sh];
+  if (tile_y) *tile_y = sh < 0 ? 0 : TYS[sh];
+  if (ms) *ms = h->pair_ms;
   return LBRB_OK;
 }
 

@@ -26,6 +26,11 @@ int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best
 cudaError_t launch_pull_fp64(const LBView<double>& V, int twall, void* outf, void* outg, cudaStream_t s);
 cudaError_t launch_pull_fp32(const LBView<float>& V, int twall, void* outf, void* outg, cudaStream_t s);
 int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_ms);
+// two steps per launch (Dirichlet walls, no ghost rows): V1 = step n, V2 = step n+1
+cudaError_t launch_pair_fp32(const LBView<float>& V1, const LBView<float>& V2, int shape, cudaStream_t s, bool pdl);
+cudaError_t launch_pair_fp64(const LBView<double>& V1, const LBView<double>& V2, int shape, cudaStream_t s, bool pdl);
+int tune_pair_fp32(const LBView<float>& V1, const LBView<float>& V2, cudaStream_t s, float* best_ms);
+int tune_pair_fp64(const LBView<double>& V1, const LBView<double>& V2, cudaStream_t s, float* best_ms);
 cudaError_t launch_particles(const void* u, const void* v, const void* ub, const void* vb,
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,
                              const int* ptype, int np, double beta, int record, int full,

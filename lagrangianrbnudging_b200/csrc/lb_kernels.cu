@@ -64,6 +64,111 @@ __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V)
   lb_update_node<Real, TWALL, REFNUDGE, Off, FAST>(V, j, x);
 }
 
+// ------------------------------------------------------- two steps per launch
+// Temporal blocking of two steps n, n+1 (Dirichlet walls, no ghost rows, no
+// nudging in between).  A block owns a TX x TY tile.  Phase 1 computes step n
+// at the tile and a one-node ring around it (x wrapped, rows outside the
+// domain skipped) from HBM, exactly as lb_update_node does, and keeps the
+// post-collision populations in shared memory; at the tile it also stores
+// u^n, v^n (and T^n on a record step) to HBM through V1, and keeps the next
+// buoyancy F^{n+1} in shared memory.  Phase 2 computes step n+1 at the tile,
+// pulling from shared memory with the same wall rules as pull_node (bounce-back
+// from the node's own opposite population, anti-bounce-back for g), and
+// stores through V2.  Populations and F cross HBM once per two steps; the
+// ring is recomputed (34 x 10 nodes for a 32 x 8 tile).  The per-node
+// arithmetic is lb_update_node's, so two steps here equal two launches of
+// lb_node_kernel bit for bit.
+template <typename Real, int TX, int TY, int MINB, typename Off>
+__global__ void __launch_bounds__(TX * TY, MINB) lb_pair_kernel(const LBView<Real> V1, const LBView<Real> V2) {
+  pdl_wait();
+  constexpr int RX = TX + 2, RY = TY + 2, RN = RX * RY;
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  Real* S = reinterpret_cast<Real*>(pair_smem);  // [2 * NPOP][RY][RX]: f then g of step n
+  Real* SF = S + 2 * NPOP * RN;                   // [TY][TX]: F^{n+1} at the tile
+  const int nx = V1.nx, ny = V1.ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int ncols = min(TX, nx - x0), nrows = min(TY, ny - y0);
+  const Off pitch = (Off)V1.pitch;
+  for (int q = threadIdx.x; q < RN; q += TX * TY) {
+    const int lx = q % RX, ly = q / RX;
+    const int jg = y0 - 1 + ly;
+    if (lx > ncols + 1 || ly > nrows + 1 || jg < 0 || jg >= ny) continue;
+    int xg = x0 - 1 + lx;
+    if (xg < 0) xg += nx;
+    else if (xg >= nx) xg -= nx;
+    Real fs[NPOP], gs[NPOP];
+    pull_node<Real, LBRB_TWALL_DIRICHLET, Off, true>(V1, jg, xg, fs, gs);
+    dirichlet_walls(V1, jg, gs);
+    const Off o = (Off)jg * pitch + (Off)xg;
+    Real Fy = V1.Fin[o], r, u, v, t;
+    lb_collide<Real, false>(
+        V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { S[(k * RY + ly) * RX + lx] = val; },
+        [&](int k, Real val) { S[((NPOP + k) * RY + ly) * RX + lx] = val; });
+    if (lx >= 1 && lx <= ncols && ly >= 1 && ly <= nrows) {
+      SF[(ly - 1) * TX + (lx - 1)] = Fy;
+      if (V1.write_uv) {
+        V1.u[o] = u;
+        V1.v[o] = v;
+      }
+      if (V1.write_rt & 1) V1.T[o] = t;
+      if (V1.write_rt & 2) V1.rho[o] = r;
+    }
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  if (tx >= ncols || ty >= nrows) return;
+  const int x = x0 + tx, j = y0 + ty;
+  Real fs[NPOP], gs[NPOP];
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    const int js = j - icy(k);
+    if (js < 0 || js >= ny) {
+      fs[k] = S[(opp(k) * RY + ty + 1) * RX + tx + 1];
+      gs[k] = Real(0);
+    } else {
+      const int lx = tx + 1 - icx(k), ly = ty + 1 - icy(k);
+      fs[k] = S[(k * RY + ly) * RX + lx];
+      gs[k] = S[((NPOP + k) * RY + ly) * RX + lx];
+    }
+  });
+  dirichlet_walls(V2, j, gs);
+  lb_finish_node<Real, false, Off>(V2, (Off)j * pitch + (Off)x, fs, gs, SF[ty * TX + tx]);
+}
+
+// pair launch shapes: (tile columns, tile rows, min blocks per SM)
+struct PairShape { int tx, ty, minb; };
+constexpr PairShape PAIR_SHAPES[] = {{32, 8, 4}, {32, 4, 6}, {32, 16, 2}, {64, 4, 3}};
+constexpr int NPAIR = sizeof(PAIR_SHAPES) / sizeof(PAIR_SHAPES[0]);
+
+template <typename Real, int TX, int TY, int MINB>
+static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2, cudaStream_t s, bool pdl) {
+  const size_t smem = ((size_t)2 * NPOP * (TX + 2) * (TY + 2) + (size_t)TX * TY) * sizeof(Real);
+  dim3 grid((V1.nx + TX - 1) / TX, (V1.ny + TY - 1) / TY);
+  auto go = [&](auto kernel) -> cudaError_t {
+    static bool attr = false;  // (per instantiation)
+    if (!attr) {
+      const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    return launch_k(kernel, grid, TX * TY, smem, s, pdl, V1, V2);
+  };
+  // (FP64 holds twice the registers per value: half the blocks per SM)
+  constexpr int MB = std::is_same<Real, double>::value ? (MINB + 1) / 2 : MINB;
+  if (off32_ok(V1.plane)) return go(lb_pair_kernel<Real, TX, TY, MB, uint32_t>);
+  return go(lb_pair_kernel<Real, TX, TY, MB, size_t>);
+}
+
+template <typename Real>
+static cudaError_t launch_pair(const LBView<Real>& V1, const LBView<Real>& V2, int shape, cudaStream_t s, bool pdl) {
+  switch (shape) {
+    case 1: return launch_pair_t<Real, 32, 4, 6>(V1, V2, s, pdl);
+    case 2: return launch_pair_t<Real, 32, 16, 2>(V1, V2, s, pdl);
+    case 3: return launch_pair_t<Real, 64, 4, 3>(V1, V2, s, pdl);
+    default: return launch_pair_t<Real, 32, 8, 4>(V1, V2, s, pdl);
+  }
+}
+
 // --------------------------------------------------------------- launch
 // launch shapes tried by tune_lb: (threads per block, min blocks per SM,
 // pull form: 1 = interior rows without wall logic and 32-bit offsets where
@@ -177,6 +282,53 @@ int tune_lb_fp64(const LBView<double>& V, int twall, cudaStream_t s, float* best
 }
 int tune_lb_fp32(const LBView<float>& V, int twall, cudaStream_t s, float* best_ms) {
   return tune<float>(V, twall, false, s, tune_reps(V), best_ms);
+}
+
+// two steps per launch: V1 is step n (its pops and F outputs unused), V2 step
+// n+1 (its pop and F inputs unused)
+cudaError_t launch_pair_fp32(const LBView<float>& V1, const LBView<float>& V2, int shape, cudaStream_t s, bool pdl) {
+  return launch_pair<float>(V1, V2, shape, s, pdl);
+}
+cudaError_t launch_pair_fp64(const LBView<double>& V1, const LBView<double>& V2, int shape, cudaStream_t s,
+                             bool pdl) {
+  return launch_pair<double>(V1, V2, shape, s, pdl);
+}
+
+// pair shape autotuner: as tune(), the trial launches write only buffers the
+// real steps overwrite (the views' destinations; no rho or T)
+template <typename Real>
+static int tune_pair(const LBView<Real>& A, const LBView<Real>& B, cudaStream_t s, float* best_ms) {
+  LBView<Real> V1 = A, V2 = B;
+  V1.write_rt = V2.write_rt = 0;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int reps = tune_reps(V1);
+  int best = 0;
+  float bt = 1e30f;
+  for (int sh = 0; sh < NPAIR; sh++) {
+    if (launch_pair<Real>(V1, V2, sh, s, false) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaEventRecord(a, s);
+    for (int r = 0; r < reps; r++) launch_pair<Real>(V1, V2, sh, s, false);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < bt) { bt = ms; best = sh; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (best_ms) *best_ms = bt / reps;
+  return best;
+}
+int tune_pair_fp32(const LBView<float>& V1, const LBView<float>& V2, cudaStream_t s, float* best_ms) {
+  return tune_pair<float>(V1, V2, s, best_ms);
+}
+int tune_pair_fp64(const LBView<double>& V1, const LBView<double>& V2, cudaStream_t s, float* best_ms) {
+  return tune_pair<double>(V1, V2, s, best_ms);
 }
 
 }  // namespace lbrb

@@ -230,25 +230,33 @@ __device__ __forceinline__ void dirichlet_walls(const LBView<Real>& V, int j, Re
 }
 
 
+// moments and collision of a pulled node (idx: its element offset, for the
+// box-nudging fields); SF(k, f_k'), SG(k, g_k') take the post-collision
+// populations and Fy_io becomes the next step's buoyancy
+template <typename Real, bool REFNUDGE, typename SF, typename SG>
+__device__ __forceinline__ void lb_collide(const LBView<Real>& V, size_t idx, Real* fs, Real* gs, Real& Fy_io,
+                                           Real& r, Real& u, Real& v, Real& t, SF&& store_f, SG&& store_g) {
+  if constexpr (std::is_same<Real, double>::value) {
+    node_ref<REFNUDGE>(V, idx, fs, gs, Fy_io, r, u, v, t, store_f, store_g);
+  } else {
+    node_shift(V, fs, gs, Fy_io, r, u, v, t);
+#pragma unroll
+    for (int k = 0; k < NPOP; k++) {
+      store_f(k, fs[k]);
+      store_g(k, gs[k]);
+    }
+  }
+}
+
 // moments, collision and stores of node o from its pulled populations and
 // this step's buoyancy Fy
 template <typename Real, bool REFNUDGE, typename Off>
 __device__ __forceinline__ void lb_finish_node(const LBView<Real>& V, Off o, Real* fs, Real* gs, Real Fy) {
   const Off pl = (Off)V.plane;
   Real r, u, v, t;
-  if constexpr (std::is_same<Real, double>::value) {
-    node_ref<REFNUDGE>(
-        V, (size_t)o, fs, gs, Fy, r, u, v, t,
-        [&](int k, double val) { __stcs(V.fdst + ((Off)k * pl + o), val); },
-        [&](int k, double val) { __stcs(V.gdst + ((Off)k * pl + o), val); });
-  } else {
-    node_shift(V, fs, gs, Fy, r, u, v, t);
-#pragma unroll
-    for (int k = 0; k < NPOP; k++) {
-      __stcs(V.fdst + ((Off)k * pl + o), fs[k]);
-      __stcs(V.gdst + ((Off)k * pl + o), gs[k]);
-    }
-  }
+  lb_collide<Real, REFNUDGE>(
+      V, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { __stcs(V.fdst + ((Off)k * pl + o), val); },
+      [&](int k, Real val) { __stcs(V.gdst + ((Off)k * pl + o), val); });
   V.Fout[o] = Fy;
   if (V.write_uv) {
     V.u[o] = u;

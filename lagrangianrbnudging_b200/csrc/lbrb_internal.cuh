@@ -208,6 +208,11 @@ struct Handle {
   // CUDA graphs of plain steps, one per buffer phase (cur * 9 + uvcur * 3 +
   // uvprev); graph_mode -1: small grids only, 0: off, 1: on
   cudaGraphExec_t graph_exec[18] = {};
+  // two steps per launch (lb_pair_kernel): pair_mode -1 auto (steps that
+  // do not replay graphs), 0 off, 1 on; pair_shape: tuned on first use
+  int pair_mode = -1;
+  int pair_shape = -1;
+  float pair_ms = 0.f;
   int graph_mode = -1;
   size_t esize = 8;   // bytes per population value
   // populations: pops[buf] holds f (9 planes) then g (9 planes)

@@ -1,0 +1,107 @@
+"""Two steps per launch (lb_pair_kernel, lbrb_set_pairs): a run stepped in
+pairs ends bit-identical to the same run stepped one launch at a time --
+populations, moments, post-stream populations of the last step, particles
+and records -- for every tile shape and the tuned one, in both precisions, on
+grids whose width and height are not multiples of the tile, with records on
+the first and on the second step of a pair, tracers and inertial particles
+with the Maxey-Riley stencil and full records, and without particles."""
+import numpy as np
+import pytest
+
+import lagrangianrbnudging_b200 as lb
+from lagrangianrbnudging_b200 import build
+
+pytestmark = pytest.mark.gpu
+
+CALLS = (1, 2, 5, 8, 31)  # odd and even calls: pairs never take a call's last step
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build.build()
+
+
+def make(precision, nx, ny, nprtcl, beta, full, pairs, shape):
+    r = lb.Run(**lb.closure(nx, ny, Ra=1e6, Pr=1.0, U=0.1), precision=precision, nprtcl=nprtcl,
+               noutconfig=3 if nprtcl else 0, record_slots=64, beta=beta, record_full=full)
+    r.set_graph(0)  # (small grids would otherwise replay graphs of single steps)
+    r.set_pairs(pairs)
+    if shape >= 0:
+        r.set_pair_shape(shape)
+    r.init_conduction(29, 3e-2)
+    if nprtcl:
+        rng = np.random.default_rng(7)
+        x = rng.uniform(0.5, nx + 0.5, nprtcl)
+        y = rng.uniform(1.0, ny, nprtcl)
+        y[:2] = [1.0, ny - 1e-9]
+        ptype = (np.arange(nprtcl) % 2).astype(np.int32)
+        invtau = np.where(ptype == 1, 1.0 / 25.0, 0.0)
+        z = np.zeros(nprtcl)
+        r.set_particles(np.arange(nprtcl, dtype=np.int32), x, y, z, z, ptype, invtau)
+    return r
+
+
+def state(r, nprtcl):
+    f, g = r.get_populations()
+    fp, gp = r.get_poststream()
+    out = dict(f=f, g=g, fp=fp, gp=gp, **r.get_moments())
+    if nprtcl:
+        out.update({"p" + k: v for k, v in r.get_particles().items()})
+        s, rec = r.drain_records_array()
+        out.update(rec_steps=s, rec=rec)
+    return out
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("nprtcl,beta,full", [(0, 0.0, 0), (80, 0.0, 0), (80, 0.5, 1)])
+@pytest.mark.parametrize("shape", [-1, 0, 1, 2, 3])
+def test_pairs_equal_single_steps(precision, nprtcl, beta, full, shape):
+    nx, ny = 200, 37
+    with make(precision, nx, ny, nprtcl, beta, full, 0, -1) as a, \
+            make(precision, nx, ny, nprtcl, beta, full, 1, shape) as b:
+        for n in CALLS:
+            a.step(n)
+            b.step(n)
+            sa, sb = state(a, nprtcl), state(b, nprtcl)
+            for k in sa:
+                np.testing.assert_array_equal(sb[k], sa[k], err_msg=k)
+        assert a.istep == b.istep == sum(CALLS)
+        ps = b.pair_shape()
+        assert ps["shape"] == (shape if shape >= 0 else ps["shape"]) and ps["shape"] >= 0
+        assert a.pair_shape()["shape"] == -1
+
+
+def test_pairs_on_a_tile_multiple_grid():
+    with make("fp32", 64, 48, 40, 0.0, 0, 0, -1) as a, make("fp32", 64, 48, 40, 0.0, 0, 1, 0) as b:
+        a.step(100)
+        b.step(100)
+        sa, sb = state(a, 40), state(b, 40)
+        for k in sa:
+            np.testing.assert_array_equal(sb[k], sa[k], err_msg=k)
+
+
+def test_record_ring_overflow_is_reported_at_the_same_step():
+    """a pair whose records would overflow the ring runs as single steps"""
+    kw = dict(**lb.closure(64, 32, Ra=1e6, Pr=1.0, U=0.1), precision="fp32", nprtcl=16, noutconfig=2,
+              record_slots=3)
+    for pairs in (0, 1):
+        with lb.Run(**kw) as r:
+            r.set_graph(0)
+            r.set_pairs(pairs)
+            r.init_conduction(3, 1e-2)
+            r.set_particles(np.arange(16, dtype=np.int32), np.full(16, 10.5), np.linspace(2, 30, 16),
+                            np.zeros(16), np.zeros(16), np.zeros(16, np.int32), np.zeros(16))
+            with pytest.raises(lb.LbrbError):
+                r.step(9)  # records at 2, 4, 6 fill the ring; step 8 overflows
+            assert r.istep == 7
+            assert r.pending_records() == 3
+
+
+def test_pair_arguments_checked():
+    with lb.Run(**lb.closure(64, 32, Ra=1e6, Pr=1.0, U=0.1), precision="fp32") as r:
+        for bad in (-2, 2):
+            with pytest.raises(lb.LbrbError):
+                r.set_pairs(bad)
+        for bad in (-2, 4):
+            with pytest.raises(lb.LbrbError):
+                r.set_pair_shape(bad)
