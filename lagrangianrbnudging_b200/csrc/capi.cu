@@ -1063,6 +1063,26 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     return launch_lb_fp64(seg_view<double>(h, src, dst, mom), h->p.twall, false, shape, st, true);
   };
   auto launch_fwd = [&](const char* src, char* dst, int mom) { return launch_fwd_on(src, dst, mom, h->stream); };
+  // two steps per launch where the state between them is not read: not an
+  // observation step, not in a segment whose states the backward pass keeps
+  const bool fwd_pairs = pairs_ok(h) && nsteps >= 2;
+  if (fwd_pairs && h->pair_shape < 0) {
+    // the pair tile shape, timed on the window's initial state (trial
+    // launches write segment slots 1 and 2, which the forward pass overwrites)
+    float ms = 0.f;
+    int sh = 0;
+    if (f32) sh = tune_pair_fp32(seg_view<float>(h, chk, seg + sb, 0), seg_view<float>(h, chk, seg + 2 * sb, 0), h->stream, &ms);
+    else sh = tune_pair_fp64(seg_view<double>(h, chk, seg + sb, 0), seg_view<double>(h, chk, seg + 2 * sb, 0), h->stream, &ms);
+    CK(h, cudaGetLastError());
+    h->pair_shape = sh;
+    h->pair_ms = ms;
+    if (h->pair_mode < 0 && h->lb_shape_ms > 0.f && ms >= 2.f * h->lb_shape_ms) h->pair_mode = 0;
+  }
+  auto residual = [&](int oi, const char* state) -> cudaError_t {
+    const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
+    return launch_obs_residual(state + (SLOT_MOM + 3) * plane * es, f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob,
+                               nob, h->adj_res + (size_t)oi * nob, h->stream);
+  };
   // ---- forward pass: checkpoints, residuals
   char* end_state = nullptr;
   for (int c = 0; c < nchk; c++) {
@@ -1072,25 +1092,41 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     // each segment buffer); inside a segment that the backward pass
     // recomputes, the states alternate between slots 1 and 2 (a footprint
     // that stays in L2)
-    const bool keep = c + 2 >= nchk;
-    auto fslot = [&](int i) -> char* {
-      if (i == 0) return state_in(c, 0);
-      return segbuf(c) + (size_t)(keep ? i : 1 + ((i - 1) & 1)) * sb;
-    };
-    for (int i = 0; i < len; i++) {
+    const bool keep = dJdT0 && c + 2 >= nchk;
+    char* const slot1 = segbuf(c) + sb;
+    char* cur_state = state_in(c, 0);
+    for (int i = 0; i < len;) {
       const int s = s0 + i + 1;
-      char* dst = (i + 1 < len) ? fslot(i + 1) : (last ? segbuf(c) + (size_t)K * sb : chk + (size_t)(c + 1) * sb);
+      // where the state after step i + q goes
+      auto out = [&](int q) -> char* {
+        if (i + q < len) return keep ? segbuf(c) + (size_t)(i + q) * sb : (cur_state == slot1 ? slot1 + sb : slot1);
+        return last ? segbuf(c) + (size_t)K * sb : chk + (size_t)(c + 1) * sb;
+      };
+      if (fwd_pairs && h->pair_mode != 0 && !keep && i + 1 < len && obs_at[s] < 0) {
+        char* dst = out(2);
+        const int oi = obs_at[s + 1];
+        const int mom = (dJdT0 && i + 2 == len) || oi >= 0;
+        if (f32)
+          CK(h, launch_pair_fp32(seg_view<float>(h, cur_state, dst, 0), seg_view<float>(h, cur_state, dst, mom),
+                                 h->pair_shape, h->stream, true));
+        else
+          CK(h, launch_pair_fp64(seg_view<double>(h, cur_state, dst, 0), seg_view<double>(h, cur_state, dst, mom),
+                                 h->pair_shape, h->stream, true));
+        if (oi >= 0) CK(h, residual(oi, dst));
+        cur_state = dst;
+        i += 2;
+        continue;
+      }
+      char* dst = out(1);
       const int oi = obs_at[s];
       // moments into every state the backward pass reads (and at observation
       // steps, for the residual's T)
-      CK(h, launch_fwd(fslot(i), dst, (dJdT0 && (keep || i + 1 == len)) || oi >= 0));
-      if (oi >= 0) {
-        const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
-        CK(h, launch_obs_residual(dst + (SLOT_MOM + 3) * plane * es, f32, nx, ny, pitch, ob, ob + nob,
-                                  ob + 2 * nob, nob, h->adj_res + (size_t)oi * nob, h->stream));
-      }
-      end_state = dst;
+      CK(h, launch_fwd(cur_state, dst, (dJdT0 && (keep || i + 1 == len)) || oi >= 0));
+      if (oi >= 0) CK(h, residual(oi, dst));
+      cur_state = dst;
+      i++;
     }
+    end_state = cur_state;
   }
   // misfit on the device (observation steps inside the window: a prefix)
   int nused = 0;
