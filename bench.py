@@ -239,7 +239,8 @@ def measured_peak():
 
 def profiled_traffic(precision: str):
     """DRAM bytes per node of one fused-kernel launch from the committed ncu
-    summary (profiles/lb_step_traffic.json), or None."""
+    summary (profiles/lb_step_traffic.json; "fp32" is the two-step launch,
+    "fp32_single" the one-step one), or None."""
     p = ROOT / "profiles" / "lb_step_traffic.json"
     if not p.exists():
         return None
@@ -377,7 +378,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     avg_lb = lb_ms / max(lb_n, 1)
     spl = K / max(lb_n, 1)
     achieved = ALG_BYTES["fp32"] * nodes * spl / (avg_lb * 1e-3) / 1e9
-    tr = profiled_traffic("fp32")
+    tr = profiled_traffic("fp32" if spl > 1.5 else "fp32_single")
     spl64 = K64 / max(timing64["lb_step"][1], 1)
     avg_lb64 = timing64["lb_step"][0] / max(timing64["lb_step"][1], 1)
     achieved64 = ALG_BYTES["fp64"] * nodes * spl64 / (avg_lb64 * 1e-3) / 1e9
@@ -406,6 +407,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
                      "node_steps_per_launch": round(spl, 4),
                      "avg_launch_ms": round(avg_lb, 5),
                      "traffic": (round(tr * nodes) if tr else None),
+                     "traffic_gbs": (round(tr * nodes / (avg_lb * 1e-3) / 1e9, 1) if tr else None),
                      "share_of_step": round(lb_ms / timing["window_ms"][0], 4),
                      "launch_shape": shape32, "pair_shape": pair32,
                      "note": "achieved = 144 B x node-steps per launch / launch time (a two-step launch moves "
@@ -1139,6 +1141,8 @@ def run_lb_only(args, torch) -> dict:
     fixed = dict(autotune=0, launch_shape=args.shape) if args.shape >= 0 else {}
     with lb.Run(**base, precision=args.precision, device=0, **fixed) as r:
         r.set_pairs(PAIRS_MODE)
+        if args.pair_shape >= 0:
+            r.set_pair_shape(args.pair_shape)
         r.init_conduction(SEED, 1e-3)
         ms, timing, _, _ = timed_steps(r, torch, args.steps, args.warmup, None, 0)
         shape = r.launch_shape()
@@ -1174,6 +1178,8 @@ def main():
     ap.add_argument("--config0", action="store_true",
                     help="the 512x256 tracer case on the GPU and the reference CPU build")
     ap.add_argument("--no-slab", action="store_true", help="skip the y-slab section")
+    ap.add_argument("--pair-shape", type=int, default=-1,
+                    help="lb-only: fixed tile shape of the two-step launch instead of the autotuner")
     ap.add_argument("--no-pairs", action="store_true",
                     help="one fused launch per step (lbrb_set_pairs 0) instead of two steps per launch")
     ap.add_argument("--slab-only", action="store_true",

@@ -179,8 +179,10 @@ LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
  * Replaces, for two steps at a time, the reference's per-step sweeps
  * (stream, moments, collide: temppart_dump.c:1674-1759). */
 LBRB_API int lbrb_set_pairs(lbrb_t *h, int mode);
-/* fix the tile shape (0: 32x8, 1: 32x4, 2: 32x16, 3: 64x4) instead of timing
- * the shapes on first use (-1) */
+/* fix the tile shape (0: 32x8, 1: 32x4, 2: 32x16, 3: 64x4, 4: 32x8 with a
+ * thread per node of the tile and its ring, 5: 30x8 likewise, 6: 32x8 at 5
+ * blocks per SM, 7: 32x6, 8: 64x8) instead of timing the shapes on first
+ * use (-1) */
 LBRB_API int lbrb_set_pair_shape(lbrb_t *h, int shape);
 LBRB_API int lbrb_get_pair_shape(const lbrb_t *h, int *shape, int *tile_x, int *tile_y, float *ms);
 /* Per-kernel device timing with CUDA events around each launch.  Classes:

@@ -1591,7 +1591,8 @@ int lbrb_set_pairs(lbrb_t* h, int mode) {
 }
 
 int lbrb_set_pair_shape(lbrb_t* h, int shape) {
-  if (!h || shape < -1 || shape > 3) return fail(h, LBRB_ERR_ARG, "set_pair_shape: shape must be -1 (tune) or 0..3");
+  if (!h || shape < -1 || shape >= NUM_PAIR_SHAPES)
+    return fail(h, LBRB_ERR_ARG, "set_pair_shape: shape must be -1 (tune) or a shape index");
   h->pair_shape = shape;
   h->pair_ms = 0.f;
   return LBRB_OK;
@@ -1599,7 +1600,8 @@ int lbrb_set_pair_shape(lbrb_t* h, int shape) {
 
 int lbrb_get_pair_shape(const lbrb_t* h, int* shape, int* tile_x, int* tile_y, float* ms) {
   if (!h) return LBRB_ERR_ARG;
-  static const int TXS[] = {32, 32, 32, 64}, TYS[] = {8, 4, 16, 4};  // (lb_kernels.cu: PAIR_SHAPES)
+  static const int TXS[] = {32, 32, 32, 64, 32, 30, 32, 32, 64}, TYS[] = {8, 4, 16, 4, 8, 8, 8, 6, 8};  // (lb_kernels.cu: PAIR_SHAPES)
+  static_assert(sizeof(TXS) / sizeof(int) == NUM_PAIR_SHAPES, "pair shape table");
   const int sh = h->pair_shape;
   if (shape) *shape = sh;
   if (tile_x) *tile_x = sh < 0 ? 0 : TXS[sh];

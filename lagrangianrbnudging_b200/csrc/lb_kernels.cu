@@ -78,8 +78,11 @@ __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V)
 // ring is recomputed (34 x 10 nodes for a 32 x 8 tile).  The per-node
 // arithmetic is lb_update_node's, so two steps here equal two launches of
 // lb_node_kernel bit for bit.
-template <typename Real, int TX, int TY, int MINB, typename Off>
-__global__ void __launch_bounds__(TX * TY, MINB) lb_pair_kernel(const LBView<Real> V1, const LBView<Real> V2) {
+// NT threads per block: TX * TY (phase 1 takes the region in passes), or
+// one per region node rounded to whole warps (phase 1 in one pass; phase 2
+// leaves the rest idle)
+template <typename Real, int TX, int TY, int NT, int MINB, typename Off>
+__global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1, const LBView<Real> V2) {
   pdl_wait();
   constexpr int RX = TX + 2, RY = TY + 2, RN = RX * RY;
   extern __shared__ __align__(16) unsigned char pair_smem[];
@@ -89,7 +92,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) lb_pair_kernel(const LBView<Rea
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int ncols = min(TX, nx - x0), nrows = min(TY, ny - y0);
   const Off pitch = (Off)V1.pitch;
-  for (int q = threadIdx.x; q < RN; q += TX * TY) {
+  for (int q = threadIdx.x; q < RN; q += NT) {
     const int lx = q % RX, ly = q / RX;
     const int jg = y0 - 1 + ly;
     if (lx > ncols + 1 || ly > nrows + 1 || jg < 0 || jg >= ny) continue;
@@ -115,6 +118,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) lb_pair_kernel(const LBView<Rea
     }
   }
   __syncthreads();
+  if (threadIdx.x >= TX * TY) return;
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   if (tx >= ncols || ty >= nrows) return;
   const int x = x0 + tx, j = y0 + ty;
@@ -135,12 +139,15 @@ __global__ void __launch_bounds__(TX * TY, MINB) lb_pair_kernel(const LBView<Rea
   lb_finish_node<Real, false, Off>(V2, (Off)j * pitch + (Off)x, fs, gs, SF[ty * TX + tx]);
 }
 
-// pair launch shapes: (tile columns, tile rows, min blocks per SM)
-struct PairShape { int tx, ty, minb; };
-constexpr PairShape PAIR_SHAPES[] = {{32, 8, 4}, {32, 4, 6}, {32, 16, 2}, {64, 4, 3}};
+// pair launch shapes: (tile columns, tile rows, threads, min blocks per SM)
+struct PairShape { int tx, ty, nt, minb; };
+constexpr PairShape PAIR_SHAPES[] = {{32, 8, 256, 4}, {32, 4, 128, 6}, {32, 16, 512, 2}, {64, 4, 256, 3},
+                                     {32, 8, 352, 2}, {30, 8, 320, 3}, {32, 8, 256, 5}, {32, 6, 192, 5},
+                                     {64, 8, 512, 2}};
 constexpr int NPAIR = sizeof(PAIR_SHAPES) / sizeof(PAIR_SHAPES[0]);
+static_assert(NPAIR == NUM_PAIR_SHAPES, "pair shape table");
 
-template <typename Real, int TX, int TY, int MINB>
+template <typename Real, int TX, int TY, int NT, int MINB>
 static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2, cudaStream_t s, bool pdl) {
   const size_t smem = ((size_t)2 * NPOP * (TX + 2) * (TY + 2) + (size_t)TX * TY) * sizeof(Real);
   dim3 grid((V1.nx + TX - 1) / TX, (V1.ny + TY - 1) / TY);
@@ -151,21 +158,26 @@ static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2,
       if (e != cudaSuccess) return e;
       attr = true;
     }
-    return launch_k(kernel, grid, TX * TY, smem, s, pdl, V1, V2);
+    return launch_k(kernel, grid, NT, smem, s, pdl, V1, V2);
   };
   // (FP64 holds twice the registers per value: half the blocks per SM)
   constexpr int MB = std::is_same<Real, double>::value ? (MINB + 1) / 2 : MINB;
-  if (off32_ok(V1.plane)) return go(lb_pair_kernel<Real, TX, TY, MB, uint32_t>);
-  return go(lb_pair_kernel<Real, TX, TY, MB, size_t>);
+  if (off32_ok(V1.plane)) return go(lb_pair_kernel<Real, TX, TY, NT, MB, uint32_t>);
+  return go(lb_pair_kernel<Real, TX, TY, NT, MB, size_t>);
 }
 
 template <typename Real>
 static cudaError_t launch_pair(const LBView<Real>& V1, const LBView<Real>& V2, int shape, cudaStream_t s, bool pdl) {
   switch (shape) {
-    case 1: return launch_pair_t<Real, 32, 4, 6>(V1, V2, s, pdl);
-    case 2: return launch_pair_t<Real, 32, 16, 2>(V1, V2, s, pdl);
-    case 3: return launch_pair_t<Real, 64, 4, 3>(V1, V2, s, pdl);
-    default: return launch_pair_t<Real, 32, 8, 4>(V1, V2, s, pdl);
+    case 1: return launch_pair_t<Real, 32, 4, 128, 6>(V1, V2, s, pdl);
+    case 2: return launch_pair_t<Real, 32, 16, 512, 2>(V1, V2, s, pdl);
+    case 3: return launch_pair_t<Real, 64, 4, 256, 3>(V1, V2, s, pdl);
+    case 4: return launch_pair_t<Real, 32, 8, 352, 2>(V1, V2, s, pdl);
+    case 5: return launch_pair_t<Real, 30, 8, 320, 3>(V1, V2, s, pdl);
+    case 6: return launch_pair_t<Real, 32, 8, 256, 5>(V1, V2, s, pdl);
+    case 7: return launch_pair_t<Real, 32, 6, 192, 5>(V1, V2, s, pdl);
+    case 8: return launch_pair_t<Real, 64, 8, 512, 2>(V1, V2, s, pdl);
+    default: return launch_pair_t<Real, 32, 8, 256, 4>(V1, V2, s, pdl);
   }
 }
 

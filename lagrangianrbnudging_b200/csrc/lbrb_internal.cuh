@@ -53,6 +53,9 @@ constexpr double CS2 = 1.0 / 3.0;
 // element offsets of a population buffer (18 planes) fit in 32 bits
 inline bool off32_ok(size_t plane) { return plane * 2 * NPOP < (size_t(1) << 32); }
 
+// tile shapes of the two-step kernel (lb_kernels.cu: PAIR_SHAPES)
+constexpr int NUM_PAIR_SHAPES = 9;
+
 // Programmatic dependent launch: a kernel launched with the attribute may
 // start while the kernel before it in the stream finishes; it waits here,
 // before touching memory, until that kernel has completed and its writes are
@@ -208,7 +211,8 @@ struct Handle {
   // CUDA graphs of plain steps, one per buffer phase (cur * 9 + uvcur * 3 +
   // uvprev); graph_mode -1: small grids only, 0: off, 1: on
   cudaGraphExec_t graph_exec[18] = {};
-  // two steps per launch (lb_pair_kernel): pair_mode -1 auto (steps that
+  // two steps per launch (lb_pair_kernel, NUM_PAIR_SHAPES tile shapes):
+  // pair_mode -1 auto (steps that
   // do not replay graphs), 0 off, 1 on; pair_shape: tuned on first use
   int pair_mode = -1;
   int pair_shape = -1;

@@ -54,7 +54,7 @@ def state(r, nprtcl):
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("nprtcl,beta,full", [(0, 0.0, 0), (80, 0.0, 0), (80, 0.5, 1)])
-@pytest.mark.parametrize("shape", [-1, 0, 1, 2, 3])
+@pytest.mark.parametrize("shape", [-1, 0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_pairs_equal_single_steps(precision, nprtcl, beta, full, shape):
     nx, ny = 200, 37
     with make(precision, nx, ny, nprtcl, beta, full, 0, -1) as a, \
@@ -102,6 +102,6 @@ def test_pair_arguments_checked():
         for bad in (-2, 2):
             with pytest.raises(lb.LbrbError):
                 r.set_pairs(bad)
-        for bad in (-2, 4):
+        for bad in (-2, 9):
             with pytest.raises(lb.LbrbError):
                 r.set_pair_shape(bad)
