@@ -342,7 +342,14 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     ms64, timing64, _, _ = timed_steps(r64, torch, K64, W, dist, device)
     shape64 = r64.launch_shape()
     pair64 = r64.pair_shape()
-    r64.step(2 * (K - K64))  # same number of steps as the FP32 run (two windows each) for the Nu comparison
+    # the same number of steps as the FP32 run (two windows each) for the Nu
+    # comparison, draining the records as they come
+    rest = 2 * (K - K64)
+    while rest > 0:
+        n = min(rest, 1000)
+        r64.step(n)
+        r64.drain_records()
+        rest -= n
     r64.sync()
     nu64 = r64.nusselt()
     ke64, _ = r64.energy()
