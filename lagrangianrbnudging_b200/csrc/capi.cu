@@ -799,20 +799,26 @@ int lbrb_step(lbrb_t* h, int n) {
       tmark_end(h, tm, h->stream);
     }
     if (parts) {
-      const int ubs[2] = {h->uvcur, A}, us[2] = {A, B}, ts[2] = {src, dst}, isteps[2] = {i1, i2};
-      const bool recs[2] = {rec1, rec2};
-      for (int q = 0; q < 2; q++) {
-        const int slot = recs[q] ? (int)(h->rec_head % h->p.record_slots) : 0;
-        double* rslot = recs[q] ? h->d_ring + (size_t)slot * h->nrec_fields * h->np : nullptr;
-        const int tm = tmark_begin(h, 1, h->stream);
-        CK(h, launch_particles(h->uv[us[q]][0], h->uv[us[q]][1], h->uv[ubs[q]][0], h->uv[ubs[q]][1], h->T[ts[q]],
-                               f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta, recs[q] ? 1 : 0,
-                               h->p.record_full, rslot, h->dflags, h->stream, pdl_ok));
-        tmark_end(h, tm, h->stream);
-        if (recs[q]) {
-          const int rc = record_copy(isteps[q], slot, rslot, h->stream);
-          if (rc) return rc;
-        }
+      // both steps of every particle in one launch; the ring slots in step order
+      long head = h->rec_head;
+      const int slot1 = rec1 ? (int)(head++ % h->p.record_slots) : 0;
+      const int slot2 = rec2 ? (int)(head % h->p.record_slots) : 0;
+      const size_t per = (size_t)h->nrec_fields * h->np;
+      double* r1 = rec1 ? h->d_ring + (size_t)slot1 * per : nullptr;
+      double* r2 = rec2 ? h->d_ring + (size_t)slot2 * per : nullptr;
+      const void* fa[5] = {h->uv[A][0], h->uv[A][1], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[src]};
+      const void* fb[5] = {h->uv[B][0], h->uv[B][1], h->uv[A][0], h->uv[A][1], h->T[dst]};
+      const int tm = tmark_begin(h, 1, h->stream);
+      CK(h, launch_particles_pair(fa, fb, f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta,
+                                  h->p.record_full, r1, r2, h->dflags, h->stream, pdl_ok));
+      tmark_end(h, tm, h->stream);
+      if (rec1) {
+        const int rc = record_copy(i1, slot1, r1, h->stream);
+        if (rc) return rc;
+      }
+      if (rec2) {
+        const int rc = record_copy(i2, slot2, r2, h->stream);
+        if (rc) return rc;
       }
       h->uvprev = A;
       h->uvcur = B;

@@ -35,6 +35,12 @@ cudaError_t launch_particles(const void* u, const void* v, const void* ub, const
                              const void* T, bool fp32, int nx, int ny, int pitch, double* P,
                              const int* ptype, int np, double beta, int record, int full,
                              double* rec, unsigned* dflags, cudaStream_t s, bool pdl = false);
+// two steps of every particle (after a two-step fused launch): fields_a and
+// fields_b = {u, v, ub, vb, T} of steps n and n+1; rec_a / rec_b: the ring
+// slots of a record step, else null
+cudaError_t launch_particles_pair(const void* const* fields_a, const void* const* fields_b, bool fp32, int nx,
+                                  int ny, int pitch, double* P, const int* ptype, int np, double beta, int full,
+                                  double* rec_a, double* rec_b, unsigned* dflags, cudaStream_t s, bool pdl);
 // y-slabs: rows5 = device tables of row pointers (u, v, ub, vb, T), one
 // entry per global row
 cudaError_t launch_particles_slab(const void* u, const void* v, const void* ub, const void* vb, const void* T,

@@ -36,6 +36,19 @@ cudaError_t launch_particles_t(const PView<Real>& V, cudaStream_t s, bool pdl) {
   return launch_k(particle_kernel<Real, false>, (V.np + 127) / 128, 128, 0, s, pdl, V);
 }
 
+// Two steps of a particle in one launch, after a two-step fused launch has
+// stored u, v (and T) of both steps: Va is step n, Vb step n+1.  The second
+// update reads the state the first one wrote (the same thread, so it sees
+// its own stores); the arithmetic is particle_update's, step by step.
+template <typename Real, bool DERIVS>
+__global__ void __launch_bounds__(128) particle_pair_kernel(const PView<Real> Va, const PView<Real> Vb) {
+  pdl_wait();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= Va.np) return;
+  particle_update<Real, DERIVS>(Va, p);
+  particle_update<Real, DERIVS>(Vb, p);
+}
+
 // ------------------------------------------------------------- y-slabs
 // A domain held as y-slabs: every slab holds all particles.  Each step, the
 // slab whose rows hold a particle's cell (its position before the step)
@@ -104,6 +117,24 @@ cudaError_t launch_particles_merge(double* P, int np, const int* own, int me, co
   if (np <= 0) return cudaSuccess;
   particle_merge_kernel<<<(np + 127) / 128, 128, 0, s>>>(P, np, own, me, Ps, rec, recs, rec_off, nrec);
   return cudaGetLastError();
+}
+
+cudaError_t launch_particles_pair(const void* const* fields_a, const void* const* fields_b, bool fp32, int nx,
+                                  int ny, int pitch, double* P, const int* ptype, int np, double beta, int full,
+                                  double* rec_a, double* rec_b, unsigned* dflags, cudaStream_t s, bool pdl) {
+  if (np <= 0) return cudaSuccess;
+  auto go = [&](auto zero) -> cudaError_t {
+    using Real = decltype(zero);
+    auto view = [&](const void* const* f, double* rec) {
+      return PView<Real>{(const Real*)f[0], (const Real*)f[1], (const Real*)f[2], (const Real*)f[3], (const Real*)f[4],
+                         nx, ny, pitch, P, ptype, np, beta, rec ? 1 : 0, full, rec, dflags};
+    };
+    const PView<Real> Va = view(fields_a, rec_a), Vb = view(fields_b, rec_b);
+    const int g = (np + 127) / 128;
+    if (beta != 0.0 || full) return launch_k(particle_pair_kernel<Real, true>, g, 128, 0, s, pdl, Va, Vb);
+    return launch_k(particle_pair_kernel<Real, false>, g, 128, 0, s, pdl, Va, Vb);
+  };
+  return fp32 ? go(0.f) : go(0.0);
 }
 
 // explicit views built by the host side
