@@ -294,11 +294,27 @@ def e2e(lb, torch, precision: str, seed: int, steps: int, device: int, dist):
     r.set_populations(f, g, layout="ref")
     r.set_moments(rho, uu, vv, Th, layout="ref")
     r.set_particles(ids, x, y, pu, pv, ptype, invtau)
-    r.step(steps)
     import ctypes as C
     st = np.empty(max(nrec, 1), np.int32)
     got = C.c_int()
-    r._ck(lb.lib().lbrb_record_drain(r.h, nrec, lb._ip(st), lb._dp(recbuf), None, C.byref(got)))
+    # as a host program runs: the steps go out in chunks, and the records of
+    # one chunk are drained (into the caller's arrays) while the next runs
+    chunk = 25 * NOUTCONFIG
+    done = drained = 0
+    prev = 0  # records of the chunk before the one in flight
+    while done < steps:
+        n = min(chunk, steps - done)
+        r.step(n)
+        done += n
+        if prev:
+            r._ck(lb.lib().lbrb_record_drain(r.h, prev, lb._ip(st[drained:]), lb._dp(recbuf[drained:]), None,
+                                             C.byref(got)))
+            drained += got.value
+        prev = (done // NOUTCONFIG) - ((done - n) // NOUTCONFIG)
+    r._ck(lb.lib().lbrb_record_drain(r.h, nrec - drained, lb._ip(st[drained:]), lb._dp(recbuf[drained:]), None,
+                                     C.byref(got)))
+    drained += got.value
+    got.value = drained
     r._ck(lb.lib().lbrb_get_moments(r.h, *[lb._dp(a) for a in out_m], lb.LAYOUT["ref"]))
     e1.record(stream)
     torch.cuda.synchronize()
