@@ -105,3 +105,32 @@ def test_pair_arguments_checked():
         for bad in (-2, 9):
             with pytest.raises(lb.LbrbError):
                 r.set_pair_shape(bad)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_pairs_on_grids_smaller_than_a_tile(precision):
+    """8 x 5 nodes: the ring wraps onto the tile itself in x, and every row
+    is a wall row or next to one"""
+    for shape in (0, 5, 8):
+        with make(precision, 8, 5, 6, 0.0, 0, 0, -1) as a, make(precision, 8, 5, 6, 0.0, 0, 1, shape) as b:
+            for n in (3, 7):
+                a.step(n)
+                b.step(n)
+                sa, sb = state(a, 6), state(b, 6)
+                for k in sa:
+                    np.testing.assert_array_equal(sb[k], sa[k], err_msg=f"shape {shape}: {k}")
+
+
+def test_pairs_are_the_default_above_the_graph_size():
+    """a grid of more than 2^20 nodes steps two per launch by default (and
+    keeps the result of single launches)"""
+    kw = dict(**lb.closure(1040, 1024, Ra=1e6, Pr=1.0, U=0.1), precision="fp32")
+    with lb.Run(**kw) as a, lb.Run(**kw) as b:
+        a.set_pairs(0)
+        for r in (a, b):
+            r.init_conduction(2, 1e-2)
+            r.step(9)
+        assert b.pair_shape()["shape"] >= 0 and a.pair_shape()["shape"] == -1
+        ma, mb = a.get_moments(), b.get_moments()
+        for k in ma:
+            np.testing.assert_array_equal(mb[k], ma[k])
