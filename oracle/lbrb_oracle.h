@@ -77,7 +77,7 @@ void orc_step(orc_t *s, int istep);
  * populations; v gets +0.5*(-gravity)*T without a rho factor. */
 void orc_moments_from_pre(orc_t *s, const double *fpre, const double *gpre);
 
-/* BASELINE initial state: linear conduction T plus seeded uniform noise,
+/* The benchmark configurations' initial state: linear conduction T plus seeded uniform noise,
  * f = feq(1,0), g = geq(T,0); moments by the restart route. */
 void orc_init_conduction(orc_t *s, unsigned long long seed, double noise_amp);
 double orc_splitmix_uniform(unsigned long long seed, unsigned long long index);
