@@ -1235,8 +1235,27 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
       // read it (segment nchk-2 is still there from the forward pass)
       const int cp = c - 1, lenp = std::min(K, nsteps - cp * K);
       CK(h, cudaStreamWaitEvent(rs, ev_bwd[b ^ 1], 0));
-      for (int i = 0; i + 1 < lenp; i++)
-        CK(h, launch_fwd_on(state_in(cp, i), segbuf(cp) + (size_t)(i + 1) * sb, 1, rs));
+      // the sweep reads each state's moments and F, never its populations,
+      // so two steps go in one launch whose first step stores only those
+      for (int i = 0; i + 1 < lenp;) {
+        char* s1p = segbuf(cp) + (size_t)(i + 1) * sb;
+        if (fwd_pairs && h->pair_mode != 0 && i + 2 < lenp) {
+          char* s2p = s1p + sb;
+          if (f32) {
+            LBView<float> V1 = seg_view<float>(h, state_in(cp, i), s1p, 1);
+            V1.write_F = 1;
+            CK(h, launch_pair_fp32(V1, seg_view<float>(h, s1p, s2p, 1), h->pair_shape, rs, true));
+          } else {
+            LBView<double> V1 = seg_view<double>(h, state_in(cp, i), s1p, 1);
+            V1.write_F = 1;
+            CK(h, launch_pair_fp64(V1, seg_view<double>(h, s1p, s2p, 1), h->pair_shape, rs, true));
+          }
+          i += 2;
+        } else {
+          CK(h, launch_fwd_on(state_in(cp, i), s1p, 1, rs));
+          i++;
+        }
+      }
       CK(h, cudaEventRecord(ev_rec[b ^ 1], rs));
     }
     if (c + 2 < nchk) CK(h, cudaStreamWaitEvent(h->stream, ev_rec[b], 0));

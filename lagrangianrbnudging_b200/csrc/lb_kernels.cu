@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
         [&](int k, Real val) { S[((NPOP + k) * RY + ly) * RX + lx] = val; });
     if (lx >= 1 && lx <= ncols && ly >= 1 && ly <= nrows) {
       SF[(ly - 1) * TX + (lx - 1)] = Fy;
+      if (V1.write_F) V1.Fout[o] = Fy;
       if (V1.write_uv) {
         V1.u[o] = u;
         V1.v[o] = v;

@@ -162,6 +162,7 @@ struct LBView {
   double alpha;
   int write_uv;
   int write_rt;  // bit 0: store T (records, nudging), bit 1: also rho (a call's last step)
+  int write_F;   // lb_pair_kernel: also store step n's F^{n+1} through V1.Fout (adjoint recompute)
   // y-slab of a larger domain: the rows below row 0 / above row ny-1 (the
   // neighbour slab's boundary row after its collision), 6 rows of nx values:
   // f then g of the three populations crossing the boundary; null = wall
