@@ -456,8 +456,9 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
         out["e2e"] = {"value": round(world * nodes * K / (e2e_ms * 1e3), 1), "unit": "MLUPS",
                       "h2d_bytes_per_step": int(e2e_h2d / K), "d2h_bytes_per_step": int(e2e_d2h / K),
                       "ms": round(e2e_ms, 2),
-                      "path": "lbrb_set_populations(REF_AOS_HALO fp64) + set_moments + "
-                              "particles_set + lbrb_step(K) + record_drain + get_moments"}
+                      "path": "lbrb_set_populations(REF_AOS_HALO fp64) + set_moments + particles_set + "
+                              "lbrb_step in chunks of 500 steps, each chunk's records drained (lbrb_record_drain) "
+                              "while the next runs + get_moments"}
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
