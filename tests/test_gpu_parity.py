@@ -31,11 +31,18 @@ def traj_run(c, precision="fp64", **extra):
     return r
 
 
+@pytest.mark.parametrize("launch", ["default", "pairs", "single"])
 @pytest.mark.parametrize("name", list(cases.TRAJ_CASES))
-def test_fp64_trajectories_bit_exact_vs_reference(name):
+def test_fp64_trajectories_bit_exact_vs_reference(name, launch):
+    """default: graph replays of one-step launches on these small grids;
+    pairs: two steps per fused launch (and per particle launch); single: one
+    launch per step, no graphs"""
     c = cases.traj_case(name)
     z = cases.load_golden(name)
     with traj_run(c) as r:
+        if launch != "default":
+            r.set_graph(0)
+            r.set_pairs(1 if launch == "pairs" else 0)
         r.step(c["nsteps"])
         r.sync()
         f, g = r.get_populations()
