@@ -145,8 +145,6 @@ static void free_all(lbrb_t* h) {
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->join_ev) cudaEventDestroy(h->join_ev);
   if (h->pstream) cudaStreamDestroy(h->pstream);
-  cudaEvent_t evs[] = {h->ev_lb, h->ev_uv[0], h->ev_uv[1], h->ev_uv[2], h->ev_T[0], h->ev_T[1], h->ev_pjoin};
-  for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
 }
 
@@ -189,11 +187,6 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
       cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->pstream, cudaStreamNonBlocking) != cudaSuccess)
     return done(LBRB_ERR_CUDA);
-  {
-    cudaEvent_t* evs[] = {&h->ev_lb, &h->ev_uv[0], &h->ev_uv[1], &h->ev_uv[2], &h->ev_T[0], &h->ev_T[1], &h->ev_pjoin};
-    for (cudaEvent_t* e : evs)
-      if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return done(LBRB_ERR_CUDA);
-  }
   h->stream = h->own_stream;
   h->pitch = (p.nx + 31) / 32 * 32;
   h->plane = (size_t)p.ny * h->pitch;
@@ -541,9 +534,6 @@ int lbrb_nudge_obs(lbrb_t* h, int first_step, int nsteps, const double* x, const
 // ------------------------------------------------------------- time loop
 }  // extern "C"
 
-// particle kernels on a second stream, overlapping the next fused kernel
-static constexpr bool kParticleStream = false;
-
 // view of one step from one state slot (SLOT_PLANES planes: pops, F,
 // moments) to another; with `mom` the step's moments go to the destination
 // slot's moment planes
@@ -617,14 +607,13 @@ constexpr int GRAPH_STEPS = 3;
 constexpr long GRAPH_MAX_NODES = 1L << 20;
 static bool graph_ok(const lbrb_t* h) {
   return h->graph_mode != 0 && (h->graph_mode == 1 || (long)h->p.nx * h->p.ny <= GRAPH_MAX_NODES) &&
-         h->stream != nullptr && h->p.nudge == LBRB_NUDGE_NONE && !h->timing && !kParticleStream && !h->slab;
+         h->stream != nullptr && h->p.nudge == LBRB_NUDGE_NONE && !h->timing && !h->slab;
 }
 
 // two steps per launch: Dirichlet walls, no nudging (it acts between the
 // steps), not a y-slab (ghost rows are exchanged every step)
 static bool pairs_ok(const lbrb_t* h) {
-  return h->pair_mode != 0 && h->p.twall == LBRB_TWALL_DIRICHLET && h->p.nudge == LBRB_NUDGE_NONE && !h->slab &&
-         !kParticleStream;
+  return h->pair_mode != 0 && h->p.twall == LBRB_TWALL_DIRICHLET && h->p.nudge == LBRB_NUDGE_NONE && !h->slab;
 }
 
 int lbrb_step(lbrb_t* h, int n) {
@@ -674,7 +663,6 @@ int lbrb_step(lbrb_t* h, int n) {
     h->join_pending = true;
     return LBRB_OK;
   };
-  bool pt_queued = false;
   // one step's launches; `last` writes the moments
   const bool pdl_ok = !h->timing;  // (per-kernel timing keeps plain launches)
   auto one = [&](bool last) -> int {
@@ -708,11 +696,6 @@ int lbrb_step(lbrb_t* h, int n) {
     const int write_rt = last ? 3 : ((rec || h->p.nudge == LBRB_NUDGE_BILINEAR) ? 1 : 0);
     const int src = h->cur, dst = h->cur ^ 1;
     const int uvn = write_uv ? 3 - h->uvcur - h->uvprev : h->uvcur;
-    // buffers read by an earlier particle kernel must be free before rewriting
-    if (h->np > 0 && kParticleStream) {
-      if (write_uv) CK(h, cudaStreamWaitEvent(h->stream, h->ev_uv[uvn], 0));
-      CK(h, cudaStreamWaitEvent(h->stream, h->ev_T[dst], 0));
-    }
     {
       const int tm = tmark_begin(h, 0, h->stream);
       // programmatic dependent launch when the kernel before it is this
@@ -721,7 +704,6 @@ int lbrb_step(lbrb_t* h, int n) {
       else CK(h, launch_lb_fp64(make_view<double>(h, src, dst, uvn, write_uv, write_rt), h->p.twall, refbox, h->lb_shape, h->stream, pdl_ok));
       tmark_end(h, tm, h->stream);
     }
-    if (h->np > 0 && kParticleStream) CK(h, cudaEventRecord(h->ev_lb, h->stream));
     if (h->slab) h->slab_obs = obs;  // (y-slabs: lbrb_slab_step nudges once every slab has stepped)
     if (obs && !h->slab) {
       const int tm = tmark_begin(h, 2, h->stream);
@@ -731,29 +713,20 @@ int lbrb_step(lbrb_t* h, int n) {
       tmark_end(h, tm, h->stream);
     }
     if (h->np > 0 && !h->slab) {  // (y-slabs: lbrb_slab_step moves the particles)
-      // Particles of step n.  With kParticleStream they run on their own
-      // stream beside the fused kernel of step n+1 (u, v rotate over three
-      // slots and T over two, ordered by events); measured on B200 the fused
-      // kernel then slows by about the particle kernel's own time, so by
-      // default they run in order on the step stream.
+      // Particles of step n, in order on the step stream.  (Run on a second
+      // stream beside the next fused kernel, with events ordering the u, v
+      // slots and T buffers, they slowed the fused kernel by about their own
+      // time on B200, so they stay in order.)
       const int ub = write_uv ? h->uvcur : h->uvprev;
       const int slot = rec ? (int)(h->rec_head % h->p.record_slots) : 0;
       double* rslot = rec ? h->d_ring + (size_t)slot * h->nrec_fields * h->np : nullptr;
-      cudaStream_t ps = kParticleStream ? h->pstream : h->stream;
-      if (kParticleStream) CK(h, cudaStreamWaitEvent(ps, h->ev_lb, 0));
-      const int tm = tmark_begin(h, 1, ps);
+      const int tm = tmark_begin(h, 1, h->stream);
       CK(h, launch_particles(h->uv[uvn][0], h->uv[uvn][1], h->uv[ub][0], h->uv[ub][1],
                              h->T[dst], f32, nx, ny, h->pitch, h->px, h->ptype, h->np, h->p.beta,
-                             rec ? 1 : 0, h->p.record_full, rslot, h->dflags, ps, pdl_ok && !kParticleStream));
-      tmark_end(h, tm, ps);
-      if (kParticleStream) {
-        CK(h, cudaEventRecord(h->ev_uv[uvn], ps));
-        CK(h, cudaEventRecord(h->ev_uv[ub], ps));
-        CK(h, cudaEventRecord(h->ev_T[dst], ps));
-        pt_queued = true;
-      }
+                             rec ? 1 : 0, h->p.record_full, rslot, h->dflags, h->stream, pdl_ok));
+      tmark_end(h, tm, h->stream);
       if (rec) {
-        const int rc = record_copy(istep, slot, rslot, ps);
+        const int rc = record_copy(istep, slot, rslot, h->stream);
         if (rc) return rc;
       }
     }
@@ -936,12 +909,7 @@ int lbrb_step(lbrb_t* h, int n) {
     if (rc) return rc;
     s++;
   }
-  // the caller's stream sees the particle kernels and record copies as part
-  // of the steps
-  if (pt_queued) {
-    CK(h, cudaEventRecord(h->ev_pjoin, h->pstream));
-    CK(h, cudaStreamWaitEvent(h->stream, h->ev_pjoin, 0));
-  }
+  // the caller's stream sees the record copies as part of the steps
   if (h->join_pending) {
     CK(h, cudaEventRecord(h->join_ev, h->copy_stream));
     CK(h, cudaStreamWaitEvent(h->stream, h->join_ev, 0));

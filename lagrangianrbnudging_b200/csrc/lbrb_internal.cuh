@@ -235,13 +235,9 @@ struct Handle {
   void* T[2] = {nullptr, nullptr};
   void* uv[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
   int uvcur = 0, uvprev = 1;
-  // second stream: particle kernels beside the fused kernel (when enabled) and
-  // the adjoint window's segment recompute; events order it against `stream`
+  // second stream: the adjoint window's segment recompute (events order it
+  // against `stream`)
   cudaStream_t pstream = nullptr;
-  cudaEvent_t ev_lb = nullptr;       // fused kernel of the last queued step done
-  cudaEvent_t ev_uv[3] = {nullptr, nullptr, nullptr};  // last particle kernel reading slot done
-  cudaEvent_t ev_T[2] = {nullptr, nullptr};            // last particle kernel reading T[b] done
-  cudaEvent_t ev_pjoin = nullptr;
   bool moments_valid = false;
   // particles (FP64)
   int np = 0;
