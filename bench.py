@@ -161,7 +161,7 @@ def init_run(r, seed: int):
     return m
 
 
-def timed_steps(r, torch, steps: int, warmup: int, dist, device: int, sampler=None, clock=None):
+def timed_steps(r, torch, steps: int, warmup: int, dist, device: int, clock=None):
     """W warm-up steps, then the timed region: K steps as a user runs them
     (CUDA events around the region only, on the handle's stream).  Then the
     same K steps again with an event pair around every launch of the handle
