@@ -418,6 +418,52 @@ cudaError_t launch_slab_pack(const void* pops, bool fp32, int nx, int ny, int pi
   return cudaGetLastError();
 }
 
+// Ghost blocks of a y-slab for two steps per launch (SLAB_GH2_PLANES planes
+// of nx values): the neighbour's boundary row r1 -- its three f and three g
+// populations that cross into this slab (the one-step ghost layout), then its
+// k = 0, 1, 3 f and g, then its F -- and the three f and three g crossing
+// populations of the row r2 beyond it.  `up` goes to the slab above (r1, r2 =
+// rows ny-1, ny-2; k = 2, 5, 6 cross), `down` to the slab below (rows 0, 1;
+// k = 4, 7, 8).
+template <typename Real>
+__global__ void slab_pack2_kernel(const Real* __restrict__ pops, const Real* __restrict__ F, int nx, int ny,
+                                  int pitch, size_t plane, Real* __restrict__ up, Real* __restrict__ down) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = blockIdx.y;  // 0..18
+  if (x >= nx) return;
+  auto value = [&](bool upward) -> Real {
+    if (p == 12) return F[(size_t)(upward ? ny - 1 : 0) * pitch + x];
+    const bool beyond = p >= 13;
+    int q = beyond ? p - 13 : p;
+    int k;
+    if (q < 6) {
+      const int m = q % 3;
+      k = upward ? (m == 0 ? 2 : (m == 1 ? 5 : 6)) : (m == 0 ? 4 : (m == 1 ? 7 : 8));
+    } else {
+      q -= 6;
+      const int m = q % 3;
+      k = m == 0 ? 0 : (m == 1 ? 1 : 3);
+    }
+    const int g = q / 3;  // 0: f, 1: g
+    const int row = upward ? (beyond ? ny - 2 : ny - 1) : (beyond ? 1 : 0);
+    return pops[((size_t)g * NPOP + k) * plane + (size_t)row * pitch + x];
+  };
+  up[(size_t)p * nx + x] = value(true);
+  down[(size_t)p * nx + x] = value(false);
+}
+
+cudaError_t launch_slab_pack2(const void* pops, const void* F, bool fp32, int nx, int ny, int pitch, size_t plane,
+                              void* up, void* down, cudaStream_t s) {
+  dim3 grid((nx + 127) / 128, SLAB_GH2_PLANES);
+  if (fp32)
+    slab_pack2_kernel<float><<<grid, 128, 0, s>>>((const float*)pops, (const float*)F, nx, ny, pitch, plane,
+                                                  (float*)up, (float*)down);
+  else
+    slab_pack2_kernel<double><<<grid, 128, 0, s>>>((const double*)pops, (const double*)F, nx, ny, pitch, plane,
+                                                   (double*)up, (double*)down);
+  return cudaGetLastError();
+}
+
 int red_blocks() { return RED_BLOCKS; }
 
 cudaError_t launch_stats(const void* rho, const void* u, const void* v, const void* T, bool fp32,

@@ -133,6 +133,7 @@ static void free_all(lbrb_t* h) {
   F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
   F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down); F(h->slab_own); F(h->slab_tab);
+  F(h->slab_gh2_lo); F(h->slab_gh2_hi); F(h->slab_up2); F(h->slab_down2);
   for (cudaGraphExec_t& g : h->graph_exec)
     if (g) cudaGraphExecDestroy(g);
   if (h->slab_ev_xfer) cudaEventDestroy(h->slab_ev_xfer);
@@ -1299,19 +1300,25 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
     return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls, no box nudging");
   CK(h, cudaSetDevice(h->dev));
   const size_t gb = lbrb_slab_ghost_bytes(h);
-  void** bufs[] = {&h->slab_ghost_lo, &h->slab_ghost_hi, &h->slab_up, &h->slab_down};
+  const size_t gb2 = (size_t)SLAB_GH2_PLANES * h->p.nx * h->esize;
+  void** bufs[] = {&h->slab_ghost_lo, &h->slab_ghost_hi, &h->slab_up, &h->slab_down,
+                   &h->slab_gh2_lo, &h->slab_gh2_hi, &h->slab_up2, &h->slab_down2};
   for (void** b : bufs) {
     if (*b) cudaFree(*b);
     *b = nullptr;
   }
   // ghost rows only across inner boundaries (none at a wall of the domain)
-  if (j0 > 0 && cudaMalloc(&h->slab_ghost_lo, gb) != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "slab ghosts");
-  if (j0 + h->p.ny < ny_total && cudaMalloc(&h->slab_ghost_hi, gb) != cudaSuccess)
+  const bool lo = j0 > 0, hi = j0 + h->p.ny < ny_total;
+  if ((lo && (cudaMalloc(&h->slab_ghost_lo, gb) != cudaSuccess || cudaMalloc(&h->slab_gh2_lo, gb2) != cudaSuccess)) ||
+      (hi && (cudaMalloc(&h->slab_ghost_hi, gb) != cudaSuccess || cudaMalloc(&h->slab_gh2_hi, gb2) != cudaSuccess)))
     return fail(h, LBRB_ERR_NOMEM, "slab ghosts");
-  if (cudaMalloc(&h->slab_up, gb) != cudaSuccess || cudaMalloc(&h->slab_down, gb) != cudaSuccess)
+  if (cudaMalloc(&h->slab_up, gb) != cudaSuccess || cudaMalloc(&h->slab_down, gb) != cudaSuccess ||
+      cudaMalloc(&h->slab_up2, gb2) != cudaSuccess || cudaMalloc(&h->slab_down2, gb2) != cudaSuccess)
     return fail(h, LBRB_ERR_NOMEM, "slab boundary rows");
   for (void* b : {h->slab_ghost_lo, h->slab_ghost_hi, h->slab_up, h->slab_down})
     if (b) CK(h, cudaMemsetAsync(b, 0, gb, h->stream));
+  for (void* b : {h->slab_gh2_lo, h->slab_gh2_hi, h->slab_up2, h->slab_down2})
+    if (b) CK(h, cudaMemsetAsync(b, 0, gb2, h->stream));
   if (!h->slab_ev_xfer) CK(h, cudaEventCreateWithFlags(&h->slab_ev_xfer, cudaEventDisableTiming));
   if (!h->slab_ev_done) CK(h, cudaEventCreateWithFlags(&h->slab_ev_done, cudaEventDisableTiming));
   if (h->np > 0) {
@@ -1501,7 +1508,118 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
     if (rc) return rc;
   }
   const size_t gb = lbrb_slab_ghost_bytes(h0);
+  const size_t gb2 = (size_t)SLAB_GH2_PLANES * h0->p.nx * h0->esize;
+  // two steps per launch: Dirichlet walls, no nudging, never the call's last
+  // step (which writes the moments)
+  bool slab_pairs = !nudge && h0->p.twall == LBRB_TWALL_DIRICHLET;
+  for (int s = 0; s < n; s++) slab_pairs = slab_pairs && slabs[s]->pair_mode != 0;
+  // Two steps of every slab: the ghost blocks (two rows deep) go across each
+  // inner boundary, then each slab runs lb_pair_kernel, whose ring rows beyond
+  // an inner boundary come from them; then the particles, step by step.
+  auto pair_iteration = [&]() -> int {
+    const int i1 = h0->istep + 1, i2 = h0->istep + 2;
+    const bool rec1 = parts && h0->p.noutconfig > 0 && i1 % h0->p.noutconfig == 0;
+    const bool rec2 = parts && h0->p.noutconfig > 0 && i2 % h0->p.noutconfig == 0;
+    for (int s = 0; s < n; s++) {
+      lbrb_t* h = slabs[s];
+      CK(h, cudaSetDevice(h->dev));
+      if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_done, 0));
+      if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_done, 0));
+      CK(h, launch_slab_pack2(h->pops[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane,
+                              h->slab_up2, h->slab_down2, h->stream));
+      if (s + 1 < n)
+        CK(h, cudaMemcpyPeerAsync(slabs[s + 1]->slab_gh2_lo, slabs[s + 1]->dev, h->slab_up2, h->dev, gb2, h->stream));
+      if (s > 0)
+        CK(h, cudaMemcpyPeerAsync(slabs[s - 1]->slab_gh2_hi, slabs[s - 1]->dev, h->slab_down2, h->dev, gb2, h->stream));
+      CK(h, cudaEventRecord(h->slab_ev_xfer, h->stream));
+    }
+    for (int s = 0; s < n; s++) {
+      lbrb_t* h = slabs[s];
+      CK(h, cudaSetDevice(h->dev));
+      if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_xfer, 0));
+      if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_xfer, 0));
+      const int src = h->cur, dst = h->cur ^ 1;
+      const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;
+      const int B = parts ? h->uvprev : h->uvcur;
+      const int wuv = parts ? 1 : 0;
+      auto views = [&](auto zero, int r1, int r2) {
+        using Real = decltype(zero);
+        LBView<Real> V1 = make_view<Real>(h, src, dst, A, wuv, r1), V2 = make_view<Real>(h, dst, dst, B, wuv, r2);
+        V1.T = (Real*)h->T[src];
+        V1.rho = (Real*)h->rho[src];
+        for (LBView<Real>* V : {&V1, &V2}) {
+          V->ghost_lo = V->gh2_lo = (const Real*)h->slab_gh2_lo;
+          V->ghost_hi = V->gh2_hi = (const Real*)h->slab_gh2_hi;
+        }
+        return std::make_pair(V1, V2);
+      };
+      if (h->pair_shape < 0) {
+        float ms = 0.f;
+        if (fp32(h)) {
+          auto v = views(0.f, 0, 0);
+          h->pair_shape = tune_pair_fp32(v.first, v.second, h->stream, &ms);
+        } else {
+          auto v = views(0.0, 0, 0);
+          h->pair_shape = tune_pair_fp64(v.first, v.second, h->stream, &ms);
+        }
+        CK(h, cudaGetLastError());
+        h->pair_ms = ms;
+      }
+      const int tm = tmark_begin(h, 0, h->stream);
+      if (fp32(h)) {
+        auto v = views(0.f, rec1 ? 1 : 0, rec2 ? 1 : 0);
+        CK(h, launch_pair_fp32(v.first, v.second, h->pair_shape, h->stream, false));
+      } else {
+        auto v = views(0.0, rec1 ? 1 : 0, rec2 ? 1 : 0);
+        CK(h, launch_pair_fp64(v.first, v.second, h->pair_shape, h->stream, false));
+      }
+      tmark_end(h, tm, h->stream);
+      CK(h, cudaEventRecord(h->slab_ev_done, h->stream));
+    }
+    // the particles of each step, with each handle's buffer state set to that
+    // step's (u^n in slot A, T^n in the source buffer)
+    for (int q = 0; q < 2; q++) {
+      for (int s = 0; s < n; s++) {
+        lbrb_t* h = slabs[s];
+        if (q == 0) {
+          // after step n: T^n in the source buffer, u^n in the free slot
+          h->pair_save[0] = h->cur, h->pair_save[1] = h->uvcur, h->pair_save[2] = h->uvprev;
+          if (parts) {
+            const int A = 3 - h->uvcur - h->uvprev;
+            h->uvprev = h->uvcur;
+            h->uvcur = A;
+          }
+          h->istep = i1;
+        } else {
+          // after step n+1: populations and T in the other buffer, u^{n+1}
+          // in the slot of u^{n-2}
+          h->cur = h->pair_save[0] ^ 1;
+          if (parts) {
+            h->uvprev = h->uvcur;
+            h->uvcur = h->pair_save[2];
+          }
+          h->istep = i2;
+        }
+      }
+      if (parts) {
+        const int rc = slab_particles(slabs, n);
+        if (rc) return rc;
+      }
+    }
+    for (int s = 0; s < n; s++) slabs[s]->prev_valid = false;
+    return LBRB_OK;
+  };
   for (int it = 0; it < nsteps; it++) {
+    if (slab_pairs && nsteps - it >= 3) {
+      int need = 0;
+      for (int q = 1; q <= 2; q++) need += parts && h0->p.noutconfig > 0 && (h0->istep + q) % h0->p.noutconfig == 0;
+      if (h0->rec_head - h0->rec_tail + need <= h0->p.record_slots) {
+        const int rc = pair_iteration();
+        if (rc) return rc;
+        it++;  // (and the loop's own increment)
+        continue;
+      }
+    }
     if (parts && h0->p.noutconfig > 0 && (h0->istep + 1) % h0->p.noutconfig == 0 &&
         h0->rec_head - h0->rec_tail >= h0->p.record_slots)
       return fail(h0, LBRB_ERR_OVERFLOW, "slab_step: record ring full, drain records first");

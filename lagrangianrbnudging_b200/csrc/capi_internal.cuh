@@ -81,6 +81,9 @@ cudaError_t launch_init_conduction(void* pops, void* rho, void* u, void* v, void
                                    int nx, int ny, int pitch, size_t plane, double Tup,
                                    double Tdown, double T0, double neg_gravity, uint64_t seed,
                                    double noise, int j0, int ny_total, cudaStream_t s);
+// ghost blocks of SLAB_GH2_PLANES rows for two steps per launch
+cudaError_t launch_slab_pack2(const void* pops, const void* F, bool fp32, int nx, int ny, int pitch, size_t plane,
+                              void* up, void* down, cudaStream_t s);
 cudaError_t launch_slab_pack(const void* pops, bool fp32, int nx, int ny, int pitch, size_t plane, void* up,
                              void* down, cudaStream_t s);
 cudaError_t launch_stats(const void* rho, const void* u, const void* v, const void* T, bool fp32,

@@ -78,6 +78,41 @@ __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V)
 // ring is recomputed (34 x 10 nodes for a 32 x 8 tile).  The per-node
 // arithmetic is lb_update_node's, so two steps here equal two launches of
 // lb_node_kernel bit for bit.
+// On a y-slab, the ring row outside the slab (row -1 or ny) is the
+// neighbour's boundary row r1: its populations of step n-1 come from the
+// ghost block (SLAB_GH2_PLANES planes: r1's crossing populations, its k = 0,
+// 1, 3, its F, then the crossing populations of the row r2 beyond), except
+// those it pulls from this slab's own boundary row.  Neither r1 nor r2 is a
+// wall row (slabs hold at least three rows).
+template <typename Real, typename Off>
+__device__ __forceinline__ void pull_ghost_row(const LBView<Real>& V, bool lo, int x, Real* fs, Real* gs, Real& Fy) {
+  const Real* G = lo ? V.gh2_lo : V.gh2_hi;
+  const int nx = V.nx;
+  const int xl = (x == 0) ? nx - 1 : x - 1, xr = (x == nx - 1) ? 0 : x + 1;
+  const Off pl = (Off)V.plane, own = (Off)(lo ? 0 : V.ny - 1) * (Off)V.pitch;
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : x);
+    if constexpr (icy(k) == 0) {
+      constexpr int m = k == 0 ? 0 : (k == 1 ? 1 : 2);
+      fs[k] = G[(size_t)(6 + m) * nx + xs];
+      gs[k] = G[(size_t)(9 + m) * nx + xs];
+    } else {
+      // from this slab's boundary row (k moving away from it), else from r2
+      const bool from_own = lo ? icy(k) == -1 : icy(k) == 1;
+      constexpr int slot = (k == 2 || k == 4) ? 0 : ((k == 5 || k == 7) ? 1 : 2);
+      if (from_own) {
+        fs[k] = V.fsrc[(Off)k * pl + own + (Off)xs];
+        gs[k] = V.gsrc[(Off)k * pl + own + (Off)xs];
+      } else {
+        fs[k] = G[(size_t)(13 + slot) * nx + xs];
+        gs[k] = G[(size_t)(16 + slot) * nx + xs];
+      }
+    }
+  });
+  Fy = G[(size_t)12 * nx + x];
+}
+
 // NT threads per block: TX * TY (phase 1 takes the region in passes), or
 // one per region node rounded to whole warps (phase 1 in one pass; phase 2
 // leaves the rest idle)
@@ -92,18 +127,25 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int ncols = min(TX, nx - x0), nrows = min(TY, ny - y0);
   const Off pitch = (Off)V1.pitch;
+  // y-slab: the rows beyond an inner boundary are computed from ghost blocks
+  const bool glo = V1.gh2_lo != nullptr, ghi = V1.gh2_hi != nullptr;
   for (int q = threadIdx.x; q < RN; q += NT) {
     const int lx = q % RX, ly = q / RX;
     const int jg = y0 - 1 + ly;
-    if (lx > ncols + 1 || ly > nrows + 1 || jg < 0 || jg >= ny) continue;
+    if (lx > ncols + 1 || ly > nrows + 1 || jg < (glo ? -1 : 0) || jg > (ghi ? ny : ny - 1)) continue;
     int xg = x0 - 1 + lx;
     if (xg < 0) xg += nx;
     else if (xg >= nx) xg -= nx;
     Real fs[NPOP], gs[NPOP];
-    pull_node<Real, LBRB_TWALL_DIRICHLET, Off, true>(V1, jg, xg, fs, gs);
-    dirichlet_walls(V1, jg, gs);
-    const Off o = (Off)jg * pitch + (Off)xg;
-    Real Fy = V1.Fin[o], r, u, v, t;
+    Real Fy, r, u, v, t;
+    const Off o = (Off)(jg < 0 ? 0 : (jg >= ny ? ny - 1 : jg)) * pitch + (Off)xg;  // (ring rows of a slab: no stores)
+    if (jg < 0 || jg >= ny) {
+      pull_ghost_row<Real, Off>(V1, jg < 0, xg, fs, gs, Fy);
+    } else {
+      pull_node<Real, LBRB_TWALL_DIRICHLET, Off, true>(V1, jg, xg, fs, gs);
+      dirichlet_walls(V1, jg, gs);
+      Fy = V1.Fin[o];
+    }
     lb_collide<Real, false>(
         V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { S[(k * RY + ly) * RX + lx] = val; },
         [&](int k, Real val) { S[((NPOP + k) * RY + ly) * RX + lx] = val; });
@@ -127,7 +169,7 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
   static_for<NPOP>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     const int js = j - icy(k);
-    if (js < 0 || js >= ny) {
+    if ((js < 0 && !glo) || (js >= ny && !ghi)) {
       fs[k] = S[(opp(k) * RY + ty + 1) * RX + tx + 1];
       gs[k] = Real(0);
     } else {

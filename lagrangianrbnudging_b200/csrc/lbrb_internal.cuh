@@ -55,6 +55,9 @@ inline bool off32_ok(size_t plane) { return plane * 2 * NPOP < (size_t(1) << 32)
 
 // tile shapes of the two-step kernel (lb_kernels.cu: PAIR_SHAPES)
 constexpr int NUM_PAIR_SHAPES = 9;
+// planes (of nx values) of a y-slab's ghost block for two steps per launch
+// (aux_kernels.cu: slab_pack2_kernel)
+constexpr int SLAB_GH2_PLANES = 19;
 
 // Programmatic dependent launch: a kernel launched with the attribute may
 // start while the kernel before it in the stream finishes; it waits here,
@@ -168,6 +171,10 @@ struct LBView {
   // f then g of the three populations crossing the boundary; null = wall
   const Real* __restrict__ ghost_lo;
   const Real* __restrict__ ghost_hi;
+  // lb_pair_kernel on a y-slab: SLAB_GH2_PLANES-plane ghost blocks (null at a
+  // wall); their first six planes are the one-step ghost rows above
+  const Real* __restrict__ gh2_lo;
+  const Real* __restrict__ gh2_hi;
 };
 
 // --------------------------------------------------------------- handle
@@ -193,6 +200,12 @@ struct Handle {
   int slab_j0 = 0, slab_ny_total = 0;
   void* slab_ghost_lo = nullptr;
   void* slab_ghost_hi = nullptr;
+  // ghost blocks for two steps per launch (SLAB_GH2_PLANES rows) and the
+  // packed boundary rows sent to the neighbours
+  void* slab_gh2_lo = nullptr;
+  void* slab_gh2_hi = nullptr;
+  void* slab_up2 = nullptr;
+  void* slab_down2 = nullptr;
   void* slab_up = nullptr;
   void* slab_down = nullptr;
   cudaEvent_t slab_ev_xfer = nullptr, slab_ev_done = nullptr;
@@ -218,6 +231,7 @@ struct Handle {
   int pair_mode = -1;
   int pair_shape = -1;
   float pair_ms = 0.f;
+  int pair_save[3] = {0, 0, 0};  // y-slab pairs: cur, uvcur, uvprev before the launch
   int graph_mode = -1;
   size_t esize = 8;   // bytes per population value
   // populations: pops[buf] holds f (9 planes) then g (9 planes)
