@@ -357,6 +357,9 @@ LBRB_API int lbrb_slab_pack(lbrb_t *h);
  * several GPUs), slabs in order of j0: per step, every slab packs and copies
  * its boundary rows into its neighbours' ghost rows (peer copies across
  * GPUs), then steps; events order the copies against the neighbours' steps.
+ * Without nudging, steps go two per launch (as lbrb_set_pairs describes;
+ * a slab's lbrb_set_pairs(h, 0) turns it off): the exchange is then two rows
+ * deep and goes every two steps; results are the same bit for bit.
  * The moments (rho, u, v, T) are written on the last of the nsteps.
  * With particles (the reference advances each rank's own particles,
  * propagate_prtcl at Trajectories/code/mympi2.h:350, and hands those that
