@@ -353,6 +353,18 @@ LBRB_API size_t lbrb_slab_ghost_bytes(const lbrb_t *h);
  * of lbrb_slab_ghost_bytes on the handle's stream), then lbrb_step(h, 1). */
 LBRB_API int lbrb_slab_buffers(lbrb_t *h, void **up, void **down, void **ghost_lo, void **ghost_hi);
 LBRB_API int lbrb_slab_pack(lbrb_t *h);
+/* Two steps per exchange (one process per GPU; no particles, no nudging):
+ * lbrb_slab_pack2 packs two-row ghost blocks of lbrb_slab_ghost2_bytes
+ * (the boundary row: its three f and three g populations that cross, its
+ * k = 0, 1, 3 f and g, its F; then the three f and three g crossing
+ * populations of the next row in); send `up` to the slab above's ghost_lo
+ * and `down` to the slab below's ghost_hi (lbrb_slab_buffers2), then
+ * lbrb_step(h, 2) advances two steps in one launch, bit-identical to two
+ * one-step exchanges.  Its second step writes the moments; the post-stream
+ * populations of the first are not kept (lbrb_get_poststream). */
+LBRB_API size_t lbrb_slab_ghost2_bytes(const lbrb_t *h);
+LBRB_API int lbrb_slab_buffers2(lbrb_t *h, void **up, void **down, void **ghost_lo, void **ghost_hi);
+LBRB_API int lbrb_slab_pack2(lbrb_t *h);
 /* nsteps steps of a whole domain whose slabs this process holds (one or
  * several GPUs), slabs in order of j0: per step, every slab packs and copies
  * its boundary rows into its neighbours' ghost rows (peer copies across

@@ -45,6 +45,7 @@ EXPORTS = [
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
+    "lbrb_slab_ghost2_bytes", "lbrb_slab_buffers2", "lbrb_slab_pack2",
     "lbrb_set_graph", "lbrb_set_pairs", "lbrb_set_pair_shape", "lbrb_get_pair_shape",
 ]
 
@@ -134,6 +135,9 @@ def lib() -> C.CDLL:
         "lbrb_slab_ghost_bytes": (C.c_size_t, [vp]),
         "lbrb_slab_buffers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
         "lbrb_slab_pack": (C.c_int, [vp]),
+        "lbrb_slab_ghost2_bytes": (C.c_size_t, [vp]),
+        "lbrb_slab_buffers2": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "lbrb_slab_pack2": (C.c_int, [vp]),
         "lbrb_slab_step": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int]),
         "lbrb_set_graph": (C.c_int, [vp, C.c_int]),
         "lbrb_set_pairs": (C.c_int, [vp, C.c_int]),

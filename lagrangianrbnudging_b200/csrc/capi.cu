@@ -617,12 +617,29 @@ static bool pairs_ok(const lbrb_t* h) {
   return h->pair_mode != 0 && h->p.twall == LBRB_TWALL_DIRICHLET && h->p.nudge == LBRB_NUDGE_NONE && !h->slab;
 }
 
+static int slab_pair_launch(lbrb_t* h, bool rec1, bool rec2, bool last);  // (y-slabs, below)
+
 int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
   if (n == 0) return LBRB_OK;
+  if (h->slab && !h->slab_stepping && n == 2 && h->np == 0 && h->p.nudge == LBRB_NUDGE_NONE &&
+      h->p.twall == LBRB_TWALL_DIRICHLET && h->pair_mode != 0) {
+    // one process per GPU: two steps from the two-row ghost blocks
+    // (lbrb_slab_pack2 and the exchange of lbrb_slab_buffers2 done)
+    if (!h->moments_valid)
+      return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
+    CK(h, cudaSetDevice(h->dev));
+    const int rc = slab_pair_launch(h, false, false, true);
+    if (rc) return rc;
+    h->cur ^= 1;
+    h->istep += 2;
+    h->prev_valid = false;
+    return LBRB_OK;
+  }
   if (h->slab && (n != 1 || ((h->np > 0 || h->p.nudge != LBRB_NUDGE_NONE) && !h->slab_stepping)))
-    return fail(h, LBRB_ERR_ARG, "step: a y-slab takes one step per boundary exchange (lbrb_slab_step)");
+    return fail(h, LBRB_ERR_ARG,
+                "step: a y-slab takes one step per boundary exchange, or two after lbrb_slab_pack2 (lbrb_slab_step)");
   if (!h->moments_valid)
     return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
   if (h->np > 0 && !h->particles_set) return fail(h, LBRB_ERR_STATE, "step: particles not set");
@@ -1335,6 +1352,27 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
 
 size_t lbrb_slab_ghost_bytes(const lbrb_t* h) { return h ? 6 * (size_t)h->p.nx * h->esize : 0; }
 
+size_t lbrb_slab_ghost2_bytes(const lbrb_t* h) { return h ? (size_t)SLAB_GH2_PLANES * h->p.nx * h->esize : 0; }
+
+int lbrb_slab_buffers2(lbrb_t* h, void** up, void** down, void** ghost_lo, void** ghost_hi) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->slab) return fail(h, LBRB_ERR_STATE, "slab_buffers2: not a y-slab (lbrb_slab_set)");
+  if (up) *up = h->slab_up2;
+  if (down) *down = h->slab_down2;
+  if (ghost_lo) *ghost_lo = h->slab_gh2_lo;
+  if (ghost_hi) *ghost_hi = h->slab_gh2_hi;
+  return LBRB_OK;
+}
+
+int lbrb_slab_pack2(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->slab) return fail(h, LBRB_ERR_STATE, "slab_pack2: not a y-slab (lbrb_slab_set)");
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, launch_slab_pack2(h->pops[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->slab_up2,
+                          h->slab_down2, h->stream));
+  return LBRB_OK;
+}
+
 int lbrb_slab_buffers(lbrb_t* h, void** up, void** down, void** ghost_lo, void** ghost_hi) {
   if (!h) return LBRB_ERR_ARG;
   if (!h->slab) return fail(h, LBRB_ERR_STATE, "slab_buffers: not a y-slab (lbrb_slab_set)");
@@ -1351,6 +1389,54 @@ int lbrb_slab_pack(lbrb_t* h) {
   CK(h, cudaSetDevice(h->dev));
   CK(h, launch_slab_pack(h->pops[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->slab_up,
                          h->slab_down, h->stream));
+  return LBRB_OK;
+}
+
+// One two-step launch of a y-slab from its two-row ghost blocks (filled by
+// the neighbours' lbrb_slab_pack2), records of the steps as flagged; `last`:
+// the second step writes the moments (it ends the call).  Buffers as two
+// one-step launches leave them; the caller updates the handle's state.
+static int slab_pair_launch(lbrb_t* h, bool rec1, bool rec2, bool last) {
+  const bool parts = h->np > 0;
+  const int src = h->cur, dst = h->cur ^ 1;
+  const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;
+  const int B = parts ? h->uvprev : h->uvcur;
+  const int wuv = parts ? 1 : 0;
+  auto views = [&](auto zero, int r1, int r2, int w2) {
+    using Real = decltype(zero);
+    LBView<Real> V1 = make_view<Real>(h, src, dst, A, wuv, r1), V2 = make_view<Real>(h, dst, dst, B, w2, r2);
+    V1.T = (Real*)h->T[src];
+    V1.rho = (Real*)h->rho[src];
+    for (LBView<Real>* V : {&V1, &V2}) {
+      V->ghost_lo = V->gh2_lo = (const Real*)h->slab_gh2_lo;
+      V->ghost_hi = V->gh2_hi = (const Real*)h->slab_gh2_hi;
+    }
+    return std::make_pair(V1, V2);
+  };
+  if (h->pair_shape < 0) {
+    // the tile shape, timed on first use (trial launches write only what the
+    // two steps overwrite)
+    float ms = 0.f;
+    if (fp32(h)) {
+      auto v = views(0.f, 0, 0, wuv);
+      h->pair_shape = tune_pair_fp32(v.first, v.second, h->stream, &ms);
+    } else {
+      auto v = views(0.0, 0, 0, wuv);
+      h->pair_shape = tune_pair_fp64(v.first, v.second, h->stream, &ms);
+    }
+    CK(h, cudaGetLastError());
+    h->pair_ms = ms;
+  }
+  const int r2 = last ? 3 : (rec2 ? 1 : 0), w2 = last ? 1 : wuv;
+  const int tm = tmark_begin(h, 0, h->stream);
+  if (fp32(h)) {
+    auto v = views(0.f, rec1 ? 1 : 0, r2, w2);
+    CK(h, launch_pair_fp32(v.first, v.second, h->pair_shape, h->stream, false));
+  } else {
+    auto v = views(0.0, rec1 ? 1 : 0, r2, w2);
+    CK(h, launch_pair_fp64(v.first, v.second, h->pair_shape, h->stream, false));
+  }
+  tmark_end(h, tm, h->stream);
   return LBRB_OK;
 }
 
@@ -1525,8 +1611,8 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
       CK(h, cudaSetDevice(h->dev));
       if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_done, 0));
       if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_done, 0));
-      CK(h, launch_slab_pack2(h->pops[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane,
-                              h->slab_up2, h->slab_down2, h->stream));
+      int rc = lbrb_slab_pack2(h);
+      if (rc) return rc;
       if (s + 1 < n)
         CK(h, cudaMemcpyPeerAsync(slabs[s + 1]->slab_gh2_lo, slabs[s + 1]->dev, h->slab_up2, h->dev, gb2, h->stream));
       if (s > 0)
@@ -1538,42 +1624,8 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
       CK(h, cudaSetDevice(h->dev));
       if (s > 0) CK(h, cudaStreamWaitEvent(h->stream, slabs[s - 1]->slab_ev_xfer, 0));
       if (s + 1 < n) CK(h, cudaStreamWaitEvent(h->stream, slabs[s + 1]->slab_ev_xfer, 0));
-      const int src = h->cur, dst = h->cur ^ 1;
-      const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;
-      const int B = parts ? h->uvprev : h->uvcur;
-      const int wuv = parts ? 1 : 0;
-      auto views = [&](auto zero, int r1, int r2) {
-        using Real = decltype(zero);
-        LBView<Real> V1 = make_view<Real>(h, src, dst, A, wuv, r1), V2 = make_view<Real>(h, dst, dst, B, wuv, r2);
-        V1.T = (Real*)h->T[src];
-        V1.rho = (Real*)h->rho[src];
-        for (LBView<Real>* V : {&V1, &V2}) {
-          V->ghost_lo = V->gh2_lo = (const Real*)h->slab_gh2_lo;
-          V->ghost_hi = V->gh2_hi = (const Real*)h->slab_gh2_hi;
-        }
-        return std::make_pair(V1, V2);
-      };
-      if (h->pair_shape < 0) {
-        float ms = 0.f;
-        if (fp32(h)) {
-          auto v = views(0.f, 0, 0);
-          h->pair_shape = tune_pair_fp32(v.first, v.second, h->stream, &ms);
-        } else {
-          auto v = views(0.0, 0, 0);
-          h->pair_shape = tune_pair_fp64(v.first, v.second, h->stream, &ms);
-        }
-        CK(h, cudaGetLastError());
-        h->pair_ms = ms;
-      }
-      const int tm = tmark_begin(h, 0, h->stream);
-      if (fp32(h)) {
-        auto v = views(0.f, rec1 ? 1 : 0, rec2 ? 1 : 0);
-        CK(h, launch_pair_fp32(v.first, v.second, h->pair_shape, h->stream, false));
-      } else {
-        auto v = views(0.0, rec1 ? 1 : 0, rec2 ? 1 : 0);
-        CK(h, launch_pair_fp64(v.first, v.second, h->pair_shape, h->stream, false));
-      }
-      tmark_end(h, tm, h->stream);
+      const int rc = slab_pair_launch(h, rec1, rec2, false);
+      if (rc) return rc;
       CK(h, cudaEventRecord(h->slab_ev_done, h->stream));
     }
     // the particles of each step, with each handle's buffer state set to that

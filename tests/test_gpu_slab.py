@@ -75,7 +75,7 @@ def test_slab_mode_rejects_what_it_does_not_cover():
         r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))
         r.init_conduction(1, 1e-3)
         with pytest.raises(lb.LbrbError):
-            r.step(2)  # one step per boundary exchange
+            r.step(3)  # one step, or two after lbrb_slab_pack2, per boundary exchange
     with lb.Run(**dict(params("fp32"), ny=24, twall="adiabatic")) as r:
         with pytest.raises(lb.LbrbError):
             r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # adiabatic walls are not covered
@@ -207,3 +207,68 @@ def test_slab_bilinear_nudging_matches_the_whole_domain(precision, npart):
                 seed_particles(free, npart, 8)
             free.step(65)
             assert not np.array_equal(free.get_moments()["T"], mw["T"])
+
+
+def cudart():
+    """the CUDA runtime, for device-to-device copies standing in for the
+    neighbour sends of one process per GPU"""
+    import ctypes as C
+    for name in ("/usr/local/cuda/lib64/libcudart.so", "libcudart.so", "libcudart.so.12"):
+        try:
+            L = C.CDLL(name)
+            break
+        except OSError:
+            continue
+    L.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    L.cudaMemcpy.restype = C.c_int
+    return L
+
+
+def exchange(dom, two):
+    """what each rank of one process per GPU does: pack its boundary rows,
+    then send `up` to the slab above's ghost_lo and `down` to the slab
+    below's ghost_hi (here copies between handles of one process)"""
+    import ctypes as C
+    L, rt = lb.lib(), cudart()
+    pack = L.lbrb_slab_pack2 if two else L.lbrb_slab_pack
+    bufs_of = L.lbrb_slab_buffers2 if two else L.lbrb_slab_buffers
+    nbytes = (L.lbrb_slab_ghost2_bytes if two else L.lbrb_slab_ghost_bytes)(dom.slabs[0].h)
+    bufs = []
+    for r in dom.slabs:
+        r._ck(pack(r.h))
+        b = [C.c_void_p() for _ in range(4)]  # up, down, ghost_lo, ghost_hi
+        r._ck(bufs_of(r.h, *[C.byref(x) for x in b]))
+        bufs.append(b)
+    for r in dom.slabs:
+        r.sync()
+    n = len(dom.slabs)
+    for s in range(n):
+        if s + 1 < n:
+            assert rt.cudaMemcpy(bufs[s + 1][2], bufs[s][0], nbytes, 3) == 0
+        if s > 0:
+            assert rt.cudaMemcpy(bufs[s - 1][3], bufs[s][1], nbytes, 3) == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_one_process_per_gpu_exchange(precision):
+    """the exchange a rank does over NCCL, done here with copies: one step per
+    exchange (lbrb_slab_pack, lbrb_step(h, 1)) and two steps per exchange
+    (lbrb_slab_pack2, lbrb_step(h, 2)) both give the whole domain's state"""
+    with lb.Run(**params(precision)) as whole, lb.SlabDomain((20, 17, 11), **params(precision)) as dom:
+        whole.init_conduction(19, 3e-2)
+        dom.init_conduction(19, 3e-2)
+        for two, calls in ((False, 9), (True, 12), (False, 3), (True, 5)):
+            for _ in range(calls):
+                exchange(dom, two)
+                for r in dom.slabs:
+                    r.step(2 if two else 1)
+            whole.step(calls * (2 if two else 1))
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+            mw, ms = whole.get_moments(), dom.get_moments()
+            for k in ("rho", "u", "v", "T"):
+                np.testing.assert_array_equal(ms[k], mw[k])
+        with pytest.raises(lb.LbrbError):
+            dom.slabs[0].step(3)  # one or two steps per exchange
