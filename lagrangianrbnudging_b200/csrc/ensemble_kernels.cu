@@ -20,6 +20,8 @@
 // The three kernels are launched with programmatic dependent launch (also
 // inside the ensemble's CUDA graph) and wait for the previous phase before
 // touching memory, so each launch overlaps only the previous one's drain.
+#include <atomic>
+
 #include "capi_internal.cuh"
 #include "ensemble.cuh"
 #include "lb_node.cuh"
@@ -121,11 +123,13 @@ static cudaError_t ens_lb_launch(const LBView<Real>* views, const int4* items, i
   if (SCHED != 0) {
     // resident blocks per SM of this variant, queried once (outside any
     // stream capture: the first launch of a variant is a tuning or direct one)
-    static int per = 0;
+    static std::atomic<int> per_cached{0};  // (the same on every device of one model)
+    int per = per_cached.load(std::memory_order_relaxed);
     if (per <= 0) {
       cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, BS, 0);
       if (e != cudaSuccess) return e;
       if (per <= 0) return cudaErrorInvalidConfiguration;
+      per_cached.store(per, std::memory_order_relaxed);
     }
     grid = std::max(1, std::min(nitems, per * nsm));
   }

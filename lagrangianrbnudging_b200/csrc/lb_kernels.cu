@@ -30,6 +30,7 @@
 // of two buffers, so a launch is a pure function of its sources: the launch
 // shape (block size, blocks per SM) is picked by timing the candidates on the
 // run's own grid (tune_lb).
+#include <atomic>
 #include <cstdlib>
 #include <type_traits>
 
@@ -195,11 +196,16 @@ static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2,
   const size_t smem = ((size_t)2 * NPOP * (TX + 2) * (TY + 2) + (size_t)TX * TY) * sizeof(Real);
   dim3 grid((V1.nx + TX - 1) / TX, (V1.ny + TY - 1) / TY);
   auto go = [&](auto kernel) -> cudaError_t {
-    static bool attr = false;  // (per instantiation)
-    if (!attr) {
+    // the shared-memory limit is a per-device attribute of the kernel: set
+    // once per device (one bit per device ordinal, per instantiation)
+    static std::atomic<unsigned long long> attr_set{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load(std::memory_order_relaxed) & bit)) {
       const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
-      attr = true;
+      attr_set.fetch_or(bit, std::memory_order_relaxed);
     }
     return launch_k(kernel, grid, NT, smem, s, pdl, V1, V2);
   };
