@@ -385,6 +385,9 @@ LBRB_API int lbrb_slab_pack2(lbrb_t *h);
  * With bilinear nudging, after every slab's step each slab scatters the
  * innovations of the observations to the cell corners in its own rows
  * (order-free fixed-point sums, so g is the whole domain's bit for bit). */
+/* Errors: a bad slab list is rejected before any launch; an error during
+ * the steps (a full record ring is checked first, so it is not one) leaves
+ * the slabs possibly at different steps: set their state again. */
 LBRB_API int lbrb_slab_step(lbrb_t *const *slabs, int nslabs, int nsteps);
 
 #ifdef __cplusplus
