@@ -315,8 +315,12 @@ LBRB_API int lbrb_ensemble_get_timing(lbrb_ensemble_t *e, double *ms, int *launc
  * row records, so ny above that is rejected with LBRB_ERR_RANGE.  Work runs
  * on `cuda_stream` (NULL: the default stream) and the call returns after it
  * finishes.  Calls share the scratch array: calls that overlap on the GPU
- * race.  The first call on a device looks up the array's address; make it
- * before any stream capture. */
+ * race.  The first call on a device looks up the array's address, which
+ * loads this library's device code on that device (with CUDA's default lazy
+ * module loading) and with it the 768 KiB array: make that first call at
+ * start-up, before memory runs short and before any stream capture; later
+ * calls take no device memory.  Only nx <= pitch is checked: each field must
+ * hold ny * pitch elements, which a device pointer does not reveal. */
 #define LBRB_STATS_NOALLOC_MAX_ROWS 16384
 LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, const void *T,
                                 int precision, int nx, int ny, int pitch, double relaxg,
@@ -361,7 +365,10 @@ LBRB_API int lbrb_slab_pack(lbrb_t *h);
  * and `down` to the slab below's ghost_hi (lbrb_slab_buffers2), then
  * lbrb_step(h, 2) advances two steps in one launch, bit-identical to two
  * one-step exchanges.  Its second step writes the moments; the post-stream
- * populations of the first are not kept (lbrb_get_poststream). */
+ * populations of the first are not kept (lbrb_get_poststream).
+ * lbrb_step(h, 2) returns LBRB_ERR_STATE unless lbrb_slab_pack2 ran on the
+ * slab since its last step (a one-step lbrb_slab_pack clears that mark); the
+ * exchange itself is the caller's and cannot be checked here. */
 LBRB_API size_t lbrb_slab_ghost2_bytes(const lbrb_t *h);
 LBRB_API int lbrb_slab_buffers2(lbrb_t *h, void **up, void **down, void **ghost_lo, void **ghost_hi);
 LBRB_API int lbrb_slab_pack2(lbrb_t *h);

@@ -662,8 +662,9 @@ template <typename Real, int TX, int TY, int NT, int MINB>
 static cudaError_t launch_pair_t(const AdjPairView<Real>& P, cudaStream_t s) {
   constexpr int NH = (TX + 2) * (TY + 2);
   constexpr size_t smem = (size_t)(2 * NPOP + 1) * NH * sizeof(double);
-  static cudaError_t attr = cudaFuncSetAttribute(adjoint_pair_kernel<Real, TX, TY, NT, MINB>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static std::atomic<unsigned long long> attr_set{0};
+  const cudaError_t attr =
+      smem_limit_once((const void*)adjoint_pair_kernel<Real, TX, TY, NT, MINB>, smem, attr_set);
   if (attr != cudaSuccess) return attr;
   dim3 grid((P.a.nx + TX - 1) / TX, (P.a.ny + TY - 1) / TY);
   return launch_k(adjoint_pair_kernel<Real, TX, TY, NT, MINB>, grid, NT, smem, s, true, P);
@@ -676,16 +677,15 @@ static cudaError_t launch_march_o(const AdjPairView<Real>& P, int waves, cudaStr
   constexpr int NT = 34 * RB;
   constexpr size_t smem = (size_t)(2 * NPOP + 1) * (2 * RB + 2) * 34 * sizeof(double);
   auto kern = adjoint_march_kernel<Real, RB, MINB, PRE, Off>;
-  static cudaError_t attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static std::atomic<unsigned long long> attr_set{0};
+  static std::atomic<int> occ_cache[MAX_DEVICES] = {};
+  const cudaError_t attr = smem_limit_once((const void*)kern, smem, attr_set);
   if (attr != cudaSuccess) return attr;
-  static int occ = 0;
-  if (occ == 0) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem);
-    if (e != cudaSuccess) return e;
-    if (occ < 1) return cudaErrorInvalidConfiguration;
-  }
+  int occ = 0;
+  cudaError_t e = occupancy_once((const void*)kern, NT, smem, occ_cache, &occ);
+  if (e != cudaSuccess) return e;
   int dev = 0, nsm = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = current_device(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
   const int nstrips = (P.a.nx + 31) / 32, ngroups = (P.a.ny + RB - 1) / RB;

@@ -629,9 +629,13 @@ int lbrb_step(lbrb_t* h, int n) {
     // (lbrb_slab_pack2 and the exchange of lbrb_slab_buffers2 done)
     if (!h->moments_valid)
       return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
+    if (!h->slab_gh2_packed)
+      return fail(h, LBRB_ERR_STATE,
+                  "step: two steps on a y-slab need lbrb_slab_pack2 and the ghost-block exchange first");
     CK(h, cudaSetDevice(h->dev));
     const int rc = slab_pair_launch(h, false, false, true);
     if (rc) return rc;
+    h->slab_gh2_packed = false;
     h->cur ^= 1;
     h->istep += 2;
     h->prev_valid = false;
@@ -933,6 +937,7 @@ int lbrb_step(lbrb_t* h, int n) {
     CK(h, cudaStreamWaitEvent(h->stream, h->join_ev, 0));
     h->join_pending = false;
   }
+  h->slab_gh2_packed = false;  // (a y-slab's two-row ghost blocks now lag its state)
   return LBRB_OK;
 }
 
@@ -1370,6 +1375,7 @@ int lbrb_slab_pack2(lbrb_t* h) {
   CK(h, cudaSetDevice(h->dev));
   CK(h, launch_slab_pack2(h->pops[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->slab_up2,
                           h->slab_down2, h->stream));
+  h->slab_gh2_packed = true;
   return LBRB_OK;
 }
 
@@ -1389,6 +1395,7 @@ int lbrb_slab_pack(lbrb_t* h) {
   CK(h, cudaSetDevice(h->dev));
   CK(h, launch_slab_pack(h->pops[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, h->slab_up,
                          h->slab_down, h->stream));
+  h->slab_gh2_packed = false;
   return LBRB_OK;
 }
 

@@ -123,14 +123,10 @@ static cudaError_t ens_lb_launch(const LBView<Real>* views, const int4* items, i
   if (SCHED != 0) {
     // resident blocks per SM of this variant, queried once (outside any
     // stream capture: the first launch of a variant is a tuning or direct one)
-    static std::atomic<int> per_cached{0};  // (the same on every device of one model)
-    int per = per_cached.load(std::memory_order_relaxed);
-    if (per <= 0) {
-      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, BS, 0);
-      if (e != cudaSuccess) return e;
-      if (per <= 0) return cudaErrorInvalidConfiguration;
-      per_cached.store(per, std::memory_order_relaxed);
-    }
+    static std::atomic<int> per_cached[MAX_DEVICES] = {};  // one entry per device ordinal
+    int per = 0;
+    const cudaError_t e = occupancy_once((const void*)k, BS, 0, per_cached, &per);
+    if (e != cudaSuccess) return e;
     grid = std::max(1, std::min(nitems, per * nsm));
   }
   if (nitems <= 0) return cudaSuccess;

@@ -199,14 +199,8 @@ static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2,
     // the shared-memory limit is a per-device attribute of the kernel: set
     // once per device (one bit per device ordinal, per instantiation)
     static std::atomic<unsigned long long> attr_set{0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (!(attr_set.load(std::memory_order_relaxed) & bit)) {
-      const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      attr_set.fetch_or(bit, std::memory_order_relaxed);
-    }
+    const cudaError_t e = smem_limit_once((const void*)kernel, smem, attr_set);
+    if (e != cudaSuccess) return e;
     return launch_k(kernel, grid, NT, smem, s, pdl, V1, V2);
   };
   // (FP64 holds twice the registers per value: half the blocks per SM)

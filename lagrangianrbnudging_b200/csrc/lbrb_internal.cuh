@@ -9,6 +9,7 @@
 // device node (x = i-1, y = j-1).  The reference's periodic halos (pbc,
 // communication) become index wrap.
 #pragma once
+#include <atomic>
 #include <utility>
 #include <vector>
 
@@ -64,6 +65,44 @@ constexpr int SLAB_GH2_PLANES = 19;
 // before touching memory, until that kernel has completed and its writes are
 // visible.  For a kernel launched without the attribute this returns at once.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Per-device caches (kernel attributes set once, occupancy queried once) keep
+// one entry per device ordinal below MAX_DEVICES; the current ordinal, checked.
+constexpr int MAX_DEVICES = 64;
+inline cudaError_t current_device(int* dev) {
+  const cudaError_t e = cudaGetDevice(dev);
+  if (e != cudaSuccess) return e;
+  return (*dev < 0 || *dev >= MAX_DEVICES) ? cudaErrorInvalidDevice : cudaSuccess;
+}
+// a kernel's dynamic shared-memory limit, set once per device: `bits` (one
+// static per kernel instantiation) holds a bit per ordinal already set
+inline cudaError_t smem_limit_once(const void* kernel, size_t smem, std::atomic<unsigned long long>& bits) {
+  int dev = 0;
+  cudaError_t e = current_device(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << dev;
+  if (bits.load(std::memory_order_relaxed) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  bits.fetch_or(bit, std::memory_order_relaxed);
+  return cudaSuccess;
+}
+// resident blocks per SM of a kernel launch shape, queried once per device
+// (`cache`: one static array per kernel instantiation)
+inline cudaError_t occupancy_once(const void* kernel, int threads, size_t smem, std::atomic<int>* cache, int* occ) {
+  int dev = 0;
+  cudaError_t e = current_device(&dev);
+  if (e != cudaSuccess) return e;
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (v < 1) return cudaErrorInvalidConfiguration;
+    cache[dev].store(v, std::memory_order_relaxed);
+  }
+  *occ = v;
+  return cudaSuccess;
+}
 
 // launch k<<<grid, block, smem, s>>>(args...), with programmatic dependent
 // launch when `pdl` (the kernel must call pdl_wait() first)
@@ -206,6 +245,9 @@ struct Handle {
   void* slab_gh2_hi = nullptr;
   void* slab_up2 = nullptr;
   void* slab_down2 = nullptr;
+  // lbrb_slab_pack2 ran since this slab's last step: lbrb_step(h, 2) may use
+  // the two-row ghost blocks (cleared by the step and by lbrb_slab_pack)
+  bool slab_gh2_packed = false;
   void* slab_up = nullptr;
   void* slab_down = nullptr;
   cudaEvent_t slab_ev_xfer = nullptr, slab_ev_done = nullptr;

@@ -19,8 +19,11 @@
 //    streams, no ordering between them) race on it and give wrong results;
 //  - each call rewrites every row record it reads, so nothing needs clearing;
 //  - the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    (cudaGetSymbolAddress) with that device current.  Under CUDA's default
+//    lazy module loading that lookup loads this library's device code, and
+//    the array with it, onto the device: the one moment the entry point
+//    takes device memory.  Make that first call at start-up, before memory
+//    runs short and before any stream capture.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -24,7 +24,9 @@ HERE = Path(__file__).resolve().parent
 SHIM = HERE / "shim"
 BUILD = HERE / "_build"
 REF_OUT = HERE / "_ref"
-REFERENCE_ROOT = Path(os.environ.get("LBRB_REFERENCE_ROOT", "/root/reference"))
+# the reference checkout: LBRB_REFERENCE_ROOT, else a checkout named
+# `reference` beside this repository
+REFERENCE_ROOT = Path(os.environ.get("LBRB_REFERENCE_ROOT", str(HERE.parent.parent / "reference")))
 
 CFLAGS = ["-std=c99", "-O2", "-ffp-contract=off", "-fPIC"]
 

@@ -247,6 +247,10 @@ def exchange(dom, two):
             assert rt.cudaMemcpy(bufs[s + 1][2], bufs[s][0], nbytes, 3) == 0
         if s > 0:
             assert rt.cudaMemcpy(bufs[s - 1][3], bufs[s][1], nbytes, 3) == 0
+    # a device-to-device cudaMemcpy may return before the copy ends, and the
+    # handles' streams do not wait for the legacy stream: finish the copies
+    # before any slab steps (a rank's NCCL recv on its stream orders this)
+    assert rt.cudaDeviceSynchronize() == 0
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
@@ -272,3 +276,9 @@ def test_one_process_per_gpu_exchange(precision):
                 np.testing.assert_array_equal(ms[k], mw[k])
         with pytest.raises(lb.LbrbError):
             dom.slabs[0].step(3)  # one or two steps per exchange
+        # two steps need this slab's lbrb_slab_pack2 since its last step
+        with pytest.raises(lb.LbrbError):
+            dom.slabs[0].step(2)
+        exchange(dom, False)  # a one-step pack does not count
+        with pytest.raises(lb.LbrbError):
+            dom.slabs[0].step(2)

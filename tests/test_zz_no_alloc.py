@@ -46,13 +46,19 @@ def test_stats_noalloc_matches_allocating_entry_points(precision, torch_dtype):
     # caller-owned device fields (allocated by the caller, not by the entry point)
     fields = [torch.tensor(m[k], dtype=dt, device="cuda").contiguous() for k in ("rho", "u", "v", "T")]
     stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
     for call in range(2):
         out = np.zeros(3)
+        # the first call on a device may load the library's device code (and
+        # the scratch array with it); a later call must take no device memory
+        free_before = torch.cuda.mem_get_info()[0]
         rc = lb.lib().lbrb_stats_noalloc(
             *[C.c_void_p(t.data_ptr()) for t in fields], lb.PREC[precision], nx, ny, nx,
             base["relaxg"], base["Tup"], base["Tdown"], C.c_void_p(stream),
             out.ctypes.data_as(C.POINTER(C.c_double)))
         assert rc == 0, (call, rc)
+        if call == 1:
+            assert torch.cuda.mem_get_info()[0] == free_before, "the call took device memory"
         assert _close(out[0], ke), (call, out[0], ke)
         assert _close(out[1], tm), (call, out[1], tm)
         assert _close(out[2], nu), (call, out[2], nu)
