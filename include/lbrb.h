@@ -239,7 +239,13 @@ LBRB_API int lbrb_energy(lbrb_t *h, double *ke_mean, double *t_mean);
 /* Volume Nusselt number 1 + <vT> ny / (kappa (Tdown-Tup)), kappa = (relaxg-1/2)/3. */
 LBRB_API int lbrb_nusselt(lbrb_t *h, double *nu);
 /* Per-row profile [ny][9]: rho, u, v, u^2, v^2, T, vT, dT/dy (profile(),
- * tempvel_nudge.c:1104-1260), and the row Nusselt number. */
+ * tempvel_nudge.c:1104-1260), and the row Nusselt number.  Means are the
+ * reference's row sums scaled by 1/nx (taken here as compensated sums);
+ * dT/dy is T(j+1) - T(j), periodic at the top row as the reference's halo
+ * row there is, and with box nudging that halo value is row 0's sum of g
+ * without the 1/2 nud_term (hydrovar forms halo rows whose nudge_vol is 0).
+ * The reference run on several ranks in y treats the last row of every rank
+ * that way; this whole-domain profile does so at the top row only. */
 LBRB_API int lbrb_profile(lbrb_t *h, double *out);
 
 /* ---- adjoint (no counterpart in the reference) ----------------------------- */

@@ -280,15 +280,19 @@ __global__ void __launch_bounds__(256) profile_kernel(const Real* __restrict__ r
                                                       const Real* __restrict__ u,
                                                       const Real* __restrict__ v,
                                                       const Real* __restrict__ T, int nx, int ny,
-                                                      int pitch, double* __restrict__ out) {
+                                                      int pitch, const double* __restrict__ Ttop,
+                                                      double* __restrict__ out) {
   const int j = blockIdx.x;
   KSum a[8];
   const int jt = (j + 1) % ny;
   for (int i = threadIdx.x; i < nx; i += blockDim.x) {
     const size_t o = (size_t)j * pitch + i, ot = (size_t)jt * pitch + i;
     const double r = rho[o], uu = u[o], vv = v[o], t = T[o];
+    // above the top row: the periodic halo row (Ttop: its value without box
+    // nudging's 1/2 nud_term, as the reference forms the halo)
+    const double tu = (Ttop && j == ny - 1) ? Ttop[i] : (double)T[ot];
     a[0].add(r); a[1].add(uu); a[2].add(vv); a[3].add(uu * uu); a[4].add(vv * vv);
-    a[5].add(t); a[6].add(vv * t); a[7].add((double)T[ot] - t);
+    a[5].add(t); a[6].add(vv * t); a[7].add(tu - t);
   }
   __shared__ double sh[8][2][256];
   for (int w = 0; w < 8; w++) {
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(256) profile_kernel(const Real* __restrict__ r
       b.add(sh[threadIdx.x][0][t]);
       b.add(sh[threadIdx.x][1][t]);
     }
-    out[(size_t)j * 9 + threadIdx.x] = b.val() / (double)nx;
+    out[(size_t)j * 9 + threadIdx.x] = b.val() * (1 / (double)nx);  // (the reference's 1/nx scaling)
   }
 }
 
@@ -481,13 +485,13 @@ cudaError_t launch_stats(const void* rho, const void* u, const void* v, const vo
 }
 
 cudaError_t launch_profile(const void* rho, const void* u, const void* v, const void* T, bool fp32,
-                           int nx, int ny, int pitch, double* out, cudaStream_t s) {
+                           int nx, int ny, int pitch, const double* Ttop, double* out, cudaStream_t s) {
   if (fp32)
     profile_kernel<float><<<ny, 256, 0, s>>>((const float*)rho, (const float*)u, (const float*)v,
-                                             (const float*)T, nx, ny, pitch, out);
+                                             (const float*)T, nx, ny, pitch, Ttop, out);
   else
     profile_kernel<double><<<ny, 256, 0, s>>>((const double*)rho, (const double*)u, (const double*)v,
-                                              (const double*)T, nx, ny, pitch, out);
+                                              (const double*)T, nx, ny, pitch, Ttop, out);
   return cudaGetLastError();
 }
 

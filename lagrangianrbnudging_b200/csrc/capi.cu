@@ -127,7 +127,7 @@ static void free_all(lbrb_t* h) {
     for (int s = 0; s < h->p.record_slots; s++) if (h->ring_ev[s]) cudaEventDestroy(h->ring_ev[s]);
     delete[] h->ring_ev;
   }
-  F(h->nb); F(h->nbi); F(h->nudge_vol); F(h->tempreadint); F(h->nud_term);
+  F(h->nb); F(h->nbi); F(h->nudge_vol); F(h->tempreadint); F(h->nud_term); F(h->tsum0);
   F(h->cell_count); F(h->cell_start); F(h->cell_fill); F(h->cell_dirty); F(h->cell_items);
   delete[] h->h_chk; delete[] h->h_oid;
   F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
@@ -227,7 +227,7 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
     const size_t nc = (size_t)h->ncx * h->ncy;
     if (dalloc(&h->nb, (size_t)NB_COUNT * n) || dalloc(&h->nbi, (size_t)NBI_COUNT * n) ||
         dalloc(&h->nudge_vol, h->plane) || dalloc(&h->tempreadint, h->plane) ||
-        dalloc(&h->nud_term, h->plane) || dalloc(&h->cell_count, nc) ||
+        dalloc(&h->nud_term, h->plane) || dalloc(&h->tsum0, (size_t)h->pitch) || dalloc(&h->cell_count, nc) ||
         dalloc(&h->cell_start, nc) || dalloc(&h->cell_fill, nc) || dalloc(&h->cell_dirty, nc) ||
         dalloc(&h->cell_items, (size_t)2 * 12 * n))
       return done(LBRB_ERR_NOMEM);
@@ -471,6 +471,7 @@ int lbrb_nudge_init(lbrb_t* h, int n, const double* x, const double* y, const do
     CK(h, cudaMemcpyAsync(nb + (size_t)dst[a] * n, src[a], b, cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemsetAsync(h->nbi, 0, sizeof(int) * NBI_COUNT * (size_t)n, h->stream));
   CK(h, cudaMemsetAsync(h->nud_term, 0, sizeof(double) * h->plane, h->stream));
+  CK(h, cudaMemsetAsync(h->tsum0, 0, sizeof(double) * h->pitch, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   std::memcpy(h->h_oid, ids, n * sizeof(int));
   std::memset(h->h_chk, 0, n * sizeof(int));
@@ -1881,8 +1882,11 @@ int lbrb_profile(lbrb_t* h, double* out) {
   if (!h->moments_valid) return fail(h, LBRB_ERR_STATE, "profile: no moments yet");
   CK(h, cudaSetDevice(h->dev));
   double* dout = h->red + (size_t)red_blocks() * 6 + 8;
+  // box nudging: the row above the top row is the reference's periodic halo
+  // row, row 0's sum of g without the 1/2 nud_term (kept by the fused step)
+  const double* Ttop = (h->p.nudge == LBRB_NUDGE_REFBOX && h->istep > 0) ? h->tsum0 : nullptr;
   CK(h, launch_profile(h->rho[h->cur], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[h->cur], fp32(h), h->p.nx,
-                       h->p.ny, h->pitch, dout, h->stream));
+                       h->p.ny, h->pitch, Ttop, dout, h->stream));
   CK(h, cudaMemcpyAsync(out, dout, (size_t)h->p.ny * 9 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   const double kappa = (h->p.relaxg - 0.5) / 3.0;

@@ -89,7 +89,7 @@ cudaError_t launch_slab_pack(const void* pops, bool fp32, int nx, int ny, int pi
 cudaError_t launch_stats(const void* rho, const void* u, const void* v, const void* T, bool fp32,
                          int nx, int ny, int pitch, double* part, double* out, cudaStream_t s);
 cudaError_t launch_profile(const void* rho, const void* u, const void* v, const void* T, bool fp32,
-                           int nx, int ny, int pitch, double* out, cudaStream_t s);
+                           int nx, int ny, int pitch, const double* Ttop, double* out, cudaStream_t s);
 cudaError_t launch_finite(const void* a, size_t n, bool fp32, unsigned* flags, cudaStream_t s);
 int red_blocks();
 cudaError_t launch_adjoint_step(bool fp32, const void* after, const void* state, const double* lf_out,
@@ -205,6 +205,7 @@ inline LBView<Real> make_view(lbrb_t* h, int src, int dst, int uvslot, int write
   V.nudge_vol = h->nudge_vol;
   V.tempreadint = h->tempreadint;
   V.nud_term = h->nud_term;
+  V.tsum0 = h->tsum0;
   V.alpha = h->p.alpha;
   V.write_uv = write_uv;
   V.write_rt = write_rt;

@@ -42,6 +42,7 @@ __device__ __forceinline__ void node_ref(const LBView<double>& V, size_t idx, do
   int nv = 0;
   if (REFNUDGE) {
     nv = V.nudge_vol[idx];
+    if (idx < (size_t)V.pitch) V.tsum0[idx] = t;  // (row 0)
     if (nv > 0) t = (t + 0.5 * V.nud_term[idx]);
   }
   const double rhoi = 1. / r;

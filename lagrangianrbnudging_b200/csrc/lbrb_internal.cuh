@@ -201,6 +201,9 @@ struct LBView {
   const int* __restrict__ nudge_vol;
   const double* __restrict__ tempreadint;
   double* __restrict__ nud_term;
+  // box nudging: row 0's sum of g before the 1/2 nud_term (the reference's
+  // halo row above the top row takes that value: lbrb_profile's top dT/dy)
+  double* __restrict__ tsum0;
   double alpha;
   int write_uv;
   int write_rt;  // bit 0: store T (records, nudging), bit 1: also rho (a call's last step)
@@ -315,6 +318,7 @@ struct Handle {
   int* nudge_vol = nullptr;
   double* tempreadint = nullptr;
   double* nud_term = nullptr;
+  double* tsum0 = nullptr;  // [pitch]: row 0's sum of g without the 1/2 nud_term (LBView::tsum0)
   int* cell_count = nullptr;
   int* cell_start = nullptr;
   int* cell_fill = nullptr;

@@ -565,6 +565,7 @@ void orc_step(orc_t *s, int istep) {
       double r = 0.0, t = 0.0;
       for (int k = 0; k < NPOP; k++) r = r + fs[pidx(s, k, i, j)];
       for (int k = 0; k < NPOP; k++) t = t + gs[pidx(s, k, i, j)];
+      s->fld[ORC_TSUM][q] = t;
       if (refbox && s->nudge_vol[q] > 0) t = (t + 0.5 * nud[q]);
       rho[q] = r;
       T[q] = t;
@@ -680,23 +681,33 @@ void orc_energy(orc_t *s, double *ke_mean, double *t_mean) {
 }
 
 /* per-row averages (tempvel_nudge.c profile(), :1186-1232): columns
- * rho, u, v, u^2, v^2, T, vT, dT/dy (T(j+1)-T(j), periodic at the top row
- * as in the reference), each divided by nx; plus column 8 = row Nusselt
- * (vT - kappa dT/dy) / (kappa dT_walls / ny) */
-void orc_profile(orc_t *s, double *out) {
+ * rho, u, v, u^2, v^2, T, vT, dT/dy (T(j+1)-T(j)), each scaled by 1/nx;
+ * plus column 8 = row Nusselt (vT - kappa dT/dy) / (kappa dT_walls / ny).
+ * At the last row of each of the reference's `ranks_y` ranks in y, T(j+1)
+ * is the halo row: hydrovar (tempvel_nudge.c:1069-1102) forms it from the
+ * halo populations that pbc copied from the next rank's first row (periodic
+ * at the top), and the halo's nudge_vol is 0, so it is that row's sum of g
+ * without box nudging's 1/2 nud_term. */
+void orc_profile(orc_t *s, double *out) { orc_profile_ranks(s, 1, out); }
+
+void orc_profile_ranks(orc_t *s, int ranks_y, double *out) {
   const int nx = s->p.nx, ny = s->p.ny;
   const double *rho = s->fld[ORC_RHO], *u = s->fld[ORC_U], *v = s->fld[ORC_V], *T = s->fld[ORC_T];
+  const double *Thalo = s->p.nudge == ORC_NUDGE_REFBOX ? s->fld[ORC_TSUM] : T;
   const double kappa = (s->p.relaxg - 0.5) / 3.0;
   const double dTw = s->p.Tdown - s->p.Tup;
+  const int NYr = ny / (ranks_y > 0 ? ranks_y : 1);
   for (int j = 0; j < ny; j++) {
     double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const double *Tup_row = ((j + 1) % NYr == 0) ? Thalo : T;
     for (int i = 0; i < nx; i++) {
       size_t q = sidx(s, i, j), qt = sidx(s, i, wrap(j + 1, ny));
       a[0] += rho[q]; a[1] += u[q]; a[2] += v[q];
       a[3] += u[q] * u[q]; a[4] += v[q] * v[q]; a[5] += T[q];
-      a[6] += v[q] * T[q]; a[7] += T[qt] - T[q];
+      a[6] += v[q] * T[q]; a[7] += Tup_row[qt] - T[q];
     }
-    for (int c = 0; c < 8; c++) out[(size_t)j * 9 + c] = a[c] / (double)nx;
+    const double norma = 1 / ((double)nx); /* the reference scales by 1/nx (:1225-1229) */
+    for (int c = 0; c < 8; c++) out[(size_t)j * 9 + c] = a[c] * norma;
     out[(size_t)j * 9 + 8] = (out[(size_t)j * 9 + 6] - kappa * out[(size_t)j * 9 + 7]) / (kappa * dTw / (double)ny);
   }
 }

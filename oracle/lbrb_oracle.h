@@ -45,7 +45,9 @@ typedef struct orc_s orc_t;
 /* field ids for orc_field() */
 enum {
   ORC_F = 0, ORC_G, ORC_RHO, ORC_U, ORC_V, ORC_T, ORC_UBEF, ORC_VBEF,
-  ORC_FY, ORC_TEMPREADINT, ORC_NUDTERM, ORC_NUDGE_SRC, ORC_NFIELDS
+  ORC_FY, ORC_TEMPREADINT, ORC_NUDTERM, ORC_NUDGE_SRC,
+  ORC_TSUM, /* sum of g of the step, before box nudging's 1/2 nud_term */
+  ORC_NFIELDS
 };
 /* particle array ids for orc_prtcl() */
 enum {
@@ -98,6 +100,9 @@ void orc_energy(orc_t *s, double *ke_mean, double *t_mean);
 /* per-row profile: out[9*ny]: rho,u,v,u2,v2,T,vT,dyT (reference profile())
  * plus row Nusselt ingredients; rows j=0..ny-1 */
 void orc_profile(orc_t *s, double *out);
+/* the same as the reference prints it from a run on `ranks_y` ranks in y
+ * (only dT/dy at the last row of each rank depends on that) */
+void orc_profile_ranks(orc_t *s, int ranks_y, double *out);
 double orc_nusselt(orc_t *s);
 
 /* FP64 tangent-linear model of an assimilation window (no counterpart in the

@@ -67,6 +67,7 @@ def lib():
         L.orc_nudge_obs.argtypes = [C.c_void_p, C.c_int, dp, dp, dp]
         L.orc_energy.argtypes = [C.c_void_p, dp, dp]
         L.orc_profile.argtypes = [C.c_void_p, dp]
+        L.orc_profile_ranks.argtypes = [C.c_void_p, C.c_int, dp]
         L.orc_nusselt.restype = C.c_double
         L.orc_nusselt.argtypes = [C.c_void_p]
         L.orc_tlm_window.argtypes = [C.c_void_p, dp, dp, C.c_int, C.c_int, ip, C.c_int, dp, dp,
@@ -185,9 +186,11 @@ class Oracle:
         lib().orc_energy(self._h, C.byref(ke), C.byref(tm))
         return ke.value, tm.value
 
-    def profile(self):
+    def profile(self, ranks_y: int = 1):
+        """per-row profiles; ranks_y: the reference's ranks in y (the last
+        row of each rank takes T(j+1) from its halo row)"""
         out = np.zeros((self.ny, 9))
-        lib().orc_profile(self._h, _dp(out))
+        lib().orc_profile_ranks(self._h, int(ranks_y), _dp(out))
         return out
 
     def nusselt(self) -> float:

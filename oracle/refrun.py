@@ -228,4 +228,15 @@ def run_nudging(refp: dict, init_obs: dict, files: dict, np_ranks: int = 2, dims
             snaps[s] = {k: np.ascontiguousarray(np.fromfile(d / f"{k}.bin").reshape(nx, ny).T)
                         for k in ("T", "u", "v")}
     out["snaps"] = snaps
+    # profiles.<istep>.dat (profile(), tempvel_nudge.c:1104-1260, every nout
+    # steps): "j rho u v u^2 v^2 T vT dT/dy" per row, each %e; the format has
+    # one %e more than its arguments (:1229), so a tenth column is whatever
+    # printf finds there and is dropped
+    profs = {}
+    for s in range(refp["nout"], nsteps + 1, refp["nout"]):
+        p = wd / f"profiles.{s}.dat"
+        if p.exists():
+            rows = [ln.split()[:9] for ln in p.read_text().splitlines() if ln.strip()]
+            profs[s] = np.array([[float(x) for x in r] for r in rows])
+    out["profiles"] = profs
     return out

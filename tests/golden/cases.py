@@ -38,6 +38,20 @@ TRAJ_CASES = {
                       inertial=True, taulag=40.0, beta=0.1, nsteps=1000, noutconfig=250),
 }
 
+# the configurations' own sizes, checked through SHA-256 digests of the full
+# arrays (the arrays themselves are too large to commit) plus sampled values
+CONFIG_CASES = {
+    # plain FP64 run: 512x256, Ra=1e6, U=0.1, conduction + 1e-3 noise, 4096
+    # seeded uniform tracers, 1000 steps, records every 10
+    "cfg0_traj": dict(nx=512, ny=256, Ra=1e6, U=0.1, seed=20240101, noise=1e-3, nprtcl=4096,
+                      inertial=False, taulag=100.0, beta=0.0, nsteps=1000, noutconfig=10),
+    # production grid: 4096x2048, Ra=1e8, U=0.05, 2^17 inertial particles of
+    # one Stokes number (the reference compiles one particle type; St=0.5:
+    # tau_p = St*Ny/U = 20480), beta=0, 10 steps, records every 5
+    "cfg1_traj": dict(nx=4096, ny=2048, Ra=1e8, U=0.05, seed=20240102, noise=1e-3, nprtcl=1 << 17,
+                      inertial=True, taulag=0.5 * 2048 / 0.05, beta=0.0, nsteps=10, noutconfig=5),
+}
+
 # runs of the host program against the reference's own scratch / restart paths
 SCRATCH_TRAJ_CASES = {
     # the reference's scratch state (tanh + rand(), one rank) and its 40x40
@@ -55,8 +69,20 @@ NUDGE_CASES = {
 }
 
 
+def bilinear_vec(fld: np.ndarray, xs: np.ndarray, ys: np.ndarray) -> np.ndarray:
+    """bilinear_np at many points: the same corner order and the same
+    operation order element by element, so the results are identical"""
+    ny, nx = fld.shape
+    x1 = xs.astype(np.int64)
+    y1 = ys.astype(np.int64)
+    x2, y2 = x1 + 1, y1 + 1
+    F = lambda i, j: fld[(j - 1) % ny, (i - 1) % nx]
+    return (F(x1, y1) * (x2 - xs) * (y2 - ys) + F(x2, y1) * (xs - x1) * (y2 - ys)
+            + F(x1, y2) * (x2 - xs) * (ys - y1) + F(x2, y2) * (xs - x1) * (ys - y1))
+
+
 def traj_case(name: str) -> dict:
-    c = dict(TRAJ_CASES[name])
+    c = dict(TRAJ_CASES[name] if name in TRAJ_CASES else CONFIG_CASES[name])
     base = closure(c["nx"], c["ny"], Ra=c["Ra"], Pr=1.0, U=c["U"])
     params = dict(base, twall="dirichlet", nudge="none", beta=c["beta"],
                   noutconfig=c["noutconfig"], record_full=True)
@@ -66,8 +92,8 @@ def traj_case(name: str) -> dict:
     n, nx, ny = c["nprtcl"], c["nx"], c["ny"]
     px = rng.uniform(0.01, nx - 0.01, n)
     py = rng.uniform(1.01, ny - 0.01, n)
-    pu = np.array([bilinear_np(o.u, a, b) for a, b in zip(px, py)])
-    pv = np.array([bilinear_np(o.v, a, b) for a, b in zip(px, py)])
+    pu = bilinear_vec(o.u, px, py)
+    pv = bilinear_vec(o.v, px, py)
     c.update(base=base, params=params, f0=o.f.copy(), g0=o.g.copy(),
              rho0=o.rho.copy(), u0=o.u.copy(), v0=o.v.copy(), T0=o.T.copy(),
              ids=np.arange(n, dtype=np.int32), px=px, py=py, pu=pu, pv=pv,
@@ -167,7 +193,12 @@ def nudge_initial_state(c: dict) -> dict:
                 rho=np.ones((ny, nx)), u=np.zeros((ny, nx)), v=np.zeros((ny, nx)), T=c["Tic"].copy())
 
 
-def run_oracle_nudge(c: dict) -> dict:
+PROFILE_EVERY = 10  # the nudging fixtures' nout: the reference writes profiles.<step>.dat
+
+
+def run_oracle_nudge(c: dict, ranks_y: int = 1) -> dict:
+    """the nudging run on the oracle; profiles every PROFILE_EVERY steps as
+    the reference prints them from a run on `ranks_y` ranks in y"""
     o = Oracle(c["params"], c["nprtcl"])
     st = nudge_initial_state(c)
     o.f[:] = st["f"]
@@ -179,13 +210,50 @@ def run_oracle_nudge(c: dict) -> dict:
     io = c["init_obs"]
     o.nudge_init(io["x"], io["y"], io["T"], io["id"])
     nt = c["ntempread"]
+    profiles = {}
     for s in range(1, c["nsteps"] + 1):
         if s % nt == 1:
             d = c["files"][s + nt - 1]
             o.nudge_load(d["x"], d["y"], d["id"], d["temp"])
         o.step(s)
+        if s % PROFILE_EVERY == 0:
+            profiles[s] = o.profile(ranks_y)
     return dict(f=o.f.copy(), g=o.g.copy(), T=o.T.copy(), u=o.u.copy(), v=o.v.copy(),
-                nudge_vol=o.nudge_vol.copy(), tempreadint=o.tempreadint.copy())
+                nudge_vol=o.nudge_vol.copy(), tempreadint=o.tempreadint.copy(), profiles=profiles)
+
+
+def sha256(a: np.ndarray) -> str:
+    """digest of an array's values in C order (little-endian)"""
+    import hashlib
+
+    a = np.ascontiguousarray(a)
+    return hashlib.sha256(a.astype(a.dtype.newbyteorder("<"), copy=False).tobytes()).hexdigest()
+
+
+def record_digest(rec: dict, fields) -> str:
+    """digest of one particle record: ids in increasing order, then each
+    field in `fields` order, rows ordered by id"""
+    import hashlib
+
+    order = np.argsort(rec["id"], kind="stable")
+    h = hashlib.sha256(np.ascontiguousarray(rec["id"][order], "<i4").tobytes())
+    for k in fields:
+        h.update(np.ascontiguousarray(rec[k][order], "<f8").tobytes())
+    return h.hexdigest()
+
+
+# the sampled values kept beside the digests: rows and every 64th column
+def sample_rows(ny: int):
+    return np.array(sorted({0, 1, ny // 2, ny - 2, ny - 1}), np.int64)
+
+
+def sample_pops(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a[:, sample_rows(a.shape[1])][:, :, ::64])
+
+
+def printed(a: np.ndarray) -> np.ndarray:
+    """values as the reference's "%e" prints them"""
+    return np.vectorize(lambda v: float("%e" % v))(a)
 
 
 def golden_path(name: str) -> Path:

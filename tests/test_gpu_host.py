@@ -117,7 +117,7 @@ def test_host_nudging_restart_route(tmp_path):
                          ("congpre", "g", rp["gpre"])):
         refrun._write_ds(wd / f"{name}.h5.d" / f"{key}.bin", refrun._to_ref_pops(a))
     b = c["base"]
-    run_host("nudging", dict(nx=c["nx"], ny=c["ny"], scratch=0, nsteps=c["nsteps"], nout=10**6,
+    run_host("nudging", dict(nx=c["nx"], ny=c["ny"], scratch=0, nsteps=c["nsteps"], nout=cases.PROFILE_EVERY,
                              noutconfig=10, ntempread=c["ntempread"], alpha=c["alpha"],
                              relax=b["relax"], relaxg=b["relaxg"], Tup=b["Tup"], Tdown=b["Tdown"],
                              gravity=b["gravity"], Nprtcl=c["nprtcl"]), wd)
@@ -129,3 +129,19 @@ def test_host_nudging_restart_route(tmp_path):
         for k in ("T", "u", "v"):
             a = np.fromfile(d / f"{k}.bin").reshape(c["nx"], c["ny"]).T
             np.testing.assert_array_equal(a, z[f"snap{s}_{k}"], err_msg=f"snap {s} {k}")
+    # profiles.<step>.dat against the reference's (run on 1 x npy ranks).  The
+    # host program is one whole domain: at the last row of an inner y-rank the
+    # reference's dT/dy took T(j+1) from a halo row without the 1/2 nud_term,
+    # there the expected value is the whole domain's (the oracle's, printed)
+    whole = cases.run_oracle_nudge(c, ranks_y=1)["profiles"]
+    nyr = c["ny"] // c["npy"]
+    for s in range(cases.PROFILE_EVERY, c["nsteps"] + 1, cases.PROFILE_EVERY):
+        got = np.loadtxt(wd / f"profiles.{s}.dat", ndmin=2)
+        ref = z[f"prof{s}"].copy()
+        for j in range(nyr - 1, c["ny"] - 1, nyr):
+            ref[j, 8] = cases.printed(whole[s][j, 7])
+        np.testing.assert_array_equal(got[:, 0], ref[:, 0])
+        # both are "%e" text (7 significant digits) of sums taken in different
+        # orders: one unit in the 7th digit, and 1e-15 for means near zero
+        np.testing.assert_allclose(got[:, 1:], ref[:, 1:], rtol=1.000001e-6, atol=1e-15,
+                                   err_msg=f"profile of step {s}")

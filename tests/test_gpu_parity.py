@@ -109,6 +109,56 @@ def test_fp64_box_nudging_bit_exact_vs_reference(name):
     np.testing.assert_array_equal(m["v"], z[f"snap{s}_v"])
 
 
+def _check_profile(p, o):
+    """lbrb_profile against the oracle: compensated sums against the
+    reference's running sums, so 1e-12 relative, with an absolute floor of
+    1e-15 for means that cancel to about zero (u, v over a row)"""
+    np.testing.assert_allclose(p[:, :8], o[:, :8], rtol=1e-12, atol=1e-15)
+    # the row Nusselt number divides by kappa dT / ny
+    np.testing.assert_allclose(p[:, 8], o[:, 8], rtol=1e-10, atol=1e-10)
+
+
+def test_fp64_profile_matches_oracle_trajectories():
+    c = cases.traj_case("traj_wide")
+    o = Oracle(c["params"], c["nprtcl"])
+    o.f[:] = c["f0"]
+    o.g[:] = c["g0"]
+    o.moments_from_pre(c["f0"], c["g0"])
+    o.set_particles(c["ids"], c["px"], c["py"], c["pu"], c["pv"], c["ptype"], c["invtau"])
+    with traj_run(c) as r:
+        for s in range(1, c["nsteps"] + 1):
+            o.step(s)
+            o.record()
+            if s % 40 == 0:
+                r.step(40)
+                r.sync()
+                _check_profile(r.profile(), o.profile())
+
+
+@pytest.mark.parametrize("name", list(cases.NUDGE_CASES))
+def test_fp64_profile_matches_oracle_box_nudging(name):
+    """the whole-domain profile of a box-nudged run (above the top row, the
+    periodic halo row without the 1/2 nud_term, as the reference forms it)"""
+    c = cases.nudge_case(name)
+    out = cases.run_oracle_nudge(c, ranks_y=1)
+    st = cases.nudge_initial_state(c)
+    with lb.Run(**c["base"], precision="fp64", twall="adiabatic", nudge="refbox",
+                alpha=c["alpha"], ntempread=c["ntempread"], nobs=c["nprtcl"]) as r:
+        r.set_populations(st["f"], st["g"])
+        r.set_moments(st["rho"], st["u"], st["v"], st["T"])
+        io = c["init_obs"]
+        r.nudge_init(io["x"], io["y"], io["T"], io["id"])
+        nt = c["ntempread"]
+        for s in range(1, c["nsteps"] + 1):
+            if s % nt == 1:
+                d = c["files"][s + nt - 1]
+                r.nudge_load(d["x"], d["y"], d["id"], d["temp"])
+            r.step(1)
+            if s in out["profiles"]:
+                r.sync()
+                _check_profile(r.profile(), out["profiles"][s])
+
+
 def test_init_conduction_matches_oracle():
     base = lb.closure(96, 48, Ra=1e6, Pr=1.0, U=0.1)
     o = Oracle(dict(base), 0)

@@ -37,8 +37,16 @@ def test_oracle_matches_golden_trajectories(name):
 @pytest.mark.parametrize("name", list(cases.NUDGE_CASES))
 def test_oracle_matches_golden_nudging(name):
     c = cases.nudge_case(name)
-    out = cases.run_oracle_nudge(c)
+    # (the fixtures come from the reference run on 1 x npy ranks)
+    out = cases.run_oracle_nudge(c, ranks_y=c["npy"])
     z = cases.load_golden(name)
+    # profiles.<step>.dat: every value as the reference printed it
+    steps = sorted(int(k[4:]) for k in z if k.startswith("prof"))
+    assert steps == sorted(out["profiles"]) and steps
+    for s in steps:
+        np.testing.assert_array_equal(z[f"prof{s}"][:, 0], np.arange(1, c["ny"] + 1))
+        np.testing.assert_array_equal(cases.printed(out["profiles"][s][:, :8]), z[f"prof{s}"][:, 1:],
+                                      err_msg=f"profile of step {s}")
     np.testing.assert_array_equal(out["f"], z["f"])
     np.testing.assert_array_equal(out["g"], z["g"])
     s = c["nsteps"]
@@ -87,3 +95,20 @@ def test_reference_decomposition_invariance():
         oa, ob = np.argsort(a["records"][s]["id"]), np.argsort(b["records"][s]["id"])
         np.testing.assert_allclose(a["records"][s]["temp"][oa], b["records"][s]["temp"][ob],
                                    rtol=0, atol=1e-12)
+
+
+def test_oracle_matches_golden_config0_digests():
+    """the configuration-size fixture (512x256, 4096 tracers, 1000 steps):
+    the oracle's populations, moments and every record against the digests
+    of the reference's run"""
+    c = cases.traj_case("cfg0_traj")
+    z = cases.load_golden("cfg0_traj")
+    out = cases.run_oracle_traj(c)
+    assert cases.sha256(out["f"]) == str(z["f_sha"])
+    assert cases.sha256(out["g"]) == str(z["g_sha"])
+    for k in ("rho", "u", "v", "T"):
+        assert cases.sha256(out[k]) == str(z[f"{k}_sha"]), k
+    fields = [str(k) for k in z["rec_fields"]]
+    assert sorted(out["records"]) == [int(s) for s in z["rec_steps"]]
+    for s, r in out["records"].items():
+        assert cases.record_digest(dict(r, id=c["ids"]), fields) == str(z[f"rec{s}_sha"]), s
