@@ -179,11 +179,18 @@ LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
  * Replaces, for two steps at a time, the reference's per-step sweeps
  * (stream, moments, collide: temppart_dump.c:1674-1759). */
 LBRB_API int lbrb_set_pairs(lbrb_t *h, int mode);
-/* fix the tile shape (0: 32x8, 1: 32x4, 2: 32x16, 3: 64x4, 4: 32x8 with a
- * thread per node of the tile and its ring, 5: 30x8 likewise, 6: 32x8 at 5
- * blocks per SM, 7: 32x6, 8: 64x8) instead of timing the shapes on first
- * use (-1) */
+/* fix the launch shape of the two-step kernel instead of timing the shapes
+ * on first use (-1).  Tiles with a one-node ring recomputed around each:
+ * 0: 32x8, 1: 32x4, 2: 32x16, 3: 64x4, 4: 32x8 with a thread per node of
+ * the tile and its ring, 5: 30x8 likewise, 6: 32x8 at 5 blocks per SM,
+ * 7: 32x6, 8: 64x8.  Strips of 32 columns walked down a chunk of rows,
+ * recomputing only two halo columns and two rows per chunk (tile_y: rows
+ * per group): 9: 8 rows, 4 blocks per SM; 10: 4 rows, 8 blocks; 11: 16 rows,
+ * 2 blocks; 12: 6 rows, 5 blocks; 13: 8 rows, 4 blocks, taller chunks;
+ * 14: 8 rows, 3 blocks. */
 LBRB_API int lbrb_set_pair_shape(lbrb_t *h, int shape);
+/* the number of launch shapes of the two-step kernel (0 .. n-1) */
+LBRB_API int lbrb_pair_shapes(void);
 LBRB_API int lbrb_get_pair_shape(const lbrb_t *h, int *shape, int *tile_x, int *tile_y, float *ms);
 /* Per-kernel device timing with CUDA events around each launch.  Classes:
  * 0 fused stream/collide, 1 particles, 2 nudging, 3 record copies.

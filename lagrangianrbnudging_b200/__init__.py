@@ -46,7 +46,7 @@ EXPORTS = [
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
     "lbrb_slab_ghost2_bytes", "lbrb_slab_buffers2", "lbrb_slab_pack2",
-    "lbrb_set_graph", "lbrb_set_pairs", "lbrb_set_pair_shape", "lbrb_get_pair_shape",
+    "lbrb_set_graph", "lbrb_set_pairs", "lbrb_set_pair_shape", "lbrb_get_pair_shape", "lbrb_pair_shapes",
 ]
 
 
@@ -142,6 +142,7 @@ def lib() -> C.CDLL:
         "lbrb_set_graph": (C.c_int, [vp, C.c_int]),
         "lbrb_set_pairs": (C.c_int, [vp, C.c_int]),
         "lbrb_set_pair_shape": (C.c_int, [vp, C.c_int]),
+        "lbrb_pair_shapes": (C.c_int, []),
         "lbrb_get_pair_shape": (C.c_int, [vp, ip, ip, ip, C.POINTER(C.c_float)]),
     }
     for name, (res, args) in sig.items():
@@ -383,8 +384,13 @@ class Run:
         """two steps per fused launch: -1 (default) and 1 where eligible, 0 off"""
         self._ck(lib().lbrb_set_pairs(self.h, int(mode)))
 
+    @staticmethod
+    def pair_shapes() -> int:
+        """launch shapes of the two-step kernel (tiles, then marching strips)"""
+        return lib().lbrb_pair_shapes()
+
     def set_pair_shape(self, shape: int):
-        """fixed tile shape of the two-step launch (0..3), or -1: timed on first use"""
+        """fixed launch shape of the two-step kernel (0 .. pair_shapes() - 1), or -1: timed on first use"""
         self._ck(lib().lbrb_set_pair_shape(self.h, int(shape)))
 
     def pair_shape(self):

@@ -1761,6 +1761,8 @@ int lbrb_set_pairs(lbrb_t* h, int mode) {
   return LBRB_OK;
 }
 
+int lbrb_pair_shapes(void) { return NUM_PAIR_SHAPES; }
+
 int lbrb_set_pair_shape(lbrb_t* h, int shape) {
   if (!h || shape < -1 || shape >= NUM_PAIR_SHAPES)
     return fail(h, LBRB_ERR_ARG, "set_pair_shape: shape must be -1 (tune) or a shape index");
@@ -1771,7 +1773,10 @@ int lbrb_set_pair_shape(lbrb_t* h, int shape) {
 
 int lbrb_get_pair_shape(const lbrb_t* h, int* shape, int* tile_x, int* tile_y, float* ms) {
   if (!h) return LBRB_ERR_ARG;
-  static const int TXS[] = {32, 32, 32, 64, 32, 30, 32, 32, 64}, TYS[] = {8, 4, 16, 4, 8, 8, 8, 6, 8};  // (lb_kernels.cu: PAIR_SHAPES)
+  // (lb_kernels.cu: PAIR_SHAPES, then MARCH_SHAPES: a strip of 32 columns
+  // walked in groups of tile_y rows)
+  static const int TXS[] = {32, 32, 32, 64, 32, 30, 32, 32, 64, 32, 32, 32, 32, 32, 32},
+                   TYS[] = {8, 4, 16, 4, 8, 8, 8, 6, 8, 8, 4, 16, 6, 8, 8};
   static_assert(sizeof(TXS) / sizeof(int) == NUM_PAIR_SHAPES, "pair shape table");
   const int sh = h->pair_shape;
   if (shape) *shape = sh;

@@ -30,6 +30,7 @@
 // of two buffers, so a launch is a pure function of its sources: the launch
 // shape (block size, blocks per SM) is picked by timing the candidates on the
 // run's own grid (tune_lb).
+#include <algorithm>
 #include <atomic>
 #include <cstdlib>
 #include <type_traits>
@@ -183,13 +184,128 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
   lb_finish_node<Real, false, Off>(V2, (Off)j * pitch + (Off)x, fs, gs, SF[ty * TX + tx]);
 }
 
+// ------------------------------------------- two steps per launch, marching
+// The same two steps as lb_pair_kernel, with far less recomputation: a block
+// owns a strip of 32 columns [x0, x0 + 32) and a chunk of rows [ya, ya + Hc)
+// and walks down it in groups of R rows.  With ly = y - ya + 1 (ring row
+// index; ly = 0 is the row below the chunk), group q does
+//   phase 1: step n at rows ly in [qR, qR + R) for the 34 region columns
+//            x0-1 .. x0+32 (R warps take the strip's columns of one row
+//            each; one more warp takes the two halo columns of all R rows),
+//            pulled from HBM exactly as lb_update_node pulls, into a ring of
+//            RING = 2R + 2 rows in shared memory; the chunk's own rows also
+//            store u^n, v^n (T^n on a record step) and keep F^{n+1};
+//   one barrier;
+//   phase 2: step n+1 at output rows ly in [qR - 1, qR + R - 1) within
+//            [1, Hc], pulled from the ring with pull_node's wall rules.
+// Phase 2 of group q reads ring rows [qR - 2, qR + R - 1]; phase 1 of group
+// q + 1 overwrites rows [qR - R - 2, qR - 3], which only phase 2 of group
+// q - 1 read, before the barrier of group q: one barrier per group orders
+// the ring.  Recomputed per strip and chunk: the two halo columns and the two
+// rows beyond the chunk (34/32 x (Hc + 2)/Hc node updates in phase 1,
+// against 34 x 10 / (32 x 8) for the 32 x 8 tile).  The per-node arithmetic
+// is lb_update_node's, so the result equals two single steps bit for bit.
+// Slabs: as in lb_pair_kernel, rows -1 and ny come from the ghost blocks.
+template <typename Real, int R, int MINB, typename Off>
+__global__ void __launch_bounds__(32 * (R + 1), MINB)
+    lb_march_kernel(const LBView<Real> V1, const LBView<Real> V2, int H) {
+  static_assert(2 * R <= 32, "the halo warp takes 2R nodes");
+  pdl_wait();
+  constexpr int RING = 2 * R + 2, CW = 34, PL = RING * CW;
+  extern __shared__ __align__(16) unsigned char march_smem[];
+  Real* S = reinterpret_cast<Real*>(march_smem);  // [2 * NPOP][RING][CW]: f then g of step n
+  Real* SF = S + 2 * NPOP * PL;                   // [RING][32]: F^{n+1} at the strip's columns
+  const int nx = V1.nx, ny = V1.ny;
+  const int nstrips = (nx + 31) >> 5;
+  const int strip = blockIdx.x % nstrips, chunk = blockIdx.x / nstrips;
+  const int x0 = strip * 32, ncols = min(32, nx - x0);
+  const int ya = chunk * H, Hc = min(H, ny - ya);
+  const Off pitch = (Off)V1.pitch;
+  const bool glo = V1.gh2_lo != nullptr, ghi = V1.gh2_hi != nullptr;
+  const int ylo = glo ? -1 : 0, yhi = ghi ? ny : ny - 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // this thread's phase-1 node: row w of the group, column x, ring column c
+  int w, x, c;
+  bool col_ok;
+  if (warp < R) {
+    w = warp;
+    x = x0 + lane;
+    c = lane + 1;
+    col_ok = lane < ncols;
+  } else {
+    const bool right = lane >= R;  // lanes [0, R): column x0 - 1; [R, 2R): x0 + ncols
+    w = right ? lane - R : lane;
+    c = right ? ncols + 1 : 0;
+    x = right ? x0 + ncols : x0 - 1;
+    if (x < 0) x += nx;
+    else if (x >= nx) x -= nx;
+    col_ok = lane < 2 * R;
+  }
+  const int Q = (Hc + 2 + R - 1) / R;
+  for (int q = 0; q < Q; q++) {
+    {
+      const int ly = q * R + w, y = ya - 1 + ly;
+      if (col_ok && ly <= Hc + 1 && y >= ylo && y <= yhi) {
+        const int slot = ly % RING;
+        Real fs[NPOP], gs[NPOP];
+        Real Fy, r, u, v, t;
+        const Off o = (Off)(y < 0 ? 0 : (y >= ny ? ny - 1 : y)) * pitch + (Off)x;  // (ghost rows: no stores)
+        if (y < 0 || y >= ny) {
+          pull_ghost_row<Real, Off>(V1, y < 0, x, fs, gs, Fy);
+        } else {
+          pull_node<Real, LBRB_TWALL_DIRICHLET, Off, true>(V1, y, x, fs, gs);
+          dirichlet_walls(V1, y, gs);
+          Fy = V1.Fin[o];
+        }
+        Real* Sc = S + slot * CW + c;
+        lb_collide<Real, false>(
+            V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { Sc[k * PL] = val; },
+            [&](int k, Real val) { Sc[(NPOP + k) * PL] = val; });
+        if (warp < R && ly >= 1 && ly <= Hc) {  // a node of this block's strip and chunk
+          SF[slot * 32 + lane] = Fy;
+          if (V1.write_F) V1.Fout[o] = Fy;
+          if (V1.write_uv) {
+            V1.u[o] = u;
+            V1.v[o] = v;
+          }
+          if (V1.write_rt & 1) V1.T[o] = t;
+          if (V1.write_rt & 2) V1.rho[o] = r;
+        }
+      }
+    }
+    __syncthreads();
+    if (warp < R) {
+      const int ly = q * R - 1 + w, y = ya - 1 + ly;
+      if (lane < ncols && ly >= 1 && ly <= Hc) {
+        const int s0 = ly % RING, sm = (ly - 1) % RING, sp = (ly + 1) % RING;
+        Real fs[NPOP], gs[NPOP];
+        static_for<NPOP>([&](auto kc) {
+          constexpr int k = decltype(kc)::value;
+          const int js = y - icy(k);
+          if ((js < 0 && !glo) || (js >= ny && !ghi)) {
+            fs[k] = S[opp(k) * PL + s0 * CW + lane + 1];
+            gs[k] = Real(0);
+          } else {
+            const int sl = icy(k) == 1 ? sm : (icy(k) == -1 ? sp : s0);
+            const int cc = lane + 1 - icx(k);
+            fs[k] = S[k * PL + sl * CW + cc];
+            gs[k] = S[(NPOP + k) * PL + sl * CW + cc];
+          }
+        });
+        dirichlet_walls(V2, y, gs);
+        lb_finish_node<Real, false, Off>(V2, (Off)y * pitch + (Off)(x0 + lane), fs, gs, SF[s0 * 32 + lane]);
+      }
+    }
+  }
+}
+
 // pair launch shapes: (tile columns, tile rows, threads, min blocks per SM)
 struct PairShape { int tx, ty, nt, minb; };
 constexpr PairShape PAIR_SHAPES[] = {{32, 8, 256, 4}, {32, 4, 128, 6}, {32, 16, 512, 2}, {64, 4, 256, 3},
                                      {32, 8, 352, 2}, {30, 8, 320, 3}, {32, 8, 256, 5}, {32, 6, 192, 5},
                                      {64, 8, 512, 2}};
 constexpr int NPAIR = sizeof(PAIR_SHAPES) / sizeof(PAIR_SHAPES[0]);
-static_assert(NPAIR == NUM_PAIR_SHAPES, "pair shape table");
+static_assert(NPAIR <= NUM_PAIR_SHAPES, "pair shape table");
 
 template <typename Real, int TX, int TY, int NT, int MINB>
 static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2, cudaStream_t s, bool pdl) {
@@ -209,8 +325,58 @@ static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2,
   return go(lb_pair_kernel<Real, TX, TY, NT, MB, size_t>);
 }
 
+// marching launch shapes: (rows per group R, min blocks per SM, waves): the
+// chunk height H = kR - 2 (whole groups) is chosen so that the grid of
+// strips x chunks holds about `waves` waves of resident blocks
+struct MarchShape { int r, minb, waves; };
+constexpr MarchShape MARCH_SHAPES[] = {{8, 4, 8}, {4, 8, 8}, {16, 2, 8}, {6, 5, 8}, {8, 4, 3}, {8, 3, 8}};
+constexpr int NMARCH = sizeof(MARCH_SHAPES) / sizeof(MARCH_SHAPES[0]);
+static_assert(NPAIR + NMARCH == NUM_PAIR_SHAPES, "pair shape table");
+
+template <typename Real, int R, int MINB>
+static cudaError_t launch_march_t(const LBView<Real>& V1, const LBView<Real>& V2, int waves, cudaStream_t s,
+                                  bool pdl) {
+  constexpr int NT = 32 * (R + 1);
+  constexpr size_t smem = ((size_t)2 * NPOP * (2 * R + 2) * 34 + (size_t)(2 * R + 2) * 32) * sizeof(Real);
+  // (FP64 holds twice the registers and shared memory per value: half the blocks per SM)
+  constexpr int MB = std::is_same<Real, double>::value ? (MINB + 1) / 2 : MINB;
+  auto go = [&](auto kernel) -> cudaError_t {
+    static std::atomic<unsigned long long> attr_set{0};
+    static std::atomic<int> occ_cache[MAX_DEVICES] = {};
+    cudaError_t e = smem_limit_once((const void*)kernel, smem, attr_set);
+    if (e != cudaSuccess) return e;
+    int occ = 0, dev = 0, nsm = 0;
+    e = occupancy_once((const void*)kernel, NT, smem, occ_cache, &occ);
+    if (e == cudaSuccess) e = current_device(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int nx = V1.nx, ny = V1.ny;
+    const long nstrips = (nx + 31) / 32;
+    const long target = std::max(1L, ((long)waves * occ * nsm + nstrips / 2) / nstrips);  // chunks
+    const int h0 = (int)((ny + target - 1) / target);
+    const int H = ((h0 + 2 + R - 1) / R) * R - 2;  // whole groups of R rows
+    const long nchunks = (ny + H - 1) / H;
+    return launch_k(kernel, dim3((unsigned)(nstrips * nchunks)), NT, smem, s, pdl, V1, V2, H);
+  };
+  if (off32_ok(V1.plane)) return go(lb_march_kernel<Real, R, MB, uint32_t>);
+  return go(lb_march_kernel<Real, R, MB, size_t>);
+}
+
+template <typename Real>
+static cudaError_t launch_march(const LBView<Real>& V1, const LBView<Real>& V2, int m, cudaStream_t s, bool pdl) {
+  const int waves = MARCH_SHAPES[m].waves;
+  switch (m) {
+    case 1: return launch_march_t<Real, 4, 8>(V1, V2, waves, s, pdl);
+    case 2: return launch_march_t<Real, 16, 2>(V1, V2, waves, s, pdl);
+    case 3: return launch_march_t<Real, 6, 5>(V1, V2, waves, s, pdl);
+    case 5: return launch_march_t<Real, 8, 3>(V1, V2, waves, s, pdl);
+    default: return launch_march_t<Real, 8, 4>(V1, V2, waves, s, pdl);  // (0 and 4: 8 rows, 4 blocks)
+  }
+}
+
 template <typename Real>
 static cudaError_t launch_pair(const LBView<Real>& V1, const LBView<Real>& V2, int shape, cudaStream_t s, bool pdl) {
+  if (shape >= NPAIR) return launch_march<Real>(V1, V2, shape - NPAIR, s, pdl);
   switch (shape) {
     case 1: return launch_pair_t<Real, 32, 4, 128, 6>(V1, V2, s, pdl);
     case 2: return launch_pair_t<Real, 32, 16, 512, 2>(V1, V2, s, pdl);
@@ -361,7 +527,7 @@ static int tune_pair(const LBView<Real>& A, const LBView<Real>& B, cudaStream_t 
   const int reps = tune_reps(V1);
   int best = 0;
   float bt = 1e30f;
-  for (int sh = 0; sh < NPAIR; sh++) {
+  for (int sh = 0; sh < NUM_PAIR_SHAPES; sh++) {
     if (launch_pair<Real>(V1, V2, sh, s, false) != cudaSuccess) {
       cudaGetLastError();
       continue;

@@ -54,8 +54,11 @@ constexpr double CS2 = 1.0 / 3.0;
 // element offsets of a population buffer (18 planes) fit in 32 bits
 inline bool off32_ok(size_t plane) { return plane * 2 * NPOP < (size_t(1) << 32); }
 
-// tile shapes of the two-step kernel (lb_kernels.cu: PAIR_SHAPES)
-constexpr int NUM_PAIR_SHAPES = 9;
+// launch shapes of the two-step kernels (lb_kernels.cu): the tiles of
+// lb_pair_kernel (PAIR_SHAPES), then the marching lb_march_kernel
+// (MARCH_SHAPES)
+constexpr int NUM_PAIR_TILES = 9;
+constexpr int NUM_PAIR_SHAPES = NUM_PAIR_TILES + 6;
 // planes (of nx values) of a y-slab's ghost block for two steps per launch
 // (aux_kernels.cu: slab_pack2_kernel)
 constexpr int SLAB_GH2_PLANES = 19;

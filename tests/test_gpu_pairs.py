@@ -1,7 +1,9 @@
-"""Two steps per launch (lb_pair_kernel, lbrb_set_pairs): a run stepped in
-pairs ends bit-identical to the same run stepped one launch at a time --
+"""Two steps per launch (lb_pair_kernel, lb_march_kernel, lbrb_set_pairs): a
+run stepped in pairs ends bit-identical to the same run stepped one launch at
+a time --
 populations, moments, post-stream populations of the last step, particles
-and records -- for every tile shape and the tuned one, in both precisions, on
+and records -- for every launch shape (tiles and marching strips) and the tuned one, in
+both precisions, on
 grids whose width and height are not multiples of the tile, with records on
 the first and on the second step of a pair, tracers and inertial particles
 with the Maxey-Riley stencil and full records, and without particles."""
@@ -52,9 +54,17 @@ def state(r, nprtcl):
     return out
 
 
+NSHAPES = 15  # lbrb_pair_shapes(): 9 tiles, then 6 marching shapes
+MARCH = list(range(9, NSHAPES))
+
+
+def test_shape_count():
+    assert lb.Run.pair_shapes() == NSHAPES
+
+
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("nprtcl,beta,full", [(0, 0.0, 0), (80, 0.0, 0), (80, 0.5, 1)])
-@pytest.mark.parametrize("shape", [-1, 0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("shape", [-1] + list(range(NSHAPES)))
 def test_pairs_equal_single_steps(precision, nprtcl, beta, full, shape):
     nx, ny = 200, 37
     with make(precision, nx, ny, nprtcl, beta, full, 0, -1) as a, \
@@ -71,13 +81,28 @@ def test_pairs_equal_single_steps(precision, nprtcl, beta, full, shape):
         assert a.pair_shape()["shape"] == -1
 
 
-def test_pairs_on_a_tile_multiple_grid():
-    with make("fp32", 64, 48, 40, 0.0, 0, 0, -1) as a, make("fp32", 64, 48, 40, 0.0, 0, 1, 0) as b:
+@pytest.mark.parametrize("shape", [0, 9, 10, 11])
+def test_pairs_on_a_tile_multiple_grid(shape):
+    with make("fp32", 64, 48, 40, 0.0, 0, 0, -1) as a, make("fp32", 64, 48, 40, 0.0, 0, 1, shape) as b:
         a.step(100)
         b.step(100)
         sa, sb = state(a, 40), state(b, 40)
         for k in sa:
             np.testing.assert_array_equal(sb[k], sa[k], err_msg=k)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("shape", MARCH)
+def test_march_on_many_chunks(precision, shape):
+    """a grid tall enough for several chunks per strip and several strips,
+    width not a multiple of 32: chunk edges, strip edges and the x wrap"""
+    with make(precision, 232, 700, 60, 0.5, 1, 0, -1) as a, make(precision, 232, 700, 60, 0.5, 1, 1, shape) as b:
+        for n in (9, 14):
+            a.step(n)
+            b.step(n)
+            sa, sb = state(a, 60), state(b, 60)
+            for k in sa:
+                np.testing.assert_array_equal(sb[k], sa[k], err_msg=k)
 
 
 def test_record_ring_overflow_is_reported_at_the_same_step():
@@ -102,7 +127,7 @@ def test_pair_arguments_checked():
         for bad in (-2, 2):
             with pytest.raises(lb.LbrbError):
                 r.set_pairs(bad)
-        for bad in (-2, 9):
+        for bad in (-2, NSHAPES):
             with pytest.raises(lb.LbrbError):
                 r.set_pair_shape(bad)
 
@@ -111,7 +136,7 @@ def test_pair_arguments_checked():
 def test_pairs_on_grids_smaller_than_a_tile(precision):
     """8 x 5 nodes: the ring wraps onto the tile itself in x, and every row
     is a wall row or next to one"""
-    for shape in (0, 5, 8):
+    for shape in (0, 5, 8, *MARCH):
         with make(precision, 8, 5, 6, 0.0, 0, 0, -1) as a, make(precision, 8, 5, 6, 0.0, 0, 1, shape) as b:
             for n in (3, 7):
                 a.step(n)

@@ -27,8 +27,15 @@ def params(precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("heights", [(24, 24), (20, 17, 11), (3, 42, 3)])
-def test_slabs_advance_as_the_whole_domain(precision, heights):
+@pytest.mark.parametrize("shape", [-1, 0, 9, 10])
+def test_slabs_advance_as_the_whole_domain(precision, heights, shape):
+    """shape: the two-step launch shape of the slabs (-1 tuned; 0 a tile;
+    9, 10 marching strips, whose rows beyond an inner boundary come from
+    the ghost blocks)"""
     with lb.Run(**params(precision)) as whole, lb.SlabDomain(heights, **params(precision)) as dom:
+        if shape >= 0:
+            for r in dom.slabs:
+                r.set_pair_shape(shape)
         whole.init_conduction(17, 2e-2)
         dom.init_conduction(17, 2e-2)
         fw, gw = whole.get_populations()
