@@ -329,6 +329,28 @@ def e2e(lb, torch, precision: str, seed: int, steps: int, device: int, dist):
     return ms, h2d, d2h
 
 
+def pinned_copy_rates(torch, device: int, nbytes: int = 1 << 29) -> tuple[float, float]:
+    """host<->device copy rates (GB/s) of pinned memory on this box: one
+    cudaMemcpyAsync each way of `nbytes`, timed with CUDA events after a
+    warm-up copy"""
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{device}")
+    rates = []
+    for to_dev in (True, False):
+        for rep in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if to_dev:
+                d.copy_(h, non_blocking=True)
+            else:
+                h.copy_(d, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+        rates.append(nbytes / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del h, d
+    return rates[0], rates[1]
+
+
 def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | None:
     import lagrangianrbnudging_b200 as lb
     from lagrangianrbnudging_b200 import build as b
@@ -379,6 +401,7 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     if not args.no_e2e:
         e2e_ms, e2e_h2d, e2e_d2h = e2e(lb, torch, "fp32", seed, K, device, dist)
         e2e_ms = max_over_ranks(torch, dist, e2e_ms)
+        h2d_gbs, d2h_gbs = pinned_copy_rates(torch, device)
     # sections with independent units: every rank takes its share (replicas
     # for the adjoint window's timing), results gathered once
     sec = {}
@@ -462,6 +485,9 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
         out["e2e"] = {"value": round(world * nodes * K / (e2e_ms * 1e3), 1), "unit": "MLUPS",
                       "h2d_bytes_per_step": int(e2e_h2d / K), "d2h_bytes_per_step": int(e2e_d2h / K),
                       "ms": round(e2e_ms, 2),
+                      # the copies alone at this box's pinned rates, plus the device-timed steps
+                      "pinned_h2d_gbs": round(h2d_gbs, 1), "pinned_d2h_gbs": round(d2h_gbs, 1),
+                      "copy_bound_ms": round(e2e_h2d / h2d_gbs / 1e6 + e2e_d2h / d2h_gbs / 1e6 + ms, 2),
                       "path": "lbrb_set_populations(REF_AOS_HALO fp64) + set_moments + particles_set + "
                               "lbrb_step in chunks of 500 steps, each chunk's records drained (lbrb_record_drain) "
                               "while the next runs + get_moments"}

@@ -95,7 +95,10 @@ typedef struct {
   int record_full;        /* Prtcl_Writefull: also record the 8 Maxey-Riley terms */
   int record_slots;       /* records held before lbrb_record_drain() must run */
   int device;             /* CUDA device ordinal */
-  int autotune;           /* 1: time the fused kernel's launch shapes on the first step */
+  int autotune;           /* 1: time the fused kernel's launch shapes on the first step
+                           * (once per process for handles on the same device with
+                           * the same grid, precision, walls, nudging mode, particle
+                           * use and slab position: later handles reuse the result) */
   int launch_shape;       /* with autotune 0: the shape used, an index into
                            * (threads per block, min blocks per SM) =
                            * (256,1) (256,2) (256,3) (128,4) (128,6) (512,1) (512,2)
@@ -174,7 +177,8 @@ LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
  * -1 (the default) and 1: pairs of steps that do not replay graphs; 0: off.
  * Used with Dirichlet walls, without nudging, not on a y-slab, and never for
  * the last step of a call (so lbrb_get_poststream keeps its meaning).
- * The tile shape is timed on first use; lbrb_get_pair_shape reports it
+ * The launch shape is timed on first use (once per process for handles
+ * of the same kind, as for autotune); lbrb_get_pair_shape reports it
  * (shape index, tile columns and rows, ms per launch; shape -1 before).
  * Replaces, for two steps at a time, the reference's per-step sweeps
  * (stream, moments, collide: temppart_dump.c:1674-1759). */

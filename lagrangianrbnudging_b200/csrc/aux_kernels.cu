@@ -103,6 +103,68 @@ __global__ void scalar_out_kernel(const Real* __restrict__ d, int layout, double
   }
 }
 
+// ------------------------------------------------ chunked host transfers
+// A host array moves in chunks of whole units through a staging slot.  A unit
+// is one halo column of the reference layout ((ny + 2) nodes of NP values:
+// unit a starts at host element a (ny + 2) NP) or one row of nx values of the
+// SoA layout (row r = k ny + j of population plane k, or row j of a scalar
+// field: unit r starts at host element r nx).  The staging slot holds units
+// [u0, u1) as they lie in the host array.  NP: 9 populations (FP32 handles
+// store them shifted by w_k base), or 1 for a scalar field.
+template <typename Real, int NP>
+__global__ void units_in_kernel(const double* __restrict__ st, int layout, Real* __restrict__ d, int nx, int ny,
+                                int pitch, size_t plane, double base, int u0, int u1) {
+  auto cv = [&](double a, int k) -> Real {
+    if constexpr (std::is_same<Real, double>::value) return a;
+    else return NP == NPOP ? (float)(a - w_of(k) * base) : (float)a;
+  };
+  if (layout == LBRB_LAYOUT_REF_AOS_HALO) {
+    // interior nodes of halo columns [u0, u1) (1 <= u0, u1 <= nx + 1)
+    const long n = (long)(u1 - u0) * ny;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+      const int a = u0 + (int)(q / ny), j = (int)(q % ny);
+      const double* src = st + ((size_t)(a - u0) * (ny + 2) + (j + 1)) * NP;
+#pragma unroll
+      for (int k = 0; k < NP; k++) d[(size_t)k * plane + (size_t)j * pitch + (a - 1)] = cv(src[k], k);
+    }
+  } else {
+    const long n = (long)(u1 - u0) * nx;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+      const int r = u0 + (int)(q / nx), i = (int)(q % nx);
+      const int k = r / ny, j = r % ny;
+      d[(size_t)k * plane + (size_t)j * pitch + i] = cv(st[(size_t)(r - u0) * nx + i], k);
+    }
+  }
+}
+
+// the other way; the reference layout's halo holds periodic copies in x and
+// y (what pbc() leaves, temppart_dump.c:234-250)
+template <typename Real, int NP>
+__global__ void units_out_kernel(const Real* __restrict__ d, int layout, double* __restrict__ st, int nx, int ny,
+                                 int pitch, size_t plane, double base, int u0, int u1) {
+  auto cv = [&](Real a, int k) -> double {
+    if constexpr (std::is_same<Real, double>::value) return a;
+    else return NP == NPOP ? (double)a + w_of(k) * base : (double)a;
+  };
+  if (layout == LBRB_LAYOUT_REF_AOS_HALO) {
+    const long n = (long)(u1 - u0) * (ny + 2);
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+      const int a = u0 + (int)(q / (ny + 2)), b = (int)(q % (ny + 2));
+      const int i = wrapn(a - 1, nx), j = wrapn(b - 1, ny);
+      double* dst = st + ((size_t)(a - u0) * (ny + 2) + b) * NP;
+#pragma unroll
+      for (int k = 0; k < NP; k++) dst[k] = cv(d[(size_t)k * plane + (size_t)j * pitch + i], k);
+    }
+  } else {
+    const long n = (long)(u1 - u0) * nx;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+      const int r = u0 + (int)(q / nx), i = (int)(q % nx);
+      const int k = r / ny, j = r % ny;
+      st[(size_t)(r - u0) * nx + i] = cv(d[(size_t)k * plane + (size_t)j * pitch + i], k);
+    }
+  }
+}
+
 // buoyancy of the first step from the moments in place (forcingconstructWW)
 template <typename Real>
 __global__ void force_kernel(const Real* __restrict__ rho, const Real* __restrict__ T,
@@ -337,6 +399,25 @@ cudaError_t launch_pops_out(const void* d, int layout, double* h, bool fp32, int
   const int g = grid_for((long)(nx + 2) * (ny + 2));
   if (fp32) pops_out_kernel<float><<<g, 256, 0, s>>>((const float*)d, layout, h, nx, ny, pitch, plane, base);
   else pops_out_kernel<double><<<g, 256, 0, s>>>((const double*)d, layout, h, nx, ny, pitch, plane, base);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_units(bool in, const void* src, void* dst, int layout, int npop, bool fp32, int nx, int ny,
+                         int pitch, size_t plane, double base, int u0, int u1, cudaStream_t s) {
+  const long per = layout == LBRB_LAYOUT_REF_AOS_HALO ? (long)(ny + 2) : (long)nx;
+  const int g = grid_for((long)(u1 - u0) * per);
+  if (u1 <= u0) return cudaSuccess;
+#define LBRB_UNITS(R, NPV)                                                                                   \
+  if (in) units_in_kernel<R, NPV><<<g, 256, 0, s>>>((const double*)src, layout, (R*)dst, nx, ny, pitch, plane, \
+                                                    base, u0, u1);                                           \
+  else units_out_kernel<R, NPV><<<g, 256, 0, s>>>((const R*)src, layout, (double*)dst, nx, ny, pitch, plane,  \
+                                                  base, u0, u1);
+  if (fp32) {
+    if (npop == NPOP) { LBRB_UNITS(float, NPOP) } else { LBRB_UNITS(float, 1) }
+  } else {
+    if (npop == NPOP) { LBRB_UNITS(double, NPOP) } else { LBRB_UNITS(double, 1) }
+  }
+#undef LBRB_UNITS
   return cudaGetLastError();
 }
 

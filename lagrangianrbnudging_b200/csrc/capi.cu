@@ -12,7 +12,10 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -36,15 +39,120 @@ static size_t host_scalar_count(const lbrb_t* h, int layout) {
                                             : (size_t)h->p.nx * h->p.ny;
 }
 
-static int ensure_staging(lbrb_t* h, size_t bytes) {
-  if (h->staging_bytes >= bytes) return LBRB_OK;
-  if (h->staging) cudaFree(h->staging);
-  h->staging = nullptr;
-  h->staging_bytes = 0;
-  cudaError_t e = cudaMalloc(&h->staging, bytes);
-  if (e != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "staging allocation", e);
-  h->staging_bytes = bytes;
+// Launch shapes timed once per process: a handle on the same device with the
+// same grid, precision, walls, nudging mode, particle use and slab ghost rows
+// starts with the shapes an earlier handle timed, without trial launches.
+struct TuneKey {
+  int dev, nx, ny, pitch, esize, twall, nudge, parts, ghosts;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, nx, ny, pitch, esize, twall, nudge, parts, ghosts) <
+           std::tie(o.dev, o.nx, o.ny, o.pitch, o.esize, o.twall, o.nudge, o.parts, o.ghosts);
+  }
+};
+struct TuneVal {
+  int shape;
+  float ms;
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneVal> g_tuned_single, g_tuned_pair;
+static TuneKey tune_key(const lbrb_t* h) {
+  return {h->dev, h->p.nx, h->p.ny, h->pitch, (int)h->esize, h->p.twall, h->p.nudge, h->np > 0 ? 1 : 0,
+          (h->slab_gh2_lo ? 1 : 0) | (h->slab_gh2_hi ? 2 : 0) | (h->slab ? 4 : 0)};
+}
+static bool tuned_get(std::map<TuneKey, TuneVal>& m, const lbrb_t* h, int* shape, float* ms) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = m.find(tune_key(h));
+  if (it == m.end()) return false;
+  *shape = it->second.shape;
+  *ms = it->second.ms;
+  return true;
+}
+static void tuned_put(std::map<TuneKey, TuneVal>& m, const lbrb_t* h, int shape, float ms) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  m[tune_key(h)] = {shape, ms};
+}
+
+// the full-size scratch of the rare paths (restart-route moments, post-stream
+// dump), allocated on first use
+static int ensure_big(lbrb_t* h, size_t bytes) {
+  if (h->big_bytes >= bytes) return LBRB_OK;
+  if (h->big) cudaFree(h->big);
+  h->big = nullptr;
+  h->big_bytes = 0;
+  cudaError_t e = cudaMalloc(&h->big, bytes);
+  if (e != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "scratch allocation", e);
+  h->big_bytes = bytes;
   return LBRB_OK;
+}
+
+// bytes per staging slot: 64 MB, or the largest host array if smaller, and
+// at least one transfer unit (a halo column of populations or a row)
+constexpr size_t STAGE_SLOT_DOUBLES = (size_t)8 << 20;
+static size_t stage_slot_doubles(const lbrb_params& p) {
+  const size_t full = (size_t)(p.nx + 2) * (p.ny + 2) * NPOP;
+  const size_t unit = std::max((size_t)(p.ny + 2) * NPOP, (size_t)p.nx);
+  return std::max(unit, std::min(full, STAGE_SLOT_DOUBLES));
+}
+
+// Host <-> device transfer of units [ub, ue) of a host array in `layout`
+// (unit u = `unit` doubles at host element u * unit; aux_kernels.cu, units_*),
+// chunk by chunk through the two staging slots; conv(slot, u0, u1) converts a
+// chunk on the handle's stream.  Upload: the copy of the next chunk (copy
+// stream) overlaps the conversion of this one; download: the conversion of
+// the next chunk overlaps the copy of this one.  A slot is reused only after
+// the last work that read it (events), also across calls; the caller
+// synchronises at the end.  One cudaMemcpyAsync per chunk.
+template <typename Conv>
+static int xfer_units(lbrb_t* h, bool in, double* host, size_t unit, int ub, int ue, Conv&& conv) {
+  const int per = (int)std::max<size_t>(1, h->stage_slot / unit);
+  double* slot[2] = {(double*)h->staging, (double*)h->staging + h->stage_slot};
+  cudaEvent_t* copied = h->xfer_ev;
+  cudaEvent_t* converted = h->xfer_ev + 2;
+  int c = 0;
+  for (int u0 = ub; u0 < ue; u0 += per, c++) {
+    const int u1 = std::min(ue, u0 + per), sl = c & 1;
+    const size_t bytes = (size_t)(u1 - u0) * unit * sizeof(double);
+    double* hp = host + (size_t)u0 * unit;
+    if (in) {
+      CK(h, cudaStreamWaitEvent(h->copy_stream, converted[sl], 0));  // the slot's last conversion read it
+      CK(h, cudaMemcpyAsync(slot[sl], hp, bytes, cudaMemcpyHostToDevice, h->copy_stream));
+      CK(h, cudaEventRecord(copied[sl], h->copy_stream));
+      CK(h, cudaStreamWaitEvent(h->stream, copied[sl], 0));
+      CK(h, conv(slot[sl], u0, u1));
+      CK(h, cudaEventRecord(converted[sl], h->stream));
+    } else {
+      CK(h, cudaStreamWaitEvent(h->stream, copied[sl], 0));  // the slot's last copy read it
+      CK(h, conv(slot[sl], u0, u1));
+      CK(h, cudaEventRecord(converted[sl], h->stream));
+      CK(h, cudaStreamWaitEvent(h->copy_stream, converted[sl], 0));
+      CK(h, cudaMemcpyAsync(hp, slot[sl], bytes, cudaMemcpyDeviceToHost, h->copy_stream));
+      CK(h, cudaEventRecord(copied[sl], h->copy_stream));
+    }
+  }
+  return LBRB_OK;
+}
+
+// units of a host array: populations (npop = 9) or a scalar field (npop = 1);
+// uploads skip the reference layout's halo columns (units 0 and nx + 1)
+static size_t unit_doubles(const lbrb_t* h, int layout, int npop) {
+  return layout == LBRB_LAYOUT_REF_AOS_HALO ? (size_t)(h->p.ny + 2) * npop : (size_t)h->p.nx;
+}
+static void unit_range(const lbrb_t* h, int layout, int npop, bool in, int* ub, int* ue) {
+  if (layout == LBRB_LAYOUT_REF_AOS_HALO) {
+    *ub = in ? 1 : 0;
+    *ue = in ? h->p.nx + 1 : h->p.nx + 2;
+  } else {
+    *ub = 0;
+    *ue = npop * h->p.ny;
+  }
+}
+static int xfer_array(lbrb_t* h, bool in, double* host, void* dev, int layout, int npop, double base) {
+  int ub, ue;
+  unit_range(h, layout, npop, in, &ub, &ue);
+  return xfer_units(h, in, host, unit_doubles(h, layout, npop), ub, ue, [&](double* st, int u0, int u1) {
+    return launch_units(in, in ? (const void*)st : dev, in ? dev : (void*)st, layout, npop, fp32(h), h->p.nx,
+                        h->p.ny, h->pitch, h->plane, base, u0, u1, h->stream);
+  });
 }
 
 // Host copies out of the pinned record ring.  A large drain (hundreds of MB
@@ -130,7 +238,7 @@ static void free_all(lbrb_t* h) {
   F(h->nb); F(h->nbi); F(h->nudge_vol); F(h->tempreadint); F(h->nud_term); F(h->tsum0);
   F(h->cell_count); F(h->cell_start); F(h->cell_fill); F(h->cell_dirty); F(h->cell_items);
   delete[] h->h_chk; delete[] h->h_oid;
-  F(h->obs); F(h->acc); F(h->staging); F(h->red); F(h->dflags);
+  F(h->obs); F(h->acc); F(h->staging); F(h->big); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
   F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down); F(h->slab_own); F(h->slab_tab);
   F(h->slab_gh2_lo); F(h->slab_gh2_hi); F(h->slab_up2); F(h->slab_down2);
@@ -145,6 +253,8 @@ static void free_all(lbrb_t* h) {
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->join_ev) cudaEventDestroy(h->join_ev);
+  for (cudaEvent_t e : h->xfer_ev)
+    if (e) cudaEventDestroy(e);
   if (h->pstream) cudaStreamDestroy(h->pstream);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
 }
@@ -237,6 +347,11 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
   if (p.nudge == LBRB_NUDGE_BILINEAR) {
     if (dalloc(&h->acc, h->plane)) return done(LBRB_ERR_NOMEM);
   }
+  h->stage_slot = stage_slot_doubles(p);
+  h->staging_bytes = 2 * h->stage_slot * sizeof(double);
+  if (cudaMalloc(&h->staging, h->staging_bytes) != cudaSuccess) return done(LBRB_ERR_NOMEM);
+  for (cudaEvent_t& ev : h->xfer_ev)
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return done(LBRB_ERR_CUDA);
   if (dalloc(&h->red, (size_t)red_blocks() * 6 + 8 + (size_t)p.ny * 9)) return done(LBRB_ERR_NOMEM);
   if (dalloc(&h->dflags, 1)) return done(LBRB_ERR_NOMEM);
   if (cudaMallocHost(&h->h_flags, sizeof(unsigned)) != cudaSuccess) return done(LBRB_ERR_NOMEM);
@@ -273,16 +388,12 @@ int lbrb_set_populations(lbrb_t* h, const double* f, const double* g, int layout
   if (!h || !f || !g || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
     return fail(h, LBRB_ERR_ARG, "set_populations: bad arguments");
   CK(h, cudaSetDevice(h->dev));
-  const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
-  int rc = ensure_staging(h, 2 * bytes);
-  if (rc) return rc;
-  double* st = (double*)h->staging;
-  CK(h, cudaMemcpyAsync(st, f, bytes, cudaMemcpyHostToDevice, h->stream));
-  CK(h, cudaMemcpyAsync(st + cnt, g, bytes, cudaMemcpyHostToDevice, h->stream));
-  CK(h, launch_pops_in(st, layout, pop_base(h, h->cur, 0), fp32(h), h->p.nx, h->p.ny, h->pitch,
-                       h->plane, 1.0, h->stream));
-  CK(h, launch_pops_in(st + cnt, layout, pop_base(h, h->cur, 1), fp32(h), h->p.nx, h->p.ny,
-                       h->pitch, h->plane, T0_of(h), h->stream));
+  const double* src[2] = {f, g};
+  for (int a = 0; a < 2; a++) {
+    const int rc = xfer_array(h, true, const_cast<double*>(src[a]), pop_base(h, h->cur, a), layout, NPOP,
+                              a ? T0_of(h) : 1.0);
+    if (rc) return rc;
+  }
   CK(h, cudaStreamSynchronize(h->stream));
   h->prev_valid = false;
   return LBRB_OK;
@@ -292,21 +403,13 @@ int lbrb_get_populations(lbrb_t* h, double* f, double* g, int layout) {
   if (!h || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
     return fail(h, LBRB_ERR_ARG, "get_populations: bad arguments");
   CK(h, cudaSetDevice(h->dev));
-  const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
-  int rc = ensure_staging(h, 2 * bytes);
-  if (rc) return rc;
-  double* st = (double*)h->staging;
-  if (f) {
-    CK(h, launch_pops_out(pop_base(h, h->cur, 0), layout, st, fp32(h), h->p.nx, h->p.ny, h->pitch,
-                          h->plane, 1.0, h->stream));
-    CK(h, cudaMemcpyAsync(f, st, bytes, cudaMemcpyDeviceToHost, h->stream));
+  double* dst[2] = {f, g};
+  for (int a = 0; a < 2; a++) {
+    if (!dst[a]) continue;
+    const int rc = xfer_array(h, false, dst[a], pop_base(h, h->cur, a), layout, NPOP, a ? T0_of(h) : 1.0);
+    if (rc) return rc;
   }
-  if (g) {
-    CK(h, launch_pops_out(pop_base(h, h->cur, 1), layout, st + cnt, fp32(h), h->p.nx, h->p.ny,
-                          h->pitch, h->plane, T0_of(h), h->stream));
-    CK(h, cudaMemcpyAsync(g, st + cnt, bytes, cudaMemcpyDeviceToHost, h->stream));
-  }
-  CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaStreamSynchronize(h->copy_stream));
   return LBRB_OK;
 }
 
@@ -315,15 +418,11 @@ int lbrb_set_moments(lbrb_t* h, const double* rho, const double* u, const double
   if (!h || !rho || !u || !v || !T || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
     return fail(h, LBRB_ERR_ARG, "set_moments: bad arguments");
   CK(h, cudaSetDevice(h->dev));
-  const size_t cnt = host_scalar_count(h, layout), bytes = cnt * sizeof(double);
-  int rc = ensure_staging(h, 4 * bytes);
-  if (rc) return rc;
-  double* st = (double*)h->staging;
   const double* src[4] = {rho, u, v, T};
   void* dst[4] = {h->rho[h->cur], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[h->cur]};
   for (int a = 0; a < 4; a++) {
-    CK(h, cudaMemcpyAsync(st + a * cnt, src[a], bytes, cudaMemcpyHostToDevice, h->stream));
-    CK(h, launch_scalar_in(st + a * cnt, layout, dst[a], fp32(h), h->p.nx, h->p.ny, h->pitch, h->stream));
+    const int rc = xfer_array(h, true, const_cast<double*>(src[a]), dst[a], layout, 1, 0.0);
+    if (rc) return rc;
   }
   CK(h, launch_force(h->rho[h->cur], h->T[h->cur], h->F[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, -h->p.gravity, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
@@ -335,18 +434,14 @@ int lbrb_get_moments(lbrb_t* h, double* rho, double* u, double* v, double* T, in
   if (!h || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
     return fail(h, LBRB_ERR_ARG, "get_moments: bad arguments");
   CK(h, cudaSetDevice(h->dev));
-  const size_t cnt = host_scalar_count(h, layout), bytes = cnt * sizeof(double);
-  int rc = ensure_staging(h, 4 * bytes);
-  if (rc) return rc;
-  double* st = (double*)h->staging;
   double* dst[4] = {rho, u, v, T};
   const void* src[4] = {h->rho[h->cur], h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->T[h->cur]};
   for (int a = 0; a < 4; a++) {
     if (!dst[a]) continue;
-    CK(h, launch_scalar_out(src[a], layout, st + a * cnt, fp32(h), h->p.nx, h->p.ny, h->pitch, h->stream));
-    CK(h, cudaMemcpyAsync(dst[a], st + a * cnt, bytes, cudaMemcpyDeviceToHost, h->stream));
+    const int rc = xfer_array(h, false, dst[a], const_cast<void*>(src[a]), layout, 1, 0.0);
+    if (rc) return rc;
   }
-  CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaStreamSynchronize(h->copy_stream));
   return LBRB_OK;
 }
 
@@ -355,9 +450,9 @@ int lbrb_moments_from_pre(lbrb_t* h, const double* fpre, const double* gpre, int
     return fail(h, LBRB_ERR_ARG, "moments_from_pre: bad arguments");
   CK(h, cudaSetDevice(h->dev));
   const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
-  int rc = ensure_staging(h, 2 * bytes);
+  int rc = ensure_big(h, 2 * bytes);
   if (rc) return rc;
-  double* st = (double*)h->staging;
+  double* st = (double*)h->big;
   CK(h, cudaMemcpyAsync(st, fpre, bytes, cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(st + cnt, gpre, bytes, cudaMemcpyHostToDevice, h->stream));
   CK(h, launch_moments_from_pre(st, st + cnt, layout, h->rho[h->cur], h->uv[h->uvcur][0],
@@ -581,9 +676,9 @@ int lbrb_get_poststream(lbrb_t* h, double* f, double* g, int layout) {
   CK(h, cudaSetDevice(h->dev));
   const size_t tmp = 2 * NPOP * h->plane * h->esize;
   const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
-  int rc = ensure_staging(h, tmp + 2 * bytes);
+  int rc = ensure_big(h, tmp + 2 * bytes);
   if (rc) return rc;
-  char* t = (char*)h->staging;
+  char* t = (char*)h->big;
   double* st = (double*)(t + tmp);
   const int prev = h->cur ^ 1;
   if (fp32(h)) CK(h, launch_pull_fp32(make_view<float>(h, prev, h->cur, h->uvcur, 0, 0), h->p.twall, t, t + tmp / 2, h->stream));
@@ -659,12 +754,14 @@ int lbrb_step(lbrb_t* h, int n) {
     // write only the buffers the real step overwrites)
     int sh = h->p.launch_shape;
     float ms = 0.f;
-    if (h->p.autotune && !refbox) {
+    if (h->p.autotune && !refbox && !tuned_get(g_tuned_single, h, &sh, &ms)) {
       // trials store u, v as the steps will (particles need them every step),
       // into the slot the first step overwrites
       const int tuv = h->np > 0 ? 3 - h->uvcur - h->uvprev : h->uvcur;
       if (f32) sh = tune_lb_fp32(make_view<float>(h, h->cur, h->cur ^ 1, tuv, h->np > 0, 0), h->p.twall, h->stream, &ms);
       else sh = tune_lb_fp64(make_view<double>(h, h->cur, h->cur ^ 1, tuv, h->np > 0, 0), h->p.twall, h->stream, &ms);
+      CK(h, cudaGetLastError());
+      tuned_put(g_tuned_single, h, sh, ms);
     }
     CK(h, cudaGetLastError());
     h->lb_shape = sh;
@@ -833,14 +930,17 @@ int lbrb_step(lbrb_t* h, int n) {
     {
       float ms = 0.f;
       int sh = 0;
-      if (f32) {
-        LBView<float> t1 = make_view<float>(h, src, dst, A, wuv, 0), t2 = make_view<float>(h, dst, dst, B, wuv, 0);
-        sh = tune_pair_fp32(t1, t2, h->stream, &ms);
-      } else {
-        LBView<double> t1 = make_view<double>(h, src, dst, A, wuv, 0), t2 = make_view<double>(h, dst, dst, B, wuv, 0);
-        sh = tune_pair_fp64(t1, t2, h->stream, &ms);
+      if (!tuned_get(g_tuned_pair, h, &sh, &ms)) {
+        if (f32) {
+          LBView<float> t1 = make_view<float>(h, src, dst, A, wuv, 0), t2 = make_view<float>(h, dst, dst, B, wuv, 0);
+          sh = tune_pair_fp32(t1, t2, h->stream, &ms);
+        } else {
+          LBView<double> t1 = make_view<double>(h, src, dst, A, wuv, 0), t2 = make_view<double>(h, dst, dst, B, wuv, 0);
+          sh = tune_pair_fp64(t1, t2, h->stream, &ms);
+        }
+        CK(h, cudaGetLastError());
+        tuned_put(g_tuned_pair, h, sh, ms);
       }
-      CK(h, cudaGetLastError());
       h->pair_shape = sh;
       h->pair_ms = ms;
       // automatic mode keeps pairs only where one beats two tuned single launches
@@ -1425,14 +1525,19 @@ static int slab_pair_launch(lbrb_t* h, bool rec1, bool rec2, bool last) {
     // the tile shape, timed on first use (trial launches write only what the
     // two steps overwrite)
     float ms = 0.f;
-    if (fp32(h)) {
-      auto v = views(0.f, 0, 0, wuv);
-      h->pair_shape = tune_pair_fp32(v.first, v.second, h->stream, &ms);
-    } else {
-      auto v = views(0.0, 0, 0, wuv);
-      h->pair_shape = tune_pair_fp64(v.first, v.second, h->stream, &ms);
+    int sh = 0;
+    if (!tuned_get(g_tuned_pair, h, &sh, &ms)) {
+      if (fp32(h)) {
+        auto v = views(0.f, 0, 0, wuv);
+        sh = tune_pair_fp32(v.first, v.second, h->stream, &ms);
+      } else {
+        auto v = views(0.0, 0, 0, wuv);
+        sh = tune_pair_fp64(v.first, v.second, h->stream, &ms);
+      }
+      CK(h, cudaGetLastError());
+      tuned_put(g_tuned_pair, h, sh, ms);
     }
-    CK(h, cudaGetLastError());
+    h->pair_shape = sh;
     h->pair_ms = ms;
   }
   const int r2 = last ? 3 : (rec2 ? 1 : 0), w2 = last ? 1 : wuv;

@@ -70,6 +70,10 @@ cudaError_t launch_pops_out(const void* d, int layout, double* h, bool fp32, int
                             int pitch, size_t plane, double base, cudaStream_t s);
 cudaError_t launch_scalar_in(const double* h, int layout, void* d, bool fp32, int nx, int ny,
                              int pitch, cudaStream_t s);
+// units [u0, u1) of a host-layout array between a staging slot and the device
+// (in: slot -> device; out: device -> slot); aux_kernels.cu describes units
+cudaError_t launch_units(bool in, const void* src, void* dst, int layout, int npop, bool fp32, int nx, int ny,
+                         int pitch, size_t plane, double base, int u0, int u1, cudaStream_t s);
 cudaError_t launch_scalar_out(const void* d, int layout, double* h, bool fp32, int nx, int ny,
                               int pitch, cudaStream_t s);
 cudaError_t launch_force(const void* rho, const void* T, void* F, bool fp32, int nx, int ny,

@@ -349,9 +349,17 @@ struct Handle {
   long long* adj_lT = nullptr;       // 2 fixed-point lambda T planes (the steps of a pair)
   double* adj_T0 = nullptr;          // [ny*nx] initial temperature / gradient
   int adj_pair_variant = -1;         // launch variant of the pair kernel (-1: tune at first use)
-  // scratch / staging
+  // scratch / staging: host transfers go through two staging slots of
+  // stage_slot doubles each (allocated at create), chunk by chunk, with
+  // events xfer_ev (copied[2], converted[2]) ordering the slots' reuse; the
+  // restart route's moments and the post-stream dump use `big`, a full-size
+  // scratch allocated on their first use
   void* staging = nullptr;
   size_t staging_bytes = 0;
+  size_t stage_slot = 0;
+  cudaEvent_t xfer_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* big = nullptr;
+  size_t big_bytes = 0;
   double* red = nullptr;    // reduction partials
   unsigned* dflags = nullptr;
   unsigned* h_flags = nullptr;
