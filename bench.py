@@ -666,6 +666,53 @@ def run_accuracy(lb, device: int, steps: int = ACC_STEPS, every: int = ACC_EVERY
             "bar": "time-averaged Nu within 0.5% of FP64"}
 
 
+def batch_mean_se(x: np.ndarray, nbatch: int = 10) -> tuple[float, float]:
+    """mean and its standard error from `nbatch` batch means (the samples of
+    a turbulent time series are correlated; batches longer than the
+    correlation time are not)"""
+    n = len(x) // nbatch * nbatch
+    b = x[len(x) - n:].reshape(nbatch, -1).mean(axis=1)
+    return float(x.mean()), float(b.std(ddof=1) / np.sqrt(nbatch))
+
+
+def run_stationary_nu(lb, device: int, tff: float = 6.0, discard: float = 3.0, every: int = 200) -> dict:
+    """FP32-shifted against FP64 on the production grid (4096x2048, Ra=1e8,
+    U=0.05) from the same seeded state over `tff` free-fall times Ny/U
+    (40,960 steps each), the first `discard` dropped as the onset transient:
+    time-averaged volume Nusselt number, row-profile Nusselt number (the
+    per-row ingredients of the reference's profile()), <u^2> and their
+    standard errors, sampled every `every` steps."""
+    base = lb.closure(NX, NY, Ra=RA, Pr=PR, U=U)
+    t_ff = int(NY / U)
+    total, skip = int(tff * t_ff) // every * every, int(discard * t_ff) // every
+    out = {"mode": "nu-stationary", "grid": f"{NX}x{NY}", "Ra": RA, "free_fall_steps": t_ff,
+           "steps": total, "discarded_steps": skip * every, "sampled_every": every}
+    series = {}
+    for prec in ("fp32", "fp64"):
+        with lb.Run(**base, precision=prec, device=device) as r:
+            r.init_conduction(SEED, 1e-3)
+            nu, nup, u2 = [], [], []
+            t0 = time.perf_counter()
+            for _ in range(total // every):
+                r.step(every)
+                nu.append(r.nusselt())
+                nup.append(float(np.mean(r.profile()[:, 8])))
+                u2.append(2.0 * r.energy()[0])
+            wall = time.perf_counter() - t0
+        series[prec] = {k: np.array(v)[skip:] for k, v in (("nu", nu), ("nu_profile", nup), ("u2", u2))}
+        out[prec] = {"wall_s": round(wall, 1), "nu_series_every_ff": [round(nu[i], 4) for i in
+                                                                         range(0, len(nu), t_ff // every)]}
+        for k, a in series[prec].items():
+            m, se = batch_mean_se(a)
+            out[prec][k] = {"mean": m, "se": se}
+    for k in ("nu", "nu_profile", "u2"):
+        a, b = out["fp32"][k], out["fp64"][k]
+        out[f"{k}_rel_diff"] = abs(a["mean"] - b["mean"]) / abs(b["mean"])
+        out[f"{k}_rel_se_of_diff"] = float(np.hypot(a["se"], b["se"]) / abs(b["mean"]))
+    out["bar"] = "time-averaged Nu of FP32 within 0.5% of FP64"
+    return out
+
+
 # ------------------------------------------------------------- nudging twin
 NUD_NX, NUD_NY, NUD_RA, NUD_TRACERS, NUD_STEPS, NUD_CHUNK = 2048, 1024, 1e7, 1 << 14, 50000, 250
 NUD_ALPHAS = (0.01, 0.1, 1.0)
@@ -771,7 +818,7 @@ def run_nudging_bench(lb, torch, device: int, steps: int = NUD_STEPS, chunk: int
 ENS_N, ENS_STEPS, ENS_TRACERS, ENS_OBS_ROWS = 64, 10000, 1024, 100
 
 
-def ensemble_members(lb, device: int, seed: int = 41, keep=None):
+def ensemble_members(lb, device: int, seed: int = 41, keep=None, precision: str = "fp32"):
     """The uneven ensemble: 64 members with Nx x Ny drawn from {256x128,
     512x256, 1024x512} and Ra log-uniform in [1e5, 1e7] (Pr=1, U=0.1), each
     with 1024 tracers and a nudging alpha drawn from {0, 0.1}; FP32-shifted
@@ -796,7 +843,7 @@ def ensemble_members(lb, device: int, seed: int = 41, keep=None):
         desc.append((nx, ny, Ra, alpha))
         if keep is not None and i not in keep:
             continue
-        kw = dict(**lb.closure(nx, ny, Ra=Ra, Pr=1.0, U=0.1), precision="fp32", nprtcl=ENS_TRACERS,
+        kw = dict(**lb.closure(nx, ny, Ra=Ra, Pr=1.0, U=0.1), precision=precision, nprtcl=ENS_TRACERS,
                   device=device)
         if alpha:
             kw.update(nudge="bilinear", alpha=alpha, nobs=ENS_TRACERS, obs_cycle=1)
@@ -809,6 +856,31 @@ def ensemble_members(lb, device: int, seed: int = 41, keep=None):
             r.nudge_obs(1, ox, oy, oT)
         members.append(r)
     return members, desc
+
+
+def ensemble_member_checks(lb, device: int, desc, checks: dict, steps: int, every: int = 500) -> dict:
+    """Every member: mass conserved, T inside the walls' range (plus the
+    nudging targets' spread); the member of lowest Nu stepped again alone,
+    in FP32 (bit-identical to the ensemble: the same Nu) and in FP64 (the
+    reference-order arithmetic), with its Nu every `every` steps."""
+    worst = min(checks, key=lambda i: checks[i]["nu"])
+    nx, ny, Ra, alpha = desc[worst]
+    alone = {}
+    for prec in ("fp32", "fp64"):
+        (r,), _ = ensemble_members(lb, device, keep={worst}, precision=prec)
+        series, done = [], 0
+        while done < steps:
+            n = min(every, steps - done)
+            r.step(n)
+            done += n
+            series.append(round(r.nusselt(), 4))
+        alone[prec] = {"nu": r.nusselt(), "nu_every_%d" % every: series}
+        r.close()
+    return {"max_mass_err": max(c["mass_err"] for c in checks.values()),
+            "T_range": [min(c["T_min"] for c in checks.values()), max(c["T_max"] for c in checks.values())],
+            "lowest_nu_member": {"index": worst, "grid": f"{nx}x{ny}", "Ra": Ra, "alpha": alpha,
+                                 "nu_in_ensemble": checks[worst]["nu"], "alone": alone,
+                                 "fp32_alone_equals_ensemble": alone["fp32"]["nu"] == checks[worst]["nu"]}}
 
 
 def ensemble_desc(seed: int = 41):
@@ -866,13 +938,21 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
         except lb.LbrbError:
             return False
 
+    def sanity(r):
+        """mass (mean rho - 1), T range and Nu of a member"""
+        m = r.get_moments()
+        return {"mass_err": float(abs(m["rho"].mean() - 1.0)), "T_min": float(m["T"].min()),
+                "T_max": float(m["T"].max()), "nu": r.nusselt()}
+
     mine = {"members": len(keep), "nodes": my_nodes, "ms": ms_mine, "schedule": sched, "timing": t,
-            "finite": all(is_finite(r) for r in members), "nus": [r.nusselt() for r in members]}
+            "finite": all(is_finite(r) for r in members), "ids": list(keep),
+            "checks": [sanity(r) for r in members]}
     for r in members:
         r.close()
     parts = shard.gather(dist, mine)
     finite = all(p["finite"] for p in parts)
-    nus = [v for p in parts for v in p["nus"]]
+    checks = {i: c for p in parts for i, c in zip(p["ids"], p["checks"])}
+    nus = [c["nu"] for c in checks.values()]
     t = parts[0]["timing"]
     sched = parts[0]["schedule"]
     peak, _ = measured_peak()
@@ -888,6 +968,8 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
            "phase_share": {k: round(v[0] / sum(x[0] for x in t.values()), 4) for k, v in t.items()},
            "launches_per_step": 3, "schedule": sched, "finite": bool(finite),
            "nu_range": [round(min(nus), 3), round(max(nus), 3)],
+           # (every member took 12 + 60 steps of tuning, capture and timing before the timed steps)
+           "member_checks": ensemble_member_checks(lb, device, desc, checks, 72 + steps) if rank == 0 else None,
            "config": f"{ENS_N} members from {{256x128, 512x256, 1024x512}}, Ra log-uniform "
                      f"[1e5,1e7], Pr=1, U=0.1, {ENS_TRACERS} tracers each, alpha in {{0,0.1}} "
                      f"({nudged} nudged), fp32-shifted; {steps} steps in CUDA-graph replays",
@@ -1250,6 +1332,10 @@ def main():
                     help="only the ensemble section (the command used for ncu captures of ens_lb_kernel)")
     ap.add_argument("--adjoint-check", action="store_true",
                     help="FD check of the adjoint gradient at the adjoint configuration")
+    ap.add_argument("--nu-stationary", action="store_true",
+                    help="FP32 vs FP64 time-averaged Nu on a statistically stationary state (minutes of GPU time)")
+    ap.add_argument("--nu-tff", type=float, default=6.0, help="free-fall times of --nu-stationary")
+    ap.add_argument("--nu-discard", type=float, default=3.0, help="free-fall times dropped as the transient")
     ap.add_argument("--lb-only", action="store_true",
                     help="fused kernel alone on --grid (the ncu capture command)")
     ap.add_argument("--grid", default="2048x1024")
@@ -1327,6 +1413,14 @@ def main():
         b.build()
         torch.cuda.set_device(0)
         print(json.dumps(run_adjoint_check(lb, torch, 0)), flush=True)
+        return
+    if args.nu_stationary:
+        import lagrangianrbnudging_b200 as lb
+        from lagrangianrbnudging_b200 import build as b
+
+        b.build()
+        torch.cuda.set_device(0)
+        print(json.dumps(run_stationary_nu(lb, 0, args.nu_tff, args.nu_discard)), flush=True)
         return
     dist = None
     if world > 1:
