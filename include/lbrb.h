@@ -175,8 +175,13 @@ LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
  * steps, are still stored for every step; the particle kernels run after
  * the launch for each step).  Results are identical to single steps.
  * -1 (the default) and 1: pairs of steps that do not replay graphs; 0: off.
- * Used with Dirichlet walls, without nudging, not on a y-slab, and never for
- * the last step of a call (so lbrb_get_poststream keeps its meaning).
+ * Used with Dirichlet walls, without nudging or with bilinear nudging, not
+ * on a y-slab, and never for the last step of a call (so
+ * lbrb_get_poststream keeps its meaning).  With bilinear nudging, step n's
+ * innovations are formed before the launch from T^n -- the moment of the
+ * populations streaming into each observation's cell corners, summed as the
+ * step sums it -- and added to g inside the launch right after the
+ * collision; step n+1's are applied after the launch, as for one step.
  * The launch shape is timed on first use (once per process for handles
  * of the same kind, as for autotune); lbrb_get_pair_shape reports it
  * (shape index, tile columns and rows, ms per launch; shape -1 before).

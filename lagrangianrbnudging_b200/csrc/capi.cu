@@ -238,7 +238,7 @@ static void free_all(lbrb_t* h) {
   F(h->nb); F(h->nbi); F(h->nudge_vol); F(h->tempreadint); F(h->nud_term); F(h->tsum0);
   F(h->cell_count); F(h->cell_start); F(h->cell_fill); F(h->cell_dirty); F(h->cell_items);
   delete[] h->h_chk; delete[] h->h_oid;
-  F(h->obs); F(h->acc); F(h->staging); F(h->big); F(h->red); F(h->dflags);
+  F(h->obs); F(h->acc); F(h->acc2); F(h->nmask); F(h->staging); F(h->big); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
   F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down); F(h->slab_own); F(h->slab_tab);
   F(h->slab_gh2_lo); F(h->slab_gh2_hi); F(h->slab_up2); F(h->slab_down2);
@@ -345,7 +345,9 @@ int lbrb_create(const lbrb_params* pin, lbrb_t** out) {
     h->h_oid = new int[n]();
   }
   if (p.nudge == LBRB_NUDGE_BILINEAR) {
-    if (dalloc(&h->acc, h->plane)) return done(LBRB_ERR_NOMEM);
+    if (dalloc(&h->acc, h->plane) || dalloc(&h->acc2, h->plane) ||
+        dalloc(&h->nmask, (size_t)p.ny * (h->pitch / 32)))
+      return done(LBRB_ERR_NOMEM);
   }
   h->stage_slot = stage_slot_doubles(p);
   h->staging_bytes = 2 * h->stage_slot * sizeof(double);
@@ -713,6 +715,14 @@ static bool pairs_ok(const lbrb_t* h) {
   return h->pair_mode != 0 && h->p.twall == LBRB_TWALL_DIRICHLET && h->p.nudge == LBRB_NUDGE_NONE && !h->slab;
 }
 
+// lbrb_step's two steps per launch: as pairs_ok, and also with bilinear
+// nudging (step n's innovations are formed before the launch and added to g
+// inside it; step n+1's are applied after it, as a single step applies them)
+static bool step_pairs_ok(const lbrb_t* h) {
+  return h->pair_mode != 0 && h->p.twall == LBRB_TWALL_DIRICHLET &&
+         (h->p.nudge == LBRB_NUDGE_NONE || h->p.nudge == LBRB_NUDGE_BILINEAR) && !h->slab;
+}
+
 static int slab_pair_launch(lbrb_t* h, bool rec1, bool rec2, bool last);  // (y-slabs, below)
 
 int lbrb_step(lbrb_t* h, int n) {
@@ -785,6 +795,14 @@ int lbrb_step(lbrb_t* h, int n) {
   };
   // one step's launches; `last` writes the moments
   const bool pdl_ok = !h->timing;  // (per-kernel timing keeps plain launches)
+  // the bilinear observations of step `istep` (rows [x][y][T] of nobs), or null
+  auto obs_row = [&](int istep) -> const double* {
+    if (!h->obs || istep < h->obs_first || (!h->p.obs_cycle && istep >= h->obs_first + h->obs_nsteps))
+      return nullptr;
+    int row = istep - h->obs_first;
+    if (h->p.obs_cycle) row %= h->obs_nsteps;
+    return h->obs + (size_t)row * 3 * h->nobs;
+  };
   auto one = [&](bool last) -> int {
     const int istep = h->istep + 1;
     const bool rec = h->np > 0 && h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
@@ -792,12 +810,8 @@ int lbrb_step(lbrb_t* h, int n) {
       return fail(h, LBRB_ERR_OVERFLOW, "step: record ring full, drain records first");
     const double* obs = nullptr;
     if (h->p.nudge == LBRB_NUDGE_BILINEAR) {
-      if (!h->obs || istep < h->obs_first ||
-          (!h->p.obs_cycle && istep >= h->obs_first + h->obs_nsteps))
-        return fail(h, LBRB_ERR_STATE, "step: no bilinear observations for this step");
-      int row = istep - h->obs_first;
-      if (h->p.obs_cycle) row %= h->obs_nsteps;
-      obs = h->obs + (size_t)row * 3 * h->nobs;
+      obs = obs_row(istep);
+      if (!obs) return fail(h, LBRB_ERR_STATE, "step: no bilinear observations for this step");
     }
     if (refbox) {
       const int nt = h->p.ntempread;
@@ -874,21 +888,51 @@ int lbrb_step(lbrb_t* h, int n) {
     const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;  // u^n
     const int B = parts ? h->uvprev : h->uvcur;                 // u^{n+1}
     const int wuv = parts ? 1 : 0;
+    // bilinear nudging: step n's innovations before the launch (into acc2 and
+    // the node mask, read inside it), step n+1's after it (T^{n+1} stored)
+    const bool nud = h->p.nudge == LBRB_NUDGE_BILINEAR;
+    const double* o1 = nud ? obs_row(i1) : nullptr;
+    const double* o2 = nud ? obs_row(i2) : nullptr;
+    const size_t no = (size_t)h->nobs;
+    if (nud) {
+      const int tm = tmark_begin(h, 2, h->stream);
+      if (f32)
+        CK(h, launch_obs_pre_fp32(make_view<float>(h, src, dst, A, 0, 0), o1, o1 + no, o1 + 2 * no, h->nobs,
+                                  h->p.alpha, h->acc2, h->nmask, h->dflags, h->stream, pdl_ok));
+      else
+        CK(h, launch_obs_pre_fp64(make_view<double>(h, src, dst, A, 0, 0), o1, o1 + no, o1 + 2 * no, h->nobs,
+                                  h->p.alpha, h->acc2, h->nmask, h->dflags, h->stream, pdl_ok));
+      tmark_end(h, tm, h->stream);
+    }
     {
       const int tm = tmark_begin(h, 0, h->stream);
+      const int rt2 = (rec2 || nud) ? 1 : 0;
       if (f32) {
         LBView<float> V1 = make_view<float>(h, src, dst, A, wuv, rec1 ? 1 : 0);
         V1.T = (float*)h->T[src];
         V1.rho = (float*)h->rho[src];
-        CK(h, launch_pair_fp32(V1, make_view<float>(h, dst, dst, B, wuv, rec2 ? 1 : 0), h->pair_shape, h->stream,
-                               pdl_ok));
+        if (nud) {
+          V1.nmask = h->nmask;
+          V1.nacc = reinterpret_cast<const unsigned long long*>(h->acc2);
+        }
+        CK(h, launch_pair_fp32(V1, make_view<float>(h, dst, dst, B, wuv, rt2), h->pair_shape, h->stream, pdl_ok));
       } else {
         LBView<double> V1 = make_view<double>(h, src, dst, A, wuv, rec1 ? 1 : 0);
         V1.T = (double*)h->T[src];
         V1.rho = (double*)h->rho[src];
-        CK(h, launch_pair_fp64(V1, make_view<double>(h, dst, dst, B, wuv, rec2 ? 1 : 0), h->pair_shape, h->stream,
-                               pdl_ok));
+        if (nud) {
+          V1.nmask = h->nmask;
+          V1.nacc = reinterpret_cast<const unsigned long long*>(h->acc2);
+        }
+        CK(h, launch_pair_fp64(V1, make_view<double>(h, dst, dst, B, wuv, rt2), h->pair_shape, h->stream, pdl_ok));
       }
+      tmark_end(h, tm, h->stream);
+    }
+    if (nud) {
+      const int tm = tmark_begin(h, 2, h->stream);
+      CK(h, launch_bilinear_nudge(h->T[dst], pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, o2, o2 + no,
+                                  o2 + 2 * no, h->nobs, h->p.alpha, h->acc, h->dflags, h->stream, pdl_ok));
+      CK(h, launch_obs_clear(nx, ny, h->pitch, o1, o1 + no, h->nobs, h->acc2, h->nmask, h->stream, pdl_ok));
       tmark_end(h, tm, h->stream);
     }
     if (parts) {
@@ -949,7 +993,7 @@ int lbrb_step(lbrb_t* h, int n) {
     return LBRB_OK;
   };
   bool graphs_on = graph_ok(h);  // (refined below for a caller's capture)
-  if (pairs_ok(h) && h->pair_shape < 0 && n >= 3) {
+  if (step_pairs_ok(h) && h->pair_shape < 0 && n >= 3) {
     // the pair shape is timed on the first call that can use pairs (trial
     // launches write only what the steps overwrite)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -1014,14 +1058,15 @@ int lbrb_step(lbrb_t* h, int n) {
         continue;
       }
     }
-    if (!graphs && h->pair_shape >= 0 && pairs_ok(h) && n - 1 - s >= 2) {
+    if (!graphs && h->pair_shape >= 0 && step_pairs_ok(h) && n - 1 - s >= 2) {
       // two steps per launch, never the call's last step; a pair whose
-      // records would not fit in the ring runs as single steps (which report
-      // the overflow at the same step)
+      // records would not fit in the ring, or whose observations are missing,
+      // runs as single steps (which report the error at the same step)
       int need = 0;
       for (int q = 1; q <= 2; q++)
         need += h->np > 0 && h->p.noutconfig > 0 && (h->istep + q) % h->p.noutconfig == 0;
-      if (h->rec_head - h->rec_tail + need <= h->p.record_slots) {
+      const bool obs_ok = h->p.nudge != LBRB_NUDGE_BILINEAR || (obs_row(h->istep + 1) && obs_row(h->istep + 2));
+      if (h->rec_head - h->rec_tail + need <= h->p.record_slots && obs_ok) {
         const int rc = two();
         if (rc) return rc;
         s += 2;

@@ -64,6 +64,15 @@ cudaError_t launch_bilinear_nudge(void* T, void* g, bool fp32, size_t plane, int
                                   int pitch, const double* ox, const double* oy, const double* oT,
                                   int nobs, double alpha, long long* acc, unsigned* dflags,
                                   cudaStream_t s, bool pdl = false);
+// two-step launches of a bilinear-nudged run (nudge_kernels.cu)
+cudaError_t launch_obs_pre_fp32(const LBView<float>& V, const double* ox, const double* oy, const double* oT,
+                                int nobs, double alpha, long long* acc, unsigned* mask, unsigned* dflags,
+                                cudaStream_t s, bool pdl);
+cudaError_t launch_obs_pre_fp64(const LBView<double>& V, const double* ox, const double* oy, const double* oT,
+                                int nobs, double alpha, long long* acc, unsigned* mask, unsigned* dflags,
+                                cudaStream_t s, bool pdl);
+cudaError_t launch_obs_clear(int nx, int ny, int pitch, const double* ox, const double* oy, int nobs, long long* acc,
+                             unsigned* mask, cudaStream_t s, bool pdl);
 cudaError_t launch_pops_in(const double* h, int layout, void* d, bool fp32, int nx, int ny,
                            int pitch, size_t plane, double base, cudaStream_t s);
 cudaError_t launch_pops_out(const void* d, int layout, double* h, bool fp32, int nx, int ny,

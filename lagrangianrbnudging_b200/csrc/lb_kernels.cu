@@ -115,6 +115,17 @@ __device__ __forceinline__ void pull_ghost_row(const LBView<Real>& V, bool lo, i
   Fy = G[(size_t)12 * nx + x];
 }
 
+// A bilinear-nudged run's two-step launch: the nudging sum of step n at
+// node (y, x) (element offset o), 0 where the mask has no bit or the sum is
+// 0 (the apply pass of a single step skips those nodes too)
+template <typename Real>
+__device__ __forceinline__ long long pair_nudge_sum(const LBView<Real>& V, int y, int x, size_t o) {
+  if (!V.nmask || y < 0 || y >= V.ny) return 0;
+  const unsigned w = V.nmask[(size_t)y * (size_t)(V.pitch >> 5) + (size_t)(x >> 5)];
+  if (!((w >> (x & 31)) & 1u)) return 0;
+  return (long long)V.nacc[o];
+}
+
 // NT threads per block: TX * TY (phase 1 takes the region in passes), or
 // one per region node rounded to whole warps (phase 1 in one pass; phase 2
 // leaves the rest idle)
@@ -148,9 +159,15 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
       dirichlet_walls(V1, jg, gs);
       Fy = V1.Fin[o];
     }
+    // (nudged run: step n's sums join g after the collision, as the apply pass does)
+    const long long nsum = pair_nudge_sum(V1, jg, xg, (size_t)o);
+    const double nsv = (double)nsum * (1.0 / FIX_SCALE);
     lb_collide<Real, false>(
         V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { S[(k * RY + ly) * RX + lx] = val; },
-        [&](int k, Real val) { S[((NPOP + k) * RY + ly) * RX + lx] = val; });
+        [&](int k, Real val) {
+          if (nsum != 0) val = val + nudge_increment<Real>(k, nsv);
+          S[((NPOP + k) * RY + ly) * RX + lx] = val;
+        });
     if (lx >= 1 && lx <= ncols && ly >= 1 && ly <= nrows) {
       SF[(ly - 1) * TX + (lx - 1)] = Fy;
       if (V1.write_F) V1.Fout[o] = Fy;
@@ -258,9 +275,14 @@ __global__ void __launch_bounds__(32 * (R + 1), MINB)
           Fy = V1.Fin[o];
         }
         Real* Sc = S + slot * CW + c;
+        const long long nsum = pair_nudge_sum(V1, y, x, (size_t)o);
+        const double nsv = (double)nsum * (1.0 / FIX_SCALE);
         lb_collide<Real, false>(
             V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { Sc[k * PL] = val; },
-            [&](int k, Real val) { Sc[(NPOP + k) * PL] = val; });
+            [&](int k, Real val) {
+              if (nsum != 0) val = val + nudge_increment<Real>(k, nsv);
+              Sc[(NPOP + k) * PL] = val;
+            });
         if (warp < R && ly >= 1 && ly <= Hc) {  // a node of this block's strip and chunk
           SF[slot * 32 + lane] = Fy;
           if (V1.write_F) V1.Fout[o] = Fy;

@@ -220,7 +220,23 @@ struct LBView {
   // wall); their first six planes are the one-step ghost rows above
   const Real* __restrict__ gh2_lo;
   const Real* __restrict__ gh2_hi;
+  // two-step launch of a bilinear-nudged run (first step's view only): the
+  // nudging sums of this step at the nodes flagged in nmask (one bit per
+  // node, pitch / 32 words per row), 2^-40 fixed point; added to g right
+  // after the collision, as the apply pass of a single step adds them
+  const unsigned* __restrict__ nmask;
+  const unsigned long long* __restrict__ nacc;
 };
+
+// 2^-40 fixed point of the bilinear nudging sums (nudge_dev.cuh)
+constexpr double FIX_SCALE = 1099511627776.0;
+
+// the apply pass's increment of g_k: w_k * S (rounded to FP32 for FP32 runs)
+template <typename Real>
+__device__ __forceinline__ Real nudge_increment(int k, double sv) {
+  if constexpr (std::is_same<Real, double>::value) return w_of(k) * sv;
+  else return (float)(w_of(k) * sv);
+}
 
 // --------------------------------------------------------------- handle
 struct Handle {
@@ -336,6 +352,10 @@ struct Handle {
   double* obs = nullptr;    // [nsteps][3][nobs]
   int obs_first = 0, obs_nsteps = 0, obs_cap_steps = 0;
   long long* acc = nullptr;
+  // two-step launches of a nudged run: the first step's sums (formed before
+  // the launch) and their node mask, cleared after the launch
+  long long* acc2 = nullptr;
+  unsigned* nmask = nullptr;
   // adjoint window
   double* adj_obs = nullptr;         // [nobs_steps][3][nobs]
   int adj_nobs = 0, adj_nsteps_obs = 0;

@@ -14,7 +14,6 @@
 
 namespace lbrb {
 
-constexpr double FIX_SCALE = 1099511627776.0;  // 2^40
 
 __device__ __forceinline__ void obs_cell(double xx, double yy, int nx, int ny, int& x1, int& y1,
                                          int& ix1, int& ix2, int& jy1, int& jy2) {
@@ -94,8 +93,7 @@ __device__ __forceinline__ void obs_apply_one(Real* __restrict__ g, size_t plane
 #pragma unroll
   for (int k = 0; k < NPOP; k++) {
     Real* a = g + (size_t)k * plane + q;
-    if constexpr (std::is_same<Real, double>::value) *a = *a + w_of(k) * sv;
-    else *a = *a + (float)(w_of(k) * sv);
+    *a = *a + nudge_increment<Real>(k, sv);
   }
 }
 

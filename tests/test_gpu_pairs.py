@@ -159,3 +159,44 @@ def test_pairs_are_the_default_above_the_graph_size():
         ma, mb = a.get_moments(), b.get_moments()
         for k in ma:
             np.testing.assert_array_equal(mb[k], ma[k])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("shape", [-1, 0, 5, 9, 10])
+def test_nudged_pairs_equal_single_steps(precision, shape):
+    """bilinear nudging with two steps per launch (step n's innovations
+    formed before the launch from T^n pulled from the previous state, added
+    to g inside it; step n+1's applied after it): bit-identical to single
+    steps, with tracers, inertial particles and records; observations
+    repeating over 7 steps, some at the walls and the x wrap"""
+    nx, ny, nobs, rows = 200, 37, 150, 7
+    rng = np.random.default_rng(11)
+    ox = rng.uniform(0.0, nx + 1.0, (rows, nobs))
+    oy = rng.uniform(1.0, ny, (rows, nobs))
+    ox[:, :3] = [0.2, nx + 0.7, 0.99]
+    oy[:, 3:6] = [1.0, ny - 1e-9, 1.5]
+    oT = rng.uniform(-0.5, 0.5, (rows, nobs))
+
+    def run(pairs):
+        r = lb.Run(**lb.closure(nx, ny, Ra=1e6, Pr=1.0, U=0.1), precision=precision, nprtcl=40, noutconfig=3,
+                   record_slots=64, beta=0.5, record_full=1, nudge="bilinear", alpha=0.3, nobs=nobs, obs_cycle=1)
+        r.set_pairs(pairs)
+        if pairs and shape >= 0:
+            r.set_pair_shape(shape)
+        r.init_conduction(29, 3e-2)
+        x = np.random.default_rng(7).uniform(0.5, nx + 0.5, 40)
+        y = np.random.default_rng(8).uniform(1.0, ny, 40)
+        ptype = (np.arange(40) % 2).astype(np.int32)
+        z = np.zeros(40)
+        r.set_particles(np.arange(40, dtype=np.int32), x, y, z, z, ptype, np.where(ptype == 1, 1 / 25.0, 0.0))
+        r.nudge_obs(1, ox, oy, oT)
+        return r
+
+    with run(0) as a, run(1) as b:
+        for n in (1, 2, 5, 8, 31):
+            a.step(n)
+            b.step(n)
+            sa, sb = state(a, 40), state(b, 40)
+            for k in sa:
+                np.testing.assert_array_equal(sb[k], sa[k], err_msg=k)
+        assert b.pair_shape()["shape"] >= 0 and a.pair_shape()["shape"] == -1

@@ -191,7 +191,14 @@ def test_reference_layout_roundtrip_and_halo():
     np.testing.assert_array_equal(fr[:, ny + 1], fr[:, 1])
 
 
-def test_fp64_bilinear_nudging_matches_oracle():
+@pytest.mark.parametrize("launch", ["single", "pairs"])
+@pytest.mark.parametrize("shape", [-1, 0, 9])
+def test_fp64_bilinear_nudging_matches_oracle(launch, shape):
+    """single: one launch per step; pairs: two steps per launch, step n's
+    innovations formed before the launch and added inside it (shape -1
+    tuned, 0 a tile, 9 a marching strip)"""
+    if launch == "single" and shape != -1:
+        pytest.skip("the launch shape applies to pairs")
     nx, ny, nobs, K = 64, 32, 200, 40
     base = lb.closure(nx, ny, Ra=1e5, Pr=1.0, U=0.1)
     rng = np.random.default_rng(5)
@@ -201,6 +208,9 @@ def test_fp64_bilinear_nudging_matches_oracle():
     o = Oracle(dict(base, nudge="bilinear", alpha=0.1), 0)
     o.init_conduction(seed=3, noise=1e-2)
     with lb.Run(**base, precision="fp64", nudge="bilinear", alpha=0.1, nobs=nobs) as r:
+        r.set_pairs(1 if launch == "pairs" else 0)
+        if shape >= 0:
+            r.set_pair_shape(shape)
         r.init_conduction(3, 1e-2)
         r.nudge_obs(1, ox, oy, oT)
         r.step(K)
