@@ -902,7 +902,7 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
     members, _ = ensemble_members(lb, device, keep=set(keep))
     nodes = sum(costs)
     my_nodes = sum(costs[i] for i in keep)
-    ms_mine, sched, t = 0.0, None, None
+    ms_mine, sched, t, pairs = 0.0, None, None, None
     ens = lb.Ensemble(members) if members else None
     if ens is not None:
         if variant >= 0:
@@ -910,8 +910,10 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
         stream = torch.cuda.Stream()
         ens.set_stream(stream.cuda_stream)
         ens.step(12)  # autotune + graph capture + warm-up
+        ens.step(25)  # (a pair graph of 12 steps needs 25-step calls)
         ens.sync()
         sched = ens.schedule()
+        pairs = ens.pairs()
         # per-launch timing of the phases (direct launches, no graph)
         ens.set_timing(True)
         ens.step(60)
@@ -944,7 +946,7 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
         return {"mass_err": float(abs(m["rho"].mean() - 1.0)), "T_min": float(m["T"].min()),
                 "T_max": float(m["T"].max()), "nu": r.nusselt()}
 
-    mine = {"members": len(keep), "nodes": my_nodes, "ms": ms_mine, "schedule": sched, "timing": t,
+    mine = {"members": len(keep), "nodes": my_nodes, "ms": ms_mine, "schedule": sched, "timing": t, "pairs": pairs,
             "finite": all(is_finite(r) for r in members), "ids": list(keep),
             "checks": [sanity(r) for r in members]}
     for r in members:
@@ -958,7 +960,8 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
     peak, _ = measured_peak()
     lb_ms = t["lb_step"][0] / max(t["lb_step"][1], 1)
     agg = nodes * ALG_BYTES["fp32"] * steps / (ms * 1e-3) / 1e9
-    lb_gbs = parts[0]["nodes"] * ALG_BYTES["fp32"] / (lb_ms * 1e-3) / 1e9
+    # the fused phase over the 60-step timing window (a launch takes one or two steps)
+    lb_gbs = parts[0]["nodes"] * ALG_BYTES["fp32"] * 60 / (t["lb_step"][0] * 1e-3) / 1e9
     nudged = sum(1 for d in desc if d[3] > 0)
     out = {"members": ENS_N, "nodes": nodes, "steps": steps, "ms": round(ms, 2),
            "mlups": round(nodes * steps / (ms * 1e3), 1),
@@ -966,10 +969,11 @@ def run_ensemble_bench(lb, torch, device: int, steps: int = ENS_STEPS, variant: 
            "lb_phase_ms": round(lb_ms, 5), "lb_phase_gbs": round(lb_gbs, 1),
            "lb_phase_frac": round(lb_gbs / peak, 4),
            "phase_share": {k: round(v[0] / sum(x[0] for x in t.values()), 4) for k, v in t.items()},
-           "launches_per_step": 3, "schedule": sched, "finite": bool(finite),
+           "launches_per_step": round(sum(v[1] for v in t.values()) / 60, 3), "schedule": sched,
+           "pairs": parts[0].get("pairs"), "finite": bool(finite),
            "nu_range": [round(min(nus), 3), round(max(nus), 3)],
-           # (every member took 12 + 60 steps of tuning, capture and timing before the timed steps)
-           "member_checks": ensemble_member_checks(lb, device, desc, checks, 72 + steps) if rank == 0 else None,
+           # (every member took 12 + 25 + 60 steps of tuning, capture and timing before the timed steps)
+           "member_checks": ensemble_member_checks(lb, device, desc, checks, 97 + steps) if rank == 0 else None,
            "config": f"{ENS_N} members from {{256x128, 512x256, 1024x512}}, Ra log-uniform "
                      f"[1e5,1e7], Pr=1, U=0.1, {ENS_TRACERS} tracers each, alpha in {{0,0.1}} "
                      f"({nudged} nudged), fp32-shifted; {steps} steps in CUDA-graph replays",

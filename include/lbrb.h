@@ -320,8 +320,23 @@ LBRB_API int lbrb_ensemble_nvariants(void);
 LBRB_API int lbrb_ensemble_set_schedule(lbrb_ensemble_t *e, int variant);
 LBRB_API int lbrb_ensemble_get_schedule(const lbrb_ensemble_t *e, int *variant, int *block,
                                         int *rows, int *schedule, int *fast_pull, float *ms);
+/* Two steps per launch for every member (as lbrb_set_pairs, with Dirichlet
+ * walls; bilinear-nudged members too): every step of a call but its last
+ * (and one more when an even count remains) goes in pairs, each pair one
+ * marching launch over strips of 32 columns x chunks of rows of all members
+ * (lb_march_kernel's block, the members' views in shared memory), with the
+ * nudged members' step-n innovations formed before it and every member's
+ * particles, step n+1 innovations and nudging apply after it; 12 steps are
+ * replayed from a CUDA graph.  Members end bit-identical to lbrb_step.
+ * mode -1 (the default) and 1: on; 0: one step per launch.  The rows per
+ * marching group (4, 8 or 16) are timed at the first paired call;
+ * lbrb_ensemble_get_pairs reports them (0 before) and ms per launch. */
+LBRB_API int lbrb_ensemble_set_pairs(lbrb_ensemble_t *e, int mode);
+LBRB_API int lbrb_ensemble_get_pairs(const lbrb_ensemble_t *e, int *mode, int *rows, float *ms);
 /* Per-launch device timing (steps then launch directly, without the graph).
- * Classes: 0 fused step, 1 particles + innovation scatter, 2 nudging apply. */
+ * Classes: 0 fused step (one or two steps), 1 particles + innovation
+ * scatter, 2 nudging (apply; with pairs also the innovations before the
+ * launch). */
 LBRB_API int lbrb_ensemble_set_timing(lbrb_ensemble_t *e, int enable);
 LBRB_API int lbrb_ensemble_get_timing(lbrb_ensemble_t *e, double *ms, int *launches, int n);
 

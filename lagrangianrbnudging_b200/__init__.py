@@ -42,6 +42,7 @@ EXPORTS = [
     "lbrb_ensemble_create", "lbrb_ensemble_destroy", "lbrb_ensemble_last_error",
     "lbrb_ensemble_step", "lbrb_ensemble_sync", "lbrb_ensemble_set_stream",
     "lbrb_ensemble_nvariants", "lbrb_ensemble_set_schedule", "lbrb_ensemble_get_schedule",
+    "lbrb_ensemble_set_pairs", "lbrb_ensemble_get_pairs",
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
@@ -125,6 +126,8 @@ def lib() -> C.CDLL:
         "lbrb_ensemble_set_stream": (C.c_int, [vp, vp]),
         "lbrb_ensemble_nvariants": (C.c_int, []),
         "lbrb_ensemble_set_schedule": (C.c_int, [vp, C.c_int]),
+        "lbrb_ensemble_set_pairs": (C.c_int, [vp, C.c_int]),
+        "lbrb_ensemble_get_pairs": (C.c_int, [vp, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_ensemble_get_schedule": (C.c_int, [vp, ip, ip, ip, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_ensemble_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_ensemble_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
@@ -601,6 +604,15 @@ class Ensemble:
 
     def set_schedule(self, variant: int):
         self._ck(lib().lbrb_ensemble_set_schedule(self.e, int(variant)))
+
+    def set_pairs(self, mode: int):
+        """two steps per launch: -1 / 1 on (default), 0 off"""
+        self._ck(lib().lbrb_ensemble_set_pairs(self.e, int(mode)))
+
+    def pairs(self) -> dict:
+        mode, rows, ms = C.c_int(), C.c_int(), C.c_float()
+        self._ck(lib().lbrb_ensemble_get_pairs(self.e, C.byref(mode), C.byref(rows), C.byref(ms)))
+        return {"mode": mode.value, "rows": rows.value, "tuned_ms": ms.value}
 
     def schedule(self) -> dict:
         v, b, r, s, f, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()

@@ -30,8 +30,8 @@ struct lbrb_ensemble_s {
   size_t vsize = 0, asize = 0;  // bytes of one LBView / EnsAux
   cudaStream_t stream = nullptr, own_stream = nullptr;
   cudaEvent_t ev = nullptr;
-  void* d_views = nullptr;      // [7][n]: phases 0..5, then the last step
-  void* d_aux = nullptr;        // [7][n]
+  void* d_views = nullptr;      // [9][n]: phases 0..5, the last step; with pairs: tail steps 7, 8
+  void* d_aux = nullptr;        // [9][n]
   int4* d_items = nullptr;
   int nitems = 0, items_variant = -1;
   int2* d_pch = nullptr;
@@ -44,6 +44,20 @@ struct lbrb_ensemble_s {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_variant = -1;
+  // two steps per launch: pair_mode -1 (default) / 1 on, 0 off; pair views
+  // [6 phases][2 steps][n] and their EnsAux, items of the marching kernel
+  // (member, first column, first row, rows), its variant (-1: tune), a graph
+  // of 6 pairs (12 steps, the period of the buffer cycle)
+  int pair_mode = -1;
+  int pair_variant = -1;
+  float pair_ms = 0.f;
+  void* d_pviews = nullptr;
+  void* d_paux = nullptr;
+  int4* d_pitems = nullptr;
+  int npitems = 0;
+  cudaGraph_t pgraph = nullptr;
+  cudaGraphExec_t pgexec = nullptr;
+  int pgraph_variant = -1;
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
   size_t evused = 0;
@@ -92,6 +106,76 @@ StepBufs step_bufs(const lbrb_t* h, MState& s, bool last) {
   return b;
 }
 
+// two steps of one launch, as lbrb_step's pairs advance the buffers
+struct PairBufs {
+  int src, dst, A, B, uvcur0, wuv;
+};
+
+PairBufs pair_bufs(const lbrb_t* h, MState& s) {
+  const bool parts = h->np > 0;
+  PairBufs b;
+  b.src = s.cur;
+  b.dst = s.cur ^ 1;
+  b.A = parts ? 3 - s.uvcur - s.uvprev : s.uvcur;  // u^n
+  b.B = parts ? s.uvprev : s.uvcur;                // u^{n+1}
+  b.uvcur0 = s.uvcur;                              // u^{n-1}
+  b.wuv = parts ? 1 : 0;
+  s.cur = b.dst;
+  if (parts) {
+    s.uvprev = b.A;
+    s.uvcur = b.B;
+  }
+  return b;
+}
+
+// a member's EnsAux for one step: particles read u (slot un), u^{n-1}
+// (slot ub) and T (buffer tb); nudging reads T and applies to g of buffer tb
+template <typename Real>
+EnsAux<Real> make_aux(lbrb_t* h, int un, int ub, int tb) {
+  EnsAux<Real> a{};
+  a.P = PView<Real>{(const Real*)h->uv[un][0], (const Real*)h->uv[un][1],
+                    (const Real*)h->uv[ub][0], (const Real*)h->uv[ub][1],
+                    (const Real*)h->T[tb], h->p.nx, h->p.ny, h->pitch, h->px, h->ptype, h->np,
+                    h->p.beta, 0, 0, nullptr, h->dflags};
+  a.T = (const Real*)h->T[tb];
+  a.g = (Real*)pop_base(h, tb, 1);
+  a.plane = h->plane;
+  a.nx = h->p.nx;
+  a.ny = h->p.ny;
+  a.pitch = h->pitch;
+  if (h->p.nudge == LBRB_NUDGE_BILINEAR) {
+    a.obs = h->obs;
+    a.nobs = h->nobs;
+    a.obs_first = h->obs_first;
+    a.obs_nsteps = h->obs_nsteps;
+    a.obs_cycle = h->p.obs_cycle;
+    a.alpha = h->p.alpha;
+    a.acc = reinterpret_cast<unsigned long long*>(h->acc);
+    a.acc2 = reinterpret_cast<unsigned long long*>(h->acc2);
+    a.nmask = h->nmask;
+  }
+  a.istep0 = h->istep;
+  a.dflags = h->dflags;
+  return a;
+}
+
+// the two views and EnsAux of a pair (lbrb_step's two(): step n's T into
+// the source buffer's T, its innovations added inside the launch)
+template <typename Real>
+void fill_pair(lbrb_t* h, const PairBufs& b, LBView<Real>* V1, LBView<Real>* V2, EnsAux<Real>* A1, EnsAux<Real>* A2) {
+  const bool nud = h->p.nudge == LBRB_NUDGE_BILINEAR;
+  *V1 = make_view<Real>(h, b.src, b.dst, b.A, b.wuv, 0);
+  V1->T = (Real*)h->T[b.src];
+  V1->rho = (Real*)h->rho[b.src];
+  if (nud) {
+    V1->nmask = h->nmask;
+    V1->nacc = reinterpret_cast<const unsigned long long*>(h->acc2);
+  }
+  *V2 = make_view<Real>(h, b.dst, b.dst, b.B, b.wuv, nud ? 1 : 0);
+  *A1 = make_aux<Real>(h, b.A, b.uvcur0, b.src);
+  *A2 = make_aux<Real>(h, b.B, b.A, b.dst);
+}
+
 template <typename Real>
 void fill_views(lbrb_t* h, const StepBufs& b, LBView<Real>* V, EnsAux<Real>* A) {
   *V = make_view<Real>(h, b.src, b.dst, b.uvn, b.write_uv, b.write_rt);
@@ -120,14 +204,24 @@ void fill_views(lbrb_t* h, const StepBufs& b, LBView<Real>* V, EnsAux<Real>* A) 
   *A = a;
 }
 
-// views of phases 0..5 and of the last step (n steps in this call)
+// Views of one call of n steps.  Single steps: phases 0..5 from the current
+// state and the last step (slot 6).  With npairs > 0 pairs first: the pair
+// views of 6 phases from the current state (pv, pa: [6][2][n]), then the
+// tail's single steps from the state after the pairs (slot 7: an extra step
+// when two remain, slot 8: the last step); slots 0..5 stay those of the
+// current state (the single-step tuner's trials read slot 0).
 template <typename Real>
-void build_views(lbrb_ensemble_t* e, int n, std::vector<char>& vbuf, std::vector<char>& abuf) {
+void build_views(lbrb_ensemble_t* e, int n, int npairs, std::vector<char>& vbuf, std::vector<char>& abuf,
+                 std::vector<char>& pvbuf, std::vector<char>& pabuf) {
   const size_t nm = e->m.size();
-  vbuf.assign(7 * nm * sizeof(LBView<Real>), 0);
-  abuf.assign(7 * nm * sizeof(EnsAux<Real>), 0);
+  vbuf.assign(9 * nm * sizeof(LBView<Real>), 0);
+  abuf.assign(9 * nm * sizeof(EnsAux<Real>), 0);
+  pvbuf.assign(12 * nm * sizeof(LBView<Real>), 0);
+  pabuf.assign(12 * nm * sizeof(EnsAux<Real>), 0);
   LBView<Real>* V = reinterpret_cast<LBView<Real>*>(vbuf.data());
   EnsAux<Real>* A = reinterpret_cast<EnsAux<Real>*>(abuf.data());
+  LBView<Real>* PV = reinterpret_cast<LBView<Real>*>(pvbuf.data());
+  EnsAux<Real>* PA = reinterpret_cast<EnsAux<Real>*>(pabuf.data());
   for (size_t i = 0; i < nm; i++) {
     lbrb_t* h = e->m[i];
     MState s{h->cur, h->uvcur, h->uvprev};
@@ -136,17 +230,36 @@ void build_views(lbrb_ensemble_t* e, int n, std::vector<char>& vbuf, std::vector
       fill_views<Real>(h, b, V + ph * nm + i, A + ph * nm + i);
     }
     MState l{h->cur, h->uvcur, h->uvprev};
-    for (int t = 0; t < (n - 1) % 6; t++) step_bufs(h, l, false);
+    if (npairs == 0) {
+      for (int t = 0; t < (n - 1) % 6; t++) step_bufs(h, l, false);
+      StepBufs b = step_bufs(h, l, true);
+      fill_views<Real>(h, b, V + 6 * nm + i, A + 6 * nm + i);
+      continue;
+    }
+    MState q{h->cur, h->uvcur, h->uvprev};
+    for (int ph = 0; ph < 6; ph++) {
+      PairBufs b = pair_bufs(h, q);
+      fill_pair<Real>(h, b, PV + (2 * ph) * nm + i, PV + (2 * ph + 1) * nm + i, PA + (2 * ph) * nm + i,
+                      PA + (2 * ph + 1) * nm + i);
+    }
+    for (int t = 0; t < npairs % 6; t++) pair_bufs(h, l);
+    if (n - 2 * npairs == 2) {
+      StepBufs b = step_bufs(h, l, false);
+      fill_views<Real>(h, b, V + 7 * nm + i, A + 7 * nm + i);
+    }
     StepBufs b = step_bufs(h, l, true);
-    fill_views<Real>(h, b, V + 6 * nm + i, A + 6 * nm + i);
+    fill_views<Real>(h, b, V + 8 * nm + i, A + 8 * nm + i);
   }
 }
 
-// the handle state lbrb_step(n) would leave
-void advance_members(lbrb_ensemble_t* e, int n) {
+// the handle state lbrb_step(n) would leave (npairs pairs, then singles)
+void advance_members(lbrb_ensemble_t* e, int n, int npairs) {
   for (lbrb_t* h : e->m) {
     MState s{h->cur, h->uvcur, h->uvprev};
-    for (int t = 0; t < (n - 1) % 6; t++) step_bufs(h, s, false);
+    for (int t = 0; t < npairs % 6; t++) pair_bufs(h, s);
+    const int singles = n - 2 * npairs;
+    const int lead = npairs > 0 ? singles - 1 : (n - 1) % 6;
+    for (int t = 0; t < lead; t++) step_bufs(h, s, false);
     step_bufs(h, s, true);
     h->cur = s.cur;
     h->uvcur = s.uvcur;
@@ -211,6 +324,121 @@ cudaError_t launch_step(lbrb_ensemble_t* e, int ph) {
     mark_end(e, k);
   }
   return c;
+}
+
+const char* pview_at(const lbrb_ensemble_t* e, int ph, int step) {
+  return (const char*)e->d_pviews + (size_t)(2 * ph + step) * e->m.size() * e->vsize;
+}
+const char* paux_at(const lbrb_ensemble_t* e, int ph, int step) {
+  return (const char*)e->d_paux + (size_t)(2 * ph + step) * e->m.size() * e->asize;
+}
+
+// two steps of every member, pair phase ph (0..5)
+cudaError_t launch_pair(lbrb_ensemble_t* e, int ph) {
+  cudaError_t c = cudaSuccess;
+  int k;
+  if (e->noch > 0) {
+    k = mark_begin(e, 2);
+    c = launch_ens_pre(e->f32, pview_at(e, ph, 0), paux_at(e, ph, 0), e->d_och, e->noch, e->d_ctr, e->stream);
+    mark_end(e, k);
+    if (c != cudaSuccess) return c;
+  }
+  k = mark_begin(e, 0);
+  c = launch_ens_march(e->f32, e->off32, e->pair_variant, pview_at(e, ph, 0), pview_at(e, ph, 1), e->d_pitems,
+                       e->npitems, e->d_ctr, e->stream);
+  mark_end(e, k);
+  if (c != cudaSuccess) return c;
+  k = mark_begin(e, 1);
+  c = launch_ens_aux2(e->f32, paux_at(e, ph, 0), paux_at(e, ph, 1), e->d_pch, e->npch, e->d_och, e->noch, e->d_ctr,
+                      e->stream);
+  mark_end(e, k);
+  if (c != cudaSuccess) return c;
+  if (e->noch > 0) {
+    k = mark_begin(e, 2);
+    c = launch_ens_apply2(e->f32, paux_at(e, ph, 0), paux_at(e, ph, 1), e->d_och, e->noch, e->d_ctr, e->stream);
+    mark_end(e, k);
+  }
+  return c;
+}
+
+// work items of the marching kernel: every member's strips of 32 columns x
+// chunks of PAIR_CHUNK rows (whole groups of 4, 8 or 16 rows with the two
+// ring rows)
+constexpr int PAIR_CHUNK = 62;
+int set_pair_items(lbrb_ensemble_t* e) {
+  if (e->d_pitems) return LBRB_OK;
+  std::vector<int4> it;
+  for (size_t i = 0; i < e->m.size(); i++) {
+    const lbrb_t* h = e->m[i];
+    for (int y = 0; y < h->p.ny; y += PAIR_CHUNK)
+      for (int x = 0; x < h->p.nx; x += 32) it.push_back(make_int4((int)i, x, y, std::min(PAIR_CHUNK, h->p.ny - y)));
+  }
+  EK(e, cudaMalloc(&e->d_pitems, it.size() * sizeof(int4)));
+  EK(e, cudaMemcpyAsync(e->d_pitems, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+  EK(e, cudaStreamSynchronize(e->stream));
+  e->npitems = (int)it.size();
+  return LBRB_OK;
+}
+
+// Pair autotuner: each variant's marching launch on pair phase 0 (trials
+// write only buffers the real pair overwrites), 3 timed launches after a
+// warm-up; the fastest is kept
+int tune_pairs(lbrb_ensemble_t* e) {
+  int rc = set_pair_items(e);
+  if (rc) return rc;
+  cudaEvent_t a, b;
+  EK(e, cudaEventCreate(&a));
+  EK(e, cudaEventCreate(&b));
+  int best = 0;
+  float bt = 1e30f;
+  for (int v = 0; v < ENS_PAIR_VARIANTS; v++) {
+    float tot = 0.f;
+    bool ok = true;
+    for (int r = 0; r < 4 && ok; r++) {
+      EK(e, cudaEventRecord(a, e->stream));
+      cudaError_t c = launch_ens_march(e->f32, e->off32, v, pview_at(e, 0, 0), pview_at(e, 0, 1), e->d_pitems,
+                                       e->npitems, e->d_ctr, e->stream);
+      if (c != cudaSuccess) {
+        cudaGetLastError();
+        ok = false;
+        break;
+      }
+      EK(e, cudaEventRecord(b, e->stream));
+      EK(e, cudaEventSynchronize(b));
+      float ms = 0.f;
+      EK(e, cudaEventElapsedTime(&ms, a, b));
+      if (r > 0) tot += ms;
+    }
+    if (ok && tot / 3 < bt) {
+      bt = tot / 3;
+      best = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  EK(e, cudaMemsetAsync(e->d_ctr, 0, 2 * sizeof(int), e->stream));
+  e->pair_variant = best;
+  e->pair_ms = bt;
+  return LBRB_OK;
+}
+
+int ensure_pair_graph(lbrb_ensemble_t* e) {
+  if (e->pgexec && e->pgraph_variant == e->pair_variant) return LBRB_OK;
+  if (e->pgexec) cudaGraphExecDestroy(e->pgexec);
+  if (e->pgraph) cudaGraphDestroy(e->pgraph);
+  e->pgexec = nullptr;
+  e->pgraph = nullptr;
+  EK(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t c = cudaSuccess;
+  for (int ph = 0; ph < 6 && c == cudaSuccess; ph++) c = launch_pair(e, ph);
+  cudaGraph_t g = nullptr;
+  cudaError_t c2 = cudaStreamEndCapture(e->stream, &g);
+  if (c != cudaSuccess) return efail(e, LBRB_ERR_CUDA, "ensemble pair graph capture", c);
+  if (c2 != cudaSuccess) return efail(e, LBRB_ERR_CUDA, "ensemble pair graph capture", c2);
+  e->pgraph = g;
+  EK(e, cudaGraphInstantiate(&e->pgexec, g, 0));
+  e->pgraph_variant = e->pair_variant;
+  return LBRB_OK;
 }
 
 int set_items(lbrb_ensemble_t* e, int variant) {
@@ -333,8 +561,10 @@ int lbrb_ensemble_create(lbrb_t* const* members, int n, lbrb_ensemble_t** out) {
   if (c == cudaSuccess) c = cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, e->dev);
   if (c == cudaSuccess) c = cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking);
   if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->ev, cudaEventDisableTiming);
-  if (c == cudaSuccess) c = cudaMalloc(&e->d_views, 7 * (size_t)n * e->vsize);
-  if (c == cudaSuccess) c = cudaMalloc(&e->d_aux, 7 * (size_t)n * e->asize);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_views, 9 * (size_t)n * e->vsize);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_aux, 9 * (size_t)n * e->asize);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_pviews, 12 * (size_t)n * e->vsize);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_paux, 12 * (size_t)n * e->asize);
   if (c == cudaSuccess) c = cudaMalloc((void**)&e->d_ctr, 4 * sizeof(int));
   if (c != cudaSuccess) return bad(c);
   e->stream = e->own_stream;
@@ -366,8 +596,10 @@ int lbrb_ensemble_destroy(lbrb_ensemble_t* e) {
   if (e->stream && e->stream != e->own_stream) cudaStreamSynchronize(e->stream);
   if (e->gexec) cudaGraphExecDestroy(e->gexec);
   if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->pgexec) cudaGraphExecDestroy(e->pgexec);
+  if (e->pgraph) cudaGraphDestroy(e->pgraph);
   for (void* p : {(void*)e->d_views, (void*)e->d_aux, (void*)e->d_items, (void*)e->d_pch, (void*)e->d_och,
-                  (void*)e->d_ctr})
+                  (void*)e->d_ctr, (void*)e->d_pviews, (void*)e->d_paux, (void*)e->d_pitems})
     if (p) cudaFree(p);
   for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
   if (e->ev) cudaEventDestroy(e->ev);
@@ -406,6 +638,20 @@ int lbrb_ensemble_get_schedule(const lbrb_ensemble_t* e, int* variant, int* bloc
   if (schedule) *schedule = v >= 0 ? ENS_TABLE[v].sched : -1;
   if (fast_pull) *fast_pull = v >= 0 ? ENS_TABLE[v].fast : -1;
   if (ms) *ms = e->variant_ms;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_set_pairs(lbrb_ensemble_t* e, int mode) {
+  if (!e || mode < -1 || mode > 1) return efail(e, LBRB_ERR_ARG, "ensemble_set_pairs: mode must be -1, 0 or 1");
+  e->pair_mode = mode;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_get_pairs(const lbrb_ensemble_t* e, int* mode, int* rows, float* ms) {
+  if (!e) return LBRB_ERR_ARG;
+  if (mode) *mode = e->pair_mode;
+  if (rows) *rows = e->pair_variant >= 0 ? ens_pair_rows(e->pair_variant) : 0;
+  if (ms) *ms = e->pair_ms;
   return LBRB_OK;
 }
 
@@ -458,11 +704,19 @@ int lbrb_ensemble_step(lbrb_ensemble_t* e, int n) {
     EK(e, cudaEventRecord(e->ev, h->stream));
     EK(e, cudaStreamWaitEvent(e->stream, e->ev, 0));
   }
-  std::vector<char> vb, ab;
-  if (e->f32) build_views<float>(e, n, vb, ab);
-  else build_views<double>(e, n, vb, ab);
+  // two steps per launch for all but the call's last step (lbrb_step's
+  // rule: a pair never takes a call's last step)
+  const bool pairs = e->pair_mode != 0 && e->twall == LBRB_TWALL_DIRICHLET && n >= 3;
+  const int npairs = pairs ? (n - 1) / 2 : 0;
+  std::vector<char> vb, ab, pvb, pab;
+  if (e->f32) build_views<float>(e, n, npairs, vb, ab, pvb, pab);
+  else build_views<double>(e, n, npairs, vb, ab, pvb, pab);
   EK(e, cudaMemcpyAsync(e->d_views, vb.data(), vb.size(), cudaMemcpyHostToDevice, e->stream));
   EK(e, cudaMemcpyAsync(e->d_aux, ab.data(), ab.size(), cudaMemcpyHostToDevice, e->stream));
+  if (npairs > 0) {
+    EK(e, cudaMemcpyAsync(e->d_pviews, pvb.data(), pvb.size(), cudaMemcpyHostToDevice, e->stream));
+    EK(e, cudaMemcpyAsync(e->d_paux, pab.data(), pab.size(), cudaMemcpyHostToDevice, e->stream));
+  }
   EK(e, cudaMemsetAsync(e->d_ctr, 0, 2 * sizeof(int), e->stream));
   if (e->variant < 0) {
     int rc = tune(e);
@@ -471,15 +725,33 @@ int lbrb_ensemble_step(lbrb_ensemble_t* e, int n) {
     int rc = set_items(e, e->variant);
     if (rc) return rc;
   }
-  int t = 0;
-  if (!e->timing && n - 1 >= 6) {
-    int rc = ensure_graph(e);
+  if (npairs > 0) {
+    if (e->pair_variant < 0) {
+      int rc = tune_pairs(e);
+      if (rc) return rc;
+    }
+    int rc = set_pair_items(e);
     if (rc) return rc;
-    for (; t + 6 <= n - 1; t += 6) EK(e, cudaGraphLaunch(e->gexec, e->stream));
+    int q = 0;
+    if (!e->timing && npairs >= 6) {
+      rc = ensure_pair_graph(e);
+      if (rc) return rc;
+      for (; q + 6 <= npairs; q += 6) EK(e, cudaGraphLaunch(e->pgexec, e->stream));
+    }
+    for (; q < npairs; q++) EK(e, launch_pair(e, q % 6));
+    if (n - 2 * npairs == 2) EK(e, launch_step(e, 7));
+    EK(e, launch_step(e, 8));
+  } else {
+    int t = 0;
+    if (!e->timing && n - 1 >= 6) {
+      int rc = ensure_graph(e);
+      if (rc) return rc;
+      for (; t + 6 <= n - 1; t += 6) EK(e, cudaGraphLaunch(e->gexec, e->stream));
+    }
+    for (; t < n - 1; t++) EK(e, launch_step(e, t % 6));
+    EK(e, launch_step(e, 6));
   }
-  for (; t < n - 1; t++) EK(e, launch_step(e, t % 6));
-  EK(e, launch_step(e, 6));
-  advance_members(e, n);
+  advance_members(e, n, npairs);
   // the members' own streams see the ensemble's steps
   EK(e, cudaEventRecord(e->ev, e->stream));
   for (lbrb_t* h : e->m) EK(e, cudaStreamWaitEvent(h->stream, e->ev, 0));

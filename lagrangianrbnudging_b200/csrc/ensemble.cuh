@@ -19,6 +19,10 @@ struct EnsAux {
   double alpha;
   unsigned long long* acc;  // fixed-point innovation sums
   unsigned* dflags;
+  // two steps per launch (the first step's view of a pair): the sums formed
+  // before the launch and their node mask
+  unsigned long long* acc2;
+  unsigned* nmask;
 };
 
 // observation row of the member's step istep0 + t + 1 (t counts the steps of
@@ -49,5 +53,24 @@ cudaError_t launch_ens_aux(bool f32, const void* aux, const int2* pchunks, int n
                            const int2* ochunks, int nochunks, int* ctr, cudaStream_t s);
 cudaError_t launch_ens_apply(bool f32, const void* aux, const int2* ochunks, int nochunks,
                              const int* ctr, cudaStream_t s);
+
+// Two steps per launch for every member (ensemble_kernels.cu).  A pair's
+// launches: ens_pre (step n's innovations of the nudged members, formed from
+// T^n before the launch), ens_march (the marching two-step kernel over work
+// items (member, first column, first row, rows); views1/views2 hold each
+// member's step n and step n+1 views), ens_aux2 (every member's particles of
+// both steps; the innovations of step n+1), ens_apply2 (the nudging apply of
+// step n+1 and the clearing of step n's sums).  aux1/aux2: EnsAux of steps n
+// and n+1.  Pair variants: rows per marching group.
+constexpr int ENS_PAIR_VARIANTS = 3;
+int ens_pair_rows(int variant);
+cudaError_t launch_ens_pre(bool f32, const void* views1, const void* aux1, const int2* ochunks, int nochunks,
+                           const int* ctr, cudaStream_t s);
+cudaError_t launch_ens_march(bool f32, bool off32, int variant, const void* views1, const void* views2,
+                             const int4* items, int nitems, int* ctr, cudaStream_t s);
+cudaError_t launch_ens_aux2(bool f32, const void* aux1, const void* aux2, const int2* pchunks, int npchunks,
+                            const int2* ochunks, int nochunks, int* ctr, cudaStream_t s);
+cudaError_t launch_ens_apply2(bool f32, const void* aux1, const void* aux2, const int2* ochunks, int nochunks,
+                              const int* ctr, cudaStream_t s);
 
 }  // namespace lbrb

@@ -24,7 +24,7 @@
 
 #include "capi_internal.cuh"
 #include "ensemble.cuh"
-#include "lb_node.cuh"
+#include "lb_pair.cuh"
 #include "nudge_dev.cuh"
 #include "particle_dev.cuh"
 
@@ -111,6 +111,159 @@ __global__ void __launch_bounds__(512)
   if (o >= A.nobs) return;
   const double* ob = ens_obs_row(A, ctr[0] - 1);
   obs_apply_one(A.g, A.plane, A.nx, A.ny, A.pitch, ob[o], ob[A.nobs + o], threadIdx.x & 3, A.acc);
+}
+
+// ------------------------------------------------- two steps per launch
+// The member's two step views are copied into shared memory; the ring of
+// march_block follows them (dynamic shared memory).  Block 0 counts the two
+// steps in ctr[0] (the later phases pick observation rows from it).
+template <typename Real, int R, int MINB, typename Off>
+__global__ void __launch_bounds__(32 * (R + 1), MINB)
+    ens_march_kernel(const LBView<Real>* __restrict__ views1, const LBView<Real>* __restrict__ views2,
+                     const int4* __restrict__ items, int* __restrict__ ctr) {
+  __shared__ LBView<Real> sV[2];
+  extern __shared__ __align__(16) unsigned char ens_march_smem[];
+  pdl_wait();
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ctr[0], 2);
+  const int4 w = items[blockIdx.x];  // (member, first column, first row, rows)
+  constexpr int WORDS = (int)(sizeof(LBView<Real>) / sizeof(int));
+  static_assert(sizeof(LBView<Real>) % sizeof(int) == 0, "view size");
+  const int* s1 = reinterpret_cast<const int*>(views1 + w.x);
+  const int* s2 = reinterpret_cast<const int*>(views2 + w.x);
+  int* d = reinterpret_cast<int*>(sV);
+  for (int i = threadIdx.x; i < 2 * WORDS; i += blockDim.x) d[i] = i < WORDS ? s1[i] : s2[i - WORDS];
+  __syncthreads();
+  march_block<Real, R, Off>(sV[0], sV[1], w.y, w.z, w.w, ens_march_smem);
+}
+
+// step n's innovations of the nudged members, before the pair's launch
+// (ctr[0] steps of this call done)
+template <typename Real>
+__global__ void __launch_bounds__(128)
+    ens_pre_kernel(const LBView<Real>* __restrict__ views1, const EnsAux<Real>* __restrict__ aux1,
+                   const int2* __restrict__ ochunks, const int* __restrict__ ctr) {
+  pdl_wait();
+  const int2 c = ochunks[blockIdx.x];
+  const EnsAux<Real>& A = aux1[c.x];
+  const int o = c.y + threadIdx.x;
+  if (o >= A.nobs) return;
+  const double* ob = ens_obs_row(A, ctr[0]);
+  obs_pre_one(views1[c.x], ob[o], ob[A.nobs + o], ob[2 * A.nobs + o], A.alpha, A.acc2, A.nmask, A.dflags);
+}
+
+// every member's particles of both steps; step n+1's innovations
+template <typename Real>
+__global__ void __launch_bounds__(128)
+    ens_aux2_kernel(const EnsAux<Real>* __restrict__ aux1, const EnsAux<Real>* __restrict__ aux2,
+                    const int2* __restrict__ pchunks, int npchunks, const int2* __restrict__ ochunks, int nochunks,
+                    int* __restrict__ ctr) {
+  pdl_wait();
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctr[1] = 0;
+  int b = blockIdx.x;
+  if (b < npchunks) {
+    const int2 c = pchunks[b];
+    const int p = c.y + threadIdx.x;
+    if (p < aux1[c.x].P.np) {
+      particle_update(aux1[c.x].P, p);
+      particle_update(aux2[c.x].P, p);
+    }
+    return;
+  }
+  b -= npchunks;
+  if (b < nochunks) {
+    const int2 c = ochunks[b];
+    const EnsAux<Real>& A = aux2[c.x];
+    const int o = c.y + threadIdx.x;
+    if (o >= A.nobs) return;
+    const double* ob = ens_obs_row(A, ctr[0] - 1);
+    obs_scatter_one(A.T, A.nx, A.ny, A.pitch, ob[o], ob[A.nobs + o], ob[2 * A.nobs + o], A.alpha, A.acc, A.dflags);
+  }
+}
+
+// step n+1's nudging apply; step n's sums and mask bits cleared (4 threads
+// per observation, its cell corners)
+template <typename Real>
+__global__ void __launch_bounds__(512)
+    ens_apply2_kernel(const EnsAux<Real>* __restrict__ aux1, const EnsAux<Real>* __restrict__ aux2,
+                      const int2* __restrict__ ochunks, const int* __restrict__ ctr) {
+  pdl_wait();
+  const int2 c = ochunks[blockIdx.x];
+  const EnsAux<Real>& A = aux2[c.x];
+  const int o = c.y + (threadIdx.x >> 2);
+  if (o >= A.nobs) return;
+  const double* ob = ens_obs_row(A, ctr[0] - 1);
+  obs_apply_one(A.g, A.plane, A.nx, A.ny, A.pitch, ob[o], ob[A.nobs + o], threadIdx.x & 3, A.acc);
+  const EnsAux<Real>& A1 = aux1[c.x];
+  const double* o1 = ens_obs_row(A1, ctr[0] - 2);
+  obs_clear_one(A1.nx, A1.ny, A1.pitch, o1[o], o1[A1.nobs + o], threadIdx.x & 3, A1.acc2, A1.nmask);
+}
+
+// pair variants: (rows per group, min blocks per SM)
+constexpr int2 ENS_PAIR_TABLE[ENS_PAIR_VARIANTS] = {{8, 4}, {4, 8}, {16, 2}};
+int ens_pair_rows(int variant) { return ENS_PAIR_TABLE[variant].x; }
+
+template <typename Real, int R, int MINB, typename Off>
+static cudaError_t ens_march_launch(const void* v1, const void* v2, const int4* items, int nitems, int* ctr,
+                                    cudaStream_t s) {
+  constexpr int MB = std::is_same<Real, double>::value ? (MINB + 1) / 2 : MINB;
+  auto k = ens_march_kernel<Real, R, MB, Off>;
+  constexpr size_t smem = march_smem_bytes<Real, R>();
+  static std::atomic<unsigned long long> attr_set{0};
+  const cudaError_t e = smem_limit_once((const void*)k, smem, attr_set);
+  if (e != cudaSuccess) return e;
+  if (nitems <= 0) return cudaSuccess;
+  return launch_k(k, nitems, 32 * (R + 1), smem, s, true, (const LBView<Real>*)v1, (const LBView<Real>*)v2,
+                  items, ctr);
+}
+
+template <typename Real, typename Off>
+static cudaError_t ens_march_dispatch(int variant, const void* v1, const void* v2, const int4* items, int nitems,
+                                      int* ctr, cudaStream_t s) {
+  switch (variant) {
+    case 1: return ens_march_launch<Real, 4, 8, Off>(v1, v2, items, nitems, ctr, s);
+    case 2: return ens_march_launch<Real, 16, 2, Off>(v1, v2, items, nitems, ctr, s);
+    default: return ens_march_launch<Real, 8, 4, Off>(v1, v2, items, nitems, ctr, s);
+  }
+}
+
+cudaError_t launch_ens_march(bool f32, bool off32, int variant, const void* views1, const void* views2,
+                             const int4* items, int nitems, int* ctr, cudaStream_t s) {
+  if (f32)
+    return off32 ? ens_march_dispatch<float, uint32_t>(variant, views1, views2, items, nitems, ctr, s)
+                 : ens_march_dispatch<float, size_t>(variant, views1, views2, items, nitems, ctr, s);
+  return off32 ? ens_march_dispatch<double, uint32_t>(variant, views1, views2, items, nitems, ctr, s)
+               : ens_march_dispatch<double, size_t>(variant, views1, views2, items, nitems, ctr, s);
+}
+
+cudaError_t launch_ens_pre(bool f32, const void* views1, const void* aux1, const int2* ochunks, int nochunks,
+                           const int* ctr, cudaStream_t s) {
+  if (nochunks <= 0) return cudaSuccess;
+  if (f32)
+    return launch_k(ens_pre_kernel<float>, nochunks, ENS_OCHUNK, 0, s, true, (const LBView<float>*)views1,
+                    (const EnsAux<float>*)aux1, ochunks, ctr);
+  return launch_k(ens_pre_kernel<double>, nochunks, ENS_OCHUNK, 0, s, true, (const LBView<double>*)views1,
+                  (const EnsAux<double>*)aux1, ochunks, ctr);
+}
+
+cudaError_t launch_ens_aux2(bool f32, const void* aux1, const void* aux2, const int2* pchunks, int npchunks,
+                            const int2* ochunks, int nochunks, int* ctr, cudaStream_t s) {
+  const int g = npchunks + nochunks;
+  if (g <= 0) return cudaSuccess;
+  if (f32)
+    return launch_k(ens_aux2_kernel<float>, g, 128, 0, s, true, (const EnsAux<float>*)aux1,
+                    (const EnsAux<float>*)aux2, pchunks, npchunks, ochunks, nochunks, ctr);
+  return launch_k(ens_aux2_kernel<double>, g, 128, 0, s, true, (const EnsAux<double>*)aux1,
+                  (const EnsAux<double>*)aux2, pchunks, npchunks, ochunks, nochunks, ctr);
+}
+
+cudaError_t launch_ens_apply2(bool f32, const void* aux1, const void* aux2, const int2* ochunks, int nochunks,
+                              const int* ctr, cudaStream_t s) {
+  if (nochunks <= 0) return cudaSuccess;
+  if (f32)
+    return launch_k(ens_apply2_kernel<float>, nochunks, 4 * ENS_OCHUNK, 0, s, true, (const EnsAux<float>*)aux1,
+                    (const EnsAux<float>*)aux2, ochunks, ctr);
+  return launch_k(ens_apply2_kernel<double>, nochunks, 4 * ENS_OCHUNK, 0, s, true, (const EnsAux<double>*)aux1,
+                  (const EnsAux<double>*)aux2, ochunks, ctr);
 }
 
 // ------------------------------------------------------------ variants

@@ -10,6 +10,7 @@
 
 #include <type_traits>
 
+#include "lb_node.cuh"
 #include "lbrb_internal.cuh"
 
 namespace lbrb {
@@ -95,6 +96,55 @@ __device__ __forceinline__ void obs_apply_one(Real* __restrict__ g, size_t plane
     Real* a = g + (size_t)k * plane + q;
     *a = *a + nudge_increment<Real>(k, sv);
   }
+}
+
+// Two-step launch of a nudged run, before the launch: the innovation of one
+// observation of step n from T^n at its cell corners.  T^n is the moment of
+// the populations streaming into a corner -- pulled from the state before
+// the step (V's sources), walls applied, summed as the fused step sums them
+// -- so it equals the T the step itself forms.  The sums go to acc (fixed
+// point, as a single step's scatter) and the corners' bits to the node mask
+// (pitch / 32 words per row), which the two-step kernels read to add the
+// sums after the collision.
+template <typename Real>
+__device__ __forceinline__ void obs_pre_one(const LBView<Real>& V, double xx, double yy, double Tobs, double alpha,
+                                            unsigned long long* __restrict__ acc, unsigned* __restrict__ mask,
+                                            unsigned* dflags) {
+  const int nx = V.nx, ny = V.ny, words = V.pitch >> 5;
+  auto Tat = [&](int j, int i) -> Real {
+    Real fs[NPOP], gs[NPOP];
+    pull_node<Real, LBRB_TWALL_DIRICHLET, size_t, true>(V, j, i, fs, gs);
+    dirichlet_walls(V, j, gs);
+    if constexpr (std::is_same<Real, double>::value) {
+      double t = 0.0;
+#pragma unroll
+      for (int k = 0; k < NPOP; k++) t = t + gs[k];
+      return t;
+    } else {
+      float dT = 0.f;
+#pragma unroll
+      for (int k = 0; k < NPOP; k++) dT += gs[k];
+      return (float)V.T0 + dT;
+    }
+  };
+  obs_scatter_rows(Tat, nx, ny, V.pitch, xx, yy, Tobs, alpha, acc, dflags, 0, ny);
+  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
+  int x1, y1, ix1, ix2, jy1, jy2;
+  obs_cell(xx, yy, nx, ny, x1, y1, ix1, ix2, jy1, jy2);
+  for (int jy : {jy1, jy2})
+    for (int ix : {ix1, ix2}) atomicOr(&mask[(size_t)jy * words + (ix >> 5)], 1u << (ix & 31));
+}
+
+// after the launch: clear corner `corner` (0..3) of an observation of step n
+__device__ __forceinline__ void obs_clear_one(int nx, int ny, int pitch, double xx, double yy, int corner,
+                                              unsigned long long* __restrict__ acc, unsigned* __restrict__ mask) {
+  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
+  int ix = ((int)xx + (corner & 1) - 1) % nx;
+  if (ix < 0) ix += nx;
+  int jy = ((int)yy + (corner >> 1) - 1) % ny;
+  if (jy < 0) jy += ny;
+  acc[(size_t)jy * pitch + ix] = 0ull;
+  atomicAnd(&mask[(size_t)jy * (pitch >> 5) + (ix >> 5)], ~(1u << (ix & 31)));
 }
 
 }  // namespace lbrb

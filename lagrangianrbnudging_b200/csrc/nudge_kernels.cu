@@ -19,7 +19,6 @@
 //   weights; contributions are summed in 2^-40 fixed point with integer
 //   atomics, so the result does not depend on their order, then added to the
 //   post-collision g as w_k * S.
-#include "lb_node.cuh"
 #include "lbrb_internal.cuh"
 #include "nudge_dev.cuh"
 
@@ -294,13 +293,8 @@ __global__ void obs_apply_kernel(Real* __restrict__ g, size_t plane, int nx, int
   obs_apply_one(g, plane, nx, ny, pitch, ox[p], oy[p], t & 3, acc);
 }
 
-// Two-step launch of a nudged run, before the launch: step n's innovations
-// from T^n at the observations' cell corners.  T^n is the moment of the
-// populations streaming into a corner -- pulled from the state before the
-// step, walls applied, summed as the fused step sums them -- so it equals
-// the T the step itself forms.  The sums go to acc (fixed point, as the
-// scatter of a single step) and the corners' bits to the node mask, which
-// lb_pair_kernel / lb_march_kernel read to add the sums after the collision.
+// Two-step launch of a nudged run: step n's innovations before the launch,
+// and the clearing of their sums and mask bits after it (nudge_dev.cuh)
 template <typename Real>
 __global__ void obs_pre_kernel(const LBView<Real> V, const double* __restrict__ ox, const double* __restrict__ oy,
                                const double* __restrict__ oT, int nobs, double alpha,
@@ -308,48 +302,17 @@ __global__ void obs_pre_kernel(const LBView<Real> V, const double* __restrict__ 
   pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nobs) return;
-  const int nx = V.nx, ny = V.ny, words = V.pitch >> 5;
-  auto Tat = [&](int j, int i) -> Real {
-    Real fs[NPOP], gs[NPOP];
-    pull_node<Real, LBRB_TWALL_DIRICHLET, size_t, true>(V, j, i, fs, gs);
-    dirichlet_walls(V, j, gs);
-    if constexpr (std::is_same<Real, double>::value) {
-      double t = 0.0;
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) t = t + gs[k];
-      return t;
-    } else {
-      float dT = 0.f;
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) dT += gs[k];
-      return (float)V.T0 + dT;
-    }
-  };
-  const double xx = ox[p], yy = oy[p];
-  obs_scatter_rows(Tat, nx, ny, V.pitch, xx, yy, oT[p], alpha, acc, dflags, 0, ny);
-  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
-  int x1, y1, ix1, ix2, jy1, jy2;
-  obs_cell(xx, yy, nx, ny, x1, y1, ix1, ix2, jy1, jy2);
-  for (int jy : {jy1, jy2})
-    for (int ix : {ix1, ix2}) atomicOr(&mask[(size_t)jy * words + (ix >> 5)], 1u << (ix & 31));
+  obs_pre_one(V, ox[p], oy[p], oT[p], alpha, acc, mask, dflags);
 }
 
-// after the launch: clear the sums and mask bits of step n's corners
 __global__ void obs_clear_kernel(int nx, int ny, int pitch, const double* __restrict__ ox,
                                  const double* __restrict__ oy, int nobs, unsigned long long* __restrict__ acc,
                                  unsigned* __restrict__ mask) {
   pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 4 * nobs) return;
-  const int p = t >> 2, corner = t & 3;
-  const double xx = ox[p], yy = oy[p];
-  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
-  int ix = ((int)xx + (corner & 1) - 1) % nx;
-  if (ix < 0) ix += nx;
-  int jy = ((int)yy + (corner >> 1) - 1) % ny;
-  if (jy < 0) jy += ny;
-  acc[(size_t)jy * pitch + ix] = 0ull;
-  atomicAnd(&mask[(size_t)jy * (pitch >> 5) + (ix >> 5)], ~(1u << (ix & 31)));
+  const int p = t >> 2;
+  obs_clear_one(nx, ny, pitch, ox[p], oy[p], t & 3, acc, mask);
 }
 
 cudaError_t launch_obs_pre_fp32(const LBView<float>& V, const double* ox, const double* oy, const double* oT,

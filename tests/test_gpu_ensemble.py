@@ -1,8 +1,9 @@
 """The ensemble (lbrb_ensemble_*): members of uneven grid size, closure,
-particles and nudging advanced by one launch per phase of the step, replayed
-from a CUDA graph, end bit-identical to the same handles advanced alone by
-lbrb_step -- whatever the launch variant, with or without the graph, and with
-per-member steps in between."""
+particles and nudging advanced by one launch per phase of the step, or two
+steps per launch (the marching kernel over all members, nudged members
+included), replayed from CUDA graphs, end bit-identical to the same handles
+advanced alone by lbrb_step -- whatever the launch variant, with or without
+the graphs, and with per-member steps in between."""
 import numpy as np
 import pytest
 
@@ -64,11 +65,16 @@ def assert_same(a, b):
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_ensemble_matches_members_stepped_alone(precision):
+@pytest.mark.parametrize("pairs", [1, 0])
+def test_ensemble_matches_members_stepped_alone(precision, pairs):
+    """pairs: 20 steps = 9 pairs (one graph of 6 pairs, 3 direct) + 2 single
+    steps, then 7 = 3 pairs + 1; singles: 3 graph replays of 6 steps, then
+    single steps"""
     A = [make_member(s, precision) for s in SPECS]
     B = [make_member(s, precision) for s in SPECS]
     with lb.Ensemble(A) as ens:
-        ens.step(20)  # 3 graph replays of 6 steps, then single steps
+        ens.set_pairs(pairs)
+        ens.step(20)
         ens.sync()
         for r in B:
             r.step(20)
@@ -88,6 +94,7 @@ def test_every_launch_variant_gives_identical_results():
     for v in range(lb.Ensemble.nvariants()):
         A = [make_member(s, "fp32") for s in SPECS]
         with lb.Ensemble(A) as ens:
+            ens.set_pairs(0)  # (every step in the variant under test)
             ens.set_schedule(v)
             ens.step(9)
             ens.sync()
@@ -122,6 +129,8 @@ def test_timing_mode_launches_directly_with_same_results():
     with lb.Ensemble(A) as ea, lb.Ensemble(B) as eb:
         eb.set_schedule(ea_variant := 4)
         ea.set_schedule(ea_variant)
+        ea.set_pairs(0)
+        eb.set_pairs(0)
         ea.set_timing(True)
         ea.step(14)
         t = ea.get_timing()
@@ -130,6 +139,40 @@ def test_timing_mode_launches_directly_with_same_results():
         eb.sync()
     assert t["lb_step"][1] == 14 and t["aux"][1] == 14 and t["apply"][1] == 14
     assert t["lb_step"][0] > 0
+    for a, b in zip(A, B):
+        assert_same(snapshot(a), snapshot(b))
+
+
+def test_pair_timing_mode_launches_directly_with_same_results():
+    """14 steps in pairs: 6 pairs (pre-innovations, marching launch, aux,
+    apply each) + 2 single steps, launched directly"""
+    A = [make_member(s, "fp32") for s in SPECS]
+    B = [make_member(s, "fp32") for s in SPECS]
+    with lb.Ensemble(A) as ea, lb.Ensemble(B) as eb:
+        ea.set_timing(True)
+        ea.step(14)
+        t = ea.get_timing()
+        eb.step(14)
+        ea.sync()
+        eb.sync()
+        p = ea.pairs()
+    assert p["mode"] == -1 and p["rows"] in (4, 8, 16) and p["tuned_ms"] > 0
+    assert t["lb_step"][1] == 8 and t["aux"][1] == 8 and t["apply"][1] == 2 * 6 + 2
+    for a, b in zip(A, B):
+        assert_same(snapshot(a), snapshot(b))
+
+
+def test_ensemble_pairs_match_single_steps_over_many_calls():
+    """calls of odd and even lengths (a pair never takes a call's last step)"""
+    A = [make_member(s, "fp32") for s in SPECS]
+    B = [make_member(s, "fp32") for s in SPECS]
+    with lb.Ensemble(A) as ea, lb.Ensemble(B) as eb:
+        eb.set_pairs(0)
+        for n in (1, 2, 3, 4, 13, 26):
+            ea.step(n)
+            eb.step(n)
+        ea.sync()
+        eb.sync()
     for a, b in zip(A, B):
         assert_same(snapshot(a), snapshot(b))
 
