@@ -240,15 +240,32 @@ def measured_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(precision: str):
-    """DRAM bytes per node of one fused-kernel launch from the committed ncu
-    summary (profiles/lb_step_traffic.json; "fp32" is the two-step launch,
-    "fp32_single" the one-step one), or None."""
+# the sources of the fused kernels: a traffic capture counts only for the build it measured
+KERNEL_SOURCES = ["lb_kernels.cu", "lb_pair.cuh", "lb_node.cuh", "lbrb_internal.cuh"]
+
+
+def kernel_sources_sha() -> str:
+    import hashlib
+
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        h.update((ROOT / "lagrangianrbnudging_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def profiled_traffic(precision: str, kernel: str):
+    """DRAM bytes per node of one launch of `kernel` from the committed ncu
+    summary (profiles/lb_step_traffic.json), or None when that capture was
+    made on other kernel sources than this build's or on another kernel."""
     p = ROOT / "profiles" / "lb_step_traffic.json"
     if not p.exists():
         return None
     try:
-        return float(json.loads(p.read_text())[precision]["bytes_per_node"])
+        d = json.loads(p.read_text())
+        e = d[precision]
+        if d.get("kernel_sources_sha") != kernel_sources_sha() or e.get("kernel") != kernel:
+            return None
+        return float(e["bytes_per_node"])
     except Exception:
         return None
 
@@ -427,11 +444,15 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     avg_lb = lb_ms / max(lb_n, 1)
     spl = K / max(lb_n, 1)
     achieved = ALG_BYTES["fp32"] * nodes * spl / (avg_lb * 1e-3) / 1e9
-    tr = profiled_traffic("fp32" if spl > 1.5 else "fp32_single")
+    tr = None  # (set below, once the kernel of the launches is known)
     spl64 = K64 / max(timing64["lb_step"][1], 1)
     avg_lb64 = timing64["lb_step"][0] / max(timing64["lb_step"][1], 1)
     achieved64 = ALG_BYTES["fp64"] * nodes * spl64 / (avg_lb64 * 1e-3) / 1e9
-    kernel32 = "lb_pair_kernel<float>" if pair32["shape"] >= 0 and spl > 1.5 else "lb_node_kernel<float>"
+    if pair32["shape"] >= 0 and spl > 1.5:
+        kernel32 = "lb_march_kernel<float>" if pair32["shape"] >= 9 else "lb_pair_kernel<float>"
+    else:
+        kernel32 = "lb_node_kernel<float>"
+    tr = profiled_traffic("fp32" if spl > 1.5 else "fp32_single", kernel32)
     out.update({
         "metric": METRIC,
         "value": round(mlups, 1),
@@ -459,6 +480,9 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
                      "node_steps_per_launch": round(spl, 4),
                      "avg_launch_ms": round(avg_lb, 5),
                      "traffic": (round(tr * nodes) if tr else None),
+                     "traffic_source": ("profiles/lb_step_traffic.json, captured on these kernel sources "
+                                        f"(sha {kernel_sources_sha()})" if tr else
+                                        "none: no ncu capture of this build's kernel on record"),
                      "traffic_gbs": (round(tr * nodes / (avg_lb * 1e-3) / 1e9, 1) if tr else None),
                      "share_of_step": round(lb_ms / timing["window_ms"][0], 4),
                      "launch_shape": shape32, "pair_shape": pair32,
