@@ -403,8 +403,9 @@ def run_ours(args, torch, dist, rank: int, world: int, device: int) -> dict | No
     # the same number of steps as the FP32 run (two windows each) for the Nu
     # comparison, draining the records as they come
     rest = 2 * (K - K64)
+    r64.drain_records()
     while rest > 0:
-        n = min(rest, 1000)
+        n = min(rest, 4 * NOUTCONFIG)  # (fewer records per call than the ring holds)
         r64.step(n)
         r64.drain_records()
         rest -= n

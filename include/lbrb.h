@@ -194,9 +194,10 @@ LBRB_API int lbrb_set_pairs(lbrb_t *h, int mode);
  * the tile and its ring, 5: 30x8 likewise, 6: 32x8 at 5 blocks per SM,
  * 7: 32x6, 8: 64x8.  Strips of 32 columns walked down a chunk of rows,
  * recomputing only two halo columns and two rows per chunk (tile_y: rows
- * per group): 9: 8 rows, 4 blocks per SM; 10: 4 rows, 8 blocks; 11: 16 rows,
- * 2 blocks; 12: 6 rows, 5 blocks; 13: 8 rows, 4 blocks, taller chunks;
- * 14: 8 rows, 3 blocks. */
+ * per group): 9: 8 rows, 3 blocks per SM; 10: 8 rows, 3 blocks, the next
+ * group's loads issued before this group's second step (software
+ * pipelining); 11: likewise, 2 blocks; 12: 6 rows, 4 blocks, pipelined;
+ * 13: 4 rows, 6 blocks, pipelined; 14: 6 rows, 3 blocks, pipelined. */
 LBRB_API int lbrb_set_pair_shape(lbrb_t *h, int shape);
 /* the number of launch shapes of the two-step kernel (0 .. n-1) */
 LBRB_API int lbrb_pair_shapes(void);

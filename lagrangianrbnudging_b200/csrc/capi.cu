@@ -1926,7 +1926,7 @@ int lbrb_get_pair_shape(const lbrb_t* h, int* shape, int* tile_x, int* tile_y, f
   // (lb_kernels.cu: PAIR_SHAPES, then MARCH_SHAPES: a strip of 32 columns
   // walked in groups of tile_y rows)
   static const int TXS[] = {32, 32, 32, 64, 32, 30, 32, 32, 64, 32, 32, 32, 32, 32, 32},
-                   TYS[] = {8, 4, 16, 4, 8, 8, 8, 6, 8, 8, 4, 16, 6, 8, 8};
+                   TYS[] = {8, 4, 16, 4, 8, 8, 8, 6, 8, 8, 8, 8, 6, 4, 6};
   static_assert(sizeof(TXS) / sizeof(int) == NUM_PAIR_SHAPES, "pair shape table");
   const int sh = h->pair_shape;
   if (shape) *shape = sh;

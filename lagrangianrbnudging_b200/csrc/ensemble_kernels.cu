@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(512)
 // The member's two step views are copied into shared memory; the ring of
 // march_block follows them (dynamic shared memory).  Block 0 counts the two
 // steps in ctr[0] (the later phases pick observation rows from it).
-template <typename Real, int R, int MINB, typename Off>
+template <typename Real, int R, int MINB, bool PRE, typename Off>
 __global__ void __launch_bounds__(32 * (R + 1), MINB)
     ens_march_kernel(const LBView<Real>* __restrict__ views1, const LBView<Real>* __restrict__ views2,
                      const int4* __restrict__ items, int* __restrict__ ctr) {
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(32 * (R + 1), MINB)
   int* d = reinterpret_cast<int*>(sV);
   for (int i = threadIdx.x; i < 2 * WORDS; i += blockDim.x) d[i] = i < WORDS ? s1[i] : s2[i - WORDS];
   __syncthreads();
-  march_block<Real, R, Off>(sV[0], sV[1], w.y, w.z, w.w, ens_march_smem);
+  march_block<Real, R, PRE, Off>(sV[0], sV[1], w.y, w.z, w.w, ens_march_smem);
 }
 
 // step n's innovations of the nudged members, before the pair's launch
@@ -198,15 +198,15 @@ __global__ void __launch_bounds__(512)
   obs_clear_one(A1.nx, A1.ny, A1.pitch, o1[o], o1[A1.nobs + o], threadIdx.x & 3, A1.acc2, A1.nmask);
 }
 
-// pair variants: (rows per group, min blocks per SM)
-constexpr int2 ENS_PAIR_TABLE[ENS_PAIR_VARIANTS] = {{8, 4}, {4, 8}, {16, 2}};
+// pair variants: (rows per group, min blocks per SM, software pipelining)
+constexpr int3 ENS_PAIR_TABLE[ENS_PAIR_VARIANTS] = {{8, 3, 0}, {8, 3, 1}, {6, 4, 1}};
 int ens_pair_rows(int variant) { return ENS_PAIR_TABLE[variant].x; }
 
-template <typename Real, int R, int MINB, typename Off>
+template <typename Real, int R, int MINB, bool PRE, typename Off>
 static cudaError_t ens_march_launch(const void* v1, const void* v2, const int4* items, int nitems, int* ctr,
                                     cudaStream_t s) {
   constexpr int MB = std::is_same<Real, double>::value ? (MINB + 1) / 2 : MINB;
-  auto k = ens_march_kernel<Real, R, MB, Off>;
+  auto k = ens_march_kernel<Real, R, MB, PRE, Off>;
   constexpr size_t smem = march_smem_bytes<Real, R>();
   static std::atomic<unsigned long long> attr_set{0};
   const cudaError_t e = smem_limit_once((const void*)k, smem, attr_set);
@@ -220,9 +220,9 @@ template <typename Real, typename Off>
 static cudaError_t ens_march_dispatch(int variant, const void* v1, const void* v2, const int4* items, int nitems,
                                       int* ctr, cudaStream_t s) {
   switch (variant) {
-    case 1: return ens_march_launch<Real, 4, 8, Off>(v1, v2, items, nitems, ctr, s);
-    case 2: return ens_march_launch<Real, 16, 2, Off>(v1, v2, items, nitems, ctr, s);
-    default: return ens_march_launch<Real, 8, 4, Off>(v1, v2, items, nitems, ctr, s);
+    case 1: return ens_march_launch<Real, 8, 3, true, Off>(v1, v2, items, nitems, ctr, s);
+    case 2: return ens_march_launch<Real, 6, 4, true, Off>(v1, v2, items, nitems, ctr, s);
+    default: return ens_march_launch<Real, 8, 3, false, Off>(v1, v2, items, nitems, ctr, s);
   }
 }
 

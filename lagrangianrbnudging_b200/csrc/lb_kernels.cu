@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
   lb_finish_node<Real, false, Off>(V2, (Off)j * pitch + (Off)x, fs, gs, SF[ty * TX + tx]);
 }
 
-template <typename Real, int R, int MINB, typename Off>
+template <typename Real, int R, int MINB, bool PRE, typename Off>
 __global__ void __launch_bounds__(32 * (R + 1), MINB)
     lb_march_kernel(const LBView<Real> V1, const LBView<Real> V2, int H) {
   pdl_wait();
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(32 * (R + 1), MINB)
   const int nstrips = (V1.nx + 31) >> 5;
   const int strip = blockIdx.x % nstrips, chunk = blockIdx.x / nstrips;
   const int ya = chunk * H;
-  march_block<Real, R, Off>(V1, V2, strip * 32, ya, min(H, V1.ny - ya), march_smem);
+  march_block<Real, R, PRE, Off>(V1, V2, strip * 32, ya, min(H, V1.ny - ya), march_smem);
 }
 
 // pair launch shapes: (tile columns, tile rows, threads, min blocks per SM)
@@ -198,12 +198,13 @@ static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2,
 // marching launch shapes: (rows per group R, min blocks per SM, waves): the
 // chunk height H = kR - 2 (whole groups) is chosen so that the grid of
 // strips x chunks holds about `waves` waves of resident blocks
-struct MarchShape { int r, minb, waves; };
-constexpr MarchShape MARCH_SHAPES[] = {{8, 4, 8}, {4, 8, 8}, {16, 2, 8}, {6, 5, 8}, {8, 4, 3}, {8, 3, 8}};
+struct MarchShape { int r, minb, waves, pre; };
+constexpr MarchShape MARCH_SHAPES[] = {{8, 3, 8, 0}, {8, 3, 8, 1}, {8, 2, 8, 1},
+                                       {6, 4, 8, 1}, {4, 6, 8, 1}, {6, 3, 8, 1}};
 constexpr int NMARCH = sizeof(MARCH_SHAPES) / sizeof(MARCH_SHAPES[0]);
 static_assert(NPAIR + NMARCH == NUM_PAIR_SHAPES, "pair shape table");
 
-template <typename Real, int R, int MINB>
+template <typename Real, int R, int MINB, bool PRE>
 static cudaError_t launch_march_t(const LBView<Real>& V1, const LBView<Real>& V2, int waves, cudaStream_t s,
                                   bool pdl) {
   constexpr int NT = 32 * (R + 1);
@@ -228,19 +229,20 @@ static cudaError_t launch_march_t(const LBView<Real>& V1, const LBView<Real>& V2
     const long nchunks = (ny + H - 1) / H;
     return launch_k(kernel, dim3((unsigned)(nstrips * nchunks)), NT, smem, s, pdl, V1, V2, H);
   };
-  if (off32_ok(V1.plane)) return go(lb_march_kernel<Real, R, MB, uint32_t>);
-  return go(lb_march_kernel<Real, R, MB, size_t>);
+  if (off32_ok(V1.plane)) return go(lb_march_kernel<Real, R, MB, PRE, uint32_t>);
+  return go(lb_march_kernel<Real, R, MB, PRE, size_t>);
 }
 
 template <typename Real>
 static cudaError_t launch_march(const LBView<Real>& V1, const LBView<Real>& V2, int m, cudaStream_t s, bool pdl) {
   const int waves = MARCH_SHAPES[m].waves;
   switch (m) {
-    case 1: return launch_march_t<Real, 4, 8>(V1, V2, waves, s, pdl);
-    case 2: return launch_march_t<Real, 16, 2>(V1, V2, waves, s, pdl);
-    case 3: return launch_march_t<Real, 6, 5>(V1, V2, waves, s, pdl);
-    case 5: return launch_march_t<Real, 8, 3>(V1, V2, waves, s, pdl);
-    default: return launch_march_t<Real, 8, 4>(V1, V2, waves, s, pdl);  // (0 and 4: 8 rows, 4 blocks)
+    case 1: return launch_march_t<Real, 8, 3, true>(V1, V2, waves, s, pdl);
+    case 2: return launch_march_t<Real, 8, 2, true>(V1, V2, waves, s, pdl);
+    case 3: return launch_march_t<Real, 6, 4, true>(V1, V2, waves, s, pdl);
+    case 4: return launch_march_t<Real, 4, 6, true>(V1, V2, waves, s, pdl);
+    case 5: return launch_march_t<Real, 6, 3, true>(V1, V2, waves, s, pdl);
+    default: return launch_march_t<Real, 8, 3, false>(V1, V2, waves, s, pdl);
   }
 }
 

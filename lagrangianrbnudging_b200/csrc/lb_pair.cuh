@@ -87,7 +87,10 @@ constexpr size_t march_smem_bytes() {
 
 // One block's strip [x0, x0 + 32) and chunk of rows [ya, ya + Hc); smem:
 // march_smem_bytes<Real, R>() of shared memory; 32 (R + 1) threads
-template <typename Real, int R, typename Off>
+// PRE: software pipelining -- a thread pulls its phase-1 inputs of group
+// q + 1 right after the barrier of group q, so the loads are in flight while
+// it computes phase 2 of group q (the inputs live in registers meanwhile)
+template <typename Real, int R, bool PRE, typename Off>
 __device__ __forceinline__ void march_block(const LBView<Real>& V1, const LBView<Real>& V2, int x0, int ya, int Hc,
                                             unsigned char* smem) {
   static_assert(2 * R <= 32, "the halo warp takes 2R nodes");
@@ -117,68 +120,83 @@ __device__ __forceinline__ void march_block(const LBView<Real>& V1, const LBView
     else if (x >= nx) x -= nx;
     col_ok = lane < 2 * R;
   }
-  const int Q = (Hc + 2 + R - 1) / R;
-  for (int q = 0; q < Q; q++) {
-    {
-      const int ly = q * R + w, y = ya - 1 + ly;
-      if (col_ok && ly <= Hc + 1 && y >= ylo && y <= yhi) {
-        const int slot = ly % RING;
-        Real fs[NPOP], gs[NPOP];
-        Real Fy, r, u, v, t;
-        const Off o = (Off)(y < 0 ? 0 : (y >= ny ? ny - 1 : y)) * pitch + (Off)x;  // (ghost rows: no stores)
-        if (y < 0 || y >= ny) {
-          pull_ghost_row<Real, Off>(V1, y < 0, x, fs, gs, Fy);
-        } else {
-          pull_node<Real, LBRB_TWALL_DIRICHLET, Off, true>(V1, y, x, fs, gs);
-          dirichlet_walls(V1, y, gs);
-          Fy = V1.Fin[o];
-        }
-        Real* Sc = S + slot * CW + c;
-        const long long nsum = pair_nudge_sum(V1, y, x, (size_t)o);
-        const double nsv = (double)nsum * (1.0 / FIX_SCALE);
-        lb_collide<Real, false>(
-            V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { Sc[k * PL] = val; },
-            [&](int k, Real val) {
-              if (nsum != 0) val = val + nudge_increment<Real>(k, nsv);
-              Sc[(NPOP + k) * PL] = val;
-            });
-        if (warp < R && ly >= 1 && ly <= Hc) {  // a node of this block's strip and chunk
-          SF[slot * 32 + lane] = Fy;
-          if (V1.write_F) V1.Fout[o] = Fy;
-          if (V1.write_uv) {
-            V1.u[o] = u;
-            V1.v[o] = v;
-          }
-          if (V1.write_rt & 1) V1.T[o] = t;
-          if (V1.write_rt & 2) V1.rho[o] = r;
-        }
-      }
+  // phase-1 inputs of this thread's node in group q: the pulled populations
+  // (walls applied), the step's buoyancy, the nudging sum of a nudged run
+  Real fs[NPOP], gs[NPOP], Fy = Real(0);
+  long long nsum = 0;
+  bool on = false;
+  int y1 = 0, slot = 0;
+  Off o1 = 0;
+  auto fetch = [&](int q) {
+    const int ly = q * R + w;
+    y1 = ya - 1 + ly;
+    on = col_ok && ly <= Hc + 1 && y1 >= ylo && y1 <= yhi;
+    if (!on) return;
+    slot = ly % RING;
+    o1 = (Off)(y1 < 0 ? 0 : (y1 >= ny ? ny - 1 : y1)) * pitch + (Off)x;  // (ghost rows: no stores)
+    if (y1 < 0 || y1 >= ny) {
+      pull_ghost_row<Real, Off>(V1, y1 < 0, x, fs, gs, Fy);
+    } else {
+      pull_node<Real, LBRB_TWALL_DIRICHLET, Off, true>(V1, y1, x, fs, gs);
+      dirichlet_walls(V1, y1, gs);
+      Fy = V1.Fin[o1];
     }
+    nsum = pair_nudge_sum(V1, y1, x, (size_t)o1);
+  };
+  // phase 1 from the fetched inputs: collide into the ring; the chunk's own
+  // nodes of the strip also store their moments and keep F^{n+1}
+  auto collide = [&]() {
+    if (!on) return;
+    Real r, u, v, t;
+    Real* Sc = S + slot * CW + c;
+    const double nsv = (double)nsum * (1.0 / FIX_SCALE);
+    lb_collide<Real, false>(
+        V1, (size_t)o1, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { Sc[k * PL] = val; },
+        [&](int k, Real val) {
+          if (nsum != 0) val = val + nudge_increment<Real>(k, nsv);
+          Sc[(NPOP + k) * PL] = val;
+        });
+    if (warp < R && y1 >= ya && y1 < ya + Hc) {  // a node of this block's strip and chunk
+      SF[slot * 32 + lane] = Fy;
+      if (V1.write_F) V1.Fout[o1] = Fy;
+      if (V1.write_uv) {
+        V1.u[o1] = u;
+        V1.v[o1] = v;
+      }
+      if (V1.write_rt & 1) V1.T[o1] = t;
+      if (V1.write_rt & 2) V1.rho[o1] = r;
+    }
+  };
+  const int Q = (Hc + 2 + R - 1) / R;
+  if (PRE) fetch(0);
+  for (int q = 0; q < Q; q++) {
+    if (!PRE) fetch(q);
+    collide();
     __syncthreads();
+    if (PRE && q + 1 < Q) fetch(q + 1);
     if (warp < R) {
       const int ly = q * R - 1 + w, y = ya - 1 + ly;
       if (lane < ncols && ly >= 1 && ly <= Hc) {
         const int s0 = ly % RING, sm = (ly - 1) % RING, sp = (ly + 1) % RING;
-        Real fs[NPOP], gs[NPOP];
+        Real f2[NPOP], g2[NPOP];
         static_for<NPOP>([&](auto kc) {
           constexpr int k = decltype(kc)::value;
           const int js = y - icy(k);
           if ((js < 0 && !glo) || (js >= ny && !ghi)) {
-            fs[k] = S[opp(k) * PL + s0 * CW + lane + 1];
-            gs[k] = Real(0);
+            f2[k] = S[opp(k) * PL + s0 * CW + lane + 1];
+            g2[k] = Real(0);
           } else {
             const int sl = icy(k) == 1 ? sm : (icy(k) == -1 ? sp : s0);
             const int cc = lane + 1 - icx(k);
-            fs[k] = S[k * PL + sl * CW + cc];
-            gs[k] = S[(NPOP + k) * PL + sl * CW + cc];
+            f2[k] = S[k * PL + sl * CW + cc];
+            g2[k] = S[(NPOP + k) * PL + sl * CW + cc];
           }
         });
-        dirichlet_walls(V2, y, gs);
-        lb_finish_node<Real, false, Off>(V2, (Off)y * pitch + (Off)(x0 + lane), fs, gs, SF[s0 * 32 + lane]);
+        dirichlet_walls(V2, y, g2);
+        lb_finish_node<Real, false, Off>(V2, (Off)y * pitch + (Off)(x0 + lane), f2, g2, SF[s0 * 32 + lane]);
       }
     }
   }
 }
-
 
 }  // namespace lbrb
