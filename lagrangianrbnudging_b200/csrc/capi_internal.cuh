@@ -215,6 +215,10 @@ inline LBView<Real> make_view(lbrb_t* h, int src, int dst, int uvslot, int write
   V.Tup = h->p.Tup;
   V.Tdown = h->p.Tdown;
   V.T0 = T0_of(h);
+  V.omega_f = (float)V.omega;
+  V.omegag_f = (float)V.omegag;
+  V.neg_gravity_f = (float)V.neg_gravity;
+  V.T0_f = (float)V.T0;
   V.nudge_vol = h->nudge_vol;
   V.tempreadint = h->tempreadint;
   V.nud_term = h->nud_term;

@@ -117,8 +117,12 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
       Fy = V1.Fin[o];
     }
     // (nudged run: step n's sums join g after the collision, as the apply pass does)
-    const long long nsum = pair_nudge_sum(V1, jg, xg, (size_t)o);
-    const double nsv = (double)nsum * (1.0 / FIX_SCALE);
+    long long nsum = 0;
+    double nsv = 0.0;
+    if (V1.nmask) {
+      nsum = pair_nudge_sum(V1, jg, xg, (size_t)o);
+      if (nsum != 0) nsv = (double)nsum * (1.0 / FIX_SCALE);
+    }
     lb_collide<Real, false>(
         V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { S[(k * RY + ly) * RX + lx] = val; },
         [&](int k, Real val) {

@@ -119,15 +119,15 @@ __device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, fl
 #pragma unroll
   for (int k = 0; k < NPOP; k++) dT += dg[k];
   const float r = 1.f + dr;
-  const float T0 = (float)V.T0;
+  const float T0 = V.T0_f;
   const float t = T0 + dT;
   const float jx = (df[1] - df[3]) + (df[5] - df[6]) + (df[8] - df[7]);
   const float jy = (df[2] - df[4]) + (df[5] - df[7]) + (df[6] - df[8]);
   const float Fy = Fy_io;
-  const float rinv = 1.f / r;
+  const float rinv = __frcp_rn(r);  // (the correctly rounded 1 / r)
   const float u = jx * rinv;
   const float v = fmaf(0.5f, Fy, jy) * rinv;
-  const float om = (float)V.omega, omg = (float)V.omegag;
+  const float om = V.omega_f, omg = V.omegag_f;
   const float srcFy = (1.f - 0.5f * om) * Fy;
   const float usq15 = 1.5f * fmaf(u, u, v * v);
   const float v3 = 3.f * v;
@@ -147,7 +147,7 @@ __device__ __forceinline__ void node_shift(const LBView<float>& V, float* df, fl
     const float dgeq = w * fmaf(t, P, dT);
     dg[k] = fmaf(omg, dgeq - dg[k], dg[k]);
   });
-  Fy_io = (float)V.neg_gravity * r * t;
+  Fy_io = V.neg_gravity_f * r * t;
   r_out = r;
   u_out = u;
   v_out = v;

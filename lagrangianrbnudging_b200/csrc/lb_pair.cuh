@@ -141,7 +141,7 @@ __device__ __forceinline__ void march_block(const LBView<Real>& V1, const LBView
       dirichlet_walls(V1, y1, gs);
       Fy = V1.Fin[o1];
     }
-    nsum = pair_nudge_sum(V1, y1, x, (size_t)o1);
+    if (V1.nmask) nsum = pair_nudge_sum(V1, y1, x, (size_t)o1);
   };
   // phase 1 from the fetched inputs: collide into the ring; the chunk's own
   // nodes of the strip also store their moments and keep F^{n+1}
@@ -149,7 +149,8 @@ __device__ __forceinline__ void march_block(const LBView<Real>& V1, const LBView
     if (!on) return;
     Real r, u, v, t;
     Real* Sc = S + slot * CW + c;
-    const double nsv = (double)nsum * (1.0 / FIX_SCALE);
+    double nsv = 0.0;
+    if (V1.nmask && nsum != 0) nsv = (double)nsum * (1.0 / FIX_SCALE);
     lb_collide<Real, false>(
         V1, (size_t)o1, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { Sc[k * PL] = val; },
         [&](int k, Real val) {

@@ -200,6 +200,9 @@ struct LBView {
   double omega, omegag;    // 1/relax, 1/relaxg
   double neg_gravity;      // -gravity
   double Tup, Tdown, T0;
+  // the same constants rounded to FP32 on the host, for the FP32 collision
+  // (the values (float)omega etc. would give, without a conversion per node)
+  float omega_f, omegag_f, neg_gravity_f, T0_f;
   // reference box nudging
   const int* __restrict__ nudge_vol;
   const double* __restrict__ tempreadint;

@@ -124,7 +124,7 @@ __device__ __forceinline__ void obs_pre_one(const LBView<Real>& V, double xx, do
       float dT = 0.f;
 #pragma unroll
       for (int k = 0; k < NPOP; k++) dT += gs[k];
-      return (float)V.T0 + dT;
+      return V.T0_f + dT;
     }
   };
   obs_scatter_rows(Tat, nx, ny, V.pitch, xx, yy, Tobs, alpha, acc, dflags, 0, ny);
