@@ -219,13 +219,7 @@ inline LBView<Real> make_view(lbrb_t* h, int src, int dst, int uvslot, int write
   V.omegag_f = (float)V.omegag;
   V.neg_gravity_f = (float)V.neg_gravity;
   V.T0_f = (float)V.T0;
-  V.om1_f = 1.f - V.omega_f;
-  V.omg1_f = 1.f - V.omegag_f;
-  for (int c = 0; c < 3; c++) {
-    const float w = (float)w_of(c == 0 ? 0 : (c == 1 ? 1 : 5));
-    V.omw_f[c] = V.omega_f * w;
-    V.omgw_f[c] = V.omegag_f * w;
-  }
+
   V.nudge_vol = h->nudge_vol;
   V.tempreadint = h->tempreadint;
   V.nud_term = h->nud_term;

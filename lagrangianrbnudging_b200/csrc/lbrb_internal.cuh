@@ -203,9 +203,6 @@ struct LBView {
   // the same constants rounded to FP32 on the host, for the FP32 collision
   // (the values (float)omega etc. would give, without a conversion per node)
   float omega_f, omegag_f, neg_gravity_f, T0_f;
-  // FP32 collision factors: 1 - omega, 1 - omegag, and omega w_k, omegag w_k
-  // for the three weight classes (rest, axis, diagonal)
-  float om1_f, omg1_f, omw_f[3], omgw_f[3];
   // reference box nudging
   const int* __restrict__ nudge_vol;
   const double* __restrict__ tempreadint;
