@@ -378,11 +378,12 @@ LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, c
  * lbrb_init_conduction on a slab gives the whole domain's profile and noise
  * at its rows; lbrb_nusselt gives the slab's mean of v T at the whole
  * domain's height (the domain's Nu is the slabs' values weighted by ny).
- * Supported: Dirichlet walls; particles; bilinear nudging (not box
- * nudging).  Every slab of the domain holds all particles and all
- * observations (lbrb_particles_set / lbrb_nudge_obs on each, in the whole
- * domain's coordinates) and lbrb_slab_step moves and applies them; a slab
- * with particles or nudging steps only through lbrb_slab_step. */
+ * Supported: Dirichlet walls; particles (held by their owner slab, below);
+ * bilinear nudging (not box nudging): every slab holds all observations
+ * (lbrb_nudge_obs on each, in the whole domain's coordinates) and
+ * lbrb_slab_step applies them; a slab with nudging steps only through
+ * lbrb_slab_step.  Create slab handles with nprtcl = 0 (lbrb_slab_set
+ * rejects a handle with whole-domain particles). */
 LBRB_API int lbrb_slab_set(lbrb_t *h, int j0, int ny_total);
 /* bytes of one packed boundary row set: 6 rows (f then g) of nx values */
 LBRB_API size_t lbrb_slab_ghost_bytes(const lbrb_t *h);
@@ -418,15 +419,10 @@ LBRB_API int lbrb_slab_pack2(lbrb_t *h);
  * a slab's lbrb_set_pairs(h, 0) turns it off): the exchange is then two rows
  * deep and goes every two steps; results are the same bit for bit.
  * The moments (rho, u, v, T) are written on the last of the nsteps.
- * With particles (the reference advances each rank's own particles,
- * propagate_prtcl at Trajectories/code/mympi2.h:350, and hands those that
- * leave its rows to the neighbour rank, toggle_prtcl at mympi2.h:568-760):
- * after every slab's step, the slab whose
- * rows hold a particle's cell advances it, reading the fields of the other
- * slabs through peer access (their GPUs must allow it); every slab then
- * copies in the particles it did not advance, and slab 0 their records, so
- * each slab's particle array and slab 0's record ring are the whole
- * domain's, bit for bit.  Drain the records from slab 0.
+ * With particles (lbrb_slab_particles_set on every slab): after every
+ * slab's step, the particle exchange below, its messages copied between the
+ * slabs around the ring (peer copies across GPUs); each slab keeps its own
+ * particles and records (lbrb_slab_particles_get, lbrb_slab_record_drain).
  * With bilinear nudging, after every slab's step each slab scatters the
  * innovations of the observations to the cell corners in its own rows
  * (order-free fixed-point sums, so g is the whole domain's bit for bit). */
@@ -434,6 +430,65 @@ LBRB_API int lbrb_slab_pack2(lbrb_t *h);
  * the steps (a full record ring is checked first, so it is not one) leaves
  * the slabs possibly at different steps: set their state again. */
 LBRB_API int lbrb_slab_step(lbrb_t *const *slabs, int nslabs, int nsteps);
+
+/* ---- particles of a y-slab, held by their owner slab ----------------------
+ * (no reference counterpart as an API; the reference's ranks keep the
+ * particles in their block, init_prtcl at Trajectories/code/mympi2.h:116-290,
+ * and hand those that leave it to the neighbour rank each step,
+ * toggle_prtcl at mympi2.h:568-760.)
+ * lbrb_slab_particles_set keeps, of the n particles given (the whole
+ * domain's, arguments as lbrb_particles_set), those whose cell lies in the
+ * slab's rows, in the order given.  capacity: particles the slab can hold
+ * (0: n); handoff_capacity: particles that may leave it per step and
+ * direction (0: min(capacity, 1024)).  A step of a slab with particles, one
+ * process per GPU (s+1 / s-1: the slabs above / below, around the ring:
+ * the top slab's "up" goes to slab 0 and slab 0's "down" to the top slab):
+ *   lbrb_slab_pack; send up -> s+1 ghost_lo, down -> s-1 ghost_hi;
+ *   lbrb_step(h, 1);
+ *   lbrb_slab_moments_pack; send mom_up -> s+1 mom_lo, mom_down -> s-1 mom_hi;
+ *   lbrb_slab_particles_step;
+ *   send hand_up -> s+1 hand_lo, hand_down -> s-1 hand_hi;
+ *   lbrb_slab_particles_recv.
+ * (The hand-off exchange may go with the next step's ghost exchange, with
+ * lbrb_slab_particles_recv before the next lbrb_step.)  Sizes are
+ * lbrb_slab_particle_bytes (mom_up, mom_down, and each hand-off list); all
+ * work and copies on the handle's stream, so a caller's NCCL send/recv on
+ * that stream orders itself.  The moment messages carry the fields one row
+ * below the slab and two above (u, v, T of the sender's top row; u, v,
+ * u^{n-1}, v^{n-1}, T of its row 0 and u, v, T of its row 1), which is all
+ * a particle stencil of the slab reads while no particle moves more than a
+ * row per step; a hand-off list carries the particles that left the slab's
+ * rows (their whole state, 80 bytes each).  Each message has a header with
+ * the sender's step and rows: a message from the wrong step or neighbour,
+ * a particle outside the slab's reach, or a full slab or list is reported
+ * by lbrb_sync (LBRB_ERR_STATE, LBRB_ERR_RANGE, LBRB_ERR_OVERFLOW).  Calls
+ * out of this order return LBRB_ERR_STATE.  A particle's state equals the
+ * whole domain's bit for bit; its record goes into the ring of the slab
+ * that advanced it. */
+LBRB_API int lbrb_slab_particles_set(lbrb_t *h, int n, const int *ids, const double *x, const double *y,
+                                     const double *u, const double *v, const int *ptype, const double *invtau,
+                                     int capacity, int handoff_capacity);
+LBRB_API int lbrb_slab_particle_bytes(const lbrb_t *h, size_t *mom_up, size_t *mom_down, size_t *handoff);
+LBRB_API int lbrb_slab_particle_buffers(lbrb_t *h, void **mom_up, void **mom_down, void **mom_lo, void **mom_hi,
+                                        void **hand_up, void **hand_down, void **hand_lo, void **hand_hi);
+LBRB_API int lbrb_slab_moments_pack(lbrb_t *h);
+LBRB_API int lbrb_slab_particles_step(lbrb_t *h);
+LBRB_API int lbrb_slab_particles_recv(lbrb_t *h);
+/* the slab's particle count and state (waits; arrays of at least max_n) */
+LBRB_API int lbrb_slab_particles_count(lbrb_t *h, int *n);
+LBRB_API int lbrb_slab_particles_get(lbrb_t *h, int max_n, int *n, int *ids, double *x, double *y, double *u,
+                                     double *v, double *xo, double *yo, double *uo, double *vo);
+/* Records of the particles the slab advanced, oldest first, one per call:
+ * step (-1 when none is pending), count, ids[count] and buf[field][count]
+ * (LBRB_REC_NBASIC or LBRB_REC_NFULL fields), arrays of at least max_n. */
+LBRB_API int lbrb_slab_record_pending(lbrb_t *h, int *count);
+LBRB_API int lbrb_slab_record_drain(lbrb_t *h, int max_n, int *step, int *count, int *ids, double *buf);
+/* byte layout of the messages (needs no device): header bytes of each
+ * message (int count, step, j0, j1, kind, 3 pad), bytes of a hand-off
+ * record (9 doubles x y u v xo yo uo vo invtau, int id, int type; after the
+ * header), offset of the first moment plane (planes of nx values, each
+ * mom plane stride = nx * element size rounded up to 256 bytes) */
+LBRB_API int lbrb_slab_particle_format(int *msg_header_bytes, int *record_bytes, int *mom_planes_offset);
 
 #ifdef __cplusplus
 }

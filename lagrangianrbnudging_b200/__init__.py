@@ -22,6 +22,7 @@ ERRORS = {
     -5: "LBRB_ERR_NONFINITE", -6: "LBRB_ERR_RANGE", -7: "LBRB_ERR_OVERFLOW", -8: "LBRB_ERR_IDS",
     -9: "LBRB_ERR_UNSUPPORTED",
 }
+ERR_CODES = {v: k for k, v in ERRORS.items()}
 PREC = {"fp64": 0, "fp32": 1}
 TWALL = {"dirichlet": 0, "adiabatic": 1}
 NUDGE = {"none": 0, "refbox": 1, "bilinear": 2}
@@ -47,6 +48,10 @@ EXPORTS = [
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
     "lbrb_slab_ghost2_bytes", "lbrb_slab_buffers2", "lbrb_slab_pack2",
+    "lbrb_slab_particles_set", "lbrb_slab_particle_bytes", "lbrb_slab_particle_buffers",
+    "lbrb_slab_moments_pack", "lbrb_slab_particles_step", "lbrb_slab_particles_recv",
+    "lbrb_slab_particles_count", "lbrb_slab_particles_get", "lbrb_slab_record_pending",
+    "lbrb_slab_record_drain", "lbrb_slab_particle_format",
     "lbrb_set_graph", "lbrb_set_pairs", "lbrb_set_pair_shape", "lbrb_get_pair_shape", "lbrb_pair_shapes",
 ]
 
@@ -142,6 +147,18 @@ def lib() -> C.CDLL:
         "lbrb_slab_buffers2": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
         "lbrb_slab_pack2": (C.c_int, [vp]),
         "lbrb_slab_step": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int]),
+        "lbrb_slab_particles_set": (C.c_int, [vp, C.c_int, ip, dp, dp, dp, dp, ip, dp, C.c_int, C.c_int]),
+        "lbrb_slab_particle_bytes": (C.c_int, [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                               C.POINTER(C.c_size_t)]),
+        "lbrb_slab_particle_buffers": (C.c_int, [vp] + [C.POINTER(vp)] * 8),
+        "lbrb_slab_moments_pack": (C.c_int, [vp]),
+        "lbrb_slab_particles_step": (C.c_int, [vp]),
+        "lbrb_slab_particles_recv": (C.c_int, [vp]),
+        "lbrb_slab_particles_count": (C.c_int, [vp, ip]),
+        "lbrb_slab_particles_get": (C.c_int, [vp, C.c_int, ip, ip] + [dp] * 8),
+        "lbrb_slab_record_pending": (C.c_int, [vp, ip]),
+        "lbrb_slab_record_drain": (C.c_int, [vp, C.c_int, ip, ip, ip, dp]),
+        "lbrb_slab_particle_format": (C.c_int, [ip, ip, ip]),
         "lbrb_set_graph": (C.c_int, [vp, C.c_int]),
         "lbrb_set_pairs": (C.c_int, [vp, C.c_int]),
         "lbrb_set_pair_shape": (C.c_int, [vp, C.c_int]),
@@ -375,6 +392,87 @@ class Run:
                                            C.byref(J), _dp(g)))
         return (J.value, g) if gradient else J.value
 
+    # ---- y-slab of a larger domain (lbrb_slab_*)
+    def slab_set(self, j0: int, ny_total: int):
+        self._ck(lib().lbrb_slab_set(self.h, int(j0), int(ny_total)))
+        self.j0, self.ny_total = int(j0), int(ny_total)
+
+    def slab_pack(self):
+        self._ck(lib().lbrb_slab_pack(self.h))
+
+    def slab_pack2(self):
+        self._ck(lib().lbrb_slab_pack2(self.h))
+
+    def slab_buffers(self, two: bool = False):
+        """device pointers (up, down, ghost_lo, ghost_hi) of the ghost-row
+        exchange (two: the two-row blocks of lbrb_slab_pack2), and its bytes"""
+        b = [C.c_void_p() for _ in range(4)]
+        fn = lib().lbrb_slab_buffers2 if two else lib().lbrb_slab_buffers
+        self._ck(fn(self.h, *[C.byref(x) for x in b]))
+        nbytes = (lib().lbrb_slab_ghost2_bytes if two else lib().lbrb_slab_ghost_bytes)(self.h)
+        return [x.value for x in b], int(nbytes)
+
+    def slab_particles_set(self, ids, x, y, u, v, ptype, invtau, capacity: int = 0, handoff_capacity: int = 0):
+        """keep, of the particles given (the whole domain's), those whose cell
+        lies in this slab's rows"""
+        ids, ptype = _i32(ids), _i32(ptype)
+        x, y, u, v, invtau = (_f64(a) for a in (x, y, u, v, invtau))
+        self._ck(lib().lbrb_slab_particles_set(self.h, len(ids), _ip(ids), _dp(x), _dp(y), _dp(u), _dp(v),
+                                               _ip(ptype), _dp(invtau), int(capacity), int(handoff_capacity)))
+
+    def slab_particle_buffers(self):
+        """{name: (device pointer, bytes)} of the particle messages: mom_up,
+        mom_down (sent), mom_lo, mom_hi (received), hand_up, hand_down,
+        hand_lo, hand_hi"""
+        sz = [C.c_size_t() for _ in range(3)]
+        self._ck(lib().lbrb_slab_particle_bytes(self.h, *[C.byref(x) for x in sz]))
+        b = [C.c_void_p() for _ in range(8)]
+        self._ck(lib().lbrb_slab_particle_buffers(self.h, *[C.byref(x) for x in b]))
+        names = ["mom_up", "mom_down", "mom_lo", "mom_hi", "hand_up", "hand_down", "hand_lo", "hand_hi"]
+        nbytes = [sz[0].value, sz[1].value, sz[0].value, sz[1].value] + [sz[2].value] * 4
+        return {k: (p.value, n) for k, p, n in zip(names, b, nbytes)}
+
+    def slab_moments_pack(self):
+        self._ck(lib().lbrb_slab_moments_pack(self.h))
+
+    def slab_particles_step(self):
+        self._ck(lib().lbrb_slab_particles_step(self.h))
+
+    def slab_particles_recv(self):
+        self._ck(lib().lbrb_slab_particles_recv(self.h))
+
+    def slab_particles_count(self) -> int:
+        n = C.c_int()
+        self._ck(lib().lbrb_slab_particles_count(self.h, C.byref(n)))
+        return n.value
+
+    def slab_particles_get(self):
+        cap = self.slab_particles_count()
+        ids = np.empty(cap, np.int32)
+        arrs = [np.empty(cap) for _ in range(8)]
+        n = C.c_int()
+        self._ck(lib().lbrb_slab_particles_get(self.h, cap, C.byref(n), _ip(ids), *[_dp(a) for a in arrs]))
+        k = n.value
+        return dict(id=ids[:k], **{f: a[:k] for f, a in zip(["x", "y", "u", "v", "xo", "yo", "uo", "vo"], arrs)})
+
+    def slab_record_pending(self) -> int:
+        c = C.c_int()
+        self._ck(lib().lbrb_slab_record_pending(self.h, C.byref(c)))
+        return c.value
+
+    def slab_record_drain(self, max_n: int):
+        """the oldest record of this slab: (step, ids[count], buf[field][count]),
+        or None when none is pending"""
+        ids = np.empty(max_n, np.int32)
+        buf = np.empty(self.nrec * max_n)
+        step, cnt = C.c_int(), C.c_int()
+        self._ck(lib().lbrb_slab_record_drain(self.h, int(max_n), C.byref(step), C.byref(cnt), _ip(ids),
+                                              _dp(buf)))
+        if step.value < 0:
+            return None
+        k = cnt.value
+        return step.value, ids[:k].copy(), buf[: self.nrec * k].reshape(self.nrec, k).copy()
+
     # ---- streams and timing
     def set_stream(self, stream_handle: int | None):
         self._ck(lib().lbrb_set_stream(self.h, C.c_void_p(stream_handle or 0)))
@@ -443,7 +541,10 @@ class SlabDomain:
 
     heights: rows per slab, bottom to top; devices: one CUDA device per slab
     (default: all on `device`); params as for Run, with ny the whole
-    domain's rows (each slab gets its own height)."""
+    domain's rows (each slab gets its own height) and nprtcl the whole
+    domain's particles: each slab holds those in its rows
+    (lbrb_slab_particles_set); particles and records come back merged, in
+    the order the particles were set."""
 
     def __init__(self, heights, devices=None, **params):
         ny_total = int(params["ny"])
@@ -455,13 +556,16 @@ class SlabDomain:
             raise ValueError("one device per slab")
         self.nx, self.ny = int(params["nx"]), ny_total
         self.heights = heights
+        self.np = int(params.get("nprtcl", 0))
+        self.nrec = 17 if params.get("record_full") else 9
+        self._order = None
         self.slabs = []
         j0 = 0
         try:
             for hgt, dev in zip(heights, devices):
-                r = Run(**dict(params, ny=hgt, device=dev))
+                r = Run(**dict(params, ny=hgt, device=dev, nprtcl=0))
                 self.slabs.append(r)
-                r._ck(lib().lbrb_slab_set(r.h, j0, ny_total))
+                r.slab_set(j0, ny_total)
                 j0 += hgt
         except Exception:
             self.close()
@@ -518,27 +622,78 @@ class SlabDomain:
         """the slabs' values weighted by their heights"""
         return float(sum(hgt * r.nusselt() for r, hgt in zip(self.slabs, self.heights)) / self.ny)
 
-    # ---- particles: every slab holds all of them (the slab that holds a
-    # particle's cell advances it each step); slab 0 keeps the records
+    # ---- particles: each slab holds those whose cell lies in its rows
     @property
     def istep(self) -> int:
         return self.slabs[0].istep
 
-    def set_particles(self, ids, x, y, u, v, ptype, invtau):
+    def set_particles(self, ids, x, y, u, v, ptype, invtau, capacity: int = 0, handoff_capacity: int = 0):
+        """the whole domain's particles (ids unique); capacity and
+        handoff_capacity per slab as lbrb_slab_particles_set takes them"""
+        ids = _i32(ids)
+        if len(ids) != self.np or len(np.unique(ids)) != len(ids):
+            raise ValueError("nprtcl particles with unique ids required")
         for r in self.slabs:
-            r.set_particles(ids, x, y, u, v, ptype, invtau)
+            r.slab_particles_set(ids, x, y, u, v, ptype, invtau, capacity, handoff_capacity)
+        self._order = ids.copy()
+        self._sorter = np.argsort(ids, kind="stable")
+
+    def _place(self, ids):
+        """positions of `ids` in the order the particles were set (each once)"""
+        srt = self._order[self._sorter]
+        k = np.searchsorted(srt, ids)
+        if len(ids) != self.np or np.any(k >= self.np) or np.any(srt[np.minimum(k, self.np - 1)] != ids):
+            raise RuntimeError("slab particles do not cover the domain's particles")
+        pos = self._sorter[k]
+        if len(np.unique(pos)) != self.np:
+            raise RuntimeError("a particle is held by two slabs")
+        return pos
 
     def get_particles(self):
-        return self.slabs[0].get_particles()
+        parts = [r.slab_particles_get() for r in self.slabs]
+        pos = self._place(np.concatenate([p["id"] for p in parts]))
+        out = {"id": self._order.copy()}
+        for k in ("x", "y", "u", "v", "xo", "yo", "uo", "vo"):
+            a = np.empty(self.np)
+            a[pos] = np.concatenate([p[k] for p in parts])
+            out[k] = a
+        return out
+
+    def slab_counts(self):
+        return [r.slab_particles_count() for r in self.slabs]
 
     def pending_records(self) -> int:
-        return self.slabs[0].pending_records()
+        return min(r.slab_record_pending() for r in self.slabs)
+
+    def drain_records_array(self, max_records: int | None = None):
+        """The pending records (all, or the oldest max_records) as (steps[k],
+        buf[k][field][nprtcl]), particles in the order they were set (each
+        slab's part of a step's record placed by id)"""
+        k = self.pending_records()
+        if max_records is not None:
+            k = min(k, int(max_records))
+        steps = np.empty(k, np.int32)
+        buf = np.empty((k, self.nrec, self.np))
+        for q in range(k):
+            recs = [r.slab_record_drain(self.np) for r in self.slabs]
+            st = {rec[0] for rec in recs}
+            if len(st) != 1:
+                raise RuntimeError("slab records of different steps")
+            steps[q] = st.pop()
+            pos = self._place(np.concatenate([rec[1] for rec in recs]))
+            buf[q][:, pos] = np.concatenate([rec[2] for rec in recs], axis=1)
+        return steps, buf
 
     def drain_records(self, max_records: int | None = None):
-        return self.slabs[0].drain_records(max_records)
-
-    def drain_records_array(self):
-        return self.slabs[0].drain_records_array()
+        """{step: {field: array}} as Run.drain_records gives it"""
+        steps, buf = self.drain_records_array(max_records)
+        out = {}
+        for q in range(len(steps)):
+            d = {"id": self._order.copy()}
+            for f in range(self.nrec):
+                d[REC_NAMES[f]] = buf[q, f].copy()
+            out[int(steps[q])] = d
+        return out
 
     def check_finite(self):
         for r in self.slabs:

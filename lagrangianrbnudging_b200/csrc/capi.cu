@@ -55,8 +55,11 @@ struct TuneVal {
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneVal> g_tuned_single, g_tuned_pair;
+// the steps store u, v every step (and T on record steps) for particles:
+// the whole domain's, or a slab's own (lbrb_slab_particles_set)
+static bool moves_particles(const lbrb_t* h) { return h->np > 0 || h->sp != nullptr; }
 static TuneKey tune_key(const lbrb_t* h) {
-  return {h->dev, h->p.nx, h->p.ny, h->pitch, (int)h->esize, h->p.twall, h->p.nudge, h->np > 0 ? 1 : 0,
+  return {h->dev, h->p.nx, h->p.ny, h->pitch, (int)h->esize, h->p.twall, h->p.nudge, moves_particles(h) ? 1 : 0,
           (h->slab_gh2_lo ? 1 : 0) | (h->slab_gh2_hi ? 2 : 0) | (h->slab ? 4 : 0)};
 }
 static bool tuned_get(std::map<TuneKey, TuneVal>& m, const lbrb_t* h, int* shape, float* ms) {
@@ -223,6 +226,25 @@ void lbrb_params_default(lbrb_params* p) {
 
 const char* lbrb_last_error(const lbrb_t* h) { return h ? h->err.c_str() : "null handle"; }
 
+static void free_sp(SlabParts* S) {
+  if (!S) return;
+  auto F = [](void* q) { if (q) cudaFree(q); };
+  for (int b = 0; b < 2; b++) {
+    F(S->P[b]); F(S->id[b]); F(S->type[b]);
+  }
+  F(S->cnt); F(S->cls); F(S->bcnt); F(S->rows); F(S->zrow); F(S->d_rec); F(S->d_rid); F(S->d_rcnt);
+  for (void* q : S->mom) F(q);
+  for (void* q : S->hand) F(q);
+  if (S->h_rec) cudaFreeHost(S->h_rec);
+  if (S->h_rid) cudaFreeHost(S->h_rid);
+  if (S->h_rcnt) cudaFreeHost(S->h_rcnt);
+  for (cudaEvent_t e : S->rev)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : {S->ev_mom, S->ev_part, S->ev_hand})
+    if (e) cudaEventDestroy(e);
+  delete S;
+}
+
 static void free_all(lbrb_t* h) {
   auto F = [](void* q) { if (q) cudaFree(q); };
   F(h->pops[0]); F(h->pops[1]); F(h->F[0]); F(h->F[1]);
@@ -240,13 +262,14 @@ static void free_all(lbrb_t* h) {
   delete[] h->h_chk; delete[] h->h_oid;
   F(h->obs); F(h->acc); F(h->acc2); F(h->nmask); F(h->staging); F(h->big); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
-  F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down); F(h->slab_own); F(h->slab_tab);
+  F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down); F(h->slab_tab);
+  free_sp(h->sp);
+  h->sp = nullptr;
   F(h->slab_gh2_lo); F(h->slab_gh2_hi); F(h->slab_up2); F(h->slab_down2);
   for (cudaGraphExec_t& g : h->graph_exec)
     if (g) cudaGraphExecDestroy(g);
   if (h->slab_ev_xfer) cudaEventDestroy(h->slab_ev_xfer);
   if (h->slab_ev_done) cudaEventDestroy(h->slab_ev_done);
-  if (h->slab_ev_part) cudaEventDestroy(h->slab_ev_part);
   delete[] h->adj_steps;
   if (h->h_flags) cudaFreeHost(h->h_flags);
   if (h->h_scalar) cudaFreeHost(h->h_scalar);
@@ -729,7 +752,7 @@ int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
   if (n == 0) return LBRB_OK;
-  if (h->slab && !h->slab_stepping && n == 2 && h->np == 0 && h->p.nudge == LBRB_NUDGE_NONE &&
+  if (h->slab && !h->slab_stepping && n == 2 && !moves_particles(h) && h->p.nudge == LBRB_NUDGE_NONE &&
       h->p.twall == LBRB_TWALL_DIRICHLET && h->pair_mode != 0) {
     // one process per GPU: two steps from the two-row ghost blocks
     // (lbrb_slab_pack2 and the exchange of lbrb_slab_buffers2 done)
@@ -747,9 +770,13 @@ int lbrb_step(lbrb_t* h, int n) {
     h->prev_valid = false;
     return LBRB_OK;
   }
-  if (h->slab && (n != 1 || ((h->np > 0 || h->p.nudge != LBRB_NUDGE_NONE) && !h->slab_stepping)))
+  if (h->slab && (n != 1 || (h->p.nudge != LBRB_NUDGE_NONE && !h->slab_stepping)))
     return fail(h, LBRB_ERR_ARG,
                 "step: a y-slab takes one step per boundary exchange, or two after lbrb_slab_pack2 (lbrb_slab_step)");
+  if (h->sp && !h->slab_stepping && (h->sp->part_step != h->istep || h->sp->recv_step != h->istep))
+    return fail(h, LBRB_ERR_STATE,
+                "step: a slab with particles steps after lbrb_slab_particles_step and lbrb_slab_particles_recv "
+                "of its last step");
   if (!h->moments_valid)
     return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
   if (h->np > 0 && !h->particles_set) return fail(h, LBRB_ERR_STATE, "step: particles not set");
@@ -767,9 +794,10 @@ int lbrb_step(lbrb_t* h, int n) {
     if (h->p.autotune && !refbox && !tuned_get(g_tuned_single, h, &sh, &ms)) {
       // trials store u, v as the steps will (particles need them every step),
       // into the slot the first step overwrites
-      const int tuv = h->np > 0 ? 3 - h->uvcur - h->uvprev : h->uvcur;
-      if (f32) sh = tune_lb_fp32(make_view<float>(h, h->cur, h->cur ^ 1, tuv, h->np > 0, 0), h->p.twall, h->stream, &ms);
-      else sh = tune_lb_fp64(make_view<double>(h, h->cur, h->cur ^ 1, tuv, h->np > 0, 0), h->p.twall, h->stream, &ms);
+      const bool mp = moves_particles(h);
+      const int tuv = mp ? 3 - h->uvcur - h->uvprev : h->uvcur;
+      if (f32) sh = tune_lb_fp32(make_view<float>(h, h->cur, h->cur ^ 1, tuv, mp, 0), h->p.twall, h->stream, &ms);
+      else sh = tune_lb_fp64(make_view<double>(h, h->cur, h->cur ^ 1, tuv, mp, 0), h->p.twall, h->stream, &ms);
       CK(h, cudaGetLastError());
       tuned_put(g_tuned_single, h, sh, ms);
     }
@@ -825,9 +853,11 @@ int lbrb_step(lbrb_t* h, int n) {
       tmark_end(h, tm, h->stream);
       if (istep % nt == 1) h->nudge_file_loaded = false;
     }
-    const int write_uv = (h->np > 0) || last;
-    // T for the records and the nudging scatter; rho only for the call's end
-    const int write_rt = last ? 3 : ((rec || h->p.nudge == LBRB_NUDGE_BILINEAR) ? 1 : 0);
+    const int write_uv = moves_particles(h) || last;
+    // T for the records (a slab's own too) and the nudging scatter; rho only
+    // for the call's end
+    const bool rec_own = h->sp && h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
+    const int write_rt = last ? 3 : ((rec || rec_own || h->p.nudge == LBRB_NUDGE_BILINEAR) ? 1 : 0);
     const int src = h->cur, dst = h->cur ^ 1;
     const int uvn = write_uv ? 3 - h->uvcur - h->uvprev : h->uvcur;
     {
@@ -1466,7 +1496,12 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
     return fail(h, LBRB_ERR_ARG, "slab_set: rows [j0, j0 + ny) must lie in [0, ny_total)");
   if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge == LBRB_NUDGE_REFBOX)
     return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls, no box nudging");
+  if (h->np > 0)
+    return fail(h, LBRB_ERR_UNSUPPORTED,
+                "slab_set: a slab's particles are set by lbrb_slab_particles_set (create it with nprtcl = 0)");
   CK(h, cudaSetDevice(h->dev));
+  free_sp(h->sp);  // (its rows change)
+  h->sp = nullptr;
   const size_t gb = lbrb_slab_ghost_bytes(h);
   const size_t gb2 = (size_t)SLAB_GH2_PLANES * h->p.nx * h->esize;
   void** bufs[] = {&h->slab_ghost_lo, &h->slab_ghost_hi, &h->slab_up, &h->slab_down,
@@ -1489,10 +1524,6 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
     if (b) CK(h, cudaMemsetAsync(b, 0, gb2, h->stream));
   if (!h->slab_ev_xfer) CK(h, cudaEventCreateWithFlags(&h->slab_ev_xfer, cudaEventDisableTiming));
   if (!h->slab_ev_done) CK(h, cudaEventCreateWithFlags(&h->slab_ev_done, cudaEventDisableTiming));
-  if (h->np > 0) {
-    if (!h->slab_own && dalloc(&h->slab_own, h->np)) return fail(h, LBRB_ERR_NOMEM, "slab particle owners");
-    if (!h->slab_ev_part) CK(h, cudaEventCreateWithFlags(&h->slab_ev_part, cudaEventDisableTiming));
-  }
   h->slab_sig.clear();  // (tables rebuilt on the next slab step)
   CK(h, cudaStreamSynchronize(h->stream));
   h->slab = true;
@@ -1545,12 +1576,320 @@ int lbrb_slab_pack(lbrb_t* h) {
   return LBRB_OK;
 }
 
+// ------------------------------------------------- owner-slab particles
+// The particles of a y-slab held by the slab whose rows hold their cell, as
+// the reference's ranks hold them (init_prtcl keeps a rank's particles,
+// Trajectories/code/mympi2.h:116-290; toggle_prtcl hands the leavers to the
+// neighbour, :568-760).  Per step, after the slab's lbrb_step(h, 1):
+// lbrb_slab_moments_pack, the exchange of the moment messages,
+// lbrb_slab_particles_step, the exchange of the hand-off lists and
+// lbrb_slab_particles_recv (own_*_kernel, particle_kernels.cu).
+
+// the cell row of a position as the device computes it (cell_row)
+static int host_cell_row(double yy, int ny) {
+  if (!(yy > -2.0 && yy < ny + 2.0)) return 0;
+  int r = ((int)yy - 1) % ny;
+  return r < 0 ? r + ny : r;
+}
+
+// the 14 field tables of the particle kernels: for every row of the domain,
+// the row in this slab's planes, in a received moment message (one row below
+// the slab, two above, periodic in y) or the zero row
+static std::vector<const void*> own_tables(const lbrb_t* h) {
+  const SlabParts& S = *h->sp;
+  const int nyT = h->slab_ny_total, j0 = h->slab_j0, nyl = h->p.ny;
+  const size_t rowb = (size_t)h->pitch * h->esize;
+  auto mplane = [&](int which, int q) -> const void* {
+    return (const char*)S.mom[which] + MOM_PLANES_OFF + (size_t)q * S.mom_pstride;
+  };
+  // per role (u, v, u^{n-1}, v^{n-1}, T): the planes of the lo message and of
+  // the hi message's two rows (-1: not sent, the zero row)
+  const int lo_q[5] = {0, 1, -1, -1, 2}, hi0_q[5] = {0, 1, 2, 3, 4}, hi1_q[5] = {5, 6, -1, -1, 7};
+  std::vector<const void*> t((size_t)OWN_TABLES * nyT, S.zrow);
+  for (int j = 0; j < nyT; j++) {
+    const int d = ((j - j0) % nyT + nyT) % nyT;
+    const bool below = j == ((j0 - 1) % nyT + nyT) % nyT;
+    for (int tab = 0; tab < OWN_TABLES; tab++) {
+      const int role = tab < 3 ? 0 : tab < 6 ? 1 : tab < 9 ? 2 : tab < 12 ? 3 : 4;
+      const void* own = role == 4 ? h->T[tab - 12] : h->uv[tab % 3][role & 1];
+      const void* r = S.zrow;
+      if (d < nyl) r = (const char*)own + (size_t)d * rowb;
+      else if (d == nyl) r = mplane(3, hi0_q[role]);
+      else if (below) r = lo_q[role] >= 0 ? mplane(2, lo_q[role]) : S.zrow;
+      else if (d == nyl + 1) r = hi1_q[role] >= 0 ? mplane(3, hi1_q[role]) : S.zrow;
+      t[(size_t)tab * nyT + j] = r;
+    }
+  }
+  return t;
+}
+
+int lbrb_slab_particle_format(int* msg_header_bytes, int* record_bytes, int* mom_planes_offset) {
+  if (msg_header_bytes) *msg_header_bytes = (int)sizeof(SlabMsg);
+  if (record_bytes) *record_bytes = (int)sizeof(HandoffRec);
+  if (mom_planes_offset) *mom_planes_offset = (int)MOM_PLANES_OFF;
+  return LBRB_OK;
+}
+
+int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, const double* y, const double* u,
+                            const double* v, const int* ptype, const double* invtau, int capacity,
+                            int handoff_capacity) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->slab) return fail(h, LBRB_ERR_STATE, "slab_particles_set: not a y-slab (lbrb_slab_set)");
+  if (n < 0 || (n > 0 && (!ids || !x || !y || !u || !v || !ptype || !invtau)) || capacity < 0 ||
+      handoff_capacity < 0)
+    return fail(h, LBRB_ERR_ARG, "slab_particles_set: bad arguments");
+  const int nyT = h->slab_ny_total, j0 = h->slab_j0, nyl = h->p.ny;
+  std::vector<int> keep;
+  for (int q = 0; q < n; q++) {
+    if (!(x[q] > -1.0 && x[q] < h->p.nx + 1.0 && y[q] >= 0.0 && y[q] <= nyT + 1.0))
+      return fail(h, LBRB_ERR_RANGE, "slab_particles_set: position outside the domain");
+    if (!(u[q] == u[q]) || !(v[q] == v[q]) || !(invtau[q] >= 0.0) ||
+        (ptype[q] != LBRB_PTYPE_TRACER && ptype[q] != LBRB_PTYPE_INERTIAL))
+      return fail(h, LBRB_ERR_ARG, "slab_particles_set: bad velocity, type or 1/tau");
+    const int cr = host_cell_row(y[q], nyT);
+    if (cr >= j0 && cr < j0 + nyl) keep.push_back(q);
+  }
+  long cap = capacity > 0 ? capacity : std::max(n, 1);
+  cap = (cap + 127) / 128 * 128;
+  if ((long)keep.size() > cap || cap > (1L << 28))
+    return fail(h, LBRB_ERR_ARG, "slab_particles_set: capacity below the slab's particles or too large");
+  const int xcap = handoff_capacity > 0 ? handoff_capacity : (int)std::min(cap, 1024L);
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaStreamSynchronize(h->stream));
+  free_sp(h->sp);
+  h->sp = new SlabParts();
+  SlabParts& S = *h->sp;
+  S.cap = (int)cap;
+  S.xcap = xcap;
+  const size_t C = (size_t)cap;
+  S.mom_pstride = ((size_t)h->p.nx * h->esize + 255) / 256 * 256;
+  S.mom_up_bytes = MOM_PLANES_OFF + MOM_UP_PLANES * S.mom_pstride;
+  S.mom_down_bytes = MOM_PLANES_OFF + MOM_DOWN_PLANES * S.mom_pstride;
+  S.hand_bytes = HAND_RECS_OFF + (size_t)xcap * sizeof(HandoffRec);
+  bool bad = false;
+  for (int b = 0; b < 2; b++)
+    bad = bad || dalloc(&S.P[b], 9 * C) || dalloc(&S.id[b], C) || dalloc(&S.type[b], C);
+  bad = bad || dalloc(&S.cnt, 2) || dalloc(&S.cls, C) || dalloc(&S.bcnt, 3 * (C / 128)) ||
+        cudaMalloc(&S.rows, (size_t)OWN_TABLES * nyT * sizeof(void*)) != cudaSuccess ||
+        cudaMalloc(&S.zrow, (size_t)h->pitch * h->esize) != cudaSuccess;
+  for (int m = 0; m < 4 && !bad; m++)
+    bad = cudaMalloc(&S.mom[m], (m & 1) ? S.mom_down_bytes : S.mom_up_bytes) != cudaSuccess ||
+          cudaMalloc(&S.hand[m], S.hand_bytes) != cudaSuccess;
+  const int slots = h->p.record_slots;
+  const int nrec = h->p.record_full ? LBRB_REC_NFULL : LBRB_REC_NBASIC;
+  if (!bad && h->p.noutconfig > 0) {
+    bad = dalloc(&S.d_rec, (size_t)slots * nrec * C) || dalloc(&S.d_rid, (size_t)slots * C) ||
+          dalloc(&S.d_rcnt, (size_t)slots) ||
+          cudaMallocHost(&S.h_rec, (size_t)slots * nrec * C * sizeof(double)) != cudaSuccess ||
+          cudaMallocHost(&S.h_rid, (size_t)slots * C * sizeof(int)) != cudaSuccess ||
+          cudaMallocHost(&S.h_rcnt, (size_t)slots * sizeof(int)) != cudaSuccess;
+    S.rstep.assign(slots, 0);
+    S.rev.assign(slots, nullptr);
+    for (int q = 0; q < slots && !bad; q++)
+      bad = cudaEventCreateWithFlags(&S.rev[q], cudaEventDisableTiming) != cudaSuccess;
+  }
+  for (cudaEvent_t* e : {&S.ev_mom, &S.ev_part, &S.ev_hand})
+    bad = bad || cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess;
+  if (bad) {
+    free_sp(h->sp);
+    h->sp = nullptr;
+    return fail(h, LBRB_ERR_NOMEM, "slab_particles_set: buffers");
+  }
+  h->nrec_fields = nrec;
+  CK(h, cudaMemsetAsync(S.zrow, 0, (size_t)h->pitch * h->esize, h->stream));
+  for (int m = 0; m < 4; m++) {
+    CK(h, cudaMemsetAsync(S.mom[m], 0, (m & 1) ? S.mom_down_bytes : S.mom_up_bytes, h->stream));
+    CK(h, cudaMemsetAsync(S.hand[m], 0, S.hand_bytes, h->stream));
+  }
+  CK(h, cudaMemsetAsync(S.cls, 3, C, h->stream));
+  // the kept particles, in the order given
+  const size_t k = keep.size();
+  std::vector<double> P(9 * C, 0.0);
+  std::vector<int> I(C, 0), T(C, 0);
+  for (size_t a = 0; a < k; a++) {
+    const int q = keep[a];
+    const double vals[9] = {x[q], y[q], u[q], v[q], x[q], y[q], u[q], v[q], invtau[q]};
+    for (int f = 0; f < 9; f++) P[(size_t)f * C + a] = vals[f];
+    I[a] = ids[q];
+    T[a] = ptype[q];
+  }
+  const int cnt[2] = {(int)k, (int)k};
+  const std::vector<const void*> tab = own_tables(h);
+  CK(h, cudaMemcpyAsync(S.P[0], P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(S.id[0], I.data(), C * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(S.type[0], T.data(), C * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(S.cnt, cnt, sizeof(cnt), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(S.rows, tab.data(), tab.size() * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  S.part_step = S.recv_step = h->istep;
+  S.mom_step = -1;
+  return LBRB_OK;
+}
+
+int lbrb_slab_particle_bytes(const lbrb_t* h, size_t* mom_up, size_t* mom_down, size_t* handoff) {
+  if (!h || !h->sp) return LBRB_ERR_ARG;
+  if (mom_up) *mom_up = h->sp->mom_up_bytes;
+  if (mom_down) *mom_down = h->sp->mom_down_bytes;
+  if (handoff) *handoff = h->sp->hand_bytes;
+  return LBRB_OK;
+}
+
+int lbrb_slab_particle_buffers(lbrb_t* h, void** mom_up, void** mom_down, void** mom_lo, void** mom_hi,
+                               void** hand_up, void** hand_down, void** hand_lo, void** hand_hi) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_particle_buffers: no slab particles (lbrb_slab_particles_set)");
+  void** out[8] = {mom_up, mom_down, mom_lo, mom_hi, hand_up, hand_down, hand_lo, hand_hi};
+  for (int m = 0; m < 4; m++) {
+    if (out[m]) *out[m] = h->sp->mom[m];
+    if (out[4 + m]) *out[4 + m] = h->sp->hand[m];
+  }
+  return LBRB_OK;
+}
+
+int lbrb_slab_moments_pack(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_moments_pack: no slab particles (lbrb_slab_particles_set)");
+  SlabParts& S = *h->sp;
+  if (h->istep != S.part_step + 1)
+    return fail(h, LBRB_ERR_STATE, "slab_moments_pack: once per step, after lbrb_step(h, 1)");
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, launch_slab_mom_pack(h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->uv[h->uvprev][0], h->uv[h->uvprev][1],
+                             h->T[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, S.mom[0], S.mom[1], S.mom_pstride,
+                             h->istep, h->slab_j0, h->stream));
+  S.mom_step = h->istep;
+  return LBRB_OK;
+}
+
+int lbrb_slab_particles_step(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_particles_step: no slab particles (lbrb_slab_particles_set)");
+  SlabParts& S = *h->sp;
+  if (h->istep != S.part_step + 1 || S.recv_step != S.part_step || S.mom_step != h->istep)
+    return fail(h, LBRB_ERR_STATE,
+                "slab_particles_step: once per step, after lbrb_step(h, 1), lbrb_slab_moments_pack and the "
+                "moment exchange");
+  const int istep = h->istep, nyT = h->slab_ny_total;
+  const bool rec = h->p.noutconfig > 0 && istep % h->p.noutconfig == 0;
+  const int slots = h->p.record_slots;
+  if (rec && S.rhead - S.rtail >= slots)
+    return fail(h, LBRB_ERR_OVERFLOW, "slab_particles_step: record ring full, drain records first");
+  CK(h, cudaSetDevice(h->dev));
+  const int slot = rec ? (int)(S.rhead % slots) : 0;
+  const size_t per = (size_t)h->nrec_fields * S.cap;
+  const void* const* tab = (const void* const*)S.rows;
+  // after the step: u, v in slot uvcur, the step's input in uvprev, T in cur
+  const void* rows5[5] = {tab + (size_t)h->uvcur * nyT, tab + (size_t)(3 + h->uvcur) * nyT,
+                          tab + (size_t)(6 + h->uvprev) * nyT, tab + (size_t)(9 + h->uvprev) * nyT,
+                          tab + (size_t)(12 + h->cur) * nyT};
+  const int tm = tmark_begin(h, 1, h->stream);
+  CK(h, launch_own_particles(rows5, fp32(h), h->p.nx, nyT, S, h->slab_j0, h->p.ny, istep, h->p.beta, rec ? 1 : 0,
+                             h->p.record_full, rec ? S.d_rec + (size_t)slot * per : nullptr,
+                             rec ? S.d_rid + (size_t)slot * S.cap : nullptr, rec ? S.d_rcnt + slot : nullptr,
+                             h->dflags, h->stream));
+  tmark_end(h, tm, h->stream);
+  S.pc ^= 1;
+  if (rec) {
+    // the record to the host ring on the copy stream
+    S.rstep[slot] = istep;
+    CK(h, cudaEventRecord(S.rev[slot], h->stream));
+    CK(h, cudaStreamWaitEvent(h->copy_stream, S.rev[slot], 0));
+    const int tc = tmark_begin(h, 3, h->copy_stream);
+    CK(h, cudaMemcpyAsync(S.h_rec + (size_t)slot * per, S.d_rec + (size_t)slot * per, per * sizeof(double),
+                          cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(h, cudaMemcpyAsync(S.h_rid + (size_t)slot * S.cap, S.d_rid + (size_t)slot * S.cap, S.cap * sizeof(int),
+                          cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(h, cudaMemcpyAsync(S.h_rcnt + slot, S.d_rcnt + slot, sizeof(int), cudaMemcpyDeviceToHost, h->copy_stream));
+    tmark_end(h, tc, h->copy_stream);
+    CK(h, cudaEventRecord(S.rev[slot], h->copy_stream));
+    S.rhead++;
+    h->join_pending = true;
+  }
+  S.part_step = istep;
+  return LBRB_OK;
+}
+
+int lbrb_slab_particles_recv(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_particles_recv: no slab particles (lbrb_slab_particles_set)");
+  SlabParts& S = *h->sp;
+  if (S.part_step != h->istep || S.part_step == S.recv_step)
+    return fail(h, LBRB_ERR_STATE, "slab_particles_recv: once per step, after lbrb_slab_particles_step");
+  CK(h, cudaSetDevice(h->dev));
+  const int tm = tmark_begin(h, 1, h->stream);
+  CK(h, launch_own_recv(S, h->slab_j0, h->p.ny, h->slab_ny_total, h->istep, h->dflags, h->stream));
+  tmark_end(h, tm, h->stream);
+  S.recv_step = h->istep;
+  return LBRB_OK;
+}
+
+int lbrb_slab_particles_count(lbrb_t* h, int* n) {
+  if (!h || !n) return LBRB_ERR_ARG;
+  if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_particles_count: no slab particles (lbrb_slab_particles_set)");
+  CK(h, cudaSetDevice(h->dev));
+  int c = 0;
+  CK(h, cudaMemcpyAsync(&c, h->sp->cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  *n = c;
+  return LBRB_OK;
+}
+
+int lbrb_slab_particles_get(lbrb_t* h, int max_n, int* n, int* ids, double* x, double* y, double* u, double* v,
+                            double* xo, double* yo, double* uo, double* vo) {
+  if (!h || !n || max_n < 0) return LBRB_ERR_ARG;
+  int cnt = 0;
+  const int rc = lbrb_slab_particles_count(h, &cnt);
+  if (rc) return rc;
+  if (cnt > max_n) return fail(h, LBRB_ERR_ARG, "slab_particles_get: max_n below the slab's particle count");
+  const SlabParts& S = *h->sp;
+  std::vector<double> P((size_t)8 * cnt);
+  for (int a = 0; a < 8 && cnt > 0; a++)
+    CK(h, cudaMemcpyAsync(P.data() + (size_t)a * cnt, S.P[S.pc] + (size_t)a * S.cap, cnt * sizeof(double),
+                          cudaMemcpyDeviceToHost, h->stream));
+  std::vector<int> I(cnt);
+  if (cnt > 0) CK(h, cudaMemcpyAsync(I.data(), S.id[S.pc], cnt * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  double* outs[8] = {x, y, u, v, xo, yo, uo, vo};
+  for (int a = 0; a < 8; a++)
+    if (outs[a] && cnt > 0) std::memcpy(outs[a], &P[(size_t)a * cnt], cnt * sizeof(double));
+  if (ids && cnt > 0) std::memcpy(ids, I.data(), cnt * sizeof(int));
+  *n = cnt;
+  return LBRB_OK;
+}
+
+int lbrb_slab_record_pending(lbrb_t* h, int* count) {
+  if (!h || !count) return LBRB_ERR_ARG;
+  *count = h->sp ? (int)(h->sp->rhead - h->sp->rtail) : 0;
+  return LBRB_OK;
+}
+
+int lbrb_slab_record_drain(lbrb_t* h, int max_n, int* step, int* count, int* ids, double* buf) {
+  if (!h || !step || !count || max_n < 0) return LBRB_ERR_ARG;
+  *step = -1;
+  *count = 0;
+  if (!h->sp || h->sp->rtail == h->sp->rhead) return LBRB_OK;
+  SlabParts& S = *h->sp;
+  const int slot = (int)(S.rtail % h->p.record_slots);
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaEventSynchronize(S.rev[slot]));
+  const int c = S.h_rcnt[slot];
+  if (c > max_n) return fail(h, LBRB_ERR_ARG, "slab_record_drain: max_n below the record's particle count");
+  const size_t per = (size_t)h->nrec_fields * S.cap;
+  if (buf)
+    for (int f = 0; f < h->nrec_fields; f++)
+      std::memcpy(buf + (size_t)f * c, S.h_rec + (size_t)slot * per + (size_t)f * S.cap, c * sizeof(double));
+  if (ids) std::memcpy(ids, S.h_rid + (size_t)slot * S.cap, c * sizeof(int));
+  *step = S.rstep[slot];
+  *count = c;
+  S.rtail++;
+  return LBRB_OK;
+}
+
 // One two-step launch of a y-slab from its two-row ghost blocks (filled by
 // the neighbours' lbrb_slab_pack2), records of the steps as flagged; `last`:
 // the second step writes the moments (it ends the call).  Buffers as two
 // one-step launches leave them; the caller updates the handle's state.
 static int slab_pair_launch(lbrb_t* h, bool rec1, bool rec2, bool last) {
-  const bool parts = h->np > 0;
+  const bool parts = moves_particles(h);
   const int src = h->cur, dst = h->cur ^ 1;
   const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;
   const int B = parts ? h->uvprev : h->uvcur;
@@ -1598,20 +1937,14 @@ static int slab_pair_launch(lbrb_t* h, bool rec1, bool rec2, bool last) {
   return LBRB_OK;
 }
 
-// Tables for the particles of a slab domain, one copy on each slab's device
-// (addresses are unified, so the copies are equal): for every global row a
-// pointer to that row of u and v (3 slots each) and T (2 buffers) in the slab
-// that holds it, then each slab's particle array and record ring, then the
-// slab of each row.  Kernels on one device read the other slabs' rows through
+// Tables for the bilinear nudging of a slab domain in one process, one copy
+// on each slab's device (addresses are unified, so the copies are equal): for
+// every row of the domain a pointer to that row of T (2 buffers) in the slab
+// that holds it.  Kernels on one device read the other slabs' rows through
 // peer access.
-static size_t tab_rows(int ny_total) { return (size_t)8 * ny_total; }
-static int slab_particle_tables(lbrb_t* const* slabs, int n) {
+static int slab_nudge_tables(lbrb_t* const* slabs, int n) {
   lbrb_t* h0 = slabs[0];
-  std::vector<const void*> sig;
-  for (int s = 0; s < n; s++) {
-    sig.push_back(slabs[s]);
-    sig.push_back(slabs[s]->px);
-  }
+  std::vector<const void*> sig(slabs, slabs + n);
   bool fresh = true;
   for (int s = 0; s < n; s++) fresh = fresh && slabs[s]->slab_sig == sig;
   if (fresh) return LBRB_OK;
@@ -1622,101 +1955,92 @@ static int slab_particle_tables(lbrb_t* const* slabs, int n) {
       int ok = 0;
       CK(slabs[s], cudaDeviceCanAccessPeer(&ok, a, b));
       if (!ok)
-        return fail(slabs[s], LBRB_ERR_UNSUPPORTED,
-                    "slab_step: particles and nudging need peer access between the slabs' GPUs");
+        return fail(slabs[s], LBRB_ERR_UNSUPPORTED, "slab_step: nudging needs peer access between the slabs' GPUs");
       CK(slabs[s], cudaSetDevice(a));
       const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
       if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
       else if (e != cudaSuccess) return fail(slabs[s], LBRB_ERR_CUDA, "slab_step: peer access", e);
     }
   const int nyT = h0->slab_ny_total;
-  const size_t nptr = tab_rows(nyT) + 2 * (size_t)n;
-  std::vector<unsigned char> tab(nptr * sizeof(void*) + (size_t)nyT * sizeof(int));
-  const void** ptr = (const void**)tab.data();
-  int* sor = (int*)(tab.data() + nptr * sizeof(void*));
+  std::vector<const void*> tab((size_t)2 * nyT);
   for (int t = 0; t < n; t++) {
     const lbrb_t* h = slabs[t];
     const size_t rowb = (size_t)h->pitch * h->esize;
-    for (int jl = 0; jl < h->p.ny; jl++) {
-      const int j = h->slab_j0 + jl;
-      for (int a = 0; a < 3; a++) {
-        ptr[(size_t)a * nyT + j] = (const char*)h->uv[a][0] + jl * rowb;
-        ptr[(size_t)(3 + a) * nyT + j] = (const char*)h->uv[a][1] + jl * rowb;
-      }
-      for (int b = 0; b < 2; b++) ptr[(size_t)(6 + b) * nyT + j] = (const char*)h->T[b] + jl * rowb;
-      sor[j] = t;
-    }
-    ptr[tab_rows(nyT) + t] = h->px;
-    ptr[tab_rows(nyT) + n + t] = h->d_ring;
+    for (int jl = 0; jl < h->p.ny; jl++)
+      for (int b = 0; b < 2; b++) tab[(size_t)b * nyT + h->slab_j0 + jl] = (const char*)h->T[b] + jl * rowb;
   }
+  const size_t bytes = tab.size() * sizeof(void*);
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
     CK(h, cudaSetDevice(h->dev));
-    if (h->slab_tab_bytes < tab.size()) {
+    if (h->slab_tab_bytes < bytes) {
       if (h->slab_tab) cudaFree(h->slab_tab);
       h->slab_tab = nullptr;
       h->slab_tab_bytes = 0;
-      if (cudaMalloc(&h->slab_tab, tab.size()) != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "slab particle tables");
-      h->slab_tab_bytes = tab.size();
+      if (cudaMalloc(&h->slab_tab, bytes) != cudaSuccess) return fail(h, LBRB_ERR_NOMEM, "slab nudging tables");
+      h->slab_tab_bytes = bytes;
     }
-    CK(h, cudaMemcpyAsync(h->slab_tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->slab_tab, tab.data(), bytes, cudaMemcpyHostToDevice, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     h->slab_sig = sig;
   }
   return LBRB_OK;
 }
 
-// Particles of one step of a slab domain, after every slab's fused kernel:
-// each slab advances the particles whose cell lies in its rows (fields read
-// through the row tables, records into its own ring slot), then each slab
-// takes the particles it did not advance from their owners, and slab 0 their
-// records, which it copies to the host like a whole domain's.
-static int slab_particles(lbrb_t* const* slabs, int n) {
-  lbrb_t* h0 = slabs[0];
-  const int np = h0->np, nyT = h0->slab_ny_total;
-  const int istep = h0->istep;  // (the step just taken)
-  const bool rec = h0->p.noutconfig > 0 && istep % h0->p.noutconfig == 0;
-  const int slot = rec ? (int)(h0->rec_head % h0->p.record_slots) : 0;
-  const size_t per = (size_t)h0->nrec_fields * np;
-  const size_t rec_off = (size_t)slot * per;
+// The particles of one step of a slab domain in one process, after every
+// slab's fused kernel: the exchange a process per GPU does over NCCL, done
+// with peer copies around the ring of slabs (up to s + 1, down to s - 1,
+// periodic).  Each copy into a neighbour's message waits for the
+// neighbour's last read of it (its previous particle step, or receive).
+static int slab_owner_particles(lbrb_t* const* slabs, int n) {
+  auto up = [&](int s) { return slabs[(s + 1) % n]; };
+  auto dn = [&](int s) { return slabs[(s + n - 1) % n]; };
+  auto wait_nb = [&](lbrb_t* h, int s, auto ev) -> int {
+    CK(h, cudaStreamWaitEvent(h->stream, ev(up(s)), 0));
+    CK(h, cudaStreamWaitEvent(h->stream, ev(dn(s)), 0));
+    return LBRB_OK;
+  };
+  auto ev_part = [](lbrb_t* t) { return t->sp->ev_part; };
+  auto ev_mom = [](lbrb_t* t) { return t->sp->ev_mom; };
+  auto ev_hand = [](lbrb_t* t) { return t->sp->ev_hand; };
+  // 1. moment messages
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
     CK(h, cudaSetDevice(h->dev));
-    for (int t = 0; t < n; t++)
-      if (t != s) CK(h, cudaStreamWaitEvent(h->stream, slabs[t]->slab_ev_done, 0));
-    const void* const* rows = (const void* const*)h->slab_tab;
-    // after the step: u, v in slot uvcur, the step's input in uvprev, T in cur
-    const void* rows5[5] = {rows + (size_t)h->uvcur * nyT, rows + (size_t)(3 + h->uvcur) * nyT,
-                            rows + (size_t)h->uvprev * nyT, rows + (size_t)(3 + h->uvprev) * nyT,
-                            rows + (size_t)(6 + h->cur) * nyT};
-    const int* sor = (const int*)(rows + tab_rows(nyT) + 2 * (size_t)n);
-    const bool f32 = fp32(h);
-    CK(h, launch_particles_slab(h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->uv[h->uvprev][0], h->uv[h->uvprev][1],
-                                h->T[h->cur], rows5, f32, h->p.nx, nyT, h->pitch, h->px, h->ptype, np, h->p.beta,
-                                rec ? 1 : 0, h->p.record_full, rec ? h->d_ring + rec_off : nullptr, h->dflags, sor,
-                                s, h->slab_own, h->stream));
-    CK(h, cudaEventRecord(h->slab_ev_part, h->stream));
+    int rc = wait_nb(h, s, ev_part);
+    if (!rc) rc = lbrb_slab_moments_pack(h);
+    if (rc) return rc;
+    CK(h, cudaMemcpyPeerAsync(up(s)->sp->mom[2], up(s)->dev, h->sp->mom[0], h->dev, h->sp->mom_up_bytes, h->stream));
+    CK(h, cudaMemcpyPeerAsync(dn(s)->sp->mom[3], dn(s)->dev, h->sp->mom[1], h->dev, h->sp->mom_down_bytes,
+                              h->stream));
+    CK(h, cudaEventRecord(h->sp->ev_mom, h->stream));
   }
+  // 2. each slab's particles
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
     CK(h, cudaSetDevice(h->dev));
-    for (int t = 0; t < n; t++)
-      if (t != s) CK(h, cudaStreamWaitEvent(h->stream, slabs[t]->slab_ev_part, 0));
-    const void* const* rows = (const void* const*)h->slab_tab;
-    const double* const* Ps = (const double* const*)(rows + tab_rows(nyT));
-    CK(h, launch_particles_merge(h->px, np, h->slab_own, s, Ps, s == 0 && rec ? h->d_ring + rec_off : nullptr,
-                                 Ps + n, rec_off, h0->nrec_fields, h->stream));
+    int rc = wait_nb(h, s, ev_mom);
+    if (!rc) rc = lbrb_slab_particles_step(h);
+    if (rc) return rc;
+    CK(h, cudaEventRecord(h->sp->ev_part, h->stream));
   }
-  if (rec) {
-    CK(h0, cudaSetDevice(h0->dev));
-    h0->h_ring_step[slot] = istep;
-    CK(h0, cudaEventRecord(h0->ring_ev[slot], h0->stream));
-    CK(h0, cudaStreamWaitEvent(h0->copy_stream, h0->ring_ev[slot], 0));
-    CK(h0, cudaMemcpyAsync(h0->h_ring + rec_off, h0->d_ring + rec_off, per * sizeof(double), cudaMemcpyDeviceToHost,
-                           h0->copy_stream));
-    CK(h0, cudaEventRecord(h0->ring_ev[slot], h0->copy_stream));
-    h0->rec_head++;
-    h0->join_pending = true;
+  // 3. hand-off lists
+  for (int s = 0; s < n; s++) {
+    lbrb_t* h = slabs[s];
+    CK(h, cudaSetDevice(h->dev));
+    const int rc = wait_nb(h, s, ev_part);
+    if (rc) return rc;
+    CK(h, cudaMemcpyPeerAsync(up(s)->sp->hand[2], up(s)->dev, h->sp->hand[0], h->dev, h->sp->hand_bytes, h->stream));
+    CK(h, cudaMemcpyPeerAsync(dn(s)->sp->hand[3], dn(s)->dev, h->sp->hand[1], h->dev, h->sp->hand_bytes, h->stream));
+    CK(h, cudaEventRecord(h->sp->ev_hand, h->stream));
+  }
+  // 4. each slab appends what it received
+  for (int s = 0; s < n; s++) {
+    lbrb_t* h = slabs[s];
+    CK(h, cudaSetDevice(h->dev));
+    int rc = wait_nb(h, s, ev_hand);
+    if (!rc) rc = lbrb_slab_particles_recv(h);
+    if (rc) return rc;
   }
   return LBRB_OK;
 }
@@ -1734,23 +2058,31 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
   }
   if (slabs[n - 1]->slab_j0 + slabs[n - 1]->p.ny != slabs[0]->slab_ny_total) return LBRB_ERR_ARG;
   lbrb_t* h0 = slabs[0];
-  const bool parts = h0->np > 0;
+  const bool parts = h0->sp != nullptr;
   const bool nudge = h0->p.nudge == LBRB_NUDGE_BILINEAR;
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
-    if (h->np != h0->np) return fail(h, LBRB_ERR_ARG, "slab_step: every slab holds all particles");
+    if ((h->sp != nullptr) != parts)
+      return fail(h, LBRB_ERR_ARG, "slab_step: every slab or none holds particles (lbrb_slab_particles_set)");
     if (h->p.nudge != h0->p.nudge || h->p.alpha != h0->p.alpha || h->nobs != h0->nobs)
       return fail(h, LBRB_ERR_ARG, "slab_step: slabs differ in nudging");
     if (!parts) continue;
-    if (!h->particles_set) return fail(h, LBRB_ERR_STATE, "slab_step: particles not set");
     if (h->p.noutconfig != h0->p.noutconfig || h->p.record_full != h0->p.record_full || h->p.beta != h0->p.beta ||
         h->istep != h0->istep || h->cur != h0->cur || h->uvcur != h0->uvcur || h->uvprev != h0->uvprev)
       return fail(h, LBRB_ERR_ARG, "slab_step: slabs differ in particle settings or step");
+    if (h->sp->part_step != h->istep || h->sp->recv_step != h->istep)
+      return fail(h, LBRB_ERR_STATE, "slab_step: a slab's particle exchange of its last step is unfinished");
   }
-  if (parts || nudge) {
-    const int rc = slab_particle_tables(slabs, n);
+  if (nudge) {
+    const int rc = slab_nudge_tables(slabs, n);
     if (rc) return rc;
   }
+  // records pending in the fullest slab ring (every slab records the same steps)
+  auto ring_used = [&]() -> long {
+    long m = 0;
+    for (int s = 0; s < n; s++) m = std::max(m, slabs[s]->sp->rhead - slabs[s]->sp->rtail);
+    return m;
+  };
   const size_t gb = lbrb_slab_ghost_bytes(h0);
   const size_t gb2 = (size_t)SLAB_GH2_PLANES * h0->p.nx * h0->esize;
   // two steps per launch: Dirichlet walls, no nudging, never the call's last
@@ -1812,7 +2144,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
         }
       }
       if (parts) {
-        const int rc = slab_particles(slabs, n);
+        const int rc = slab_owner_particles(slabs, n);
         if (rc) return rc;
       }
     }
@@ -1823,7 +2155,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
     if (slab_pairs && nsteps - it >= 3) {
       int need = 0;
       for (int q = 1; q <= 2; q++) need += parts && h0->p.noutconfig > 0 && (h0->istep + q) % h0->p.noutconfig == 0;
-      if (h0->rec_head - h0->rec_tail + need <= h0->p.record_slots) {
+      if (!parts || ring_used() + need <= h0->p.record_slots) {
         const int rc = pair_iteration();
         if (rc) return rc;
         it++;  // (and the loop's own increment)
@@ -1831,7 +2163,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
       }
     }
     if (parts && h0->p.noutconfig > 0 && (h0->istep + 1) % h0->p.noutconfig == 0 &&
-        h0->rec_head - h0->rec_tail >= h0->p.record_slots)
+        ring_used() >= h0->p.record_slots)
       return fail(h0, LBRB_ERR_OVERFLOW, "slab_step: record ring full, drain records first");
     // 1. each slab packs its boundary rows and copies them into its
     //    neighbours' ghost rows, once the neighbours' previous step (which
@@ -1873,7 +2205,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
         for (int t = 0; t < n; t++)
           if (t != s) CK(h, cudaStreamWaitEvent(h->stream, slabs[t]->slab_ev_done, 0));
         const double* obs = h->slab_obs;
-        const void* const* Trows = (const void* const*)h->slab_tab + (size_t)(6 + h->cur) * h->slab_ny_total;
+        const void* const* Trows = (const void* const*)h->slab_tab + (size_t)h->cur * h->slab_ny_total;
         const int tm = tmark_begin(h, 2, h->stream);
         CK(h, launch_bilinear_nudge_slab(Trows, pop_base(h, h->cur, 1), fp32(h), h->plane, h->p.nx, h->slab_ny_total,
                                          h->slab_j0, h->p.ny, h->pitch, obs, obs + h->nobs, obs + 2 * (size_t)h->nobs,
@@ -1881,20 +2213,21 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
         tmark_end(h, tm, h->stream);
       }
     }
-    // 4. the particles of the step (next step's fused kernels run after them:
-    //    each slab's stream holds its merge, which waited for every slab's
-    //    particle kernel)
+    // 4. the particles of the step (each slab's next fused kernel runs after
+    //    its receive on its stream)
     if (parts) {
-      const int rc = slab_particles(slabs, n);
+      const int rc = slab_owner_particles(slabs, n);
       if (rc) return rc;
     }
   }
-  if (h0->join_pending) {
-    // the record copies are part of the steps for slab 0's stream
-    CK(h0, cudaSetDevice(h0->dev));
-    CK(h0, cudaEventRecord(h0->join_ev, h0->copy_stream));
-    CK(h0, cudaStreamWaitEvent(h0->stream, h0->join_ev, 0));
-    h0->join_pending = false;
+  for (int s = 0; s < n; s++) {
+    lbrb_t* h = slabs[s];
+    if (!h->join_pending) continue;
+    // the record copies are part of the steps for each slab's stream
+    CK(h, cudaSetDevice(h->dev));
+    CK(h, cudaEventRecord(h->join_ev, h->copy_stream));
+    CK(h, cudaStreamWaitEvent(h->stream, h->join_ev, 0));
+    h->join_pending = false;
   }
   return LBRB_OK;
 }
@@ -1984,6 +2317,10 @@ int lbrb_sync(lbrb_t* h) {
   if (f & DFLAG_NONFINITE) return fail(h, LBRB_ERR_NONFINITE, "device: non-finite value seen");
   if (f & DFLAG_RANGE) return fail(h, LBRB_ERR_RANGE, "device: particle or observation outside the domain");
   if (f & DFLAG_BOXCAP) return fail(h, LBRB_ERR_STATE, "device: box nudging list inconsistent");
+  if (f & DFLAG_XCAP)
+    return fail(h, LBRB_ERR_OVERFLOW, "device: a slab's particles or a hand-off list over its capacity");
+  if (f & DFLAG_XMSG)
+    return fail(h, LBRB_ERR_STATE, "device: a slab message from the wrong step or neighbour (exchange missing?)");
   return LBRB_OK;
 }
 

@@ -43,14 +43,18 @@ cudaError_t launch_particles_pair(const void* const* fields_a, const void* const
                                   double* rec_a, double* rec_b, unsigned* dflags, cudaStream_t s, bool pdl);
 // y-slabs: rows5 = device tables of row pointers (u, v, ub, vb, T), one
 // entry per global row
-cudaError_t launch_particles_slab(const void* u, const void* v, const void* ub, const void* vb, const void* T,
-                                  const void* const* rows5, bool fp32, int nx, int ny_total, int pitch,
-                                  double* P, const int* ptype, int np, double beta, int record, int full,
-                                  double* rec, unsigned* dflags, const int* slab_of_row, int me, int* own,
-                                  cudaStream_t s);
-cudaError_t launch_particles_merge(double* P, int np, const int* own, int me, const double* const* Ps,
-                                   double* rec, const double* const* recs, size_t rec_off, int nrec,
-                                   cudaStream_t s);
+// y-slabs holding their own particles (particle_kernels.cu): the moment
+// messages of a slab; one particle step (advance, classify, compact, pack
+// the hand-off lists) through the 5 field tables rows5; the append of the
+// received lists
+cudaError_t launch_slab_mom_pack(const void* u, const void* v, const void* ub, const void* vb, const void* T,
+                                 bool fp32, int nx, int nyl, int pitch, void* mup, void* mdown, size_t pstride,
+                                 int istep, int j0, cudaStream_t s);
+cudaError_t launch_own_particles(const void* const* rows5, bool fp32, int nx, int ny_total, const SlabParts& S,
+                                 int j0, int nyl, int istep, double beta, int record, int full, double* rec,
+                                 int* rid, int* rcnt, unsigned* dflags, cudaStream_t s);
+cudaError_t launch_own_recv(const SlabParts& S, int j0, int nyl, int nyT, int istep, unsigned* dflags,
+                            cudaStream_t s);
 // y-slabs: Trows = device table of T row pointers, one per global row
 cudaError_t launch_bilinear_nudge_slab(const void* Trows, void* g, bool fp32, size_t plane, int nx, int ny_total,
                                        int j0, int nyl, int pitch, const double* ox, const double* oy,

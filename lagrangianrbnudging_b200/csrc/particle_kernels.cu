@@ -50,72 +50,278 @@ __global__ void __launch_bounds__(128) particle_pair_kernel(const PView<Real> Va
 }
 
 // ------------------------------------------------------------- y-slabs
-// A domain held as y-slabs: every slab holds all particles.  Each step, the
-// slab whose rows hold a particle's cell (its position before the step)
-// advances it, reading the fields through the view's row tables; every slab
-// notes that owner.  The merge then copies each particle it did not own (and,
-// on record steps, its record) from its owner.  (The reference keeps each
-// rank's particles in that rank and sends those that leave its rows to the
-// neighbour, toggle_prtcl in Trajectories/code/mympi2.h:568-760; replicated
-// arrays need no compaction and keep the whole domain's particle order.)
+// A domain held as y-slabs, one handle each (one process per GPU, or several
+// in one process): each slab holds the particles whose cell lies in its rows,
+// as the reference's ranks do (toggle_prtcl, Trajectories/code/mympi2.h:
+// 568-760, sends the particles that leave a rank's block to the neighbour).
+// Per step, after the slab's fused kernel and the exchange of the moment
+// rows (slab_mom_pack_kernel): own_step_kernel advances the slab's particles,
+// reading the fields through row tables (own rows, the neighbours' rows
+// from the moment messages, a zero row elsewhere) and classifies each by the
+// cell it ends in; own_scan_kernel turns the per-block counts into offsets;
+// own_scatter_kernel compacts the kept particles, in order, into the other
+// buffer and writes the leavers, in order, into the hand-off lists; after
+// the exchange of the lists own_recv_kernel appends the particles from below
+// and then those from above.  A particle's arithmetic is particle_update's,
+// so its state equals the whole domain's bit for bit.
 __device__ __forceinline__ int cell_row(double yy, int ny) {
   if (!(yy > -2.0 && yy < ny + 2.0)) return 0;  // (flagged by make_cell)
   return wrapi((int)yy - 1, ny);
 }
 
-template <typename Real, bool DERIVS>
-__global__ void __launch_bounds__(128)
-    particle_slab_kernel(const PView<Real> V, const int* __restrict__ slab_of_row, int me, int* __restrict__ own) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= V.np) return;
-  const int o = slab_of_row[cell_row(V.P[V.np + p], V.ny)];
-  own[p] = o;
-  if (o != me) return;
-  particle_update<Real, DERIVS, true>(V, p);
+// a row of the domain within reach of the slab [j0, j0 + nyl): its own rows,
+// one below and two above (periodic in y)
+__device__ __forceinline__ bool in_reach(int j, int j0, int nyl, int nyT) {
+  const int d = wrapi(j - j0 + 1, nyT);  // 0: the row below
+  return d <= nyl + 2;
 }
 
-__global__ void __launch_bounds__(128)
-    particle_merge_kernel(double* __restrict__ P, int np, const int* __restrict__ own, int me,
-                          const double* const* __restrict__ Ps, double* __restrict__ rec,
-                          const double* const* __restrict__ recs, size_t rec_off, int nrec) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
-  const int o = own[p];
-  if (o == me) return;
-  const double* Q = Ps[o];
-#pragma unroll
-  for (int k = 0; k < 8; k++) P[(size_t)k * np + p] = Q[(size_t)k * np + p];
-  if (rec) {
-    const double* R = recs[o] + rec_off;
-    for (int f = 0; f < nrec; f++) rec[(size_t)f * np + p] = R[(size_t)f * np + p];
+struct OwnArgs {
+  const int* cnt;
+  const int* id;
+  int* rid;         // record ids (record steps) or null
+  int* rcnt;        // record count (record steps) or null
+  unsigned char* cls;
+  int* bcnt;
+  int j0, nyl, istep;
+  const SlabMsg* mlo;  // moment rows from the slab below
+  const SlabMsg* mhi;  // from the slab above
+};
+
+template <typename Real, bool DERIVS>
+__global__ void __launch_bounds__(128) own_step_kernel(const PView<Real> V, const OwnArgs A) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;  // (the grid covers the capacity)
+  const int n = A.cnt[1], nyT = V.ny;
+  if (p == 0) {
+    const SlabMsg lo = *A.mlo, hi = *A.mhi;
+    const bool ok = lo.kind == MSG_MOM_UP && lo.step == A.istep && wrapi(lo.j1, nyT) == A.j0 &&
+                    hi.kind == MSG_MOM_DOWN && hi.step == A.istep && hi.j0 == wrapi(A.j0 + A.nyl, nyT);
+    if (!ok) atomicOr(V.dflags, DFLAG_XMSG);
+    if (A.rcnt) *A.rcnt = n;
+  }
+  int c = 3;
+  if (p < n) {
+    const int cr = cell_row(V.P[V.np + p], nyT);
+    if (cr < A.j0 || cr >= A.j0 + A.nyl) {
+      atomicOr(V.dflags, DFLAG_RANGE);  // (a particle that moved past a neighbour slab)
+      c = 0;
+    } else {
+      particle_update<Real, DERIVS, true>(V, p);
+      if (V.record) {
+        A.rid[p] = A.id[p];
+        // the record's T was read at the new position: rows within reach?
+        const double yr = V.rec[(size_t)LBRB_REC_Y * V.np + p];
+        if (yr > -2.0 && yr < nyT + 2.0) {
+          const int y1 = (int)yr;
+          if (!in_reach(wrapi(y1 - 1, nyT), A.j0, A.nyl, nyT) || !in_reach(wrapi(y1, nyT), A.j0, A.nyl, nyT))
+            atomicOr(V.dflags, DFLAG_RANGE);
+        }
+      }
+      const double yn = V.P[V.np + p];
+      const int cn = cell_row(yn, nyT);
+      c = !(yn > -2.0 && yn < nyT + 2.0) ? 0 : (cn < A.j0 ? 2 : (cn >= A.j0 + A.nyl ? 1 : 0));
+    }
+  }
+  A.cls[p] = (unsigned char)c;
+  const int k0 = __syncthreads_count(c == 0), k1 = __syncthreads_count(c == 1), k2 = __syncthreads_count(c == 2);
+  if (threadIdx.x == 0) {
+    A.bcnt[blockIdx.x * 3 + 0] = k0;
+    A.bcnt[blockIdx.x * 3 + 1] = k1;
+    A.bcnt[blockIdx.x * 3 + 2] = k2;
   }
 }
 
-cudaError_t launch_particles_slab(const void* u, const void* v, const void* ub, const void* vb, const void* T,
-                                  const void* const* rows5, bool fp32, int nx, int ny_total, int pitch,
-                                  double* P, const int* ptype, int np, double beta, int record, int full,
-                                  double* rec, unsigned* dflags, const int* slab_of_row, int me, int* own,
-                                  cudaStream_t s) {
-  if (np <= 0) return cudaSuccess;
-  const int g = (np + 127) / 128;
+// one block: exclusive offsets of the per-block counts (each thread scans a
+// run of consecutive blocks), the kept count and the hand-off headers
+__global__ void __launch_bounds__(1024)
+    own_scan_kernel(int* __restrict__ bcnt, int nblk, int* __restrict__ cnt, SlabMsg* hup, SlabMsg* hdown, int xcap,
+                    int istep, int j0, int j1, unsigned* dflags) {
+  __shared__ int s[3][1024];
+  const int t = threadIdx.x;
+  const int per = (nblk + 1023) / 1024;
+  const int b0 = min(nblk, t * per), b1 = min(nblk, b0 + per);
+  int loc[3] = {0, 0, 0};
+  for (int b = b0; b < b1; b++)
+    for (int k = 0; k < 3; k++) loc[k] += bcnt[b * 3 + k];
+  for (int k = 0; k < 3; k++) s[k][t] = loc[k];
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    int v[3];
+    for (int k = 0; k < 3; k++) v[k] = t >= off ? s[k][t - off] : 0;
+    __syncthreads();
+    for (int k = 0; k < 3; k++) s[k][t] += v[k];
+    __syncthreads();
+  }
+  int run[3];
+  for (int k = 0; k < 3; k++) run[k] = s[k][t] - loc[k];
+  for (int b = b0; b < b1; b++)
+    for (int k = 0; k < 3; k++) {
+      const int c = bcnt[b * 3 + k];
+      bcnt[b * 3 + k] = run[k];
+      run[k] += c;
+    }
+  if (t == 1023) {
+    const int kept = s[0][1023], up = s[1][1023], down = s[2][1023];
+    cnt[0] = kept;
+    cnt[1] = kept;
+    if (up > xcap || down > xcap) atomicOr(dflags, DFLAG_XCAP);
+    *hup = SlabMsg{min(up, xcap), istep, j0, j1, MSG_HAND_UP, {0, 0, 0}};
+    *hdown = SlabMsg{min(down, xcap), istep, j0, j1, MSG_HAND_DOWN, {0, 0, 0}};
+  }
+}
+
+__device__ __forceinline__ void put_rec(HandoffRec* r, const double* __restrict__ P, int cap, int p, int id,
+                                        int type) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) r->P[k] = P[(size_t)k * cap + p];
+  r->id = id;
+  r->type = type;
+}
+
+__global__ void __launch_bounds__(128)
+    own_scatter_kernel(const double* __restrict__ P, const int* __restrict__ id, const int* __restrict__ type, int cap,
+                       const unsigned char* __restrict__ cls, const int* __restrict__ bcnt, double* __restrict__ P2,
+                       int* __restrict__ id2, int* __restrict__ type2, HandoffRec* __restrict__ up,
+                       HandoffRec* __restrict__ down, int xcap) {
+  __shared__ int wc[3][4];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = cls[p];
+  unsigned m[3];
+  for (int k = 0; k < 3; k++) m[k] = __ballot_sync(0xffffffffu, c == k);
+  if (lane == 0)
+    for (int k = 0; k < 3; k++) wc[k][w] = __popc(m[k]);
+  __syncthreads();
+  if (c == 3) return;
+  int at = bcnt[blockIdx.x * 3 + c] + __popc(m[c] & ((1u << lane) - 1u));
+  for (int q = 0; q < w; q++) at += wc[c][q];
+  if (c == 0) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) P2[(size_t)k * cap + at] = P[(size_t)k * cap + p];
+    id2[at] = id[p];
+    type2[at] = type[p];
+  } else if (at < xcap) {
+    put_rec((c == 1 ? up : down) + at, P, cap, p, id[p], type[p]);
+  }
+}
+
+// the particles handed over by the slab below (lo) and the slab above (hi),
+// appended after the kept ones in that order
+__global__ void __launch_bounds__(128)
+    own_recv_kernel(double* __restrict__ P, int* __restrict__ id, int* __restrict__ type, int cap, int* cnt,
+                    const SlabMsg* hlo, const HandoffRec* __restrict__ rlo, const SlabMsg* hhi,
+                    const HandoffRec* __restrict__ rhi, int xcap, int istep, int j0, int j1, int nyT,
+                    unsigned* dflags) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const SlabMsg lo = *hlo, hi = *hhi;
+  const bool ok = lo.kind == MSG_HAND_UP && lo.step == istep && wrapi(lo.j1, nyT) == j0 && lo.count >= 0 &&
+                  lo.count <= xcap && hi.kind == MSG_HAND_DOWN && hi.step == istep && hi.j0 == wrapi(j1, nyT) &&
+                  hi.count >= 0 && hi.count <= xcap;
+  const int nlo = ok ? lo.count : 0, nhi = ok ? hi.count : 0;
+  const int n0 = cnt[0];
+  if (t == 0) {
+    if (!ok) atomicOr(dflags, DFLAG_XMSG);
+    if (n0 + nlo + nhi > cap) atomicOr(dflags, DFLAG_XCAP);
+    cnt[1] = min(cap, n0 + nlo + nhi);
+  }
+  const HandoffRec* r = nullptr;
+  int at = 0;
+  if (t < xcap) {
+    if (t < nlo) r = rlo + t, at = n0 + t;
+  } else if (t - xcap < nhi) {
+    r = rhi + (t - xcap), at = n0 + nlo + (t - xcap);
+  }
+  if (!r || at >= cap) return;
+#pragma unroll
+  for (int k = 0; k < 9; k++) P[(size_t)k * cap + at] = r->P[k];
+  id[at] = r->id;
+  type[at] = r->type;
+}
+
+// the moment rows a slab sends: up (u, v, T of its top row) and down (u, v,
+// u^{n-1}, v^{n-1}, T of row 0, u, v, T of row 1)
+template <typename Real>
+__global__ void __launch_bounds__(256)
+    slab_mom_pack_kernel(const Real* __restrict__ u, const Real* __restrict__ v, const Real* __restrict__ ub,
+                         const Real* __restrict__ vb, const Real* __restrict__ T, int nx, int nyl, int pitch,
+                         char* mup, char* mdown, size_t pstride, int istep, int j0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.y;  // plane: 0-2 up, 3-10 down
+  if (q == 0 && i == 0) {
+    *(SlabMsg*)mup = SlabMsg{MOM_UP_PLANES, istep, j0, j0 + nyl, MSG_MOM_UP, {0, 0, 0}};
+    *(SlabMsg*)mdown = SlabMsg{MOM_DOWN_PLANES, istep, j0, j0 + nyl, MSG_MOM_DOWN, {0, 0, 0}};
+  }
+  if (i >= nx) return;
+  const size_t top = (size_t)(nyl - 1) * pitch, r1 = (size_t)pitch;
+  const Real* src;
+  char* dst;
+  switch (q) {
+    case 0: src = u + top; break;
+    case 1: src = v + top; break;
+    case 2: src = T + top; break;
+    case 3: src = u; break;
+    case 4: src = v; break;
+    case 5: src = ub; break;
+    case 6: src = vb; break;
+    case 7: src = T; break;
+    case 8: src = u + r1; break;
+    case 9: src = v + r1; break;
+    default: src = T + r1; break;
+  }
+  dst = q < 3 ? mup + MOM_PLANES_OFF + q * pstride : mdown + MOM_PLANES_OFF + (q - 3) * pstride;
+  ((Real*)dst)[i] = src[i];
+}
+
+cudaError_t launch_slab_mom_pack(const void* u, const void* v, const void* ub, const void* vb, const void* T,
+                                 bool fp32, int nx, int nyl, int pitch, void* mup, void* mdown, size_t pstride,
+                                 int istep, int j0, cudaStream_t s) {
+  const dim3 g((nx + 255) / 256, MOM_UP_PLANES + MOM_DOWN_PLANES);
+  if (fp32)
+    slab_mom_pack_kernel<float><<<g, 256, 0, s>>>((const float*)u, (const float*)v, (const float*)ub,
+                                                   (const float*)vb, (const float*)T, nx, nyl, pitch, (char*)mup,
+                                                   (char*)mdown, pstride, istep, j0);
+  else
+    slab_mom_pack_kernel<double><<<g, 256, 0, s>>>((const double*)u, (const double*)v, (const double*)ub,
+                                                    (const double*)vb, (const double*)T, nx, nyl, pitch, (char*)mup,
+                                                    (char*)mdown, pstride, istep, j0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_own_particles(const void* const* rows5, bool fp32, int nx, int ny_total, const SlabParts& S,
+                                 int j0, int nyl, int istep, double beta, int record, int full, double* rec,
+                                 int* rid, int* rcnt, unsigned* dflags, cudaStream_t s) {
+  const int nblk = S.cap / 128, o = S.pc;
+  OwnArgs A{S.cnt, S.id[o], rid, rcnt, S.cls, S.bcnt, j0, nyl, istep,
+            (const SlabMsg*)S.mom[2], (const SlabMsg*)S.mom[3]};
   auto go = [&](auto zero) -> cudaError_t {
     using Real = decltype(zero);
     using Rows = const Real* const*;
-    PView<Real> V{(const Real*)u, (const Real*)v, (const Real*)ub, (const Real*)vb, (const Real*)T, nx, ny_total,
-                  pitch, P, ptype, np, beta, record, full, rec, dflags, (Rows)rows5[0], (Rows)rows5[1],
-                  (Rows)rows5[2], (Rows)rows5[3], (Rows)rows5[4]};
-    if (beta != 0.0 || full) particle_slab_kernel<Real, true><<<g, 128, 0, s>>>(V, slab_of_row, me, own);
-    else particle_slab_kernel<Real, false><<<g, 128, 0, s>>>(V, slab_of_row, me, own);
+    PView<Real> V{nullptr, nullptr, nullptr, nullptr, nullptr, nx, ny_total, 0, S.P[o], S.type[o], S.cap, beta,
+                  record, full, rec, dflags, (Rows)rows5[0], (Rows)rows5[1], (Rows)rows5[2], (Rows)rows5[3],
+                  (Rows)rows5[4]};
+    if (beta != 0.0 || full) own_step_kernel<Real, true><<<nblk, 128, 0, s>>>(V, A);
+    else own_step_kernel<Real, false><<<nblk, 128, 0, s>>>(V, A);
     return cudaGetLastError();
   };
-  return fp32 ? go(0.f) : go(0.0);
+  cudaError_t e = fp32 ? go(0.f) : go(0.0);
+  if (e != cudaSuccess) return e;
+  own_scan_kernel<<<1, 1024, 0, s>>>(S.bcnt, nblk, S.cnt, (SlabMsg*)S.hand[0], (SlabMsg*)S.hand[1], S.xcap, istep,
+                                     j0, j0 + nyl, dflags);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  own_scatter_kernel<<<nblk, 128, 0, s>>>(S.P[o], S.id[o], S.type[o], S.cap, S.cls, S.bcnt, S.P[o ^ 1],
+                                          S.id[o ^ 1], S.type[o ^ 1],
+                                          (HandoffRec*)((char*)S.hand[0] + HAND_RECS_OFF),
+                                          (HandoffRec*)((char*)S.hand[1] + HAND_RECS_OFF), S.xcap);
+  return cudaGetLastError();
 }
 
-cudaError_t launch_particles_merge(double* P, int np, const int* own, int me, const double* const* Ps,
-                                   double* rec, const double* const* recs, size_t rec_off, int nrec,
-                                   cudaStream_t s) {
-  if (np <= 0) return cudaSuccess;
-  particle_merge_kernel<<<(np + 127) / 128, 128, 0, s>>>(P, np, own, me, Ps, rec, recs, rec_off, nrec);
+cudaError_t launch_own_recv(const SlabParts& S, int j0, int nyl, int nyT, int istep, unsigned* dflags,
+                            cudaStream_t s) {
+  const int o = S.pc;
+  own_recv_kernel<<<(2 * S.xcap + 127) / 128, 128, 0, s>>>(
+      S.P[o], S.id[o], S.type[o], S.cap, S.cnt, (const SlabMsg*)S.hand[2],
+      (const HandoffRec*)((const char*)S.hand[2] + HAND_RECS_OFF), (const SlabMsg*)S.hand[3],
+      (const HandoffRec*)((const char*)S.hand[3] + HAND_RECS_OFF), S.xcap, istep, j0, j0 + nyl, nyT, dflags);
   return cudaGetLastError();
 }
 

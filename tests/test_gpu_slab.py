@@ -90,12 +90,24 @@ def test_slab_mode_rejects_what_it_does_not_cover():
         with pytest.raises(lb.LbrbError):
             r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # box nudging is not covered
     with lb.Run(**dict(params("fp32"), ny=24, nprtcl=8)) as r:
-        r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))
-        r.init_conduction(1, 1e-3)
-        r.set_particles(np.arange(8, dtype=np.int32), np.full(8, 5.0), np.full(8, 40.0), np.zeros(8),
-                        np.zeros(8), np.zeros(8, np.int32), np.zeros(8))  # (y in the whole domain)
         with pytest.raises(lb.LbrbError):
-            r.step(1)  # particles move through lbrb_slab_step only
+            r.slab_set(0, NY)  # a slab holds its own particles (lbrb_slab_particles_set)
+    with lb.Run(**dict(params("fp32"), ny=24)) as r:
+        r.slab_set(0, NY)
+        r.init_conduction(1, 1e-3)
+        with pytest.raises(lb.LbrbError):
+            r.slab_particles_step()  # no particles set
+        r.slab_particles_set(np.arange(8, dtype=np.int32), np.full(8, 5.0), np.linspace(1.5, 40.0, 8),
+                             np.zeros(8), np.zeros(8), np.zeros(8, np.int32), np.zeros(8))
+        assert r.slab_particles_count() == 6  # (y in the whole domain: cells in rows 0-23)
+        with pytest.raises(lb.LbrbError):
+            r.slab_moments_pack()  # after the slab's step
+        r.slab_pack()
+        r.step(1)
+        with pytest.raises(lb.LbrbError):
+            r.slab_particles_step()  # after the moment pack (and its exchange)
+        with pytest.raises(lb.LbrbError):
+            r.step(1)  # the particles of the last step first
     with pytest.raises(ValueError):
         lb.SlabDomain((20, 20), **params("fp32"))  # heights must add up to ny
     with lb.SlabDomain((24, 24), **params("fp32")) as dom:

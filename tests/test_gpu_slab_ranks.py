@@ -1,0 +1,205 @@
+"""One process per GPU with particles (lbrb_slab_particles_* and
+lagrangianrbnudging_b200.slabrank), with the ranks' exchanges done as
+copies between slab handles on one GPU (slabrank.run_local): each slab holds
+the particles in its rows, hands the leavers to its neighbours and receives
+theirs; states, records and populations equal the whole domain's bit for
+bit.  Also the protocol's checks: a message missing from the exchange, a
+full hand-off list, calls out of order."""
+import numpy as np
+import pytest
+
+import lagrangianrbnudging_b200 as lb
+from lagrangianrbnudging_b200 import build, slabrank
+
+pytestmark = pytest.mark.gpu
+
+NX, NY = 64, 48
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build.build()
+
+
+def params(precision, **kw):
+    return dict(**lb.closure(NX, NY, Ra=1e6, Pr=1.0, U=0.1), precision=precision, **kw)
+
+
+def seed(d, n, s):
+    rng = np.random.default_rng(s)
+    x = rng.uniform(0.5, NX + 0.5, n)
+    y = rng.uniform(1.0, NY, n)
+    y[:8] = [1.0, 19.9, 20.0, 20.05, 36.98, 37.0, NY - 0.01, NY - 0.5]  # beside the slab edges and walls
+    ptype = (np.arange(n) % 2).astype(np.int32)
+    invtau = np.where(ptype == 1, 1.0 / 40.0, 0.0)
+    u0 = rng.uniform(-0.02, 0.02, n)
+    d.set_particles((np.arange(n, dtype=np.int32) * 5 + 1)[::-1].copy(), x, y, u0, -u0, ptype, invtau)
+
+
+def developed(precision):
+    with lb.Run(**params(precision)) as dev:
+        dev.init_conduction(23, 5e-2)
+        dev.step(3000)
+        return dev.get_populations(), dev.get_moments()
+
+
+def ranks_of(dom, torch, pairs=False):
+    st = torch.cuda.current_stream().cuda_stream
+    out = []
+    for r in dom.slabs:
+        r.set_stream(st)  # the handles' work in order with the copies between them
+        out.append(slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=dom.np > 0, pairs=pairs))
+    return out
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("heights,beta,full", [((20, 17, 11), 0.0, 0), ((20, 17, 11), 0.5, 1),
+                                                ((24, 24), 0.5, 0), ((16, 3, 29), 0.0, 1)])
+def test_slab_ranks_match_the_whole_domain(precision, heights, beta, full):
+    torch = pytest.importorskip("torch")
+    npart = 400
+    kw = params(precision, nprtcl=npart, noutconfig=7, record_slots=64, beta=beta, record_full=full)
+    (f, g), m = developed(precision)
+    with lb.Run(**kw) as whole, lb.SlabDomain(heights, **kw) as dom:
+        for d in (whole, dom):
+            d.set_populations(f, g)
+            d.set_moments(m["rho"], m["u"], m["v"], m["T"])
+            seed(d, npart, 4)
+        y0 = whole.get_particles()["y"]
+        ranks = ranks_of(dom, torch)
+        for n in (1, 6, 90, 200):
+            whole.step(n)
+            slabrank.run_local(ranks, n)
+            torch.cuda.synchronize()
+            for r in dom.slabs:
+                r.sync()
+            pw, ps = whole.get_particles(), dom.get_particles()
+            for k in pw:
+                np.testing.assert_array_equal(ps[k], pw[k])
+            sw, rw = whole.drain_records_array()
+            ss, rs = dom.drain_records_array()
+            np.testing.assert_array_equal(ss, sw)
+            np.testing.assert_array_equal(rs, rw)
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+        assert sum(dom.slab_counts()) == npart
+        edges = np.cumsum(heights)[:-1]
+        moved = (np.searchsorted(edges, np.floor(y0) - 1, side="right")
+                 != np.searchsorted(edges, np.floor(pw["y"]) - 1, side="right"))
+        assert moved.sum() > 10, "particles changed slabs"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_slab_step_in_one_process_holds_particles_by_owner(precision):
+    """lbrb_slab_step with particles: the same exchange by peer copies; each
+    slab holds only its own particles"""
+    npart = 300
+    kw = params(precision, nprtcl=npart, noutconfig=5, record_slots=64, beta=0.5)
+    (f, g), m = developed(precision)
+    with lb.Run(**kw) as whole, lb.SlabDomain((20, 17, 11), **kw) as dom:
+        for d in (whole, dom):
+            d.set_populations(f, g)
+            d.set_moments(m["rho"], m["u"], m["v"], m["T"])
+            seed(d, npart, 9)
+        counts0 = dom.slab_counts()
+        assert sum(counts0) == npart and max(counts0) < npart
+        for n in (1, 2, 3, 150):
+            whole.step(n)
+            dom.step(n)
+            pw, ps = whole.get_particles(), dom.get_particles()
+            for k in pw:
+                np.testing.assert_array_equal(ps[k], pw[k])
+            sw, rw = whole.drain_records_array()
+            ss, rs = dom.drain_records_array()
+            np.testing.assert_array_equal(ss, sw)
+            np.testing.assert_array_equal(rs, rw)
+        assert sum(dom.slab_counts()) == npart
+
+
+def test_one_slab_rank_of_the_whole_domain():
+    """a single rank: the ring messages go to itself (run_distributed, world 1)"""
+    torch = pytest.importorskip("torch")
+    npart = 200
+    kw = params("fp32", nprtcl=npart, noutconfig=4, record_slots=64)
+    (f, g), m = developed("fp32")
+    with lb.Run(**kw) as whole, lb.SlabDomain((NY,), **kw) as dom:
+        for d in (whole, dom):
+            d.set_populations(f, g)
+            d.set_moments(m["rho"], m["u"], m["v"], m["T"])
+            seed(d, npart, 2)
+        (rank,) = ranks_of(dom, torch)
+        whole.step(40)
+        slabrank.run_distributed(rank, 40, None, 0, 1)
+        torch.cuda.synchronize()
+        pw, ps = whole.get_particles(), dom.get_particles()
+        for k in pw:
+            np.testing.assert_array_equal(ps[k], pw[k])
+        np.testing.assert_array_equal(dom.drain_records_array()[1], whole.drain_records_array()[1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_slab_ranks_two_steps_per_exchange_without_particles(precision):
+    torch = pytest.importorskip("torch")
+    with lb.Run(**params(precision)) as whole, lb.SlabDomain((20, 17, 11), **params(precision)) as dom:
+        whole.init_conduction(19, 3e-2)
+        dom.init_conduction(19, 3e-2)
+        ranks = ranks_of(dom, torch, pairs=True)
+        for n in (1, 8, 33):
+            whole.step(n)
+            slabrank.run_local(ranks, n)
+            torch.cuda.synchronize()
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+
+
+def test_missing_message_and_full_list_are_reported():
+    torch = pytest.importorskip("torch")
+    npart = 300
+    kw = params("fp32", nprtcl=npart)
+    (f, g), m = developed("fp32")
+    # a moment message that never arrives: the receiver's header is stale
+    with lb.SlabDomain((24, 24), **kw) as dom:
+        dom.set_populations(f, g)
+        dom.set_moments(m["rho"], m["u"], m["v"], m["T"])
+        seed(dom, npart, 3)
+        ranks = ranks_of(dom, torch)
+        slabrank.run_local(ranks, 3)
+        torch.cuda.synchronize()
+        a, b = dom.slabs
+        for r in (a, b):
+            r.slab_pack()
+        # (the ghost exchange and the step, then no moment exchange)
+        bufs = [slabrank.device_buffers(r, torch) for r in (a, b)]
+        bufs[1]["ghost_lo"].copy_(bufs[0]["up"])
+        bufs[0]["ghost_hi"].copy_(bufs[1]["down"])
+        for r in (a, b):
+            r.step(1)
+            r.slab_moments_pack()
+            r.slab_particles_step()
+        torch.cuda.synchronize()
+        with pytest.raises(lb.LbrbError) as e:
+            a.sync()
+        assert e.value.code == lb.ERR_CODES["LBRB_ERR_STATE"]
+    # a hand-off list of one record while many particles cross
+    with lb.SlabDomain((24, 24), **kw) as dom:
+        dom.set_populations(f, g)
+        dom.set_moments(m["rho"], m["u"], m["v"], m["T"])
+        rng = np.random.default_rng(1)
+        y = 24.9 + rng.uniform(-0.05, 0.05, npart)  # all beside the inner edge, moving across it
+        dom.set_particles(np.arange(npart, dtype=np.int32), rng.uniform(1, NX, npart), y, np.zeros(npart),
+                          np.where(np.arange(npart) % 2 == 0, 0.8, -0.8), np.zeros(npart, np.int32),
+                          np.zeros(npart), handoff_capacity=1)
+        ranks = ranks_of(dom, torch)
+        slabrank.run_local(ranks, 2)
+        torch.cuda.synchronize()
+        codes = []
+        for r in dom.slabs:
+            try:
+                r.sync()
+            except lb.LbrbError as err:
+                codes.append(err.code)
+        assert lb.ERR_CODES["LBRB_ERR_OVERFLOW"] in codes
