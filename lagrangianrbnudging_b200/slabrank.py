@@ -25,7 +25,8 @@ rank over torch.distributed point-to-point operations (NCCL on GPUs, gloo on
 CPU); `run_local` drives several ranks of one process in lockstep with
 copies (slabs on one GPU, or a test).  Message buffers are torch tensors of
 bytes: device memory of the handle (`device_buffers`), or host arrays of a
-stand-in slab in a CPU test.
+stand-in slab in a CPU test.  On GPUs the handles' work and the exchange
+share one stream (`bind_stream`).
 """
 from __future__ import annotations
 
@@ -166,6 +167,22 @@ def run_local(ranks: list, n: int, local_copy: Callable[[Any, Any], None] | None
                     copy(reqs[up][e].lo, ex.up)
                 if dn is not None:
                     copy(reqs[dn][e].hi, ex.down)
+
+
+def bind_stream(runs, torch, stream=None):
+    """Queue every handle's work on one torch stream (a new one of the first
+    handle's device by default) and return it.  Run the drivers under
+    `torch.cuda.stream(stream)`: the copies between slabs and the NCCL
+    operations are then ordered against the handles' kernels.  (A handle
+    given stream 0 keeps its own non-blocking stream, which the legacy
+    default stream does not order against, so that stream is refused.)"""
+    if stream is None:
+        stream = torch.cuda.Stream(device=torch.device("cuda", runs[0].p.device))
+    if stream.cuda_stream == 0:
+        raise ValueError("the slab exchange needs a stream other than the legacy default stream")
+    for r in runs:
+        r.set_stream(stream.cuda_stream)
+    return stream
 
 
 def device_buffers(run, torch) -> dict:

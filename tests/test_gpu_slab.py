@@ -99,7 +99,7 @@ def test_slab_mode_rejects_what_it_does_not_cover():
             r.slab_particles_step()  # no particles set
         r.slab_particles_set(np.arange(8, dtype=np.int32), np.full(8, 5.0), np.linspace(1.5, 40.0, 8),
                              np.zeros(8), np.zeros(8), np.zeros(8, np.int32), np.zeros(8))
-        assert r.slab_particles_count() == 6  # (y in the whole domain: cells in rows 0-23)
+        assert r.slab_particles_count() == 5  # (y in the whole domain: cells in rows 0-23)
         with pytest.raises(lb.LbrbError):
             r.slab_moments_pack()  # after the slab's step
         r.slab_pack()

@@ -44,12 +44,17 @@ def developed(precision):
 
 
 def ranks_of(dom, torch, pairs=False):
-    st = torch.cuda.current_stream().cuda_stream
-    out = []
-    for r in dom.slabs:
-        r.set_stream(st)  # the handles' work in order with the copies between them
-        out.append(slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=dom.np > 0, pairs=pairs))
-    return out
+    """the slabs as ranks, their work on one stream with the copies between
+    them (run the drivers under torch.cuda.stream(dom.stream))"""
+    dom.stream = slabrank.bind_stream(dom.slabs, torch)
+    return [slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=dom.np > 0, pairs=pairs)
+            for r in dom.slabs]
+
+
+def drive(dom, ranks, n, torch):
+    with torch.cuda.stream(dom.stream):
+        slabrank.run_local(ranks, n)
+    torch.cuda.synchronize()
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
@@ -69,8 +74,7 @@ def test_slab_ranks_match_the_whole_domain(precision, heights, beta, full):
         ranks = ranks_of(dom, torch)
         for n in (1, 6, 90, 200):
             whole.step(n)
-            slabrank.run_local(ranks, n)
-            torch.cuda.synchronize()
+            drive(dom, ranks, n, torch)
             for r in dom.slabs:
                 r.sync()
             pw, ps = whole.get_particles(), dom.get_particles()
@@ -131,7 +135,8 @@ def test_one_slab_rank_of_the_whole_domain():
             seed(d, npart, 2)
         (rank,) = ranks_of(dom, torch)
         whole.step(40)
-        slabrank.run_distributed(rank, 40, None, 0, 1)
+        with torch.cuda.stream(dom.stream):
+            slabrank.run_distributed(rank, 40, None, 0, 1)
         torch.cuda.synchronize()
         pw, ps = whole.get_particles(), dom.get_particles()
         for k in pw:
@@ -148,8 +153,7 @@ def test_slab_ranks_two_steps_per_exchange_without_particles(precision):
         ranks = ranks_of(dom, torch, pairs=True)
         for n in (1, 8, 33):
             whole.step(n)
-            slabrank.run_local(ranks, n)
-            torch.cuda.synchronize()
+            drive(dom, ranks, n, torch)
             fw, gw = whole.get_populations()
             fs, gs = dom.get_populations()
             np.testing.assert_array_equal(fs, fw)
@@ -167,19 +171,19 @@ def test_missing_message_and_full_list_are_reported():
         dom.set_moments(m["rho"], m["u"], m["v"], m["T"])
         seed(dom, npart, 3)
         ranks = ranks_of(dom, torch)
-        slabrank.run_local(ranks, 3)
-        torch.cuda.synchronize()
+        drive(dom, ranks, 3, torch)
         a, b = dom.slabs
-        for r in (a, b):
-            r.slab_pack()
-        # (the ghost exchange and the step, then no moment exchange)
-        bufs = [slabrank.device_buffers(r, torch) for r in (a, b)]
-        bufs[1]["ghost_lo"].copy_(bufs[0]["up"])
-        bufs[0]["ghost_hi"].copy_(bufs[1]["down"])
-        for r in (a, b):
-            r.step(1)
-            r.slab_moments_pack()
-            r.slab_particles_step()
+        with torch.cuda.stream(dom.stream):
+            for r in (a, b):
+                r.slab_pack()
+            # (the ghost exchange and the step, then no moment exchange)
+            bufs = [slabrank.device_buffers(r, torch) for r in (a, b)]
+            bufs[1]["ghost_lo"].copy_(bufs[0]["up"])
+            bufs[0]["ghost_hi"].copy_(bufs[1]["down"])
+            for r in (a, b):
+                r.step(1)
+                r.slab_moments_pack()
+                r.slab_particles_step()
         torch.cuda.synchronize()
         with pytest.raises(lb.LbrbError) as e:
             a.sync()
@@ -194,8 +198,7 @@ def test_missing_message_and_full_list_are_reported():
                           np.where(np.arange(npart) % 2 == 0, 0.8, -0.8), np.zeros(npart, np.int32),
                           np.zeros(npart), handoff_capacity=1)
         ranks = ranks_of(dom, torch)
-        slabrank.run_local(ranks, 2)
-        torch.cuda.synchronize()
+        drive(dom, ranks, 2, torch)
         codes = []
         for r in dom.slabs:
             try:
