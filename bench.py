@@ -254,18 +254,18 @@ def kernel_sources_sha() -> str:
 
 
 def profiled_traffic(precision: str, kernel: str):
-    """DRAM bytes per node of one launch of `kernel` from the committed ncu
-    summary (profiles/lb_step_traffic.json), or None when that capture was
-    made on other kernel sources than this build's or on another kernel."""
+    """DRAM bytes per node of one launch of `kernel` ("lb_pair_kernel<float>",
+    ...) from the committed ncu summary (profiles/lb_step_traffic.json: per
+    precision, an entry per kernel), or None when that capture was made on
+    other kernel sources than this build's or holds no such kernel."""
     p = ROOT / "profiles" / "lb_step_traffic.json"
     if not p.exists():
         return None
     try:
         d = json.loads(p.read_text())
-        e = d[precision]
-        if d.get("kernel_sources_sha") != kernel_sources_sha() or e.get("kernel") != kernel:
+        if d.get("kernel_sources_sha") != kernel_sources_sha():
             return None
-        return float(e["bytes_per_node"])
+        return float(d[precision][kernel]["bytes_per_node"])
     except Exception:
         return None
 
@@ -1073,15 +1073,48 @@ def run_slab_bench(lb, torch, device: int, steps: int = SLAB_STEPS, devices=None
 
     with lb.Run(**pk, device=device) as whole:
         ms1, p1, r1 = timed_p(whole, whole.set_stream)
+    # each slab holds the particles in its rows (owner arrays, hand-off lists
+    # between neighbours each step)
+    for n in (2, 4):
+        with lb.SlabDomain([NY // n] * n, devices=devices, **pk, device=device) as dom:
+            ms, p2, r2 = timed_p(dom, lambda st: [r.set_stream(st) for r in dom.slabs])
+            counts = dom.slab_counts()
+            for r in dom.slabs:
+                r.set_stream(None)
+        exact = all(np.array_equal(p1[k], p2[k]) for k in p1) and all(np.array_equal(a, b) for a, b in zip(r1, r2))
+        out[f"particles_{n}_slabs"] = {"nprtcl": NPRTCL, "records_every": NOUTCONFIG,
+                                       "single_handle_mlups": round(nodes * steps / (ms1 * 1e3), 1),
+                                       "mlups": round(nodes * steps / (ms * 1e3), 1),
+                                       "vs_single_handle": round(ms1 / ms, 4), "particles_per_slab": counts,
+                                       "bit_exact_particles_records": bool(exact)}
+    # the one-process-per-GPU protocol (lagrangianrbnudging_b200.slabrank),
+    # its ranks' sends done as copies on one GPU: per step a ghost exchange
+    # (with the last step's hand-off lists), the step, a moment exchange and
+    # the particle step, one step per launch
+    from lagrangianrbnudging_b200 import slabrank
     with lb.SlabDomain([NY // 2] * 2, devices=devices, **pk, device=device) as dom:
-        ms, p2, r2 = timed_p(dom, lambda st: [r.set_stream(st) for r in dom.slabs])
+        st = slabrank.bind_stream(dom.slabs, torch, stream)
+        init_run(dom, SEED)
+        ranks = [slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=True) for r in dom.slabs]
+        with torch.cuda.stream(st):
+            slabrank.run_local(ranks, 20)
+        dom.drain_records_array()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            e0.record(st)
+            slabrank.run_local(ranks, steps)
+            e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        p2, r2 = dom.get_particles(), dom.drain_records_array()
         for r in dom.slabs:
             r.set_stream(None)
     exact = all(np.array_equal(p1[k], p2[k]) for k in p1) and all(np.array_equal(a, b) for a, b in zip(r1, r2))
-    out["particles_2_slabs"] = {"nprtcl": NPRTCL, "records_every": NOUTCONFIG,
-                                "single_handle_mlups": round(nodes * steps / (ms1 * 1e3), 1),
-                                "mlups": round(nodes * steps / (ms * 1e3), 1), "vs_single_handle": round(ms1 / ms, 4),
-                                "bit_exact_particles_records": bool(exact)}
+    out["rank_protocol_2_slabs"] = {"nprtcl": NPRTCL, "mlups": round(nodes * steps / (ms * 1e3), 1),
+                                    "vs_single_handle": round(ms1 / ms, 4),
+                                    "bit_exact_particles_records": bool(exact),
+                                    "note": "one step per exchange; across GPUs the copies are NCCL send/recv"}
     out["note"] = ("slabs on one GPU and one stream: the figure is the exchange's overhead; "
                    "across GPUs each slab runs on its own device")
     return out
