@@ -232,7 +232,7 @@ static void free_sp(SlabParts* S) {
   for (int b = 0; b < 2; b++) {
     F(S->P[b]); F(S->id[b]); F(S->type[b]);
   }
-  F(S->cnt); F(S->cls); F(S->bcnt); F(S->rows); F(S->zrow); F(S->d_rec); F(S->d_rid); F(S->d_rcnt);
+  F(S->cnt); F(S->cls); F(S->bcnt); F(S->done); F(S->rows); F(S->zrow); F(S->d_rec); F(S->d_rid); F(S->d_rcnt);
   for (void* q : S->mom) F(q);
   for (void* q : S->hand) F(q);
   if (S->h_rec) cudaFreeHost(S->h_rec);
@@ -1651,7 +1651,7 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
   }
   long cap = capacity > 0 ? capacity : std::max(n, 1);
   cap = (cap + 127) / 128 * 128;
-  if ((long)keep.size() > cap || cap > (1L << 28))
+  if ((long)keep.size() > cap || cap > (1L << 22))
     return fail(h, LBRB_ERR_ARG, "slab_particles_set: capacity below the slab's particles or too large");
   const int xcap = handoff_capacity > 0 ? handoff_capacity : (int)std::min(cap, 1024L);
   CK(h, cudaSetDevice(h->dev));
@@ -1669,7 +1669,7 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
   bool bad = false;
   for (int b = 0; b < 2; b++)
     bad = bad || dalloc(&S.P[b], 9 * C) || dalloc(&S.id[b], C) || dalloc(&S.type[b], C);
-  bad = bad || dalloc(&S.cnt, 2) || dalloc(&S.cls, C) || dalloc(&S.bcnt, 3 * (C / 128)) ||
+  bad = bad || dalloc(&S.cnt, 2) || dalloc(&S.cls, C) || dalloc(&S.bcnt, 3 * (C / 128)) || dalloc(&S.done, 1) ||
         cudaMalloc(&S.rows, (size_t)OWN_TABLES * nyT * sizeof(void*)) != cudaSuccess ||
         cudaMalloc(&S.zrow, (size_t)h->pitch * h->esize) != cudaSuccess;
   for (int m = 0; m < 4 && !bad; m++)
@@ -1702,6 +1702,7 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
     CK(h, cudaMemsetAsync(S.hand[m], 0, S.hand_bytes, h->stream));
   }
   CK(h, cudaMemsetAsync(S.cls, 3, C, h->stream));
+  CK(h, cudaMemsetAsync(S.done, 0, sizeof(unsigned), h->stream));
   // the kept particles, in the order given
   const size_t k = keep.size();
   std::vector<double> P(9 * C, 0.0);
@@ -1754,8 +1755,9 @@ int lbrb_slab_moments_pack(lbrb_t* h) {
     return fail(h, LBRB_ERR_STATE, "slab_moments_pack: once per step, after lbrb_step(h, 1)");
   CK(h, cudaSetDevice(h->dev));
   CK(h, launch_slab_mom_pack(h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->uv[h->uvprev][0], h->uv[h->uvprev][1],
-                             h->T[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, S.mom[0], S.mom[1], S.mom_pstride,
-                             h->istep, h->slab_j0, h->stream));
+                             h->T[h->cur], fp32(h), h->p.nx, h->p.ny, h->pitch, S.dst_mom[0] ? S.dst_mom[0] : S.mom[0],
+                             S.dst_mom[1] ? S.dst_mom[1] : S.mom[1], S.mom_pstride, h->istep, h->slab_j0, h->stream,
+                             !h->timing));
   S.mom_step = h->istep;
   return LBRB_OK;
 }
@@ -1782,10 +1784,11 @@ int lbrb_slab_particles_step(lbrb_t* h) {
                           tab + (size_t)(6 + h->uvprev) * nyT, tab + (size_t)(9 + h->uvprev) * nyT,
                           tab + (size_t)(12 + h->cur) * nyT};
   const int tm = tmark_begin(h, 1, h->stream);
-  CK(h, launch_own_particles(rows5, fp32(h), h->p.nx, nyT, S, h->slab_j0, h->p.ny, istep, h->p.beta, rec ? 1 : 0,
-                             h->p.record_full, rec ? S.d_rec + (size_t)slot * per : nullptr,
+  CK(h, launch_own_particles(rows5, fp32(h), h->p.nx, nyT, S, S.dst_hand[0] ? S.dst_hand[0] : S.hand[0],
+                             S.dst_hand[1] ? S.dst_hand[1] : S.hand[1], h->slab_j0, h->p.ny, istep, h->p.beta,
+                             rec ? 1 : 0, h->p.record_full, rec ? S.d_rec + (size_t)slot * per : nullptr,
                              rec ? S.d_rid + (size_t)slot * S.cap : nullptr, rec ? S.d_rcnt + slot : nullptr,
-                             h->dflags, h->stream));
+                             h->dflags, h->stream, !h->timing));
   tmark_end(h, tm, h->stream);
   S.pc ^= 1;
   if (rec) {
@@ -1816,7 +1819,7 @@ int lbrb_slab_particles_recv(lbrb_t* h) {
     return fail(h, LBRB_ERR_STATE, "slab_particles_recv: once per step, after lbrb_slab_particles_step");
   CK(h, cudaSetDevice(h->dev));
   const int tm = tmark_begin(h, 1, h->stream);
-  CK(h, launch_own_recv(S, h->slab_j0, h->p.ny, h->slab_ny_total, h->istep, h->dflags, h->stream));
+  CK(h, launch_own_recv(S, h->slab_j0, h->p.ny, h->slab_ny_total, h->istep, h->dflags, h->stream, !h->timing));
   tmark_end(h, tm, h->stream);
   S.recv_step = h->istep;
   return LBRB_OK;
@@ -1942,25 +1945,31 @@ static int slab_pair_launch(lbrb_t* h, bool rec1, bool rec2, bool last) {
 // every row of the domain a pointer to that row of T (2 buffers) in the slab
 // that holds it.  Kernels on one device read the other slabs' rows through
 // peer access.
+// peer access between every pair of the slabs' GPUs (kernels of one slab
+// then read or write another slab's memory); false if a pair cannot have it
+static bool peers_on(lbrb_t* const* slabs, int n) {
+  for (int s = 0; s < n; s++)
+    for (int t = 0; t < n; t++) {
+      const int a = slabs[s]->dev, b = slabs[t]->dev;
+      if (a == b) continue;
+      int ok = 0;
+      if (cudaDeviceCanAccessPeer(&ok, a, b) != cudaSuccess || !ok) return false;
+      if (cudaSetDevice(a) != cudaSuccess) return false;
+      const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
+      if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
+      else if (e != cudaSuccess) return false;
+    }
+  return true;
+}
+
 static int slab_nudge_tables(lbrb_t* const* slabs, int n) {
   lbrb_t* h0 = slabs[0];
   std::vector<const void*> sig(slabs, slabs + n);
   bool fresh = true;
   for (int s = 0; s < n; s++) fresh = fresh && slabs[s]->slab_sig == sig;
   if (fresh) return LBRB_OK;
-  for (int s = 0; s < n; s++)
-    for (int t = 0; t < n; t++) {
-      const int a = slabs[s]->dev, b = slabs[t]->dev;
-      if (a == b) continue;
-      int ok = 0;
-      CK(slabs[s], cudaDeviceCanAccessPeer(&ok, a, b));
-      if (!ok)
-        return fail(slabs[s], LBRB_ERR_UNSUPPORTED, "slab_step: nudging needs peer access between the slabs' GPUs");
-      CK(slabs[s], cudaSetDevice(a));
-      const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
-      if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
-      else if (e != cudaSuccess) return fail(slabs[s], LBRB_ERR_CUDA, "slab_step: peer access", e);
-    }
+  if (!peers_on(slabs, n))
+    return fail(slabs[0], LBRB_ERR_UNSUPPORTED, "slab_step: nudging needs peer access between the slabs' GPUs");
   const int nyT = h0->slab_ny_total;
   std::vector<const void*> tab((size_t)2 * nyT);
   for (int t = 0; t < n; t++) {
@@ -1988,11 +1997,15 @@ static int slab_nudge_tables(lbrb_t* const* slabs, int n) {
 }
 
 // The particles of one step of a slab domain in one process, after every
-// slab's fused kernel: the exchange a process per GPU does over NCCL, done
-// with peer copies around the ring of slabs (up to s + 1, down to s - 1,
-// periodic).  Each copy into a neighbour's message waits for the
-// neighbour's last read of it (its previous particle step, or receive).
-static int slab_owner_particles(lbrb_t* const* slabs, int n) {
+// slab's fused kernel: the exchange a process per GPU does over NCCL, around
+// the ring of slabs (up to s + 1, down to s - 1, periodic).  `direct` (the
+// slabs' GPUs reach each other's memory): the moment-row pack and the
+// particle step write straight into the neighbours' receive buffers; else
+// each slab's messages are peer-copied there.  A write into a neighbour's
+// buffer waits for the neighbour's last read of it: the moment messages were
+// last read by its previous particle step (ev_part), the hand-off lists by
+// its previous receive, which comes before its moment pack (ev_mom).
+static int slab_owner_particles(lbrb_t* const* slabs, int n, bool direct) {
   auto up = [&](int s) { return slabs[(s + 1) % n]; };
   auto dn = [&](int s) { return slabs[(s + n - 1) % n]; };
   auto wait_nb = [&](lbrb_t* h, int s, auto ev) -> int {
@@ -2006,39 +2019,57 @@ static int slab_owner_particles(lbrb_t* const* slabs, int n) {
   // 1. moment messages
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
+    SlabParts& S = *h->sp;
     CK(h, cudaSetDevice(h->dev));
     int rc = wait_nb(h, s, ev_part);
-    if (!rc) rc = lbrb_slab_moments_pack(h);
     if (rc) return rc;
-    CK(h, cudaMemcpyPeerAsync(up(s)->sp->mom[2], up(s)->dev, h->sp->mom[0], h->dev, h->sp->mom_up_bytes, h->stream));
-    CK(h, cudaMemcpyPeerAsync(dn(s)->sp->mom[3], dn(s)->dev, h->sp->mom[1], h->dev, h->sp->mom_down_bytes,
-                              h->stream));
-    CK(h, cudaEventRecord(h->sp->ev_mom, h->stream));
+    if (direct) {
+      S.dst_mom[0] = up(s)->sp->mom[2];
+      S.dst_mom[1] = dn(s)->sp->mom[3];
+    }
+    rc = lbrb_slab_moments_pack(h);
+    S.dst_mom[0] = S.dst_mom[1] = nullptr;
+    if (rc) return rc;
+    if (!direct) {
+      CK(h, cudaMemcpyPeerAsync(up(s)->sp->mom[2], up(s)->dev, S.mom[0], h->dev, S.mom_up_bytes, h->stream));
+      CK(h, cudaMemcpyPeerAsync(dn(s)->sp->mom[3], dn(s)->dev, S.mom[1], h->dev, S.mom_down_bytes, h->stream));
+    }
+    CK(h, cudaEventRecord(S.ev_mom, h->stream));
   }
-  // 2. each slab's particles
+  // 2. each slab's particles (and, direct, its hand-off lists into the neighbours)
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
+    SlabParts& S = *h->sp;
     CK(h, cudaSetDevice(h->dev));
     int rc = wait_nb(h, s, ev_mom);
-    if (!rc) rc = lbrb_slab_particles_step(h);
     if (rc) return rc;
-    CK(h, cudaEventRecord(h->sp->ev_part, h->stream));
-  }
-  // 3. hand-off lists
-  for (int s = 0; s < n; s++) {
-    lbrb_t* h = slabs[s];
-    CK(h, cudaSetDevice(h->dev));
-    const int rc = wait_nb(h, s, ev_part);
+    if (direct) {
+      S.dst_hand[0] = up(s)->sp->hand[2];
+      S.dst_hand[1] = dn(s)->sp->hand[3];
+    }
+    rc = lbrb_slab_particles_step(h);
+    S.dst_hand[0] = S.dst_hand[1] = nullptr;
     if (rc) return rc;
-    CK(h, cudaMemcpyPeerAsync(up(s)->sp->hand[2], up(s)->dev, h->sp->hand[0], h->dev, h->sp->hand_bytes, h->stream));
-    CK(h, cudaMemcpyPeerAsync(dn(s)->sp->hand[3], dn(s)->dev, h->sp->hand[1], h->dev, h->sp->hand_bytes, h->stream));
-    CK(h, cudaEventRecord(h->sp->ev_hand, h->stream));
+    CK(h, cudaEventRecord(S.ev_part, h->stream));
   }
+  // 3. hand-off lists (copies)
+  if (!direct)
+    for (int s = 0; s < n; s++) {
+      lbrb_t* h = slabs[s];
+      CK(h, cudaSetDevice(h->dev));
+      const int rc = wait_nb(h, s, ev_part);
+      if (rc) return rc;
+      CK(h, cudaMemcpyPeerAsync(up(s)->sp->hand[2], up(s)->dev, h->sp->hand[0], h->dev, h->sp->hand_bytes,
+                                h->stream));
+      CK(h, cudaMemcpyPeerAsync(dn(s)->sp->hand[3], dn(s)->dev, h->sp->hand[1], h->dev, h->sp->hand_bytes,
+                                h->stream));
+      CK(h, cudaEventRecord(h->sp->ev_hand, h->stream));
+    }
   // 4. each slab appends what it received
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
     CK(h, cudaSetDevice(h->dev));
-    int rc = wait_nb(h, s, ev_hand);
+    int rc = wait_nb(h, s, direct ? ev_part : ev_hand);
     if (!rc) rc = lbrb_slab_particles_recv(h);
     if (rc) return rc;
   }
@@ -2077,6 +2108,9 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
     const int rc = slab_nudge_tables(slabs, n);
     if (rc) return rc;
   }
+  // particle messages written straight into the neighbours' buffers when
+  // every slab's GPU reaches the others' memory (one GPU: always)
+  const bool direct = parts && peers_on(slabs, n);
   // records pending in the fullest slab ring (every slab records the same steps)
   auto ring_used = [&]() -> long {
     long m = 0;
@@ -2144,7 +2178,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
         }
       }
       if (parts) {
-        const int rc = slab_owner_particles(slabs, n);
+        const int rc = slab_owner_particles(slabs, n, direct);
         if (rc) return rc;
       }
     }
@@ -2216,7 +2250,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
     // 4. the particles of the step (each slab's next fused kernel runs after
     //    its receive on its stream)
     if (parts) {
-      const int rc = slab_owner_particles(slabs, n);
+      const int rc = slab_owner_particles(slabs, n, direct);
       if (rc) return rc;
     }
   }

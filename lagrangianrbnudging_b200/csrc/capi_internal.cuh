@@ -49,12 +49,13 @@ cudaError_t launch_particles_pair(const void* const* fields_a, const void* const
 // received lists
 cudaError_t launch_slab_mom_pack(const void* u, const void* v, const void* ub, const void* vb, const void* T,
                                  bool fp32, int nx, int nyl, int pitch, void* mup, void* mdown, size_t pstride,
-                                 int istep, int j0, cudaStream_t s);
+                                 int istep, int j0, cudaStream_t s, bool pdl);
 cudaError_t launch_own_particles(const void* const* rows5, bool fp32, int nx, int ny_total, const SlabParts& S,
-                                 int j0, int nyl, int istep, double beta, int record, int full, double* rec,
-                                 int* rid, int* rcnt, unsigned* dflags, cudaStream_t s);
+                                 void* hand_up, void* hand_down, int j0, int nyl, int istep, double beta, int record,
+                                 int full, double* rec, int* rid, int* rcnt, unsigned* dflags, cudaStream_t s,
+                                 bool pdl);
 cudaError_t launch_own_recv(const SlabParts& S, int j0, int nyl, int nyT, int istep, unsigned* dflags,
-                            cudaStream_t s);
+                            cudaStream_t s, bool pdl);
 // y-slabs: Trows = device table of T row pointers, one per global row
 cudaError_t launch_bilinear_nudge_slab(const void* Trows, void* g, bool fp32, size_t plane, int nx, int ny_total,
                                        int j0, int nyl, int pitch, const double* ox, const double* oy,

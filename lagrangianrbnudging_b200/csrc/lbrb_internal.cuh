@@ -288,9 +288,15 @@ struct SlabParts {
   int* cnt = nullptr;       // device: [0] particles kept by the last step, [1] with the received ones
   unsigned char* cls = nullptr;  // [cap]: 0 kept, 1 up, 2 down, 3 none
   int* bcnt = nullptr;      // [cap / 128][3] block counts, then offsets
+  unsigned* done = nullptr; // blocks of the particle step finished (reset by its last block)
   void* mom[4] = {nullptr, nullptr, nullptr, nullptr};   // up, down (sent), lo, hi (received)
   void* hand[4] = {nullptr, nullptr, nullptr, nullptr};  // up, down (sent), lo, hi (received)
   size_t mom_pstride = 0, mom_up_bytes = 0, mom_down_bytes = 0, hand_bytes = 0;
+  // where the moment rows and hand-off lists are written (up, down): the
+  // slab's own send buffers, or, inside lbrb_slab_step, the neighbours'
+  // receive buffers directly (null: own)
+  void* dst_mom[2] = {nullptr, nullptr};
+  void* dst_hand[2] = {nullptr, nullptr};
   void* rows = nullptr;     // device: OWN_TABLES x ny_total row pointers
   void* zrow = nullptr;     // a row of zeros (rows outside the slab's reach)
   // records: per slot nrec_fields x cap doubles, cap ids and the count

@@ -58,8 +58,8 @@ __global__ void __launch_bounds__(128) particle_pair_kernel(const PView<Real> Va
 // rows (slab_mom_pack_kernel): own_step_kernel advances the slab's particles,
 // reading the fields through row tables (own rows, the neighbours' rows
 // from the moment messages, a zero row elsewhere) and classifies each by the
-// cell it ends in; own_scan_kernel turns the per-block counts into offsets;
-// own_scatter_kernel compacts the kept particles, in order, into the other
+// cell it ends in, and its last block turns the per-block counts into
+// offsets; own_scatter_kernel compacts the kept particles, in order, into the other
 // buffer and writes the leavers, in order, into the hand-off lists; after
 // the exchange of the lists own_recv_kernel appends the particles from below
 // and then those from above.  A particle's arithmetic is particle_update's,
@@ -77,19 +77,65 @@ __device__ __forceinline__ bool in_reach(int j, int j0, int nyl, int nyT) {
 }
 
 struct OwnArgs {
-  const int* cnt;
+  int* cnt;
   const int* id;
   int* rid;         // record ids (record steps) or null
   int* rcnt;        // record count (record steps) or null
   unsigned char* cls;
   int* bcnt;
-  int j0, nyl, istep;
+  unsigned* done;   // blocks finished (the last one scans; it resets this)
+  int j0, nyl, istep, xcap;
   const SlabMsg* mlo;  // moment rows from the slab below
   const SlabMsg* mhi;  // from the slab above
+  SlabMsg* hup;        // hand-off headers written (own lists or the neighbours' received ones)
+  SlabMsg* hdown;
 };
+
+// The last block of own_step_kernel to finish turns the per-block counts
+// into exclusive offsets (each of its threads scans a run of consecutive
+// blocks) and writes the kept count and the hand-off headers: the pattern of
+// a reduction whose last block, found by an atomic counter after a memory
+// fence, finishes it (no block waits for another).
+__device__ void own_scan_last(const OwnArgs& A, unsigned* dflags) {
+  __shared__ int s[3][128];
+  const int t = threadIdx.x, nblk = gridDim.x;
+  const int per = (nblk + 127) / 128;
+  const int b0 = min(nblk, t * per), b1 = min(nblk, b0 + per);
+  int loc[3] = {0, 0, 0};
+  for (int b = b0; b < b1; b++)
+    for (int k = 0; k < 3; k++) loc[k] += __ldcg(A.bcnt + b * 3 + k);
+  for (int k = 0; k < 3; k++) s[k][t] = loc[k];
+  __syncthreads();
+  for (int off = 1; off < 128; off <<= 1) {
+    int v[3];
+    for (int k = 0; k < 3; k++) v[k] = t >= off ? s[k][t - off] : 0;
+    __syncthreads();
+    for (int k = 0; k < 3; k++) s[k][t] += v[k];
+    __syncthreads();
+  }
+  int run[3];
+  for (int k = 0; k < 3; k++) run[k] = s[k][t] - loc[k];
+  for (int b = b0; b < b1; b++)
+    for (int k = 0; k < 3; k++) {
+      const int c = __ldcg(A.bcnt + b * 3 + k);
+      A.bcnt[b * 3 + k] = run[k];
+      run[k] += c;
+    }
+  if (t == 127) {
+    const int kept = s[0][127], up = s[1][127], down = s[2][127];
+    A.cnt[0] = kept;
+    A.cnt[1] = kept;
+    if (up > A.xcap || down > A.xcap) atomicOr(dflags, DFLAG_XCAP);
+    const int j1 = A.j0 + A.nyl;
+    *A.hup = SlabMsg{min(up, A.xcap), A.istep, A.j0, j1, MSG_HAND_UP, {0, 0, 0}};
+    *A.hdown = SlabMsg{min(down, A.xcap), A.istep, A.j0, j1, MSG_HAND_DOWN, {0, 0, 0}};
+    *A.done = 0u;  // (for the next launch)
+  }
+}
 
 template <typename Real, bool DERIVS>
 __global__ void __launch_bounds__(128) own_step_kernel(const PView<Real> V, const OwnArgs A) {
+  pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;  // (the grid covers the capacity)
   const int n = A.cnt[1], nyT = V.ny;
   if (p == 0) {
@@ -124,50 +170,18 @@ __global__ void __launch_bounds__(128) own_step_kernel(const PView<Real> V, cons
   }
   A.cls[p] = (unsigned char)c;
   const int k0 = __syncthreads_count(c == 0), k1 = __syncthreads_count(c == 1), k2 = __syncthreads_count(c == 2);
+  __shared__ bool last;
   if (threadIdx.x == 0) {
     A.bcnt[blockIdx.x * 3 + 0] = k0;
     A.bcnt[blockIdx.x * 3 + 1] = k1;
     A.bcnt[blockIdx.x * 3 + 2] = k2;
+    __threadfence();
+    last = atomicAdd(A.done, 1u) == gridDim.x - 1;
   }
-}
-
-// one block: exclusive offsets of the per-block counts (each thread scans a
-// run of consecutive blocks), the kept count and the hand-off headers
-__global__ void __launch_bounds__(1024)
-    own_scan_kernel(int* __restrict__ bcnt, int nblk, int* __restrict__ cnt, SlabMsg* hup, SlabMsg* hdown, int xcap,
-                    int istep, int j0, int j1, unsigned* dflags) {
-  __shared__ int s[3][1024];
-  const int t = threadIdx.x;
-  const int per = (nblk + 1023) / 1024;
-  const int b0 = min(nblk, t * per), b1 = min(nblk, b0 + per);
-  int loc[3] = {0, 0, 0};
-  for (int b = b0; b < b1; b++)
-    for (int k = 0; k < 3; k++) loc[k] += bcnt[b * 3 + k];
-  for (int k = 0; k < 3; k++) s[k][t] = loc[k];
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    int v[3];
-    for (int k = 0; k < 3; k++) v[k] = t >= off ? s[k][t - off] : 0;
-    __syncthreads();
-    for (int k = 0; k < 3; k++) s[k][t] += v[k];
-    __syncthreads();
-  }
-  int run[3];
-  for (int k = 0; k < 3; k++) run[k] = s[k][t] - loc[k];
-  for (int b = b0; b < b1; b++)
-    for (int k = 0; k < 3; k++) {
-      const int c = bcnt[b * 3 + k];
-      bcnt[b * 3 + k] = run[k];
-      run[k] += c;
-    }
-  if (t == 1023) {
-    const int kept = s[0][1023], up = s[1][1023], down = s[2][1023];
-    cnt[0] = kept;
-    cnt[1] = kept;
-    if (up > xcap || down > xcap) atomicOr(dflags, DFLAG_XCAP);
-    *hup = SlabMsg{min(up, xcap), istep, j0, j1, MSG_HAND_UP, {0, 0, 0}};
-    *hdown = SlabMsg{min(down, xcap), istep, j0, j1, MSG_HAND_DOWN, {0, 0, 0}};
-  }
+  if (!last) return;
+  __threadfence();
+  own_scan_last(A, V.dflags);
 }
 
 __device__ __forceinline__ void put_rec(HandoffRec* r, const double* __restrict__ P, int cap, int p, int id,
@@ -183,6 +197,7 @@ __global__ void __launch_bounds__(128)
                        const unsigned char* __restrict__ cls, const int* __restrict__ bcnt, double* __restrict__ P2,
                        int* __restrict__ id2, int* __restrict__ type2, HandoffRec* __restrict__ up,
                        HandoffRec* __restrict__ down, int xcap) {
+  pdl_wait();
   __shared__ int wc[3][4];
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -212,6 +227,7 @@ __global__ void __launch_bounds__(128)
                     const SlabMsg* hlo, const HandoffRec* __restrict__ rlo, const SlabMsg* hhi,
                     const HandoffRec* __restrict__ rhi, int xcap, int istep, int j0, int j1, int nyT,
                     unsigned* dflags) {
+  pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const SlabMsg lo = *hlo, hi = *hhi;
   const bool ok = lo.kind == MSG_HAND_UP && lo.step == istep && wrapi(lo.j1, nyT) == j0 && lo.count >= 0 &&
@@ -245,6 +261,7 @@ __global__ void __launch_bounds__(256)
     slab_mom_pack_kernel(const Real* __restrict__ u, const Real* __restrict__ v, const Real* __restrict__ ub,
                          const Real* __restrict__ vb, const Real* __restrict__ T, int nx, int nyl, int pitch,
                          char* mup, char* mdown, size_t pstride, int istep, int j0) {
+  pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int q = blockIdx.y;  // plane: 0-2 up, 3-10 down
   if (q == 0 && i == 0) {
@@ -274,55 +291,48 @@ __global__ void __launch_bounds__(256)
 
 cudaError_t launch_slab_mom_pack(const void* u, const void* v, const void* ub, const void* vb, const void* T,
                                  bool fp32, int nx, int nyl, int pitch, void* mup, void* mdown, size_t pstride,
-                                 int istep, int j0, cudaStream_t s) {
+                                 int istep, int j0, cudaStream_t s, bool pdl) {
   const dim3 g((nx + 255) / 256, MOM_UP_PLANES + MOM_DOWN_PLANES);
   if (fp32)
-    slab_mom_pack_kernel<float><<<g, 256, 0, s>>>((const float*)u, (const float*)v, (const float*)ub,
-                                                   (const float*)vb, (const float*)T, nx, nyl, pitch, (char*)mup,
-                                                   (char*)mdown, pstride, istep, j0);
-  else
-    slab_mom_pack_kernel<double><<<g, 256, 0, s>>>((const double*)u, (const double*)v, (const double*)ub,
-                                                    (const double*)vb, (const double*)T, nx, nyl, pitch, (char*)mup,
-                                                    (char*)mdown, pstride, istep, j0);
-  return cudaGetLastError();
+    return launch_k(slab_mom_pack_kernel<float>, g, 256, 0, s, pdl, (const float*)u, (const float*)v,
+                    (const float*)ub, (const float*)vb, (const float*)T, nx, nyl, pitch, (char*)mup, (char*)mdown,
+                    pstride, istep, j0);
+  return launch_k(slab_mom_pack_kernel<double>, g, 256, 0, s, pdl, (const double*)u, (const double*)v,
+                  (const double*)ub, (const double*)vb, (const double*)T, nx, nyl, pitch, (char*)mup, (char*)mdown,
+                  pstride, istep, j0);
 }
 
 cudaError_t launch_own_particles(const void* const* rows5, bool fp32, int nx, int ny_total, const SlabParts& S,
-                                 int j0, int nyl, int istep, double beta, int record, int full, double* rec,
-                                 int* rid, int* rcnt, unsigned* dflags, cudaStream_t s) {
+                                 void* hand_up, void* hand_down, int j0, int nyl, int istep, double beta, int record,
+                                 int full, double* rec, int* rid, int* rcnt, unsigned* dflags, cudaStream_t s,
+                                 bool pdl) {
   const int nblk = S.cap / 128, o = S.pc;
-  OwnArgs A{S.cnt, S.id[o], rid, rcnt, S.cls, S.bcnt, j0, nyl, istep,
-            (const SlabMsg*)S.mom[2], (const SlabMsg*)S.mom[3]};
+  OwnArgs A{S.cnt, S.id[o], rid, rcnt, S.cls, S.bcnt, S.done, j0, nyl, istep, S.xcap,
+            (const SlabMsg*)S.mom[2], (const SlabMsg*)S.mom[3], (SlabMsg*)hand_up, (SlabMsg*)hand_down};
   auto go = [&](auto zero) -> cudaError_t {
     using Real = decltype(zero);
     using Rows = const Real* const*;
     PView<Real> V{nullptr, nullptr, nullptr, nullptr, nullptr, nx, ny_total, 0, S.P[o], S.type[o], S.cap, beta,
                   record, full, rec, dflags, (Rows)rows5[0], (Rows)rows5[1], (Rows)rows5[2], (Rows)rows5[3],
                   (Rows)rows5[4]};
-    if (beta != 0.0 || full) own_step_kernel<Real, true><<<nblk, 128, 0, s>>>(V, A);
-    else own_step_kernel<Real, false><<<nblk, 128, 0, s>>>(V, A);
-    return cudaGetLastError();
+    if (beta != 0.0 || full) return launch_k(own_step_kernel<Real, true>, nblk, 128, 0, s, pdl, V, A);
+    return launch_k(own_step_kernel<Real, false>, nblk, 128, 0, s, pdl, V, A);
   };
   cudaError_t e = fp32 ? go(0.f) : go(0.0);
   if (e != cudaSuccess) return e;
-  own_scan_kernel<<<1, 1024, 0, s>>>(S.bcnt, nblk, S.cnt, (SlabMsg*)S.hand[0], (SlabMsg*)S.hand[1], S.xcap, istep,
-                                     j0, j0 + nyl, dflags);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  own_scatter_kernel<<<nblk, 128, 0, s>>>(S.P[o], S.id[o], S.type[o], S.cap, S.cls, S.bcnt, S.P[o ^ 1],
-                                          S.id[o ^ 1], S.type[o ^ 1],
-                                          (HandoffRec*)((char*)S.hand[0] + HAND_RECS_OFF),
-                                          (HandoffRec*)((char*)S.hand[1] + HAND_RECS_OFF), S.xcap);
-  return cudaGetLastError();
+  return launch_k(own_scatter_kernel, nblk, 128, 0, s, pdl, (const double*)S.P[o], (const int*)S.id[o],
+                  (const int*)S.type[o], S.cap, (const unsigned char*)S.cls, (const int*)S.bcnt, S.P[o ^ 1],
+                  S.id[o ^ 1], S.type[o ^ 1], (HandoffRec*)((char*)hand_up + HAND_RECS_OFF),
+                  (HandoffRec*)((char*)hand_down + HAND_RECS_OFF), S.xcap);
 }
 
 cudaError_t launch_own_recv(const SlabParts& S, int j0, int nyl, int nyT, int istep, unsigned* dflags,
-                            cudaStream_t s) {
+                            cudaStream_t s, bool pdl) {
   const int o = S.pc;
-  own_recv_kernel<<<(2 * S.xcap + 127) / 128, 128, 0, s>>>(
-      S.P[o], S.id[o], S.type[o], S.cap, S.cnt, (const SlabMsg*)S.hand[2],
-      (const HandoffRec*)((const char*)S.hand[2] + HAND_RECS_OFF), (const SlabMsg*)S.hand[3],
-      (const HandoffRec*)((const char*)S.hand[3] + HAND_RECS_OFF), S.xcap, istep, j0, j0 + nyl, nyT, dflags);
-  return cudaGetLastError();
+  return launch_k(own_recv_kernel, (2 * S.xcap + 127) / 128, 128, 0, s, pdl, S.P[o], S.id[o], S.type[o], S.cap,
+                  S.cnt, (const SlabMsg*)S.hand[2], (const HandoffRec*)((const char*)S.hand[2] + HAND_RECS_OFF),
+                  (const SlabMsg*)S.hand[3], (const HandoffRec*)((const char*)S.hand[3] + HAND_RECS_OFF), S.xcap,
+                  istep, j0, j0 + nyl, nyT, dflags);
 }
 
 cudaError_t launch_particles_pair(const void* const* fields_a, const void* const* fields_b, bool fp32, int nx,
