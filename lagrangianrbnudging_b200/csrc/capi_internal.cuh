@@ -9,6 +9,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include "lbrb_internal.cuh"
+#include "slab_parts.cuh"
 
 namespace lbrb {
 // an NVTX range over a C-ABI call (free when no tool is attached)

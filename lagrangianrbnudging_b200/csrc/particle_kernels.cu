@@ -17,6 +17,7 @@
 // at its 4 cell corners from a 4x4 stencil of u, v and the 2x2 u^{n-1}.
 // Built with --fmad=false: the FP64 results match the reference bit for bit.
 #include "particle_dev.cuh"
+#include "slab_parts.cuh"
 
 namespace lbrb {
 
