@@ -960,9 +960,11 @@ int lbrb_step(lbrb_t* h, int n) {
     }
     if (nud) {
       const int tm = tmark_begin(h, 2, h->stream);
-      CK(h, launch_bilinear_nudge(h->T[dst], pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, o2, o2 + no,
-                                  o2 + 2 * no, h->nobs, h->p.alpha, h->acc, h->dflags, h->stream, pdl_ok));
-      CK(h, launch_obs_clear(nx, ny, h->pitch, o1, o1 + no, h->nobs, h->acc2, h->nmask, h->stream, pdl_ok));
+      // step n+1's scatter, then its apply pass together with the clearing
+      // of step n's in-launch sums
+      CK(h, launch_bilinear_nudge_clear(h->T[dst], pop_base(h, dst, 1), f32, h->plane, nx, ny, h->pitch, o2, o2 + no,
+                                        o2 + 2 * no, h->nobs, h->p.alpha, h->acc, o1, o1 + no, h->acc2, h->nmask,
+                                        h->dflags, h->stream, pdl_ok));
       tmark_end(h, tm, h->stream);
     }
     if (parts) {

@@ -77,8 +77,12 @@ cudaError_t launch_obs_pre_fp32(const LBView<float>& V, const double* ox, const 
 cudaError_t launch_obs_pre_fp64(const LBView<double>& V, const double* ox, const double* oy, const double* oT,
                                 int nobs, double alpha, long long* acc, unsigned* mask, unsigned* dflags,
                                 cudaStream_t s, bool pdl);
-cudaError_t launch_obs_clear(int nx, int ny, int pitch, const double* ox, const double* oy, int nobs, long long* acc,
-                             unsigned* mask, cudaStream_t s, bool pdl);
+// after a nudged two-step launch: step n+1's scatter and apply pass, and
+// the clearing of step n's in-launch sums (acc2) and mask bits
+cudaError_t launch_bilinear_nudge_clear(void* T, void* g, bool fp32, size_t plane, int nx, int ny, int pitch,
+                                        const double* ox, const double* oy, const double* oT, int nobs, double alpha,
+                                        long long* acc, const double* ox1, const double* oy1, long long* acc2,
+                                        unsigned* mask, unsigned* dflags, cudaStream_t s, bool pdl);
 cudaError_t launch_pops_in(const double* h, int layout, void* d, bool fp32, int nx, int ny,
                            int pitch, size_t plane, double base, cudaStream_t s);
 cudaError_t launch_pops_out(const void* d, int layout, double* h, bool fp32, int nx, int ny,

@@ -135,6 +135,69 @@ __device__ __forceinline__ void obs_pre_one(const LBView<Real>& V, double xx, do
     for (int ix : {ix1, ix2}) atomicOr(&mask[(size_t)jy * words + (ix >> 5)], 1u << (ix & 31));
 }
 
+// T^n at node (i, j) as the fused step forms it: the sum of the g streaming
+// into the node (Dirichlet walls, no slab ghost rows), in the step's order --
+// the g half of pull_node and dirichlet_walls
+template <typename Real>
+__device__ __forceinline__ Real pulled_T(const LBView<Real>& V, int j, int i) {
+  const int xl = (i == 0) ? V.nx - 1 : i - 1, xr = (i == V.nx - 1) ? 0 : i + 1;
+  Real gs[NPOP];
+  static_for<NPOP>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    const int xs = icx(k) == 1 ? xl : (icx(k) == -1 ? xr : i);
+    const int js = j - icy(k);
+    gs[k] = (js < 0 || js >= V.ny) ? Real(0) : V.gsrc[(size_t)k * V.plane + (size_t)js * V.pitch + xs];
+  });
+  dirichlet_walls(V, j, gs);
+  if constexpr (std::is_same<Real, double>::value) {
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < NPOP; k++) t = t + gs[k];
+    return t;
+  } else {
+    float dT = 0.f;
+#pragma unroll
+    for (int k = 0; k < NPOP; k++) dT += gs[k];
+    return V.T0_f + dT;
+  }
+}
+
+// obs_pre_one with four threads per observation (lanes 4p .. 4p+3 of a warp,
+// one per cell corner): each forms its corner's T^n, the group shares them
+// by shuffles, every lane forms the innovation with obs_scatter_rows'
+// expressions, and each adds its own corner's share and mask bit.  The sums
+// and bits are obs_pre_one's, bit for bit.  All 32 lanes of the warp must
+// call it (live: the lane's observation exists).
+template <typename Real>
+__device__ __forceinline__ void obs_pre_corner(const LBView<Real>& V, bool live, double xx, double yy, double Tobs,
+                                               double alpha, int corner, unsigned long long* __restrict__ acc,
+                                               unsigned* __restrict__ mask, unsigned* dflags) {
+  const int nx = V.nx, ny = V.ny;
+  const bool inr = live && xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0;
+  if (live && !inr && corner == 0) atomicOr(dflags, DFLAG_RANGE);
+  int x1, y1, ix1, ix2, jy1, jy2;
+  obs_cell(inr ? xx : 1.0, inr ? yy : 1.0, nx, ny, x1, y1, ix1, ix2, jy1, jy2);
+  const int ix = (corner & 1) ? ix2 : ix1, jy = (corner >> 1) ? jy2 : jy1;
+  const Real Tc = inr ? pulled_T(V, jy, ix) : Real(0);
+  const int base = (threadIdx.x & 31) & ~3;
+  const double u11 = (double)__shfl_sync(0xffffffffu, Tc, base + 0);
+  const double u21 = (double)__shfl_sync(0xffffffffu, Tc, base + 1);
+  const double u12 = (double)__shfl_sync(0xffffffffu, Tc, base + 2);
+  const double u22 = (double)__shfl_sync(0xffffffffu, Tc, base + 3);
+  if (!inr) return;
+  const int x2 = x1 + 1, y2 = y1 + 1;
+  const double val1 = u11 * ((double)x2 - xx) * ((double)y2 - yy);
+  const double val2 = u21 * (xx - (double)x1) * ((double)y2 - yy);
+  const double val3 = u12 * ((double)x2 - xx) * (yy - (double)y1);
+  const double val4 = u22 * (xx - (double)x1) * (yy - (double)y1);
+  const double tm = val1 + val2 + val3 + val4;
+  const double dlt = alpha * (Tobs - tm);
+  const double wx = (corner & 1) ? xx - (double)x1 : (double)x2 - xx;
+  const double wy = (corner >> 1) ? yy - (double)y1 : (double)y2 - yy;
+  atomicAdd(&acc[(size_t)jy * V.pitch + ix], (unsigned long long)__double2ll_rn(dlt * (wx * wy) * FIX_SCALE));
+  atomicOr(&mask[(size_t)jy * (V.pitch >> 5) + (ix >> 5)], 1u << (ix & 31));
+}
+
 // after the launch: clear corner `corner` (0..3) of an observation of step n
 __device__ __forceinline__ void obs_clear_one(int nx, int ny, int pitch, double xx, double yy, int corner,
                                               unsigned long long* __restrict__ acc, unsigned* __restrict__ mask) {

@@ -293,47 +293,70 @@ __global__ void obs_apply_kernel(Real* __restrict__ g, size_t plane, int nx, int
   obs_apply_one(g, plane, nx, ny, pitch, ox[p], oy[p], t & 3, acc);
 }
 
-// Two-step launch of a nudged run: step n's innovations before the launch,
-// and the clearing of their sums and mask bits after it (nudge_dev.cuh)
+// Two-step launch of a nudged run: step n's innovations before the launch
+// (four threads per observation, obs_pre_corner in nudge_dev.cuh), and the
+// clearing of their sums and mask bits after it
 template <typename Real>
-__global__ void obs_pre_kernel(const LBView<Real> V, const double* __restrict__ ox, const double* __restrict__ oy,
-                               const double* __restrict__ oT, int nobs, double alpha,
-                               unsigned long long* __restrict__ acc, unsigned* __restrict__ mask, unsigned* dflags) {
+__global__ void __launch_bounds__(128) obs_pre4_kernel(const LBView<Real> V, const double* __restrict__ ox,
+                                                       const double* __restrict__ oy, const double* __restrict__ oT,
+                                                       int nobs, double alpha, unsigned long long* __restrict__ acc,
+                                                       unsigned* __restrict__ mask, unsigned* dflags) {
   pdl_wait();
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nobs) return;
-  obs_pre_one(V, ox[p], oy[p], oT[p], alpha, acc, mask, dflags);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = t >> 2;
+  const bool live = p < nobs;
+  obs_pre_corner(V, live, live ? ox[p] : 0.0, live ? oy[p] : 0.0, live ? oT[p] : 0.0, alpha, t & 3, acc, mask,
+                 dflags);
 }
 
-__global__ void obs_clear_kernel(int nx, int ny, int pitch, const double* __restrict__ ox,
-                                 const double* __restrict__ oy, int nobs, unsigned long long* __restrict__ acc,
-                                 unsigned* __restrict__ mask) {
+// after a nudged two-step launch: step n+1's apply pass (acc) and the
+// clearing of step n's in-launch sums and mask bits (acc2, mask) in one
+// launch -- corner t & 3 of observation t >> 2 of each step
+template <typename Real>
+__global__ void obs_apply_clear_kernel(Real* __restrict__ g, size_t plane, int nx, int ny, int pitch,
+                                       const double* __restrict__ ox2, const double* __restrict__ oy2, int nobs,
+                                       unsigned long long* __restrict__ acc, const double* __restrict__ ox1,
+                                       const double* __restrict__ oy1, unsigned long long* __restrict__ acc2,
+                                       unsigned* __restrict__ mask) {
   pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 4 * nobs) return;
   const int p = t >> 2;
-  obs_clear_one(nx, ny, pitch, ox[p], oy[p], t & 3, acc, mask);
+  obs_apply_one(g, plane, nx, ny, pitch, ox2[p], oy2[p], t & 3, acc);
+  obs_clear_one(nx, ny, pitch, ox1[p], oy1[p], t & 3, acc2, mask);
 }
 
 cudaError_t launch_obs_pre_fp32(const LBView<float>& V, const double* ox, const double* oy, const double* oT,
                                 int nobs, double alpha, long long* acc, unsigned* mask, unsigned* dflags,
                                 cudaStream_t s, bool pdl) {
   if (nobs <= 0) return cudaSuccess;
-  return launch_k(obs_pre_kernel<float>, (nobs + 127) / 128, 128, 0, s, pdl, V, ox, oy, oT, nobs, alpha,
+  return launch_k(obs_pre4_kernel<float>, (4 * nobs + 127) / 128, 128, 0, s, pdl, V, ox, oy, oT, nobs, alpha,
                   reinterpret_cast<unsigned long long*>(acc), mask, dflags);
 }
 cudaError_t launch_obs_pre_fp64(const LBView<double>& V, const double* ox, const double* oy, const double* oT,
                                 int nobs, double alpha, long long* acc, unsigned* mask, unsigned* dflags,
                                 cudaStream_t s, bool pdl) {
   if (nobs <= 0) return cudaSuccess;
-  return launch_k(obs_pre_kernel<double>, (nobs + 127) / 128, 128, 0, s, pdl, V, ox, oy, oT, nobs, alpha,
+  return launch_k(obs_pre4_kernel<double>, (4 * nobs + 127) / 128, 128, 0, s, pdl, V, ox, oy, oT, nobs, alpha,
                   reinterpret_cast<unsigned long long*>(acc), mask, dflags);
 }
-cudaError_t launch_obs_clear(int nx, int ny, int pitch, const double* ox, const double* oy, int nobs, long long* acc,
-                             unsigned* mask, cudaStream_t s, bool pdl) {
+cudaError_t launch_bilinear_nudge_clear(void* T, void* g, bool fp32, size_t plane, int nx, int ny, int pitch,
+                                        const double* ox, const double* oy, const double* oT, int nobs, double alpha,
+                                        long long* acc, const double* ox1, const double* oy1, long long* acc2,
+                                        unsigned* mask, unsigned* dflags, cudaStream_t s, bool pdl) {
   if (nobs <= 0) return cudaSuccess;
-  return launch_k(obs_clear_kernel, (4 * nobs + 127) / 128, 128, 0, s, pdl, nx, ny, pitch, ox, oy, nobs,
-                  reinterpret_cast<unsigned long long*>(acc), mask);
+  const int tb = 128;
+  unsigned long long* a = reinterpret_cast<unsigned long long*>(acc);
+  unsigned long long* a2 = reinterpret_cast<unsigned long long*>(acc2);
+  auto go = [&](auto zero) -> cudaError_t {
+    using Real = decltype(zero);
+    cudaError_t e = launch_k(obs_scatter_kernel<Real>, (nobs + tb - 1) / tb, tb, 0, s, pdl, (const Real*)T, nx, ny,
+                             pitch, ox, oy, oT, nobs, alpha, a, dflags);
+    if (e != cudaSuccess) return e;
+    return launch_k(obs_apply_clear_kernel<Real>, (4 * nobs + tb - 1) / tb, tb, 0, s, pdl, (Real*)g, plane, nx, ny,
+                    pitch, ox, oy, nobs, a, ox1, oy1, a2, mask);
+  };
+  return fp32 ? go(0.f) : go(0.0);
 }
 
 // y-slab: the observations' innovations read T of the whole domain through
