@@ -137,18 +137,20 @@ __global__ void __launch_bounds__(32 * (R + 1), MINB)
 }
 
 // step n's innovations of the nudged members, before the pair's launch
-// (ctr[0] steps of this call done)
+// (ctr[0] steps of this call done): 4 threads per observation, one per cell
+// corner (obs_pre_corner; every lane of a warp takes part)
 template <typename Real>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(4 * ENS_OCHUNK)
     ens_pre_kernel(const LBView<Real>* __restrict__ views1, const EnsAux<Real>* __restrict__ aux1,
                    const int2* __restrict__ ochunks, const int* __restrict__ ctr) {
   pdl_wait();
   const int2 c = ochunks[blockIdx.x];
   const EnsAux<Real>& A = aux1[c.x];
-  const int o = c.y + threadIdx.x;
-  if (o >= A.nobs) return;
+  const int o = c.y + (threadIdx.x >> 2);
+  const bool live = o < A.nobs;
   const double* ob = ens_obs_row(A, ctr[0]);
-  obs_pre_one(views1[c.x], ob[o], ob[A.nobs + o], ob[2 * A.nobs + o], A.alpha, A.acc2, A.nmask, A.dflags);
+  obs_pre_corner(views1[c.x], live, live ? ob[o] : 0.0, live ? ob[A.nobs + o] : 0.0,
+                 live ? ob[2 * A.nobs + o] : 0.0, A.alpha, threadIdx.x & 3, A.acc2, A.nmask, A.dflags);
 }
 
 // every member's particles of both steps; step n+1's innovations
@@ -239,9 +241,9 @@ cudaError_t launch_ens_pre(bool f32, const void* views1, const void* aux1, const
                            const int* ctr, cudaStream_t s) {
   if (nochunks <= 0) return cudaSuccess;
   if (f32)
-    return launch_k(ens_pre_kernel<float>, nochunks, ENS_OCHUNK, 0, s, true, (const LBView<float>*)views1,
+    return launch_k(ens_pre_kernel<float>, nochunks, 4 * ENS_OCHUNK, 0, s, true, (const LBView<float>*)views1,
                     (const EnsAux<float>*)aux1, ochunks, ctr);
-  return launch_k(ens_pre_kernel<double>, nochunks, ENS_OCHUNK, 0, s, true, (const LBView<double>*)views1,
+  return launch_k(ens_pre_kernel<double>, nochunks, 4 * ENS_OCHUNK, 0, s, true, (const LBView<double>*)views1,
                   (const EnsAux<double>*)aux1, ochunks, ctr);
 }
 

@@ -98,43 +98,6 @@ __device__ __forceinline__ void obs_apply_one(Real* __restrict__ g, size_t plane
   }
 }
 
-// Two-step launch of a nudged run, before the launch: the innovation of one
-// observation of step n from T^n at its cell corners.  T^n is the moment of
-// the populations streaming into a corner -- pulled from the state before
-// the step (V's sources), walls applied, summed as the fused step sums them
-// -- so it equals the T the step itself forms.  The sums go to acc (fixed
-// point, as a single step's scatter) and the corners' bits to the node mask
-// (pitch / 32 words per row), which the two-step kernels read to add the
-// sums after the collision.
-template <typename Real>
-__device__ __forceinline__ void obs_pre_one(const LBView<Real>& V, double xx, double yy, double Tobs, double alpha,
-                                            unsigned long long* __restrict__ acc, unsigned* __restrict__ mask,
-                                            unsigned* dflags) {
-  const int nx = V.nx, ny = V.ny, words = V.pitch >> 5;
-  auto Tat = [&](int j, int i) -> Real {
-    Real fs[NPOP], gs[NPOP];
-    pull_node<Real, LBRB_TWALL_DIRICHLET, size_t, true>(V, j, i, fs, gs);
-    dirichlet_walls(V, j, gs);
-    if constexpr (std::is_same<Real, double>::value) {
-      double t = 0.0;
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) t = t + gs[k];
-      return t;
-    } else {
-      float dT = 0.f;
-#pragma unroll
-      for (int k = 0; k < NPOP; k++) dT += gs[k];
-      return V.T0_f + dT;
-    }
-  };
-  obs_scatter_rows(Tat, nx, ny, V.pitch, xx, yy, Tobs, alpha, acc, dflags, 0, ny);
-  if (!(xx > -2.0 && xx < nx + 2.0 && yy > -2.0 && yy < ny + 2.0)) return;
-  int x1, y1, ix1, ix2, jy1, jy2;
-  obs_cell(xx, yy, nx, ny, x1, y1, ix1, ix2, jy1, jy2);
-  for (int jy : {jy1, jy2})
-    for (int ix : {ix1, ix2}) atomicOr(&mask[(size_t)jy * words + (ix >> 5)], 1u << (ix & 31));
-}
-
 // T^n at node (i, j) as the fused step forms it: the sum of the g streaming
 // into the node (Dirichlet walls, no slab ghost rows), in the step's order --
 // the g half of pull_node and dirichlet_walls
@@ -162,12 +125,18 @@ __device__ __forceinline__ Real pulled_T(const LBView<Real>& V, int j, int i) {
   }
 }
 
-// obs_pre_one with four threads per observation (lanes 4p .. 4p+3 of a warp,
-// one per cell corner): each forms its corner's T^n, the group shares them
-// by shuffles, every lane forms the innovation with obs_scatter_rows'
-// expressions, and each adds its own corner's share and mask bit.  The sums
-// and bits are obs_pre_one's, bit for bit.  All 32 lanes of the warp must
-// call it (live: the lane's observation exists).
+// Two-step launch of a nudged run, before the launch: the innovation of one
+// observation of step n from T^n at its cell corners, with four threads per
+// observation (lanes 4p .. 4p+3 of a warp, one per corner).  T^n is the
+// moment of the g populations streaming into a corner -- pulled from the
+// state before the step (V's sources), walls applied, summed as the fused
+// step sums it (pulled_T) -- so it equals the T the step itself forms.  The
+// lanes share their corners' T by shuffles, every lane forms the innovation
+// with obs_scatter_rows' expressions, and each adds its own corner's share
+// to acc (fixed point, as a single step's scatter) and its bit to the node
+// mask (pitch / 32 words per row), which the two-step kernels read to add
+// the sums after the collision.  All 32 lanes of the warp must call it
+// (live: the lane's observation exists).
 template <typename Real>
 __device__ __forceinline__ void obs_pre_corner(const LBView<Real>& V, bool live, double xx, double yy, double Tobs,
                                                double alpha, int corner, unsigned long long* __restrict__ acc,
