@@ -381,9 +381,9 @@ LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, c
  * Supported: Dirichlet walls; particles (held by their owner slab, below);
  * bilinear nudging (not box nudging): every slab holds all observations
  * (lbrb_nudge_obs on each, in the whole domain's coordinates) and
- * lbrb_slab_step applies them; a slab with nudging steps only through
- * lbrb_slab_step.  Create slab handles with nprtcl = 0 (lbrb_slab_set
- * rejects a handle with whole-domain particles). */
+ * lbrb_slab_step applies them (one process per GPU: lbrb_slab_nudge).
+ * Create slab handles with nprtcl = 0 (lbrb_slab_set rejects a handle with
+ * whole-domain particles). */
 LBRB_API int lbrb_slab_set(lbrb_t *h, int j0, int ny_total);
 /* bytes of one packed boundary row set: 6 rows (f then g) of nx values */
 LBRB_API size_t lbrb_slab_ghost_bytes(const lbrb_t *h);
@@ -464,7 +464,10 @@ LBRB_API int lbrb_slab_step(lbrb_t *const *slabs, int nslabs, int nsteps);
  * by lbrb_sync (LBRB_ERR_STATE, LBRB_ERR_RANGE, LBRB_ERR_OVERFLOW).  Calls
  * out of this order return LBRB_ERR_STATE.  A particle's state equals the
  * whole domain's bit for bit; its record goes into the ring of the slab
- * that advanced it. */
+ * that advanced it.
+ * capacity -1 (with n = 0): no particles, only the moment messages, for a
+ * nudged slab without particles (lbrb_slab_particles_step and _recv are
+ * then not called; the other calls of the step stay). */
 LBRB_API int lbrb_slab_particles_set(lbrb_t *h, int n, const int *ids, const double *x, const double *y,
                                      const double *u, const double *v, const int *ptype, const double *invtau,
                                      int capacity, int handoff_capacity);
@@ -474,6 +477,16 @@ LBRB_API int lbrb_slab_particle_buffers(lbrb_t *h, void **mom_up, void **mom_dow
 LBRB_API int lbrb_slab_moments_pack(lbrb_t *h);
 LBRB_API int lbrb_slab_particles_step(lbrb_t *h);
 LBRB_API int lbrb_slab_particles_recv(lbrb_t *h);
+/* Bilinear nudging of a y-slab stepped by its own process: after
+ * lbrb_step(h, 1), lbrb_slab_moments_pack and the moment exchange, the
+ * step's observations (lbrb_nudge_obs with the whole domain's
+ * coordinates) whose cell has a corner in the slab's rows are interpolated
+ * from T of the slab's rows and of the received moment rows, and their
+ * shares added at the corners in the slab's rows; the slab's g then equals
+ * the whole domain's bit for bit.  Once per step; lbrb_step refuses the next
+ * step of a nudged slab until it ran.  (No reference counterpart as an API:
+ * the reference's nudged run is not decomposed in y in this way.) */
+LBRB_API int lbrb_slab_nudge(lbrb_t *h);
 /* the slab's particle count and state (waits; arrays of at least max_n) */
 LBRB_API int lbrb_slab_particles_count(lbrb_t *h, int *n);
 LBRB_API int lbrb_slab_particles_get(lbrb_t *h, int max_n, int *n, int *ids, double *x, double *y, double *u,

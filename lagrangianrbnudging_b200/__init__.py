@@ -51,7 +51,7 @@ EXPORTS = [
     "lbrb_slab_particles_set", "lbrb_slab_particle_bytes", "lbrb_slab_particle_buffers",
     "lbrb_slab_moments_pack", "lbrb_slab_particles_step", "lbrb_slab_particles_recv",
     "lbrb_slab_particles_count", "lbrb_slab_particles_get", "lbrb_slab_record_pending",
-    "lbrb_slab_record_drain", "lbrb_slab_particle_format",
+    "lbrb_slab_record_drain", "lbrb_slab_particle_format", "lbrb_slab_nudge",
     "lbrb_set_graph", "lbrb_set_pairs", "lbrb_set_pair_shape", "lbrb_get_pair_shape", "lbrb_pair_shapes",
 ]
 
@@ -159,6 +159,7 @@ def lib() -> C.CDLL:
         "lbrb_slab_record_pending": (C.c_int, [vp, ip]),
         "lbrb_slab_record_drain": (C.c_int, [vp, C.c_int, ip, ip, ip, dp]),
         "lbrb_slab_particle_format": (C.c_int, [ip, ip, ip]),
+        "lbrb_slab_nudge": (C.c_int, [vp]),
         "lbrb_set_graph": (C.c_int, [vp, C.c_int]),
         "lbrb_set_pairs": (C.c_int, [vp, C.c_int]),
         "lbrb_set_pair_shape": (C.c_int, [vp, C.c_int]),
@@ -434,6 +435,17 @@ class Run:
 
     def slab_moments_pack(self):
         self._ck(lib().lbrb_slab_moments_pack(self.h))
+
+    def slab_nudge(self):
+        """this step's bilinear nudging at the slab's corners (after the moment exchange)"""
+        self._ck(lib().lbrb_slab_nudge(self.h))
+
+    def slab_messages_only(self):
+        """the moment messages without particles (a nudged slab without particles)"""
+        e = np.empty(0)
+        i = np.empty(0, np.int32)
+        self._ck(lib().lbrb_slab_particles_set(self.h, 0, _ip(i), _dp(e), _dp(e), _dp(e), _dp(e), _ip(i), _dp(e),
+                                               -1, 0))
 
     def slab_particles_step(self):
         self._ck(lib().lbrb_slab_particles_step(self.h))

@@ -57,7 +57,7 @@ static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneVal> g_tuned_single, g_tuned_pair;
 // the steps store u, v every step (and T on record steps) for particles:
 // the whole domain's, or a slab's own (lbrb_slab_particles_set)
-static bool moves_particles(const lbrb_t* h) { return h->np > 0 || h->sp != nullptr; }
+static bool moves_particles(const lbrb_t* h) { return h->np > 0 || (h->sp && h->sp->cap > 0); }
 static TuneKey tune_key(const lbrb_t* h) {
   return {h->dev, h->p.nx, h->p.ny, h->pitch, (int)h->esize, h->p.twall, h->p.nudge, moves_particles(h) ? 1 : 0,
           (h->slab_gh2_lo ? 1 : 0) | (h->slab_gh2_hi ? 2 : 0) | (h->slab ? 4 : 0)};
@@ -770,13 +770,17 @@ int lbrb_step(lbrb_t* h, int n) {
     h->prev_valid = false;
     return LBRB_OK;
   }
-  if (h->slab && (n != 1 || (h->p.nudge != LBRB_NUDGE_NONE && !h->slab_stepping)))
+  if (h->slab && (n != 1 || (h->p.nudge != LBRB_NUDGE_NONE && !h->slab_stepping && !h->sp)))
     return fail(h, LBRB_ERR_ARG,
-                "step: a y-slab takes one step per boundary exchange, or two after lbrb_slab_pack2 (lbrb_slab_step)");
-  if (h->sp && !h->slab_stepping && (h->sp->part_step != h->istep || h->sp->recv_step != h->istep))
+                "step: a y-slab takes one step per boundary exchange, or two after lbrb_slab_pack2 (lbrb_slab_step); "
+                "a nudged slab stepped alone needs the moment messages (lbrb_slab_particles_set)");
+  if (h->sp && !h->slab_stepping && h->sp->cap > 0 &&
+      (h->sp->part_step != h->istep || h->sp->recv_step != h->istep))
     return fail(h, LBRB_ERR_STATE,
                 "step: a slab with particles steps after lbrb_slab_particles_step and lbrb_slab_particles_recv "
                 "of its last step");
+  if (h->sp && !h->slab_stepping && h->p.nudge == LBRB_NUDGE_BILINEAR && h->sp->nudge_step != h->istep)
+    return fail(h, LBRB_ERR_STATE, "step: a nudged slab applies lbrb_slab_nudge after each step");
   if (!h->moments_valid)
     return fail(h, LBRB_ERR_STATE, "step: set the moments (set_moments, moments_from_pre or init_conduction) first");
   if (h->np > 0 && !h->particles_set) return fail(h, LBRB_ERR_STATE, "step: particles not set");
@@ -1637,8 +1641,10 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
                             int handoff_capacity) {
   if (!h) return LBRB_ERR_ARG;
   if (!h->slab) return fail(h, LBRB_ERR_STATE, "slab_particles_set: not a y-slab (lbrb_slab_set)");
-  if (n < 0 || (n > 0 && (!ids || !x || !y || !u || !v || !ptype || !invtau)) || capacity < 0 ||
-      handoff_capacity < 0)
+  // capacity -1: no particles, the moment messages only (bilinear nudging)
+  const bool msg_only = capacity == -1;
+  if (n < 0 || (n > 0 && (!ids || !x || !y || !u || !v || !ptype || !invtau)) || capacity < -1 ||
+      handoff_capacity < 0 || (msg_only && n > 0))
     return fail(h, LBRB_ERR_ARG, "slab_particles_set: bad arguments");
   const int nyT = h->slab_ny_total, j0 = h->slab_j0, nyl = h->p.ny;
   std::vector<int> keep;
@@ -1651,11 +1657,11 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
     const int cr = host_cell_row(y[q], nyT);
     if (cr >= j0 && cr < j0 + nyl) keep.push_back(q);
   }
-  long cap = capacity > 0 ? capacity : std::max(n, 1);
+  long cap = msg_only ? 0 : (capacity > 0 ? capacity : std::max(n, 1));
   cap = (cap + 127) / 128 * 128;
   if ((long)keep.size() > cap || cap > (1L << 22))
     return fail(h, LBRB_ERR_ARG, "slab_particles_set: capacity below the slab's particles or too large");
-  const int xcap = handoff_capacity > 0 ? handoff_capacity : (int)std::min(cap, 1024L);
+  const int xcap = msg_only ? 0 : (handoff_capacity > 0 ? handoff_capacity : (int)std::min(cap, 1024L));
   CK(h, cudaSetDevice(h->dev));
   CK(h, cudaStreamSynchronize(h->stream));
   free_sp(h->sp);
@@ -1667,19 +1673,21 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
   S.mom_pstride = ((size_t)h->p.nx * h->esize + 255) / 256 * 256;
   S.mom_up_bytes = MOM_PLANES_OFF + MOM_UP_PLANES * S.mom_pstride;
   S.mom_down_bytes = MOM_PLANES_OFF + MOM_DOWN_PLANES * S.mom_pstride;
-  S.hand_bytes = HAND_RECS_OFF + (size_t)xcap * sizeof(HandoffRec);
+  S.hand_bytes = msg_only ? 0 : HAND_RECS_OFF + (size_t)xcap * sizeof(HandoffRec);
   bool bad = false;
-  for (int b = 0; b < 2; b++)
-    bad = bad || dalloc(&S.P[b], 9 * C) || dalloc(&S.id[b], C) || dalloc(&S.type[b], C);
-  bad = bad || dalloc(&S.cnt, 2) || dalloc(&S.cls, C) || dalloc(&S.bcnt, 3 * (C / 128)) || dalloc(&S.done, 1) ||
-        cudaMalloc(&S.rows, (size_t)OWN_TABLES * nyT * sizeof(void*)) != cudaSuccess ||
+  if (!msg_only) {
+    for (int b = 0; b < 2; b++)
+      bad = bad || dalloc(&S.P[b], 9 * C) || dalloc(&S.id[b], C) || dalloc(&S.type[b], C);
+    bad = bad || dalloc(&S.cnt, 2) || dalloc(&S.cls, C) || dalloc(&S.bcnt, 3 * (C / 128)) || dalloc(&S.done, 1);
+  }
+  bad = bad || cudaMalloc(&S.rows, (size_t)OWN_TABLES * nyT * sizeof(void*)) != cudaSuccess ||
         cudaMalloc(&S.zrow, (size_t)h->pitch * h->esize) != cudaSuccess;
   for (int m = 0; m < 4 && !bad; m++)
     bad = cudaMalloc(&S.mom[m], (m & 1) ? S.mom_down_bytes : S.mom_up_bytes) != cudaSuccess ||
-          cudaMalloc(&S.hand[m], S.hand_bytes) != cudaSuccess;
+          (!msg_only && cudaMalloc(&S.hand[m], S.hand_bytes) != cudaSuccess);
   const int slots = h->p.record_slots;
   const int nrec = h->p.record_full ? LBRB_REC_NFULL : LBRB_REC_NBASIC;
-  if (!bad && h->p.noutconfig > 0) {
+  if (!bad && !msg_only && h->p.noutconfig > 0) {
     bad = dalloc(&S.d_rec, (size_t)slots * nrec * C) || dalloc(&S.d_rid, (size_t)slots * C) ||
           dalloc(&S.d_rcnt, (size_t)slots) ||
           cudaMallocHost(&S.h_rec, (size_t)slots * nrec * C * sizeof(double)) != cudaSuccess ||
@@ -1701,7 +1709,15 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
   CK(h, cudaMemsetAsync(S.zrow, 0, (size_t)h->pitch * h->esize, h->stream));
   for (int m = 0; m < 4; m++) {
     CK(h, cudaMemsetAsync(S.mom[m], 0, (m & 1) ? S.mom_down_bytes : S.mom_up_bytes, h->stream));
-    CK(h, cudaMemsetAsync(S.hand[m], 0, S.hand_bytes, h->stream));
+    if (!msg_only) CK(h, cudaMemsetAsync(S.hand[m], 0, S.hand_bytes, h->stream));
+  }
+  const std::vector<const void*> tab = own_tables(h);
+  CK(h, cudaMemcpyAsync(S.rows, tab.data(), tab.size() * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
+  S.part_step = S.recv_step = S.nudge_step = h->istep;
+  S.mom_step = -1;
+  if (msg_only) {
+    CK(h, cudaStreamSynchronize(h->stream));
+    return LBRB_OK;
   }
   CK(h, cudaMemsetAsync(S.cls, 3, C, h->stream));
   CK(h, cudaMemsetAsync(S.done, 0, sizeof(unsigned), h->stream));
@@ -1717,15 +1733,11 @@ int lbrb_slab_particles_set(lbrb_t* h, int n, const int* ids, const double* x, c
     T[a] = ptype[q];
   }
   const int cnt[2] = {(int)k, (int)k};
-  const std::vector<const void*> tab = own_tables(h);
   CK(h, cudaMemcpyAsync(S.P[0], P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(S.id[0], I.data(), C * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(S.type[0], T.data(), C * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemcpyAsync(S.cnt, cnt, sizeof(cnt), cudaMemcpyHostToDevice, h->stream));
-  CK(h, cudaMemcpyAsync(S.rows, tab.data(), tab.size() * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
-  S.part_step = S.recv_step = h->istep;
-  S.mom_step = -1;
   return LBRB_OK;
 }
 
@@ -1753,7 +1765,7 @@ int lbrb_slab_moments_pack(lbrb_t* h) {
   if (!h) return LBRB_ERR_ARG;
   if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_moments_pack: no slab particles (lbrb_slab_particles_set)");
   SlabParts& S = *h->sp;
-  if (h->istep != S.part_step + 1)
+  if (S.cap > 0 ? h->istep != S.part_step + 1 : S.mom_step == h->istep)
     return fail(h, LBRB_ERR_STATE, "slab_moments_pack: once per step, after lbrb_step(h, 1)");
   CK(h, cudaSetDevice(h->dev));
   CK(h, launch_slab_mom_pack(h->uv[h->uvcur][0], h->uv[h->uvcur][1], h->uv[h->uvprev][0], h->uv[h->uvprev][1],
@@ -1768,6 +1780,7 @@ int lbrb_slab_particles_step(lbrb_t* h) {
   if (!h) return LBRB_ERR_ARG;
   if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_particles_step: no slab particles (lbrb_slab_particles_set)");
   SlabParts& S = *h->sp;
+  if (S.cap == 0) return fail(h, LBRB_ERR_STATE, "slab_particles_step: the slab holds no particles (capacity -1)");
   if (h->istep != S.part_step + 1 || S.recv_step != S.part_step || S.mom_step != h->istep)
     return fail(h, LBRB_ERR_STATE,
                 "slab_particles_step: once per step, after lbrb_step(h, 1), lbrb_slab_moments_pack and the "
@@ -1817,6 +1830,7 @@ int lbrb_slab_particles_recv(lbrb_t* h) {
   if (!h) return LBRB_ERR_ARG;
   if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_particles_recv: no slab particles (lbrb_slab_particles_set)");
   SlabParts& S = *h->sp;
+  if (S.cap == 0) return fail(h, LBRB_ERR_STATE, "slab_particles_recv: the slab holds no particles (capacity -1)");
   if (S.part_step != h->istep || S.part_step == S.recv_step)
     return fail(h, LBRB_ERR_STATE, "slab_particles_recv: once per step, after lbrb_slab_particles_step");
   CK(h, cudaSetDevice(h->dev));
@@ -1827,11 +1841,45 @@ int lbrb_slab_particles_recv(lbrb_t* h) {
   return LBRB_OK;
 }
 
+// Bilinear nudging of a y-slab stepped by its own process (the in-process
+// lbrb_slab_step reads T through peer tables instead): the step's
+// observations whose cell has a corner in the slab's rows are interpolated
+// from T^n -- the slab's own rows and the received moment messages' T rows,
+// which hold every corner row within one of the slab -- and their shares
+// are scattered to, and applied at, the corners in the slab's rows.  The
+// integer sums do not depend on which slab adds them, so g equals the whole
+// domain's bit for bit.
+int lbrb_slab_nudge(lbrb_t* h) {
+  if (!h) return LBRB_ERR_ARG;
+  if (!h->slab || !h->sp)
+    return fail(h, LBRB_ERR_STATE, "slab_nudge: a y-slab with the moment messages (lbrb_slab_particles_set) only");
+  if (h->p.nudge != LBRB_NUDGE_BILINEAR) return fail(h, LBRB_ERR_STATE, "slab_nudge: bilinear nudging only");
+  SlabParts& S = *h->sp;
+  if (S.mom_step != h->istep || S.nudge_step == h->istep || !h->slab_obs)
+    return fail(h, LBRB_ERR_STATE,
+                "slab_nudge: once per step, after lbrb_step(h, 1), lbrb_slab_moments_pack and the moment exchange");
+  CK(h, cudaSetDevice(h->dev));
+  const int nyT = h->slab_ny_total;
+  const double* obs = h->slab_obs;
+  const void* const* Trows = (const void* const*)S.rows + (size_t)(12 + h->cur) * nyT;
+  const int tm = tmark_begin(h, 2, h->stream);
+  CK(h, launch_bilinear_nudge_slab(Trows, pop_base(h, h->cur, 1), fp32(h), h->plane, h->p.nx, nyT, h->slab_j0,
+                                   h->p.ny, h->pitch, obs, obs + h->nobs, obs + 2 * (size_t)h->nobs, h->nobs,
+                                   h->p.alpha, h->acc, h->dflags, h->stream));
+  tmark_end(h, tm, h->stream);
+  S.nudge_step = h->istep;
+  return LBRB_OK;
+}
+
 int lbrb_slab_particles_count(lbrb_t* h, int* n) {
   if (!h || !n) return LBRB_ERR_ARG;
   if (!h->sp) return fail(h, LBRB_ERR_STATE, "slab_particles_count: no slab particles (lbrb_slab_particles_set)");
   CK(h, cudaSetDevice(h->dev));
   int c = 0;
+  if (h->sp->cap == 0) {
+    *n = 0;
+    return LBRB_OK;
+  }
   CK(h, cudaMemcpyAsync(&c, h->sp->cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   *n = c;
@@ -2091,11 +2139,12 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
   }
   if (slabs[n - 1]->slab_j0 + slabs[n - 1]->p.ny != slabs[0]->slab_ny_total) return LBRB_ERR_ARG;
   lbrb_t* h0 = slabs[0];
-  const bool parts = h0->sp != nullptr;
+  auto holds = [](const lbrb_t* h) { return h->sp != nullptr && h->sp->cap > 0; };
+  const bool parts = holds(h0);
   const bool nudge = h0->p.nudge == LBRB_NUDGE_BILINEAR;
   for (int s = 0; s < n; s++) {
     lbrb_t* h = slabs[s];
-    if ((h->sp != nullptr) != parts)
+    if (holds(h) != parts)
       return fail(h, LBRB_ERR_ARG, "slab_step: every slab or none holds particles (lbrb_slab_particles_set)");
     if (h->p.nudge != h0->p.nudge || h->p.alpha != h0->p.alpha || h->nobs != h0->nobs)
       return fail(h, LBRB_ERR_ARG, "slab_step: slabs differ in nudging");
@@ -2247,6 +2296,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
                                          h->slab_j0, h->p.ny, h->pitch, obs, obs + h->nobs, obs + 2 * (size_t)h->nobs,
                                          h->nobs, h->p.alpha, h->acc, h->dflags, h->stream));
         tmark_end(h, tm, h->stream);
+        if (h->sp) h->sp->nudge_step = h->istep;
       }
     }
     // 4. the particles of the step (each slab's next fused kernel runs after

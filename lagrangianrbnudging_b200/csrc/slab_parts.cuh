@@ -45,7 +45,7 @@ constexpr int MOM_UP_PLANES = 3, MOM_DOWN_PLANES = 8;
 constexpr int OWN_TABLES = 14;
 
 struct SlabParts {
-  int cap = 0;   // particles the slab can hold (a multiple of 128)
+  int cap = 0;   // particles the slab can hold (a multiple of 128; 0: moment messages only)
   int xcap = 0;  // records per hand-off list
   double* P[2] = {nullptr, nullptr};  // [9][cap]: x y u v xo yo uo vo invtau
   int* id[2] = {nullptr, nullptr};
@@ -75,8 +75,9 @@ struct SlabParts {
   std::vector<int> rstep;
   std::vector<cudaEvent_t> rev;
   long rhead = 0, rtail = 0;
-  // protocol: the step of the last moment pack, particle step and receive
-  int mom_step = -1, part_step = 0, recv_step = 0;
+  // protocol: the step of the last moment pack, particle step, receive and
+  // bilinear nudging (lbrb_slab_nudge)
+  int mom_step = -1, part_step = 0, recv_step = 0, nudge_step = 0;
   cudaEvent_t ev_mom = nullptr, ev_part = nullptr, ev_hand = nullptr;
 };
 

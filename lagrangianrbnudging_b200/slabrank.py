@@ -11,6 +11,7 @@ after lbrb_slab_set) and, per step:
     [lbrb_slab_particles_recv]     (the previous step's hand-off lists)
     lbrb_step(h, 1)
     lbrb_slab_moments_pack         moment rows  up -> s+1 lo, down -> s-1 hi (ring)
+    [lbrb_slab_nudge]              (bilinear nudging)
     lbrb_slab_particles_step       hand-off     up -> s+1 lo, down -> s-1 hi (ring)
 
 The hand-off lists of a step travel with the next step's ghost rows (one
@@ -76,13 +77,15 @@ def p2p_ops(dist, ex: Exchange, rank: int, world: int) -> list:
 
 class SlabRank:
     """The protocol of one slab.  `slab` has the lbrb.Run slab methods
-    (slab_pack, slab_pack2, step, slab_moments_pack, slab_particles_step,
-    slab_particles_recv); `bufs` maps the buffer names of `device_buffers`
-    to tensors.  particles: the slab holds particles (every rank alike)."""
+    (slab_pack, slab_pack2, step, slab_moments_pack, slab_nudge,
+    slab_particles_step, slab_particles_recv); `bufs` maps the buffer names
+    of `device_buffers` to tensors.  particles: the slab holds particles;
+    nudging: bilinear nudging (every rank alike; both need the moment
+    messages, lbrb_slab_particles_set)."""
 
-    def __init__(self, slab, bufs: dict, particles: bool, pairs: bool = False):
-        self.slab, self.b, self.particles = slab, bufs, particles
-        self.pairs = pairs and not particles
+    def __init__(self, slab, bufs: dict, particles: bool, pairs: bool = False, nudging: bool = False):
+        self.slab, self.b, self.particles, self.nudging = slab, bufs, particles, nudging
+        self.pairs = pairs and not particles and not nudging
         self.pending = False  # hand-off lists packed, not yet exchanged
 
     def _ghosts(self, two: bool) -> Exchange:
@@ -116,11 +119,14 @@ class SlabRank:
                 self.pending = False
             s.step(2 if two else 1)
             left -= 2 if two else 1
-            if self.particles:
+            if self.particles or self.nudging:
                 s.slab_moments_pack()
                 yield [self._mom()]
-                s.slab_particles_step()
-                self.pending = True
+                if self.nudging:
+                    s.slab_nudge()
+                if self.particles:
+                    s.slab_particles_step()
+                    self.pending = True
         if self.pending:
             yield [self._hand()]
             s.slab_particles_recv()

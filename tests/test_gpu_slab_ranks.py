@@ -206,3 +206,64 @@ def test_missing_message_and_full_list_are_reported():
             except lb.LbrbError as err:
                 codes.append(err.code)
         assert lb.ERR_CODES["LBRB_ERR_OVERFLOW"] in codes
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("npart", [0, 150])
+def test_slab_ranks_with_bilinear_nudging_match_the_whole_domain(precision, npart):
+    """one process per GPU with bilinear nudging (lbrb_slab_nudge after the
+    moment exchange): each slab interpolates T at an observation's corners
+    from its own rows and the received moment rows, and adds the shares at
+    its own corners.  Observations straddle both inner edges and, through
+    the periodic wrap of the cell rows, the walls; with and without
+    particles (a slab without them holds the moment messages only)."""
+    torch = pytest.importorskip("torch")
+    nobs, nst = 90, 5
+    rng = np.random.default_rng(31)
+    ox = rng.uniform(0.0, NX + 1.0, (nst, nobs))
+    oy = rng.uniform(0.5, NY + 0.5, (nst, nobs))
+    oy[:, :9] = [19.5, 20.0, 20.5, 21.0, 36.2, 37.0, 37.9, 0.7, NY + 0.3]
+    oT = rng.uniform(-0.5, 0.5, (nst, nobs))
+    kw = params(precision, nudge="bilinear", alpha=0.3, nobs=nobs, obs_cycle=1, nprtcl=npart,
+                noutconfig=5 if npart else 0, record_slots=64)
+    with lb.Run(**kw) as whole, lb.SlabDomain((20, 17, 11), **kw) as dom:
+        for d in (whole, dom):
+            d.init_conduction(41, 2e-2)
+            d.nudge_obs(1, ox, oy, oT)
+            if npart:
+                seed(d, npart, 8)
+        if not npart:
+            for r in dom.slabs:
+                r.slab_messages_only()
+        dom.stream = slabrank.bind_stream(dom.slabs, torch)
+        ranks = [slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=npart > 0, nudging=True)
+                 for r in dom.slabs]
+        for n in (1, 4, 60):
+            whole.step(n)
+            drive(dom, ranks, n, torch)
+            for r in dom.slabs:
+                r.sync()
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+            if npart:
+                pw, ps = whole.get_particles(), dom.get_particles()
+                for k in pw:
+                    np.testing.assert_array_equal(ps[k], pw[k])
+                np.testing.assert_array_equal(dom.drain_records_array()[1], whole.drain_records_array()[1])
+        # the nudging acted, and a nudged slab does not step on before it ran
+        with lb.Run(**dict(kw, nudge="none", nobs=0)) as free:
+            free.init_conduction(41, 2e-2)
+            if npart:
+                seed(free, npart, 8)
+            free.step(65)
+            assert not np.array_equal(free.get_populations()[1], gw)
+        a = dom.slabs[0]
+        with torch.cuda.stream(dom.stream):
+            a.slab_pack()
+            a.step(1)
+            a.slab_moments_pack()
+            with pytest.raises(lb.LbrbError):
+                a.slab_pack()
+                a.step(1)  # lbrb_slab_nudge of the last step first
