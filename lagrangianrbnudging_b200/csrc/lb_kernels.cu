@@ -146,19 +146,31 @@ __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1
   if (tx >= ncols || ty >= nrows) return;
   const int x = x0 + tx, j = y0 + ty;
   Real fs[NPOP], gs[NPOP];
-  static_for<NPOP>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    const int js = j - icy(k);
-    if ((js < 0 && !glo) || (js >= ny && !ghi)) {
-      fs[k] = S[(opp(k) * RY + ty + 1) * RX + tx + 1];
-      gs[k] = Real(0);
-    } else {
+  // a tile whose rows and their neighbours all lie in the domain (or beyond
+  // an inner slab edge) pulls with no wall rule (block-uniform)
+  const bool inner = (y0 > 0 || glo) && (y0 + nrows < ny || ghi);
+  if (inner) {
+    static_for<NPOP>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
       const int lx = tx + 1 - icx(k), ly = ty + 1 - icy(k);
       fs[k] = S[(k * RY + ly) * RX + lx];
       gs[k] = S[((NPOP + k) * RY + ly) * RX + lx];
-    }
-  });
-  dirichlet_walls(V2, j, gs);
+    });
+  } else {
+    static_for<NPOP>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      const int js = j - icy(k);
+      if ((js < 0 && !glo) || (js >= ny && !ghi)) {
+        fs[k] = S[(opp(k) * RY + ty + 1) * RX + tx + 1];
+        gs[k] = Real(0);
+      } else {
+        const int lx = tx + 1 - icx(k), ly = ty + 1 - icy(k);
+        fs[k] = S[(k * RY + ly) * RX + lx];
+        gs[k] = S[((NPOP + k) * RY + ly) * RX + lx];
+      }
+    });
+    dirichlet_walls(V2, j, gs);
+  }
   lb_finish_node<Real, false, Off>(V2, (Off)j * pitch + (Off)x, fs, gs, SF[ty * TX + tx]);
 }
 
