@@ -1095,7 +1095,8 @@ def run_slab_bench(lb, torch, device: int, steps: int = SLAB_STEPS, devices=None
     with lb.SlabDomain([NY // 2] * 2, devices=devices, **pk, device=device) as dom:
         st = slabrank.bind_stream(dom.slabs, torch, stream)
         init_run(dom, SEED)
-        ranks = [slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=True) for r in dom.slabs]
+        ranks = [slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=True, pairs=True)
+                 for r in dom.slabs]
         with torch.cuda.stream(st):
             slabrank.run_local(ranks, 20)
         dom.drain_records_array()
@@ -1114,7 +1115,8 @@ def run_slab_bench(lb, torch, device: int, steps: int = SLAB_STEPS, devices=None
     out["rank_protocol_2_slabs"] = {"nprtcl": NPRTCL, "mlups": round(nodes * steps / (ms * 1e3), 1),
                                     "vs_single_handle": round(ms1 / ms, 4),
                                     "bit_exact_particles_records": bool(exact),
-                                    "note": "one step per exchange; across GPUs the copies are NCCL send/recv"}
+                                    "note": "two steps per launch, the particle exchange of each step in turn; "
+                                            "across GPUs the copies are NCCL send/recv"}
     out["note"] = ("slabs on one GPU and one stream: the figure is the exchange's overhead; "
                    "across GPUs each slab runs on its own device")
     return out

@@ -450,7 +450,11 @@ LBRB_API int lbrb_slab_step(lbrb_t *const *slabs, int nslabs, int nsteps);
  *   send hand_up -> s+1 hand_lo, hand_down -> s-1 hand_hi;
  *   lbrb_slab_particles_recv.
  * (The hand-off exchange may go with the next step's ghost exchange, with
- * lbrb_slab_particles_recv before the next lbrb_step.)  Sizes are
+ * lbrb_slab_particles_recv before the next lbrb_step.)  Two steps per
+ * launch: lbrb_slab_pack2 and its exchange, lbrb_step(h, 2), then the
+ * moment pack / exchange / particle step / hand-off exchange / receive of
+ * the first step, whose receive moves the handle on to the second step,
+ * and the same again for the second (no nudging).  Sizes are
  * lbrb_slab_particle_bytes (mom_up, mom_down, and each hand-off list); all
  * work and copies on the handle's stream, so a caller's NCCL send/recv on
  * that stream orders itself.  The moment messages carry the fields one row

@@ -752,7 +752,7 @@ int lbrb_step(lbrb_t* h, int n) {
   if (!h || n < 0) return fail(h, LBRB_ERR_ARG, "step: bad arguments");
   NvtxRange nvtx("lbrb_step");
   if (n == 0) return LBRB_OK;
-  if (h->slab && !h->slab_stepping && n == 2 && !moves_particles(h) && h->p.nudge == LBRB_NUDGE_NONE &&
+  if (h->slab && !h->slab_stepping && n == 2 && h->p.nudge == LBRB_NUDGE_NONE &&
       h->p.twall == LBRB_TWALL_DIRICHLET && h->pair_mode != 0) {
     // one process per GPU: two steps from the two-row ghost blocks
     // (lbrb_slab_pack2 and the exchange of lbrb_slab_buffers2 done)
@@ -761,13 +761,33 @@ int lbrb_step(lbrb_t* h, int n) {
     if (!h->slab_gh2_packed)
       return fail(h, LBRB_ERR_STATE,
                   "step: two steps on a y-slab need lbrb_slab_pack2 and the ghost-block exchange first");
+    const bool own = moves_particles(h);  // (the slab holds its own particles)
+    if (own && (h->sp->part_step != h->istep || h->sp->recv_step != h->istep))
+      return fail(h, LBRB_ERR_STATE,
+                  "step: a slab with particles steps after lbrb_slab_particles_step and lbrb_slab_particles_recv "
+                  "of its last step");
     CK(h, cudaSetDevice(h->dev));
-    const int rc = slab_pair_launch(h, false, false, true);
+    const int i1 = h->istep + 1, i2 = h->istep + 2;
+    const bool rec1 = own && h->p.noutconfig > 0 && i1 % h->p.noutconfig == 0;
+    const bool rec2 = own && h->p.noutconfig > 0 && i2 % h->p.noutconfig == 0;
+    const int rc = slab_pair_launch(h, rec1, rec2, true);
     if (rc) return rc;
     h->slab_gh2_packed = false;
-    h->cur ^= 1;
-    h->istep += 2;
     h->prev_valid = false;
+    if (!own) {
+      h->cur ^= 1;
+      h->istep += 2;
+      return LBRB_OK;
+    }
+    // the first step's state (u^n in the free slot, T^n in the source
+    // buffer): its particle exchange runs next, and its
+    // lbrb_slab_particles_recv moves the handle on to the second step's
+    h->pair_save[0] = h->cur, h->pair_save[1] = h->uvcur, h->pair_save[2] = h->uvprev;
+    const int A = 3 - h->uvcur - h->uvprev;
+    h->uvprev = h->uvcur;
+    h->uvcur = A;
+    h->istep = i1;
+    h->sp->pair_pending = true;
     return LBRB_OK;
   }
   if (h->slab && (n != 1 || (h->p.nudge != LBRB_NUDGE_NONE && !h->slab_stepping && !h->sp)))
@@ -1838,6 +1858,15 @@ int lbrb_slab_particles_recv(lbrb_t* h) {
   CK(h, launch_own_recv(S, h->slab_j0, h->p.ny, h->slab_ny_total, h->istep, h->dflags, h->stream, !h->timing));
   tmark_end(h, tm, h->stream);
   S.recv_step = h->istep;
+  if (S.pair_pending) {
+    // the second step of lbrb_step(h, 2): populations and T in the other
+    // buffer, u^{n+1} in the slot of u^{n-2}
+    h->cur = h->pair_save[0] ^ 1;
+    h->uvprev = h->uvcur;
+    h->uvcur = h->pair_save[2];
+    h->istep += 1;
+    S.pair_pending = false;
+  }
   return LBRB_OK;
 }
 

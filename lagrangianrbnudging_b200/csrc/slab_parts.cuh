@@ -78,6 +78,9 @@ struct SlabParts {
   // protocol: the step of the last moment pack, particle step, receive and
   // bilinear nudging (lbrb_slab_nudge)
   int mom_step = -1, part_step = 0, recv_step = 0, nudge_step = 0;
+  // lbrb_step(h, 2) left the handle at the first of its two steps: the
+  // first lbrb_slab_particles_recv moves it on to the second
+  bool pair_pending = false;
   cudaEvent_t ev_mom = nullptr, ev_part = nullptr, ev_hand = nullptr;
 };
 

@@ -17,8 +17,8 @@ after lbrb_slab_set) and, per step:
 The hand-off lists of a step travel with the next step's ghost rows (one
 batch of point-to-point operations); a call of `steps` ends with their own
 exchange and receive, so the slab's particles are complete between calls.
-Without particles, two steps go per exchange (lbrb_slab_pack2, lbrb_step(h,
-2)) when `pairs` is set.
+With `pairs`, two steps go per launch (lbrb_slab_pack2, lbrb_step(h, 2)),
+the particle exchange of each following in turn (no nudging).
 
 `SlabRank.steps(n)` yields, at each exchange, a list of `Exchange`
 requests; a driver fills them and resumes it.  `run_distributed` drives one
@@ -85,7 +85,7 @@ class SlabRank:
 
     def __init__(self, slab, bufs: dict, particles: bool, pairs: bool = False, nudging: bool = False):
         self.slab, self.b, self.particles, self.nudging = slab, bufs, particles, nudging
-        self.pairs = pairs and not particles and not nudging
+        self.pairs = pairs and not nudging
         self.pending = False  # hand-off lists packed, not yet exchanged
 
     def _ghosts(self, two: bool) -> Exchange:
@@ -120,13 +120,20 @@ class SlabRank:
             s.step(2 if two else 1)
             left -= 2 if two else 1
             if self.particles or self.nudging:
-                s.slab_moments_pack()
-                yield [self._mom()]
-                if self.nudging:
-                    s.slab_nudge()
-                if self.particles:
-                    s.slab_particles_step()
-                    self.pending = True
+                # each step of the launch in turn; after a two-step launch the
+                # first step's receive moves the handle on to the second step
+                for q in range(2 if two else 1):
+                    s.slab_moments_pack()
+                    yield [self._mom()]
+                    if self.nudging:
+                        s.slab_nudge()
+                    if self.particles:
+                        s.slab_particles_step()
+                        if two and q == 0:
+                            yield [self._hand()]
+                            s.slab_particles_recv()
+                        else:
+                            self.pending = True
         if self.pending:
             yield [self._hand()]
             s.slab_particles_recv()

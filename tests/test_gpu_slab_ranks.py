@@ -267,3 +267,48 @@ def test_slab_ranks_with_bilinear_nudging_match_the_whole_domain(precision, npar
             with pytest.raises(lb.LbrbError):
                 a.slab_pack()
                 a.step(1)  # lbrb_slab_nudge of the last step first
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("heights", [(20, 17, 11), (24, 24)])
+def test_slab_ranks_with_particles_two_steps_per_launch(precision, heights):
+    """lbrb_step(h, 2) on slabs holding particles: one two-step launch, then
+    the particle exchange of each of its steps in turn (the first step's
+    receive moves the handle on to the second); odd call lengths end with a
+    single step.  States, records (at odd and even steps) and populations
+    equal the whole domain's bit for bit."""
+    torch = pytest.importorskip("torch")
+    npart = 400
+    kw = params(precision, nprtcl=npart, noutconfig=7, record_slots=64, beta=0.5, record_full=1)
+    (f, g), m = developed(precision)
+    with lb.Run(**kw) as whole, lb.SlabDomain(heights, **kw) as dom:
+        for d in (whole, dom):
+            d.set_populations(f, g)
+            d.set_moments(m["rho"], m["u"], m["v"], m["T"])
+            seed(d, npart, 5)
+        ranks = ranks_of(dom, torch, pairs=True)
+        for n in (1, 6, 91, 200):
+            whole.step(n)
+            drive(dom, ranks, n, torch)
+            for r in dom.slabs:
+                r.sync()
+            pw, ps = whole.get_particles(), dom.get_particles()
+            for k in pw:
+                np.testing.assert_array_equal(ps[k], pw[k])
+            sw, rw = whole.drain_records_array()
+            ss, rs = dom.drain_records_array()
+            np.testing.assert_array_equal(ss, sw)
+            np.testing.assert_array_equal(rs, rw)
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+        assert sum(dom.slab_counts()) == npart
+        # after a two-step launch the handle takes no further step until
+        # both steps' particle exchanges have run
+        a = dom.slabs[0]
+        with torch.cuda.stream(dom.stream):
+            a.slab_pack2()
+            a.step(2)
+            with pytest.raises(lb.LbrbError):
+                a.step(1)
