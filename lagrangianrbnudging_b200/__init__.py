@@ -622,6 +622,14 @@ class SlabDomain:
             r.set_moments(rho[j0:j0 + hgt], u[j0:j0 + hgt], v[j0:j0 + hgt], T[j0:j0 + hgt])
             j0 += hgt
 
+    def moments_from_pre(self, fpre, gpre):
+        """the restart route's moments from whole-domain post-stream
+        populations, SoA (9, ny, nx) each (node by node: each slab its rows)"""
+        j0 = 0
+        for r, hgt in zip(self.slabs, self.heights):
+            r.moments_from_pre(np.ascontiguousarray(fpre[:, j0:j0 + hgt]), np.ascontiguousarray(gpre[:, j0:j0 + hgt]))
+            j0 += hgt
+
     def get_populations(self):
         parts = [r.get_populations() for r in self.slabs]
         return np.concatenate([p[0] for p in parts], axis=1), np.concatenate([p[1] for p in parts], axis=1)

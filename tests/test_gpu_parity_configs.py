@@ -57,8 +57,12 @@ def run_case(c, precision, launch):
 
 
 def check_fp64(name, launch):
+    c, _ = case(name)
+    check_fp64_outputs(name, *run_case(c, "fp64", launch))
+
+
+def check_fp64_outputs(name, f, g, m, recs, fields_only=False):
     c, z = case(name)
-    f, g, m, recs = run_case(c, "fp64", launch)
     rows = cases.sample_rows(c["ny"])
     np.testing.assert_array_equal(cases.sample_pops(f), z["f_sample"])
     np.testing.assert_array_equal(cases.sample_pops(g), z["g_sample"])
@@ -67,6 +71,8 @@ def check_fp64(name, launch):
     for k in ("rho", "u", "v", "T"):
         np.testing.assert_array_equal(m[k][rows][:, ::64], z[f"{k}_sample"], err_msg=k)
         assert cases.sha256(m[k]) == str(z[f"{k}_sha"]), k
+    if fields_only:
+        return
     fields = [str(k) for k in z["rec_fields"]]
     steps = [int(s) for s in z["rec_steps"]]
     assert sorted(recs) == steps
@@ -110,3 +116,73 @@ def test_config_fp32_shifted_close_to_reference(name):
     np.testing.assert_allclose(last["x"][order], z["rec_last_x"], rtol=0, atol=1e-4)
     np.testing.assert_allclose(last["y"][order], z["rec_last_y"], rtol=0, atol=1e-4)
     np.testing.assert_allclose(last["temp"][order], z["rec_last_temp"], rtol=0, atol=2e-5)
+
+
+def run_case_slabs(c, heights, protocol):
+    """the same run as one domain cut into y-slabs on this GPU: through
+    lbrb_slab_step (one process), or the one-process-per-GPU protocol with
+    two steps per launch (slabrank, copies between the slabs)"""
+    kw = dict(c["base"], precision="fp64", twall="dirichlet", nudge="none", beta=c["beta"],
+              nprtcl=c["nprtcl"], noutconfig=c["noutconfig"], record_full=True,
+              record_slots=c["nsteps"] // c["noutconfig"] + 2)
+    with lb.SlabDomain(heights, **kw) as dom:
+        dom.set_populations(c["f0"], c["g0"])
+        dom.moments_from_pre(c["f0"], c["g0"])
+        dom.set_particles(c["ids"], c["px"], c["py"], c["pu"], c["pv"], c["ptype"], c["invtau"])
+        if protocol == "slab_step":
+            dom.step(c["nsteps"])
+        else:
+            import torch
+
+            from lagrangianrbnudging_b200 import slabrank
+            st = slabrank.bind_stream(dom.slabs, torch)
+            ranks = [slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=True, pairs=True)
+                     for r in dom.slabs]
+            with torch.cuda.stream(st):
+                slabrank.run_local(ranks, c["nsteps"])
+            torch.cuda.synchronize()
+        for r in dom.slabs:
+            r.sync()
+        f, g = dom.get_populations()
+        m = dom.get_moments()
+        recs = dom.drain_records()
+    return f, g, m, recs
+
+
+@pytest.mark.parametrize("protocol", ["slab_step", "ranks_pairs"])
+def test_config0_fp64_slabs_bit_exact_vs_reference(protocol):
+    """three uneven y-slabs, each holding its own particles, against the
+    reference's digests: populations, moments and every record"""
+    c, _ = case("cfg0_traj")
+    check_fp64_outputs("cfg0_traj", *run_case_slabs(c, (100, 90, 66), protocol))
+
+
+def test_config1_fp64_slabs_bit_exact_vs_reference():
+    """4096x2048 with 2^17 particles as two slabs through the
+    one-process-per-GPU protocol, against the reference's digests"""
+    c, _ = case("cfg1_traj")
+    check_fp64_outputs("cfg1_traj", *run_case_slabs(c, (1024, 1024), "ranks_pairs"))
+
+
+def test_config0_fp64_ensemble_member_bit_exact_vs_reference():
+    """the configuration's fields as a member of an ensemble (two-step
+    launches in graph replays, beside a member of another size) against the
+    reference's digests of f, g and the moments (ensemble members keep no
+    records; the particles do not act on the fields)"""
+    c, _ = case("cfg0_traj")
+    kw = dict(c["base"], precision="fp64", twall="dirichlet", nudge="none", nprtcl=0)
+    a = lb.Run(**kw)
+    b = lb.Run(**lb.closure(256, 128, Ra=1e6, Pr=1.0, U=0.1), precision="fp64")
+    try:
+        a.set_populations(c["f0"], c["g0"])
+        a.moments_from_pre(c["f0"], c["g0"])
+        b.init_conduction(5, 1e-2)
+        with lb.Ensemble([a, b]) as e:
+            e.step(c["nsteps"])
+            e.sync()
+        f, g = a.get_populations()
+        m = a.get_moments()
+    finally:
+        a.close()
+        b.close()
+    check_fp64_outputs("cfg0_traj", f, g, m, None, fields_only=True)
