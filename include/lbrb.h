@@ -165,7 +165,9 @@ LBRB_API int lbrb_set_stream(lbrb_t *h, void *cuda_stream);
  * replay a graph of the same launches (one graph per buffer phase, captured
  * on first use), so small grids are not bound by the host's per-launch
  * enqueue.  Results are identical either way.  -1 (the default): grids of
- * at most 2^20 nodes; 0: off; 1: every grid.  Not used with nudging,
+ * at most 2^20 nodes where two steps per launch do not apply (lbrb_set_pairs;
+ * a two-step launch is faster than a replay of two single steps); 0: off;
+ * 1: every grid, ahead of two-step launches.  Not used with nudging,
  * per-kernel timing, a y-slab, the legacy default stream, or while the
  * caller captures the handle's stream.  No counterpart in the reference. */
 LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
@@ -174,7 +176,9 @@ LBRB_API int lbrb_set_graph(lbrb_t *h, int mode);
  * so populations and F cross HBM once per two steps (u, v, and T on record
  * steps, are still stored for every step; the particle kernels run after
  * the launch for each step).  Results are identical to single steps.
- * -1 (the default) and 1: pairs of steps that do not replay graphs; 0: off.
+ * -1 (the default): pairs where a timed pair launch beats two single ones;
+ * 1: always; 0: off (pairs give way to graph replays forced by
+ * lbrb_set_graph(h, 1)).
  * Used with Dirichlet walls, without nudging or with bilinear nudging, not
  * on a y-slab, and never for the last step of a call (so
  * lbrb_get_poststream keeps its meaning).  With bilinear nudging, step n's

@@ -291,7 +291,8 @@ struct Handle {
   SlabParts* sp = nullptr;
   const double* slab_obs = nullptr;  // bilinear observations of the step just taken (lbrb_slab_step applies them)
   // CUDA graphs of plain steps, one per buffer phase (cur * 9 + uvcur * 3 +
-  // uvprev); graph_mode -1: small grids only, 0: off, 1: on
+  // uvprev); graph_mode -1: small grids where two-step launches do not
+  // apply, 0: off, 1: on (ahead of two-step launches)
   cudaGraphExec_t graph_exec[18] = {};
   // two steps per launch (lb_pair_kernel, NUM_PAIR_SHAPES tile shapes):
   // pair_mode -1 auto (steps that
