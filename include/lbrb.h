@@ -382,10 +382,15 @@ LBRB_API int lbrb_stats_noalloc(const void *rho, const void *u, const void *v, c
  * lbrb_init_conduction on a slab gives the whole domain's profile and noise
  * at its rows; lbrb_nusselt gives the slab's mean of v T at the whole
  * domain's height (the domain's Nu is the slabs' values weighted by ny).
- * Supported: Dirichlet walls; particles (held by their owner slab, below);
- * bilinear nudging (not box nudging): every slab holds all observations
- * (lbrb_nudge_obs on each, in the whole domain's coordinates) and
- * lbrb_slab_step applies them (one process per GPU: lbrb_slab_nudge).
+ * Supported: Dirichlet and adiabatic walls (the walls of the domain only);
+ * particles (held by their owner slab, below); bilinear nudging: every slab
+ * holds all observations (lbrb_nudge_obs on each, in the whole domain's
+ * coordinates) and lbrb_slab_step applies them (one process per GPU:
+ * lbrb_slab_nudge); box nudging (FP64): every slab takes all observations
+ * (lbrb_nudge_init / lbrb_nudge_load on each) and keeps the running means
+ * of the boxes' nodes in its own rows, inside its lbrb_step, as the
+ * reference's ranks in y do.  Two steps per launch need Dirichlet walls and
+ * no nudging.
  * Create slab handles with nprtcl = 0 (lbrb_slab_set rejects a handle with
  * whole-domain particles). */
 LBRB_API int lbrb_slab_set(lbrb_t *h, int j0, int ny_total);

@@ -725,6 +725,17 @@ class SlabDomain:
         for r in self.slabs:
             r.nudge_obs(first_step, x, y, T)
 
+    def nudge_init(self, x, y, T, ids):
+        """box nudging: the initial observations, given to every slab (each
+        keeps the running means of the boxes' nodes in its own rows)"""
+        for r in self.slabs:
+            r.nudge_init(x, y, T, ids)
+
+    def nudge_load(self, x, y, ids, T):
+        """box nudging: the next observation file, given to every slab"""
+        for r in self.slabs:
+            r.nudge_load(x, y, ids, T)
+
 
 class Ensemble:
     """Independent runs advanced together (lbrb_ensemble_*): one launch per

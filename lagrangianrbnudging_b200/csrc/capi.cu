@@ -795,7 +795,7 @@ int lbrb_step(lbrb_t* h, int n) {
     h->sp->pair_pending = true;
     return LBRB_OK;
   }
-  if (h->slab && (n != 1 || (h->p.nudge != LBRB_NUDGE_NONE && !h->slab_stepping && !h->sp)))
+  if (h->slab && (n != 1 || (h->p.nudge == LBRB_NUDGE_BILINEAR && !h->slab_stepping && !h->sp)))
     return fail(h, LBRB_ERR_ARG,
                 "step: a y-slab takes one step per boundary exchange, or two after lbrb_slab_pack2 (lbrb_slab_step); "
                 "a nudged slab stepped alone needs the moment messages (lbrb_slab_particles_set)");
@@ -875,7 +875,8 @@ int lbrb_step(lbrb_t* h, int n) {
       if (istep % nt == 1 && !h->nudge_file_loaded)
         return fail(h, LBRB_ERR_STATE, "step: observation file for this interval not loaded");
       const int tm = tmark_begin(h, 2, h->stream);
-      CK(h, launch_box_nudge(h->nb, h->nbi, h->nobs, nx, ny, nt, istep, h->ncx, h->ncy,
+      CK(h, launch_box_nudge(h->nb, h->nbi, h->nobs, nx, ny, h->slab ? h->slab_ny_total : ny, h->slab ? h->slab_j0 : 0,
+                             nt, istep, h->ncx, h->ncy,
                              h->cell_count, h->cell_start, h->cell_fill, h->cell_dirty,
                              h->cell_items, h->nudge_vol, h->tempreadint, h->pitch, h->dflags,
                              h->stream));
@@ -1525,8 +1526,6 @@ int lbrb_slab_set(lbrb_t* h, int j0, int ny_total) {
   if (!h) return LBRB_ERR_ARG;
   if (j0 < 0 || ny_total < 2 || j0 + h->p.ny > ny_total)
     return fail(h, LBRB_ERR_ARG, "slab_set: rows [j0, j0 + ny) must lie in [0, ny_total)");
-  if (h->p.twall != LBRB_TWALL_DIRICHLET || h->p.nudge == LBRB_NUDGE_REFBOX)
-    return fail(h, LBRB_ERR_UNSUPPORTED, "slab_set: Dirichlet walls, no box nudging");
   if (h->np > 0)
     return fail(h, LBRB_ERR_UNSUPPORTED,
                 "slab_set: a slab's particles are set by lbrb_slab_particles_set (create it with nprtcl = 0)");

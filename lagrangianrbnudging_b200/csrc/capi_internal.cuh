@@ -62,7 +62,7 @@ cudaError_t launch_bilinear_nudge_slab(const void* Trows, void* g, bool fp32, si
                                        int j0, int nyl, int pitch, const double* ox, const double* oy,
                                        const double* oT, int nobs, double alpha, long long* acc, unsigned* dflags,
                                        cudaStream_t s);
-cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt, int istep,
+cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int ny_total, int j0, int nt, int istep,
                              int ncx, int ncy, int* cell_count, int* cell_start, int* cell_fill,
                              int* cell_dirty, int* items, int* nudge_vol, double* tempreadint,
                              int pitch, unsigned* dflags, cudaStream_t s);

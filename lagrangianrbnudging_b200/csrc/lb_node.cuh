@@ -184,7 +184,10 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
     });
     return;
   }
-  const bool adia_wall = TWALL == LBRB_TWALL_ADIABATIC && (j == 0 || j == V.ny - 1);
+  // adiabatic g walls at the domain's walls only (a y-slab's inner edge
+  // has ghost rows instead)
+  const bool wall_lo = !V.ghost_lo, wall_hi = !V.ghost_hi;
+  const bool adia_wall = TWALL == LBRB_TWALL_ADIABATIC && ((j == 0 && wall_lo) || (j == V.ny - 1 && wall_hi));
   const int jc = (j == 0) ? 1 : V.ny - 2;
   static_for<NPOP>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
@@ -207,8 +210,8 @@ __device__ __forceinline__ void pull_node(const LBView<Real>& V, int j, int x, R
     } else {
       int jg = js;
       if (TWALL == LBRB_TWALL_ADIABATIC) {
-        if (jg == 0) jg = 1;
-        else if (jg == V.ny - 1) jg = V.ny - 2;
+        if (jg == 0 && wall_lo) jg = 1;
+        else if (jg == V.ny - 1 && wall_hi) jg = V.ny - 2;
       }
       gs[k] = (jg < 0 || jg >= V.ny) ? Real(0)
                                       : __ldcs(V.gsrc + ((Off)k * pl + (Off)jg * pitch + (Off)xs));

@@ -35,7 +35,10 @@ enum { NBI_CHK = 0, NBI_BC, NBI_XIDX, NBI_YIDX, NBI_COUNT };
 struct BoxView {
   double* nb;
   int* nbi;
-  int n, nx, ny, nt, istep;
+  // ny: the handle's rows (of nudge_vol, tempreadint and the cells); nyT:
+  // the whole domain's rows (positions and boxes); j0: the handle's first
+  // row in the domain (0 unless a y-slab)
+  int n, nx, ny, nt, istep, nyT, j0;
   int ncx, ncy;
   int* cell_count;
   int* cell_start;
@@ -56,7 +59,7 @@ __device__ __forceinline__ int* NBI(const BoxView& B, int a) { return B.nbi + (s
 __global__ void box_interp_kernel(const BoxView B) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= B.n) return;
-  const int nx = B.nx, ny = B.ny, nt = B.nt;
+  const int nx = B.nx, ny = B.nyT, nt = B.nt;
   double *ox = NB(B, NB_OX), *oy = NB(B, NB_OY), *oT = NB(B, NB_OT);
   double *fx = NB(B, NB_FX), *fy = NB(B, NB_FY), *fT = NB(B, NB_FT);
   double *xint = NB(B, NB_XINT), *yint = NB(B, NB_YINT), *Tint = NB(B, NB_TINT);
@@ -142,8 +145,8 @@ __global__ void box_commit_file_kernel(const BoxView B) {
   NB(B, NB_OT)[i] = NB(B, NB_FT)[i];
 }
 
-// node box of contribution (k, img), reference 1-based node coordinates,
-// clipped to the interior; false when empty.  img 0: main 7x7 box; img 1:
+// node box of contribution (k, img), reference 1-based node coordinates of
+// the whole domain, clipped to its interior; false when empty.  img 0: main 7x7 box; img 1:
 // left periodic image (xidx < 4); img 2: right periodic image (xidx > nx-2).
 __device__ __forceinline__ bool contrib_box(const BoxView& B, int k, int img, int& xa, int& xb,
                                             int& ya, int& yb) {
@@ -161,7 +164,7 @@ __device__ __forceinline__ bool contrib_box(const BoxView& B, int k, int img, in
   if (xa < 1) xa = 1;
   if (xb > B.nx) xb = B.nx;
   if (ya < 1) ya = 1;
-  if (yb > B.ny) yb = B.ny;
+  if (yb > B.nyT) yb = B.nyT;
   return xa <= xb && ya <= yb;
 }
 
@@ -172,8 +175,12 @@ __global__ void box_bin_kernel(const BoxView B) {
   const int k = t / 3, img = t - 3 * k;
   int xa, xb, ya, yb;
   if (!contrib_box(B, k, img, xa, xb, ya, yb)) return;
+  // the rows of this handle (a y-slab bins only what reaches its rows)
+  ya = max(ya, B.j0 + 1);
+  yb = min(yb, B.j0 + B.ny);
+  if (ya > yb) return;
   const int ca = (xa - 1) / CELL, cb = (xb - 1) / CELL;
-  const int ra = (ya - 1) / CELL, rb = (yb - 1) / CELL;
+  const int ra = (ya - 1 - B.j0) / CELL, rb = (yb - 1 - B.j0) / CELL;
   for (int cy = ra; cy <= rb; cy++)
     for (int cx = ca; cx <= cb; cx++) {
       const int c = cy * B.ncx + cx;
@@ -219,8 +226,8 @@ __global__ void __launch_bounds__(CELL * CELL) box_cells_kernel(const BoxView B)
   if (cnt == 0 && !dirty) return;
   const int cx = c % B.ncx, cy = c / B.ncx;
   const int tid = threadIdx.x;
-  const int i = cx * CELL + (tid % CELL) + 1;  // reference node coordinates
-  const int j = cy * CELL + (tid / CELL) + 1;
+  const int i = cx * CELL + (tid % CELL) + 1;  // reference node coordinates (of the domain)
+  const int j = B.j0 + cy * CELL + (tid / CELL) + 1;
   const int st = B.cell_start[c];
   // rank sort (keys are unique)
   for (int a = tid; a < cnt; a += blockDim.x) {
@@ -243,20 +250,20 @@ __global__ void __launch_bounds__(CELL * CELL) box_cells_kernel(const BoxView B)
       nv = nv + 1;
     }
   }
-  if (i <= B.nx && j <= B.ny) {
-    const size_t q = (size_t)(j - 1) * B.pitch + (i - 1);
+  if (i <= B.nx && j <= B.j0 + B.ny) {
+    const size_t q = (size_t)(j - 1 - B.j0) * B.pitch + (i - 1);
     B.nudge_vol[q] = nv;
     B.tempreadint[q] = tri;
   }
   if (tid == 0) B.cell_dirty[c] = cnt > 0;
 }
 
-cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int nt, int istep,
+cudaError_t launch_box_nudge(double* nb, int* nbi, int n, int nx, int ny, int ny_total, int j0, int nt, int istep,
                              int ncx, int ncy, int* cell_count, int* cell_start, int* cell_fill,
                              int* cell_dirty, int* items, int* nudge_vol, double* tempreadint,
                              int pitch, unsigned* dflags, cudaStream_t s) {
   const int ncell = ncx * ncy;
-  BoxView B{nb, nbi, n, nx, ny, nt, istep, ncx, ncy, cell_count, cell_start, cell_fill,
+  BoxView B{nb, nbi, n, nx, ny, nt, istep, ny_total, j0, ncx, ncy, cell_count, cell_start, cell_fill,
             cell_dirty, items, items + (size_t)n * 3 * 4, nudge_vol, tempreadint, pitch, dflags};
   const int tb = 128;
   box_interp_kernel<<<(n + tb - 1) / tb, tb, 0, s>>>(B);

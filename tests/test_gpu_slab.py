@@ -1,7 +1,8 @@
 """One domain cut into y-slabs (lbrb_slab_set / lbrb_slab_step): the slabs
 advance exactly as the whole domain in one handle, bit for bit, in both
-precisions and with uneven slab heights, particles, their records and
-bilinear nudging included; the slabs' initial state is the whole domain's; the
+precisions and with uneven slab heights, particles, their records,
+bilinear nudging and adiabatic walls included; box nudging bit for bit against
+the reference's own run; the slabs' initial state is the whole domain's; the
 height-weighted Nu is the whole domain's.  On one GPU the
 slabs are handles on the same device: the exchange is the same peer copy as
 across GPUs (cudaMemcpyPeerAsync), ordered by the same events."""
@@ -10,6 +11,7 @@ import pytest
 
 import lagrangianrbnudging_b200 as lb
 from lagrangianrbnudging_b200 import build
+from tests.golden import cases
 
 pytestmark = pytest.mark.gpu
 
@@ -83,12 +85,11 @@ def test_slab_mode_rejects_what_it_does_not_cover():
         r.init_conduction(1, 1e-3)
         with pytest.raises(lb.LbrbError):
             r.step(3)  # one step, or two after lbrb_slab_pack2, per boundary exchange
-    with lb.Run(**dict(params("fp32"), ny=24, twall="adiabatic")) as r:
+    with lb.Run(**dict(params("fp32"), ny=24)) as r:
+        r.slab_set(0, NY)
+        r.init_conduction(1, 1e-3)
         with pytest.raises(lb.LbrbError):
-            r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # adiabatic walls are not covered
-    with lb.Run(**dict(params("fp64"), ny=24, nudge="refbox", nobs=4, ntempread=10)) as r:
-        with pytest.raises(lb.LbrbError):
-            r._ck(lb.lib().lbrb_slab_set(r.h, 0, NY))  # box nudging is not covered
+            r.step(2)  # two steps need lbrb_slab_pack2 first
     with lb.Run(**dict(params("fp32"), ny=24, nprtcl=8)) as r:
         with pytest.raises(lb.LbrbError):
             r.slab_set(0, NY)  # a slab holds its own particles (lbrb_slab_particles_set)
@@ -301,3 +302,68 @@ def test_one_process_per_gpu_exchange(precision):
         exchange(dom, False)  # a one-step pack does not count
         with pytest.raises(lb.LbrbError):
             dom.slabs[0].step(2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_slabs_with_adiabatic_walls_advance_as_the_whole_domain(precision):
+    """adiabatic T walls (the nudging run's) hold at the domain's walls only;
+    inner slab edges take ghost rows"""
+    kw = dict(params(precision), twall="adiabatic")
+    with lb.Run(**kw) as whole, lb.SlabDomain((20, 17, 11), **kw) as dom:
+        whole.init_conduction(17, 2e-2)
+        dom.init_conduction(17, 2e-2)
+        for n in (1, 37, 300):
+            whole.step(n)
+            dom.step(n)
+            fw, gw = whole.get_populations()
+            fs, gs = dom.get_populations()
+            np.testing.assert_array_equal(fs, fw)
+            np.testing.assert_array_equal(gs, gw)
+
+
+@pytest.mark.parametrize("name", list(cases.NUDGE_CASES))
+@pytest.mark.parametrize("heights,protocol", [((12, 11, 9), "slab_step"), ((8, 8, 8, 8), "slab_step"),
+                                              ((16, 16), "ranks")])
+def test_slab_box_nudging_bit_exact_vs_reference(name, heights, protocol):
+    """the reference's box nudging (FP64, adiabatic walls) on y-slabs, as the
+    reference runs it over ranks in y: every slab takes all observations and
+    keeps the running means of the boxes' nodes in its own rows.  Populations
+    and moments equal the reference's own run bit for bit, through
+    lbrb_slab_step and through the one-process-per-GPU protocol (box nudging
+    needs no exchange beyond the ghost rows)."""
+    c = cases.nudge_case(name)
+    z = cases.load_golden(name)
+    st = cases.nudge_initial_state(c)
+    kw = dict(**c["base"], precision="fp64", twall="adiabatic", nudge="refbox", alpha=c["alpha"],
+              ntempread=c["ntempread"], nobs=c["nprtcl"])
+    with lb.SlabDomain(heights, **kw) as dom:
+        dom.set_populations(st["f"], st["g"])
+        dom.set_moments(st["rho"], st["u"], st["v"], st["T"])
+        io = c["init_obs"]
+        dom.nudge_init(io["x"], io["y"], io["T"], io["id"])
+        nt = c["ntempread"]
+        if protocol == "ranks":
+            torch = pytest.importorskip("torch")
+            from lagrangianrbnudging_b200 import slabrank
+            stream = slabrank.bind_stream(dom.slabs, torch)
+            ranks = [slabrank.SlabRank(r, slabrank.device_buffers(r, torch), particles=False) for r in dom.slabs]
+        for s in range(1, c["nsteps"] + 1):
+            if s % nt == 1:
+                d = c["files"][s + nt - 1]
+                dom.nudge_load(d["x"], d["y"], d["id"], d["temp"])
+            if protocol == "ranks":
+                with torch.cuda.stream(stream):
+                    slabrank.run_local(ranks, 1)
+                torch.cuda.synchronize()
+            else:
+                dom.step(1)
+        for r in dom.slabs:
+            r.sync()
+        f, g = dom.get_populations()
+        m = dom.get_moments()
+    np.testing.assert_array_equal(f, z["f"])
+    np.testing.assert_array_equal(g, z["g"])
+    s = c["nsteps"]
+    np.testing.assert_array_equal(m["T"], z[f"snap{s}_T"])
+    np.testing.assert_array_equal(m["u"], z[f"snap{s}_u"])
+    np.testing.assert_array_equal(m["v"], z[f"snap{s}_v"])
