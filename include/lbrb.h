@@ -328,16 +328,25 @@ LBRB_API int lbrb_ensemble_get_schedule(const lbrb_ensemble_t *e, int *variant, 
 /* Two steps per launch for every member (as lbrb_set_pairs, with Dirichlet
  * walls; bilinear-nudged members too): every step of a call but its last
  * (and one more when an even count remains) goes in pairs, each pair one
- * marching launch over strips of 32 columns x chunks of rows of all members
- * (lb_march_kernel's block, the members' views in shared memory), with the
- * nudged members' step-n innovations formed before it and every member's
- * particles, step n+1 innovations and nudging apply after it; 12 steps are
- * replayed from a CUDA graph.  Members end bit-identical to lbrb_step.
- * mode -1 (the default) and 1: on; 0: one step per launch.  The rows per
- * marching group (4, 8 or 16) are timed at the first paired call;
- * lbrb_ensemble_get_pairs reports them (0 before) and ms per launch. */
+ * launch over all members -- marching over strips of 32 columns x chunks of
+ * rows (lb_march_kernel's block) or over tiles (lb_pair_kernel's block), the
+ * members' views in shared memory -- with the nudged members' step-n
+ * innovations formed before it and every member's particles, step n+1
+ * innovations and nudging apply after it; 12 steps are replayed from a CUDA
+ * graph.  Members end bit-identical to lbrb_step.
+ * mode -1 (the default) and 1: on; 0: one step per launch.  The launch
+ * variant (lbrb_ensemble_pair_variants() of them: marching with 6 or 8 rows
+ * per group, tiles of 32 x 8 or 30 x 8 nodes) is timed at the first paired
+ * call unless set; lbrb_ensemble_get_pairs reports its rows per group or per
+ * tile (0 before) and ms per launch (0 when set rather than timed). */
 LBRB_API int lbrb_ensemble_set_pairs(lbrb_ensemble_t *e, int mode);
 LBRB_API int lbrb_ensemble_get_pairs(const lbrb_ensemble_t *e, int *mode, int *rows, float *ms);
+LBRB_API int lbrb_ensemble_pair_variants(void);
+/* variant -1: time the variants at the next paired call (the default);
+ * 0 .. lbrb_ensemble_pair_variants() - 1: use that one.  get: the variant
+ * (-1 before timing) and its tile columns (0 for a marching variant). */
+LBRB_API int lbrb_ensemble_set_pair_variant(lbrb_ensemble_t *e, int variant);
+LBRB_API int lbrb_ensemble_get_pair_variant(const lbrb_ensemble_t *e, int *variant, int *tile_cols);
 /* Per-launch device timing (steps then launch directly, without the graph).
  * Classes: 0 fused step (one or two steps), 1 particles + innovation
  * scatter, 2 nudging (apply; with pairs also the innovations before the

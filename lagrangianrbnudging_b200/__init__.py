@@ -43,7 +43,8 @@ EXPORTS = [
     "lbrb_ensemble_create", "lbrb_ensemble_destroy", "lbrb_ensemble_last_error",
     "lbrb_ensemble_step", "lbrb_ensemble_sync", "lbrb_ensemble_set_stream",
     "lbrb_ensemble_nvariants", "lbrb_ensemble_set_schedule", "lbrb_ensemble_get_schedule",
-    "lbrb_ensemble_set_pairs", "lbrb_ensemble_get_pairs",
+    "lbrb_ensemble_set_pairs", "lbrb_ensemble_get_pairs", "lbrb_ensemble_pair_variants",
+    "lbrb_ensemble_set_pair_variant", "lbrb_ensemble_get_pair_variant",
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
@@ -133,6 +134,9 @@ def lib() -> C.CDLL:
         "lbrb_ensemble_set_schedule": (C.c_int, [vp, C.c_int]),
         "lbrb_ensemble_set_pairs": (C.c_int, [vp, C.c_int]),
         "lbrb_ensemble_get_pairs": (C.c_int, [vp, ip, ip, C.POINTER(C.c_float)]),
+        "lbrb_ensemble_pair_variants": (C.c_int, []),
+        "lbrb_ensemble_set_pair_variant": (C.c_int, [vp, C.c_int]),
+        "lbrb_ensemble_get_pair_variant": (C.c_int, [vp, ip, ip]),
         "lbrb_ensemble_get_schedule": (C.c_int, [vp, ip, ip, ip, ip, ip, C.POINTER(C.c_float)]),
         "lbrb_ensemble_set_timing": (C.c_int, [vp, C.c_int]),
         "lbrb_ensemble_get_timing": (C.c_int, [vp, dp, ip, C.c_int]),
@@ -798,7 +802,19 @@ class Ensemble:
     def pairs(self) -> dict:
         mode, rows, ms = C.c_int(), C.c_int(), C.c_float()
         self._ck(lib().lbrb_ensemble_get_pairs(self.e, C.byref(mode), C.byref(rows), C.byref(ms)))
-        return {"mode": mode.value, "rows": rows.value, "tuned_ms": ms.value}
+        v, cols = C.c_int(), C.c_int()
+        self._ck(lib().lbrb_ensemble_get_pair_variant(self.e, C.byref(v), C.byref(cols)))
+        return {"mode": mode.value, "rows": rows.value, "tuned_ms": ms.value, "variant": v.value,
+                "tile_cols": cols.value}
+
+    def set_pair_variant(self, variant: int) -> None:
+        """-1: time the two-step launch variants at the next paired call;
+        else use that one (pair_variants() of them)"""
+        self._ck(lib().lbrb_ensemble_set_pair_variant(self.e, int(variant)))
+
+    @staticmethod
+    def pair_variants() -> int:
+        return int(lib().lbrb_ensemble_pair_variants())
 
     def schedule(self) -> dict:
         v, b, r, s, f, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()

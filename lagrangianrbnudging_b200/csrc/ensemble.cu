@@ -46,7 +46,8 @@ struct lbrb_ensemble_s {
   int graph_variant = -1;
   // two steps per launch: pair_mode -1 (default) / 1 on, 0 off; pair views
   // [6 phases][2 steps][n] and their EnsAux, items of the marching kernel
-  // (member, first column, first row, rows), its variant (-1: tune), a graph
+  // (member, first column, first row, rows) and of each tile variant
+  // (member, first column, first row, 0), the variant (-1: tune), a graph
   // of 6 pairs (12 steps, the period of the buffer cycle)
   int pair_mode = -1;
   int pair_variant = -1;
@@ -55,6 +56,8 @@ struct lbrb_ensemble_s {
   void* d_paux = nullptr;
   int4* d_pitems = nullptr;
   int npitems = 0;
+  int4* d_titems[ENS_PAIR_VARIANTS - ENS_MARCH_VARIANTS] = {};
+  int ntitems[ENS_PAIR_VARIANTS - ENS_MARCH_VARIANTS] = {};
   cudaGraph_t pgraph = nullptr;
   cudaGraphExec_t pgexec = nullptr;
   int pgraph_variant = -1;
@@ -333,6 +336,14 @@ const char* paux_at(const lbrb_ensemble_t* e, int ph, int step) {
   return (const char*)e->d_paux + (size_t)(2 * ph + step) * e->m.size() * e->asize;
 }
 
+// the two-step LB launch of variant v over every member, pair phase ph
+static cudaError_t launch_pair_lb(lbrb_ensemble_t* e, int v, int ph) {
+  const bool tile = v >= ENS_MARCH_VARIANTS;
+  return launch_ens_march(e->f32, e->off32, v, pview_at(e, ph, 0), pview_at(e, ph, 1),
+                          tile ? e->d_titems[v - ENS_MARCH_VARIANTS] : e->d_pitems,
+                          tile ? e->ntitems[v - ENS_MARCH_VARIANTS] : e->npitems, e->d_ctr, e->stream);
+}
+
 // two steps of every member, pair phase ph (0..5)
 cudaError_t launch_pair(lbrb_ensemble_t* e, int ph) {
   cudaError_t c = cudaSuccess;
@@ -344,8 +355,7 @@ cudaError_t launch_pair(lbrb_ensemble_t* e, int ph) {
     if (c != cudaSuccess) return c;
   }
   k = mark_begin(e, 0);
-  c = launch_ens_march(e->f32, e->off32, e->pair_variant, pview_at(e, ph, 0), pview_at(e, ph, 1), e->d_pitems,
-                       e->npitems, e->d_ctr, e->stream);
+  c = launch_pair_lb(e, e->pair_variant, ph);
   mark_end(e, k);
   if (c != cudaSuccess) return c;
   k = mark_begin(e, 1);
@@ -362,9 +372,17 @@ cudaError_t launch_pair(lbrb_ensemble_t* e, int ph) {
 }
 
 // work items of the marching kernel: every member's strips of 32 columns x
-// chunks of PAIR_CHUNK rows (whole groups of 4, 8 or 16 rows with the two
-// ring rows)
+// chunks of PAIR_CHUNK rows (whole groups of 6 or 8 rows with the two ring
+// rows); of a tile variant: every member's tiles, row by row
 constexpr int PAIR_CHUNK = 62;
+static int upload_items(lbrb_ensemble_t* e, const std::vector<int4>& it, int4** d, int* n) {
+  EK(e, cudaMalloc(d, it.size() * sizeof(int4)));
+  EK(e, cudaMemcpyAsync(*d, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+  EK(e, cudaStreamSynchronize(e->stream));
+  *n = (int)it.size();
+  return LBRB_OK;
+}
+
 int set_pair_items(lbrb_ensemble_t* e) {
   if (e->d_pitems) return LBRB_OK;
   std::vector<int4> it;
@@ -373,11 +391,18 @@ int set_pair_items(lbrb_ensemble_t* e) {
     for (int y = 0; y < h->p.ny; y += PAIR_CHUNK)
       for (int x = 0; x < h->p.nx; x += 32) it.push_back(make_int4((int)i, x, y, std::min(PAIR_CHUNK, h->p.ny - y)));
   }
-  EK(e, cudaMalloc(&e->d_pitems, it.size() * sizeof(int4)));
-  EK(e, cudaMemcpyAsync(e->d_pitems, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
-  EK(e, cudaStreamSynchronize(e->stream));
-  e->npitems = (int)it.size();
-  return LBRB_OK;
+  int rc = upload_items(e, it, &e->d_pitems, &e->npitems);
+  for (int v = ENS_MARCH_VARIANTS; v < ENS_PAIR_VARIANTS && rc == LBRB_OK; v++) {
+    const int tx = ens_pair_tile_cols(v), ty = ens_pair_rows(v);
+    it.clear();
+    for (size_t i = 0; i < e->m.size(); i++) {
+      const lbrb_t* h = e->m[i];
+      for (int y = 0; y < h->p.ny; y += ty)
+        for (int x = 0; x < h->p.nx; x += tx) it.push_back(make_int4((int)i, x, y, 0));
+    }
+    rc = upload_items(e, it, &e->d_titems[v - ENS_MARCH_VARIANTS], &e->ntitems[v - ENS_MARCH_VARIANTS]);
+  }
+  return rc;
 }
 
 // Pair autotuner: each variant's marching launch on pair phase 0 (trials
@@ -396,8 +421,7 @@ int tune_pairs(lbrb_ensemble_t* e) {
     bool ok = true;
     for (int r = 0; r < 4 && ok; r++) {
       EK(e, cudaEventRecord(a, e->stream));
-      cudaError_t c = launch_ens_march(e->f32, e->off32, v, pview_at(e, 0, 0), pview_at(e, 0, 1), e->d_pitems,
-                                       e->npitems, e->d_ctr, e->stream);
+      cudaError_t c = launch_pair_lb(e, v, 0);
       if (c != cudaSuccess) {
         cudaGetLastError();
         ok = false;
@@ -601,6 +625,8 @@ int lbrb_ensemble_destroy(lbrb_ensemble_t* e) {
   for (void* p : {(void*)e->d_views, (void*)e->d_aux, (void*)e->d_items, (void*)e->d_pch, (void*)e->d_och,
                   (void*)e->d_ctr, (void*)e->d_pviews, (void*)e->d_paux, (void*)e->d_pitems})
     if (p) cudaFree(p);
+  for (int4* p : e->d_titems)
+    if (p) cudaFree(p);
   for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
   if (e->ev) cudaEventDestroy(e->ev);
   if (e->own_stream) cudaStreamDestroy(e->own_stream);
@@ -644,6 +670,23 @@ int lbrb_ensemble_get_schedule(const lbrb_ensemble_t* e, int* variant, int* bloc
 int lbrb_ensemble_set_pairs(lbrb_ensemble_t* e, int mode) {
   if (!e || mode < -1 || mode > 1) return efail(e, LBRB_ERR_ARG, "ensemble_set_pairs: mode must be -1, 0 or 1");
   e->pair_mode = mode;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_pair_variants(void) { return ENS_PAIR_VARIANTS; }
+
+int lbrb_ensemble_set_pair_variant(lbrb_ensemble_t* e, int variant) {
+  if (!e || variant < -1 || variant >= ENS_PAIR_VARIANTS)
+    return efail(e, LBRB_ERR_ARG, "ensemble_set_pair_variant: variant out of range");
+  e->pair_variant = variant;
+  e->pair_ms = 0.f;
+  return LBRB_OK;
+}
+
+int lbrb_ensemble_get_pair_variant(const lbrb_ensemble_t* e, int* variant, int* tile_cols) {
+  if (!e) return LBRB_ERR_ARG;
+  if (variant) *variant = e->pair_variant;
+  if (tile_cols) *tile_cols = e->pair_variant >= 0 ? ens_pair_tile_cols(e->pair_variant) : 0;
   return LBRB_OK;
 }
 

@@ -61,9 +61,13 @@ cudaError_t launch_ens_apply(bool f32, const void* aux, const int2* ochunks, int
 // member's step n and step n+1 views), ens_aux2 (every member's particles of
 // both steps; the innovations of step n+1), ens_apply2 (the nudging apply of
 // step n+1 and the clearing of step n's sums).  aux1/aux2: EnsAux of steps n
-// and n+1.  Pair variants: rows per marching group.
-constexpr int ENS_PAIR_VARIANTS = 3;
-int ens_pair_rows(int variant);
+// and n+1.  Pair variants: [0, ENS_MARCH_VARIANTS) march (items: a strip of
+// 32 columns and a chunk of rows), the rest take tiles (ens_tile, items: a
+// tile's first column and row; ens_pair_tile_cols columns).
+constexpr int ENS_MARCH_VARIANTS = 3;
+constexpr int ENS_PAIR_VARIANTS = 5;
+int ens_pair_rows(int variant);  // rows per marching group, or per tile
+int ens_pair_tile_cols(int variant);  // 0: a marching variant
 cudaError_t launch_ens_pre(bool f32, const void* views1, const void* aux1, const int2* ochunks, int nochunks,
                            const int* ctr, cudaStream_t s);
 cudaError_t launch_ens_march(bool f32, bool off32, int variant, const void* views1, const void* views2,

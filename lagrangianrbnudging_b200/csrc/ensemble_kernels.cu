@@ -136,6 +136,26 @@ __global__ void __launch_bounds__(32 * (R + 1), MINB)
   march_block<Real, R, PRE, Off>(sV[0], sV[1], w.y, w.z, w.w, ens_march_smem);
 }
 
+// The tile variant: work items (member, x0, y0, 0), one TX x TY tile each
+// (tile_block), the views as in ens_march_kernel
+template <typename Real, int TX, int TY, int NT, int MINB, typename Off>
+__global__ void __launch_bounds__(NT, MINB)
+    ens_tile_kernel(const LBView<Real>* __restrict__ views1, const LBView<Real>* __restrict__ views2,
+                    const int4* __restrict__ items, int* __restrict__ ctr) {
+  __shared__ LBView<Real> sV[2];
+  extern __shared__ __align__(16) unsigned char ens_tile_smem[];
+  pdl_wait();
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ctr[0], 2);
+  const int4 w = items[blockIdx.x];
+  constexpr int WORDS = (int)(sizeof(LBView<Real>) / sizeof(int));
+  const int* s1 = reinterpret_cast<const int*>(views1 + w.x);
+  const int* s2 = reinterpret_cast<const int*>(views2 + w.x);
+  int* d = reinterpret_cast<int*>(sV);
+  for (int i = threadIdx.x; i < 2 * WORDS; i += NT) d[i] = i < WORDS ? s1[i] : s2[i - WORDS];
+  __syncthreads();
+  tile_block<Real, TX, TY, NT, Off>(sV[0], sV[1], w.y, w.z, ens_tile_smem);
+}
+
 // step n's innovations of the nudged members, before the pair's launch
 // (ctr[0] steps of this call done): 4 threads per observation, one per cell
 // corner (obs_pre_corner; every lane of a warp takes part)
@@ -200,9 +220,17 @@ __global__ void __launch_bounds__(512)
   obs_clear_one(A1.nx, A1.ny, A1.pitch, o1[o], o1[A1.nobs + o], threadIdx.x & 3, A1.acc2, A1.nmask);
 }
 
-// pair variants: (rows per group, min blocks per SM, software pipelining)
-constexpr int3 ENS_PAIR_TABLE[ENS_PAIR_VARIANTS] = {{8, 3, 0}, {8, 3, 1}, {6, 4, 1}};
-int ens_pair_rows(int variant) { return ENS_PAIR_TABLE[variant].x; }
+// pair variants 0-2, marching: (rows per group, min blocks per SM, software
+// pipelining); 3-4, tiles: (tile columns, tile rows, threads, min blocks per
+// SM), as the single runs' pair shapes 6 and 5
+constexpr int3 ENS_PAIR_TABLE[ENS_MARCH_VARIANTS] = {{8, 3, 0}, {8, 3, 1}, {6, 4, 1}};
+constexpr int4 ENS_TILE_TABLE[ENS_PAIR_VARIANTS - ENS_MARCH_VARIANTS] = {{32, 8, 256, 5}, {30, 8, 320, 3}};
+int ens_pair_rows(int variant) {
+  return variant < ENS_MARCH_VARIANTS ? ENS_PAIR_TABLE[variant].x : ENS_TILE_TABLE[variant - ENS_MARCH_VARIANTS].y;
+}
+int ens_pair_tile_cols(int variant) {
+  return variant < ENS_MARCH_VARIANTS ? 0 : ENS_TILE_TABLE[variant - ENS_MARCH_VARIANTS].x;
+}
 
 template <typename Real, int R, int MINB, bool PRE, typename Off>
 static cudaError_t ens_march_launch(const void* v1, const void* v2, const int4* items, int nitems, int* ctr,
@@ -218,12 +246,28 @@ static cudaError_t ens_march_launch(const void* v1, const void* v2, const int4* 
                   items, ctr);
 }
 
+template <typename Real, int TX, int TY, int NT, int MINB, typename Off>
+static cudaError_t ens_tile_launch(const void* v1, const void* v2, const int4* items, int nitems, int* ctr,
+                                   cudaStream_t s) {
+  constexpr int MB = std::is_same<Real, double>::value ? (MINB + 1) / 2 : MINB;
+  auto k = ens_tile_kernel<Real, TX, TY, NT, MB, Off>;
+  constexpr size_t smem = tile_smem_bytes<Real, TX, TY>();
+  static std::atomic<unsigned long long> attr_set{0};
+  const cudaError_t e = smem_limit_once((const void*)k, smem, attr_set);
+  if (e != cudaSuccess) return e;
+  if (nitems <= 0) return cudaSuccess;
+  return launch_k(k, nitems, NT, smem, s, true, (const LBView<Real>*)v1, (const LBView<Real>*)v2, items, ctr);
+}
+
 template <typename Real, typename Off>
 static cudaError_t ens_march_dispatch(int variant, const void* v1, const void* v2, const int4* items, int nitems,
                                       int* ctr, cudaStream_t s) {
+  static_assert(ENS_PAIR_VARIANTS == 5, "pair variants");
   switch (variant) {
     case 1: return ens_march_launch<Real, 8, 3, true, Off>(v1, v2, items, nitems, ctr, s);
     case 2: return ens_march_launch<Real, 6, 4, true, Off>(v1, v2, items, nitems, ctr, s);
+    case 3: return ens_tile_launch<Real, 32, 8, 256, 5, Off>(v1, v2, items, nitems, ctr, s);
+    case 4: return ens_tile_launch<Real, 30, 8, 320, 3, Off>(v1, v2, items, nitems, ctr, s);
     default: return ens_march_launch<Real, 8, 3, false, Off>(v1, v2, items, nitems, ctr, s);
   }
 }

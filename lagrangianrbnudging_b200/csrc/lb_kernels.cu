@@ -67,142 +67,13 @@ __global__ void __launch_bounds__(BS, MINB) lb_node_kernel(const LBView<Real> V)
 }
 
 // ------------------------------------------------------- two steps per launch
-// Temporal blocking of two steps n, n+1 (Dirichlet walls, no ghost rows, no
-// nudging in between).  A block owns a TX x TY tile.  Phase 1 computes step n
-// at the tile and a one-node ring around it (x wrapped, rows outside the
-// domain skipped) from HBM, exactly as lb_update_node does, and keeps the
-// post-collision populations in shared memory; at the tile it also stores
-// u^n, v^n (and T^n on a record step) to HBM through V1, and keeps the next
-// buoyancy F^{n+1} in shared memory.  Phase 2 computes step n+1 at the tile,
-// pulling from shared memory with the same wall rules as pull_node (bounce-back
-// from the node's own opposite population, anti-bounce-back for g), and
-// stores through V2.  Populations and F cross HBM once per two steps; the
-// ring is recomputed (34 x 10 nodes for a 32 x 8 tile).  The per-node
-// arithmetic is lb_update_node's, so two steps here equal two launches of
-// lb_node_kernel bit for bit.
-// On a y-slab the ring rows beyond an inner boundary come from the ghost
-// blocks (lb_pair.cuh: pull_ghost_row).
-
-// NT threads per block: TX * TY (phase 1 takes the region in passes), or
-// one per region node rounded to whole warps (phase 1 in one pass; phase 2
-// leaves the rest idle)
+// Temporal blocking of two steps n, n+1 in TX x TY tiles, one per block
+// (lb_pair.cuh: tile_block, the per-block work).
 template <typename Real, int TX, int TY, int NT, int MINB, typename Off>
 __global__ void __launch_bounds__(NT, MINB) lb_pair_kernel(const LBView<Real> V1, const LBView<Real> V2) {
   pdl_wait();
-  constexpr int RX = TX + 2, RY = TY + 2, RN = RX * RY;
   extern __shared__ __align__(16) unsigned char pair_smem[];
-  Real* S = reinterpret_cast<Real*>(pair_smem);  // [2 * NPOP][RY][RX]: f then g of step n
-  Real* SF = S + 2 * NPOP * RN;                   // [TY][TX]: F^{n+1} at the tile
-  const int nx = V1.nx, ny = V1.ny;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int ncols = min(TX, nx - x0), nrows = min(TY, ny - y0);
-  const Off pitch = (Off)V1.pitch;
-  // y-slab: the rows beyond an inner boundary are computed from ghost blocks
-  const bool glo = V1.gh2_lo != nullptr, ghi = V1.gh2_hi != nullptr;
-  // FP64: a full tile whose ring, and the ring's pulls, lie strictly inside
-  // the domain (no x wrap, no wall row, no slab ghost row) in a run without
-  // in-launch nudging sums takes phase 1 by fixed offsets from each node:
-  // the values pull_node's interior path reads, without its bounds, wrap and
-  // wall logic (block-uniform).  (In FP32 the second copy of the phase made
-  // the launch 10% slower, so FP32 keeps the one general phase.)
-  const bool fast = ncols == TX && nrows == TY && x0 >= 2 && x0 + TX + 1 <= nx - 1 && y0 >= 2 &&
-                    y0 + TY + 1 <= ny - 1 && !V1.nmask;
-  auto phase1 = [&](auto fastc) {
-    constexpr bool FAST = decltype(fastc)::value;
-    for (int q = threadIdx.x; q < RN; q += NT) {
-      const int lx = q % RX, ly = q / RX;
-      const int jg = y0 - 1 + ly;
-      Real fs[NPOP], gs[NPOP];
-      Real Fy, r, u, v, t;
-      Off o;
-      long long nsum = 0;
-      double nsv = 0.0;
-      if constexpr (FAST) {
-        const int xg = x0 - 1 + lx;
-        o = (Off)jg * pitch + (Off)xg;
-        const Off pl = (Off)V1.plane;
-        static_for<NPOP>([&](auto kc) {
-          constexpr int k = decltype(kc)::value;
-          const Off src = (Off)k * pl + o + (Off)(-icy(k) * V1.pitch - icx(k));  // (modular: a negative shift wraps)
-          fs[k] = __ldcs(V1.fsrc + src);
-          gs[k] = __ldcs(V1.gsrc + src);
-        });
-        Fy = V1.Fin[o];
-      } else {
-        if (lx > ncols + 1 || ly > nrows + 1 || jg < (glo ? -1 : 0) || jg > (ghi ? ny : ny - 1)) continue;
-        int xg = x0 - 1 + lx;
-        if (xg < 0) xg += nx;
-        else if (xg >= nx) xg -= nx;
-        o = (Off)(jg < 0 ? 0 : (jg >= ny ? ny - 1 : jg)) * pitch + (Off)xg;  // (ring rows of a slab: no stores)
-        if (jg < 0 || jg >= ny) {
-          pull_ghost_row<Real, Off>(V1, jg < 0, xg, fs, gs, Fy);
-        } else {
-          pull_node<Real, LBRB_TWALL_DIRICHLET, Off, true>(V1, jg, xg, fs, gs);
-          dirichlet_walls(V1, jg, gs);
-          Fy = V1.Fin[o];
-        }
-        // (nudged run: step n's sums join g after the collision, as the apply pass does)
-        if (V1.nmask) {
-          nsum = pair_nudge_sum(V1, jg, xg, (size_t)o);
-          if (nsum != 0) nsv = (double)nsum * (1.0 / FIX_SCALE);
-        }
-      }
-      lb_collide<Real, false>(
-          V1, (size_t)o, fs, gs, Fy, r, u, v, t, [&](int k, Real val) { S[(k * RY + ly) * RX + lx] = val; },
-          [&](int k, Real val) {
-            if (!FAST && nsum != 0) val = val + nudge_increment<Real>(k, nsv);
-            S[((NPOP + k) * RY + ly) * RX + lx] = val;
-          });
-      if (lx >= 1 && lx <= ncols && ly >= 1 && ly <= nrows) {
-        SF[(ly - 1) * TX + (lx - 1)] = Fy;
-        if (V1.write_F) V1.Fout[o] = Fy;
-        if (V1.write_uv) {
-          V1.u[o] = u;
-          V1.v[o] = v;
-        }
-        if (V1.write_rt & 1) V1.T[o] = t;
-        if (V1.write_rt & 2) V1.rho[o] = r;
-      }
-    }
-  };
-  if constexpr (std::is_same<Real, double>::value) {
-    if (fast) phase1(std::true_type{});
-    else phase1(std::false_type{});
-  } else {
-    phase1(std::false_type{});
-  }
-  __syncthreads();
-  if (threadIdx.x >= TX * TY) return;
-  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-  if (tx >= ncols || ty >= nrows) return;
-  const int x = x0 + tx, j = y0 + ty;
-  Real fs[NPOP], gs[NPOP];
-  // a tile whose rows and their neighbours all lie in the domain (or beyond
-  // an inner slab edge) pulls with no wall rule (block-uniform)
-  const bool inner = (y0 > 0 || glo) && (y0 + nrows < ny || ghi);
-  if (inner) {
-    static_for<NPOP>([&](auto kc) {
-      constexpr int k = decltype(kc)::value;
-      const int lx = tx + 1 - icx(k), ly = ty + 1 - icy(k);
-      fs[k] = S[(k * RY + ly) * RX + lx];
-      gs[k] = S[((NPOP + k) * RY + ly) * RX + lx];
-    });
-  } else {
-    static_for<NPOP>([&](auto kc) {
-      constexpr int k = decltype(kc)::value;
-      const int js = j - icy(k);
-      if ((js < 0 && !glo) || (js >= ny && !ghi)) {
-        fs[k] = S[(opp(k) * RY + ty + 1) * RX + tx + 1];
-        gs[k] = Real(0);
-      } else {
-        const int lx = tx + 1 - icx(k), ly = ty + 1 - icy(k);
-        fs[k] = S[(k * RY + ly) * RX + lx];
-        gs[k] = S[((NPOP + k) * RY + ly) * RX + lx];
-      }
-    });
-    dirichlet_walls(V2, j, gs);
-  }
-  lb_finish_node<Real, false, Off>(V2, (Off)j * pitch + (Off)x, fs, gs, SF[ty * TX + tx]);
+  tile_block<Real, TX, TY, NT, Off>(V1, V2, blockIdx.x * TX, blockIdx.y * TY, pair_smem);
 }
 
 template <typename Real, int R, int MINB, bool PRE, typename Off>
@@ -226,7 +97,7 @@ static_assert(NPAIR <= NUM_PAIR_SHAPES, "pair shape table");
 
 template <typename Real, int TX, int TY, int NT, int MINB>
 static cudaError_t launch_pair_t(const LBView<Real>& V1, const LBView<Real>& V2, cudaStream_t s, bool pdl) {
-  const size_t smem = ((size_t)2 * NPOP * (TX + 2) * (TY + 2) + (size_t)TX * TY) * sizeof(Real);
+  constexpr size_t smem = tile_smem_bytes<Real, TX, TY>();
   dim3 grid((V1.nx + TX - 1) / TX, (V1.ny + TY - 1) / TY);
   auto go = [&](auto kernel) -> cudaError_t {
     // the shared-memory limit is a per-device attribute of the kernel: set

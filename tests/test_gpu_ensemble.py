@@ -1,7 +1,7 @@
 """The ensemble (lbrb_ensemble_*): members of uneven grid size, closure,
 particles and nudging advanced by one launch per phase of the step, or two
-steps per launch (the marching kernel over all members, nudged members
-included), replayed from CUDA graphs, end bit-identical to the same handles
+steps per launch (a marching or tile kernel over all members, nudged
+members included), replayed from CUDA graphs, end bit-identical to the same handles
 advanced alone by lbrb_step -- whatever the launch variant, with or without
 the graphs, and with per-member steps in between."""
 import numpy as np
@@ -89,6 +89,28 @@ def test_ensemble_matches_members_stepped_alone(precision, pairs):
         assert_same(snapshot(a), snapshot(b))
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_every_pair_variant_matches_members_stepped_alone(precision):
+    """each two-step launch variant (marching groups, 32 x 8 and 30 x 8
+    tiles, ragged at the members' edges), 14 steps = 6 pairs from the graph
+    + 1 pair + 1 single step"""
+    B = [make_member(s, precision) for s in SPECS]
+    for r in B:
+        r.step(14)
+    ref = [snapshot(b) for b in B]
+    for v in range(lb.Ensemble.pair_variants()):
+        A = [make_member(s, precision) for s in SPECS]
+        with lb.Ensemble(A) as ens:
+            ens.set_pairs(1)
+            ens.set_pair_variant(v)
+            ens.step(14)
+            ens.sync()
+            p = ens.pairs()
+        assert p["variant"] == v and p["tuned_ms"] == 0
+        for a, b in zip(A, ref):
+            assert_same(snapshot(a), b)
+
+
 def test_every_launch_variant_gives_identical_results():
     ref = None
     for v in range(lb.Ensemble.nvariants()):
@@ -156,7 +178,8 @@ def test_pair_timing_mode_launches_directly_with_same_results():
         ea.sync()
         eb.sync()
         p = ea.pairs()
-    assert p["mode"] == -1 and p["rows"] in (4, 8, 16) and p["tuned_ms"] > 0
+    assert p["mode"] == -1 and p["rows"] in (6, 8) and p["tuned_ms"] > 0
+    assert 0 <= p["variant"] < lb.Ensemble.pair_variants() and p["tile_cols"] in (0, 30, 32)
     assert t["lb_step"][1] == 8 and t["aux"][1] == 8 and t["apply"][1] == 2 * 6 + 2
     for a, b in zip(A, B):
         assert_same(snapshot(a), snapshot(b))
