@@ -575,18 +575,28 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = 
             w.adjoint_set_variant(variant)
         stream = torch.cuda.Stream()
         w.set_stream(stream.cuda_stream)
-        # warm-up at the window's own size: checkpoint and segment buffers,
-        # launch-shape and pair-kernel autotuning happen here, untimed
+        # warm-up at the window's own size: the state store (the default when
+        # it fits) or checkpoint and segment buffers, launch-shape and
+        # pair-kernel autotuning happen here, untimed
         w.adjoint_window(T0, nsteps, K, gradient=True)
         pair_variant = w.adjoint_variant()
+        store = w.adjoint_store()
         sync_ranks(torch, dist)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
         ev[0].record(stream)
         w.adjoint_window(T0, nsteps, K, gradient=False)
         ev[1].record(stream)
         ev[2].record(stream)
         J, grad = w.adjoint_window(T0, nsteps, K, gradient=True)
         ev[3].record(stream)
+        # the same gradient window with checkpoints every K steps and the
+        # segments recomputed (the form for windows whose store does not
+        # fit), after its own untimed warm-up
+        w.adjoint_set_store(0)
+        w.adjoint_window(T0, nsteps, K, gradient=True)
+        ev[6].record(stream)
+        Jr, gradr = w.adjoint_window(T0, nsteps, K, gradient=True)
+        ev[7].record(stream)
         # plain forward steps of the same grid, for the cost ratio
         w.init_conduction(1, 1e-3)
         w.step(10)
@@ -596,6 +606,7 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = 
         torch.cuda.synchronize()
         t_fwd_window = max_over_ranks(torch, dist, ev[0].elapsed_time(ev[1]))
         t_adj = max_over_ranks(torch, dist, ev[2].elapsed_time(ev[3]))
+        t_rec = max_over_ranks(torch, dist, ev[6].elapsed_time(ev[7]))
         t_step = max_over_ranks(torch, dist, ev[4].elapsed_time(ev[5]) / nsteps)
         w.set_stream(None)
     fd = adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir=8, dist=dist, rank=rank,
@@ -615,7 +626,12 @@ def run_adjoint_bench(lb, torch, device: int, nsteps: int = ADJ_STEPS, K: int = 
             # the backward sweep alone (recompute + adjoint) per step, in plain forward steps
             "backward_sweep_vs_forward_steps": round((t_adj - t_fwd_window) / (nsteps * t_step), 2),
             # gradient over function: the gradient window against the misfit window
-            "gradient_over_misfit": round(t_adj / t_fwd_window, 2)}
+            "gradient_over_misfit": round(t_adj / t_fwd_window, 2),
+            "states": ("store of every state's F and moments, " f"{store['bytes'] / 1e9:.1f} GB"
+                       if store["used_last"] else f"checkpoints every {K} steps, segments recomputed"),
+            "checkpoint_recompute": {"ms_gradient_window": round(t_rec, 2),
+                                     "cost_vs_forward_steps": round(t_rec / (nsteps * t_step), 2),
+                                     "same_gradient": bool(J == Jr and np.array_equal(grad, gradr))}}
 
 
 def adjoint_fd_check(lb, base, steps, ox, oy, oT, T0, nsteps, device, ndir, h=1e-6, seed=2024,

@@ -280,9 +280,12 @@ LBRB_API int lbrb_adjoint_set_obs(lbrb_t *h, int nobs_steps, const int *steps, i
  * return the misfit J = sum over the observations of (T(x,t) - T_obs)^2,
  * T(x,t) the bilinear interpolation of the step's temperature.  If dJdT0 is
  * not NULL, also its gradient with respect to T0 ([ny][nx]) by the adjoint
- * of the time step, recomputing the forward from checkpoints taken every
- * `checkpoint_every` steps.  Dirichlet walls, no nudging; the handle's state
- * ends at the end of the window; particles are not advanced. */
+ * of the time step.  The backward pass reads each forward state's F and
+ * moments: from a store of all of them (see lbrb_adjoint_set_store), or by
+ * recomputing the forward from checkpoints taken every `checkpoint_every`
+ * steps (`checkpoint_every` is unused in store mode).  Dirichlet walls, no
+ * nudging; the handle's state ends at the end of the window; particles are
+ * not advanced. */
 LBRB_API int lbrb_adjoint_window(lbrb_t *h, const double *T0, int nsteps, int checkpoint_every,
                                  double *J, double *dJdT0);
 /* Launch variant of the two-step adjoint kernel, 0 .. lbrb_adjoint_variants()-1:
@@ -293,6 +296,20 @@ LBRB_API int lbrb_adjoint_window(lbrb_t *h, const double *T0, int nsteps, int ch
 LBRB_API int lbrb_adjoint_variants(void);
 LBRB_API int lbrb_adjoint_set_variant(lbrb_t *h, int variant);
 LBRB_API int lbrb_adjoint_get_variant(const lbrb_t *h, int *variant);
+/* How a gradient window keeps the forward states for its backward pass.
+ * 1: a store of every state's F and moments, 5 planes per step, (nsteps+1) x
+ *    5 x pitch x ny elements of the handle's precision (21 GB at 1024x512 over
+ *    2000 steps in FP32), allocated by the window and kept by the handle for
+ *    the next one; nothing is recomputed.  LBRB_ERR_NOMEM if it cannot be
+ *    allocated.
+ * 0: checkpoints every checkpoint_every steps, each segment recomputed during
+ *    the backward pass (memory of two segments); frees a store.
+ * -1 (the default): the store when it fits in half of the device's free
+ *    memory, else checkpoints.
+ * Both give the same J and gradient, bit for bit.  get_store: the mode, whether
+ * the last gradient window stored (1) or recomputed (0), and the store's size. */
+LBRB_API int lbrb_adjoint_set_store(lbrb_t *h, int mode);
+LBRB_API int lbrb_adjoint_get_store(const lbrb_t *h, int *mode, int *used_last, size_t *bytes);
 
 /* ---- ensemble (no counterpart in the reference) ---------------------------
  * Independent runs ("members": handles made by lbrb_create, of any grid size

@@ -47,6 +47,7 @@ EXPORTS = [
     "lbrb_ensemble_set_pair_variant", "lbrb_ensemble_get_pair_variant",
     "lbrb_ensemble_set_timing", "lbrb_ensemble_get_timing",
     "lbrb_adjoint_variants", "lbrb_adjoint_set_variant", "lbrb_adjoint_get_variant",
+    "lbrb_adjoint_set_store", "lbrb_adjoint_get_store",
     "lbrb_slab_set", "lbrb_slab_ghost_bytes", "lbrb_slab_buffers", "lbrb_slab_pack", "lbrb_slab_step",
     "lbrb_slab_ghost2_bytes", "lbrb_slab_buffers2", "lbrb_slab_pack2",
     "lbrb_slab_particles_set", "lbrb_slab_particle_bytes", "lbrb_slab_particle_buffers",
@@ -143,6 +144,8 @@ def lib() -> C.CDLL:
         "lbrb_adjoint_variants": (C.c_int, []),
         "lbrb_adjoint_set_variant": (C.c_int, [vp, C.c_int]),
         "lbrb_adjoint_get_variant": (C.c_int, [vp, ip]),
+        "lbrb_adjoint_set_store": (C.c_int, [vp, C.c_int]),
+        "lbrb_adjoint_get_store": (C.c_int, [vp, ip, ip, C.POINTER(C.c_size_t)]),
         "lbrb_slab_set": (C.c_int, [vp, C.c_int, C.c_int]),
         "lbrb_slab_ghost_bytes": (C.c_size_t, [vp]),
         "lbrb_slab_buffers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
@@ -382,6 +385,16 @@ class Run:
         v = C.c_int()
         self._ck(lib().lbrb_adjoint_get_variant(self.h, C.byref(v)))
         return v.value
+
+    def adjoint_set_store(self, mode: int):
+        """1: keep every forward state's F and moments; 0: checkpoints and
+        recompute; -1: the store when it fits (lbrb_adjoint_set_store)"""
+        self._ck(lib().lbrb_adjoint_set_store(self.h, int(mode)))
+
+    def adjoint_store(self) -> dict:
+        m, u, b = C.c_int(), C.c_int(), C.c_size_t()
+        self._ck(lib().lbrb_adjoint_get_store(self.h, C.byref(m), C.byref(u), C.byref(b)))
+        return {"mode": m.value, "used_last": u.value, "bytes": b.value}
 
     def adjoint_set_obs(self, steps, x, y, T):
         steps = _i32(steps)

@@ -708,11 +708,12 @@ static cudaError_t launch_march_t(const AdjPairView<Real>& P, int waves, cudaStr
 constexpr int ADJ_NPAIR_VARIANTS = 10;
 int adjoint_pair_variants() { return ADJ_NPAIR_VARIANTS; }
 
-// steps n and n-1 from three state slots: after_a (the state after step n:
-// its moment planes are step n's linearisation point), state_a (before step
-// n: F^n, and in its moment planes step n-1's), state_b (before step n-1:
-// F^{n-1}); lambda^n in (lf_out, lg_out), lambda^{n-2} out (lf_in, lg_in),
-// lambda F^{n+1} in (lF_in), lambda F^{n-1} out (lF_out)
+// steps n and n-1 from the moment blocks (MB_PLANES planes: F, rho, u, v, T)
+// of three states: after_a (the state after step n: its moments are step n's
+// linearisation point), state_a (before step n: F^n, and its moments are
+// step n-1's), state_b (before step n-1: F^{n-1}); lambda^n in (lf_out,
+// lg_out), lambda^{n-2} out (lf_in, lg_in), lambda F^{n+1} in (lF_in),
+// lambda F^{n-1} out (lF_out)
 cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* after_a, const void* state_a,
                                 const void* state_b, const double* lf_out, const double* lg_out,
                                 double* lf_in, double* lg_in, double* lF_in, double* lF_out,
@@ -725,11 +726,11 @@ cudaError_t launch_adjoint_pair(bool fp32, int variant, const void* after_a, con
     const Real* a = (const Real*)state_a;
     const Real* b = (const Real*)state_b;
     AdjPairView<Real> P{};
-    P.a = AdjView<Real>{n1 + SLOT_MOM * plane, a + SLOT_F * plane, lf_out, lg_out, nullptr, nullptr,
+    P.a = AdjView<Real>{n1 + plane, a, lf_out, lg_out, nullptr, nullptr,
                         lF_in, const_cast<long long*>(lT_a), nx, ny, pitch, plane, omega, omegag,
                         gbeta, T0, Tup, Tdown};
-    P.mom_b = a + SLOT_MOM * plane;
-    P.Fin_b = b + SLOT_F * plane;
+    P.mom_b = a + plane;
+    P.Fin_b = b;
     P.lT_b = lT_b;
     P.lf_in = lf_in;
     P.lg_in = lg_in;
@@ -756,20 +757,20 @@ static cudaError_t launch_adj_t(const AdjView<Real>& V, cudaStream_t s) {
   return launch_k(adjoint_step_kernel<Real>, grid, 128, 0, s, true, V);
 }
 
-// one step from two state slots: `after` (its moments: the step's
-// linearisation point) and `state` (before the step: F)
+// one step from the moment blocks of two states: `after` (its moments: the
+// step's linearisation point) and `state` (before the step: F)
 cudaError_t launch_adjoint_step(bool fp32, const void* after, const void* state, const double* lf_out,
                                 const double* lg_out, double* lf_in, double* lg_in, double* lF,
                                 long long* lT, int nx, int ny, int pitch, size_t plane, double omega,
                                 double omegag, double gbeta, double T0, double Tup, double Tdown,
                                 cudaStream_t s) {
   if (fp32) {
-    AdjView<float> V{(const float*)after + SLOT_MOM * plane, (const float*)state + SLOT_F * plane, lf_out,
+    AdjView<float> V{(const float*)after + plane, (const float*)state, lf_out,
                      lg_out, lf_in, lg_in, lF, lT, nx, ny, pitch, plane, omega, omegag, gbeta, T0, Tup,
                      Tdown};
     return launch_adj_t(V, s);
   }
-  AdjView<double> V{(const double*)after + SLOT_MOM * plane, (const double*)state + SLOT_F * plane, lf_out,
+  AdjView<double> V{(const double*)after + plane, (const double*)state, lf_out,
                     lg_out, lf_in, lg_in, lF, lT, nx, ny, pitch, plane, omega, omegag, gbeta, T0, Tup,
                     Tdown};
   return launch_adj_t(V, s);

@@ -262,6 +262,7 @@ static void free_all(lbrb_t* h) {
   delete[] h->h_chk; delete[] h->h_oid;
   F(h->obs); F(h->acc); F(h->acc2); F(h->nmask); F(h->staging); F(h->big); F(h->red); F(h->dflags);
   F(h->adj_obs); F(h->adj_res); F(h->adj_chk); F(h->adj_seg); F(h->adj_lam); F(h->adj_lT); F(h->adj_T0);
+  F(h->adj_store);
   F(h->slab_ghost_lo); F(h->slab_ghost_hi); F(h->slab_up); F(h->slab_down); F(h->slab_tab);
   free_sp(h->sp);
   h->sp = nullptr;
@@ -1192,12 +1193,18 @@ static int grow(lbrb_t* h, void** p, size_t* have, size_t need) {
   return LBRB_OK;
 }
 
-// Assimilation window with checkpoints every K steps.
-// Forward: step i of segment c reads its input state from checkpoint c (i = 0)
-// or segment slot i, and writes its output to slot i+1 -- or, for the
-// segment's last step, to checkpoint c+1 (the window's end state: slot K).
-// The last segment's states are therefore still in the slots when the
-// backward pass starts and need no recompute.
+// Assimilation window, in one of two forms that give the same J and gradient
+// bit for bit.
+// Store (a gradient window whose moment blocks fit, or lbrb_adjoint_set_store
+// 1): the forward pass writes every state's moment block (F and the
+// moments, MB_PLANES planes) to the store, two steps per launch, the
+// populations alternating between two slots; the backward pass reads the
+// store and recomputes nothing.
+// Checkpoints every K steps (otherwise): step i of segment c reads its input
+// state from checkpoint c (i = 0) or segment slot i, and writes its output to
+// slot i+1 -- or, for the segment's last step, to checkpoint c+1 (the
+// window's end state: slot K).  The last segment's states are therefore still
+// in the slots when the backward pass starts and need no recompute.
 // Backward: segments last to first; each is recomputed into the slots (all
 // but the last), then its steps run in reverse, two at a time through the
 // pair kernel (lambda crosses HBM once per two steps) and one at a time for
@@ -1214,14 +1221,33 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   const int nx = h->p.nx, ny = h->p.ny, pitch = h->pitch;
   const size_t plane = h->plane, es = h->esize;
   const size_t sb = SLOT_PLANES * plane * es;  // one state slot: pops, F, moments
+  const size_t mbb = MB_PLANES * plane * es;    // one moment block: F, moments
   const size_t nn = (size_t)nx * ny;
-  if (K > nsteps) K = nsteps;
-  const int nchk = (nsteps + K - 1) / K;
   int rc;
-  if ((rc = grow(h, &h->adj_chk, &h->adj_chk_bytes, (size_t)nchk * sb))) return rc;
+  // store mode: every state's moment block, when asked or when it fits in
+  // half of the free device memory (the store of an earlier window counts
+  // as free: it is released before a larger one is allocated)
+  bool store = false;
+  if (dJdT0 && h->adj_store_mode != 0) {
+    const size_t need = (size_t)(nsteps + 1) * mbb;
+    store = h->adj_store_mode == 1 || h->adj_store_bytes >= need;
+    if (!store) {
+      size_t fr = 0, tot = 0;
+      CK(h, cudaMemGetInfo(&fr, &tot));
+      store = need <= (fr + h->adj_store_bytes) / 2;
+    }
+    if (store && (rc = grow(h, &h->adj_store, &h->adj_store_bytes, need))) return rc;
+  }
+  h->adj_store_used = store ? 1 : 0;
+  // store mode: one segment of the whole window (no checkpoints), the
+  // populations alternating between checkpoint slots 0 and 1 (slot 2 takes
+  // the pair tuner's second output)
+  if (K > nsteps || store) K = nsteps;
+  const int nchk = (nsteps + K - 1) / K;
+  if ((rc = grow(h, &h->adj_chk, &h->adj_chk_bytes, (size_t)(store ? 3 : nchk) * sb))) return rc;
   // two segment buffers: the backward sweep of one segment reads one while
   // the recompute of the segment before it fills the other
-  if ((rc = grow(h, &h->adj_seg, &h->adj_seg_bytes, 2 * (size_t)(K + 1) * sb))) return rc;
+  if (!store && (rc = grow(h, &h->adj_seg, &h->adj_seg_bytes, 2 * (size_t)(K + 1) * sb))) return rc;
   if (!h->adj_T0 && cudaMalloc(&h->adj_T0, nn * sizeof(double)) != cudaSuccess)
     return fail(h, LBRB_ERR_NOMEM, "adjoint T0");
   CK(h, cudaMemcpyAsync(h->adj_T0, T0, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -1234,6 +1260,10 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   const int nob = h->adj_nobs;
   char* chk = (char*)h->adj_chk;
   char* seg = (char*)h->adj_seg;
+  char* const mstore = (char*)h->adj_store;
+  // where the tuners' trial launches write (overwritten by the forward pass)
+  char* const trial1 = store ? chk + sb : seg + sb;
+  char* const trial2 = store ? chk + 2 * sb : seg + 2 * sb;
   // segment c's states live in buffer (nchk-1-c) % 2: the last segment, which
   // the forward pass leaves in place, in buffer 0
   auto segbuf = [&](int c) -> char* { return seg + (size_t)((nchk - 1 - c) & 1) * (K + 1) * sb; };
@@ -1244,17 +1274,21 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     if (i < std::min(K, nsteps - c * K)) return state_in(c, i);
     return c + 1 < nchk ? chk + (size_t)(c + 1) * sb : segbuf(c) + (size_t)K * sb;
   };
-  // the window's initial state in checkpoint 0 (pops + F), moments in buffer 0
+  // the moment block of a slot, and of state s in the store
+  auto mb = [&](char* slot) -> char* { return slot + (size_t)SLOT_F * plane * es; };
+  auto mblk = [&](int s) -> char* { return mstore + (size_t)s * mbb; };
+  // the window's initial state in checkpoint 0 (pops + F), moments in
+  // buffer 0; in store mode F also in the store's block 0
   CK(h, launch_init_from_T0(h->adj_T0, chk, h->rho[0], h->uv[h->uvcur][0], h->uv[h->uvcur][1],
-                            h->T[0], chk + 2 * NPOP * plane * es, f32, nx, ny, pitch, plane, T0ref,
-                            ng, h->stream));
+                            h->T[0], mb(chk), f32, nx, ny, pitch, plane, T0ref, ng, h->stream));
+  if (store) CK(h, cudaMemcpyAsync(mblk(0), mb(chk), plane * es, cudaMemcpyDeviceToDevice, h->stream));
   if (h->lb_shape < 0) {
     // the fused kernel's launch shape, timed on this window's initial state
     int sh = h->p.launch_shape;
     float ms = 0.f;
     if (h->p.autotune) {
-      if (f32) sh = tune_lb_fp32(seg_view<float>(h, chk, seg + sb, 0), h->p.twall, h->stream, &ms);
-      else sh = tune_lb_fp64(seg_view<double>(h, chk, seg + sb, 0), h->p.twall, h->stream, &ms);
+      if (f32) sh = tune_lb_fp32(seg_view<float>(h, chk, trial1, 0), h->p.twall, h->stream, &ms);
+      else sh = tune_lb_fp64(seg_view<double>(h, chk, trial1, 0), h->p.twall, h->stream, &ms);
     }
     CK(h, cudaGetLastError());
     h->lb_shape = sh;
@@ -1273,24 +1307,78 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   const bool fwd_pairs = pairs_ok(h) && nsteps >= 2;
   if (fwd_pairs && h->pair_shape < 0) {
     // the pair tile shape, timed on the window's initial state (trial
-    // launches write segment slots 1 and 2, which the forward pass overwrites)
+    // launches write two slots that the forward pass overwrites)
     float ms = 0.f;
     int sh = 0;
-    if (f32) sh = tune_pair_fp32(seg_view<float>(h, chk, seg + sb, 0), seg_view<float>(h, chk, seg + 2 * sb, 0), h->stream, &ms);
-    else sh = tune_pair_fp64(seg_view<double>(h, chk, seg + sb, 0), seg_view<double>(h, chk, seg + 2 * sb, 0), h->stream, &ms);
+    if (f32) sh = tune_pair_fp32(seg_view<float>(h, chk, trial1, 0), seg_view<float>(h, chk, trial2, 0), h->stream, &ms);
+    else sh = tune_pair_fp64(seg_view<double>(h, chk, trial1, 0), seg_view<double>(h, chk, trial2, 0), h->stream, &ms);
     CK(h, cudaGetLastError());
     h->pair_shape = sh;
     h->pair_ms = ms;
     if (h->pair_mode < 0 && h->lb_shape_ms > 0.f && ms >= 2.f * h->lb_shape_ms) h->pair_mode = 0;
   }
-  auto residual = [&](int oi, const char* state) -> cudaError_t {
+  // residual of observation step oi from a moment block's T
+  auto residual = [&](int oi, const char* mblock) -> cudaError_t {
     const double* ob = h->adj_obs + (size_t)oi * 3 * nob;
-    return launch_obs_residual(state + (SLOT_MOM + 3) * plane * es, f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob,
+    return launch_obs_residual(mblock + 4 * plane * es, f32, nx, ny, pitch, ob, ob + nob, ob + 2 * nob,
                                nob, h->adj_res + (size_t)oi * nob, h->stream);
   };
-  // ---- forward pass: checkpoints, residuals
-  char* end_state = nullptr;
-  for (int c = 0; c < nchk; c++) {
+  // ---- forward pass: checkpoints (or the store), residuals
+  char* end_state = nullptr;  // populations of the window's end state
+  char* end_F = nullptr;      // its F
+  if (store) {
+    // every state's moment block into the store; two steps per launch, the
+    // first step's F and moments stored too, so observation steps need not
+    // end a launch
+    char* pop[2] = {chk, chk + sb};
+    int pc = 0;
+    // one step's view: populations pop[pc] -> pop[pc ^ 1], F of state s in,
+    // F and moments of state s + 1 out
+    auto sview = [&](auto zero, int s) {
+      using Real = decltype(zero);
+      LBView<Real> V = make_view<Real>(h, 0, 1, h->uvcur, 1, 3);
+      const Real* a = (const Real*)pop[pc];
+      Real* b = (Real*)pop[pc ^ 1];
+      const Real* mi = (const Real*)mblk(s);
+      Real* mo = (Real*)mblk(s + 1);
+      V.fsrc = a;
+      V.gsrc = a + NPOP * plane;
+      V.fdst = b;
+      V.gdst = b + NPOP * plane;
+      V.Fin = mi;
+      V.Fout = mo;
+      V.rho = mo + plane;
+      V.u = mo + 2 * plane;
+      V.v = mo + 3 * plane;
+      V.T = mo + 4 * plane;
+      return V;
+    };
+    for (int s = 0; s < nsteps;) {
+      if (fwd_pairs && h->pair_mode != 0 && s + 2 <= nsteps) {
+        if (f32) {
+          LBView<float> V1 = sview(0.f, s);
+          V1.write_F = 1;
+          CK(h, launch_pair_fp32(V1, sview(0.f, s + 1), h->pair_shape, h->stream, true));
+        } else {
+          LBView<double> V1 = sview(0.0, s);
+          V1.write_F = 1;
+          CK(h, launch_pair_fp64(V1, sview(0.0, s + 1), h->pair_shape, h->stream, true));
+        }
+        for (int q = 1; q <= 2; q++)
+          if (obs_at[s + q] >= 0) CK(h, residual(obs_at[s + q], mblk(s + q)));
+        s += 2;
+      } else {
+        if (f32) CK(h, launch_lb_fp32(sview(0.f, s), h->p.twall, shape, h->stream, true));
+        else CK(h, launch_lb_fp64(sview(0.0, s), h->p.twall, false, shape, h->stream, true));
+        if (obs_at[s + 1] >= 0) CK(h, residual(obs_at[s + 1], mblk(s + 1)));
+        s += 1;
+      }
+      pc ^= 1;
+    }
+    end_state = pop[pc];
+    end_F = mblk(nsteps);
+  }
+  for (int c = 0; c < nchk && !store; c++) {
     const int s0 = c * K, len = std::min(K, nsteps - s0);
     const bool last = c + 1 == nchk;
     // the last two segments keep every state for the backward pass (one in
@@ -1317,7 +1405,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
         else
           CK(h, launch_pair_fp64(seg_view<double>(h, cur_state, dst, 0), seg_view<double>(h, cur_state, dst, mom),
                                  h->pair_shape, h->stream, true));
-        if (oi >= 0) CK(h, residual(oi, dst));
+        if (oi >= 0) CK(h, residual(oi, mb(dst)));
         cur_state = dst;
         i += 2;
         continue;
@@ -1327,11 +1415,12 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
       // moments into every state the backward pass reads (and at observation
       // steps, for the residual's T)
       CK(h, launch_fwd(cur_state, dst, (dJdT0 && (keep || i + 1 == len)) || oi >= 0));
-      if (oi >= 0) CK(h, residual(oi, dst));
+      if (oi >= 0) CK(h, residual(oi, mb(dst)));
       cur_state = dst;
       i++;
     }
     end_state = cur_state;
+    end_F = mb(cur_state);
   }
   // misfit on the device (observation steps inside the window: a prefix)
   int nused = 0;
@@ -1343,7 +1432,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   {
     const size_t popb = 2 * NPOP * plane * es;
     CK(h, cudaMemcpyAsync(h->pops[h->cur], end_state, popb, cudaMemcpyDeviceToDevice, h->stream));
-    CK(h, cudaMemcpyAsync(h->F[h->cur], end_state + popb, plane * es, cudaMemcpyDeviceToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->F[h->cur], end_F, plane * es, cudaMemcpyDeviceToDevice, h->stream));
     h->prev_valid = false;
   }
   if (!dJdT0) {
@@ -1363,6 +1452,10 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
   CK(h, cudaMemsetAsync(h->adj_lam, 0, (4 * lp + 2 * plane) * sizeof(double), h->stream));
   CK(h, cudaMemsetAsync(h->adj_lT, 0, 2 * plane * sizeof(long long), h->stream));
   int lc = 0, fc = 0;  // lam[lc]: adjoint of the current state; lF[fc]: lambda F of the next step
+  // the moment blocks the backward pass reads: state i of segment c, and the
+  // state after i steps of segment c (in store mode, one segment: state i)
+  auto m_in = [&](int c, int i) -> char* { return store ? mblk(c * K + i) : mb(state_in(c, i)); };
+  auto m_after = [&](int c, int i) -> char* { return store ? mblk(c * K + i) : mb(after(c, i)); };
   auto scatter = [&](int s, long long* acc) -> cudaError_t {
     const int oi = obs_at[s];
     if (oi < 0) return cudaSuccess;
@@ -1388,8 +1481,8 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
       float best = 1e30f;
       for (int v = 0; v < adjoint_pair_variants(); v++) {
         auto trial = [&]() {
-          return launch_adjoint_pair(f32, v, after(nchk - 1, il + 1), state_in(nchk - 1, il),
-                                     state_in(nchk - 1, il - 1),
+          return launch_adjoint_pair(f32, v, m_after(nchk - 1, il + 1), m_in(nchk - 1, il),
+                                     m_in(nchk - 1, il - 1),
                                      lam[lc][0], lam[lc][1], lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc],
                                      lF[fc ^ 1], nullptr, nullptr, nx, ny, pitch, plane, om, omg, ng, T0ref,
                                      h->p.Tup, h->p.Tdown, h->stream);
@@ -1466,7 +1559,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
         CK(h, scatter(s, lT[0]));
         CK(h, scatter(s - 1, lT[1]));
         auto pair = [&](int variant) {
-          return launch_adjoint_pair(f32, variant, after(c, i + 1), state_in(c, i), state_in(c, i - 1),
+          return launch_adjoint_pair(f32, variant, m_after(c, i + 1), m_in(c, i), m_in(c, i - 1),
                                      lam[lc][0], lam[lc][1],
                                      lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc], lF[fc ^ 1],
                                      obs_at[s] >= 0 ? lT[0] : nullptr, obs_at[s - 1] >= 0 ? lT[1] : nullptr,
@@ -1481,7 +1574,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
         s -= 2;
       } else {
         CK(h, scatter(s, lT[0]));
-        CK(h, launch_adjoint_step(f32, after(c, i + 1), state_in(c, i),
+        CK(h, launch_adjoint_step(f32, m_after(c, i + 1), m_in(c, i),
                                   lam[lc][0], lam[lc][1], lam[lc ^ 1][0], lam[lc ^ 1][1], lF[fc],
                                   obs_at[s] >= 0 ? lT[0] : nullptr, nx, ny, pitch, plane, om, omg, ng,
                                   T0ref, h->p.Tup, h->p.Tdown, h->stream));
@@ -1511,6 +1604,27 @@ int lbrb_adjoint_set_variant(lbrb_t* h, int variant) {
 int lbrb_adjoint_get_variant(const lbrb_t* h, int* variant) {
   if (!h || !variant) return LBRB_ERR_ARG;
   *variant = h->adj_pair_variant;
+  return LBRB_OK;
+}
+
+int lbrb_adjoint_set_store(lbrb_t* h, int mode) {
+  if (!h || mode < -1 || mode > 1) return fail(h, LBRB_ERR_ARG, "adjoint_set_store: mode must be -1, 0 or 1");
+  h->adj_store_mode = mode;
+  if (mode == 0 && h->adj_store) {
+    CK(h, cudaSetDevice(h->dev));
+    CK(h, cudaStreamSynchronize(h->stream));
+    cudaFree(h->adj_store);
+    h->adj_store = nullptr;
+    h->adj_store_bytes = 0;
+  }
+  return LBRB_OK;
+}
+
+int lbrb_adjoint_get_store(const lbrb_t* h, int* mode, int* used_last, size_t* bytes) {
+  if (!h) return LBRB_ERR_ARG;
+  if (mode) *mode = h->adj_store_mode;
+  if (used_last) *used_last = h->adj_store_used;
+  if (bytes) *bytes = h->adj_store_bytes;
   return LBRB_OK;
 }
 

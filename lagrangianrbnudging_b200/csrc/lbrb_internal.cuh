@@ -129,6 +129,11 @@ inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t s
 // populations, F, then the moments the step that produced the state formed
 // (rho, u, v, T; the next step's adjoint linearises around them)
 constexpr int SLOT_F = 2 * NPOP, SLOT_MOM = 2 * NPOP + 1, SLOT_PLANES = 2 * NPOP + 5;
+// a state's moment block, all the adjoint reads of a state: F, then rho, u,
+// v, T -- a slot's planes SLOT_F .. SLOT_PLANES-1, or one entry of the
+// window's moment store (every state's block, when it fits)
+constexpr int MB_PLANES = SLOT_PLANES - SLOT_F;
+static_assert(SLOT_MOM == SLOT_F + 1 && MB_PLANES == 5, "moment block: F then the four moments");
 
 // x / c for a divisor c fixed at compile time, equal to the IEEE quotient
 // RN(x / c) without a division: with rc = RN(1 / c), q0 = RN(x rc) is within
@@ -374,6 +379,10 @@ struct Handle {
   long long* adj_lT = nullptr;       // 2 fixed-point lambda T planes (the steps of a pair)
   double* adj_T0 = nullptr;          // [ny*nx] initial temperature / gradient
   int adj_pair_variant = -1;         // launch variant of the pair kernel (-1: tune at first use)
+  void* adj_store = nullptr;         // every state's moment block (store mode)
+  size_t adj_store_bytes = 0;
+  int adj_store_mode = -1;           // 1 store, 0 checkpoint-recompute, -1 store when it fits
+  int adj_store_used = 0;            // the last gradient window stored (1) or recomputed (0)
   // scratch / staging: host transfers go through two staging slots of
   // stage_slot doubles each (allocated at create), chunk by chunk, with
   // events xfer_ev (copied[2], converted[2]) ordering the slots' reuse; the

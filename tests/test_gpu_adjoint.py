@@ -1,6 +1,8 @@
 """The CUDA adjoint of the time step (lbrb_adjoint_window) against the FP64
 tangent-linear model of the oracle, against central finite differences of the
-GPU's own FP64 forward, and across checkpoint intervals and precisions."""
+GPU's own FP64 forward, and across checkpoint intervals, the two ways of
+keeping the forward states (a store of every state, or checkpoints and
+recompute) and precisions."""
 import numpy as np
 import pytest
 
@@ -18,10 +20,14 @@ def case():
     return adjoint_case(seed=3)
 
 
-def gpu_window(c, precision, K, gradient=True, T0=None):
+def gpu_window(c, precision, K, gradient=True, T0=None, store=-1):
     with lb.Run(**c["base"], precision=precision) as r:
+        r.adjoint_set_store(store)
         r.adjoint_set_obs(c["steps"], c["ox"], c["oy"], c["oT"])
-        return r.adjoint_window(c["T0"] if T0 is None else T0, c["nsteps"], K, gradient=gradient)
+        out = r.adjoint_window(c["T0"] if T0 is None else T0, c["nsteps"], K, gradient=gradient)
+        if gradient and store >= 0:
+            assert r.adjoint_store()["used_last"] == store
+        return out
 
 
 def test_fp64_adjoint_matches_tangent_linear_model(case):
@@ -55,23 +61,60 @@ def test_fp64_adjoint_matches_gpu_finite_differences(case):
 
 def test_checkpoint_interval_does_not_change_the_gradient(case):
     c = case
-    g1 = gpu_window(c, "fp64", K=1)[1]
-    g7 = gpu_window(c, "fp64", K=7)[1]
-    gall = gpu_window(c, "fp64", K=c["nsteps"])[1]
+    g1 = gpu_window(c, "fp64", K=1, store=0)[1]
+    g7 = gpu_window(c, "fp64", K=7, store=0)[1]
+    gall = gpu_window(c, "fp64", K=c["nsteps"], store=0)[1]
     np.testing.assert_array_equal(g1, g7)
     np.testing.assert_array_equal(g1, gall)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("shape", [None, (40, 13)])
-def test_every_pair_kernel_variant_gives_the_same_gradient(case, precision, shape):
+def test_state_store_equals_checkpoint_recompute(case, precision, shape):
+    """every state's moments kept (no recompute) against checkpoints every K
+    steps with the segments recomputed: J and gradient bit-identical, on an
+    even window (the 48x24 case) and an odd one (17 steps, partial strips)"""
+    c = case if shape is None else adjoint_case(seed=9, nx=shape[0], ny=shape[1], nsteps=17, every=3,
+                                                nobs=11)
+    Js, gs = gpu_window(c, precision, K=5, store=1)
+    for K in (1, 5, c["nsteps"]):
+        Jr, gr = gpu_window(c, precision, K=K, store=0)
+        assert Js == Jr
+        np.testing.assert_array_equal(gs, gr)
+
+
+def test_state_store_kept_for_the_next_window_and_freed(case):
+    """the store stays with the handle across windows (the second window's
+    gradient unchanged) and mode 0 frees it"""
+    c = case
+    with lb.Run(**c["base"], precision="fp32") as r:
+        r.adjoint_set_store(1)
+        r.adjoint_set_obs(c["steps"], c["ox"], c["oy"], c["oT"])
+        _, g1 = r.adjoint_window(c["T0"], c["nsteps"], 8)
+        st = r.adjoint_store()
+        assert st["used_last"] == 1 and st["bytes"] > 0
+        _, g2 = r.adjoint_window(c["T0"], c["nsteps"], 8)
+        np.testing.assert_array_equal(g1, g2)
+        r.adjoint_set_store(0)
+        assert r.adjoint_store()["bytes"] == 0
+        _, g3 = r.adjoint_window(c["T0"], c["nsteps"], 8)
+        assert r.adjoint_store()["used_last"] == 0
+        np.testing.assert_array_equal(g1, g3)
+
+
+@pytest.mark.parametrize("store", [1, 0])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [None, (40, 13)])
+def test_every_pair_kernel_variant_gives_the_same_gradient(case, precision, shape, store):
     """the tiled and the marching two-step kernels, every launch variant, on
-    the 48x24 case and on a grid of partial strips and row groups"""
+    the 48x24 case and on a grid of partial strips and row groups, with the
+    state store and with checkpoints"""
     c = case if shape is None else adjoint_case(seed=9, nx=shape[0], ny=shape[1], nsteps=17, every=3,
                                                 nobs=11)
     grads = []
     for v in range(lb.Run.adjoint_variants()):
         with lb.Run(**c["base"], precision=precision) as r:
+            r.adjoint_set_store(store)
             r.adjoint_set_variant(v)
             r.adjoint_set_obs(c["steps"], c["ox"], c["oy"], c["oT"])
             grads.append(r.adjoint_window(c["T0"], c["nsteps"], 8)[1])
