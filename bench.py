@@ -1376,7 +1376,10 @@ def run_lb_only(args, torch) -> dict:
     return {"mode": "lb-only", "grid": f"{nx}x{ny}", "precision": args.precision,
             "steps": args.steps, "avg_lb_ms": round(avg, 5), "ms_per_step_fused": round(lb_ms / args.steps, 5),
             "node_steps_per_launch": round(spl, 4), "alg_gbs": round(gbs, 1),
-            "mlups": round(nx * ny * args.steps / (ms * 1e3), 1), "launch_shape": shape, "pair_shape": pair}
+            # from the fused launches' own event times (the uninstrumented window's
+            # total can include one-time work after a short warm-up)
+            "mlups": round(nx * ny * args.steps / (lb_ms * 1e3), 1), "window_ms": round(ms, 3),
+            "launch_shape": shape, "pair_shape": pair}
 
 
 def main():
