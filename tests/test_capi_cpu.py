@@ -83,3 +83,10 @@ def test_ensemble_create_rejects_bad_arguments(L):
     empty = (C.c_void_p * 1)(None)
     assert L.lbrb_ensemble_create(empty, 1, C.byref(e)) == -1
     assert L.lbrb_ensemble_nvariants() >= 1
+
+
+def test_adjoint_store_rejects_bad_arguments(L):
+    """the state-store switch of the adjoint window checks its arguments
+    before touching a device"""
+    assert L.lbrb_adjoint_set_store(None, 1) == -1
+    assert L.lbrb_adjoint_get_store(None, None, None, None) == -1
