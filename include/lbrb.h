@@ -305,7 +305,8 @@ LBRB_API int lbrb_adjoint_get_variant(const lbrb_t *h, int *variant);
  * 0: checkpoints every checkpoint_every steps, each segment recomputed during
  *    the backward pass (memory of two segments); frees a store.
  * -1 (the default): the store when it fits in half of the device's free
- *    memory, else checkpoints.
+ *    memory (an earlier window's store counted as free), else checkpoints,
+ *    releasing an earlier window's store first.
  * Both give the same J and gradient, bit for bit.  get_store: the mode, whether
  * the last gradient window stored (1) or recomputed (0), and the store's size. */
 LBRB_API int lbrb_adjoint_set_store(lbrb_t *h, int mode);

@@ -1238,6 +1238,13 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     }
     if (store && (rc = grow(h, &h->adj_store, &h->adj_store_bytes, need))) return rc;
   }
+  if (dJdT0 && !store && h->adj_store) {
+    // a window too long for the store: release an earlier window's store
+    // before the checkpoint buffers are allocated
+    cudaFree(h->adj_store);
+    h->adj_store = nullptr;
+    h->adj_store_bytes = 0;
+  }
   h->adj_store_used = store ? 1 : 0;
   // store mode: one segment of the whole window (no checkpoints), the
   // populations alternating between checkpoint slots 0 and 1 (slot 2 takes
