@@ -127,7 +127,9 @@ LBRB_API int lbrb_get_populations(lbrb_t *h, double *f, double *g, int layout);
 /* Post-stream (pre-collision) populations of the last step, walls applied:
  * what dumpfpre/dumpgpre write (temppart_dump.c:143-232, called at
  * :1702-1710).  Rebuilt from the state before the last step, which the
- * ping-pong layout keeps; any pointer may be NULL. */
+ * ping-pong layout keeps; when the call's last two steps ran in one two-step
+ * launch, that state is first formed again by one step from the state before
+ * the launch (bit-identical).  Any pointer may be NULL. */
 LBRB_API int lbrb_get_poststream(lbrb_t *h, double *f, double *g, int layout);
 /* Moments of the last step (rhopre, upre, vpre, temppre); any pointer may be
  * NULL on get.  The next step's buoyancy uses rho and T (forcingconstructWW,

@@ -422,6 +422,7 @@ int lbrb_set_populations(lbrb_t* h, const double* f, const double* g, int layout
   }
   CK(h, cudaStreamSynchronize(h->stream));
   h->prev_valid = false;
+  h->prev_pair = false;
   return LBRB_OK;
 }
 
@@ -697,18 +698,49 @@ int lbrb_get_launch_shape(const lbrb_t* h, int* shape, int* block, int* min_bloc
 int lbrb_get_poststream(lbrb_t* h, double* f, double* g, int layout) {
   if (!h || (layout != LBRB_LAYOUT_REF_AOS_HALO && layout != LBRB_LAYOUT_SOA))
     return fail(h, LBRB_ERR_ARG, "get_poststream: bad arguments");
-  if (!h->prev_valid)
+  if (!h->prev_valid && !h->prev_pair)
     return fail(h, LBRB_ERR_STATE, "get_poststream: no step since the populations were set");
   CK(h, cudaSetDevice(h->dev));
   const size_t tmp = 2 * NPOP * h->plane * h->esize;
   const size_t cnt = host_pops_count(h, layout), bytes = cnt * sizeof(double);
-  int rc = ensure_big(h, tmp + 2 * bytes);
+  // (a call that ended with a two-step launch: room for the rebuilt state
+  // before its last step and that step's F)
+  const size_t extra = h->prev_valid ? 0 : tmp + h->plane * h->esize;
+  int rc = ensure_big(h, tmp + 2 * bytes + extra);
   if (rc) return rc;
   char* t = (char*)h->big;
   double* st = (double*)(t + tmp);
   const int prev = h->cur ^ 1;
-  if (fp32(h)) CK(h, launch_pull_fp32(make_view<float>(h, prev, h->cur, h->uvcur, 0, 0), h->p.twall, t, t + tmp / 2, h->stream));
-  else CK(h, launch_pull_fp64(make_view<double>(h, prev, h->cur, h->uvcur, 0, 0), h->p.twall, t, t + tmp / 2, h->stream));
+  if (h->prev_valid) {
+    if (fp32(h)) CK(h, launch_pull_fp32(make_view<float>(h, prev, h->cur, h->uvcur, 0, 0), h->p.twall, t, t + tmp / 2, h->stream));
+    else CK(h, launch_pull_fp64(make_view<double>(h, prev, h->cur, h->uvcur, 0, 0), h->p.twall, t, t + tmp / 2, h->stream));
+  } else {
+    // the state before the last step is the first step of the last launch,
+    // taken again from the state before that launch (its populations and F
+    // are still in the other buffer): one single step into scratch, which
+    // equals the two-step launch's first step bit for bit, then the pull
+    char* scr = t + tmp + 2 * bytes;
+    char* scrF = scr + tmp;
+    const int shape = h->lb_shape >= 0 ? h->lb_shape : h->p.launch_shape;
+    auto rebuild = [&](auto zero) -> cudaError_t {
+      using Real = decltype(zero);
+      LBView<Real> V = make_view<Real>(h, prev, h->cur, h->uvcur, 0, 0);
+      V.fdst = (Real*)scr;
+      V.gdst = (Real*)scr + NPOP * h->plane;
+      V.Fout = (Real*)scrF;
+      cudaError_t e;
+      if constexpr (std::is_same<Real, float>::value) e = launch_lb_fp32(V, h->p.twall, shape, h->stream, false);
+      else e = launch_lb_fp64(V, h->p.twall, false, shape, h->stream, false);
+      if (e != cudaSuccess) return e;
+      LBView<Real> P = make_view<Real>(h, prev, h->cur, h->uvcur, 0, 0);
+      P.fsrc = (const Real*)scr;
+      P.gsrc = (const Real*)scr + NPOP * h->plane;
+      if constexpr (std::is_same<Real, float>::value) return launch_pull_fp32(P, h->p.twall, t, t + tmp / 2, h->stream);
+      else return launch_pull_fp64(P, h->p.twall, t, t + tmp / 2, h->stream);
+    };
+    if (fp32(h)) CK(h, rebuild(0.f));
+    else CK(h, rebuild(0.0));
+  }
   if (f) {
     CK(h, launch_pops_out(t, layout, st, fp32(h), h->p.nx, h->p.ny, h->pitch, h->plane, 1.0, h->stream));
     CK(h, cudaMemcpyAsync(f, st, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -780,6 +812,7 @@ int lbrb_step(lbrb_t* h, int n) {
     if (rc) return rc;
     h->slab_gh2_packed = false;
     h->prev_valid = false;
+    h->prev_pair = false;
     if (!own) {
       h->cur ^= 1;
       h->istep += 2;
@@ -927,6 +960,7 @@ int lbrb_step(lbrb_t* h, int n) {
     }
     h->cur = dst;
     h->prev_valid = true;
+    h->prev_pair = false;
     if (write_uv) {
       h->uvprev = h->uvcur;
       h->uvcur = uvn;
@@ -938,16 +972,20 @@ int lbrb_step(lbrb_t* h, int n) {
   // of each.  Step n's T goes to the source buffer T[cur] (its particle
   // records read it there), step n+1's to T[cur ^ 1]; u, v of step n go to
   // the free slot and of step n+1 to the slot of u^{n-2}, as two `one` calls
-  // would rotate them.  The intermediate populations stay in shared memory,
-  // so get_poststream needs the call's last step, which is never in a pair.
-  auto two = [&]() -> int {
+  // would rotate them.  `last`: step n+1 ends the call and also stores rho
+  // and u, v, as `one(true)` does.  The intermediate populations stay in
+  // shared memory; the source buffer and F keep the state before the launch,
+  // from which get_poststream rebuilds step n.
+  auto two = [&](bool last) -> int {
     const int i1 = h->istep + 1, i2 = h->istep + 2;
     const bool parts = h->np > 0;
     const bool rec1 = parts && h->p.noutconfig > 0 && i1 % h->p.noutconfig == 0;
     const bool rec2 = parts && h->p.noutconfig > 0 && i2 % h->p.noutconfig == 0;
     const int src = h->cur, dst = h->cur ^ 1;
     const int A = parts ? 3 - h->uvcur - h->uvprev : h->uvcur;  // u^n
-    const int B = parts ? h->uvprev : h->uvcur;                 // u^{n+1}
+    // u^{n+1}: the slot of u^{n-2}; without particles only the call's last
+    // step stores u, v, in the free slot as one(true) would
+    const int B = parts ? h->uvprev : (last ? 3 - h->uvcur - h->uvprev : h->uvcur);
     const int wuv = parts ? 1 : 0;
     // bilinear nudging: step n's innovations before the launch (into acc2 and
     // the node mask, read inside it), step n+1's after it (T^{n+1} stored)
@@ -967,7 +1005,7 @@ int lbrb_step(lbrb_t* h, int n) {
     }
     {
       const int tm = tmark_begin(h, 0, h->stream);
-      const int rt2 = (rec2 || nud) ? 1 : 0;
+      const int rt2 = last ? 3 : ((rec2 || nud) ? 1 : 0);
       if (f32) {
         LBView<float> V1 = make_view<float>(h, src, dst, A, wuv, rec1 ? 1 : 0);
         V1.T = (float*)h->T[src];
@@ -976,7 +1014,8 @@ int lbrb_step(lbrb_t* h, int n) {
           V1.nmask = h->nmask;
           V1.nacc = reinterpret_cast<const unsigned long long*>(h->acc2);
         }
-        CK(h, launch_pair_fp32(V1, make_view<float>(h, dst, dst, B, wuv, rt2), h->pair_shape, h->stream, pdl_ok));
+        CK(h, launch_pair_fp32(V1, make_view<float>(h, dst, dst, B, wuv || last, rt2), h->pair_shape, h->stream,
+                               pdl_ok));
       } else {
         LBView<double> V1 = make_view<double>(h, src, dst, A, wuv, rec1 ? 1 : 0);
         V1.T = (double*)h->T[src];
@@ -985,7 +1024,8 @@ int lbrb_step(lbrb_t* h, int n) {
           V1.nmask = h->nmask;
           V1.nacc = reinterpret_cast<const unsigned long long*>(h->acc2);
         }
-        CK(h, launch_pair_fp64(V1, make_view<double>(h, dst, dst, B, wuv, rt2), h->pair_shape, h->stream, pdl_ok));
+        CK(h, launch_pair_fp64(V1, make_view<double>(h, dst, dst, B, wuv || last, rt2), h->pair_shape, h->stream,
+                               pdl_ok));
       }
       tmark_end(h, tm, h->stream);
     }
@@ -1022,9 +1062,13 @@ int lbrb_step(lbrb_t* h, int n) {
       }
       h->uvprev = A;
       h->uvcur = B;
+    } else if (last) {
+      h->uvprev = h->uvcur;
+      h->uvcur = B;
     }
     h->cur = dst;
     h->prev_valid = false;
+    h->prev_pair = !nud;
     h->istep = i2;
     return LBRB_OK;
   };
@@ -1116,21 +1160,26 @@ int lbrb_step(lbrb_t* h, int n) {
           }
         }
         h->prev_valid = true;
+        h->prev_pair = false;
         h->istep += GRAPH_STEPS;
         s += GRAPH_STEPS;
         continue;
       }
     }
-    if (!graphs && h->pair_shape >= 0 && step_pairs_ok(h) && n - 1 - s >= 2) {
-      // two steps per launch, never the call's last step; a pair whose
-      // records would not fit in the ring, or whose observations are missing,
-      // runs as single steps (which report the error at the same step)
+    // the call's last step joins a pair when the call's remaining steps
+    // are exactly two and no nudging acts between them (get_poststream
+    // rebuilds it from the state before the pair)
+    const bool last_pair = n - s == 2 && h->p.nudge == LBRB_NUDGE_NONE;
+    if (!graphs && h->pair_shape >= 0 && step_pairs_ok(h) && (n - 1 - s >= 2 || last_pair)) {
+      // two steps per launch; a pair whose records would not fit in the
+      // ring, or whose observations are missing, runs as single steps (which
+      // report the error at the same step)
       int need = 0;
       for (int q = 1; q <= 2; q++)
         need += h->np > 0 && h->p.noutconfig > 0 && (h->istep + q) % h->p.noutconfig == 0;
       const bool obs_ok = h->p.nudge != LBRB_NUDGE_BILINEAR || (obs_row(h->istep + 1) && obs_row(h->istep + 2));
       if (h->rec_head - h->rec_tail + need <= h->p.record_slots && obs_ok) {
-        const int rc = two();
+        const int rc = two(n - s == 2);
         if (rc) return rc;
         s += 2;
         continue;
@@ -1441,6 +1490,7 @@ int lbrb_adjoint_window(lbrb_t* h, const double* T0, int nsteps, int K, double* 
     CK(h, cudaMemcpyAsync(h->pops[h->cur], end_state, popb, cudaMemcpyDeviceToDevice, h->stream));
     CK(h, cudaMemcpyAsync(h->F[h->cur], end_F, plane * es, cudaMemcpyDeviceToDevice, h->stream));
     h->prev_valid = false;
+    h->prev_pair = false;
   }
   if (!dJdT0) {
     CK(h, cudaStreamSynchronize(h->stream));
@@ -2387,7 +2437,7 @@ int lbrb_slab_step(lbrb_t* const* slabs, int n, int nsteps) {
         if (rc) return rc;
       }
     }
-    for (int s = 0; s < n; s++) slabs[s]->prev_valid = false;
+    for (int s = 0; s < n; s++) slabs[s]->prev_valid = false, slabs[s]->prev_pair = false;
     return LBRB_OK;
   };
   for (int it = 0; it < nsteps; it++) {

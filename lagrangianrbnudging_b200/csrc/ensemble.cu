@@ -269,6 +269,7 @@ void advance_members(lbrb_ensemble_t* e, int n, int npairs) {
     h->uvprev = s.uvprev;
     h->istep += n;
     h->prev_valid = true;
+    h->prev_pair = false;
   }
 }
 

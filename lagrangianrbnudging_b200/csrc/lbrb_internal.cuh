@@ -312,6 +312,10 @@ struct Handle {
   void* pops[2] = {nullptr, nullptr};
   int cur = 0;        // buffer holding the current post-collision state
   bool prev_valid = false;  // pops[cur^1] holds the state before the last step
+  // the call ended with a two-step launch without nudging: pops[cur^1] and
+  // F[cur^1] hold the state before that launch (lbrb_get_poststream rebuilds
+  // the state before the last step from them)
+  bool prev_pair = false;
   // scalar fields (Real)
   void* F[2] = {nullptr, nullptr};  // buoyancy for the step after the state in pops[cur] is F[cur]
   int lb_shape = -1;                // launch shape picked by the autotuner (-1: not tuned yet)

@@ -15,7 +15,7 @@ from lagrangianrbnudging_b200 import build
 
 pytestmark = pytest.mark.gpu
 
-CALLS = (1, 2, 5, 8, 31)  # odd and even calls: pairs never take a call's last step
+CALLS = (1, 2, 5, 8, 31)  # odd calls end on a single step, even calls on a pair
 
 
 @pytest.fixture(scope="module", autouse=True)
